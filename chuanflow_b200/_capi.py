@@ -1,0 +1,416 @@
+"""ctypes bindings of include/chuanflow_b200.h."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "libchuanflow_b200.so")
+
+BC = {"fixedValue": 0, "zeroGradient": 1, "fixedGradient": 2, "symmetry": 3, "outlet": 4, "wall": 5,
+      "empty": 6}
+GRAD = {"linear": 0, "corrected": 1, "leastSquares": 2}
+DIV = {"upwind": 0, "linear": 1, "blend": 2}
+PRECOND = {"Jacobi": 0, "DIC": 1}
+
+_f64p = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+
+
+class CfgError(RuntimeError):
+    """A non-zero status from the library, with its message."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class _Schemes(C.Structure):
+    _fields_ = [("div", C.c_int32), ("laplacian_corrected", C.c_int32), ("grad", C.c_int32),
+                ("blend_coeff", C.c_double)]
+
+
+class _Controls(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("continuity_tol", C.c_double), ("pcorr_tol", C.c_double),
+                ("momentum_tol", C.c_double), ("linear_tol", C.c_double), ("linear_max_iter", C.c_int32),
+                ("non_orth_correctors", C.c_int32), ("relax_u", C.c_double), ("relax_p", C.c_double),
+                ("p_relax_start", C.c_double), ("body_force", C.c_double * 3), ("nu", C.c_double),
+                ("p_precond", C.c_int32), ("verbose", C.c_int32), ("p_ref_cell", C.c_int64),
+                ("p_ref_value", C.c_double)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("final_continuity_error", C.c_double),
+                ("final_momentum_residual", C.c_double), ("last_dp", C.c_double),
+                ("last_continuity_corrected", C.c_double), ("u_inner_iterations", C.c_int64),
+                ("p_inner_iterations", C.c_int64), ("diverged", C.c_int32)]
+
+
+class _Report(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("initial_residual", C.c_double),
+                ("final_residual", C.c_double)]
+
+
+_lib = None
+
+
+def lib_path():
+    return _SO
+
+
+def lib():
+    """The loaded library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SO):
+            raise ImportError(f"chuanflow_b200: {_SO} is missing; build it with `make -C chuanflow_b200/csrc`")
+        _lib = C.CDLL(_SO)
+        _lib.cfg_version.restype = C.c_char_p
+        _lib.cfg_last_error.restype = C.c_size_t
+        _lib.cfg_mesh_jitter_interior.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
+        _lib.cfg_mesh_destroy.argtypes = [C.c_void_p]
+        _lib.cfg_ctx_destroy.argtypes = [C.c_void_p]
+        _lib.cfg_set_patch_bc.argtypes = [C.c_void_p, C.c_char, C.c_int32, C.c_int32, _f64p]
+    return _lib
+
+
+def _err():
+    buf = C.create_string_buffer(1024)
+    lib().cfg_last_error(buf, 1024)
+    return buf.value.decode()
+
+
+def _check(rc):
+    if rc != 0:
+        raise CfgError(rc, _err())
+
+
+def _dp(a):
+    return a.ctypes.data_as(_f64p)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_i64p)
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a.reshape(shape) if shape is not None else a
+
+
+# --------------------------------------------------------------------------
+# mesh
+# --------------------------------------------------------------------------
+
+class PolyMesh:
+    """polyMesh held by the library (host addressing + geometry)."""
+
+    def __init__(self, points, face_offsets, face_verts, owner, neighbour, patches):
+        """patches: list of (name, type, start, size)."""
+        pts = _f64(points).reshape(-1, 3)
+        fo = np.ascontiguousarray(face_offsets, np.int64)
+        fv = np.ascontiguousarray(face_verts, np.int64)
+        own = np.ascontiguousarray(owner, np.int64)
+        nbr = np.ascontiguousarray(neighbour, np.int64)
+        names = (C.c_char_p * len(patches))(*[p[0].encode() for p in patches])
+        types = (C.c_char_p * len(patches))(*[p[1].encode() for p in patches])
+        ps = np.array([p[2] for p in patches], np.int64)
+        pz = np.array([p[3] for p in patches], np.int64)
+        h = C.c_void_p()
+        _check(lib().cfg_mesh_create(_dp(pts), C.c_int64(pts.shape[0]), _ip(fo), _ip(fv), C.c_int64(own.size),
+                                     _ip(own), _ip(nbr) if nbr.size else None, C.c_int64(nbr.size),
+                                     C.c_int32(len(patches)), names, types, _ip(ps), _ip(pz), C.byref(h)))
+        self._h = h
+        self._counts()
+
+    @classmethod
+    def block(cls, mn, mx, cells, sides=None):
+        """BlockMesh::create; sides maps xmin..zmax to (name, type)."""
+        order = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
+        sides = sides or {}
+        names = (C.c_char_p * 6)(*[(sides[k][0].encode() if k in sides else None) for k in order])
+        types = (C.c_char_p * 6)(*[(sides[k][1].encode() if k in sides else None) for k in order])
+        mn = _f64(mn)
+        mx = _f64(mx)
+        h = C.c_void_p()
+        _check(lib().cfg_mesh_block(_dp(mn), _dp(mx), C.c_int64(cells[0]), C.c_int64(cells[1]),
+                                    C.c_int64(cells[2]), names, types, C.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self._counts()
+        return self
+
+    def _counts(self):
+        c = np.zeros(5, np.int64)
+        _check(lib().cfg_mesh_counts(self._h, _ip(c)))
+        self.n_points, self.n_cells, self.n_faces, self.n_internal_faces, self.n_patches = (int(x) for x in c)
+        self.patches = []
+        for i in range(self.n_patches):
+            nb = C.create_string_buffer(256)
+            tb = C.create_string_buffer(256)
+            s = C.c_int64()
+            z = C.c_int64()
+            _check(lib().cfg_mesh_patch(self._h, C.c_int32(i), nb, 256, tb, 256, C.byref(s), C.byref(z)))
+            self.patches.append((nb.value.decode(), tb.value.decode(), s.value, z.value))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.cfg_mesh_destroy(h)
+            self._h = None
+
+    @property
+    def n_boundary_faces(self):
+        return self.n_faces - self.n_internal_faces
+
+    def patch_id(self, name):
+        for i, p in enumerate(self.patches):
+            if p[0] == name:
+                return i
+        raise CfgError(4, f"polyMesh: no patch named '{name}'")
+
+    def move_points(self, points):
+        pts = _f64(points).reshape(-1, 3)
+        _check(lib().cfg_mesh_move_points(self._h, _dp(pts), C.c_int64(pts.shape[0])))
+
+    def jitter_interior(self, fraction, seed):
+        _check(lib().cfg_mesh_jitter_interior(self._h, C.c_double(fraction), C.c_uint64(seed)))
+
+    def addressing(self):
+        pts = np.zeros((self.n_points, 3))
+        fo = np.zeros(self.n_faces + 1, np.int64)
+        _check(lib().cfg_mesh_addressing(self._h, None, _ip(fo), None, None, None))
+        fv = np.zeros(int(fo[-1]), np.int64)
+        own = np.zeros(self.n_faces, np.int64)
+        nbr = np.zeros(max(self.n_internal_faces, 1), np.int64)
+        _check(lib().cfg_mesh_addressing(self._h, _dp(pts), _ip(fo), _ip(fv), _ip(own), _ip(nbr)))
+        return {"points": pts, "face_offsets": fo, "face_verts": fv, "owner": own,
+                "neighbour": nbr[:self.n_internal_faces]}
+
+    def geometry(self):
+        N, F = self.n_cells, self.n_faces
+        g = {"V": np.zeros(N), "C": np.zeros((N, 3)), "Cf": np.zeros((F, 3)), "Sf": np.zeros((F, 3)),
+             "magSf": np.zeros(F), "d": np.zeros((F, 3)), "invDist": np.zeros(F)}
+        _check(lib().cfg_mesh_geometry(self._h, *[_dp(g[k]) for k in ("V", "C", "Cf", "Sf", "magSf", "d",
+                                                                        "invDist")]))
+        return g
+
+    def weights(self):
+        ow = np.zeros(max(1, self.n_internal_faces))
+        sk = np.zeros((self.n_faces, 3))
+        _check(lib().cfg_mesh_weights(self._h, _dp(ow), _dp(sk)))
+        return ow, sk
+
+
+# --------------------------------------------------------------------------
+# case
+# --------------------------------------------------------------------------
+
+@dataclass
+class Schemes:
+    """Schemes (src/3d/include/cf/fvm/FvMatrix.h:30-38)."""
+    div: str = "upwind"
+    laplacian: str = "corrected"
+    grad: str = "corrected"
+    blend_coeff: float = 0.9
+
+    def _c(self):
+        return _Schemes(DIV[self.div], int(self.laplacian == "corrected"), GRAD.get(self.grad, 0),
+                        self.blend_coeff)
+
+
+@dataclass
+class SimpleControls:
+    """SimpleControls (src/3d/include/cf/fvm/SimpleSolver.h:13-64) with the
+    reference's defaults, plus the gpu{} settings."""
+    max_iterations: int = 200
+    continuity_tol: float = 1e-6
+    pcorr_tol: float = 0.0
+    momentum_tol: float = 0.0
+    linear_tol: float = 1e-7
+    linear_max_iter: int = 2000
+    non_orth_correctors: int = 2
+    relax_u: float = 0.7
+    relax_p: float = 0.3
+    p_relax_start: float = 0.0
+    body_force: tuple = (0.0, 0.0, 0.0)
+    nu: float = 1e-4
+    p_preconditioner: str = "Jacobi"
+    verbose: bool = False
+    p_ref_cell: int = -1
+    p_ref_value: float = 0.0
+
+    def _c(self):
+        c = _Controls()
+        c.max_iterations = self.max_iterations
+        c.continuity_tol = self.continuity_tol
+        c.pcorr_tol = self.pcorr_tol
+        c.momentum_tol = self.momentum_tol
+        c.linear_tol = self.linear_tol
+        c.linear_max_iter = self.linear_max_iter
+        c.non_orth_correctors = self.non_orth_correctors
+        c.relax_u = self.relax_u
+        c.relax_p = self.relax_p
+        c.p_relax_start = self.p_relax_start
+        for i in range(3):
+            c.body_force[i] = self.body_force[i]
+        c.nu = self.nu
+        c.p_precond = PRECOND[self.p_preconditioner]
+        c.verbose = int(self.verbose)
+        c.p_ref_cell = self.p_ref_cell
+        c.p_ref_value = self.p_ref_value
+        return c
+
+
+@dataclass
+class SimpleResult:
+    iterations: int
+    converged: bool
+    final_continuity_error: float
+    final_momentum_residual: float
+    last_dp: float
+    last_continuity_corrected: float
+    u_inner_iterations: int
+    p_inner_iterations: int
+    diverged: bool
+
+
+@dataclass
+class SolverReport:
+    iterations: int
+    converged: bool
+    initial_residual: float
+    final_residual: float
+
+
+class SimpleCase:
+    """U, p, phi and their boundary conditions on one device."""
+
+    def __init__(self, mesh: PolyMesh, device: int = 0, schemes: Schemes | None = None):
+        self.mesh = mesh
+        h = C.c_void_p()
+        _check(lib().cfg_ctx_create(mesh._h, C.c_int32(device), None, C.byref(h)))
+        self._h = h
+        self.set_schemes(schemes or Schemes())
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.cfg_ctx_destroy(h)
+            self._h = None
+
+    def _patch(self, patch):
+        return patch if isinstance(patch, int) else self.mesh.patch_id(patch)
+
+    def set_patch_bc(self, field_name, patch, bc_type, value=0.0):
+        """volVectorField / volScalarField ::setPatchValue."""
+        v = _f64(np.atleast_1d(value))
+        if field_name == "U" and v.size != 3:
+            v = _f64(np.zeros(3) + v[0])
+        _check(lib().cfg_set_patch_bc(self._h, field_name.encode(), self._patch(patch), BC[bc_type], _dp(v)))
+
+    def set_face_values_U(self, faces, values):
+        f = np.ascontiguousarray(faces, np.int64)
+        v = _f64(values).reshape(-1, 3)
+        _check(lib().cfg_set_face_values_U(self._h, C.c_int64(f.size), _ip(f), _dp(v)))
+
+    def set_schemes(self, schemes: Schemes):
+        self.schemes = schemes
+        s = schemes._c()
+        _check(lib().cfg_set_schemes(self._h, C.byref(s)))
+
+    def upload(self, U=None, p=None, phi=None):
+        _check(lib().cfg_fields_upload(self._h, _dp(_f64(U)) if U is not None else None,
+                                       _dp(_f64(p)) if p is not None else None,
+                                       _dp(_f64(phi)) if phi is not None else None))
+
+    def download(self):
+        U = np.zeros((self.mesh.n_cells, 3))
+        p = np.zeros(self.mesh.n_cells)
+        phi = np.zeros(self.mesh.n_faces)
+        _check(lib().cfg_fields_download(self._h, _dp(U), _dp(p), _dp(phi)))
+        return U, p, phi
+
+    def init_flux(self, u0=None):
+        _check(lib().cfg_fields_init_flux(self._h, _dp(_f64(u0)) if u0 is not None else None))
+
+    def solve(self, controls: SimpleControls) -> SimpleResult:
+        """solveIncompressibleSimple on the device fields."""
+        r = _Result()
+        c = controls._c()
+        _check(lib().cfg_simple_iterate(self._h, C.byref(c), C.byref(r)))
+        return SimpleResult(r.iterations, bool(r.converged), r.final_continuity_error,
+                            r.final_momentum_residual, r.last_dp, r.last_continuity_corrected,
+                            r.u_inner_iterations, r.p_inner_iterations, bool(r.diverged))
+
+    def last_timing(self):
+        ms = np.zeros(8)
+        n = C.c_int64()
+        _check(lib().cfg_last_timing(self._h, _dp(ms), C.byref(n)))
+        return ms, n.value
+
+    # ---- diagnostics ----
+    def probe_equations(self, controls: SimpleControls, xprobe):
+        N, F = self.mesh.n_cells, self.mesh.n_faces
+        sizes = [("gradPn", 3 * N), ("U_diag", 3 * N), ("U_h0", 3 * N), ("U_h1", 3 * N), ("rAUf", F),
+                 ("divPhi", N), ("contErr", 1), ("p_diag", N), ("p_h0", N), ("p_h1", N), ("gradPFull", 3 * N),
+                 ("phiCorrected", F)]
+        out = np.zeros(sum(s for _, s in sizes))
+        c = controls._c()
+        _check(lib().cfg_probe_equations(self._h, C.byref(c), _dp(_f64(xprobe)), _dp(out)))
+        res, o = {}, 0
+        for k, s in sizes:
+            res[k] = out[o:o + s].copy()
+            o += s
+        for k in ("gradPn", "gradPFull"):
+            res[k] = res[k].reshape(3, N).T.copy()
+        for k in ("U_diag", "U_h0", "U_h1"):
+            res[k] = res[k].reshape(3, N)
+        return res
+
+    def gradient(self, data, bvals, scheme, vol_quirk=False):
+        out = np.zeros((self.mesh.n_cells, 3))
+        _check(lib().cfg_gradient(self._h, _dp(_f64(data)), _dp(_f64(bvals)), C.c_int32(GRAD.get(scheme, 0)),
+                                  C.c_int32(int(vol_quirk)), _dp(out)))
+        return out
+
+
+# --------------------------------------------------------------------------
+# linear solvers and the case-file runner
+# --------------------------------------------------------------------------
+
+def _sparse(method, row_start, cols, vals, b, x0, tol, max_iter, device):
+    rs = np.ascontiguousarray(row_start, np.int64)
+    cl = np.ascontiguousarray(cols, np.int64)
+    vl = _f64(vals)
+    x = np.array(x0, dtype=np.float64, copy=True)
+    r = _Report()
+    _check(lib().cfg_sparse_solve(None, C.c_int32(device), C.c_int64(rs.size - 1), _ip(rs), _ip(cl), _dp(vl),
+                                  _dp(_f64(b)), _dp(x), C.c_double(tol), C.c_int32(max_iter), C.c_int32(method),
+                                  C.byref(r)))
+    return x, SolverReport(r.iterations, bool(r.converged), r.initial_residual, r.final_residual)
+
+
+def solve_cg(row_start, cols, vals, b, x0, tol, max_iter, device=0):
+    """solveCG on a CSR matrix (Matrix.cpp:153-222)."""
+    return _sparse(0, row_start, cols, vals, b, x0, tol, max_iter, device)
+
+
+def solve_bicgstab(row_start, cols, vals, b, x0, tol, max_iter, device=0):
+    """solveBiCGStab on a CSR matrix (Matrix.cpp:224-319)."""
+    return _sparse(1, row_start, cols, vals, b, x0, tol, max_iter, device)
+
+
+def run_case_file(path, device=0):
+    """A chflow-simple-foam case file end to end; returns (result, U, p, phi)."""
+    counts = np.zeros(5, np.int64)
+    r = _Result()
+    # two calls: the first sizes the fields
+    _check(lib().cfg_run_case_file(str(path).encode(), C.c_int32(device), C.byref(r), _ip(counts), None, None,
+                                   None))
+    return SimpleResult(r.iterations, bool(r.converged), r.final_continuity_error, r.final_momentum_residual,
+                        r.last_dp, r.last_continuity_corrected, r.u_inner_iterations, r.p_inner_iterations,
+                        bool(r.diverged)), counts

@@ -1,0 +1,536 @@
+// The extern "C" boundary: status codes, the per-thread error message, and
+// the case-file runner.
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "cfg_internal.h"
+#include "ctx.h"
+#include "dict.h"
+
+namespace
+{
+
+thread_local std::string g_lastError;
+
+template <class F>
+int guard(F&& f)
+{
+    try
+    {
+        f();
+        return CFG_OK;
+    }
+    catch (const cfg::Error& e)
+    {
+        g_lastError = e.what();
+        return e.code;
+    }
+    catch (const std::bad_alloc&)
+    {
+        g_lastError = "out of host memory";
+        return CFG_ENOMEM;
+    }
+    catch (const std::exception& e)
+    {
+        g_lastError = e.what();
+        return CFG_EINVAL;
+    }
+}
+
+void need(bool ok, const char* what)
+{
+    if (!ok) cfg::fail(CFG_EINVAL, what);
+}
+
+int bcFromName(const std::string& s)
+{
+    if (s == "fixedValue") return CFG_BC_FIXED_VALUE;
+    if (s == "zeroGradient") return CFG_BC_ZERO_GRADIENT;
+    if (s == "fixedGradient") return CFG_BC_FIXED_GRADIENT;
+    if (s == "symmetry") return CFG_BC_SYMMETRY;
+    if (s == "outlet") return CFG_BC_OUTLET;
+    if (s == "wall") return CFG_BC_WALL;
+    if (s == "empty") return CFG_BC_EMPTY;
+    cfg::fail(CFG_ESETUP, "unknown patch bc type '" + s + "'");
+}
+
+uint64_t splitmix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t cfg_last_error(char* buf, size_t size)
+{
+    if (buf && size)
+    {
+        const size_t n = std::min(size - 1, g_lastError.size());
+        std::memcpy(buf, g_lastError.data(), n);
+        buf[n] = 0;
+    }
+    return g_lastError.size();
+}
+
+const char* cfg_version(void) { return "chuanflow_b200 0.1"; }
+
+int cfg_mesh_create(const double* points, int64_t nP, const int64_t* faceOffsets, const int64_t* faceVerts,
+                    int64_t nF, const int64_t* owner, const int64_t* neighbour, int64_t nInt, int32_t nPatch,
+                    const char* const* names, const char* const* types, const int64_t* pStart,
+                    const int64_t* pSize, cfg_mesh** out)
+{
+    return guard([&] {
+        need(out && points && faceOffsets && faceVerts && owner && nP > 0 && nF > 0, "cfg_mesh_create: null argument");
+        need(nInt >= 0 && nInt <= nF && (nInt == 0 || neighbour), "cfg_mesh_create: bad internal face count");
+        auto m = std::make_unique<cfg_mesh>();
+        m->m.points.resize(nP);
+        for (int64_t i = 0; i < nP; ++i) m->m.points[i] = {points[3 * i], points[3 * i + 1], points[3 * i + 2]};
+        m->m.faceOffsets.assign(faceOffsets, faceOffsets + nF + 1);
+        need(faceOffsets[0] == 0, "cfg_mesh_create: face_offsets[0] must be 0");
+        m->m.faceVerts.assign(faceVerts, faceVerts + faceOffsets[nF]);
+        m->m.owner.assign(owner, owner + nF);
+        m->m.neighbour.assign(neighbour, neighbour + nInt);
+        for (int32_t i = 0; i < nPatch; ++i)
+        {
+            cfg::Mesh::Patch p;
+            p.name = names && names[i] ? names[i] : "patch" + std::to_string(i);
+            p.type = types && types[i] ? types[i] : "wall";
+            p.start = pStart[i];
+            p.size = pSize[i];
+            m->m.patches.push_back(p);
+        }
+        m->m.finish();
+        *out = m.release();
+    });
+}
+
+int cfg_mesh_block(const double mn[3], const double mx[3], int64_t nx, int64_t ny, int64_t nz,
+                   const char* const* sideNames, const char* const* sideTypes, cfg_mesh** out)
+{
+    return guard([&] {
+        need(out && mn && mx, "cfg_mesh_block: null argument");
+        // BlockSides defaults (src/3d/include/cf/fvm/BlockMesh.h:13-21)
+        std::vector<std::string> names = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+        std::vector<std::string> types = {"wall", "wall", "wall", "wall", "symmetry", "symmetry"};
+        for (int s = 0; s < 6; ++s)
+        {
+            if (sideNames && sideNames[s]) names[s] = sideNames[s];
+            if (sideTypes && sideTypes[s]) types[s] = sideTypes[s];
+        }
+        auto m = std::make_unique<cfg_mesh>();
+        m->m = cfg::blockMesh({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, nx, ny, nz, names, types);
+        *out = m.release();
+    });
+}
+
+int cfg_mesh_move_points(cfg_mesh* mesh, const double* points, int64_t nP)
+{
+    return guard([&] {
+        need(mesh && points, "cfg_mesh_move_points: null argument");
+        if (nP != static_cast<int64_t>(mesh->m.points.size()))
+            cfg::fail(CFG_EMESH, "polyMesh::movePoints: point count changed; topology is fixed in ALE");
+        for (int64_t i = 0; i < nP; ++i) mesh->m.points[i] = {points[3 * i], points[3 * i + 1], points[3 * i + 2]};
+        mesh->m.calcGeometry();
+    });
+}
+
+int cfg_mesh_jitter_interior(cfg_mesh* mesh, double fraction, uint64_t seed)
+{
+    return guard([&] {
+        need(mesh, "cfg_mesh_jitter_interior: null mesh");
+        cfg::Mesh& M = mesh->m;
+        if (M.bnx < 0) cfg::fail(CFG_EINVAL, "cfg_mesh_jitter_interior: mesh did not come from a block");
+        const int64_t nx = M.bnx, ny = M.bny, nz = M.bnz;
+        const double h[3] = {(M.bmax.x - M.bmin.x) / static_cast<double>(nx),
+                             (M.bmax.y - M.bmin.y) / static_cast<double>(ny),
+                             (M.bmax.z - M.bmin.z) / static_cast<double>(nz)};
+        const uint64_t s0 = seed * 0x100000001B3ULL;
+        for (int64_t k = 1; k < nz; ++k)
+            for (int64_t j = 1; j < ny; ++j)
+                for (int64_t i = 1; i < nx; ++i)
+                {
+                    const int64_t pidx = i + (nx + 1) * (j + (ny + 1) * k);
+                    double* c[3] = {&M.points[pidx].x, &M.points[pidx].y, &M.points[pidx].z};
+                    for (int a = 0; a < 3; ++a)
+                    {
+                        const uint64_t r = splitmix64(s0 ^ (static_cast<uint64_t>(pidx) * 3ULL + static_cast<uint64_t>(a)));
+                        const double u = static_cast<double>(r >> 11) * (1.0 / 9007199254740992.0);
+                        *c[a] += (u * 2.0 - 1.0) * fraction * h[a];
+                    }
+                }
+        M.calcGeometry();
+    });
+}
+
+void cfg_mesh_destroy(cfg_mesh* mesh) { delete mesh; }
+
+int cfg_mesh_counts(const cfg_mesh* mesh, int64_t counts[5])
+{
+    return guard([&] {
+        need(mesh && counts, "cfg_mesh_counts: null argument");
+        counts[0] = static_cast<int64_t>(mesh->m.points.size());
+        counts[1] = mesh->m.nCells;
+        counts[2] = mesh->m.nFaces();
+        counts[3] = mesh->m.nInternal();
+        counts[4] = static_cast<int64_t>(mesh->m.patches.size());
+    });
+}
+
+int cfg_mesh_patch(const cfg_mesh* mesh, int32_t patch, char* name, size_t nameSize, char* type, size_t typeSize,
+                   int64_t* start, int64_t* size)
+{
+    return guard([&] {
+        need(mesh && patch >= 0 && patch < static_cast<int32_t>(mesh->m.patches.size()), "cfg_mesh_patch: bad patch");
+        const auto& p = mesh->m.patches[patch];
+        if (name && nameSize) std::snprintf(name, nameSize, "%s", p.name.c_str());
+        if (type && typeSize) std::snprintf(type, typeSize, "%s", p.type.c_str());
+        if (start) *start = p.start;
+        if (size) *size = p.size;
+    });
+}
+
+int cfg_mesh_patch_id(const cfg_mesh* mesh, const char* name)
+{
+    if (!mesh || !name) return -1;
+    for (size_t i = 0; i < mesh->m.patches.size(); ++i)
+        if (mesh->m.patches[i].name == name) return static_cast<int>(i);
+    g_lastError = std::string("polyMesh: no patch named '") + name + "'";
+    return -1;
+}
+
+int cfg_mesh_addressing(const cfg_mesh* mesh, double* points, int64_t* faceOffsets, int64_t* faceVerts,
+                        int64_t* owner, int64_t* neighbour)
+{
+    return guard([&] {
+        need(mesh != nullptr, "cfg_mesh_addressing: null mesh");
+        const cfg::Mesh& M = mesh->m;
+        if (points)
+            for (size_t i = 0; i < M.points.size(); ++i)
+            {
+                points[3 * i] = M.points[i].x;
+                points[3 * i + 1] = M.points[i].y;
+                points[3 * i + 2] = M.points[i].z;
+            }
+        if (faceOffsets) std::memcpy(faceOffsets, M.faceOffsets.data(), M.faceOffsets.size() * sizeof(int64_t));
+        if (faceVerts) std::memcpy(faceVerts, M.faceVerts.data(), M.faceVerts.size() * sizeof(int64_t));
+        if (owner) std::memcpy(owner, M.owner.data(), M.owner.size() * sizeof(int64_t));
+        if (neighbour && !M.neighbour.empty()) std::memcpy(neighbour, M.neighbour.data(), M.neighbour.size() * sizeof(int64_t));
+    });
+}
+
+int cfg_mesh_geometry(const cfg_mesh* mesh, double* V, double* C, double* Cf, double* Sf, double* magSf, double* d,
+                      double* invDist)
+{
+    return guard([&] {
+        need(mesh != nullptr, "cfg_mesh_geometry: null mesh");
+        const cfg::Mesh& M = mesh->m;
+        auto vec = [](double* out, const std::vector<cfg::Vec>& v) {
+            if (!out) return;
+            for (size_t i = 0; i < v.size(); ++i)
+            {
+                out[3 * i] = v[i].x;
+                out[3 * i + 1] = v[i].y;
+                out[3 * i + 2] = v[i].z;
+            }
+        };
+        if (V) std::memcpy(V, M.V.data(), M.V.size() * sizeof(double));
+        vec(C, M.C);
+        vec(Cf, M.Cf);
+        vec(Sf, M.Sf);
+        if (magSf) std::memcpy(magSf, M.magSf.data(), M.magSf.size() * sizeof(double));
+        vec(d, M.d);
+        if (invDist) std::memcpy(invDist, M.invDist.data(), M.invDist.size() * sizeof(double));
+    });
+}
+
+int cfg_mesh_weights(const cfg_mesh* mesh, double* ow, double* skew)
+{
+    return guard([&] {
+        need(mesh != nullptr, "cfg_mesh_weights: null mesh");
+        const auto w = mesh->m.ownerWeights();
+        if (ow) std::memcpy(ow, w.data(), w.size() * sizeof(double));
+        if (skew)
+        {
+            const auto s = mesh->m.skewVectors(w);
+            for (size_t i = 0; i < s.size(); ++i)
+            {
+                skew[3 * i] = s[i].x;
+                skew[3 * i + 1] = s[i].y;
+                skew[3 * i + 2] = s[i].z;
+            }
+        }
+    });
+}
+
+int cfg_mesh_device_order(const cfg_mesh* mesh, int64_t* newToOld)
+{
+    return guard([&] {
+        need(mesh && newToOld, "cfg_mesh_device_order: null argument");
+        for (int64_t c = 0; c < mesh->m.nCells; ++c) newToOld[c] = c;
+    });
+}
+
+int cfg_ctx_create(const cfg_mesh* mesh, int32_t device, void* stream, cfg_ctx** out)
+{
+    return guard([&] {
+        need(mesh && out, "cfg_ctx_create: null argument");
+        auto c = std::make_unique<cfg_ctx>();
+        c->c = std::make_unique<cfg::Ctx>(mesh->m, device, static_cast<cudaStream_t>(stream));
+        *out = c.release();
+    });
+}
+
+void cfg_ctx_destroy(cfg_ctx* ctx) { delete ctx; }
+
+int cfg_set_patch_bc(cfg_ctx* ctx, char field, int32_t patch, int32_t type, const double* value)
+{
+    return guard([&] {
+        need(ctx != nullptr, "cfg_set_patch_bc: null context");
+        ctx->c->setPatchBC(field, patch, type, value);
+    });
+}
+
+int cfg_set_face_values_U(cfg_ctx* ctx, int64_t n, const int64_t* faces, const double* values)
+{
+    return guard([&] {
+        need(ctx && (n == 0 || (faces && values)), "cfg_set_face_values_U: null argument");
+        ctx->c->setFaceValuesU(n, faces, values);
+    });
+}
+
+int cfg_clear_face_values_U(cfg_ctx* ctx)
+{
+    return guard([&] {
+        need(ctx != nullptr, "null context");
+        ctx->c->clearFaceValuesU();
+    });
+}
+
+int cfg_set_schemes(cfg_ctx* ctx, const cfg_schemes* s)
+{
+    return guard([&] {
+        need(ctx && s, "cfg_set_schemes: null argument");
+        need(s->div >= 0 && s->div <= 2 && s->grad >= 0 && s->grad <= 2, "cfg_set_schemes: unknown scheme");
+        ctx->c->setSchemes(*s);
+    });
+}
+
+int cfg_fields_upload(cfg_ctx* ctx, const double* U, const double* p, const double* phi)
+{
+    return guard([&] {
+        need(ctx != nullptr, "null context");
+        ctx->c->upload(U, p, phi);
+    });
+}
+
+int cfg_fields_download(cfg_ctx* ctx, double* U, double* p, double* phi)
+{
+    return guard([&] {
+        need(ctx != nullptr, "null context");
+        ctx->c->download(U, p, phi);
+    });
+}
+
+int cfg_fields_init_flux(cfg_ctx* ctx, const double* u0)
+{
+    return guard([&] {
+        need(ctx != nullptr, "null context");
+        ctx->c->initFlux(u0);
+    });
+}
+
+int cfg_simple_iterate(cfg_ctx* ctx, const cfg_simple_controls* ctl, cfg_simple_result* res)
+{
+    return guard([&] {
+        need(ctx && ctl && res, "cfg_simple_iterate: null argument");
+        need(ctl->linear_max_iter >= 0 && ctl->max_iterations >= 0, "cfg_simple_iterate: negative iteration limit");
+        ctx->c->iterate(*ctl, *res);
+    });
+}
+
+int cfg_last_timing(const cfg_ctx* ctx, double ms[8], int64_t* launches)
+{
+    return guard([&] {
+        need(ctx && ms, "cfg_last_timing: null argument");
+        for (int i = 0; i < 8; ++i) ms[i] = ctx->c->lastMs[i];
+        if (launches) *launches = ctx->c->lastLaunches;
+    });
+}
+
+int cfg_sparse_solve(const cfg_ctx* ctx, int32_t device, int64_t n, const int64_t* rs, const int64_t* cols,
+                     const double* vals, const double* b, double* x, double tol, int32_t maxIter, int32_t method,
+                     cfg_solver_report* rep)
+{
+    (void)ctx;
+    return guard([&] {
+        need(rs && cols && vals && b && x && rep, "cfg_sparse_solve: null argument");
+        need(method == CFG_SOLVE_CG || method == CFG_SOLVE_BICGSTAB, "cfg_sparse_solve: unknown method");
+        cfg::Ctx::sparseSolve(device, n, rs, cols, vals, b, x, tol, maxIter, method, rep);
+    });
+}
+
+/* test diagnostics (not part of the reference surface) */
+int cfg_probe_equations(cfg_ctx* ctx, const cfg_simple_controls* ctl, const double* xprobe, double* out)
+{
+    return guard([&] {
+        need(ctx && ctl && xprobe && out, "cfg_probe_equations: null argument");
+        ctx->c->probeEquations(*ctl, xprobe, out);
+    });
+}
+
+int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t scheme, int32_t volQuirk, double* out)
+{
+    return guard([&] {
+        need(ctx && data && bvals && out, "cfg_gradient: null argument");
+        ctx->c->gradient(data, bvals, scheme, volQuirk, out);
+    });
+}
+
+int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* result, int64_t counts[5], double* U,
+                      double* p, double* phi)
+{
+    return guard([&] {
+        need(path && result, "cfg_run_case_file: null argument");
+        const cfg::Dict d = cfg::Dict::parseFile(path);
+        // mesh: block{} (BlockMesh::fromDict, blockMesh.cpp:191-223)
+        if (!d.has("block")) cfg::fail(CFG_ESETUP, "case: only block {} meshes are read by cfg_run_case_file");
+        const cfg::Dict& b = d.dict("block");
+        const auto mn = b.numbers("min"), mx = b.numbers("max"), nc = b.numbers("cells");
+        if (mn.size() != 3 || mx.size() != 3 || nc.size() != 3)
+            cfg::fail(CFG_ESETUP, "blockMesh: min/max/cells need 3 values each");
+        const char* keys[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+        std::vector<std::string> names = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+        std::vector<std::string> types = {"wall", "wall", "wall", "wall", "symmetry", "symmetry"};
+        for (int s = 0; s < 6; ++s)
+            if (b.has(keys[s]))
+            {
+                const cfg::Dict& sd = b.dict(keys[s]);
+                names[s] = sd.wordOr("name", keys[s]);
+                types[s] = sd.wordOr("type", "wall");
+            }
+        cfg::Mesh M = cfg::blockMesh({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, static_cast<int64_t>(nc[0]),
+                                     static_cast<int64_t>(nc[1]), static_cast<int64_t>(nc[2]), names, types);
+        const int32_t dev = device;
+        cfg::Ctx ctx(M, dev, nullptr);
+        // patches{} (simpleFoamApp.cpp:54-91)
+        if (d.has("patches"))
+        {
+            const cfg::Dict& ps = d.dict("patches");
+            for (const auto& name : ps.keys())
+            {
+                const cfg::Dict& pd = ps.dict(name);
+                int patch = -1;
+                for (size_t i = 0; i < M.patches.size(); ++i)
+                    if (M.patches[i].name == name) patch = static_cast<int>(i);
+                if (patch < 0) cfg::fail(CFG_ESETUP, "polyMesh: no patch named '" + name + "'");
+                if (pd.has("U"))
+                {
+                    const auto ul = pd.numbers("U");
+                    ctx.setPatchBC('U', patch, bcFromName(pd.wordOr("UType", "fixedValue")), ul.data());
+                }
+                else
+                {
+                    const bool isWall = M.patches[patch].type == "wall";
+                    const double z[3] = {0, 0, 0};
+                    ctx.setPatchBC('U', patch, isWall ? CFG_BC_FIXED_VALUE : bcFromName(pd.wordOr("UType", "zeroGradient")), z);
+                }
+                if (pd.has("p"))
+                {
+                    const double v = pd.number("p");
+                    ctx.setPatchBC('p', patch, bcFromName(pd.wordOr("pType", "fixedValue")), &v);
+                }
+                else
+                {
+                    const double z = 0;
+                    ctx.setPatchBC('p', patch, CFG_BC_ZERO_GRADIENT, &z);
+                }
+            }
+        }
+        // initial flux and optional initial{U} (simpleFoamApp.cpp:93-95, caseInit.h:18-31)
+        if (d.has("initial") && d.dict("initial").has("U"))
+        {
+            const auto u0 = d.dict("initial").numbers("U");
+            ctx.initFlux(nullptr);
+            ctx.initFlux(u0.data());
+        }
+        else
+        {
+            ctx.initFlux(nullptr);
+        }
+        // schemes{} (fvMatrix.cpp:148-160)
+        cfg_schemes sc{CFG_DIV_UPWIND, 1, CFG_GRAD_CORRECTED, 0.9};
+        if (d.has("schemes"))
+        {
+            const cfg::Dict& s = d.dict("schemes");
+            const std::string div = s.wordOr("div", "upwind");
+            sc.div = div == "linear" ? CFG_DIV_LINEAR : (div == "blend" ? CFG_DIV_BLEND : CFG_DIV_UPWIND);
+            sc.laplacian_corrected = s.wordOr("laplacian", "corrected") == "corrected";
+            const std::string g = s.wordOr("grad", "corrected");
+            sc.grad = g == "corrected" ? CFG_GRAD_CORRECTED : (g == "leastSquares" ? CFG_GRAD_LEAST_SQUARES : CFG_GRAD_LINEAR);
+            sc.blend_coeff = s.numberOr("blendCoeff", 0.9);
+        }
+        ctx.setSchemes(sc);
+        // simple{} (SimpleSolver.h:13-64 defaults; simpleFoamApp.cpp:115-132,
+        // linearTol/linearMaxIter as multiCoupledApp.cpp:41-57 reads them)
+        cfg_simple_controls c{};
+        c.p_ref_cell = -1;
+        c.max_iterations = 200;
+        c.continuity_tol = 1e-6;
+        c.linear_tol = 1e-7;
+        c.linear_max_iter = 2000;
+        c.non_orth_correctors = 2;
+        c.relax_u = 0.7;
+        c.relax_p = 0.3;
+        c.nu = d.number("nu");
+        if (d.has("simple"))
+        {
+            const cfg::Dict& s = d.dict("simple");
+            c.max_iterations = static_cast<int32_t>(s.numberOr("maxIterations", c.max_iterations));
+            c.continuity_tol = s.numberOr("continuityTol", c.continuity_tol);
+            c.pcorr_tol = s.numberOr("pcorrTol", c.pcorr_tol);
+            c.relax_u = s.numberOr("relaxU", c.relax_u);
+            c.relax_p = s.numberOr("relaxP", c.relax_p);
+            c.p_relax_start = s.numberOr("pRelaxStart", c.p_relax_start);
+            c.non_orth_correctors = static_cast<int32_t>(s.numberOr("nonOrthCorrectors", c.non_orth_correctors));
+            c.momentum_tol = s.numberOr("momentumTol", c.momentum_tol);
+            c.linear_tol = s.numberOr("linearTol", c.linear_tol);
+            c.linear_max_iter = static_cast<int32_t>(s.numberOr("linearMaxIter", c.linear_max_iter));
+            if (s.has("force"))
+            {
+                const auto f = s.numbers("force");
+                for (int i = 0; i < 3; ++i) c.body_force[i] = f[i];
+            }
+        }
+        if (d.has("gpu"))
+        {
+            const cfg::Dict& g = d.dict("gpu");
+            c.p_precond = g.wordOr("pPreconditioner", "Jacobi") == "DIC" ? CFG_PRECOND_DIC : CFG_PRECOND_JACOBI;
+            c.p_ref_cell = static_cast<int64_t>(g.numberOr("pRefCell", -1));
+            c.p_ref_value = g.numberOr("pRefValue", 0.0);
+            c.verbose = static_cast<int32_t>(g.numberOr("verbose", 1));
+        }
+        else
+        {
+            c.verbose = 1;
+        }
+        ctx.iterate(c, *result);
+        if (counts)
+        {
+            counts[0] = static_cast<int64_t>(M.points.size());
+            counts[1] = M.nCells;
+            counts[2] = M.nFaces();
+            counts[3] = M.nInternal();
+            counts[4] = static_cast<int64_t>(M.patches.size());
+        }
+        ctx.download(U, p, phi);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+// Internal declarations shared by the host C++ and the CUDA sources of
+// libchuanflow_b200.so.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "chuanflow_b200.h"
+
+namespace cfg
+{
+
+/// Error carried to the C boundary as a status code + message.
+struct Error : std::runtime_error
+{
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+struct Vec
+{
+    double x = 0, y = 0, z = 0;
+};
+
+inline Vec operator+(const Vec& a, const Vec& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline Vec operator-(const Vec& a, const Vec& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline Vec operator*(const Vec& a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline Vec operator/(const Vec& a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+
+/// Host mesh: the reference polyMesh's addressing plus its geometry,
+/// computed in the reference's operation order (polyMesh.cpp:83-288).
+struct Mesh
+{
+    std::vector<Vec> points;
+    std::vector<int64_t> faceOffsets, faceVerts, owner, neighbour;
+    struct Patch
+    {
+        std::string name, type;
+        int64_t start = 0, size = 0;
+    };
+    std::vector<Patch> patches;
+    int64_t nCells = 0;
+
+    // block-structured origin (for the interior jitter helper); nx < 0 if none
+    int64_t bnx = -1, bny = -1, bnz = -1;
+    Vec bmin, bmax;
+
+    // geometry
+    std::vector<double> V;
+    std::vector<Vec> C, Cf, Sf, d;
+    std::vector<double> magSf, invDist;
+    std::vector<int64_t> facePatch;
+
+    int64_t nFaces() const { return static_cast<int64_t>(owner.size()); }
+    int64_t nInternal() const { return static_cast<int64_t>(neighbour.size()); }
+    int64_t nBoundary() const { return nFaces() - nInternal(); }
+
+    void finish();       // addressing checks + geometry
+    void calcGeometry();
+    std::vector<double> ownerWeights() const;  // size max(1, nInt)
+    std::vector<Vec> skewVectors(const std::vector<double>& ow) const;
+};
+
+Mesh blockMesh(const Vec& mn, const Vec& mx, int64_t nx, int64_t ny, int64_t nz,
+               const std::vector<std::string>& names, const std::vector<std::string>& types);
+
+}  // namespace cfg
+
+struct cfg_mesh
+{
+    cfg::Mesh m;
+};

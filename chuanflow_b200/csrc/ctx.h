@@ -1,0 +1,138 @@
+// The per-case device context (host declarations; kernels in simple.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "cfg_internal.h"
+#include "dev_types.h"
+
+namespace cfg
+{
+
+/// Device state of one Jacobi-PCG or 3-component BiCGStab solve.
+struct SolveState
+{
+    double tol;
+    int maxIter;
+    int nComp;
+    // per component
+    double bnorm[3], init[3], fin[3];
+    double rho[3], alpha[3], omega[3], beta[3];
+    double rz[3], pAp[3];
+    double sMax[3];
+    int it[3], done[3], conv[3], special[3];
+    int allDone;
+    unsigned int ticket[8];
+};
+
+struct Timing
+{
+    cudaEvent_t ev[16];
+    double ms[8];
+    int64_t launches;
+};
+
+class Ctx
+{
+public:
+    Ctx(const Mesh& mesh, int device, cudaStream_t stream);
+    ~Ctx();
+
+    // boundary conditions and schemes
+    void setPatchBC(char field, int patch, int type, const double* value);
+    void setFaceValuesU(int64_t n, const int64_t* faces, const double* values);
+    void clearFaceValuesU();
+    void setSchemes(const cfg_schemes& s) { schemes_ = s; }
+
+    void upload(const double* U, const double* p, const double* phi);
+    void download(double* U, double* p, double* phi);
+    void initFlux(const double* u0);
+    void iterate(const cfg_simple_controls& ctl, cfg_simple_result& res);
+
+    // diagnostics used by the parity tests
+    void probeEquations(const cfg_simple_controls& ctl, const double* xprobe, double* out);
+    void gradient(const double* data, const double* bvals, int scheme, int volQuirk, double* out);
+
+    /// solveCG / solveBiCGStab on a host CSR (Matrix.cpp:153-319)
+    static void sparseSolve(int device, int64_t n, const int64_t* rs, const int64_t* cols, const double* vals,
+                            const double* b, double* x, double tol, int maxIter, int method,
+                            cfg_solver_report* rep);
+
+    double lastMs[8] = {0};
+    int64_t lastLaunches = 0;
+
+    const Mesh& mesh() const { return mesh_; }
+
+private:
+    template <class T>
+    T* alloc(size_t n);
+    template <class T>
+    T* upload(const std::vector<T>& v);
+
+    void buildDevice();
+    void refreshBc();
+    void gradCells(const double* const* x, int nComp, const BcTab& bc, int scheme, bool volQuirk, V3P* out);
+    void solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, int64_t& inner);
+    void solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner);
+    void runCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+               cfg_solver_report* rep);
+    void runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
+                  cfg_solver_report* reps);
+    void launchCheck(const char* what);
+    void setNu(double nu);
+    void checkMomentumBcs() const;
+
+    Mesh mesh_;
+    int device_;
+    cudaStream_t stream_;
+    bool ownStream_ = false;
+    int G_ = 0;        // grid of row kernels
+    int GF_ = 0;       // grid of face kernels
+    int nSlices_ = 0;
+    std::vector<void*> allocs_;
+    DMesh dm_{};
+
+    // boundary conditions (host)
+    std::vector<int> uType_, pType_;
+    std::vector<Vec> uVal_;
+    std::vector<double> pVal_;
+    std::map<int64_t, Vec> uFace_;
+    bool bcDirty_ = true;
+    cfg_schemes schemes_{CFG_DIV_UPWIND, 1, CFG_GRAD_CORRECTED, 0.9};
+
+    // device BC tables
+    double *uc_[3], *uk_[3], *hc_[3], *hk_[3], *pc_, *pk_;
+    int64_t nFreeUFaces_ = 0;  // faces of patches whose U is not fixedValue
+
+    // fields
+    V3P U_, gPn_, gPF_, Hf_, gA_, gB_, uBase_, uRhs_, ux_;
+    double *p_, *phi_, *rAUr_, *rAUf_, *uDiag_, *pDiag_, *pBase_, *pRhs_, *px_, *mVal_, *pVal_d_;
+    double* gU_ = nullptr;   // harmonic face viscosity for the current nu
+    double* fScratch_ = nullptr;  // nFaces
+    double* bScratch_ = nullptr;  // 2 nBoundary
+    double lastNu_ = -1.0;
+    // adjustPhi addressing (patch ranges, which patches have a free U)
+    int *dpStart_, *dpSize_, *dpFree_, *dFreeFace_, *dEmptyFace_;
+    bool needReference_ = true;
+    // solver work
+    double *cr_, *cp_, *cAp_;
+    V3P br_, br0_, bp_, bv_, bs_, bsh_, bt_, bz_;
+    double* partials_;
+    SolveState* st_;
+    SolveState* stHost_;
+    double* scal_;      // device scalars of one outer iteration
+    double* scalHost_;  // pinned copy
+    Timing tm_{};
+    int64_t launches_ = 0;
+};
+
+}  // namespace cfg
+
+struct cfg_ctx
+{
+    std::unique_ptr<cfg::Ctx> c;
+};

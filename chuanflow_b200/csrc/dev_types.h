@@ -1,0 +1,76 @@
+// Layout types shared by host and device code, and the checked CUDA call.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "cfg_internal.h"
+
+namespace cfg
+{
+
+constexpr int TPB = 256;  // threads per block of every row/face kernel
+
+#define CFG_CUDA(call)                                                                        \
+    do                                                                                        \
+    {                                                                                         \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            ::cfg::fail(CFG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+/// Three device arrays, one per vector component (structure of arrays).
+struct V3P
+{
+    double* c[3];
+};
+struct CV3P
+{
+    const double* c[3];
+};
+
+/// Boundary linearisation face = c * cell + k for every boundary face and
+/// component (volFields.cpp:117-147, :246-283), one table per field.
+struct BcTab
+{
+    const double* c[3];
+    const double* k[3];
+};
+
+/// Device mesh.  Face arrays are in the mesh's original face order; cell
+/// arrays in device cell order (the identity unless renumbered).
+struct DMesh
+{
+    int nC, nF, nI, nB;
+    int nRowsPad;  // nC rounded up to a multiple of 32
+    const int* own;   // nF
+    const int* nbr;   // nI
+    const double *sfx, *sfy, *sfz;  // face area vectors
+    const double* ow;               // bounded owner weight (internal faces)
+    const double* wq;               // volScalarField::faceValue weight (internal faces)
+    const double *skx, *sky, *skz;  // skew vectors (internal faces)
+    const double* oc;               // (Sf.d)/|d|^2
+    const double* sfd;              // Sf.d
+    const double* dd2;              // d.d
+    const double *cvx, *cvy, *cvz;  // non-orthogonal vector Sf - dh (Sf.dh)
+    const double* V;                // cell volumes
+    const double* lscale;           // largest face area of each cell
+    const double *cx, *cy, *cz;     // cell centres
+    const double *fcx, *fcy, *fcz;  // face centres
+    // cell -> faces, SELL-32 (slice-major, slot-major inside a slice): each
+    // cell's faces in ascending original face order; code = face<<1 | side
+    // (side 1: the cell is the face's neighbour), -1 pads; other = the cell
+    // across an internal face or the boundary index of a boundary face
+    const int* cfStart;  // nSlices+1, in entries
+    const int* cfCode;
+    const int* cfOther;
+    // matrix rows, SELL-32: entries in the reference CSR's column order with
+    // the diagonal in place; code = face<<1|side, -2 diagonal, -1 pad
+    const int* mStart;
+    const int* mCol;
+    const int* mCode;
+};
+
+}  // namespace cfg

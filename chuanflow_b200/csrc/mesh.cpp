@@ -1,0 +1,303 @@
+// Host mesh: block generation, addressing checks and geometry.
+//
+// The geometry must be bit-identical to the reference's polyMesh, so every
+// quantity below is evaluated with the same IEEE operations in the same order
+// as src/3d/src/mesh/polyMesh.cpp:83-288 (this file is compiled with
+// -ffp-contract=off so no multiply-add is fused).  The block generator emits
+// the face order that BlockMesh::create's first-registration deduplication
+// produces (src/3d/src/mesh/blockMesh.cpp:76-185), derived in closed form
+// instead of through a face map.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "cfg_internal.h"
+
+namespace cfg
+{
+namespace
+{
+
+inline double dot(const Vec& a, const Vec& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline Vec cross(const Vec& a, const Vec& b)
+{
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline double mag(const Vec& a) { return std::sqrt(dot(a, a)); }
+
+}  // namespace
+
+Mesh blockMesh(const Vec& mn, const Vec& mx, int64_t nx, int64_t ny, int64_t nz,
+               const std::vector<std::string>& names, const std::vector<std::string>& types)
+{
+    if (nx <= 0 || ny <= 0 || nz <= 0) fail(CFG_EMESH, "blockMesh: cell counts must be positive");
+    Mesh m;
+    m.bnx = nx;
+    m.bny = ny;
+    m.bnz = nz;
+    m.bmin = mn;
+    m.bmax = mx;
+    auto pid = [&](int64_t i, int64_t j, int64_t k) { return i + (nx + 1) * (j + (ny + 1) * k); };
+    m.points.resize(static_cast<size_t>((nx + 1) * (ny + 1) * (nz + 1)));
+    for (int64_t k = 0; k <= nz; ++k)
+        for (int64_t j = 0; j <= ny; ++j)
+            for (int64_t i = 0; i <= nx; ++i)
+                m.points[static_cast<size_t>(pid(i, j, k))] = {
+                    mn.x + (mx.x - mn.x) * static_cast<double>(i) / static_cast<double>(nx),
+                    mn.y + (mx.y - mn.y) * static_cast<double>(j) / static_cast<double>(ny),
+                    mn.z + (mx.z - mn.z) * static_cast<double>(k) / static_cast<double>(nz)};
+
+    // A hex face is registered first by the lower-numbered of its two cells,
+    // and cells are visited in id order with faces zlo zhi ylo yhi xlo xhi.
+    // So at cell (i,j,k) the new faces are: zlo iff k==0, zhi always, ylo iff
+    // j==0, yhi always, xlo iff i==0, xhi always; a new face is internal iff
+    // the cell across it exists.  Boundary faces then go to their side's list.
+    const int64_t nInt = (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1);
+    const int64_t nBnd = 2 * (ny * nz + nx * nz + nx * ny);
+    std::vector<int64_t> intVerts;
+    intVerts.reserve(static_cast<size_t>(4 * nInt));
+    m.owner.reserve(static_cast<size_t>(nInt + nBnd));
+    m.neighbour.reserve(static_cast<size_t>(nInt));
+    std::vector<int64_t> sideVerts[6], sideOwner[6];
+    for (int64_t k = 0; k < nz; ++k)
+        for (int64_t j = 0; j < ny; ++j)
+            for (int64_t i = 0; i < nx; ++i)
+            {
+                const int64_t c = i + nx * (j + ny * k);
+                const int64_t v0 = pid(i, j, k), v1 = pid(i + 1, j, k), v2 = pid(i + 1, j + 1, k),
+                              v3 = pid(i, j + 1, k), v4 = pid(i, j, k + 1), v5 = pid(i + 1, j, k + 1),
+                              v6 = pid(i + 1, j + 1, k + 1), v7 = pid(i, j + 1, k + 1);
+                struct Kind
+                {
+                    int64_t v[4];
+                    bool isNew;
+                    int64_t other;  // -1: boundary
+                    int side;
+                };
+                const Kind kinds[6] = {
+                    {{v0, v1, v2, v3}, k == 0, -1, 4},
+                    {{v4, v5, v6, v7}, true, k + 1 < nz ? c + nx * ny : -1, 5},
+                    {{v0, v1, v5, v4}, j == 0, -1, 2},
+                    {{v2, v3, v7, v6}, true, j + 1 < ny ? c + nx : -1, 3},
+                    {{v0, v3, v7, v4}, i == 0, -1, 0},
+                    {{v1, v2, v6, v5}, true, i + 1 < nx ? c + 1 : -1, 1}};
+                for (const Kind& kd : kinds)
+                {
+                    if (!kd.isNew) continue;
+                    if (kd.other >= 0)
+                    {
+                        intVerts.insert(intVerts.end(), kd.v, kd.v + 4);
+                        m.owner.push_back(c);
+                        m.neighbour.push_back(kd.other);
+                    }
+                    else
+                    {
+                        sideVerts[kd.side].insert(sideVerts[kd.side].end(), kd.v, kd.v + 4);
+                        sideOwner[kd.side].push_back(c);
+                    }
+                }
+            }
+    m.faceVerts = std::move(intVerts);
+    for (int s = 0; s < 6; ++s)
+    {
+        if (sideOwner[s].empty()) continue;
+        Mesh::Patch p;
+        p.name = names[static_cast<size_t>(s)];
+        p.type = types[static_cast<size_t>(s)];
+        p.start = static_cast<int64_t>(m.owner.size());
+        p.size = static_cast<int64_t>(sideOwner[s].size());
+        m.faceVerts.insert(m.faceVerts.end(), sideVerts[s].begin(), sideVerts[s].end());
+        m.owner.insert(m.owner.end(), sideOwner[s].begin(), sideOwner[s].end());
+        m.patches.push_back(std::move(p));
+    }
+    m.faceOffsets.resize(m.owner.size() + 1);
+    for (size_t f = 0; f <= m.owner.size(); ++f) m.faceOffsets[f] = static_cast<int64_t>(4 * f);
+    m.finish();
+    return m;
+}
+
+void Mesh::finish()
+{
+    const int64_t nF = nFaces(), nI = nInternal();
+    if (static_cast<int64_t>(faceOffsets.size()) != nF + 1) fail(CFG_EMESH, "polyMesh: face offsets size");
+    nCells = 0;
+    for (int64_t o : owner) nCells = std::max(nCells, o + 1);
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        if (faceOffsets[f + 1] - faceOffsets[f] < 3) fail(CFG_EMESH, "polyMesh: face with fewer than 3 vertices");
+        if (owner[f] < 0) fail(CFG_EMESH, "polyMesh: negative owner");
+        for (int64_t q = faceOffsets[f]; q < faceOffsets[f + 1]; ++q)
+            if (faceVerts[q] < 0 || faceVerts[q] >= static_cast<int64_t>(points.size()))
+                fail(CFG_EMESH, "polyMesh: face vertex out of range");
+        if (f < nI && (neighbour[f] < 0 || neighbour[f] >= nCells))
+            fail(CFG_EMESH, "polyMesh: neighbour out of range at face " + std::to_string(f));
+    }
+    // face -> patch, patches must cover every boundary face exactly once
+    // (polyMesh.cpp:35-61)
+    facePatch.assign(static_cast<size_t>(nF), -1);
+    for (size_t i = 0; i < patches.size(); ++i)
+    {
+        const Patch& p = patches[i];
+        for (int64_t f = p.start; f < p.start + p.size; ++f)
+        {
+            if (f < nI) fail(CFG_EMESH, "polyMesh: patch '" + p.name + "' covers internal face " + std::to_string(f));
+            if (f >= nF) fail(CFG_EMESH, "polyMesh: patch '" + p.name + "' beyond the last face");
+            if (facePatch[static_cast<size_t>(f)] >= 0)
+                fail(CFG_EMESH, "polyMesh: boundary face " + std::to_string(f) + " in two patches");
+            facePatch[static_cast<size_t>(f)] = static_cast<int64_t>(i);
+        }
+    }
+    for (int64_t f = nI; f < nF; ++f)
+        if (facePatch[static_cast<size_t>(f)] < 0)
+            fail(CFG_EMESH, "polyMesh: boundary face " + std::to_string(f) + " is not in any patch");
+    calcGeometry();
+}
+
+void Mesh::calcGeometry()
+{
+    const int64_t nF = nFaces(), nI = nInternal();
+    Cf.assign(static_cast<size_t>(nF), Vec{});
+    Sf.assign(static_cast<size_t>(nF), Vec{});
+    auto P = [&](int64_t v) -> const Vec& { return points[static_cast<size_t>(v)]; };
+
+    // fan-triangle area vectors and face centroids
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        const int64_t* vs = faceVerts.data() + faceOffsets[f];
+        const int64_t nv = faceOffsets[f + 1] - faceOffsets[f];
+        const Vec v0 = P(vs[0]);
+        Vec n{};
+        for (int64_t i = 1; i + 1 < nv; ++i) n = n + cross(P(vs[i]) - v0, P(vs[i + 1]) - v0);
+        Sf[static_cast<size_t>(f)] = n * 0.5;
+        bool exactMean = nv == 3;
+        if (nv == 4)
+        {
+            const Vec a = P(vs[0]) + P(vs[2]), b = P(vs[1]) + P(vs[3]);
+            exactMean = a.x == b.x && a.y == b.y && a.z == b.z;
+        }
+        Vec c{};
+        const double wSum = exactMean ? 0.0 : dot(n, n);
+        if (!exactMean && wSum > 0)
+        {
+            for (int64_t i = 1; i + 1 < nv; ++i)
+            {
+                const Vec vi = P(vs[i]), vj = P(vs[i + 1]);
+                const double w = dot(cross(vi - v0, vj - v0), n);
+                c = c + (v0 + vi + vj) * w;
+            }
+            Cf[static_cast<size_t>(f)] = c / (3.0 * wSum);
+        }
+        else
+        {
+            for (int64_t i = 0; i < nv; ++i) c = c + P(vs[i]);
+            Cf[static_cast<size_t>(f)] = c / static_cast<double>(nv);
+        }
+    }
+
+    // provisional cell centres (mean of face centres), used only to orient
+    std::vector<Vec> est(static_cast<size_t>(nCells));
+    std::vector<int64_t> cnt(static_cast<size_t>(nCells), 0);
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        const size_t o = static_cast<size_t>(owner[f]);
+        est[o] = est[o] + Cf[static_cast<size_t>(f)];
+        ++cnt[o];
+        if (f < nI)
+        {
+            const size_t nb = static_cast<size_t>(neighbour[f]);
+            est[nb] = est[nb] + Cf[static_cast<size_t>(f)];
+            ++cnt[nb];
+        }
+    }
+    for (size_t c = 0; c < est.size(); ++c)
+        if (cnt[c] > 0) est[c] = est[c] / static_cast<double>(cnt[c]);
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        const size_t o = static_cast<size_t>(owner[f]);
+        const Vec dd = f < nI ? est[static_cast<size_t>(neighbour[f])] - est[o] : Cf[static_cast<size_t>(f)] - est[o];
+        Vec& sf = Sf[static_cast<size_t>(f)];
+        const double side = dot(sf, dd);
+        const double tol = 1e-12 * mag(sf) * mag(dd);
+        if (side < -tol) sf = Vec{-sf.x, -sf.y, -sf.z};
+    }
+    magSf.resize(static_cast<size_t>(nF));
+    for (int64_t f = 0; f < nF; ++f) magSf[static_cast<size_t>(f)] = mag(Sf[static_cast<size_t>(f)]);
+
+    // volumes and centroids through the divergence theorem over fan tets
+    V.assign(static_cast<size_t>(nCells), 0.0);
+    C.assign(static_cast<size_t>(nCells), Vec{});
+    std::vector<Vec> moment(static_cast<size_t>(nCells));
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        const int64_t* vs = faceVerts.data() + faceOffsets[f];
+        const int64_t nv = faceOffsets[f + 1] - faceOffsets[f];
+        const Vec v0 = P(vs[0]);
+        double fv = 0;
+        Vec fm{}, raw{};
+        for (int64_t i = 1; i + 1 < nv; ++i)
+        {
+            const Vec a = P(vs[i]) - v0, b = P(vs[i + 1]) - v0;
+            const double tV = dot(v0, cross(a, b)) / 6.0;
+            fv += tV;
+            fm = fm + ((v0 + P(vs[i]) + P(vs[i + 1])) / 4.0) * tV;
+        }
+        for (int64_t i = 1; i + 1 < nv; ++i) raw = raw + cross(P(vs[i]) - v0, P(vs[i + 1]) - v0);
+        const double s = dot(raw, Sf[static_cast<size_t>(f)]) >= 0 ? 1.0 : -1.0;
+        const size_t o = static_cast<size_t>(owner[f]);
+        V[o] += s * fv;
+        moment[o] = moment[o] + fm * s;
+        if (f < nI)
+        {
+            const size_t nb = static_cast<size_t>(neighbour[f]);
+            V[nb] -= s * fv;
+            moment[nb] = moment[nb] - fm * s;
+        }
+    }
+    for (size_t c = 0; c < V.size(); ++c)
+    {
+        C[c] = moment[c] / V[c];
+        V[c] = std::abs(V[c]);
+        if (!(V[c] > 0)) fail(CFG_EMESH, "polyMesh: degenerate cell volume for cell " + std::to_string(c));
+    }
+    d.resize(static_cast<size_t>(nF));
+    invDist.resize(static_cast<size_t>(nF));
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        const size_t o = static_cast<size_t>(owner[f]);
+        d[static_cast<size_t>(f)] = f < nI ? C[static_cast<size_t>(neighbour[f])] - C[o] : Cf[static_cast<size_t>(f)] - C[o];
+        const double dm = mag(d[static_cast<size_t>(f)]);
+        if (!(dm > 0)) fail(CFG_EMESH, "polyMesh: zero owner-neighbour distance at face " + std::to_string(f));
+        invDist[static_cast<size_t>(f)] = 1.0 / dm;
+    }
+}
+
+std::vector<double> Mesh::ownerWeights() const
+{
+    // makeInternalOwnerWeights (interpolate.cpp:15-35): 1 - clamp(t, 0, 1),
+    // t the owner-to-face-centre projection on d over |d|^2
+    const int64_t nI = nInternal();
+    std::vector<double> w(static_cast<size_t>(std::max<int64_t>(1, nI)), 0.5);
+    for (int64_t f = 0; f < nI; ++f)
+    {
+        const Vec& dd = d[static_cast<size_t>(f)];
+        const double t = dot(Cf[static_cast<size_t>(f)] - C[static_cast<size_t>(owner[f])], dd) / dot(dd, dd);
+        const double tc = t < 0.0 ? 0.0 : (1.0 < t ? 1.0 : t);
+        w[static_cast<size_t>(f)] = 1.0 - tc;
+    }
+    return w;
+}
+
+std::vector<Vec> Mesh::skewVectors(const std::vector<double>& ow) const
+{
+    // makeFaceSkewVectors (interpolate.cpp:37-48)
+    std::vector<Vec> s(static_cast<size_t>(nFaces()));
+    for (int64_t f = 0; f < nInternal(); ++f)
+    {
+        const Vec& co = C[static_cast<size_t>(owner[f])];
+        const Vec& cn = C[static_cast<size_t>(neighbour[f])];
+        s[static_cast<size_t>(f)] = Cf[static_cast<size_t>(f)] - (co + (cn - co) * (1.0 - ow[static_cast<size_t>(f)]));
+    }
+    return s;
+}
+
+}  // namespace cfg

@@ -1,0 +1,1606 @@
+// The SIMPLE outer iteration on the device (src/3d/src/solvers/simpleSolver.cpp:33-394)
+// and the host driver that sequences its kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "ctx.h"
+#include "kernels.cuh"
+#include "solvers.cuh"
+
+namespace cfg
+{
+
+// scalar slots of one outer iteration (device array scal_)
+enum Slot
+{
+    S_CONT = 0,     // continuityError of the predictor flux
+    S_CONT_AFTER,   // continuityError after correctFluxes
+    S_PSTEP,        // max |pFull - p|
+    S_PSCALE,       // max |p|
+    S_AP,           // the pressure relaxation used
+    S_PDELTA,       // max |aP (pFull - p)|
+    S_UMAX,
+    S_DUMAX,
+    S_NONFINITE,
+    S_NET,          // adjustPhi sums
+    S_FREE,
+    S_COUNT
+};
+
+// ---------------------------------------------------------------------------
+// momentum assembly: fvm::div (divScheme.cpp:11-62) + fvm::laplacian with
+// the harmonic face viscosity (laplacianScheme.cpp:146-215), sign -1, plus
+// the deferred pressure-gradient source (simpleSolver.cpp:99-112).  One row
+// per thread: the diagonal as the reference's face loops add into it (all
+// convection terms in face order, then all diffusion terms), the row's
+// entries in CSR column order, and the three base right-hand sides.
+// ---------------------------------------------------------------------------
+
+struct MomArgs
+{
+    const double* phi;
+    const double* gamma;
+    BcTab ub;
+    double alpha;  // 0 upwind, 1 linear, blendCoeff for blend
+    double force[3];
+    CV3P gPn;
+    double* mVal;
+    double* uDiag;
+    V3P base;
+};
+
+__device__ __forceinline__ void div_weights(double p, double alpha, double ow, double& wPo, double& wNo)
+{
+    wPo = 0.0;
+    wNo = 0.0;
+    if (p >= 0) wPo = 1.0;
+    else wNo = 1.0;
+    if (alpha > 0)
+    {
+        wPo = alpha * ow + (1.0 - alpha) * wPo;
+        wNo = alpha * (1.0 - ow) + (1.0 - alpha) * wNo;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_assemble_U(DMesh m, MomArgs a)
+{
+    ROW_LOOP(c, m.nC)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        const int e0 = m.cfStart[sl] + lane, e1 = m.cfStart[sl + 1];
+        double diag = 0.0;
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+        for (int e = e0; e < e1; e += 32)  // convection
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const int f = code >> 1, side = code & 1;
+            const double p = a.phi[f];
+            if (f < m.nI)
+            {
+                double wPo, wNo;
+                div_weights(p, a.alpha, m.ow[f], wPo, wNo);
+                diag += side ? -(p * wNo) : p * wPo;
+            }
+            else
+            {
+                const int b = m.cfOther[e];
+                diag += p * a.ub.c[0][b];
+                r0 += (-p) * a.ub.k[0][b];
+                r1 += (-p) * a.ub.k[1][b];
+                r2 += (-p) * a.ub.k[2][b];
+            }
+        }
+        for (int e = e0; e < e1; e += 32)  // diffusion
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const int f = code >> 1;
+            const double coef = a.gamma[f] * m.oc[f];
+            if (f < m.nI)
+            {
+                diag += coef;
+            }
+            else
+            {
+                const int b = m.cfOther[e];
+                diag += (-coef) * (a.ub.c[0][b] - 1.0);
+                r0 += coef * a.ub.k[0][b];
+                r1 += coef * a.ub.k[1][b];
+                r2 += coef * a.ub.k[2][b];
+            }
+        }
+        const double v = m.V[c];
+        r0 += ((a.force[0] + 0.0) - a.gPn.c[0][c]) * v;
+        r1 += ((a.force[1] + 0.0) - a.gPn.c[1][c]) * v;
+        r2 += ((a.force[2] + 0.0) - a.gPn.c[2][c]) * v;
+        a.uDiag[c] = diag;
+        a.base.c[0][c] = r0;
+        a.base.c[1][c] = r1;
+        a.base.c[2][c] = r2;
+        const int me1 = m.mStart[sl + 1];
+        for (int e = m.mStart[sl] + lane; e < me1; e += 32)
+        {
+            const int code = m.mCode[e];
+            if (code == -1) break;
+            double val;
+            if (code == -2)
+            {
+                val = diag;
+            }
+            else
+            {
+                const int f = code >> 1, side = code & 1;
+                const double p = a.phi[f];
+                double wPo, wNo;
+                div_weights(p, a.alpha, m.ow[f], wPo, wNo);
+                const double conv = side ? -(p * wPo) : p * wNo;
+                val = conv + (-(a.gamma[f] * m.oc[f]));
+            }
+            a.mVal[e] = val;
+        }
+    }
+}
+
+/// Pressure equation: fvm::laplacianFace(rAUf) sign -1 plus -div(phi)
+/// (simpleSolver.cpp:265-273), and continuityError of the same flux
+/// (pressureCorrection.cpp:90-125).
+__global__ void __launch_bounds__(TPB) k_assemble_p(DMesh m, const double* __restrict__ phi,
+                                                    const double* __restrict__ rAUf, const double* __restrict__ pc,
+                                                    const double* __restrict__ pk, double* pVal, double* pDiag,
+                                                    double* pBase, double* scal, int refCell, double refValue)
+{
+    double cmax = 0.0;
+    ROW_LOOP(c, m.nC)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        const int e0 = m.cfStart[sl] + lane, e1 = m.cfStart[sl + 1];
+        double dv = 0.0;
+        for (int e = e0; e < e1; e += 32)
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const double ph = phi[code >> 1];
+            dv = (code & 1) ? dv - ph : dv + ph;
+        }
+        cmax = smax(cmax, fabs(dv) / smax(m.lscale[c], 1e-300));
+        double diag = 0.0, r = 0.0;
+        for (int e = e0; e < e1; e += 32)
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const int f = code >> 1;
+            const double coef = rAUf[f] * m.oc[f];
+            if (f < m.nI)
+            {
+                diag += coef;
+            }
+            else
+            {
+                const int b = m.cfOther[e];
+                diag += (-coef) * (pc[b] - 1.0);
+                r += coef * pk[b];
+            }
+        }
+        r += -dv;
+        if (c == refCell)
+        {
+            r += diag * refValue;
+            diag += diag;
+        }
+        pDiag[c] = diag;
+        pBase[c] = r;
+        const int me1 = m.mStart[sl + 1];
+        for (int e = m.mStart[sl] + lane; e < me1; e += 32)
+        {
+            const int code = m.mCode[e];
+            if (code == -1) break;
+            pVal[e] = code == -2 ? diag : -(rAUf[code >> 1] * m.oc[code >> 1]);
+        }
+    }
+    double v[1] = {cmax};
+    block_max<1>(v);
+    if (threadIdx.x == 0) atomic_max_nonneg(scal + S_CONT, v[0]);
+}
+
+/// continuityError alone (the corrected flux).
+__global__ void __launch_bounds__(TPB) k_continuity(DMesh m, const double* __restrict__ phi, double* scal, int slot)
+{
+    double cmax = 0.0;
+    ROW_LOOP(c, m.nC)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        double dv = 0.0;
+        const int e1 = m.cfStart[sl + 1];
+        for (int e = m.cfStart[sl] + lane; e < e1; e += 32)
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const double ph = phi[code >> 1];
+            dv = (code & 1) ? dv - ph : dv + ph;
+        }
+        cmax = smax(cmax, fabs(dv) / smax(m.lscale[c], 1e-300));
+    }
+    double v[1] = {cmax};
+    block_max<1>(v);
+    if (threadIdx.x == 0) atomic_max_nonneg(scal + slot, v[0]);
+}
+
+/// fvc::divPhi (interpolate.cpp:419-432)
+__global__ void __launch_bounds__(TPB) k_divphi(DMesh m, const double* __restrict__ phi, double* out)
+{
+    ROW_LOOP(c, m.nC)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        double dv = 0.0;
+        const int e1 = m.cfStart[sl + 1];
+        for (int e = m.cfStart[sl] + lane; e < e1; e += 32)
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const double ph = phi[code >> 1];
+            dv = (code & 1) ? dv - ph : dv + ph;
+        }
+        out[c] = dv;
+    }
+}
+
+/// The non-orthogonal corrector of assembleLaplacian (laplacianScheme.cpp:217-263):
+/// rhs = base + sum over faces in order of +-gamma_f (cfVec . grad_f), with
+/// grad_f the owner-weighted face interpolation of the cell gradients.
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_corrector(DMesh m, const double* __restrict__ gamma, CGrad3 g, CV3P base,
+                                                   V3P rhs)
+{
+    ROW_LOOP(c, m.nC)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        double r[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) r[q] = base.c[q][c];
+        const int e1 = m.cfStart[sl + 1];
+        for (int e = m.cfStart[sl] + lane; e < e1; e += 32)
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const int f = code >> 1, side = code & 1;
+            const double cvx = m.cvx[f], cvy = m.cvy[f], cvz = m.cvz[f], gm = gamma[f];
+            if (f < m.nI)
+            {
+                const int other = m.cfOther[e];
+                const int o = side ? other : c, n = side ? c : other;
+                const double w = m.ow[f], w1 = 1.0 - w;
+#pragma unroll
+                for (int q = 0; q < NC; ++q)
+                {
+                    const double gx = g.g[q].c[0][o] * w + g.g[q].c[0][n] * w1;
+                    const double gy = g.g[q].c[1][o] * w + g.g[q].c[1][n] * w1;
+                    const double gz = g.g[q].c[2][o] * w + g.g[q].c[2][n] * w1;
+                    const double corr = gm * (cvx * gx + cvy * gy + cvz * gz);
+                    r[q] = side ? r[q] + (-corr) : r[q] + corr;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < NC; ++q)
+                {
+                    const double corr =
+                        gm * (cvx * g.g[q].c[0][c] + cvy * g.g[q].c[1][c] + cvz * g.g[q].c[2][c]);
+                    r[q] = r[q] + corr;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q) rhs.c[q][c] = r[q];
+    }
+}
+
+/// rAU = V / aDiag and the pressure-free blend Hfree (simpleSolver.cpp:123-172).
+__global__ void __launch_bounds__(TPB) k_hfree(DMesh m, const double* __restrict__ uDiag, CV3P U, CV3P x,
+                                               double relaxU, V3P Hf, double* rAUr)
+{
+    ROW_LOOP(c, m.nC)
+    {
+        rAUr[c] = m.V[c] / smax(uDiag[c], 1e-300);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) Hf.c[q][c] = (1.0 - relaxU) * U.c[q][c] + relaxU * x.c[q][c];
+    }
+}
+
+/// phi from a cell vector field: updatePhiInternal (pressureCorrection.cpp:10-25)
+/// and correctBoundaryFlux (volFields.cpp:294-306) under a linearisation table.
+__global__ void __launch_bounds__(TPB) k_flux(DMesh m, CV3P H, BcTab hb, const int* __restrict__ emptyFace,
+                                              double* phi)
+{
+    ROW_LOOP(f, m.nF)
+    {
+        const int o = m.own[f];
+        double ux, uy, uz;
+        if (f < m.nI)
+        {
+            const int n = m.nbr[f];
+            const double w = m.ow[f], w1 = 1.0 - w;
+            ux = H.c[0][o] * w + H.c[0][n] * w1;
+            uy = H.c[1][o] * w + H.c[1][n] * w1;
+            uz = H.c[2][o] * w + H.c[2][n] * w1;
+        }
+        else
+        {
+            const int b = f - m.nI;
+            if (emptyFace && emptyFace[b])
+            {
+                phi[f] = 0.0;
+                continue;
+            }
+            ux = hb.c[0][b] * H.c[0][o] + hb.k[0][b];
+            uy = hb.c[1][b] * H.c[1][o] + hb.k[1][b];
+            uz = hb.c[2][b] * H.c[2][o] + hb.k[2][b];
+        }
+        phi[f] = ux * m.sfx[f] + uy * m.sfy[f] + uz * m.sfz[f];
+    }
+}
+
+/// internal phi only (updatePhiInternal), used for the initial flux
+__global__ void __launch_bounds__(TPB) k_flux_internal(DMesh m, CV3P U, double* phi)
+{
+    ROW_LOOP(f, m.nI)
+    {
+        const int o = m.own[f], n = m.nbr[f];
+        const double w = m.ow[f], w1 = 1.0 - w;
+        const double ux = U.c[0][o] * w + U.c[0][n] * w1;
+        const double uy = U.c[1][o] * w + U.c[1][n] * w1;
+        const double uz = U.c[2][o] * w + U.c[2][n] * w1;
+        phi[f] = ux * m.sfx[f] + uy * m.sfy[f] + uz * m.sfz[f];
+    }
+}
+
+/// adjustPhi sums (simpleSolver.cpp:220-232), serial in the reference's
+/// order: patch by patch, face by face.
+__global__ void k_adjust_sums(const double* phi, const int* pStart, const int* pSize, const int* pFree, int nPatch,
+                              double* scal)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double netSum = 0, freeSum = 0;
+    for (int pi = 0; pi < nPatch; ++pi)
+    {
+        double s = 0;
+        for (int f = pStart[pi]; f < pStart[pi] + pSize[pi]; ++f) s += phi[f];
+        netSum += s;
+        if (pFree[pi]) freeSum += s;
+    }
+    scal[S_NET] = netSum;
+    scal[S_FREE] = freeSum;
+}
+
+__global__ void __launch_bounds__(TPB) k_adjust_scale(int nB, int nI, const int* __restrict__ freeFace,
+                                                      double* phi, const double* scal)
+{
+    const double freeSum = scal[S_FREE], netSum = scal[S_NET];
+    if (!(fabs(freeSum) > 1e-30)) return;
+    const double scale = (freeSum - netSum) / freeSum;
+    ROW_LOOP(b, nB)
+    if (freeFace[b]) phi[nI + b] *= scale;
+}
+
+/// interpolateToFaces (pressureCorrection.cpp:27-35)
+__global__ void __launch_bounds__(TPB) k_face_interp(DMesh m, const double* __restrict__ cell, double* face)
+{
+    ROW_LOOP(f, m.nF)
+    {
+        const int o = m.own[f];
+        face[f] = f < m.nI ? m.ow[f] * cell[o] + (1.0 - m.ow[f]) * cell[m.nbr[f]] : cell[o];
+    }
+}
+
+/// correctFluxes (pressureCorrection.cpp:37-88)
+__global__ void __launch_bounds__(TPB) k_correct_flux(DMesh m, const double* __restrict__ pF, CV3P gP,
+                                                      const double* __restrict__ rAUf, const double* __restrict__ pc,
+                                                      const double* __restrict__ pk, int corrected, double* phi)
+{
+    ROW_LOOP(f, m.nF)
+    {
+        const double d2 = m.dd2[f];
+        if (d2 <= 0) continue;
+        const double rf = rAUf[f];
+        const double coef = rf * m.sfd[f] / d2;
+        const int o = m.own[f];
+        double corr = 0;
+        if (corrected)
+        {
+            double gx, gy, gz;
+            if (f < m.nI)
+            {
+                const int n = m.nbr[f];
+                const double w = m.ow[f], w1 = 1.0 - w;
+                gx = gP.c[0][o] * w + gP.c[0][n] * w1;
+                gy = gP.c[1][o] * w + gP.c[1][n] * w1;
+                gz = gP.c[2][o] * w + gP.c[2][n] * w1;
+            }
+            else
+            {
+                gx = gP.c[0][o];
+                gy = gP.c[1][o];
+                gz = gP.c[2][o];
+            }
+            corr = rf * (m.cvx[f] * gx + m.cvy[f] * gy + m.cvz[f] * gz);
+        }
+        if (f < m.nI)
+        {
+            const double dp = pF[m.nbr[f]] - pF[o];
+            phi[f] = phi[f] - (coef * dp + corr);
+        }
+        else
+        {
+            const int b = f - m.nI;
+            phi[f] = phi[f] - (coef * ((pc[b] - 1.0) * pF[o] + pk[b]) + corr);
+        }
+    }
+}
+
+/// max |pFull - p| and max |p| (simpleSolver.cpp:303-309)
+__global__ void __launch_bounds__(TPB) k_pstep(int n, const double* __restrict__ pF, const double* __restrict__ p,
+                                               double* scal)
+{
+    double v[2] = {0.0, 0.0};
+    ROW_LOOP(c, n)
+    {
+        v[0] = smax(v[0], fabs(pF[c] - p[c]));
+        v[1] = smax(v[1], fabs(p[c]));
+    }
+    block_max<2>(v);
+    if (threadIdx.x == 0)
+    {
+        atomic_max_nonneg(scal + S_PSTEP, v[0]);
+        atomic_max_nonneg(scal + S_PSCALE, v[1]);
+    }
+}
+
+/// aP, the pressure relaxation and the velocity correction, and the
+/// residual maxima (simpleSolver.cpp:310-348)
+__global__ void __launch_bounds__(TPB) k_update(int n, const double* __restrict__ pF, double* p, V3P U, CV3P Hf,
+                                                CV3P gPF, CV3P gPn, const double* __restrict__ rAUr, double relaxP,
+                                                double pRelaxStart, double* scal)
+{
+    const double pStep = scal[S_PSTEP], pScale = scal[S_PSCALE];
+    const double aP = pRelaxStart > 0 ? smin(relaxP, smax(pRelaxStart, 0.15 * pScale / smax(pStep, 1e-300))) : relaxP;
+    double v[3] = {0.0, 0.0, 0.0};
+    int bad = 0;
+    ROW_LOOP(c, n)
+    {
+        const double po = p[c];
+        const double dp = aP * (pF[c] - po);
+        v[0] = smax(v[0], fabs(dp));
+        const double pn = po + dp;
+        p[c] = pn;
+        const double s = aP * rAUr[c];
+        double un[3], du[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+            un[q] = Hf.c[q][c] - (gPF.c[q][c] - gPn.c[q][c]) * s;
+            du[q] = un[q] - U.c[q][c];
+            U.c[q][c] = un[q];
+        }
+        v[1] = smax(v[1], sqrt(un[0] * un[0] + un[1] * un[1] + un[2] * un[2]));
+        v[2] = smax(v[2], sqrt(du[0] * du[0] + du[1] * du[1] + du[2] * du[2]));
+        if (!isfinite(un[0]) || !isfinite(un[1]) || !isfinite(un[2]) || !isfinite(pn)) bad = 1;
+    }
+    block_max<3>(v);
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0)
+    {
+        atomic_max_nonneg(scal + S_PDELTA, v[0]);
+        atomic_max_nonneg(scal + S_UMAX, v[1]);
+        atomic_max_nonneg(scal + S_DUMAX, v[2]);
+        if (bad) atomic_max_nonneg(scal + S_NONFINITE, 1.0);
+        if (blockIdx.x == 0) scal[S_AP] = aP;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_axpby_rhs(int n, CV3P base, V3P rhs, int nc)
+{
+    ROW_LOOP(c, n)
+    for (int q = 0; q < nc; ++q) rhs.c[q][c] = base.c[q][c];
+}
+
+/// h = rhs - (A x - diag x) (fvMatrix::explicitOperator, fvMatrix.cpp:131-146)
+__global__ void __launch_bounds__(TPB) k_explicit_op(DMat A, const double* __restrict__ val,
+                                                     const double* __restrict__ diag, const double* __restrict__ rhs,
+                                                     const double* __restrict__ x, double* h)
+{
+    const double* xs[1] = {x};
+    ROW_LOOP(c, A.n)
+    {
+        double y[1];
+        spmv_row<1>(A, val, c, xs, y);
+        h[c] = rhs[c] - (y[0] - diag[c] * x[c]);
+    }
+}
+
+// ===========================================================================
+// host side
+// ===========================================================================
+
+template <class T>
+T* Ctx::alloc(size_t n)
+{
+    void* p = nullptr;
+    CFG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    allocs_.push_back(p);
+    CFG_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), stream_));
+    return static_cast<T*>(p);
+}
+
+template <class T>
+T* Ctx::upload(const std::vector<T>& v)
+{
+    T* p = alloc<T>(v.size());
+    if (!v.empty()) CFG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    return p;
+}
+
+namespace
+{
+inline double hdot(const Vec& a, const Vec& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+}
+
+Ctx::Ctx(const Mesh& mesh, int device, cudaStream_t stream) : mesh_(mesh), device_(device), stream_(stream)
+{
+    if (mesh_.nCells >= (1LL << 30) || mesh_.nFaces() >= (1LL << 30))
+        fail(CFG_EINVAL, "mesh too large for 32-bit device indices");
+    CFG_CUDA(cudaSetDevice(device_));
+    if (!stream_)
+    {
+        CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        ownStream_ = true;
+    }
+    const size_t nP = mesh_.patches.size();
+    uType_.assign(nP, CFG_BC_ZERO_GRADIENT);
+    pType_.assign(nP, CFG_BC_ZERO_GRADIENT);
+    uVal_.assign(nP, Vec{});
+    pVal_.assign(nP, 0.0);
+    for (int i = 0; i < 16; ++i) CFG_CUDA(cudaEventCreate(&tm_.ev[i]));
+    buildDevice();
+}
+
+Ctx::~Ctx()
+{
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    for (void* p : allocs_) cudaFree(p);
+    if (stHost_) cudaFreeHost(stHost_);
+    if (scalHost_) cudaFreeHost(scalHost_);
+    for (int i = 0; i < 16; ++i) cudaEventDestroy(tm_.ev[i]);
+    if (ownStream_) cudaStreamDestroy(stream_);
+}
+
+void Ctx::buildDevice()
+{
+    const Mesh& M = mesh_;
+    const int nC = static_cast<int>(M.nCells), nF = static_cast<int>(M.nFaces()), nI = static_cast<int>(M.nInternal());
+    const int nB = nF - nI;
+    nSlices_ = (nC + 31) / 32;
+    DMesh& d = dm_;
+    d.nC = nC;
+    d.nF = nF;
+    d.nI = nI;
+    d.nB = nB;
+    d.nRowsPad = nSlices_ * 32;
+    int sms = 0;
+    CFG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+    G_ = std::max(1, std::min((nC + TPB - 1) / TPB, sms * 8));
+    GF_ = std::max(1, std::min((nF + TPB - 1) / TPB, sms * 8));
+
+    // ---- per-face geometry derived on the host in the reference's order ----
+    std::vector<int> own(nF), nbr(std::max(nI, 1));
+    std::vector<double> sfx(nF), sfy(nF), sfz(nF), oc(nF), sfd(nF), dd2(nF), cvx(nF), cvy(nF), cvz(nF);
+    std::vector<double> wq(std::max(nI, 1)), skx(std::max(nI, 1)), sky(std::max(nI, 1)), skz(std::max(nI, 1));
+    std::vector<double> fcx(nF), fcy(nF), fcz(nF), cx(nC), cy(nC), cz(nC), lscale(nC, 0.0);
+    const std::vector<double> ow = M.ownerWeights();
+    const std::vector<Vec> skew = M.skewVectors(ow);
+    for (int f = 0; f < nF; ++f)
+    {
+        own[f] = static_cast<int>(M.owner[f]);
+        const Vec& s = M.Sf[f];
+        const Vec& dv = M.d[f];
+        sfx[f] = s.x;
+        sfy[f] = s.y;
+        sfz[f] = s.z;
+        const double d2 = hdot(dv, dv);
+        dd2[f] = d2;
+        sfd[f] = hdot(s, dv);
+        oc[f] = hdot(s, dv) / d2;  // orthoCoeff (laplacianScheme.cpp:122-129)
+        const double dm = std::sqrt(hdot(dv, dv));
+        const Vec dh{dv.x / dm, dv.y / dm, dv.z / dm};
+        const double sdh = hdot(s, dh);
+        cvx[f] = s.x - dh.x * sdh;
+        cvy[f] = s.y - dh.y * sdh;
+        cvz[f] = s.z - dh.z * sdh;
+        fcx[f] = M.Cf[f].x;
+        fcy[f] = M.Cf[f].y;
+        fcz[f] = M.Cf[f].z;
+        const double a = M.magSf[f];
+        const int o = own[f];
+        lscale[o] = lscale[o] < a ? a : lscale[o];
+        if (f < nI)
+        {
+            const int n = static_cast<int>(M.neighbour[f]);
+            nbr[f] = n;
+            lscale[n] = lscale[n] < a ? a : lscale[n];
+            // volScalarField::faceValue weight (volFields.cpp:104-109)
+            const Vec t = M.Cf[f] - M.C[o];
+            const double x = d2 > 0 ? hdot(t, dv) / d2 : 0.0;
+            const double mx0 = (0.0 < x) ? x : 0.0;
+            wq[f] = d2 > 0 ? ((mx0 < 1.0) ? mx0 : 1.0) : 0.5;
+            skx[f] = skew[f].x;
+            sky[f] = skew[f].y;
+            skz[f] = skew[f].z;
+        }
+    }
+    for (int c = 0; c < nC; ++c)
+    {
+        cx[c] = M.C[c].x;
+        cy[c] = M.C[c].y;
+        cz[c] = M.C[c].z;
+    }
+
+    // ---- cell -> face lists (ascending faces) and matrix rows ----
+    std::vector<int> cnt(nC, 0), rowCnt(nC, 1);
+    for (int f = 0; f < nF; ++f)
+    {
+        ++cnt[own[f]];
+        if (f < nI)
+        {
+            ++cnt[nbr[f]];
+            ++rowCnt[own[f]];
+            ++rowCnt[nbr[f]];
+        }
+    }
+    std::vector<int> cStart(nC + 1, 0);
+    for (int c = 0; c < nC; ++c) cStart[c + 1] = cStart[c] + cnt[c];
+    std::vector<int> listF(cStart[nC]), fill(nC, 0);
+    for (int f = 0; f < nF; ++f)
+    {
+        const int o = own[f];
+        listF[cStart[o] + fill[o]++] = f << 1;
+        if (f < nI)
+        {
+            const int n = nbr[f];
+            listF[cStart[n] + fill[n]++] = (f << 1) | 1;
+        }
+    }
+    std::vector<int> cfStart(nSlices_ + 1, 0), mStart(nSlices_ + 1, 0);
+    for (int s = 0; s < nSlices_; ++s)
+    {
+        int w = 0, wm = 0;
+        for (int l = 0; l < 32; ++l)
+        {
+            const int c = 32 * s + l;
+            if (c >= nC) break;
+            w = std::max(w, cnt[c]);
+            wm = std::max(wm, rowCnt[c]);
+        }
+        cfStart[s + 1] = cfStart[s] + 32 * w;
+        mStart[s + 1] = mStart[s] + 32 * wm;
+    }
+    std::vector<int> cfCode(cfStart[nSlices_], -1), cfOther(cfStart[nSlices_], 0);
+    std::vector<int> mCol(mStart[nSlices_], -1), mCode(mStart[nSlices_], -1);
+    std::vector<std::pair<int, int>> row;  // (col, code)
+    for (int c = 0; c < nC; ++c)
+    {
+        const int s = c >> 5, l = c & 31;
+        row.clear();
+        row.push_back({c, -2});
+        for (int k = 0; k < cnt[c]; ++k)
+        {
+            const int code = listF[cStart[c] + k];
+            const int f = code >> 1;
+            const int e = cfStart[s] + 32 * k + l;
+            cfCode[e] = code;
+            if (f < nI)
+            {
+                const int other = (code & 1) ? own[f] : nbr[f];
+                cfOther[e] = other;
+                row.push_back({other, code});
+            }
+            else
+            {
+                cfOther[e] = f - nI;
+            }
+        }
+        // CSR column order (Matrix.cpp:72-76); entries with equal columns
+        // (two faces between the same cells) stay separate, in face order
+        std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (size_t k = 0; k < row.size(); ++k)
+        {
+            const int e = mStart[s] + 32 * static_cast<int>(k) + l;
+            mCol[e] = row[k].first;
+            mCode[e] = row[k].second;
+        }
+    }
+
+    d.own = upload(own);
+    d.nbr = upload(nbr);
+    d.sfx = upload(sfx);
+    d.sfy = upload(sfy);
+    d.sfz = upload(sfz);
+    {
+        std::vector<double> owv(ow.begin(), ow.end());
+        d.ow = upload(owv);
+    }
+    d.wq = upload(wq);
+    d.skx = upload(skx);
+    d.sky = upload(sky);
+    d.skz = upload(skz);
+    d.oc = upload(oc);
+    d.sfd = upload(sfd);
+    d.dd2 = upload(dd2);
+    d.cvx = upload(cvx);
+    d.cvy = upload(cvy);
+    d.cvz = upload(cvz);
+    d.V = upload(M.V);
+    d.lscale = upload(lscale);
+    d.cx = upload(cx);
+    d.cy = upload(cy);
+    d.cz = upload(cz);
+    d.fcx = upload(fcx);
+    d.fcy = upload(fcy);
+    d.fcz = upload(fcz);
+    d.cfStart = upload(cfStart);
+    d.cfCode = upload(cfCode);
+    d.cfOther = upload(cfOther);
+    d.mStart = upload(mStart);
+    d.mCol = upload(mCol);
+    d.mCode = upload(mCode);
+
+    const size_t nE = static_cast<size_t>(mStart[nSlices_]);
+    auto v3 = [&](V3P& v, size_t n) {
+        for (int q = 0; q < 3; ++q) v.c[q] = alloc<double>(n);
+    };
+    for (int q = 0; q < 3; ++q)
+    {
+        uc_[q] = alloc<double>(nB);
+        uk_[q] = alloc<double>(nB);
+        hc_[q] = alloc<double>(nB);
+        hk_[q] = alloc<double>(nB);
+    }
+    pc_ = alloc<double>(nB);
+    pk_ = alloc<double>(nB);
+    v3(U_, nC);
+    v3(gPn_, nC);
+    v3(gPF_, nC);
+    v3(Hf_, nC);
+    v3(gA_, nC);
+    v3(gB_, nC);
+    v3(uBase_, nC);
+    v3(uRhs_, nC);
+    v3(ux_, nC);
+    p_ = alloc<double>(nC);
+    phi_ = alloc<double>(nF);
+    rAUr_ = alloc<double>(nC);
+    rAUf_ = alloc<double>(nF);
+    uDiag_ = alloc<double>(nC);
+    pDiag_ = alloc<double>(nC);
+    pBase_ = alloc<double>(nC);
+    pRhs_ = alloc<double>(nC);
+    px_ = alloc<double>(nC);
+    mVal_ = alloc<double>(nE);
+    pVal_d_ = alloc<double>(nE);
+    cr_ = alloc<double>(nC);
+    cp_ = alloc<double>(nC);
+    cAp_ = alloc<double>(nC);
+    v3(br_, nC);
+    v3(br0_, nC);
+    v3(bp_, nC);
+    v3(bv_, nC);
+    v3(bs_, nC);
+    v3(bsh_, nC);
+    v3(bt_, nC);
+    v3(bz_, nC);
+    gU_ = alloc<double>(nF);
+    fScratch_ = alloc<double>(nF);
+    bScratch_ = alloc<double>(2 * static_cast<size_t>(nB));
+    {
+        std::vector<int> ps, pz;
+        for (const auto& p : M.patches)
+        {
+            ps.push_back(static_cast<int>(p.start));
+            pz.push_back(static_cast<int>(p.size));
+        }
+        dpStart_ = upload(ps);
+        dpSize_ = upload(pz);
+        dpFree_ = alloc<int>(ps.size());
+        dFreeFace_ = alloc<int>(nB);
+        dEmptyFace_ = alloc<int>(nB);
+    }
+    partials_ = alloc<double>(static_cast<size_t>(16) * std::max(G_, GF_));
+    st_ = alloc<SolveState>(1);
+    scal_ = alloc<double>(S_COUNT);
+    CFG_CUDA(cudaMallocHost(&stHost_, sizeof(SolveState)));
+    CFG_CUDA(cudaMallocHost(&scalHost_, sizeof(double) * S_COUNT));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::setPatchBC(char field, int patch, int type, const double* value)
+{
+    if (patch < 0 || patch >= static_cast<int>(mesh_.patches.size())) fail(CFG_EINVAL, "patch index out of range");
+    if (type < CFG_BC_FIXED_VALUE || type > CFG_BC_EMPTY) fail(CFG_EINVAL, "unknown boundary-condition type");
+    if (field == 'U')
+    {
+        uType_[patch] = type;
+        uVal_[patch] = value ? Vec{value[0], value[1], value[2]} : Vec{};
+    }
+    else if (field == 'p')
+    {
+        pType_[patch] = type;
+        pVal_[patch] = value ? value[0] : 0.0;
+    }
+    else
+    {
+        fail(CFG_EINVAL, "field must be 'U' or 'p'");
+    }
+    bcDirty_ = true;
+}
+
+void Ctx::setFaceValuesU(int64_t n, const int64_t* faces, const double* values)
+{
+    for (int64_t i = 0; i < n; ++i)
+    {
+        const int64_t f = faces[i];
+        if (f < mesh_.nInternal() || f >= mesh_.nFaces())
+            fail(CFG_EINVAL, "volVectorField::setFaceValue: internal face " + std::to_string(f));
+        uFace_[f] = Vec{values[3 * i], values[3 * i + 1], values[3 * i + 2]};
+    }
+    bcDirty_ = true;
+}
+
+void Ctx::clearFaceValuesU()
+{
+    uFace_.clear();
+    bcDirty_ = true;
+}
+
+namespace
+{
+// volVectorField::linearise for one face and component (volFields.cpp:246-283)
+void linVector(const Mesh& M, int type, const Vec& patchVal, const Vec* faceVal, int64_t f, int comp, double& c,
+               double& k)
+{
+    const Vec value = faceVal ? *faceVal : patchVal;
+    auto cmp = [](const Vec& v, int q) { return q == 0 ? v.x : (q == 1 ? v.y : v.z); };
+    switch (type)
+    {
+    case CFG_BC_FIXED_VALUE:
+        c = 0;
+        k = cmp(value, comp);
+        return;
+    case CFG_BC_FIXED_GRADIENT:
+    {
+        const Vec& sf = M.Sf[f];
+        const double a = std::sqrt(hdot(sf, sf));
+        const Vec n{sf.x / a, sf.y / a, sf.z / a};
+        c = 1;
+        k = cmp(patchVal, comp) * hdot(M.d[f], n);
+        return;
+    }
+    case CFG_BC_ZERO_GRADIENT:
+    case CFG_BC_OUTLET:
+        c = 1;
+        k = 0;
+        return;
+    case CFG_BC_SYMMETRY:
+    case CFG_BC_WALL:
+    {
+        const Vec& sf = M.Sf[f];
+        const double a = std::sqrt(hdot(sf, sf));
+        const double ax = std::abs(sf.x / a), ay = std::abs(sf.y / a), az = std::abs(sf.z / a);
+        int axis;
+        double big;
+        if (ax >= ay && ax >= az) { axis = 0; big = ax; }
+        else if (ay >= az) { axis = 1; big = ay; }
+        else { axis = 2; big = az; }
+        if (big < 1.0 - 1e-6) fail(CFG_ESETUP, "fields: symmetry normal not axis aligned");
+        c = (comp == axis) ? 0.0 : 1.0;
+        k = 0;
+        return;
+    }
+    default:
+        fail(CFG_ESETUP, "volVectorField: unknown patch bc type");
+    }
+}
+
+// volScalarField::linearise (volFields.cpp:117-147)
+void linScalar(const Mesh& M, int type, double value, int64_t f, double& c, double& k)
+{
+    switch (type)
+    {
+    case CFG_BC_FIXED_VALUE:
+        c = 0;
+        k = value;
+        return;
+    case CFG_BC_FIXED_GRADIENT:
+    {
+        const Vec& sf = M.Sf[f];
+        const double a = std::sqrt(hdot(sf, sf));
+        const Vec n{sf.x / a, sf.y / a, sf.z / a};
+        c = 1;
+        k = value * hdot(M.d[f], n);
+        return;
+    }
+    case CFG_BC_ZERO_GRADIENT:
+    case CFG_BC_SYMMETRY:
+    case CFG_BC_OUTLET:
+        c = 1;
+        k = 0;
+        return;
+    default:
+        fail(CFG_ESETUP, "volScalarField: unknown patch bc type");
+    }
+}
+}  // namespace
+
+void Ctx::refreshBc()
+{
+    if (!bcDirty_) return;
+    const Mesh& M = mesh_;
+    const int64_t nI = M.nInternal(), nB = M.nBoundary();
+    std::vector<double> uc[3], uk[3], hc[3], hk[3], pc(nB), pk(nB);
+    for (int q = 0; q < 3; ++q)
+    {
+        uc[q].resize(nB);
+        uk[q].resize(nB);
+        hc[q].resize(nB);
+        hk[q].resize(nB);
+    }
+    nFreeUFaces_ = 0;
+    for (int64_t b = 0; b < nB; ++b)
+    {
+        const int64_t f = nI + b;
+        const int pi = static_cast<int>(M.facePatch[f]);
+        auto it = uFace_.find(f);
+        const Vec* fv = it == uFace_.end() ? nullptr : &it->second;
+        const int ut = uType_[pi];
+        // constrainHbyA (simpleSolver.cpp:175-187): fixedValue where U is,
+        // zeroGradient elsewhere, with U's per-face values adopted
+        const bool fixed = ut == CFG_BC_FIXED_VALUE;
+        for (int q = 0; q < 3; ++q)
+        {
+            if (ut == CFG_BC_EMPTY)
+            {
+                uc[q][b] = 0;
+                uk[q][b] = 0;
+            }
+            else
+            {
+                linVector(M, ut, uVal_[pi], fv, f, q, uc[q][b], uk[q][b]);
+            }
+            linVector(M, fixed ? CFG_BC_FIXED_VALUE : CFG_BC_ZERO_GRADIENT, fixed ? uVal_[pi] : Vec{}, fv, f, q,
+                      hc[q][b], hk[q][b]);
+        }
+        const int pt = pType_[pi];
+        if (pt == CFG_BC_FIXED_VALUE || pt == CFG_BC_FIXED_GRADIENT || pt == CFG_BC_ZERO_GRADIENT ||
+            pt == CFG_BC_SYMMETRY || pt == CFG_BC_OUTLET)
+            linScalar(M, pt, pVal_[pi], f, pc[b], pk[b]);
+        else
+            pc[b] = pk[b] = NAN;  // rejected when the pressure equation is built
+        if (!fixed) ++nFreeUFaces_;
+    }
+    for (int q = 0; q < 3; ++q)
+    {
+        CFG_CUDA(cudaMemcpyAsync(uc_[q], uc[q].data(), nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaMemcpyAsync(uk_[q], uk[q].data(), nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaMemcpyAsync(hc_[q], hc[q].data(), nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaMemcpyAsync(hk_[q], hk[q].data(), nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    }
+    {
+        std::vector<int> pfree(M.patches.size()), ffree(nB), fempty(nB);
+        needReference_ = true;
+        for (size_t pi = 0; pi < M.patches.size(); ++pi)
+        {
+            pfree[pi] = uType_[pi] != CFG_BC_FIXED_VALUE;
+            if (pType_[pi] == CFG_BC_FIXED_VALUE) needReference_ = false;
+        }
+        for (int64_t b = 0; b < nB; ++b)
+        {
+            const int pi = static_cast<int>(M.facePatch[nI + b]);
+            ffree[b] = pfree[pi];
+            fempty[b] = uType_[pi] == CFG_BC_EMPTY;
+        }
+        if (!pfree.empty())
+            CFG_CUDA(cudaMemcpyAsync(dpFree_, pfree.data(), pfree.size() * sizeof(int), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaMemcpyAsync(dFreeFace_, ffree.data(), nB * sizeof(int), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaMemcpyAsync(dEmptyFace_, fempty.data(), nB * sizeof(int), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+    }
+    CFG_CUDA(cudaMemcpyAsync(pc_, pc.data(), nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(pk_, pk.data(), nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    bcDirty_ = false;
+}
+
+void Ctx::launchCheck(const char* what)
+{
+    ++launches_;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) fail(CFG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace
+{
+CV3P cv(const V3P& v) { return CV3P{{v.c[0], v.c[1], v.c[2]}}; }
+}  // namespace
+
+/// fvc::grad of NC cell fields into gA_ (NC = 1) or gA_/gB_/... (see callers):
+/// scheme linear | corrected | leastSquares; volQuirk selects the
+/// volScalarField overload's internal face value for the linear scheme.
+void Ctx::gradCells(const double* const* x, int nComp, const BcTab& bc, int scheme, bool volQuirk, V3P* out)
+{
+    CV3P xs{{x[0], nComp > 1 ? x[1] : x[0], nComp > 2 ? x[2] : x[0]}};
+    Grad3 o{};
+    for (int q = 0; q < nComp; ++q) o.g[q] = out[q];
+    if (scheme == CFG_GRAD_LEAST_SQUARES)
+    {
+        // stage 1 into out, stage 2 reads it and writes the scratch set, then copy back
+        if (nComp == 1)
+        {
+            k_grad_ls1<1><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, o);
+            launchCheck("grad_ls1");
+            Grad3 o2{};
+            o2.g[0] = gB_;
+            k_grad_ls2<1><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, CGrad3{{cv(out[0])}}, o2);
+            launchCheck("grad_ls2");
+            for (int q = 0; q < 3; ++q)
+                CFG_CUDA(cudaMemcpyAsync(out[0].c[q], gB_.c[q], dm_.nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        }
+        else
+        {
+            // three components: stage 1 into out, stage 2 into the U-equation
+            // scratch (solver work vectors are free while gradients run)
+            k_grad_ls1<3><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, o);
+            launchCheck("grad_ls1");
+            Grad3 o2{};
+            o2.g[0] = bs_;
+            o2.g[1] = bsh_;
+            o2.g[2] = bt_;
+            k_grad_ls2<3><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, CGrad3{{cv(out[0]), cv(out[1]), cv(out[2])}}, o2);
+            launchCheck("grad_ls2");
+            for (int q = 0; q < 3; ++q)
+                for (int k = 0; k < 3; ++k)
+                    CFG_CUDA(cudaMemcpyAsync(out[q].c[k], o2.g[q].c[k], dm_.nC * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, stream_));
+        }
+        return;
+    }
+    const bool corrected = scheme == CFG_GRAD_CORRECTED;
+    if (nComp == 1)
+    {
+        k_grad_gauss0<1><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, (!corrected && volQuirk) ? 1 : 0, o);
+        launchCheck("grad_gauss0");
+        if (!corrected) return;
+        Grad3 t{};
+        t.g[0] = gB_;
+        k_grad_gauss_corr<1><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, CGrad3{{cv(out[0])}}, t);
+        launchCheck("grad_corr");
+        k_grad_gauss_corr<1><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, CGrad3{{cv(gB_)}}, o);
+        launchCheck("grad_corr");
+    }
+    else
+    {
+        k_grad_gauss0<3><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, 0, o);
+        launchCheck("grad_gauss0");
+        if (!corrected) return;
+        Grad3 t{};
+        t.g[0] = bs_;
+        t.g[1] = bsh_;
+        t.g[2] = bt_;
+        k_grad_gauss_corr<3><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, CGrad3{{cv(out[0]), cv(out[1]), cv(out[2])}}, t);
+        launchCheck("grad_corr");
+        k_grad_gauss_corr<3><<<G_, TPB, 0, stream_>>>(dm_, xs, bc, CGrad3{{cv(bs_), cv(bsh_), cv(bt_)}}, o);
+        launchCheck("grad_corr");
+    }
+}
+
+void Ctx::runCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                cfg_solver_report* rep)
+{
+    const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
+    SolveState init{};
+    init.tol = tol;
+    init.maxIter = maxIter;
+    init.nComp = 1;
+    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    k_cg_init<<<G_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
+    launchCheck("cg_init");
+    int launched = 0;
+    int chunk = 8;
+    for (;;)
+    {
+        CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        if (stHost_->allDone || launched >= maxIter) break;
+        const int n = std::min(chunk, maxIter - launched);
+        for (int k = 0; k < n; ++k)
+        {
+            k_cg_spmv<<<G_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
+            k_cg_update<<<G_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
+            k_cg_p<<<G_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
+            launches_ += 2;
+            launchCheck("cg_iter");
+        }
+        launched += n;
+        chunk = std::min(chunk * 2, 64);
+    }
+    rep->iterations = stHost_->it[0];
+    rep->converged = stHost_->conv[0];
+    rep->initial_residual = stHost_->init[0];
+    rep->final_residual = stHost_->conv[0] && stHost_->it[0] == 0 ? stHost_->init[0] : stHost_->fin[0];
+}
+
+void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
+                   cfg_solver_report* reps)
+{
+    const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
+    SolveState init{};
+    init.tol = tol;
+    init.maxIter = maxIter;
+    init.nComp = nComp;
+    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    const int n = dm_.nC;
+#define BI_LAUNCH(NC)                                                                                        \
+    k_bi_init<NC><<<G_, TPB, 0, stream_>>>(A, vals, b, x, br_, br0_, bp_, bv_, partials_, st_);              \
+    launchCheck("bicg_init");                                                                                \
+    for (int launched = 0, chunk = 4;;)                                                                      \
+    {                                                                                                        \
+        CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));       \
+        CFG_CUDA(cudaStreamSynchronize(stream_));                                                            \
+        if (stHost_->allDone || launched >= maxIter) break;                                                  \
+        const int m = std::min(chunk, maxIter - launched);                                                   \
+        for (int k = 0; k < m; ++k)                                                                          \
+        {                                                                                                    \
+            k_bi_p<NC><<<G_, TPB, 0, stream_>>>(n, diag, br_, bp_, bv_, bz_, st_);                           \
+            k_bi_spmv1<NC><<<G_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);                \
+            k_bi_s<NC><<<G_, TPB, 0, stream_>>>(n, diag, x, bz_, br_, bv_, bs_, bsh_, partials_, st_);       \
+            k_bi_spmv2<NC><<<G_, TPB, 0, stream_>>>(A, vals, bsh_, bt_, bs_, partials_, st_);                \
+            k_bi_x<NC><<<G_, TPB, 0, stream_>>>(n, x, bsh_, bs_, bt_, br_, br0_, partials_, st_);            \
+            launches_ += 4;                                                                                  \
+            launchCheck("bicg_iter");                                                                        \
+        }                                                                                                    \
+        launched += m;                                                                                       \
+        chunk = std::min(chunk * 2, 32);                                                                     \
+    }
+    if (nComp == 3) { BI_LAUNCH(3) }
+    else { BI_LAUNCH(1) }
+#undef BI_LAUNCH
+    for (int q = 0; q < nComp; ++q)
+    {
+        reps[q].iterations = stHost_->it[q];
+        reps[q].converged = stHost_->conv[q];
+        reps[q].initial_residual = stHost_->init[q];
+        reps[q].final_residual = stHost_->fin[q];
+    }
+}
+
+/// fvMatrix::solve for the momentum equation (fvMatrix.cpp:73-129): x from
+/// zero, nonOrth+1 passes when the laplacian is corrected, each restoring the
+/// base rhs and adding the corrector evaluated on the current x.
+void Ctx::solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, int64_t& inner)
+{
+    const int n = dm_.nC;
+    for (int q = 0; q < 3; ++q) CFG_CUDA(cudaMemsetAsync(ux_.c[q], 0, n * sizeof(double), stream_));
+    const bool corr = schemes_.laplacian_corrected != 0;
+    const int passes = corr ? std::max(1, nonOrth + 1) : 1;
+    const BcTab ub{{uc_[0], uc_[1], uc_[2]}, {uk_[0], uk_[1], uk_[2]}};
+    for (int pass = 0; pass < passes; ++pass)
+    {
+        if (corr)
+        {
+            const double* xs[3] = {ux_.c[0], ux_.c[1], ux_.c[2]};
+            V3P g[3] = {gA_, gB_, Hf_};  // Hf_ is free until the solve ends
+            // gradCells with 3 components uses bs_/bsh_/bt_ as scratch
+            gradCells(xs, 3, ub, gradScheme, false, g);
+            k_corrector<3><<<G_, TPB, 0, stream_>>>(dm_, gU_, CGrad3{{cv(g[0]), cv(g[1]), cv(g[2])}},
+                                                   cv(uBase_), uRhs_);
+            launchCheck("corrector_U");
+        }
+        else
+        {
+            for (int q = 0; q < 3; ++q)
+                CFG_CUDA(cudaMemcpyAsync(uRhs_.c[q], uBase_.c[q], n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        }
+        cfg_solver_report reps[3];
+        runBiCG3(mVal_, uDiag_, uRhs_, ux_, 3, tol, maxIter, reps);
+        for (int q = 0; q < 3; ++q) inner += reps[q].iterations;
+    }
+}
+
+void Ctx::setNu(double nu)
+{
+    if (nu == lastNu_) return;
+    // harmonicFaceGamma of a uniform cell viscosity (laplacianScheme.cpp:146-171)
+    const Mesh& M = mesh_;
+    const int64_t nF = M.nFaces(), nI = M.nInternal();
+    std::vector<double> g(static_cast<size_t>(nF));
+    for (int64_t f = 0; f < nF; ++f)
+    {
+        if (f < nI)
+        {
+            const double gp = nu, gn = nu;
+            const Vec& cP = M.C[M.owner[f]];
+            const Vec& cN = M.C[M.neighbour[f]];
+            const Vec& cf = M.Cf[f];
+            const Vec a{cf.x - cP.x, cf.y - cP.y, cf.z - cP.z}, b{cN.x - cf.x, cN.y - cf.y, cN.z - cf.z};
+            const double dP = std::sqrt(hdot(a, a)), dN = std::sqrt(hdot(b, b));
+            const double tot = dP + dN;
+            g[f] = (tot > 0 && gp > 0 && gn > 0) ? tot * gp * gn / (dN * gp + dP * gn) : 0.5 * (gp + gn);
+        }
+        else
+        {
+            g[f] = nu;
+        }
+    }
+    CFG_CUDA(cudaMemcpyAsync(gU_, g.data(), nF * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    lastNu_ = nu;
+}
+
+void Ctx::checkMomentumBcs() const
+{
+    // the reference builds the momentum matrix with the BC linearisation of
+    // every component; symmetry / wall velocity conditions give components
+    // different diagonals, which solveIncompressibleSimple rejects
+    // (simpleSolver.cpp:123-138), and an unknown type is fatal at the first
+    // linearisation (volFields.cpp:279-282)
+    for (size_t pi = 0; pi < mesh_.patches.size(); ++pi)
+    {
+        if (mesh_.patches[pi].size == 0) continue;
+        const int t = uType_[pi];
+        if (t == CFG_BC_SYMMETRY || t == CFG_BC_WALL)
+            fail(CFG_ENUMERIC, "SIMPLE: momentum diagonal differs between components");
+        if (t == CFG_BC_EMPTY) fail(CFG_ESETUP, "volVectorField: unknown patch bc type 'empty'");
+        const int pt = pType_[pi];
+        if (pt == CFG_BC_WALL || pt == CFG_BC_EMPTY) fail(CFG_ESETUP, "volScalarField: unknown patch bc type");
+    }
+}
+
+void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner)
+{
+    (void)precond;
+    const int n = dm_.nC;
+    CFG_CUDA(cudaMemsetAsync(px_, 0, n * sizeof(double), stream_));
+    const bool corr = schemes_.laplacian_corrected != 0;
+    const int passes = corr ? std::max(1, nonOrth + 1) : 1;
+    const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
+    for (int pass = 0; pass < passes; ++pass)
+    {
+        if (corr)
+        {
+            const double* xs[1] = {px_};
+            V3P g[1] = {gA_};
+            gradCells(xs, 1, pb, gradScheme, false, g);
+            k_corrector<1><<<G_, TPB, 0, stream_>>>(dm_, rAUf_, CGrad3{{cv(gA_)}}, CV3P{{pBase_, pBase_, pBase_}},
+                                                   V3P{{pRhs_, pRhs_, pRhs_}});
+            launchCheck("corrector_p");
+        }
+        else
+        {
+            CFG_CUDA(cudaMemcpyAsync(pRhs_, pBase_, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        }
+        cfg_solver_report rep;
+        runCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
+        inner += rep.iterations;
+    }
+}
+
+void Ctx::upload(const double* U, const double* p, const double* phi)
+{
+    const int nC = dm_.nC, nF = dm_.nF;
+    if (U)
+    {
+        std::vector<double> t(static_cast<size_t>(nC));
+        for (int q = 0; q < 3; ++q)
+        {
+            for (int c = 0; c < nC; ++c) t[c] = U[3 * static_cast<size_t>(c) + q];
+            CFG_CUDA(cudaMemcpyAsync(U_.c[q], t.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+        }
+    }
+    if (p) CFG_CUDA(cudaMemcpyAsync(p_, p, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    if (phi) CFG_CUDA(cudaMemcpyAsync(phi_, phi, nF * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::download(double* U, double* p, double* phi)
+{
+    const int nC = dm_.nC, nF = dm_.nF;
+    if (U)
+    {
+        std::vector<double> t(static_cast<size_t>(nC));
+        for (int q = 0; q < 3; ++q)
+        {
+            CFG_CUDA(cudaMemcpyAsync(t.data(), U_.c[q], nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+            for (int c = 0; c < nC; ++c) U[3 * static_cast<size_t>(c) + q] = t[c];
+        }
+    }
+    if (p) CFG_CUDA(cudaMemcpyAsync(p, p_, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    if (phi) CFG_CUDA(cudaMemcpyAsync(phi, phi_, nF * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::initFlux(const double* u0)
+{
+    refreshBc();
+    const BcTab ub{{uc_[0], uc_[1], uc_[2]}, {uk_[0], uk_[1], uk_[2]}};
+    if (u0)
+    {
+        std::vector<double> t(static_cast<size_t>(dm_.nC));
+        for (int q = 0; q < 3; ++q)
+        {
+            std::fill(t.begin(), t.end(), u0[q]);
+            CFG_CUDA(cudaMemcpyAsync(U_.c[q], t.data(), dm_.nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+        }
+    }
+    // correctBoundaryFlux(U) (+ updatePhiInternal first when seeded; the
+    // internal flux is untouched otherwise, as in simpleFoamApp.cpp:94-95)
+    if (u0)
+    {
+        k_flux_internal<<<GF_, TPB, 0, stream_>>>(dm_, cv(U_), phi_);
+        launchCheck("flux_internal");
+    }
+    // boundary faces: the flux kernel into scratch, then only the boundary
+    // part copied over, so internal faces keep their values
+    const int nF = dm_.nF, nI = dm_.nI;
+    k_flux<<<GF_, TPB, 0, stream_>>>(dm_, cv(U_), ub, dEmptyFace_, fScratch_);
+    launchCheck("flux");
+    if (nF > nI)
+        CFG_CUDA(cudaMemcpyAsync(phi_ + nI, fScratch_ + nI, (nF - nI) * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
+{
+    CFG_CUDA(cudaSetDevice(device_));
+    refreshBc();
+    checkMomentumBcs();
+    setNu(ctl.nu);
+    std::memset(&res, 0, sizeof res);
+    const int nC = dm_.nC;
+    const int gs = schemes_.grad;
+    const double alpha = schemes_.div == CFG_DIV_BLEND ? schemes_.blend_coeff : (schemes_.div == CFG_DIV_LINEAR ? 1.0 : 0.0);
+    const BcTab ub{{uc_[0], uc_[1], uc_[2]}, {uk_[0], uk_[1], uk_[2]}};
+    const BcTab hb{{hc_[0], hc_[1], hc_[2]}, {hk_[0], hk_[1], hk_[2]}};
+    const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
+    const bool doAdjust = needReference_ && nFreeUFaces_ > 0;
+    if (ctl.p_ref_cell >= nC) fail(CFG_EINVAL, "p_ref_cell beyond the last cell");
+    const int refCell = ctl.p_ref_cell >= 0 ? static_cast<int>(ctl.p_ref_cell) : -1;
+    double contLag1 = INFINITY, contLag2 = INFINITY;
+    launches_ = 0;
+    for (int k = 0; k < 8; ++k) lastMs[k] = 0.0;
+    CFG_CUDA(cudaEventRecord(tm_.ev[0], stream_));
+    for (int iter = 1; iter <= ctl.max_iterations; ++iter)
+    {
+        CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
+        // ---- momentum ----
+        {
+            const double* xs[1] = {p_};
+            V3P g[1] = {gPn_};
+            gradCells(xs, 1, pb, gs, true, g);
+        }
+        MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
+                   mVal_, uDiag_, uBase_};
+        k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
+        launchCheck("assemble_U");
+        solveMomentum(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, res.u_inner_iterations);
+        k_hfree<<<G_, TPB, 0, stream_>>>(dm_, uDiag_, cv(U_), cv(ux_), ctl.relax_u, Hf_, rAUr_);
+        launchCheck("hfree");
+        // ---- predictor flux ----
+        k_flux<<<GF_, TPB, 0, stream_>>>(dm_, cv(Hf_), hb, nullptr, phi_);
+        launchCheck("flux");
+        if (doAdjust)
+        {
+            k_adjust_sums<<<1, 32, 0, stream_>>>(phi_, dpStart_, dpSize_, dpFree_,
+                                                 static_cast<int>(mesh_.patches.size()), scal_);
+            launchCheck("adjust_sums");
+            k_adjust_scale<<<GF_, TPB, 0, stream_>>>(dm_.nB, dm_.nI, dFreeFace_, phi_, scal_);
+            launchCheck("adjust_scale");
+        }
+        // ---- pressure ----
+        k_face_interp<<<GF_, TPB, 0, stream_>>>(dm_, rAUr_, rAUf_);
+        launchCheck("face_interp");
+        k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, phi_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_, refCell,
+                                              ctl.p_ref_value);
+        launchCheck("assemble_p");
+        solvePressure(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, ctl.p_precond,
+                      res.p_inner_iterations);
+        {
+            const double* xs[1] = {px_};
+            V3P g[1] = {gPF_};
+            gradCells(xs, 1, pb, gs, true, g);
+        }
+        k_correct_flux<<<GF_, TPB, 0, stream_>>>(dm_, px_, cv(gPF_), rAUf_, pc_, pk_, schemes_.laplacian_corrected,
+                                                 phi_);
+        launchCheck("correct_flux");
+        k_pstep<<<G_, TPB, 0, stream_>>>(nC, px_, p_, scal_);
+        launchCheck("pstep");
+        k_update<<<G_, TPB, 0, stream_>>>(nC, px_, p_, U_, cv(Hf_), cv(gPF_), cv(gPn_), rAUr_, ctl.relax_p,
+                                          ctl.p_relax_start, scal_);
+        launchCheck("update");
+        k_continuity<<<G_, TPB, 0, stream_>>>(dm_, phi_, scal_, S_CONT_AFTER);
+        launchCheck("continuity");
+        CFG_CUDA(cudaMemcpyAsync(scalHost_, scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        const double* S = scalHost_;
+        const double contErr = S[S_CONT], errAfter = S[S_CONT_AFTER], pDeltaMax = S[S_PDELTA];
+        const double uRes = S[S_DUMAX] / std::max(S[S_UMAX], 1e-300);
+        if (ctl.verbose)
+            std::printf("[chflow] SIMPLE iter %d: continuity %g (corrected %g, dp %g, dU %g)\n", iter, contErr, errAfter,
+                        pDeltaMax, uRes);
+        res.iterations = iter;
+        res.final_continuity_error = contErr;
+        res.final_momentum_residual = uRes;
+        res.last_dp = pDeltaMax;
+        res.last_continuity_corrected = errAfter;
+        if (!std::isfinite(contErr) || !std::isfinite(pDeltaMax) || S[S_NONFINITE] > 0)
+        {
+            res.diverged = 1;
+            if (ctl.verbose) std::printf("[chflow] error: SIMPLE: diverged at iteration %d\n", iter);
+            break;
+        }
+        const bool settled = contErr <= contLag2 * 1.01 + 1e-12;
+        const bool momentumSettled = !(ctl.momentum_tol > 0) || uRes <= ctl.momentum_tol;
+        if (momentumSettled && (contErr < ctl.continuity_tol ||
+                                (iter >= 5 && ctl.pcorr_tol > 0 && pDeltaMax < ctl.pcorr_tol && settled)))
+        {
+            res.converged = 1;
+            break;
+        }
+        contLag2 = contLag1;
+        contLag1 = contErr;
+    }
+    CFG_CUDA(cudaEventRecord(tm_.ev[1], stream_));
+    CFG_CUDA(cudaEventSynchronize(tm_.ev[1]));
+    float ms = 0;
+    CFG_CUDA(cudaEventElapsedTime(&ms, tm_.ev[0], tm_.ev[1]));
+    lastMs[7] = ms;
+    lastLaunches = launches_;
+}
+
+void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, double* out)
+{
+    // the equations of one outer iteration built from the current fields,
+    // as oracle/ref_driver.cpp's `eqns` mode builds them; out holds, in
+    // order: gradPn (3N), U diag (3N), U h0 (3N), U h1 (3N), rAUf (F),
+    // divPhi (N), contErr (1), p diag (N), p h0 (N), p h1 (N), gradPFull (3N),
+    // phiCorrected (F).  Vectors are component-major.
+    CFG_CUDA(cudaSetDevice(device_));
+    refreshBc();
+    checkMomentumBcs();
+    setNu(ctl.nu);
+    const int nC = dm_.nC, nF = dm_.nF;
+    const int gs = schemes_.grad;
+    const double alpha = schemes_.div == CFG_DIV_BLEND ? schemes_.blend_coeff : (schemes_.div == CFG_DIV_LINEAR ? 1.0 : 0.0);
+    const BcTab ub{{uc_[0], uc_[1], uc_[2]}, {uk_[0], uk_[1], uk_[2]}};
+    const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
+    const DMat A{nC, dm_.mStart, dm_.mCol};
+    double* o = out;
+    auto d2h = [&](const double* src, size_t n) {
+        CFG_CUDA(cudaMemcpyAsync(o, src, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        o += n;
+    };
+    CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
+    double* xp = cr_;
+    CFG_CUDA(cudaMemcpyAsync(xp, xprobe, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    {
+        const double* xs[1] = {p_};
+        V3P g[1] = {gPn_};
+        gradCells(xs, 1, pb, gs, true, g);
+    }
+    for (int q = 0; q < 3; ++q) d2h(gPn_.c[q], nC);
+    MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_), mVal_,
+               uDiag_, uBase_};
+    k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
+    launchCheck("assemble_U");
+    // one pass with maxIter 0: rhs = base + corrector(x = 0)
+    for (int q = 0; q < 3; ++q) CFG_CUDA(cudaMemsetAsync(ux_.c[q], 0, nC * sizeof(double), stream_));
+    if (schemes_.laplacian_corrected)
+    {
+        const double* xs[3] = {ux_.c[0], ux_.c[1], ux_.c[2]};
+        V3P g[3] = {gA_, gB_, Hf_};
+        gradCells(xs, 3, ub, gs, false, g);
+        k_corrector<3><<<G_, TPB, 0, stream_>>>(dm_, gU_, CGrad3{{cv(g[0]), cv(g[1]), cv(g[2])}}, cv(uBase_), uRhs_);
+        launchCheck("corrector_U");
+    }
+    else
+    {
+        for (int q = 0; q < 3; ++q)
+            CFG_CUDA(cudaMemcpyAsync(uRhs_.c[q], uBase_.c[q], nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    }
+    for (int q = 0; q < 3; ++q) d2h(uDiag_, nC);
+    for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < 3; ++q)
+        {
+            k_explicit_op<<<G_, TPB, 0, stream_>>>(A, mVal_, uDiag_, uRhs_.c[q], pass ? xp : ux_.c[0], cAp_);
+            launchCheck("explicit_op");
+            d2h(cAp_, nC);
+        }
+    k_hfree<<<G_, TPB, 0, stream_>>>(dm_, uDiag_, cv(U_), cv(ux_), 1.0, Hf_, rAUr_);
+    launchCheck("hfree");
+    k_face_interp<<<GF_, TPB, 0, stream_>>>(dm_, rAUr_, rAUf_);
+    launchCheck("face_interp");
+    d2h(rAUf_, nF);
+    const int refCell = ctl.p_ref_cell >= 0 && ctl.p_ref_cell < nC ? static_cast<int>(ctl.p_ref_cell) : -1;
+    k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, phi_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_, refCell,
+                                          ctl.p_ref_value);
+    launchCheck("assemble_p");
+    std::vector<double> hostScal(S_COUNT);
+    CFG_CUDA(cudaMemcpyAsync(hostScal.data(), scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    k_divphi<<<G_, TPB, 0, stream_>>>(dm_, phi_, cAp_);
+    launchCheck("divphi");
+    d2h(cAp_, nC);
+    *o++ = hostScal[S_CONT];
+    // pressure equation rhs = base + corrector(x = 0)
+    CFG_CUDA(cudaMemsetAsync(px_, 0, nC * sizeof(double), stream_));
+    if (schemes_.laplacian_corrected)
+    {
+        const double* xs[1] = {px_};
+        V3P g[1] = {gA_};
+        gradCells(xs, 1, pb, gs, false, g);
+        k_corrector<1><<<G_, TPB, 0, stream_>>>(dm_, rAUf_, CGrad3{{cv(gA_)}}, CV3P{{pBase_, pBase_, pBase_}},
+                                               V3P{{pRhs_, pRhs_, pRhs_}});
+        launchCheck("corrector_p");
+    }
+    else
+    {
+        CFG_CUDA(cudaMemcpyAsync(pRhs_, pBase_, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    }
+    d2h(pDiag_, nC);
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        k_explicit_op<<<G_, TPB, 0, stream_>>>(A, pVal_d_, pDiag_, pRhs_, pass ? xp : px_, cAp_);
+        launchCheck("explicit_op");
+        d2h(cAp_, nC);
+    }
+    {
+        const double* xs[1] = {xp};
+        V3P g[1] = {gPF_};
+        gradCells(xs, 1, pb, gs, true, g);
+    }
+    for (int q = 0; q < 3; ++q) d2h(gPF_.c[q], nC);
+    CFG_CUDA(cudaMemcpyAsync(fScratch_, phi_, nF * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    k_correct_flux<<<GF_, TPB, 0, stream_>>>(dm_, xp, cv(gPF_), rAUf_, pc_, pk_, schemes_.laplacian_corrected,
+                                             fScratch_);
+    launchCheck("correct_flux");
+    d2h(fScratch_, nF);
+}
+
+void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQuirk, double* out)
+{
+    // fvc::grad of one cell field with fixed boundary face values
+    CFG_CUDA(cudaSetDevice(device_));
+    const int nC = dm_.nC, nB = dm_.nB;
+    double* x = cr_;
+    double* k = bScratch_;
+    double* c0 = bScratch_ + nB;
+    CFG_CUDA(cudaMemcpyAsync(x, data, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(k, bvals, nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaMemsetAsync(c0, 0, nB * sizeof(double), stream_));
+    const BcTab bt{{c0, c0, c0}, {k, k, k}};
+    const double* xs[1] = {x};
+    V3P g[1] = {gPF_};
+    gradCells(xs, 1, bt, scheme, volQuirk != 0, g);
+    std::vector<double> t(nC);
+    for (int q = 0; q < 3; ++q)
+    {
+        CFG_CUDA(cudaMemcpyAsync(t.data(), gPF_.c[q], nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        for (int c = 0; c < nC; ++c) out[3 * static_cast<size_t>(c) + q] = t[c];
+    }
+}
+
+}  // namespace cfg

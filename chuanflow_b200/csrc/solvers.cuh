@@ -1,0 +1,551 @@
+// Jacobi-preconditioned CG and BiCGStab (src/common/src/Matrix.cpp:153-319)
+// as sequences of row kernels with device-resident scalars.  The global dot
+// products are block partials plus a fixed-order reduction done by the block
+// that finishes last (no block ever waits for another); that block also
+// advances the solver's scalar state, which the next kernel reads.
+#pragma once
+
+#include "ctx.h"
+#include "kernels.cuh"
+
+namespace cfg
+{
+
+__device__ __forceinline__ double inv_diag_cg(double d) { return (fabs(d) > 1e-300) ? 1.0 / d : 1.0; }
+__device__ __forceinline__ double inv_diag_bicg(double d) { return (d > 1e-300) ? 1.0 / d : 1.0; }
+
+// ------------------------------- CG ---------------------------------------
+
+/// r = b - A x; z = D^-1 r; p = z; initial residual, |b|, and r.z.
+static __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __restrict__ val,
+                                                 const double* __restrict__ diag, const double* __restrict__ b,
+                                                 const double* __restrict__ x, double* __restrict__ r,
+                                                 double* __restrict__ p, double* partials, SolveState* st)
+{
+    double mx[3] = {0.0, 0.0, 0.0};  // |r|, |b|, nan flag
+    double sm[1] = {0.0};            // r.z
+    const double* xs[1] = {x};
+    ROW_LOOP(c, A.n)
+    {
+        double y[1];
+        spmv_row<1>(A, val, c, xs, y);
+        const double bi = b[c];
+        const double ri = bi - y[0];
+        r[c] = ri;
+        const double zi = inv_diag_cg(diag[c]) * ri;
+        p[c] = zi;
+        if (isnan(ri)) mx[2] = 1.0;
+        mx[0] = smax(mx[0], fabs(ri));
+        if (isnan(bi)) mx[2] = 1.0;
+        mx[1] = smax(mx[1], fabs(bi));
+        sm[0] += ri * zi;
+    }
+    block_max<3>(mx);
+    __syncthreads();
+    block_sum<1>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = mx[0];
+        partials[G + blockIdx.x] = mx[1];
+        partials[2 * G + blockIdx.x] = mx[2];
+        partials[3 * G + blockIdx.x] = sm[0];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double fm[3], fs[1];
+    final_max<3>(partials, G, fm);
+    __syncthreads();
+    final_sum<1>(partials + 3 * G, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        const double init = fm[2] > 0 ? NAN : fm[0];
+        const double bn = smax(fm[1], 1e-300);
+        st->init[0] = init;
+        st->bnorm[0] = bn;
+        st->it[0] = 0;
+        st->conv[0] = 0;
+        st->done[0] = 0;
+        st->fin[0] = 0.0;
+        st->rz[0] = fs[0];
+        if (init / bn < st->tol)
+        {
+            st->conv[0] = 1;
+            st->done[0] = 1;
+            st->fin[0] = init;
+        }
+        else if (st->maxIter <= 0)
+        {
+            st->done[0] = 1;
+        }
+        st->allDone = st->done[0];
+    }
+}
+
+/// Ap = A p and p.Ap; breakdown test and alpha (Matrix.cpp:187-194).
+static __global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const double* __restrict__ val, const double* __restrict__ p,
+                                                 double* __restrict__ Ap, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double sm[1] = {0.0};
+    const double* xs[1] = {p};
+    ROW_LOOP(c, A.n)
+    {
+        double y[1];
+        spmv_row<1>(A, val, c, xs, y);
+        Ap[c] = y[0];
+        sm[0] += p[c] * y[0];
+    }
+    block_sum<1>(sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
+    if (!last_block(&st->ticket[0])) return;
+    double fs[1];
+    final_sum<1>(partials, gridDim.x, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        const double pAp = fs[0];
+        const double rz = st->rz[0];
+        st->pAp[0] = pAp;
+        if (pAp <= 0 || fabs(rz) < 1e-300)
+        {
+            st->done[0] = 1;
+            st->allDone = 1;
+        }
+        else
+        {
+            st->alpha[0] = rz / pAp;
+        }
+    }
+}
+
+/// x += alpha p; r -= alpha Ap; |r|inf test; z = D^-1 r; beta (Matrix.cpp:195-217).
+static __global__ void __launch_bounds__(TPB) k_cg_update(int n, const double* __restrict__ diag, const double* __restrict__ p,
+                                                   const double* __restrict__ Ap, double* __restrict__ x,
+                                                   double* __restrict__ r, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    const double alpha = st->alpha[0];
+    double mx[2] = {0.0, 0.0};
+    double sm[1] = {0.0};
+    ROW_LOOP(c, n)
+    {
+        x[c] = x[c] + alpha * p[c];
+        const double ri = r[c] - alpha * Ap[c];
+        r[c] = ri;
+        if (isnan(ri)) mx[1] = 1.0;
+        mx[0] = smax(mx[0], fabs(ri));
+        const double zi = inv_diag_cg(diag[c]) * ri;
+        sm[0] += ri * zi;
+    }
+    block_max<2>(mx);
+    __syncthreads();
+    block_sum<1>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = mx[0];
+        partials[G + blockIdx.x] = mx[1];
+        partials[2 * G + blockIdx.x] = sm[0];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double fm[2], fs[1];
+    final_max<2>(partials, G, fm);
+    __syncthreads();
+    final_sum<1>(partials + 2 * G, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        const int it = st->it[0] + 1;
+        st->it[0] = it;
+        const double fin = fm[1] > 0 ? NAN : fm[0];
+        st->fin[0] = fin;
+        if (fin / st->bnorm[0] < st->tol)
+        {
+            st->conv[0] = 1;
+            st->done[0] = 1;
+        }
+        else if (isnan(fin))
+        {
+            // the reference keeps iterating on NaN until maxIter; the
+            // iterate stays NaN, so stop here and report what it reports
+            st->it[0] = st->maxIter;
+            st->done[0] = 1;
+        }
+        else
+        {
+            const double rzNew = fs[0];
+            st->beta[0] = rzNew / st->rz[0];
+            st->rz[0] = rzNew;
+            if (it >= st->maxIter) st->done[0] = 1;
+        }
+        st->allDone = st->done[0];
+    }
+}
+
+/// p = z + beta p.
+static __global__ void __launch_bounds__(TPB) k_cg_p(int n, const double* __restrict__ diag, const double* __restrict__ r,
+                                              double* __restrict__ p, const SolveState* st)
+{
+    if (st->allDone) return;
+    const double beta = st->beta[0];
+    ROW_LOOP(c, n) p[c] = inv_diag_cg(diag[c]) * r[c] + beta * p[c];
+}
+
+// ------------------------ BiCGStab, 1..3 right-hand sides ------------------
+// The components of the momentum equation share their matrix (the reference
+// asserts equal diagonals, simpleSolver.cpp:123-144, and every off-diagonal
+// term is component-independent), so up to three BiCGStab iterations run in
+// lockstep over one matrix read; each component keeps its own scalars and
+// stops on its own test exactly where the serial loop would.
+
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_bi_init(DMat A, const double* __restrict__ val, V3P b, V3P x, V3P r, V3P r0,
+                                                 V3P p, V3P v, double* partials, SolveState* st)
+{
+    double mx[3 * NC];  // |r|, |b|, nan per comp
+    double sm[NC];      // r.r
+#pragma unroll
+    for (int q = 0; q < 3 * NC; ++q) mx[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < NC; ++q) sm[q] = 0.0;
+    const double* xs[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) xs[q] = x.c[q];
+    ROW_LOOP(c, A.n)
+    {
+        double y[NC];
+        spmv_row<NC>(A, val, c, xs, y);
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            const double bi = b.c[q][c];
+            const double ri = bi - y[q];
+            r.c[q][c] = ri;
+            r0.c[q][c] = ri;
+            p.c[q][c] = 0.0;
+            v.c[q][c] = 0.0;
+            if (isnan(ri) || isnan(bi)) mx[2 * NC + q] = 1.0;
+            mx[q] = smax(mx[q], fabs(ri));
+            mx[NC + q] = smax(mx[NC + q], fabs(bi));
+            sm[q] += ri * ri;
+        }
+    }
+    block_max<3 * NC>(mx);
+    __syncthreads();
+    block_sum<NC>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+#pragma unroll
+        for (int q = 0; q < 3 * NC; ++q) partials[q * G + blockIdx.x] = mx[q];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) partials[(3 * NC + q) * G + blockIdx.x] = sm[q];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double fm[3 * NC], fs[NC];
+    final_max<3 * NC>(partials, G, fm);
+    __syncthreads();
+    final_sum<NC>(partials + 3 * NC * G, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        int all = 1;
+        for (int q = 0; q < NC; ++q)
+        {
+            const double init = fm[2 * NC + q] > 0 ? NAN : fm[q];
+            const double bn = smax(fm[NC + q], 1e-300);
+            st->init[q] = init;
+            st->bnorm[q] = bn;
+            st->it[q] = 0;
+            st->conv[q] = 0;
+            st->done[q] = 0;
+            st->special[q] = 0;
+            st->fin[q] = 0.0;
+            st->rho[q] = 1.0;
+            st->alpha[q] = 1.0;
+            st->omega[q] = 1.0;
+            st->rz[q] = fs[q];  // rhoNew of the first iteration: r0.r = r.r
+            if (init / bn < st->tol)
+            {
+                st->conv[q] = 1;
+                st->done[q] = 1;
+                st->fin[q] = init;
+            }
+            else if (st->maxIter <= 0 || fabs(fs[q]) < 1e-300)
+            {
+                st->done[q] = 1;
+            }
+            all &= st->done[q];
+        }
+        st->allDone = all;
+    }
+}
+
+/// p = r + beta (p - omega v); z = p D^-1   (Matrix.cpp:262-272)
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_bi_p(int n, const double* __restrict__ diag, V3P r, V3P p, V3P v, V3P z,
+                                              const SolveState* st)
+{
+    if (st->allDone) return;
+    double beta[NC], om[NC];
+    int dn[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+    {
+        dn[q] = st->done[q];
+        beta[q] = (st->rz[q] / st->rho[q]) * (st->alpha[q] / st->omega[q]);
+        om[q] = st->omega[q];
+    }
+    ROW_LOOP(c, n)
+    {
+        const double id = inv_diag_bicg(diag[c]);
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            if (dn[q]) continue;
+            const double pi = r.c[q][c] + beta[q] * (p.c[q][c] - om[q] * v.c[q][c]);
+            p.c[q][c] = pi;
+            z.c[q][c] = pi * id;
+        }
+    }
+}
+
+/// v = A z; r0.v; alpha (Matrix.cpp:273-276)
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_bi_spmv1(DMat A, const double* __restrict__ val, V3P z, V3P v, V3P r0,
+                                                  double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double sm[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) sm[q] = 0.0;
+    const double* xs[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) xs[q] = z.c[q];
+    ROW_LOOP(c, A.n)
+    {
+        double y[NC];
+        spmv_row<NC>(A, val, c, xs, y);
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            v.c[q][c] = y[q];
+            sm[q] += r0.c[q][c] * y[q];
+        }
+    }
+    block_sum<NC>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NC; ++q) partials[q * G + blockIdx.x] = sm[q];
+    if (!last_block(&st->ticket[0])) return;
+    double fs[NC];
+    final_sum<NC>(partials, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        int all = 1;
+        for (int q = 0; q < NC; ++q)
+        {
+            if (!st->done[q])
+            {
+                st->rho[q] = st->rz[q];
+                const double denom = fs[q];
+                if (fabs(denom) < 1e-300) st->done[q] = 1;
+                else st->alpha[q] = st->rho[q] / denom;
+            }
+            all &= st->done[q];
+        }
+        st->allDone = all;
+    }
+}
+
+/// x += alpha z; s = r - alpha v; sh = s D^-1; |s|inf (Matrix.cpp:277-289)
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_bi_s(int n, const double* __restrict__ diag, V3P x, V3P z, V3P r, V3P v,
+                                              V3P s, V3P sh, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double al[NC];
+    int dn[NC];
+    double mx[2 * NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+    {
+        dn[q] = st->done[q];
+        al[q] = st->alpha[q];
+        mx[q] = mx[NC + q] = 0.0;
+    }
+    ROW_LOOP(c, n)
+    {
+        const double id = inv_diag_bicg(diag[c]);
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            if (dn[q]) continue;
+            x.c[q][c] = x.c[q][c] + al[q] * z.c[q][c];
+            const double si = r.c[q][c] - al[q] * v.c[q][c];
+            s.c[q][c] = si;
+            sh.c[q][c] = si * id;
+            if (isnan(si)) mx[NC + q] = 1.0;
+            mx[q] = smax(mx[q], fabs(si));
+        }
+    }
+    block_max<2 * NC>(mx);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = mx[q];
+    if (!last_block(&st->ticket[0])) return;
+    double fm[2 * NC];
+    final_max<2 * NC>(partials, G, fm);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        for (int q = 0; q < NC; ++q) st->sMax[q] = fm[NC + q] > 0 ? NAN : fm[q];
+    }
+}
+
+/// t = A sh; t.t and t.s; omega, or the tDenom breakdown exit (Matrix.cpp:290-300)
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restrict__ val, V3P sh, V3P t, V3P s,
+                                                  double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double sm[2 * NC];
+#pragma unroll
+    for (int q = 0; q < 2 * NC; ++q) sm[q] = 0.0;
+    const double* xs[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) xs[q] = sh.c[q];
+    ROW_LOOP(c, A.n)
+    {
+        double y[NC];
+        spmv_row<NC>(A, val, c, xs, y);
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            t.c[q][c] = y[q];
+            sm[q] += y[q] * y[q];
+            sm[NC + q] += y[q] * s.c[q][c];
+        }
+    }
+    block_sum<2 * NC>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = sm[q];
+    if (!last_block(&st->ticket[0])) return;
+    double fs[2 * NC];
+    final_sum<2 * NC>(partials, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        int all = 1;
+        for (int q = 0; q < NC; ++q)
+        {
+            if (!st->done[q])
+            {
+                const double tDenom = fs[q];
+                if (tDenom < 1e-300)
+                {
+                    // r = s; the iteration counts and ends here
+                    st->it[q] = st->it[q] + 1;
+                    st->fin[q] = st->sMax[q];
+                    st->conv[q] = st->fin[q] / st->bnorm[q] < st->tol;
+                    st->done[q] = 1;
+                }
+                else
+                {
+                    st->omega[q] = fs[NC + q] / tDenom;
+                }
+            }
+            all &= st->done[q];
+        }
+        st->allDone = all;
+    }
+}
+
+/// x += omega sh; r = s - omega t; |r|inf test; next r0.r (Matrix.cpp:301-315, :263-264)
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_bi_x(int n, V3P x, V3P sh, V3P s, V3P t, V3P r, V3P r0, double* partials,
+                                              SolveState* st)
+{
+    if (st->allDone) return;
+    double om[NC];
+    int dn[NC];
+    double mx[2 * NC], sm[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+    {
+        dn[q] = st->done[q];
+        om[q] = st->omega[q];
+        mx[q] = mx[NC + q] = 0.0;
+        sm[q] = 0.0;
+    }
+    ROW_LOOP(c, n)
+    {
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            if (dn[q]) continue;
+            x.c[q][c] = x.c[q][c] + om[q] * sh.c[q][c];
+            const double ri = s.c[q][c] - om[q] * t.c[q][c];
+            r.c[q][c] = ri;
+            if (isnan(ri)) mx[NC + q] = 1.0;
+            mx[q] = smax(mx[q], fabs(ri));
+            sm[q] += r0.c[q][c] * ri;
+        }
+    }
+    block_max<2 * NC>(mx);
+    __syncthreads();
+    block_sum<NC>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+#pragma unroll
+        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = mx[q];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) partials[(2 * NC + q) * G + blockIdx.x] = sm[q];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double fm[2 * NC], fs[NC];
+    final_max<2 * NC>(partials, G, fm);
+    __syncthreads();
+    final_sum<NC>(partials + 2 * NC * G, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        int all = 1;
+        for (int q = 0; q < NC; ++q)
+        {
+            if (!st->done[q])
+            {
+                const int it = st->it[q] + 1;
+                st->it[q] = it;
+                const double fin = fm[NC + q] > 0 ? NAN : fm[q];
+                st->fin[q] = fin;
+                if (fin / st->bnorm[q] < st->tol)
+                {
+                    st->conv[q] = 1;
+                    st->done[q] = 1;
+                }
+                else if (isnan(fin))
+                {
+                    st->it[q] = st->maxIter;
+                    st->done[q] = 1;
+                }
+                else
+                {
+                    st->rz[q] = fs[q];
+                    if (it >= st->maxIter || fabs(fs[q]) < 1e-300) st->done[q] = 1;
+                }
+            }
+            all &= st->done[q];
+        }
+        st->allDone = all;
+    }
+}
+
+}  // namespace cfg

@@ -1,0 +1,253 @@
+/*
+ * chuanflow_b200 -- C ABI of the B200 (sm_100a) implementation of ChuanFlow's
+ * 3D unstructured finite-volume SIMPLE path.
+ *
+ * Conventions
+ *   - every entry point returns an int status: CFG_OK (0) or a CFG_E* code;
+ *     cfg_last_error() gives the message of the last failure on the calling
+ *     thread.  No C++ exception crosses this boundary.
+ *   - meshes and contexts are opaque handles; a context owns all device
+ *     memory of one case on one device and one CUDA stream, and is confined
+ *     to the thread that uses it (no global mutable state is shared).
+ *   - indices on this boundary are int64 (the reference's `label`), reals
+ *     are double (its `scalar`); vectors are packed xyz triples.
+ *   - host pointers unless the name says `_dev`.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the ChuanFlow source tree).
+ */
+#ifndef CHUANFLOW_B200_H
+#define CHUANFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFG_OK 0
+#define CFG_EINVAL 1    /* bad argument or inconsistent input */
+#define CFG_ECUDA 2     /* a CUDA call failed */
+#define CFG_EMESH 3     /* invalid mesh (cfFatal in polyMesh / blockMesh) */
+#define CFG_ESETUP 4    /* case set-up error (BC types, dictionary keys) */
+#define CFG_ENOMEM 5
+#define CFG_ENUMERIC 6  /* a check of the algorithm failed (e.g. unequal momentum diagonals) */
+
+typedef struct cfg_mesh cfg_mesh;
+typedef struct cfg_ctx cfg_ctx;
+
+/* boundary-condition kinds, as volScalarField / volVectorField know them
+ * (src/3d/include/cf/fvm/Fields.h:14-22, src/3d/src/fields/volFields.cpp:117-147,246-283) */
+enum cfg_bc_type
+{
+    CFG_BC_FIXED_VALUE = 0,
+    CFG_BC_ZERO_GRADIENT = 1,
+    CFG_BC_FIXED_GRADIENT = 2,
+    CFG_BC_SYMMETRY = 3,
+    CFG_BC_OUTLET = 4,
+    CFG_BC_WALL = 5,
+    CFG_BC_EMPTY = 6
+};
+
+enum cfg_grad_scheme { CFG_GRAD_LINEAR = 0, CFG_GRAD_CORRECTED = 1, CFG_GRAD_LEAST_SQUARES = 2 };
+enum cfg_div_scheme { CFG_DIV_UPWIND = 0, CFG_DIV_LINEAR = 1, CFG_DIV_BLEND = 2 };
+enum cfg_lin_method { CFG_SOLVE_CG = 0, CFG_SOLVE_BICGSTAB = 1 };
+/* pressure preconditioner: the reference's Jacobi PCG, or this library's
+ * multicolour DIC (no reference counterpart) */
+enum cfg_precond { CFG_PRECOND_JACOBI = 0, CFG_PRECOND_DIC = 1 };
+
+/* Schemes (src/3d/include/cf/fvm/FvMatrix.h:30-38) */
+typedef struct cfg_schemes
+{
+    int32_t div;        /* cfg_div_scheme, default upwind */
+    int32_t laplacian_corrected; /* 1 = "corrected" (default), 0 = "none" */
+    int32_t grad;       /* cfg_grad_scheme, default corrected */
+    double blend_coeff; /* default 0.9 */
+} cfg_schemes;
+
+/* SimpleControls (src/3d/include/cf/fvm/SimpleSolver.h:13-64) plus the
+ * GPU-only settings of the case dictionary's optional gpu{} block */
+typedef struct cfg_simple_controls
+{
+    int32_t max_iterations;   /* 200 */
+    double continuity_tol;    /* 1e-6 */
+    double pcorr_tol;         /* 0 */
+    double momentum_tol;      /* 0 */
+    double linear_tol;        /* 1e-7 */
+    int32_t linear_max_iter;  /* 2000 */
+    int32_t non_orth_correctors; /* 2 */
+    double relax_u;           /* 0.7 */
+    double relax_p;           /* 0.3 */
+    double p_relax_start;     /* 0 */
+    double body_force[3];     /* 0 */
+    double nu;                /* kinematic viscosity */
+    /* gpu{} -- defaults reproduce the reference */
+    int32_t p_precond;        /* cfg_precond, default JACOBI */
+    int32_t verbose;          /* 1: print the reference's per-iteration log line */
+    /* pressure reference cell, -1 = none (the reference has none: a case with
+     * no fixed-value pressure patch leaves the singular Neumann system to CG).
+     * A pinned cell follows OpenFOAM's fvMatrix::setReference: its source
+     * gains diag * p_ref_value and its diagonal doubles. */
+    int64_t p_ref_cell;
+    double p_ref_value;
+} cfg_simple_controls;
+
+/* SimpleResult (SimpleSolver.h:66-72) plus inner-solver statistics */
+typedef struct cfg_simple_result
+{
+    int32_t iterations;
+    int32_t converged;
+    double final_continuity_error;
+    double final_momentum_residual;
+    double last_dp;            /* pDeltaMax of the last iteration */
+    double last_continuity_corrected;
+    int64_t u_inner_iterations; /* summed over components, passes and outer iterations */
+    int64_t p_inner_iterations;
+    int32_t diverged;
+} cfg_simple_result;
+
+/* SolverReport (src/common/include/cf/common/Matrix.h:58-64) */
+typedef struct cfg_solver_report
+{
+    int32_t iterations;
+    int32_t converged;
+    double initial_residual;
+    double final_residual;
+} cfg_solver_report;
+
+/* ---- errors ------------------------------------------------------------ */
+
+/* Copies the last error message of this thread into buf; returns its length. */
+size_t cfg_last_error(char* buf, size_t size);
+const char* cfg_version(void);
+
+/* ---- mesh ---------------------------------------------------------------- */
+
+/* polyMesh(points, faces, owner, neighbour, patches)
+ * (src/3d/include/cf/fvm/PolyMesh.h:30-34, src/3d/src/mesh/polyMesh.cpp:12-64).
+ * Faces are given as a CSR of vertex lists.  Patch i covers faces
+ * [patch_start[i], patch_start[i]+patch_size[i]).  Geometry is computed on the
+ * host in the reference's operation order (polyMesh.cpp:83-288). */
+int cfg_mesh_create(const double* points, int64_t n_points, const int64_t* face_offsets,
+                    const int64_t* face_verts, int64_t n_faces, const int64_t* owner,
+                    const int64_t* neighbour, int64_t n_internal, int32_t n_patches,
+                    const char* const* patch_names, const char* const* patch_types,
+                    const int64_t* patch_start, const int64_t* patch_size, cfg_mesh** out);
+
+/* BlockMesh::create (src/3d/include/cf/fvm/BlockMesh.h:44-46,
+ * src/3d/src/mesh/blockMesh.cpp:36-189).  side_names/side_types are in the
+ * order xmin xmax ymin ymax zmin zmax; NULL gives the reference's defaults. */
+int cfg_mesh_block(const double min[3], const double max[3], int64_t nx, int64_t ny, int64_t nz,
+                   const char* const* side_names, const char* const* side_types, cfg_mesh** out);
+
+/* polyMesh::movePoints (polyMesh.cpp:320-329): same topology, new points,
+ * geometry recomputed. */
+int cfg_mesh_move_points(cfg_mesh* mesh, const double* points, int64_t n_points);
+
+/* Synthetic-mesh helper with no reference counterpart: displaces every
+ * interior point of a blockMesh box by an independent uniform offset in
+ * [-fraction*h, fraction*h) per axis (h the local cell size along that
+ * axis), from a counter-based hash of (seed, point, axis). */
+int cfg_mesh_jitter_interior(cfg_mesh* mesh, double fraction, uint64_t seed);
+
+void cfg_mesh_destroy(cfg_mesh* mesh);
+
+/* counts[5] = nPoints nCells nFaces nInternalFaces nPatches */
+int cfg_mesh_counts(const cfg_mesh* mesh, int64_t counts[5]);
+/* patch names/types (buffers of `size` bytes) and ranges */
+int cfg_mesh_patch(const cfg_mesh* mesh, int32_t patch, char* name, size_t name_size, char* type,
+                   size_t type_size, int64_t* start, int64_t* size);
+int cfg_mesh_patch_id(const cfg_mesh* mesh, const char* name);
+/* addressing copies: points nP*3, face_offsets nF+1, face_verts, owner nF, neighbour nInt */
+int cfg_mesh_addressing(const cfg_mesh* mesh, double* points, int64_t* face_offsets,
+                        int64_t* face_verts, int64_t* owner, int64_t* neighbour);
+/* polyMesh geometry accessors (PolyMesh.h:51-65); any pointer may be NULL */
+int cfg_mesh_geometry(const cfg_mesh* mesh, double* cell_volumes, double* cell_centres,
+                      double* face_centres, double* face_sf, double* face_areas, double* delta_vec,
+                      double* delta_coeff);
+/* makeInternalOwnerWeights / makeFaceSkewVectors (src/3d/src/discrete/interpolate.cpp:28-48) */
+int cfg_mesh_weights(const cfg_mesh* mesh, double* owner_weights, double* skew);
+/* The cell order the device arrays are laid out in (new -> original); the
+ * identity unless the mesh was renumbered (no reference counterpart). */
+int cfg_mesh_device_order(const cfg_mesh* mesh, int64_t* new_to_old);
+
+/* ---- case context on one device ------------------------------------------ */
+
+/* Uploads the mesh to `device` and allocates the case state there. `stream`
+ * is a cudaStream_t (NULL = a stream created and owned by the context). */
+int cfg_ctx_create(const cfg_mesh* mesh, int32_t device, void* stream, cfg_ctx** out);
+void cfg_ctx_destroy(cfg_ctx* ctx);
+
+/* volVectorField::setPatchValue / volScalarField::setPatchValue
+ * (Fields.h:42, :90; volFields.cpp:57-62, :175-180).  field 'U' or 'p'. */
+int cfg_set_patch_bc(cfg_ctx* ctx, char field, int32_t patch, int32_t bc_type, const double* value);
+/* volVectorField::setFaceValue (Fields.h:97, volFields.cpp:187-201): a
+ * per-face prescribed velocity for a boundary face; n faces at once. */
+int cfg_set_face_values_U(cfg_ctx* ctx, int64_t n, const int64_t* faces, const double* values);
+int cfg_clear_face_values_U(cfg_ctx* ctx);
+int cfg_set_schemes(cfg_ctx* ctx, const cfg_schemes* schemes);
+
+/* Field transfers.  U: nCells*3, p: nCells, phi: nFaces, all in the mesh's
+ * original cell and face order; NULL skips a field. */
+int cfg_fields_upload(cfg_ctx* ctx, const double* U, const double* p, const double* phi);
+int cfg_fields_download(cfg_ctx* ctx, double* U, double* p, double* phi);
+
+/* The initial flux of src/3d/apps/simpleFoamApp.cpp:94-95 and
+ * src/3d/apps/caseInit.h:18-31: boundary phi from U's conditions
+ * (surfaceScalarField::correctBoundaryFlux), and when `u0` is non-NULL every
+ * cell set to u0 and the internal flux interpolated from it. */
+int cfg_fields_init_flux(cfg_ctx* ctx, const double* u0);
+
+/* solveIncompressibleSimple (src/3d/include/cf/fvm/SimpleSolver.h:119-127,
+ * src/3d/src/solvers/simpleSolver.cpp:33-394), laminar and steady.  Runs up
+ * to controls->max_iterations outer iterations on the device fields. */
+int cfg_simple_iterate(cfg_ctx* ctx, const cfg_simple_controls* controls, cfg_simple_result* result);
+
+/* Wall time (ms) of the device work of the last cfg_simple_iterate call,
+ * measured with CUDA events on the context's stream, and the launch count.
+ * kernel_ms[0..7] split it by family: gradient, assembly, momentum solve,
+ * pressure solve, flux/update, continuity, other, total. */
+int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
+
+/* ---- the linear-solver call surface ------------------------------------ */
+
+/* solveCG / solveBiCGStab on a CSR matrix (src/common/include/cf/common/Matrix.h:67-73,
+ * src/common/src/Matrix.cpp:153-319): host CSR (rows sorted by column, the
+ * diagonal present), b and x (x: initial guess in, solution out).  The
+ * matrix and vectors are copied to the device and back inside the call. */
+int cfg_sparse_solve(const cfg_ctx* ctx_or_null, int32_t device, int64_t n, const int64_t* row_start,
+                     const int64_t* cols, const double* vals, const double* b, double* x, double tol,
+                     int32_t max_iter, int32_t method, cfg_solver_report* report);
+
+/* ---- diagnostics used by the parity tests (no reference counterpart) ----- */
+
+/* The equations of one outer iteration built from the context's current
+ * fields: out receives gradPn (3N), the momentum diagonal (3N), the
+ * momentum explicit operator h = rhs - (A x - diag x) at x = 0 (3N) and at
+ * x = xprobe (3N), rAUf (F), div(phi) (N), the predictor continuity error
+ * (1), the pressure diagonal (N), its h at 0 and at xprobe (2N), the
+ * gradient of xprobe under p's conditions (3N), and phi corrected with
+ * xprobe as the solved pressure (F).  Vector blocks are component-major. */
+int cfg_probe_equations(cfg_ctx* ctx, const cfg_simple_controls* controls, const double* xprobe, double* out);
+
+/* fvc::grad of a cell field with fixed boundary face values bvals[f - nInternal]
+ * (gradScheme.cpp:246-277); vol_quirk 1 selects the volScalarField overload's
+ * internal face value for the linear scheme.  out: nCells*3. */
+int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t scheme, int32_t vol_quirk,
+                 double* out);
+
+/* ---- case dictionary (the reference's case.dict grammar) ----------------- */
+
+/* Runs a chflow-simple-foam case file end to end (src/3d/apps/simpleFoamApp.cpp:33-209
+ * without turbulence/energy/output): mesh from block{}, patches{}, schemes{},
+ * simple{} (with linearTol/linearMaxIter as in
+ * src/coupling/apps/multiCoupledApp.cpp:41-57) and an optional gpu{} block.
+ * Fields are returned through U/p/phi if non-NULL (sizes from counts). */
+int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* result, int64_t counts[5],
+                      double* U, double* p, double* phi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHUANFLOW_B200_H */

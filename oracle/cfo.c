@@ -1373,6 +1373,12 @@ static void build_peqn(fvmat* P, const simple_ws* w, const cfo_controls* ctl, co
     memcpy(P->bc_k, pk, sizeof(double) * (size_t)nB);
     fvm_laplacian(P, &w->g, rAUf, ctl->laplacianCorrected, -1);
     for (int64_t c = 0; c < m->nC; ++c) P->rhs[c] += -dphi[c];
+    if (ctl->pRefCell >= 0 && ctl->pRefCell < m->nC)
+    {
+        const int64_t r = ctl->pRefCell;
+        P->rhs[r] += P->diag[r] * ctl->pRefValue;
+        P->diag[r] += P->diag[r];
+    }
 }
 
 static void interp_to_faces(const simple_ws* w, const double* cell, double* face)

@@ -90,6 +90,11 @@ typedef struct cfo_controls
     int32_t div, laplacianCorrected, grad;
     double blendCoeff;
     int32_t verbose;
+    /* pressure reference cell (-1: none, the reference's behaviour); a pinned
+     * cell follows OpenFOAM's fvMatrix::setReference: source += diag * value,
+     * then diag += diag.  No counterpart in the reference. */
+    int64_t pRefCell;
+    double pRefValue;
 } cfo_controls;
 
 typedef struct cfo_result

@@ -1,0 +1,232 @@
+"""Case definitions shared by the tests, the fixture generator and bench.py's
+parity leg: the synthetic meshes, their boundary conditions and controls, and
+the analytic fields of the reference's gradient test."""
+from __future__ import annotations
+
+import numpy as np
+
+import _oracle as O
+
+# the linear and quadratic fields of the reference's gradient test
+# (tests/unit/gradientTests.cpp: linear anchor T = 1 + 2x - y + 0.5z and the
+# quadratic of tests/cases/parallelDecomposition/caseTet.dict)
+POLY_FIELDS = {
+    "lin": [1, 2, -1, 0.5, 0, 0, 0, 0, 0, 0],
+    "quad": [1, 2, -1, 0.5, 3, -0.25, 0, 1.5, -2, 0.75],
+}
+
+
+def poly(c, p):
+    p = np.asarray(p, np.float64)
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    return (c[0] + c[1] * x + c[2] * y + c[3] * z + c[4] * x * x + c[5] * y * y + c[6] * z * z
+            + c[7] * x * y + c[8] * y * z + c[9] * z * x)
+
+
+def poly_grad(c, p):
+    p = np.asarray(p, np.float64)
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    return np.stack([c[1] + 2.0 * c[4] * x + c[7] * y + c[9] * z,
+                     c[2] + 2.0 * c[5] * y + c[7] * x + c[8] * z,
+                     c[3] + 2.0 * c[6] * z + c[8] * y + c[9] * x], -1)
+
+
+_M64 = (1 << 64) - 1
+
+
+def _splitmix(x):
+    x = (x + 0x9E3779B97F4A7C15) & _M64
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def jitter_points(points, cells, mn, mx, fraction, seed):
+    """The interior-point jitter of cfg_mesh_jitter_interior, restated: every
+    interior point of the block moves by (2u - 1) fraction h per axis, u from
+    splitmix64(seed * 0x100000001B3 ^ (3 * point + axis)) >> 11 over 2^53."""
+    nx, ny, nz = cells
+    pts = np.array(points, np.float64, copy=True).reshape(-1, 3)
+    h = [(mx[a] - mn[a]) / float(cells[a]) for a in range(3)]
+    s0 = (seed * 0x100000001B3) & _M64
+    for k in range(1, nz):
+        for j in range(1, ny):
+            for i in range(1, nx):
+                pid = i + (nx + 1) * (j + (ny + 1) * k)
+                for a in range(3):
+                    r = _splitmix(s0 ^ ((pid * 3 + a) & _M64))
+                    u = float(r >> 11) * (1.0 / 9007199254740992.0)
+                    pts[pid, a] += (u * 2.0 - 1.0) * fraction * h[a]
+    return pts
+
+
+SIDES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
+
+
+def _block(mn, mx, cells, names, types, jitter, seed):
+    m = O.block_mesh(mn, mx, cells, names, types)
+    if jitter:
+        m = m.with_points(jitter_points(m.points, cells, mn, mx, jitter, seed))
+    return m
+
+
+# ---- the lid-driven cavity (the 128^3 benchmark's family) -----------------
+
+CAVITY_NAMES = ["left", "right", "bottom", "lid", "front", "back"]
+
+
+def cavity_case(nx, ny, nz, jitter=0.1, seed=7, nu=0.01, iters=3, linear_tol=1e-10, non_orth=1):
+    m = _block((0, 0, 0), (1, 1, 1), (nx, ny, nz), CAVITY_NAMES, ["wall"] * 6, jitter, seed)
+    u_val = [(1.0, 0, 0) if n == "lid" else (0, 0, 0) for n in m.patch_names]
+    return O.Case(m, u_type=["fixedValue"] * 6, u_value=u_val, p_type=["zeroGradient"] * 6, p_value=[0] * 6,
+                  nu=nu, max_iterations=iters, linear_tol=linear_tol, non_orth=non_orth, relax_u=0.7,
+                  relax_p=0.3)
+
+
+def cavity_dict(nx, ny, nz, nu=0.01, iters=3, linear_tol=1e-10, non_orth=1, max_iter=2000):
+    sides = "\n".join(f"    {s} {{ name {n}; type wall; }}" for s, n in zip(SIDES, CAVITY_NAMES))
+    pats = "\n".join(f"    {n} {{ U ({'1' if n == 'lid' else '0'} 0 0); }}" for n in CAVITY_NAMES)
+    return f"""block
+{{
+    min (0 0 0);
+    max (1 1 1);
+    cells ({nx} {ny} {nz});
+{sides}
+}}
+nu {nu!r};
+patches
+{{
+{pats}
+}}
+schemes {{ ddt steady; div upwind; laplacian corrected; grad corrected; }}
+simple
+{{
+    maxIterations {iters};
+    relaxU 0.7;
+    relaxP 0.3;
+    nonOrthCorrectors {non_orth};
+    linearTol {linear_tol!r};
+    linearMaxIter {max_iter};
+}}
+"""
+
+
+def cavity_product(nx, ny, nz, jitter=0.1, seed=7, device=0, schemes=None):
+    """The same cavity through chuanflow_b200 (mesh, BCs, initial flux)."""
+    import chuanflow_b200 as cf
+    mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (nx, ny, nz),
+                             {s: (n, "wall") for s, n in zip(SIDES, CAVITY_NAMES)})
+    if jitter:
+        mesh.jitter_interior(jitter, seed)
+    case = cf.SimpleCase(mesh, device, schemes)
+    for n in CAVITY_NAMES:
+        case.set_patch_bc("U", n, "fixedValue", (1.0, 0, 0) if n == "lid" else (0, 0, 0))
+        case.set_patch_bc("p", n, "zeroGradient", 0.0)
+    case.init_flux()
+    return mesh, case
+
+
+# ---- the inlet/outlet channel (the 16,000-cell benchmark's family) --------
+
+CHANNEL_NAMES = ["inlet", "outlet", "bottom", "top", "front", "back"]
+CHANNEL_TYPES = ["inlet", "outlet", "wall", "wall", "wall", "wall"]
+
+
+def channel_case(nx, ny, nz, jitter=0.1, seed=5, nu=1e-3, iters=4, linear_tol=1e-10, non_orth=2,
+                 L=(1.0, 0.2, 0.2)):
+    m = _block((0, 0, 0), L, (nx, ny, nz), CHANNEL_NAMES, CHANNEL_TYPES, jitter, seed)
+    ut = ["fixedValue", "zeroGradient", "fixedValue", "fixedValue", "fixedValue", "fixedValue"]
+    uv = [(0.1, 0, 0)] + [(0, 0, 0)] * 5
+    pt = ["zeroGradient", "fixedValue"] + ["zeroGradient"] * 4
+    return O.Case(m, u_type=ut, u_value=uv, p_type=pt, p_value=[0] * 6, nu=nu, max_iterations=iters,
+                  linear_tol=linear_tol, non_orth=non_orth, relax_u=0.9, relax_p=0.03, p_relax_start=0.02)
+
+
+def channel_dict(nx, ny, nz, nu=1e-3, iters=4, linear_tol=1e-10, non_orth=2, L=(1.0, 0.2, 0.2)):
+    sides = "\n".join(f"    {s} {{ name {n}; type {t}; }}" for s, n, t in zip(SIDES, CHANNEL_NAMES, CHANNEL_TYPES))
+    return f"""block
+{{
+    min (0 0 0);
+    max ({L[0]!r} {L[1]!r} {L[2]!r});
+    cells ({nx} {ny} {nz});
+{sides}
+}}
+nu {nu!r};
+patches
+{{
+    inlet  {{ U (0.1 0 0); UType fixedValue;  pType zeroGradient; }}
+    outlet {{ UType zeroGradient; p 0;        pType fixedValue;   }}
+    bottom {{ U (0 0 0); }}
+    top    {{ U (0 0 0); }}
+    front  {{ U (0 0 0); }}
+    back   {{ U (0 0 0); }}
+}}
+schemes {{ ddt steady; div upwind; laplacian corrected; grad corrected; }}
+simple
+{{
+    maxIterations {iters};
+    relaxU 0.9;
+    relaxP 0.03;
+    pRelaxStart 0.02;
+    nonOrthCorrectors {non_orth};
+    linearTol {linear_tol!r};
+}}
+"""
+
+
+def channel_product(nx, ny, nz, jitter=0.1, seed=5, device=0, L=(1.0, 0.2, 0.2), schemes=None):
+    import chuanflow_b200 as cf
+    mesh = cf.PolyMesh.block((0, 0, 0), L, (nx, ny, nz),
+                             {s: (n, t) for s, n, t in zip(SIDES, CHANNEL_NAMES, CHANNEL_TYPES)})
+    if jitter:
+        mesh.jitter_interior(jitter, seed)
+    case = cf.SimpleCase(mesh, device, schemes)
+    case.set_patch_bc("U", "inlet", "fixedValue", (0.1, 0, 0))
+    case.set_patch_bc("p", "inlet", "zeroGradient", 0.0)
+    case.set_patch_bc("U", "outlet", "zeroGradient", (0, 0, 0))
+    case.set_patch_bc("p", "outlet", "fixedValue", 0.0)
+    for n in ("bottom", "top", "front", "back"):
+        case.set_patch_bc("U", n, "fixedValue", (0, 0, 0))
+        case.set_patch_bc("p", n, "zeroGradient", 0.0)
+    case.init_flux()
+    return mesh, case
+
+
+def controls_from(case: O.Case, **over):
+    """The product's SimpleControls for an oracle Case."""
+    import chuanflow_b200 as cf
+    c = cf.SimpleControls(max_iterations=case.max_iterations, continuity_tol=case.continuity_tol,
+                          pcorr_tol=case.pcorr_tol, momentum_tol=case.momentum_tol, linear_tol=case.linear_tol,
+                          linear_max_iter=case.linear_max_iter, non_orth_correctors=case.non_orth,
+                          relax_u=case.relax_u, relax_p=case.relax_p, p_relax_start=case.p_relax_start,
+                          body_force=tuple(case.body_force), nu=case.nu)
+    c.p_ref_cell = case.p_ref_cell
+    c.p_ref_value = case.p_ref_value
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+def test_matrix(n, rng, symmetric):
+    """A random diagonally dominant sparse matrix, CSR with sorted columns."""
+    rows = {i: {} for i in range(n)}
+    for i in range(n):
+        for j in rng.choice(n, size=4, replace=False):
+            if j == i:
+                continue
+            v = -rng.uniform(0.1, 1.0)
+            rows[i][j] = rows[i].get(j, 0) + v
+            if symmetric:
+                rows[j][i] = rows[j].get(i, 0) + v
+            else:
+                rows[j][i] = rows[j].get(i, 0) + v * rng.uniform(0.2, 1.8)
+    rs, cols, vals = [0], [], []
+    for i in range(n):
+        off = sum(abs(v) for v in rows[i].values())
+        rows[i][i] = off + rng.uniform(0.05, 0.5)
+        for j in sorted(rows[i]):
+            cols.append(j)
+            vals.append(rows[i][j])
+        rs.append(len(cols))
+    return np.array(rs, np.int64), np.array(cols, np.int64), np.array(vals, np.float64)

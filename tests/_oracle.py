@@ -51,7 +51,8 @@ class Controls(C.Structure):
                 ("nonOrthCorrectors", C.c_int32), ("relaxU", C.c_double), ("relaxP", C.c_double),
                 ("pRelaxStart", C.c_double), ("bodyForce", C.c_double * 3), ("nu", C.c_double),
                 ("div", C.c_int32), ("laplacianCorrected", C.c_int32), ("grad", C.c_int32),
-                ("blendCoeff", C.c_double), ("verbose", C.c_int32)]
+                ("blendCoeff", C.c_double), ("verbose", C.c_int32), ("pRefCell", C.c_int64),
+                ("pRefValue", C.c_double)]
 
 
 class Result(C.Structure):
@@ -201,6 +202,8 @@ class Case:
     p_relax_start: float = 0.0
     body_force: tuple = (0.0, 0.0, 0.0)
     u_face_values: dict = None
+    p_ref_cell: int = -1
+    p_ref_value: float = 0.0
 
     def controls(self, verbose=False):
         c = Controls()
@@ -222,6 +225,8 @@ class Case:
         c.grad = GRAD.get(self.grad, 0)
         c.blendCoeff = self.blend
         c.verbose = int(verbose)
+        c.pRefCell = self.p_ref_cell
+        c.pRefValue = self.p_ref_value
         return c
 
     def bcs(self):

@@ -1,0 +1,170 @@
+"""Generates the golden fixtures in this directory by running the reference
+itself: oracle/_ref/cf_ref_driver, which oracle/Makefile compiles from the
+reference's own sources.  Run here, where the reference tree is present:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Fixtures (small .npz files):
+  mesh_block_2x2x2.npz     BlockMesh 2x2x2 unit cube: addressing + geometry
+  mesh_tets22.npz          the reference's skewed tet cube (tests/meshes/cubeTets_22.msh)
+                           through its gmsh reader: addressing, geometry, weights,
+                           and fvc::grad of its two test fields under all schemes
+  mesh_hex41.npz           the orthogonal hex cube (tests/meshes/cubeHex_41.msh), same
+  simple_cavity.npz        jittered 6x5x4 lid-driven cavity: 3 SIMPLE iterations
+  simple_channel.npz       10x6x5 inlet/outlet channel: 4 SIMPLE iterations
+  eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
+  solve_cg.npz, solve_bicgstab.npz   one CSR solve each
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+import _oracle as O  # noqa: E402
+import _cases as K  # noqa: E402
+
+REF_MESHES = "/root/reference/tests/meshes"
+
+
+def mesh_npz(name, case_text, points=None, grad_fields=False):
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(case_text)
+        r = O.ref_mesh(cp, points)
+        out = {k: v for k, v in r.items() if k not in ("counts", "patches")}
+        out["counts"] = np.array(r["counts"], np.int64)
+        out["patch_names"] = np.array([p[0] for p in r["patches"]])
+        out["patch_types"] = np.array([p[1] for p in r["patches"]])
+        out["patch_start"] = np.array([int(p[2]) for p in r["patches"]], np.int64)
+        out["patch_size"] = np.array([int(p[3]) for p in r["patches"]], np.int64)
+        if grad_fields:
+            C, Cf = r["C"], r["Cf"]
+            nInt = r["neighbour"].size
+            for fname, coef in K.POLY_FIELDS.items():
+                t = K.poly(coef, C)
+                b = K.poly(coef, Cf[nInt:])
+                tp = os.path.join(td, "t.f64")
+                bp = os.path.join(td, "b.f64")
+                t.tofile(tp)
+                b.tofile(bp)
+                O.ref_run(["grad", cp, td, "-", tp, bp])
+                out[f"T_{fname}"] = t
+                out[f"B_{fname}"] = b
+                for s in ("linear", "corrected", "leastSquares"):
+                    out[f"grad_fn_{s}_{fname}"] = O.read(os.path.join(td, f"grad_fn_{s}.f64"), shape=(-1, 3))
+                    out[f"grad_vol_{s}_{fname}"] = O.read(os.path.join(td, f"grad_vol_{s}.f64"), shape=(-1, 3))
+        np.savez_compressed(os.path.join(HERE, name), **out)
+        print("wrote", name)
+
+
+def simple_npz(name, case, iters_dict_text, points, state=None):
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(iters_dict_text)
+        pp = os.path.join(td, "points.f64")
+        np.ascontiguousarray(points).tofile(pp)
+        args = ["simple", cp, td, pp]
+        if state is not None:
+            sd = os.path.join(td, "state")
+            os.makedirs(sd)
+            for k, v in state.items():
+                np.ascontiguousarray(v).tofile(os.path.join(sd, k + ".f64"))
+            args.append(sd)
+        O.ref_run(args)
+        res = open(os.path.join(td, "result.txt")).read().split()
+        out = {"points": points, "U": O.read(os.path.join(td, "U.f64"), shape=(-1, 3)),
+               "p": O.read(os.path.join(td, "p.f64")), "phi": O.read(os.path.join(td, "phi.f64")),
+               "iterations": int(res[0]), "continuity": float(res[1]), "momentum": float(res[2]),
+               "converged": int(res[3]), "dict": np.array(iters_dict_text)}
+        if state is not None:
+            for k, v in state.items():
+                out["init_" + k] = v
+        np.savez_compressed(os.path.join(HERE, name), **out)
+        print("wrote", name, res[:4])
+
+
+def eqns_npz(name, dict_text, points, state):
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(dict_text)
+        pp = os.path.join(td, "points.f64")
+        np.ascontiguousarray(points).tofile(pp)
+        sd = os.path.join(td, "state")
+        os.makedirs(sd)
+        for k, v in state.items():
+            np.ascontiguousarray(v).tofile(os.path.join(sd, k + ".f64"))
+        O.ref_run(["eqns", cp, td, pp, sd])
+        out = {"points": points, "dict": np.array(dict_text)}
+        out.update({"in_" + k: v for k, v in state.items()})
+        for k in ("gradPn", "gradPFull"):
+            out[k] = O.read(os.path.join(td, k + ".f64"), shape=(-1, 3))
+        for q in range(3):
+            out[f"U_diag{q}"] = O.read(os.path.join(td, f"U_diag{q}.f64"))
+            out[f"U_h0_{q}"] = O.read(os.path.join(td, f"U_h0_{q}.f64"))
+            out[f"U_h1_{q}"] = O.read(os.path.join(td, f"U_h1_{q}.f64"))
+        for k in ("rAUf", "divPhi", "contErr", "p_diag", "p_h0", "p_h1", "phiCorrected"):
+            out[k] = O.read(os.path.join(td, k + ".f64"))
+        np.savez_compressed(os.path.join(HERE, name), **out)
+        print("wrote", name)
+
+
+def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
+    n = rs.size - 1
+    rows = np.repeat(np.arange(n), np.diff(rs))
+    off = rows != cols
+    diag = np.zeros(n)
+    diag[rows[~off]] = vals[~off]
+    with tempfile.TemporaryDirectory() as td:
+        trip = np.stack([rows[off], cols[off]], 1).astype(np.int64)
+        trip.tofile(os.path.join(td, "t.i64"))
+        vals[off].astype(np.float64).tofile(os.path.join(td, "v.f64"))
+        diag.tofile(os.path.join(td, "d.f64"))
+        b.tofile(os.path.join(td, "b.f64"))
+        x0.tofile(os.path.join(td, "x0.f64"))
+        O.ref_run(["solve", td, n, os.path.join(td, "t.i64"), os.path.join(td, "v.f64"), os.path.join(td, "d.f64"),
+                   os.path.join(td, "b.f64"), os.path.join(td, "x0.f64"), method, repr(tol), max_iter])
+        rep = open(os.path.join(td, "report.txt")).read().split()
+        np.savez_compressed(os.path.join(HERE, name), row_start=rs, cols=cols, vals=vals, b=b, x0=x0,
+                            x=O.read(os.path.join(td, "x.f64")), tol=tol, max_iter=max_iter,
+                            iterations=int(rep[0]), initial=float(rep[1]), final=float(rep[2]),
+                            converged=int(rep[3]))
+        print("wrote", name, rep[:4])
+
+
+def main():
+    if not O.have_ref():
+        sys.exit("oracle/_ref/cf_ref_driver missing: run `make -C oracle` where the reference is present")
+    mesh_npz("mesh_block_2x2x2.npz", "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\n")
+    mesh_npz("mesh_tets22.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeTets_22.msh"; }}\n', grad_fields=True)
+    mesh_npz("mesh_hex41.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeHex_41.msh"; }}\n', grad_fields=True)
+
+    cav = K.cavity_case(6, 5, 4)
+    simple_npz("simple_cavity.npz", cav, K.cavity_dict(6, 5, 4, iters=3), cav.mesh.points)
+    ch = K.channel_case(10, 6, 5)
+    simple_npz("simple_channel.npz", ch, K.channel_dict(10, 6, 5, iters=4), ch.mesh.points)
+
+    rng = np.random.default_rng(11)
+    m = cav.mesh
+    U = rng.normal(size=(m.nC, 3)) * 0.3
+    p = rng.normal(size=m.nC)
+    phi = cav.initial_flux(U) + rng.normal(size=m.nF) * 1e-3 * (np.arange(m.nF) < m.nInt)
+    xprobe = rng.normal(size=m.nC)
+    eqns_npz("eqns_cavity.npz", K.cavity_dict(6, 5, 4, iters=1), m.points, {"U": U, "p": p, "phi": phi,
+                                                                           "xprobe": xprobe})
+
+    # one pressure-like SPD system and one convection-diffusion system
+    n = 60
+    rs, cols, vals = K.test_matrix(n, rng, symmetric=True)
+    b = rng.normal(size=n)
+    solve_npz("solve_cg.npz", "cg", rs, cols, vals, b, np.zeros(n), 1e-10, 500)
+    rs, cols, vals = K.test_matrix(n, rng, symmetric=False)
+    solve_npz("solve_bicgstab.npz", "bicgstab", rs, cols, vals, b, np.zeros(n), 1e-10, 500)
+
+
+if __name__ == "__main__":
+    main()
