@@ -352,6 +352,15 @@ class SimpleCase:
         _check(lib().cfg_last_timing(self._h, _dp(ms), C.byref(n)))
         return ms, n.value
 
+    def kernel_timing(self, enable=True):
+        _check(lib().cfg_kernel_timing(self._h, C.c_int32(int(enable))))
+
+    def kernel_stats(self):
+        out = np.zeros(6)
+        _check(lib().cfg_kernel_stats(self._h, _dp(out)))
+        names = ("cg_spmv", "cg_update", "cg_p")
+        return {n: (int(out[2 * i]), float(out[2 * i + 1])) for i, n in enumerate(names)}
+
     # ---- diagnostics ----
     def probe_equations(self, controls: SimpleControls, xprobe):
         N, F = self.mesh.n_cells, self.mesh.n_faces

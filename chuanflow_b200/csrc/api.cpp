@@ -364,6 +364,26 @@ int cfg_last_timing(const cfg_ctx* ctx, double ms[8], int64_t* launches)
     });
 }
 
+int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable)
+{
+    return guard([&] {
+        need(ctx != nullptr, "null context");
+        ctx->c->setKernelTiming(enable != 0);
+    });
+}
+
+int cfg_kernel_stats(const cfg_ctx* ctx, double out[6])
+{
+    return guard([&] {
+        need(ctx && out, "cfg_kernel_stats: null argument");
+        for (int k = 0; k < 3; ++k)
+        {
+            out[2 * k] = ctx->c->kstat[k][0];
+            out[2 * k + 1] = ctx->c->kstat[k][1];
+        }
+    });
+}
+
 int cfg_sparse_solve(const cfg_ctx* ctx, int32_t device, int64_t n, const int64_t* rs, const int64_t* cols,
                      const double* vals, const double* b, double* x, double tol, int32_t maxIter, int32_t method,
                      cfg_solver_report* rep)

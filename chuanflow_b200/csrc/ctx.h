@@ -65,6 +65,11 @@ public:
     double lastMs[8] = {0};
     int64_t lastLaunches = 0;
 
+    /// Per-kernel CUDA-event timing of the pressure-PCG kernels (opt-in):
+    /// kstat[k] = {launches, total ms} for k = spmv, update, p-update.
+    void setKernelTiming(bool on);
+    double kstat[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+
     const Mesh& mesh() const { return mesh_; }
 
 private:
@@ -92,6 +97,8 @@ private:
     bool ownStream_ = false;
     int G_ = 0;        // grid of row kernels
     int GF_ = 0;       // grid of face kernels
+    int GS_ = 0;       // grid of solver kernels (RPT rows per thread)
+    int maxW_ = 0;     // longest matrix row
     int nSlices_ = 0;
     std::vector<void*> allocs_;
     DMesh dm_{};
@@ -128,6 +135,8 @@ private:
     double* scalHost_;  // pinned copy
     Timing tm_{};
     int64_t launches_ = 0;
+    bool ktime_ = false;
+    std::vector<cudaEvent_t> kev_;  // 6 events per CG iteration of a chunk
 };
 
 }  // namespace cfg

@@ -324,23 +324,63 @@ __global__ void __launch_bounds__(TPB) k_grad_ls2(DMesh m, CV3P x, BcTab bc, CGr
 // ---------------------------------------------------------------------------
 
 /// One row of y = A x for NC vectors sharing A; entries in the reference
-/// CSR's column order (SparseMatrix::product, Matrix.cpp:119-133).
-template <int NC>
+/// CSR's column order (SparseMatrix::product, Matrix.cpp:119-133).  W is a
+/// compile-time bound on the row length: all column indices and values of
+/// the row are loaded first and then all gathers issued, so a thread keeps W
+/// independent loads in flight instead of walking a dependent chain.  W = 0
+/// walks rows of any length.  Entries are added in order, skipping only the
+/// trailing pads, so the sum is the reference's.
+template <int W, int NC>
 __device__ __forceinline__ void spmv_row(const DMat& A, const double* __restrict__ val, int c,
                                          const double* const (&x)[NC], double (&y)[NC])
 {
 #pragma unroll
     for (int q = 0; q < NC; ++q) y[q] = 0.0;
     const int sl = c >> 5, lane = c & 31;
-    const int e1 = A.start[sl + 1];
-    for (int e = A.start[sl] + lane; e < e1; e += 32)
+    const int e0 = __ldg(A.start + sl) + lane, e1 = __ldg(A.start + sl + 1);
+    if constexpr (W > 0)
     {
-        const int col = A.col[e];
-        if (col < 0) break;
-        const double v = val[e];
+        int col[W];
+        double v[W];
 #pragma unroll
-        for (int q = 0; q < NC; ++q) y[q] += v * x[q][col];
+        for (int k = 0; k < W; ++k)
+        {
+            const int e = e0 + 32 * k;
+            col[k] = e < e1 ? __ldg(A.col + e) : -1;
+            v[k] = e < e1 ? __ldg(val + e) : 0.0;
+        }
+        double xv[NC][W];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+#pragma unroll
+            for (int q = 0; q < NC; ++q) xv[q][k] = col[k] >= 0 ? __ldg(x[q] + col[k]) : 0.0;
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if (col[k] >= 0)
+#pragma unroll
+                for (int q = 0; q < NC; ++q) y[q] += v[k] * xv[q][k];
+    }
+    else
+    {
+        for (int e = e0; e < e1; e += 32)
+        {
+            const int col = A.col[e];
+            if (col < 0) break;
+            const double v = val[e];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) y[q] += v * x[q][col];
+        }
     }
 }
+
+/// Rows handled per thread by the solver kernels: RPT rows TPB apart, so a
+/// warp's rows stay contiguous and each thread has two rows' loads in flight.
+constexpr int RPT = 2;
+#define FOR_ROWS(c, n)                                                                                \
+    _Pragma("unroll") for (int rr_ = 0; rr_ < ::cfg::RPT; ++rr_) if (const int c =                   \
+                                                                       (blockIdx.x * ::cfg::RPT + rr_) * \
+                                                                           ::cfg::TPB +             \
+                                                                       threadIdx.x;                 \
+                                                                   c < (n))
 
 }  // namespace cfg

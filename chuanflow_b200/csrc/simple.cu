@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 
 #include "ctx.h"
 #include "kernels.cuh"
@@ -515,7 +516,7 @@ __global__ void __launch_bounds__(TPB) k_explicit_op(DMat A, const double* __res
     ROW_LOOP(c, A.n)
     {
         double y[1];
-        spmv_row<1>(A, val, c, xs, y);
+        spmv_row<0, 1>(A, val, c, xs, y);
         h[c] = rhs[c] - (y[0] - diag[c] * x[c]);
     }
 }
@@ -574,6 +575,7 @@ Ctx::~Ctx()
     if (stHost_) cudaFreeHost(stHost_);
     if (scalHost_) cudaFreeHost(scalHost_);
     for (int i = 0; i < 16; ++i) cudaEventDestroy(tm_.ev[i]);
+    for (auto& e : kev_) cudaEventDestroy(e);
     if (ownStream_) cudaStreamDestroy(stream_);
 }
 
@@ -592,6 +594,7 @@ void Ctx::buildDevice()
     int sms = 0;
     CFG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     G_ = std::max(1, std::min((nC + TPB - 1) / TPB, sms * 8));
+    GS_ = std::max(1, (nC + RPT * TPB - 1) / (RPT * TPB));
     GF_ = std::max(1, std::min((nF + TPB - 1) / TPB, sms * 8));
 
     // ---- per-face geometry derived on the host in the reference's order ----
@@ -685,6 +688,7 @@ void Ctx::buildDevice()
         }
         cfStart[s + 1] = cfStart[s] + 32 * w;
         mStart[s + 1] = mStart[s] + 32 * wm;
+        maxW_ = std::max(maxW_, wm);
     }
     std::vector<int> cfCode(cfStart[nSlices_], -1), cfOther(cfStart[nSlices_], 0);
     std::vector<int> mCol(mStart[nSlices_], -1), mCode(mStart[nSlices_], -1);
@@ -816,7 +820,7 @@ void Ctx::buildDevice()
         dFreeFace_ = alloc<int>(nB);
         dEmptyFace_ = alloc<int>(nB);
     }
-    partials_ = alloc<double>(static_cast<size_t>(16) * std::max(G_, GF_));
+    partials_ = alloc<double>(static_cast<size_t>(16) * std::max(std::max(G_, GF_), GS_));
     st_ = alloc<SolveState>(1);
     scal_ = alloc<double>(S_COUNT);
     CFG_CUDA(cudaMallocHost(&stHost_, sizeof(SolveState)));
@@ -1103,6 +1107,19 @@ void Ctx::gradCells(const double* const* x, int nComp, const BcTab& bc, int sche
     }
 }
 
+namespace
+{
+/// Calls f(std::integral_constant<int, W>) with the smallest compiled row
+/// width W that holds every row (0: rows of any length).
+template <class F>
+void dispatchW(int maxW, F&& f)
+{
+    if (maxW <= 7) f(std::integral_constant<int, 7>{});
+    else if (maxW <= 16) f(std::integral_constant<int, 16>{});
+    else f(std::integral_constant<int, 0>{});
+}
+}  // namespace
+
 void Ctx::runCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
                 cfg_solver_report* rep)
 {
@@ -1112,27 +1129,53 @@ void Ctx::runCG(const double* vals, const double* diag, const double* b, double*
     init.maxIter = maxIter;
     init.nComp = 1;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
-    k_cg_init<<<G_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
-    launchCheck("cg_init");
-    int launched = 0;
-    int chunk = 8;
-    for (;;)
-    {
-        CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
-        CFG_CUDA(cudaStreamSynchronize(stream_));
-        if (stHost_->allDone || launched >= maxIter) break;
-        const int n = std::min(chunk, maxIter - launched);
-        for (int k = 0; k < n; ++k)
+    dispatchW(maxW_, [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        k_cg_init<W><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
+        launchCheck("cg_init");
+        int launched = 0;
+        int chunk = 8;
+        int itBefore = 0, lastChunk = 0;
+        for (;;)
         {
-            k_cg_spmv<<<G_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
-            k_cg_update<<<G_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
-            k_cg_p<<<G_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
-            launches_ += 2;
-            launchCheck("cg_iter");
+            CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+            if (ktime_ && lastChunk > 0)
+            {
+                // only the iterations that ran (the rest returned on the done flag)
+                const int ran = std::min(lastChunk, std::max(0, stHost_->it[0] - itBefore));
+                for (int k = 0; k < ran; ++k)
+                    for (int q = 0; q < 3; ++q)
+                    {
+                        float ms = 0;
+                        CFG_CUDA(cudaEventElapsedTime(&ms, kev_[6 * k + 2 * q], kev_[6 * k + 2 * q + 1]));
+                        kstat[q][0] += 1;
+                        kstat[q][1] += ms;
+                    }
+            }
+            itBefore = stHost_->it[0];
+            if (stHost_->allDone || launched >= maxIter) break;
+            const int n = std::min(chunk, maxIter - launched);
+            for (int k = 0; k < n; ++k)
+            {
+                cudaEvent_t* ev = ktime_ ? &kev_[6 * k] : nullptr;
+                if (ev) CFG_CUDA(cudaEventRecord(ev[0], stream_));
+                k_cg_spmv<W><<<GS_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
+                if (ev) CFG_CUDA(cudaEventRecord(ev[1], stream_));
+                if (ev) CFG_CUDA(cudaEventRecord(ev[2], stream_));
+                k_cg_update<<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
+                if (ev) CFG_CUDA(cudaEventRecord(ev[3], stream_));
+                if (ev) CFG_CUDA(cudaEventRecord(ev[4], stream_));
+                k_cg_p<<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
+                if (ev) CFG_CUDA(cudaEventRecord(ev[5], stream_));
+                launches_ += 2;
+                launchCheck("cg_iter");
+            }
+            launched += n;
+            lastChunk = n;
+            chunk = std::min(chunk * 2, 64);
         }
-        launched += n;
-        chunk = std::min(chunk * 2, 64);
-    }
+    });
     rep->iterations = stHost_->it[0];
     rep->converged = stHost_->conv[0];
     rep->initial_residual = stHost_->init[0];
@@ -1149,31 +1192,35 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     init.nComp = nComp;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     const int n = dm_.nC;
-#define BI_LAUNCH(NC)                                                                                        \
-    k_bi_init<NC><<<G_, TPB, 0, stream_>>>(A, vals, b, x, br_, br0_, bp_, bv_, partials_, st_);              \
-    launchCheck("bicg_init");                                                                                \
-    for (int launched = 0, chunk = 4;;)                                                                      \
-    {                                                                                                        \
-        CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));       \
-        CFG_CUDA(cudaStreamSynchronize(stream_));                                                            \
-        if (stHost_->allDone || launched >= maxIter) break;                                                  \
-        const int m = std::min(chunk, maxIter - launched);                                                   \
-        for (int k = 0; k < m; ++k)                                                                          \
-        {                                                                                                    \
-            k_bi_p<NC><<<G_, TPB, 0, stream_>>>(n, diag, br_, bp_, bv_, bz_, st_);                           \
-            k_bi_spmv1<NC><<<G_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);                \
-            k_bi_s<NC><<<G_, TPB, 0, stream_>>>(n, diag, x, bz_, br_, bv_, bs_, bsh_, partials_, st_);       \
-            k_bi_spmv2<NC><<<G_, TPB, 0, stream_>>>(A, vals, bsh_, bt_, bs_, partials_, st_);                \
-            k_bi_x<NC><<<G_, TPB, 0, stream_>>>(n, x, bsh_, bs_, bt_, br_, br0_, partials_, st_);            \
-            launches_ += 4;                                                                                  \
-            launchCheck("bicg_iter");                                                                        \
-        }                                                                                                    \
-        launched += m;                                                                                       \
-        chunk = std::min(chunk * 2, 32);                                                                     \
-    }
-    if (nComp == 3) { BI_LAUNCH(3) }
-    else { BI_LAUNCH(1) }
-#undef BI_LAUNCH
+    auto loop = [&](auto Wc, auto NCc) {
+        constexpr int W = decltype(Wc)::value;
+        constexpr int NC = decltype(NCc)::value;
+        k_bi_init<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, b, x, br_, br0_, bp_, bv_, partials_, st_);
+        launchCheck("bicg_init");
+        for (int launched = 0, chunk = 4;;)
+        {
+            CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+            if (stHost_->allDone || launched >= maxIter) break;
+            const int m = std::min(chunk, maxIter - launched);
+            for (int k = 0; k < m; ++k)
+            {
+                k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, diag, br_, bp_, bv_, bz_, st_);
+                k_bi_spmv1<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
+                k_bi_s<NC><<<GS_, TPB, 0, stream_>>>(n, diag, x, bz_, br_, bv_, bs_, bsh_, partials_, st_);
+                k_bi_spmv2<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bt_, bs_, partials_, st_);
+                k_bi_x<NC><<<GS_, TPB, 0, stream_>>>(n, x, bsh_, bs_, bt_, br_, br0_, partials_, st_);
+                launches_ += 4;
+                launchCheck("bicg_iter");
+            }
+            launched += m;
+            chunk = std::min(chunk * 2, 32);
+        }
+    };
+    dispatchW(maxW_, [&](auto Wc) {
+        if (nComp == 3) loop(Wc, std::integral_constant<int, 3>{});
+        else loop(Wc, std::integral_constant<int, 1>{});
+    });
     for (int q = 0; q < nComp; ++q)
     {
         reps[q].iterations = stHost_->it[q];
@@ -1214,6 +1261,17 @@ void Ctx::solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, in
         runBiCG3(mVal_, uDiag_, uRhs_, ux_, 3, tol, maxIter, reps);
         for (int q = 0; q < 3; ++q) inner += reps[q].iterations;
     }
+}
+
+void Ctx::setKernelTiming(bool on)
+{
+    if (on && kev_.empty())
+    {
+        kev_.resize(6 * 64);
+        for (auto& e : kev_) CFG_CUDA(cudaEventCreate(&e));
+    }
+    ktime_ = on;
+    for (auto& r : kstat) r[0] = r[1] = 0.0;
 }
 
 void Ctx::setNu(double nu)

@@ -17,7 +17,8 @@ __device__ __forceinline__ double inv_diag_bicg(double d) { return (d > 1e-300) 
 // ------------------------------- CG ---------------------------------------
 
 /// r = b - A x; z = D^-1 r; p = z; initial residual, |b|, and r.z.
-static __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __restrict__ val,
+template <int W>
+__global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __restrict__ val,
                                                  const double* __restrict__ diag, const double* __restrict__ b,
                                                  const double* __restrict__ x, double* __restrict__ r,
                                                  double* __restrict__ p, double* partials, SolveState* st)
@@ -25,10 +26,10 @@ static __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __
     double mx[3] = {0.0, 0.0, 0.0};  // |r|, |b|, nan flag
     double sm[1] = {0.0};            // r.z
     const double* xs[1] = {x};
-    ROW_LOOP(c, A.n)
+    FOR_ROWS(c, A.n)
     {
         double y[1];
-        spmv_row<1>(A, val, c, xs, y);
+        spmv_row<W, 1>(A, val, c, xs, y);
         const double bi = b[c];
         const double ri = bi - y[0];
         r[c] = ri;
@@ -83,16 +84,17 @@ static __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __
 }
 
 /// Ap = A p and p.Ap; breakdown test and alpha (Matrix.cpp:187-194).
-static __global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const double* __restrict__ val, const double* __restrict__ p,
+template <int W>
+__global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const double* __restrict__ val, const double* __restrict__ p,
                                                  double* __restrict__ Ap, double* partials, SolveState* st)
 {
     if (st->allDone) return;
     double sm[1] = {0.0};
     const double* xs[1] = {p};
-    ROW_LOOP(c, A.n)
+    FOR_ROWS(c, A.n)
     {
         double y[1];
-        spmv_row<1>(A, val, c, xs, y);
+        spmv_row<W, 1>(A, val, c, xs, y);
         Ap[c] = y[0];
         sm[0] += p[c] * y[0];
     }
@@ -128,7 +130,7 @@ static __global__ void __launch_bounds__(TPB) k_cg_update(int n, const double* _
     const double alpha = st->alpha[0];
     double mx[2] = {0.0, 0.0};
     double sm[1] = {0.0};
-    ROW_LOOP(c, n)
+    FOR_ROWS(c, n)
     {
         x[c] = x[c] + alpha * p[c];
         const double ri = r[c] - alpha * Ap[c];
@@ -189,7 +191,7 @@ static __global__ void __launch_bounds__(TPB) k_cg_p(int n, const double* __rest
 {
     if (st->allDone) return;
     const double beta = st->beta[0];
-    ROW_LOOP(c, n) p[c] = inv_diag_cg(diag[c]) * r[c] + beta * p[c];
+    FOR_ROWS(c, n) p[c] = inv_diag_cg(diag[c]) * r[c] + beta * p[c];
 }
 
 // ------------------------ BiCGStab, 1..3 right-hand sides ------------------
@@ -199,7 +201,7 @@ static __global__ void __launch_bounds__(TPB) k_cg_p(int n, const double* __rest
 // lockstep over one matrix read; each component keeps its own scalars and
 // stops on its own test exactly where the serial loop would.
 
-template <int NC>
+template <int W, int NC>
 __global__ void __launch_bounds__(TPB) k_bi_init(DMat A, const double* __restrict__ val, V3P b, V3P x, V3P r, V3P r0,
                                                  V3P p, V3P v, double* partials, SolveState* st)
 {
@@ -212,10 +214,10 @@ __global__ void __launch_bounds__(TPB) k_bi_init(DMat A, const double* __restric
     const double* xs[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q) xs[q] = x.c[q];
-    ROW_LOOP(c, A.n)
+    FOR_ROWS(c, A.n)
     {
         double y[NC];
-        spmv_row<NC>(A, val, c, xs, y);
+        spmv_row<W, NC>(A, val, c, xs, y);
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(TPB) k_bi_p(int n, const double* __restrict__ 
         beta[q] = (st->rz[q] / st->rho[q]) * (st->alpha[q] / st->omega[q]);
         om[q] = st->omega[q];
     }
-    ROW_LOOP(c, n)
+    FOR_ROWS(c, n)
     {
         const double id = inv_diag_bicg(diag[c]);
 #pragma unroll
@@ -312,7 +314,7 @@ __global__ void __launch_bounds__(TPB) k_bi_p(int n, const double* __restrict__ 
 }
 
 /// v = A z; r0.v; alpha (Matrix.cpp:273-276)
-template <int NC>
+template <int W, int NC>
 __global__ void __launch_bounds__(TPB) k_bi_spmv1(DMat A, const double* __restrict__ val, V3P z, V3P v, V3P r0,
                                                   double* partials, SolveState* st)
 {
@@ -323,10 +325,10 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv1(DMat A, const double* __restri
     const double* xs[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q) xs[q] = z.c[q];
-    ROW_LOOP(c, A.n)
+    FOR_ROWS(c, A.n)
     {
         double y[NC];
-        spmv_row<NC>(A, val, c, xs, y);
+        spmv_row<W, NC>(A, val, c, xs, y);
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(TPB) k_bi_s(int n, const double* __restrict__ 
         al[q] = st->alpha[q];
         mx[q] = mx[NC + q] = 0.0;
     }
-    ROW_LOOP(c, n)
+    FOR_ROWS(c, n)
     {
         const double id = inv_diag_bicg(diag[c]);
 #pragma unroll
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(TPB) k_bi_s(int n, const double* __restrict__ 
 }
 
 /// t = A sh; t.t and t.s; omega, or the tDenom breakdown exit (Matrix.cpp:290-300)
-template <int NC>
+template <int W, int NC>
 __global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restrict__ val, V3P sh, V3P t, V3P s,
                                                   double* partials, SolveState* st)
 {
@@ -419,10 +421,10 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restri
     const double* xs[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q) xs[q] = sh.c[q];
-    ROW_LOOP(c, A.n)
+    FOR_ROWS(c, A.n)
     {
         double y[NC];
-        spmv_row<NC>(A, val, c, xs, y);
+        spmv_row<W, NC>(A, val, c, xs, y);
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(TPB) k_bi_x(int n, V3P x, V3P sh, V3P s, V3P t
         mx[q] = mx[NC + q] = 0.0;
         sm[q] = 0.0;
     }
-    ROW_LOOP(c, n)
+    FOR_ROWS(c, n)
     {
 #pragma unroll
         for (int q = 0; q < NC; ++q)

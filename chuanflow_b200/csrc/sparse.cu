@@ -1,6 +1,7 @@
 // solveCG / solveBiCGStab on a caller's CSR matrix (src/common/src/Matrix.cpp:153-319):
 // the drop-in for the reference's linear-solver call surface.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "ctx.h"
@@ -105,6 +106,9 @@ void Ctx::sparseSolve(int device, int64_t n64, const int64_t* rs, const int64_t*
     int sms = 0;
     CFG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int G = std::max(1, std::min((n + TPB - 1) / TPB, sms * 8));
+    const int GS = std::max(1, (n + RPT * TPB - 1) / (RPT * TPB));
+    int maxW = 0;
+    for (int sl = 0; sl < nS; ++sl) maxW = std::max(maxW, (start[sl + 1] - start[sl]) / 32);
     int* dStart = buf.get<int>(start.size());
     int* dCol = buf.get<int>(col.size());
     int* dIsDiag = buf.get<int>(isDiag.size());
@@ -120,7 +124,7 @@ void Ctx::sparseSolve(int device, int64_t n64, const int64_t* rs, const int64_t*
     CFG_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
     const DMat A{n, dStart, dCol};
     k_diag_from_sell<<<G, TPB, 0, s>>>(A, dIsDiag, dVal, dDiag);
-    double* partials = buf.get<double>(16 * static_cast<size_t>(G));
+    double* partials = buf.get<double>(16 * static_cast<size_t>(std::max(G, GS)));
     SolveState* st = buf.get<SolveState>(1);
     SolveState* hst = nullptr;
     CFG_CUDA(cudaMallocHost(&hst, sizeof(SolveState)));
@@ -139,59 +143,65 @@ void Ctx::sparseSolve(int device, int64_t n64, const int64_t* rs, const int64_t*
         CFG_CUDA(cudaStreamSynchronize(s));
         return hst->allDone != 0;
     };
-    if (method == CFG_SOLVE_CG)
-    {
-        double* r = buf.get<double>(n);
-        double* p = buf.get<double>(n);
-        double* Ap = buf.get<double>(n);
-        k_cg_init<<<G, TPB, 0, s>>>(A, dVal, dDiag, db, dx, r, p, partials, st);
-        CFG_CUDA(cudaGetLastError());
-        for (int launched = 0, chunk = 8; !poll() && launched < maxIter; chunk = std::min(2 * chunk, 64))
+    auto run = [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        if (method == CFG_SOLVE_CG)
         {
-            const int m = std::min(chunk, maxIter - launched);
-            for (int k = 0; k < m; ++k)
-            {
-                k_cg_spmv<<<G, TPB, 0, s>>>(A, dVal, p, Ap, partials, st);
-                k_cg_update<<<G, TPB, 0, s>>>(n, dDiag, p, Ap, dx, r, partials, st);
-                k_cg_p<<<G, TPB, 0, s>>>(n, dDiag, r, p, st);
-            }
+            double* r = buf.get<double>(n);
+            double* p = buf.get<double>(n);
+            double* Ap = buf.get<double>(n);
+            k_cg_init<W><<<GS, TPB, 0, s>>>(A, dVal, dDiag, db, dx, r, p, partials, st);
             CFG_CUDA(cudaGetLastError());
-            launched += m;
-        }
-    }
-    else
-    {
-        V3P r{}, r0{}, p{}, v{}, sv{}, sh{}, t{}, z{}, bb{}, xx{};
-        for (int q = 0; q < 3; ++q)
-        {
-            r.c[q] = buf.get<double>(n);
-            r0.c[q] = buf.get<double>(n);
-            p.c[q] = buf.get<double>(n);
-            v.c[q] = buf.get<double>(n);
-            sv.c[q] = buf.get<double>(n);
-            sh.c[q] = buf.get<double>(n);
-            t.c[q] = buf.get<double>(n);
-            z.c[q] = buf.get<double>(n);
-            bb.c[q] = db;
-            xx.c[q] = dx;
-        }
-        k_bi_init<1><<<G, TPB, 0, s>>>(A, dVal, bb, xx, r, r0, p, v, partials, st);
-        CFG_CUDA(cudaGetLastError());
-        for (int launched = 0, chunk = 4; !poll() && launched < maxIter; chunk = std::min(2 * chunk, 32))
-        {
-            const int m = std::min(chunk, maxIter - launched);
-            for (int k = 0; k < m; ++k)
+            for (int launched = 0, chunk = 8; !poll() && launched < maxIter; chunk = std::min(2 * chunk, 64))
             {
-                k_bi_p<1><<<G, TPB, 0, s>>>(n, dDiag, r, p, v, z, st);
-                k_bi_spmv1<1><<<G, TPB, 0, s>>>(A, dVal, z, v, r0, partials, st);
-                k_bi_s<1><<<G, TPB, 0, s>>>(n, dDiag, xx, z, r, v, sv, sh, partials, st);
-                k_bi_spmv2<1><<<G, TPB, 0, s>>>(A, dVal, sh, t, sv, partials, st);
-                k_bi_x<1><<<G, TPB, 0, s>>>(n, xx, sh, sv, t, r, r0, partials, st);
+                const int m = std::min(chunk, maxIter - launched);
+                for (int k = 0; k < m; ++k)
+                {
+                    k_cg_spmv<W><<<GS, TPB, 0, s>>>(A, dVal, p, Ap, partials, st);
+                    k_cg_update<<<GS, TPB, 0, s>>>(n, dDiag, p, Ap, dx, r, partials, st);
+                    k_cg_p<<<GS, TPB, 0, s>>>(n, dDiag, r, p, st);
+                }
+                CFG_CUDA(cudaGetLastError());
+                launched += m;
             }
-            CFG_CUDA(cudaGetLastError());
-            launched += m;
         }
-    }
+        else
+        {
+            V3P r{}, r0{}, p{}, v{}, sv{}, sh{}, t{}, z{}, bb{}, xx{};
+            for (int q = 0; q < 3; ++q)
+            {
+                r.c[q] = buf.get<double>(n);
+                r0.c[q] = buf.get<double>(n);
+                p.c[q] = buf.get<double>(n);
+                v.c[q] = buf.get<double>(n);
+                sv.c[q] = buf.get<double>(n);
+                sh.c[q] = buf.get<double>(n);
+                t.c[q] = buf.get<double>(n);
+                z.c[q] = buf.get<double>(n);
+                bb.c[q] = db;
+                xx.c[q] = dx;
+            }
+            k_bi_init<W, 1><<<GS, TPB, 0, s>>>(A, dVal, bb, xx, r, r0, p, v, partials, st);
+            CFG_CUDA(cudaGetLastError());
+            for (int launched = 0, chunk = 4; !poll() && launched < maxIter; chunk = std::min(2 * chunk, 32))
+            {
+                const int m = std::min(chunk, maxIter - launched);
+                for (int k = 0; k < m; ++k)
+                {
+                    k_bi_p<1><<<GS, TPB, 0, s>>>(n, dDiag, r, p, v, z, st);
+                    k_bi_spmv1<W, 1><<<GS, TPB, 0, s>>>(A, dVal, z, v, r0, partials, st);
+                    k_bi_s<1><<<GS, TPB, 0, s>>>(n, dDiag, xx, z, r, v, sv, sh, partials, st);
+                    k_bi_spmv2<W, 1><<<GS, TPB, 0, s>>>(A, dVal, sh, t, sv, partials, st);
+                    k_bi_x<1><<<GS, TPB, 0, s>>>(n, xx, sh, sv, t, r, r0, partials, st);
+                }
+                CFG_CUDA(cudaGetLastError());
+                launched += m;
+            }
+        }
+    };
+    if (maxW <= 7) run(std::integral_constant<int, 7>{});
+    else if (maxW <= 16) run(std::integral_constant<int, 16>{});
+    else run(std::integral_constant<int, 0>{});
     CFG_CUDA(cudaMemcpyAsync(x, dx, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CFG_CUDA(cudaStreamSynchronize(s));
     rep->iterations = hst->it[0];

@@ -210,6 +210,13 @@ int cfg_simple_iterate(cfg_ctx* ctx, const cfg_simple_controls* controls, cfg_si
  * pressure solve, flux/update, continuity, other, total. */
 int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
 
+/* Opt-in CUDA-event timing of every pressure-PCG kernel launch on the
+ * context's stream (no reference counterpart).  Enabling clears the counts;
+ * cfg_kernel_stats gives {launches, total ms} for the SpMV + p.Ap kernel,
+ * the x/r update + |r| + r.z kernel, and the search-direction update. */
+int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable);
+int cfg_kernel_stats(const cfg_ctx* ctx, double out[6]);
+
 /* ---- the linear-solver call surface ------------------------------------ */
 
 /* solveCG / solveBiCGStab on a CSR matrix (src/common/include/cf/common/Matrix.h:67-73,

@@ -1122,6 +1122,8 @@ static void fvmat_build_csr(fvmat* e)
 }
 
 /* fvMatrix::solve (fvMatrix.cpp:73-129), relaxation 1 */
+static int64_t g_innerSum;
+
 static cfo_report fvmat_solve(fvmat* e, const geo_ctx* g, double tol, int maxIter, int nonOrth, int gradScheme)
 {
     const int64_t n = e->n;
@@ -1144,6 +1146,7 @@ static cfo_report fvmat_solve(fvmat* e, const geo_ctx* g, double tol, int maxIte
                 cfo_solve_bicgstab(n, e->rs, e->cols, e->vals + q * e->nnz, e->rhs + q * n, e->x + q * n, tol,
                                    maxIter, &rep);
             last = rep;
+            g_innerSum += rep.iterations;
         }
     }
     free(base);
@@ -1435,7 +1438,9 @@ int cfo_simple(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, do
         vol_grad(&w, p, pc, pk, ctl->grad, gradPn);
         fvmat UE;
         build_ueqn(&UE, &w, ctl, uc, uk, phi, gradPn);
+        g_innerSum = 0;
         const cfo_report uRep = fvmat_solve(&UE, &w.g, ctl->linearTol, ctl->linearMaxIter, ctl->nonOrthCorrectors, ctl->grad);
+        res->uItersTotal += g_innerSum;
         res->lastUIters = uRep.iterations;
         memcpy(UOld, U, sizeof(double) * (size_t)(3 * nC));
         for (int q = 1; q < 3; ++q)
@@ -1481,7 +1486,9 @@ int cfo_simple(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, do
         interp_to_faces(&w, rAUr, rAUf);
         fvmat PE;
         build_peqn(&PE, &w, ctl, pc, pk, rAUf, dphi);
+        g_innerSum = 0;
         const cfo_report pRep = fvmat_solve(&PE, &w.g, ctl->linearTol, ctl->linearMaxIter, ctl->nonOrthCorrectors, ctl->grad);
+        res->pItersTotal += g_innerSum;
         res->lastPIters = pRep.iterations;
         memcpy(pNew, PE.x, sizeof(double) * (size_t)nC);
         fvmat_free(&PE);

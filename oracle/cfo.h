@@ -105,6 +105,7 @@ typedef struct cfo_result
     double finalMomentumResidual;
     int32_t lastUIters, lastPIters;
     int32_t error;
+    int64_t uItersTotal, pItersTotal; /* summed over components, passes, iterations */
 } cfo_result;
 
 typedef struct cfo_report

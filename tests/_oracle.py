@@ -58,7 +58,7 @@ class Controls(C.Structure):
 class Result(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("finalContinuityError", C.c_double),
                 ("finalMomentumResidual", C.c_double), ("lastUIters", C.c_int32), ("lastPIters", C.c_int32),
-                ("error", C.c_int32)]
+                ("error", C.c_int32), ("uItersTotal", C.c_int64), ("pItersTotal", C.c_int64)]
 
 
 class Report(C.Structure):
