@@ -25,6 +25,7 @@ from ._capi import (  # noqa: F401
     SimpleResult,
     SolverReport,
     lib,
+    inspect_case_file,
     lib_path,
     run_case_file,
     solve_bicgstab,
@@ -32,4 +33,4 @@ from ._capi import (  # noqa: F401
 )
 
 __all__ = ["BC", "DIV", "GRAD", "CfgError", "PolyMesh", "Schemes", "SimpleCase", "SimpleControls",
-           "SimpleResult", "SolverReport", "lib", "lib_path", "run_case_file", "solve_bicgstab", "solve_cg"]
+           "SimpleResult", "SolverReport", "inspect_case_file", "lib", "lib_path", "run_case_file", "solve_bicgstab", "solve_cg"]

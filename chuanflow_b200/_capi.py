@@ -413,6 +413,21 @@ def solve_bicgstab(row_start, cols, vals, b, x0, tol, max_iter, device=0):
     return _sparse(1, row_start, cols, vals, b, x0, tol, max_iter, device)
 
 
+def inspect_case_file(path):
+    """Host-only parse of a case file: a dict of what the runner would use."""
+    buf = C.create_string_buffer(1 << 16)
+    _check(lib().cfg_case_inspect(str(path).encode(), buf, C.c_size_t(1 << 16)))
+    out = {"patches": {}}
+    for ln in buf.value.decode().splitlines():
+        k, *v = ln.split()
+        if k == "patch":
+            out["patches"][v[0]] = {"type": v[1], "start": int(v[2]), "size": int(v[3]), "U_type": int(v[5]),
+                                    "U": tuple(float(x) for x in v[6:9]), "p_type": int(v[10]), "p": float(v[11])}
+        else:
+            out[k] = [float(x) if any(ch in x for ch in ".e") or x.lstrip("-").isdigit() else x for x in v]
+    return out
+
+
 def run_case_file(path, device=0):
     """A chflow-simple-foam case file end to end; returns (result, U, p, phi)."""
     counts = np.zeros(5, np.int64)

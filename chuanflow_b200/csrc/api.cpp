@@ -1,6 +1,8 @@
 // The extern "C" boundary: status codes, the per-thread error message, and
 // the case-file runner.
+#include <array>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <string>
 
@@ -413,134 +415,206 @@ int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t 
     });
 }
 
+}  // extern "C"
+
+namespace
+{
+
+/// A chflow-simple-foam case parsed on the host: mesh, boundary conditions
+/// (per patch: U type/value, p type/value), initial U, schemes, controls.
+struct CaseSpec
+{
+    cfg::Mesh mesh;
+    std::vector<int> uType, pType;
+    std::vector<std::array<double, 3>> uVal;
+    std::vector<double> pVal;
+    bool hasU0 = false;
+    double u0[3] = {0, 0, 0};
+    cfg_schemes schemes{CFG_DIV_UPWIND, 1, CFG_GRAD_CORRECTED, 0.9};
+    cfg_simple_controls ctl{};
+};
+
+CaseSpec parseCase(const char* path)
+{
+    const cfg::Dict d = cfg::Dict::parseFile(path);
+    CaseSpec cs;
+    // mesh: block{} (BlockMesh::fromDict, blockMesh.cpp:191-223)
+    if (!d.has("block")) cfg::fail(CFG_ESETUP, "case: only block {} meshes are read from a case file");
+    const cfg::Dict& b = d.dict("block");
+    const auto mn = b.numbers("min"), mx = b.numbers("max"), nc = b.numbers("cells");
+    if (mn.size() != 3 || mx.size() != 3 || nc.size() != 3)
+        cfg::fail(CFG_ESETUP, "blockMesh: min/max/cells need 3 values each");
+    const char* keys[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+    std::vector<std::string> names = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+    std::vector<std::string> types = {"wall", "wall", "wall", "wall", "symmetry", "symmetry"};
+    for (int s = 0; s < 6; ++s)
+        if (b.has(keys[s]))
+        {
+            const cfg::Dict& sd = b.dict(keys[s]);
+            names[s] = sd.wordOr("name", keys[s]);
+            types[s] = sd.wordOr("type", "wall");
+        }
+    cs.mesh = cfg::blockMesh({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, static_cast<int64_t>(nc[0]),
+                             static_cast<int64_t>(nc[1]), static_cast<int64_t>(nc[2]), names, types);
+    const cfg::Mesh& M = cs.mesh;
+    const size_t nP = M.patches.size();
+    // the fields' defaults: every patch zeroGradient (volFields.cpp:46-50)
+    cs.uType.assign(nP, CFG_BC_ZERO_GRADIENT);
+    cs.pType.assign(nP, CFG_BC_ZERO_GRADIENT);
+    cs.uVal.assign(nP, {0, 0, 0});
+    cs.pVal.assign(nP, 0.0);
+    // patches{} (simpleFoamApp.cpp:54-91)
+    if (d.has("patches"))
+    {
+        const cfg::Dict& ps = d.dict("patches");
+        for (const auto& name : ps.keys())
+        {
+            const cfg::Dict& pd = ps.dict(name);
+            int patch = -1;
+            for (size_t i = 0; i < nP; ++i)
+                if (M.patches[i].name == name) patch = static_cast<int>(i);
+            if (patch < 0) cfg::fail(CFG_ESETUP, "polyMesh: no patch named '" + name + "'");
+            if (pd.has("U"))
+            {
+                const auto ul = pd.numbers("U");
+                if (ul.size() != 3) cfg::fail(CFG_ESETUP, "patch U needs 3 values");
+                cs.uType[patch] = bcFromName(pd.wordOr("UType", "fixedValue"));
+                cs.uVal[patch] = {ul[0], ul[1], ul[2]};
+            }
+            else
+            {
+                const bool isWall = M.patches[patch].type == "wall";
+                cs.uType[patch] = isWall ? CFG_BC_FIXED_VALUE : bcFromName(pd.wordOr("UType", "zeroGradient"));
+            }
+            if (pd.has("p"))
+            {
+                cs.pType[patch] = bcFromName(pd.wordOr("pType", "fixedValue"));
+                cs.pVal[patch] = pd.number("p");
+            }
+            else
+            {
+                cs.pType[patch] = CFG_BC_ZERO_GRADIENT;
+            }
+        }
+    }
+    // initial{U} (caseInit.h:18-31)
+    if (d.has("initial") && d.dict("initial").has("U"))
+    {
+        const auto u0 = d.dict("initial").numbers("U");
+        cs.hasU0 = true;
+        for (int i = 0; i < 3; ++i) cs.u0[i] = u0[i];
+    }
+    // schemes{} (fvMatrix.cpp:148-160)
+    if (d.has("schemes"))
+    {
+        const cfg::Dict& s = d.dict("schemes");
+        const std::string div = s.wordOr("div", "upwind");
+        cs.schemes.div = div == "linear" ? CFG_DIV_LINEAR : (div == "blend" ? CFG_DIV_BLEND : CFG_DIV_UPWIND);
+        cs.schemes.laplacian_corrected = s.wordOr("laplacian", "corrected") == "corrected";
+        const std::string g = s.wordOr("grad", "corrected");
+        cs.schemes.grad =
+            g == "corrected" ? CFG_GRAD_CORRECTED : (g == "leastSquares" ? CFG_GRAD_LEAST_SQUARES : CFG_GRAD_LINEAR);
+        cs.schemes.blend_coeff = s.numberOr("blendCoeff", 0.9);
+    }
+    // simple{} (SimpleSolver.h:13-64 defaults; simpleFoamApp.cpp:115-132,
+    // linearTol / linearMaxIter read as multiCoupledApp.cpp:41-57 reads them)
+    cfg_simple_controls& c = cs.ctl;
+    c.max_iterations = 200;
+    c.continuity_tol = 1e-6;
+    c.linear_tol = 1e-7;
+    c.linear_max_iter = 2000;
+    c.non_orth_correctors = 2;
+    c.relax_u = 0.7;
+    c.relax_p = 0.3;
+    c.p_ref_cell = -1;
+    c.verbose = 1;
+    c.nu = d.number("nu");
+    if (d.has("simple"))
+    {
+        const cfg::Dict& s = d.dict("simple");
+        c.max_iterations = static_cast<int32_t>(s.numberOr("maxIterations", c.max_iterations));
+        c.continuity_tol = s.numberOr("continuityTol", c.continuity_tol);
+        c.pcorr_tol = s.numberOr("pcorrTol", c.pcorr_tol);
+        c.relax_u = s.numberOr("relaxU", c.relax_u);
+        c.relax_p = s.numberOr("relaxP", c.relax_p);
+        c.p_relax_start = s.numberOr("pRelaxStart", c.p_relax_start);
+        c.non_orth_correctors = static_cast<int32_t>(s.numberOr("nonOrthCorrectors", c.non_orth_correctors));
+        c.momentum_tol = s.numberOr("momentumTol", c.momentum_tol);
+        c.linear_tol = s.numberOr("linearTol", c.linear_tol);
+        c.linear_max_iter = static_cast<int32_t>(s.numberOr("linearMaxIter", c.linear_max_iter));
+        if (s.has("force"))
+        {
+            const auto f = s.numbers("force");
+            if (f.size() != 3) cfg::fail(CFG_ESETUP, "simple force needs 3 values");
+            for (int i = 0; i < 3; ++i) c.body_force[i] = f[i];
+        }
+    }
+    // gpu{}: settings the reference does not have; defaults reproduce it
+    if (d.has("gpu"))
+    {
+        const cfg::Dict& g = d.dict("gpu");
+        c.p_precond = g.wordOr("pPreconditioner", "Jacobi") == "DIC" ? CFG_PRECOND_DIC : CFG_PRECOND_JACOBI;
+        c.p_ref_cell = static_cast<int64_t>(g.numberOr("pRefCell", -1));
+        c.p_ref_value = g.numberOr("pRefValue", 0.0);
+        c.verbose = static_cast<int32_t>(g.numberOr("verbose", 1));
+    }
+    return cs;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfg_case_inspect(const char* path, char* out, size_t size)
+{
+    return guard([&] {
+        need(path && out && size, "cfg_case_inspect: null argument");
+        const CaseSpec cs = parseCase(path);
+        std::string s;
+        char buf[256];
+        auto add = [&](const char* fmt, auto... v) {
+            std::snprintf(buf, sizeof buf, fmt, v...);
+            s += buf;
+        };
+        add("cells %lld\nfaces %lld\ninternal %lld\n", static_cast<long long>(cs.mesh.nCells),
+            static_cast<long long>(cs.mesh.nFaces()), static_cast<long long>(cs.mesh.nInternal()));
+        for (size_t i = 0; i < cs.mesh.patches.size(); ++i)
+            add("patch %s %s %lld %lld U %d %.17g %.17g %.17g p %d %.17g\n", cs.mesh.patches[i].name.c_str(),
+                cs.mesh.patches[i].type.c_str(), static_cast<long long>(cs.mesh.patches[i].start),
+                static_cast<long long>(cs.mesh.patches[i].size), cs.uType[i], cs.uVal[i][0], cs.uVal[i][1],
+                cs.uVal[i][2], cs.pType[i], cs.pVal[i]);
+        add("schemes %d %d %d %.17g\n", cs.schemes.div, cs.schemes.laplacian_corrected, cs.schemes.grad,
+            cs.schemes.blend_coeff);
+        const cfg_simple_controls& c = cs.ctl;
+        add("simple %d %.17g %.17g %.17g %.17g %d %d %.17g %.17g %.17g\n", c.max_iterations, c.continuity_tol,
+            c.pcorr_tol, c.momentum_tol, c.linear_tol, c.linear_max_iter, c.non_orth_correctors, c.relax_u, c.relax_p,
+            c.p_relax_start);
+        add("force %.17g %.17g %.17g\nnu %.17g\n", c.body_force[0], c.body_force[1], c.body_force[2], c.nu);
+        add("gpu %d %lld %.17g\n", c.p_precond, static_cast<long long>(c.p_ref_cell), c.p_ref_value);
+        if (cs.hasU0) add("initialU %.17g %.17g %.17g\n", cs.u0[0], cs.u0[1], cs.u0[2]);
+        std::snprintf(out, size, "%s", s.c_str());
+    });
+}
+
 int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* result, int64_t counts[5], double* U,
                       double* p, double* phi)
 {
     return guard([&] {
         need(path && result, "cfg_run_case_file: null argument");
-        const cfg::Dict d = cfg::Dict::parseFile(path);
-        // mesh: block{} (BlockMesh::fromDict, blockMesh.cpp:191-223)
-        if (!d.has("block")) cfg::fail(CFG_ESETUP, "case: only block {} meshes are read by cfg_run_case_file");
-        const cfg::Dict& b = d.dict("block");
-        const auto mn = b.numbers("min"), mx = b.numbers("max"), nc = b.numbers("cells");
-        if (mn.size() != 3 || mx.size() != 3 || nc.size() != 3)
-            cfg::fail(CFG_ESETUP, "blockMesh: min/max/cells need 3 values each");
-        const char* keys[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
-        std::vector<std::string> names = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
-        std::vector<std::string> types = {"wall", "wall", "wall", "wall", "symmetry", "symmetry"};
-        for (int s = 0; s < 6; ++s)
-            if (b.has(keys[s]))
-            {
-                const cfg::Dict& sd = b.dict(keys[s]);
-                names[s] = sd.wordOr("name", keys[s]);
-                types[s] = sd.wordOr("type", "wall");
-            }
-        cfg::Mesh M = cfg::blockMesh({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, static_cast<int64_t>(nc[0]),
-                                     static_cast<int64_t>(nc[1]), static_cast<int64_t>(nc[2]), names, types);
-        const int32_t dev = device;
-        cfg::Ctx ctx(M, dev, nullptr);
-        // patches{} (simpleFoamApp.cpp:54-91)
-        if (d.has("patches"))
+        const CaseSpec cs = parseCase(path);
+        const cfg::Mesh& M = cs.mesh;
+        cfg::Ctx ctx(M, device, nullptr);
+        for (size_t i = 0; i < M.patches.size(); ++i)
         {
-            const cfg::Dict& ps = d.dict("patches");
-            for (const auto& name : ps.keys())
-            {
-                const cfg::Dict& pd = ps.dict(name);
-                int patch = -1;
-                for (size_t i = 0; i < M.patches.size(); ++i)
-                    if (M.patches[i].name == name) patch = static_cast<int>(i);
-                if (patch < 0) cfg::fail(CFG_ESETUP, "polyMesh: no patch named '" + name + "'");
-                if (pd.has("U"))
-                {
-                    const auto ul = pd.numbers("U");
-                    ctx.setPatchBC('U', patch, bcFromName(pd.wordOr("UType", "fixedValue")), ul.data());
-                }
-                else
-                {
-                    const bool isWall = M.patches[patch].type == "wall";
-                    const double z[3] = {0, 0, 0};
-                    ctx.setPatchBC('U', patch, isWall ? CFG_BC_FIXED_VALUE : bcFromName(pd.wordOr("UType", "zeroGradient")), z);
-                }
-                if (pd.has("p"))
-                {
-                    const double v = pd.number("p");
-                    ctx.setPatchBC('p', patch, bcFromName(pd.wordOr("pType", "fixedValue")), &v);
-                }
-                else
-                {
-                    const double z = 0;
-                    ctx.setPatchBC('p', patch, CFG_BC_ZERO_GRADIENT, &z);
-                }
-            }
+            const int pi = static_cast<int>(i);
+            ctx.setPatchBC('U', pi, cs.uType[i], cs.uVal[i].data());
+            ctx.setPatchBC('p', pi, cs.pType[i], &cs.pVal[i]);
         }
-        // initial flux and optional initial{U} (simpleFoamApp.cpp:93-95, caseInit.h:18-31)
-        if (d.has("initial") && d.dict("initial").has("U"))
-        {
-            const auto u0 = d.dict("initial").numbers("U");
-            ctx.initFlux(nullptr);
-            ctx.initFlux(u0.data());
-        }
-        else
-        {
-            ctx.initFlux(nullptr);
-        }
-        // schemes{} (fvMatrix.cpp:148-160)
-        cfg_schemes sc{CFG_DIV_UPWIND, 1, CFG_GRAD_CORRECTED, 0.9};
-        if (d.has("schemes"))
-        {
-            const cfg::Dict& s = d.dict("schemes");
-            const std::string div = s.wordOr("div", "upwind");
-            sc.div = div == "linear" ? CFG_DIV_LINEAR : (div == "blend" ? CFG_DIV_BLEND : CFG_DIV_UPWIND);
-            sc.laplacian_corrected = s.wordOr("laplacian", "corrected") == "corrected";
-            const std::string g = s.wordOr("grad", "corrected");
-            sc.grad = g == "corrected" ? CFG_GRAD_CORRECTED : (g == "leastSquares" ? CFG_GRAD_LEAST_SQUARES : CFG_GRAD_LINEAR);
-            sc.blend_coeff = s.numberOr("blendCoeff", 0.9);
-        }
-        ctx.setSchemes(sc);
-        // simple{} (SimpleSolver.h:13-64 defaults; simpleFoamApp.cpp:115-132,
-        // linearTol/linearMaxIter as multiCoupledApp.cpp:41-57 reads them)
-        cfg_simple_controls c{};
-        c.p_ref_cell = -1;
-        c.max_iterations = 200;
-        c.continuity_tol = 1e-6;
-        c.linear_tol = 1e-7;
-        c.linear_max_iter = 2000;
-        c.non_orth_correctors = 2;
-        c.relax_u = 0.7;
-        c.relax_p = 0.3;
-        c.nu = d.number("nu");
-        if (d.has("simple"))
-        {
-            const cfg::Dict& s = d.dict("simple");
-            c.max_iterations = static_cast<int32_t>(s.numberOr("maxIterations", c.max_iterations));
-            c.continuity_tol = s.numberOr("continuityTol", c.continuity_tol);
-            c.pcorr_tol = s.numberOr("pcorrTol", c.pcorr_tol);
-            c.relax_u = s.numberOr("relaxU", c.relax_u);
-            c.relax_p = s.numberOr("relaxP", c.relax_p);
-            c.p_relax_start = s.numberOr("pRelaxStart", c.p_relax_start);
-            c.non_orth_correctors = static_cast<int32_t>(s.numberOr("nonOrthCorrectors", c.non_orth_correctors));
-            c.momentum_tol = s.numberOr("momentumTol", c.momentum_tol);
-            c.linear_tol = s.numberOr("linearTol", c.linear_tol);
-            c.linear_max_iter = static_cast<int32_t>(s.numberOr("linearMaxIter", c.linear_max_iter));
-            if (s.has("force"))
-            {
-                const auto f = s.numbers("force");
-                for (int i = 0; i < 3; ++i) c.body_force[i] = f[i];
-            }
-        }
-        if (d.has("gpu"))
-        {
-            const cfg::Dict& g = d.dict("gpu");
-            c.p_precond = g.wordOr("pPreconditioner", "Jacobi") == "DIC" ? CFG_PRECOND_DIC : CFG_PRECOND_JACOBI;
-            c.p_ref_cell = static_cast<int64_t>(g.numberOr("pRefCell", -1));
-            c.p_ref_value = g.numberOr("pRefValue", 0.0);
-            c.verbose = static_cast<int32_t>(g.numberOr("verbose", 1));
-        }
-        else
-        {
-            c.verbose = 1;
-        }
-        ctx.iterate(c, *result);
+        // the initial flux (simpleFoamApp.cpp:93-95) and the seeded field
+        ctx.initFlux(nullptr);
+        if (cs.hasU0) ctx.initFlux(cs.u0);
+        ctx.setSchemes(cs.schemes);
+        ctx.iterate(cs.ctl, *result);
         if (counts)
         {
             counts[0] = static_cast<int64_t>(M.points.size());

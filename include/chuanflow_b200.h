@@ -254,6 +254,10 @@ int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t 
 int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* result, int64_t counts[5],
                       double* U, double* p, double* phi);
 
+/* Parses a case file on the host only (no device): writes a text summary
+ * of the mesh counts, every patch's U/p conditions, schemes and controls. */
+int cfg_case_inspect(const char* path, char* out, size_t size);
+
 #ifdef __cplusplus
 }
 #endif

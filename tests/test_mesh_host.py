@@ -1,0 +1,88 @@
+"""The product's host-side mesh (libchuanflow_b200.so, no device needed):
+blockMesh addressing, geometry, weights and the interior jitter, bit-for-bit
+against the reference (fixtures) and the oracle, plus the reference's mesh
+errors.  CPU only."""
+import numpy as np
+import pytest
+
+import _cases as K
+import _oracle as O
+
+cf = pytest.importorskip("chuanflow_b200")
+
+
+def check_same(mesh, om):
+    a = mesh.addressing()
+    g = mesh.geometry()
+    for k in ("face_offsets", "face_verts", "owner", "neighbour", "points"):
+        assert np.array_equal(a[k], getattr(om, k)), k
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(g[k], getattr(om, k)), k
+    ow, sk = mesh.weights()
+    assert np.array_equal(ow, om.owner_weights())
+    assert np.array_equal(sk, om.skew())
+
+
+def test_block_matches_fixture(golden):
+    g = golden("mesh_block_2x2x2.npz")
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (2, 2, 2))
+    assert (m.n_cells, m.n_internal_faces, m.n_boundary_faces) == (8, 12, 24)
+    a = m.addressing()
+    for k in ("face_offsets", "face_verts", "owner", "neighbour", "points"):
+        assert np.array_equal(a[k], g[k]), k
+    geo = m.geometry()
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(geo[k], g[k]), k
+    assert [p[0] for p in m.patches] == ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
+    assert [p[1] for p in m.patches] == ["wall", "wall", "wall", "wall", "symmetry", "symmetry"]
+
+
+@pytest.mark.parametrize("cells,jitter", [((6, 5, 4), 0.1), ((9, 3, 7), 0.2), ((1, 1, 1), 0.0), ((12, 1, 3), 0.1)])
+def test_block_and_jitter_match_oracle(cells, jitter):
+    mn, mx = (0.0, -1.0, 0.5), (2.0, 0.5, 1.25)
+    mesh = cf.PolyMesh.block(mn, mx, cells, {s: (n, "wall") for s, n in zip(K.SIDES, K.CAVITY_NAMES)})
+    om = O.block_mesh(mn, mx, cells, K.CAVITY_NAMES, ["wall"] * 6)
+    if jitter:
+        mesh.jitter_interior(jitter, 99)
+        om = om.with_points(K.jitter_points(om.points, cells, mn, mx, jitter, 99))
+    check_same(mesh, om)
+
+
+@pytest.mark.parametrize("fixture", ["mesh_tets22.npz", "mesh_hex41.npz"])
+def test_general_mesh_geometry_matches_reference(golden, fixture):
+    g = golden(fixture)
+    pats = [(str(n), str(t), int(s), int(z)) for n, t, s, z in
+            zip(g["patch_names"], g["patch_types"], g["patch_start"], g["patch_size"])]
+    m = cf.PolyMesh(g["points"], g["face_offsets"], g["face_verts"], g["owner"], g["neighbour"], pats)
+    geo = m.geometry()
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(geo[k], g[k]), k
+    ow, sk = m.weights()
+    assert np.array_equal(ow, g["ow"]) and np.array_equal(sk, g["skew"])
+
+
+def test_move_points_recomputes_geometry():
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (3, 3, 3))
+    pts = m.addressing()["points"] * 2.0
+    m.move_points(pts)
+    assert abs(m.geometry()["V"].sum() - 8.0) < 1e-12
+    with pytest.raises(cf.CfgError, match="point count changed"):
+        m.move_points(pts[:-1])
+
+
+def test_mesh_errors_follow_reference():
+    g = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (2, 1, 1))
+    a = g.addressing()
+    nI = g.n_internal_faces
+    ok = [(p[0], p[1], p[2], p[3]) for p in g.patches]
+    bad_internal = [("a", "wall", 0, 1)] + ok
+    with pytest.raises(cf.CfgError, match="covers internal face"):
+        cf.PolyMesh(a["points"], a["face_offsets"], a["face_verts"], a["owner"], a["neighbour"], bad_internal)
+    with pytest.raises(cf.CfgError, match="is not in any patch"):
+        cf.PolyMesh(a["points"], a["face_offsets"], a["face_verts"], a["owner"], a["neighbour"], ok[1:])
+    twice = ok + [("dup", "wall", ok[0][2], 1)]
+    with pytest.raises(cf.CfgError, match="in two patches"):
+        cf.PolyMesh(a["points"], a["face_offsets"], a["face_verts"], a["owner"], a["neighbour"], twice)
+    with pytest.raises(cf.CfgError, match="cell counts must be positive"):
+        cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (0, 1, 1))
+    assert nI == 1

@@ -1,0 +1,185 @@
+"""Pins the C restatement in oracle/ (the checker of the GPU tests) to the
+reference: bit-for-bit against the golden fixtures the reference produced,
+and, where the reference driver is built (oracle/_ref), against fresh runs
+of the reference on cases the fixtures do not cover.  CPU only."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import _cases as K
+import _oracle as O
+
+
+def omesh_from_fixture(g):
+    return O.OMesh(g["points"], g["face_offsets"], g["face_verts"], g["owner"], g["neighbour"],
+                   [str(x) for x in g["patch_names"]], [str(x) for x in g["patch_types"]], g["patch_start"],
+                   g["patch_size"])
+
+
+@pytest.mark.parametrize("fixture", ["mesh_block_2x2x2.npz", "mesh_tets22.npz", "mesh_hex41.npz"])
+def test_geometry_matches_reference(golden, fixture):
+    g = golden(fixture)
+    m = omesh_from_fixture(g)
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(getattr(m, k), g[k]), k
+    ow = m.owner_weights()
+    assert np.array_equal(ow, g["ow"])
+    assert np.array_equal(m.skew(ow), g["skew"])
+    assert np.array_equal(m.harmonic_gamma(1e-4), g["gammaHarm"])
+
+
+def test_block_addressing_matches_reference(golden):
+    g = golden("mesh_block_2x2x2.npz")
+    m = O.block_mesh((0, 0, 0), (1, 1, 1), (2, 2, 2))
+    for k in ("face_offsets", "face_verts", "owner", "neighbour", "points"):
+        assert np.array_equal(getattr(m, k), g[k]), k
+    assert list(m.patch_start) == list(g["patch_start"])
+
+
+def test_reference_kernel_unit_facts(golden):
+    """tests/unit/kernelTests.cpp:58-83 on the 2x2x2 block."""
+    g = golden("mesh_block_2x2x2.npz")
+    nP, nC, nF, nInt, nPatch = g["counts"]
+    assert nC == 8 and nInt == 12 and nF - nInt == 24
+    assert abs(g["V"].sum() - 1.0) < 1e-10 and abs(g["V"][0] - 0.125) < 1e-10
+    sums = np.zeros((nC, 3))
+    np.add.at(sums, g["owner"], g["Sf"])
+    np.add.at(sums, g["neighbour"], -g["Sf"][:nInt])
+    assert np.abs(sums).max() < 1e-12
+
+
+@pytest.mark.parametrize("fixture", ["mesh_tets22.npz", "mesh_hex41.npz"])
+def test_gradients_match_reference(golden, fixture):
+    g = golden(fixture)
+    m = omesh_from_fixture(g)
+    for fname in K.POLY_FIELDS:
+        for s in ("linear", "corrected", "leastSquares"):
+            assert np.array_equal(m.grad(g[f"T_{fname}"], g[f"B_{fname}"], s), g[f"grad_fn_{s}_{fname}"])
+            assert np.array_equal(m.grad(g[f"T_{fname}"], g[f"B_{fname}"], s, vol_quirk=True),
+                                  g[f"grad_vol_{s}_{fname}"])
+
+
+def test_reference_gradient_unit_facts(golden):
+    """tests/unit/gradientTests.cpp:92-154 on the oracle's gradients."""
+    g = golden("mesh_tets22.npz")
+    assert int(g["counts"][1]) == 95
+    m = omesh_from_fixture(g)
+    ow = m.owner_weights()
+    nInt = m.nInt
+    co = m.C[m.owner[:nInt]]
+    d = m.d[:nInt]
+    expected = 1.0 - np.clip(np.einsum("ij,ij->i", m.Cf[:nInt] - co, d) / np.einsum("ij,ij->i", d, d), 0, 1)
+    assert np.abs(ow[:nInt] - expected).max() < 1e-15
+    assert np.abs(ow[:nInt] - 0.5).max() > 0.05
+
+    def err(mesh, c, s):
+        t = K.poly(c, mesh.C)
+        b = K.poly(c, mesh.Cf[mesh.nInt:])
+        e = mesh.grad(t, b, s) - K.poly_grad(c, mesh.C)
+        return np.sqrt((e ** 2).sum(1)).max()
+
+    lin, quad = K.POLY_FIELDS["lin"], K.POLY_FIELDS["quad"]
+    assert err(m, lin, "corrected") < 0.5 * err(m, lin, "linear")
+    assert err(m, lin, "leastSquares") < 1e-9
+    assert err(m, quad, "corrected") < 0.5 * err(m, quad, "linear")
+    assert err(m, quad, "leastSquares") < err(m, quad, "corrected")
+    assert err(m, lin, "unheard-of") == err(m, lin, "linear")
+    h = omesh_from_fixture(golden("mesh_hex41.npz"))
+    assert err(h, lin, "linear") < 1e-9 and err(h, lin, "corrected") < 1e-9 and err(h, lin, "leastSquares") < 1e-9
+    assert abs(err(h, quad, "corrected") - err(h, quad, "linear")) < 1e-12
+    assert err(h, quad, "leastSquares") < 1e-9
+
+
+@pytest.mark.parametrize("fixture,builder", [("simple_cavity.npz", "cavity"), ("simple_channel.npz", "channel")])
+def test_simple_matches_reference(golden, fixture, builder):
+    g = golden(fixture)
+    case = K.cavity_case(6, 5, 4) if builder == "cavity" else K.channel_case(10, 6, 5)
+    assert np.array_equal(case.mesh.points, g["points"])
+    U, p, phi, res = case.run()
+    assert res.iterations == int(g["iterations"])
+    for a, k in ((U, "U"), (p, "p"), (phi, "phi")):
+        assert np.array_equal(a, g[k]), k
+
+
+def test_equations_match_reference(golden):
+    g = golden("eqns_cavity.npz")
+    case = K.cavity_case(6, 5, 4)
+    out = case.eqns(g["in_U"], g["in_p"], g["in_phi"], g["in_xprobe"])
+    assert np.array_equal(out["gradPn"], g["gradPn"])
+    for q in range(3):
+        assert np.array_equal(out["U_diag"][q], g[f"U_diag{q}"])
+        assert np.array_equal(out["U_h0"][q], g[f"U_h0_{q}"])
+        assert np.array_equal(out["U_h1"][q], g[f"U_h1_{q}"])
+    for k in ("rAUf", "divPhi", "p_diag", "p_h0", "p_h1", "phiCorrected", "gradPFull"):
+        assert np.array_equal(out[k], g[k]), k
+    assert out["contErr"][0] == g["contErr"][0]
+
+
+@pytest.mark.parametrize("fixture,method", [("solve_cg.npz", "cg"), ("solve_bicgstab.npz", "bicgstab")])
+def test_solvers_match_reference(golden, fixture, method):
+    g = golden(fixture)
+    x, rep = O.solve(method, g["row_start"], g["cols"], g["vals"], g["b"], g["x0"], float(g["tol"]),
+                     int(g["max_iter"]))
+    assert np.array_equal(x, g["x"])
+    assert rep.iterations == int(g["iterations"]) and rep.converged == int(g["converged"])
+
+
+def test_csr_build_merges_duplicates():
+    """finishWithDiagonal: sorted rows and columns, duplicates summed, the
+    diagonal in its column slot (Matrix.cpp:56-117)."""
+    rs, cols, vals = O.csr_from_triplets(3, [2, 0, 0, 1, 0], [0, 2, 2, 2, 1], [1.0, 2.0, 3.0, 4.0, 5.0],
+                                         [10.0, 20.0, 30.0])
+    assert list(rs) == [0, 3, 5, 7]
+    assert list(cols) == [0, 1, 2, 1, 2, 0, 2]
+    assert list(vals) == [10.0, 5.0, 5.0, 20.0, 4.0, 1.0, 30.0]
+
+
+# ---- fresh reference runs on cases the fixtures do not cover -------------
+
+ref = pytest.mark.skipif(not O.have_ref(), reason="reference driver not built (oracle/_ref)")
+
+
+def _variant_dict(text, **repl):
+    for k, v in repl.items():
+        text = text.replace(k, v)
+    return text
+
+
+@ref
+@pytest.mark.parametrize("schemes", [
+    ("upwind", "corrected", "linear"),
+    ("blend", "corrected", "leastSquares"),
+    ("linear", "none", "corrected"),
+])
+def test_simple_variants_match_fresh_reference(schemes):
+    div, lap, grad = schemes
+    case = K.channel_case(9, 5, 4, iters=3, seed=11)
+    case.div, case.laplacian, case.grad = div, lap, grad
+    text = _variant_dict(K.channel_dict(9, 5, 4, iters=3),
+                         **{"div upwind; laplacian corrected; grad corrected;":
+                            f"div {div}; laplacian {lap}; grad {grad}; blendCoeff 0.9;"})
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(text)
+        pp = os.path.join(td, "points.f64")
+        case.mesh.points.tofile(pp)
+        O.ref_run(["simple", cp, td, pp])
+        rU = O.read(os.path.join(td, "U.f64"), shape=(-1, 3))
+        rp = O.read(os.path.join(td, "p.f64"))
+    U, p, phi, res = case.run()
+    assert np.array_equal(U, rU) and np.array_equal(p, rp)
+
+
+@ref
+def test_jitter_and_blockmesh_match_fresh_reference():
+    case = K.cavity_case(7, 6, 5, seed=3)
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(K.cavity_dict(7, 6, 5))
+        r = O.ref_mesh(cp, case.mesh.points)
+    for k in ("face_offsets", "face_verts", "owner", "neighbour"):
+        assert np.array_equal(getattr(case.mesh, k), r[k])
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(getattr(case.mesh, k), r[k]), k
