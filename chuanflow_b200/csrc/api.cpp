@@ -68,6 +68,11 @@ uint64_t splitmix64(uint64_t x)
 
 }  // namespace
 
+namespace cfg
+{
+void setLastError(const std::string& msg) { g_lastError = msg; }
+}  // namespace cfg
+
 extern "C" {
 
 size_t cfg_last_error(char* buf, size_t size)

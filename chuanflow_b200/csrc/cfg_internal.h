@@ -21,6 +21,9 @@ struct Error : std::runtime_error
 
 [[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
 
+/// Sets the calling thread's message for cfg_last_error (api.cpp).
+void setLastError(const std::string& msg);
+
 struct Vec
 {
     double x = 0, y = 0, z = 0;

@@ -244,6 +244,25 @@ int cfg_probe_equations(cfg_ctx* ctx, const cfg_simple_controls* controls, const
 int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t scheme, int32_t vol_quirk,
                  double* out);
 
+/* Jacobi-preconditioned CG on a CSR matrix that is already in device memory,
+ * for callers that cannot let a library allocate: a solver inside a host
+ * framework whose memory manager owns the whole GPU, or one that overlaps
+ * other streams and cannot afford the device-wide synchronisation of
+ * cudaMalloc / cudaFree.  No counterpart in the reference.  The same
+ * algorithm as cfg_sparse_solve's CG; the caller passes device pointers
+ * (row_start n+1 and cols int32, vals, b, x; x holds the initial guess and
+ * receives the solution) and a cudaStream_t (NULL: the default stream), and
+ * this call allocates nothing: its work vectors live in one static device
+ * array of the library, sized for at most 262,144 rows (about 8.5 MB, held
+ * on every GPU that loads the library until the process exits); larger n is
+ * rejected with CFG_EINVAL.  The first call on each device looks that
+ * array's address up, so make it before any stream capture.  Calls share the
+ * array and keep no state between them, but two calls whose work overlaps on
+ * the GPU (different streams or host threads at once) race on it. */
+int cfg_pcg_solve_static(int32_t device, int64_t n, const int32_t* row_start_dev, const int32_t* cols_dev,
+                         const double* vals_dev, const double* b_dev, double* x_dev, double tol, int32_t max_iter,
+                         void* stream, cfg_solver_report* report);
+
 /* ---- case dictionary (the reference's case.dict grammar) ----------------- */
 
 /* Runs a chflow-simple-foam case file end to end (src/3d/apps/simpleFoamApp.cpp:33-209
