@@ -52,7 +52,7 @@ def workload_config(n):
             "precision": "FP64 throughout"}
 
 
-def make_case(n, device):
+def make_case(n, device, precond="Jacobi"):
     import chuanflow_b200 as cf
     mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (n, n, n), {s: (nm, "wall") for s, nm in zip(SIDES, NAMES)})
     mesh.jitter_interior(JITTER, SEED)
@@ -62,7 +62,8 @@ def make_case(n, device):
         case.set_patch_bc("p", nm, "zeroGradient", 0.0)
     case.init_flux()
     ctl = cf.SimpleControls(max_iterations=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02, non_orth_correctors=1,
-                            linear_tol=1e-8, linear_max_iter=2000, nu=NU, p_ref_cell=0, p_ref_value=0.0)
+                            linear_tol=1e-8, linear_max_iter=2000, nu=NU, p_ref_cell=0, p_ref_value=0.0,
+                            p_preconditioner=precond)
     return mesh, case, ctl
 
 
@@ -218,6 +219,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-cells", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--p-precond", default="Jacobi", choices=["Jacobi", "DIC"])
     args = ap.parse_args()
     world, rank, local, dist = dist_setup()
     if args.impl == "reference":
@@ -227,7 +229,7 @@ def main():
         return
 
     n = args.cells
-    mesh, case, ctl = make_case(n, local)
+    mesh, case, ctl = make_case(n, local, args.p_precond)
     ncell = mesh.n_cells
     for _ in range(max(3, args.warmup)):
         case.solve(ctl)
@@ -288,7 +290,7 @@ def main():
     cnt, tot = kstats["cg_spmv"]
     spmv_ms = tot / max(cnt, 1)
     it_ms = sum(kstats[k][1] for k in kstats) / max(cnt, 1)
-    achieved = alg_spmv / (spmv_ms * 1e-3) / 1e9
+    achieved = alg_spmv / (spmv_ms * 1e-3) / 1e9 if cnt else 0.0
     traffic = None
     tp = os.environ.get("CFG_SPMV_TRAFFIC_BYTES")
     if tp:
@@ -298,7 +300,7 @@ def main():
             "peak_source": peak_src, "traffic": traffic,
             "algorithmic_bytes_per_launch": alg_spmv, "launches_timed": cnt, "avg_launch_us": spmv_ms * 1e3,
             "pcg_iteration": {"algorithmic_bytes": alg_iter, "avg_us": it_ms * 1e3,
-                              "achieved_gbs": alg_iter / (it_ms * 1e-3) / 1e9}}
+                              "achieved_gbs": alg_iter / (it_ms * 1e-3) / 1e9 if cnt else 0.0}}
 
     out = {"metric": METRIC, "value": value, "unit": "cell-iter/s", "n_gpus": world, "steps": args.steps,
            "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,

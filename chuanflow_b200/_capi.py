@@ -380,6 +380,14 @@ class SimpleCase:
             res[k] = res[k].reshape(3, N)
         return res
 
+    def probe_dic(self, r):
+        n = self.mesh.n_cells
+        z = np.zeros(n)
+        rd = np.zeros(n)
+        nc = C.c_int32()
+        _check(lib().cfg_probe_dic(self._h, _dp(_f64(r)), _dp(z), _dp(rd), C.byref(nc)))
+        return z, rd, nc.value
+
     def gradient(self, data, bvals, scheme, vol_quirk=False):
         out = np.zeros((self.mesh.n_cells, 3))
         _check(lib().cfg_gradient(self._h, _dp(_f64(data)), _dp(_f64(bvals)), C.c_int32(GRAD.get(scheme, 0)),

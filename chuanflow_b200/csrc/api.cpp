@@ -412,6 +412,15 @@ int cfg_probe_equations(cfg_ctx* ctx, const cfg_simple_controls* ctl, const doub
     });
 }
 
+int cfg_probe_dic(cfg_ctx* ctx, const double* r, double* z, double* rdinv, int32_t* n_colours)
+{
+    return guard([&] {
+        need(ctx && r && z && rdinv, "cfg_probe_dic: null argument");
+        ctx->c->probeDIC(r, z, rdinv);
+        if (n_colours) *n_colours = ctx->c->nColours();
+    });
+}
+
 int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t scheme, int32_t volQuirk, double* out)
 {
     return guard([&] {

@@ -13,22 +13,6 @@
 namespace cfg
 {
 
-/// Device state of one Jacobi-PCG or 3-component BiCGStab solve.
-struct SolveState
-{
-    double tol;
-    int maxIter;
-    int nComp;
-    // per component
-    double bnorm[3], init[3], fin[3];
-    double rho[3], alpha[3], omega[3], beta[3];
-    double rz[3], pAp[3];
-    double sMax[3];
-    int it[3], done[3], conv[3], special[3];
-    int allDone;
-    unsigned int ticket[8];
-};
-
 struct Timing
 {
     cudaEvent_t ev[16];
@@ -56,6 +40,8 @@ public:
     // diagnostics used by the parity tests
     void probeEquations(const cfg_simple_controls& ctl, const double* xprobe, double* out);
     void gradient(const double* data, const double* bvals, int scheme, int volQuirk, double* out);
+    void probeDIC(const double* r, double* z, double* rDinv);
+    int nColours() const { return nColours_; }
 
     /// solveCG / solveBiCGStab on a host CSR (Matrix.cpp:153-319)
     static void sparseSolve(int device, int64_t n, const int64_t* rs, const int64_t* cols, const double* vals,
@@ -88,6 +74,10 @@ private:
     void runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
                   cfg_solver_report* reps);
     void launchCheck(const char* what);
+    void dicSetup(const double* vals, const double* diag);
+    void dicApply(const double* r, double* z);
+    void runDICCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                  cfg_solver_report* rep);
     void setNu(double nu);
     void checkMomentumBcs() const;
 
@@ -126,7 +116,11 @@ private:
     int *dpStart_, *dpSize_, *dpFree_, *dFreeFace_, *dEmptyFace_;
     bool needReference_ = true;
     // solver work
-    double *cr_, *cp_, *cAp_;
+    double *cr_, *cp_, *cAp_, *cz_;
+    // multicolour DIC
+    DDic dic_{};
+    std::vector<DicPhase> dicPhase_;
+    int nColours_ = 0, nLo_ = 0, nUp_ = 0, dicPartials_ = 1;
     V3P br_, br0_, bp_, bv_, bs_, bsh_, bt_, bz_;
     double* partials_;
     SolveState* st_;

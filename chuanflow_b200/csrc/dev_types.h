@@ -73,4 +73,43 @@ struct DMesh
     const int* mCode;
 };
 
+/// Device state of one Jacobi-PCG or 3-component BiCGStab solve.
+struct SolveState
+{
+    double tol;
+    int maxIter;
+    int nComp;
+    // per component
+    double bnorm[3], init[3], fin[3];
+    double rho[3], alpha[3], omega[3], beta[3];
+    double rz[3], pAp[3];
+    double sMax[3];
+    int it[3], done[3], conv[3], special[3];
+    int allDone;
+    unsigned int ticket[8];
+};
+
+/// Multicolour DIC layout (see dic.cuh).
+struct DDic
+{
+    int nColours;
+    const int* rows;      // cells grouped by colour, ascending within a colour
+    const int* lStart;    // lower SELL: slice offsets (all colours, concatenated)
+    const int* lCol;
+    const int* lSrc;      // index of the entry in the main matrix SELL
+    const int* uStart;    // upper SELL
+    const int* uCol;
+    const int* uSrc;
+    double* lVal;
+    double* uVal;
+    double* rD;
+    double* rDinv;
+};
+
+/// one colour: cnt rows starting at rows[off], slices starting at slice0
+struct DicPhase
+{
+    int off, cnt, slice0, partialOff;
+};
+
 }  // namespace cfg

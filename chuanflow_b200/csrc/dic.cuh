@@ -1,0 +1,176 @@
+// Multicolour DIC preconditioner for the pressure PCG (no reference
+// counterpart: the reference's "DICG" is Jacobi-preconditioned CG,
+// src/common/include/cf/common/Matrix.h:65-72).  OpenFOAM's DIC keeps the
+// matrix's off-diagonals and modifies only the diagonal, eliminating in
+// face (owner < neighbour) order, which is sequential.  Here the cells are
+// coloured so that no two neighbours share a colour, and "lower" means "of
+// a smaller colour": every colour is then one parallel phase.
+//   colours: greedy first-fit over cells in ascending order;
+//   factor:  colour by colour, rD_i = ((a_ii - a_ij1^2/rD_j1) - ...) over the
+//            lower neighbours in ascending column order, stored as 1/rD_i;
+//   apply:   forward z_i = rDinv_i (r_i - sum_lower a_ij z_j) colour by
+//            colour, then backward z_i -= rDinv_i sum_upper a_ij z_j over the
+//            colours in reverse, all but the last.
+// Each colour's lower and upper entries sit in their own SELL-32 arrays over
+// that colour's rows, so a phase reads only its own part of the matrix.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace cfg
+{
+
+__global__ void __launch_bounds__(TPB) k_dic_gather(int n, const int* __restrict__ src, const double* __restrict__ val,
+                                                    double* __restrict__ out)
+{
+    ROW_LOOP(e, n) out[e] = src[e] >= 0 ? val[src[e]] : 0.0;
+}
+
+/// rD_i = a_ii - sum a_ij^2 / rD_j over the lower entries, one colour
+__global__ void __launch_bounds__(TPB) k_dic_factor(DDic D, DicPhase ph, const double* __restrict__ diag)
+{
+    FOR_ROWS(t, ph.cnt)
+    {
+        const int i = D.rows[ph.off + t];
+        const int sl = ph.slice0 + (t >> 5), lane = t & 31;
+        double d = diag[i];
+        for (int e = D.lStart[sl] + lane; e < D.lStart[sl + 1]; e += 32)
+        {
+            const int j = D.lCol[e];
+            if (j < 0) break;
+            const double a = D.lVal[e];
+            d = d - a * a / D.rD[j];
+        }
+        D.rD[i] = d;
+        D.rDinv[i] = 1.0 / d;
+    }
+}
+
+/// forward phase of one colour: z_i = rDinv_i (r_i - sum_lower a_ij z_j);
+/// the last colour's rows also contribute their r_i z_i partials
+__global__ void __launch_bounds__(TPB) k_dic_fwd(DDic D, DicPhase ph, const double* __restrict__ r, double* z,
+                                                 int last, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double sm[1] = {0.0};
+    FOR_ROWS(t, ph.cnt)
+    {
+        const int i = D.rows[ph.off + t];
+        const int sl = ph.slice0 + (t >> 5), lane = t & 31;
+        double s = 0.0;
+        for (int e = D.lStart[sl] + lane; e < D.lStart[sl + 1]; e += 32)
+        {
+            const int j = D.lCol[e];
+            if (j < 0) break;
+            s += D.lVal[e] * z[j];
+        }
+        const double ri = r[i];
+        const double zi = D.rDinv[i] * (ri - s);
+        z[i] = zi;
+        sm[0] += ri * zi;
+    }
+    if (!last) return;
+    block_sum<1>(sm);
+    if (threadIdx.x == 0) partials[ph.partialOff + blockIdx.x] = sm[0];
+}
+
+/// backward phase of one colour: z_i -= rDinv_i sum_upper a_ij z_j, with
+/// the r_i z_i partials; `final` (the phase that runs last) also reduces
+/// all colours' partials into r.z and advances beta
+__global__ void __launch_bounds__(TPB) k_dic_bwd(DDic D, DicPhase ph, const double* __restrict__ r, double* z,
+                                                 int final, int nPartials, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double sm[1] = {0.0};
+    FOR_ROWS(t, ph.cnt)
+    {
+        const int i = D.rows[ph.off + t];
+        const int sl = ph.slice0 + (t >> 5), lane = t & 31;
+        double s = 0.0;
+        for (int e = D.uStart[sl] + lane; e < D.uStart[sl + 1]; e += 32)
+        {
+            const int j = D.uCol[e];
+            if (j < 0) break;
+            s += D.uVal[e] * z[j];
+        }
+        const double zi = z[i] - D.rDinv[i] * s;
+        z[i] = zi;
+        sm[0] += r[i] * zi;
+    }
+    block_sum<1>(sm);
+    if (threadIdx.x == 0) partials[ph.partialOff + blockIdx.x] = sm[0];
+    if (!final) return;
+    if (!last_block(&st->ticket[0])) return;
+    double fs[1];
+    final_sum<1>(partials, nPartials, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        const double rzNew = fs[0];
+        // the first application (it == 0) sets p = z: beta 0 with p = 0
+        st->beta[0] = st->it[0] == 0 ? 0.0 : rzNew / st->rz[0];
+        st->rz[0] = rzNew;
+    }
+}
+
+/// x += alpha p; r -= alpha Ap; |r|inf test (Matrix.cpp:195-208), without z
+static __global__ void __launch_bounds__(TPB) k_cg_update_nz(int n, const double* __restrict__ p,
+                                                             const double* __restrict__ Ap, double* __restrict__ x,
+                                                             double* __restrict__ r, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    const double alpha = st->alpha[0];
+    double mx[2] = {0.0, 0.0};
+    FOR_ROWS(c, n)
+    {
+        x[c] = x[c] + alpha * p[c];
+        const double ri = r[c] - alpha * Ap[c];
+        r[c] = ri;
+        if (isnan(ri)) mx[1] = 1.0;
+        mx[0] = smax(mx[0], fabs(ri));
+    }
+    block_max<2>(mx);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = mx[0];
+        partials[G + blockIdx.x] = mx[1];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double fm[2];
+    final_max<2>(partials, G, fm);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        const int it = st->it[0] + 1;
+        st->it[0] = it;
+        const double fin = fm[1] > 0 ? NAN : fm[0];
+        st->fin[0] = fin;
+        if (fin / st->bnorm[0] < st->tol)
+        {
+            st->conv[0] = 1;
+            st->done[0] = 1;
+        }
+        else if (isnan(fin))
+        {
+            st->it[0] = st->maxIter;
+            st->done[0] = 1;
+        }
+        else if (it >= st->maxIter)
+        {
+            st->done[0] = 1;
+        }
+        st->allDone = st->done[0];
+    }
+}
+
+/// p = z + beta p
+static __global__ void __launch_bounds__(TPB) k_cg_pz(int n, const double* __restrict__ z, double* __restrict__ p,
+                                                      const SolveState* st)
+{
+    if (st->allDone) return;
+    const double beta = st->beta[0];
+    FOR_ROWS(c, n) p[c] = z[c] + beta * p[c];
+}
+
+}  // namespace cfg

@@ -9,6 +9,7 @@
 #include "ctx.h"
 #include "kernels.cuh"
 #include "solvers.cuh"
+#include "dic.cuh"
 
 namespace cfg
 {
@@ -726,6 +727,100 @@ void Ctx::buildDevice()
         }
     }
 
+    // ---- multicolour DIC layouts (dic.cuh) ----
+    {
+        std::vector<int> colour(nC, -1), mark(nC + 2, -1);
+        int nCol = 0;
+        for (int c = 0; c < nC; ++c)
+        {
+            const int s0 = c >> 5, l0 = c & 31;
+            for (int k = 0;; ++k)
+            {
+                const int e = mStart[s0] + 32 * k + l0;
+                if (e >= mStart[s0 + 1] || mCol[e] < 0) break;
+                const int j = mCol[e];
+                if (j != c && colour[j] >= 0) mark[colour[j]] = c;
+            }
+            int col = 0;
+            while (mark[col] == c) ++col;
+            colour[c] = col;
+            nCol = std::max(nCol, col + 1);
+        }
+        nColours_ = nCol;
+        std::vector<int> rows;
+        std::vector<int> lStart{0}, uStart{0}, lCol, lSrc, uCol, uSrc;
+        dicPhase_.clear();
+        int slice = 0, pOff = 0;
+        for (int col = 0; col < nCol; ++col)
+        {
+            DicPhase ph{static_cast<int>(rows.size()), 0, slice, pOff};
+            for (int c = 0; c < nC; ++c)
+                if (colour[c] == col) rows.push_back(c);
+            ph.cnt = static_cast<int>(rows.size()) - ph.off;
+            const int nSl = (ph.cnt + 31) / 32;
+            for (int sl = 0; sl < nSl; ++sl)
+            {
+                std::vector<std::vector<std::pair<int, int>>> lo(32), up(32);
+                int wl = 0, wu = 0;
+                for (int l = 0; l < 32; ++l)
+                {
+                    const int t = 32 * sl + l;
+                    if (t >= ph.cnt) break;
+                    const int c = rows[ph.off + t];
+                    const int s0 = c >> 5, l0 = c & 31;
+                    for (int k = 0;; ++k)
+                    {
+                        const int e = mStart[s0] + 32 * k + l0;
+                        if (e >= mStart[s0 + 1] || mCol[e] < 0) break;
+                        const int j = mCol[e];
+                        if (j == c) continue;
+                        (colour[j] < col ? lo : up)[l].push_back({j, e});
+                    }
+                    wl = std::max(wl, static_cast<int>(lo[l].size()));
+                    wu = std::max(wu, static_cast<int>(up[l].size()));
+                }
+                const size_t lb = lCol.size(), ub = uCol.size();
+                lCol.resize(lb + 32 * wl, -1);
+                lSrc.resize(lb + 32 * wl, -1);
+                uCol.resize(ub + 32 * wu, -1);
+                uSrc.resize(ub + 32 * wu, -1);
+                for (int l = 0; l < 32; ++l)
+                {
+                    for (size_t k = 0; k < lo[l].size(); ++k)
+                    {
+                        lCol[lb + 32 * k + l] = lo[l][k].first;
+                        lSrc[lb + 32 * k + l] = lo[l][k].second;
+                    }
+                    for (size_t k = 0; k < up[l].size(); ++k)
+                    {
+                        uCol[ub + 32 * k + l] = up[l][k].first;
+                        uSrc[ub + 32 * k + l] = up[l][k].second;
+                    }
+                }
+                lStart.push_back(static_cast<int>(lCol.size()));
+                uStart.push_back(static_cast<int>(uCol.size()));
+            }
+            slice += nSl;
+            pOff += std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB));
+            dicPhase_.push_back(ph);
+        }
+        dicPartials_ = pOff + 1;
+        dic_.nColours = nCol;
+        dic_.rows = upload(rows);
+        dic_.lStart = upload(lStart);
+        dic_.lCol = upload(lCol);
+        dic_.lSrc = upload(lSrc);
+        dic_.uStart = upload(uStart);
+        dic_.uCol = upload(uCol);
+        dic_.uSrc = upload(uSrc);
+        dic_.lVal = alloc<double>(lCol.size());
+        dic_.uVal = alloc<double>(uCol.size());
+        dic_.rD = alloc<double>(nC);
+        dic_.rDinv = alloc<double>(nC);
+        nLo_ = static_cast<int>(lCol.size());
+        nUp_ = static_cast<int>(uCol.size());
+    }
+
     d.own = upload(own);
     d.nbr = upload(nbr);
     d.sfx = upload(sfx);
@@ -796,6 +891,7 @@ void Ctx::buildDevice()
     cr_ = alloc<double>(nC);
     cp_ = alloc<double>(nC);
     cAp_ = alloc<double>(nC);
+    cz_ = alloc<double>(nC);
     v3(br_, nC);
     v3(br0_, nC);
     v3(bp_, nC);
@@ -820,7 +916,7 @@ void Ctx::buildDevice()
         dFreeFace_ = alloc<int>(nB);
         dEmptyFace_ = alloc<int>(nB);
     }
-    partials_ = alloc<double>(static_cast<size_t>(16) * std::max(std::max(G_, GF_), GS_));
+    partials_ = alloc<double>(static_cast<size_t>(16) * std::max(std::max(std::max(G_, GF_), GS_), dicPartials_));
     st_ = alloc<SolveState>(1);
     scal_ = alloc<double>(S_COUNT);
     CFG_CUDA(cudaMallocHost(&stHost_, sizeof(SolveState)));
@@ -1230,6 +1326,90 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     }
 }
 
+void Ctx::dicSetup(const double* vals, const double* diag)
+{
+    k_dic_gather<<<std::max(1, std::min((nLo_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nLo_, dic_.lSrc, vals,
+                                                                                           dic_.lVal);
+    k_dic_gather<<<std::max(1, std::min((nUp_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nUp_, dic_.uSrc, vals,
+                                                                                           dic_.uVal);
+    launchCheck("dic_gather");
+    for (const DicPhase& ph : dicPhase_)
+    {
+        k_dic_factor<<<std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)), TPB, 0, stream_>>>(dic_, ph, diag);
+        launchCheck("dic_factor");
+    }
+}
+
+void Ctx::dicApply(const double* r, double* z)
+{
+    const int C = dic_.nColours;
+    for (int c = 0; c < C; ++c)
+    {
+        const DicPhase& ph = dicPhase_[c];
+        k_dic_fwd<<<std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)), TPB, 0, stream_>>>(dic_, ph, r, z, c == C - 1,
+                                                                                           partials_, st_);
+    }
+    if (C == 1)
+    {
+        // no backward phase: a one-block final reduction of the forward partials
+        const DicPhase none{0, 0, 0, dicPartials_ - 1};
+        k_dic_bwd<<<1, TPB, 0, stream_>>>(dic_, none, r, z, 1, dicPartials_, partials_, st_);
+    }
+    for (int c = C - 2; c >= 0; --c)
+    {
+        const DicPhase& ph = dicPhase_[c];
+        k_dic_bwd<<<std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)), TPB, 0, stream_>>>(
+            dic_, ph, r, z, c == 0, c == 0 ? dicPartials_ - 1 : 0, partials_, st_);
+    }
+    launches_ += 2 * C;
+    launchCheck("dic_apply");
+}
+
+/// PCG of Matrix.cpp:153-222 with z = M^-1 r from the multicolour DIC.
+void Ctx::runDICCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                   cfg_solver_report* rep)
+{
+    const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
+    SolveState init{};
+    init.tol = tol;
+    init.maxIter = maxIter;
+    init.nComp = 1;
+    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    dicSetup(vals, diag);
+    dispatchW(maxW_, [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        k_cg_init<W><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
+        launchCheck("cg_init");
+        dicApply(cr_, cz_);
+        k_cg_pz<<<GS_, TPB, 0, stream_>>>(dm_.nC, cz_, cp_, st_);
+        launchCheck("cg_pz");
+        int launched = 0;
+        int chunk = 8;
+        for (;;)
+        {
+            CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+            if (stHost_->allDone || launched >= maxIter) break;
+            const int n = std::min(chunk, maxIter - launched);
+            for (int k = 0; k < n; ++k)
+            {
+                k_cg_spmv<W><<<GS_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
+                k_cg_update_nz<<<GS_, TPB, 0, stream_>>>(dm_.nC, cp_, cAp_, x, cr_, partials_, st_);
+                dicApply(cr_, cz_);
+                k_cg_pz<<<GS_, TPB, 0, stream_>>>(dm_.nC, cz_, cp_, st_);
+                launches_ += 3;
+                launchCheck("dic_cg_iter");
+            }
+            launched += n;
+            chunk = std::min(chunk * 2, 64);
+        }
+    });
+    rep->iterations = stHost_->it[0];
+    rep->converged = stHost_->conv[0];
+    rep->initial_residual = stHost_->init[0];
+    rep->final_residual = stHost_->conv[0] && stHost_->it[0] == 0 ? stHost_->init[0] : stHost_->fin[0];
+}
+
 /// fvMatrix::solve for the momentum equation (fvMatrix.cpp:73-129): x from
 /// zero, nonOrth+1 passes when the laplacian is corrected, each restoring the
 /// base rhs and adding the corrector evaluated on the current x.
@@ -1325,7 +1505,6 @@ void Ctx::checkMomentumBcs() const
 
 void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner)
 {
-    (void)precond;
     const int n = dm_.nC;
     CFG_CUDA(cudaMemsetAsync(px_, 0, n * sizeof(double), stream_));
     const bool corr = schemes_.laplacian_corrected != 0;
@@ -1347,7 +1526,8 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
             CFG_CUDA(cudaMemcpyAsync(pRhs_, pBase_, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
         }
         cfg_solver_report rep;
-        runCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
+        if (precond == CFG_PRECOND_DIC) runDICCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
+        else runCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
         inner += rep.iterations;
     }
 }
@@ -1635,6 +1815,23 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
                                              fScratch_);
     launchCheck("correct_flux");
     d2h(fScratch_, nF);
+}
+
+void Ctx::probeDIC(const double* r, double* z, double* rDinv)
+{
+    // the DIC of the pressure matrix last assembled (by probeEquations or an
+    // outer iteration): factor, then one application to r
+    CFG_CUDA(cudaSetDevice(device_));
+    const int nC = dm_.nC;
+    SolveState init{};
+    init.maxIter = 1;
+    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    dicSetup(pVal_d_, pDiag_);
+    CFG_CUDA(cudaMemcpyAsync(cr_, r, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    dicApply(cr_, cz_);
+    CFG_CUDA(cudaMemcpyAsync(z, cz_, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaMemcpyAsync(rDinv, dic_.rDinv, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQuirk, double* out)

@@ -238,6 +238,11 @@ int cfg_sparse_solve(const cfg_ctx* ctx_or_null, int32_t device, int64_t n, cons
  * xprobe as the solved pressure (F).  Vector blocks are component-major. */
 int cfg_probe_equations(cfg_ctx* ctx, const cfg_simple_controls* controls, const double* xprobe, double* out);
 
+/* The multicolour DIC of the pressure matrix last assembled in the context
+ * (by cfg_probe_equations or an outer iteration): its factor (1/rD per cell)
+ * and one application z = M^-1 r, and the number of colours. */
+int cfg_probe_dic(cfg_ctx* ctx, const double* r, double* z, double* rdinv, int32_t* n_colours);
+
 /* fvc::grad of a cell field with fixed boundary face values bvals[f - nInternal]
  * (gradScheme.cpp:246-277); vol_quirk 1 selects the volScalarField overload's
  * internal face value for the linear scheme.  out: nCells*3. */

@@ -933,6 +933,7 @@ typedef struct
     int64_t* tc;
     double* tv;    /* nComp * capTrip */
     int preferCG;
+    int useDIC; /* pressure: multicolour-DIC PCG instead of Jacobi */
     /* the laplacian corrector (laplacianScheme.cpp:217-263), if registered */
     int hasCorrector;
     double* corrGamma; /* nF */
@@ -1123,6 +1124,8 @@ static void fvmat_build_csr(fvmat* e)
 
 /* fvMatrix::solve (fvMatrix.cpp:73-129), relaxation 1 */
 static int64_t g_innerSum;
+int cfo_solve_dic_cg(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const double* b, double* x,
+                     double tol, int32_t maxIter, cfo_report* rep);
 
 static cfo_report fvmat_solve(fvmat* e, const geo_ctx* g, double tol, int maxIter, int nonOrth, int gradScheme)
 {
@@ -1140,7 +1143,10 @@ static cfo_report fvmat_solve(fvmat* e, const geo_ctx* g, double tol, int maxIte
         for (int q = 0; q < e->nComp; ++q)
         {
             cfo_report rep;
-            if (e->preferCG)
+            if (e->preferCG && e->useDIC)
+                cfo_solve_dic_cg(n, e->rs, e->cols, e->vals + q * e->nnz, e->rhs + q * n, e->x + q * n, tol, maxIter,
+                                 &rep);
+            else if (e->preferCG)
                 cfo_solve_cg(n, e->rs, e->cols, e->vals + q * e->nnz, e->rhs + q * n, e->x + q * n, tol, maxIter, &rep);
             else
                 cfo_solve_bicgstab(n, e->rs, e->cols, e->vals + q * e->nnz, e->rhs + q * n, e->x + q * n, tol,
@@ -1376,6 +1382,7 @@ static void build_peqn(fvmat* P, const simple_ws* w, const cfo_controls* ctl, co
     memcpy(P->bc_k, pk, sizeof(double) * (size_t)nB);
     fvm_laplacian(P, &w->g, rAUf, ctl->laplacianCorrected, -1);
     for (int64_t c = 0; c < m->nC; ++c) P->rhs[c] += -dphi[c];
+    P->useDIC = ctl->pPrecond == 1;
     if (ctl->pRefCell >= 0 && ctl->pRefCell < m->nC)
     {
         const int64_t r = ctl->pRefCell;
@@ -1600,4 +1607,179 @@ out:
     free(uc); free(uk); free(pc); free(pk); free(zero); free(rAUr);
     ws_free(&w);
     return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Multicolour DIC preconditioner (no reference counterpart; the reference's */
+/* "DICG" stand-in is Jacobi, src/common/include/cf/common/Matrix.h:65-72).  */
+/* Restates the definition chuanflow_b200 implements so its device result   */
+/* can be checked bit-for-bit:                                               */
+/*   colours: greedy first-fit over cells in ascending order, the smallest   */
+/*            colour not used by an already-coloured neighbour;              */
+/*   lower(i): off-diagonal entries of row i whose column has a smaller      */
+/*            colour, in ascending column order; upper(i) likewise larger;   */
+/*   factor:  colour by colour ascending, rD_i = ((a_ii - t_1) - t_2) ...,   */
+/*            t_k = a_ij^2 / rD_j over lower(i), stored as 1 / rD_i;         */
+/*   apply:   forward colour by colour, z_i = rDinv_i (r_i - sum a_ij z_j)   */
+/*            over lower(i); backward colours descending (all but the last), */
+/*            z_i = z_i - rDinv_i (sum a_ij z_j) over upper(i).              */
+/* ------------------------------------------------------------------------ */
+
+int cfo_colour_cells(int64_t n, const int64_t* rs, const int64_t* cols, int32_t* colour)
+{
+    int32_t* mark = (int32_t*)xcalloc((size_t)(n + 2), sizeof(int32_t));
+    for (int64_t i = 0; i < n; ++i) colour[i] = -1;
+    int32_t nColours = 0;
+    for (int64_t i = 0; i < n; ++i)
+    {
+        for (int64_t k = rs[i]; k < rs[i + 1]; ++k)
+        {
+            const int64_t j = cols[k];
+            if (j != i && colour[j] >= 0) mark[colour[j]] = (int32_t)(i + 1);
+        }
+        int32_t c = 0;
+        while (mark[c] == (int32_t)(i + 1)) ++c;
+        colour[i] = c;
+        if (c + 1 > nColours) nColours = c + 1;
+    }
+    free(mark);
+    return nColours;
+}
+
+int cfo_dic_factor(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const int32_t* colour,
+                   int32_t nColours, double* rDinv)
+{
+    double* rD = (double*)xcalloc((size_t)n, sizeof(double));
+    for (int32_t c = 0; c < nColours; ++c)
+        for (int64_t i = 0; i < n; ++i)
+        {
+            if (colour[i] != c) continue;
+            double d = 0;
+            for (int64_t k = rs[i]; k < rs[i + 1]; ++k)
+                if (cols[k] == i) { d = vals[k]; break; }
+            for (int64_t k = rs[i]; k < rs[i + 1]; ++k)
+            {
+                const int64_t j = cols[k];
+                if (j != i && colour[j] < c) d = d - vals[k] * vals[k] / rD[j];
+            }
+            rD[i] = d;
+            rDinv[i] = 1.0 / d;
+        }
+    free(rD);
+    return 0;
+}
+
+void cfo_dic_apply(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const int32_t* colour,
+                   int32_t nColours, const double* rDinv, const double* r, double* z)
+{
+    for (int32_t c = 0; c < nColours; ++c)
+        for (int64_t i = 0; i < n; ++i)
+        {
+            if (colour[i] != c) continue;
+            double s = 0;
+            for (int64_t k = rs[i]; k < rs[i + 1]; ++k)
+            {
+                const int64_t j = cols[k];
+                if (j != i && colour[j] < c) s += vals[k] * z[j];
+            }
+            z[i] = rDinv[i] * (r[i] - s);
+        }
+    for (int32_t c = nColours - 2; c >= 0; --c)
+        for (int64_t i = 0; i < n; ++i)
+        {
+            if (colour[i] != c) continue;
+            double s = 0;
+            for (int64_t k = rs[i]; k < rs[i + 1]; ++k)
+            {
+                const int64_t j = cols[k];
+                if (j != i && colour[j] > c) s += vals[k] * z[j];
+            }
+            z[i] = z[i] - rDinv[i] * s;
+        }
+}
+
+/* PCG of Matrix.cpp:153-222 with z = M^-1 r from the multicolour DIC */
+int cfo_solve_dic_cg(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const double* b, double* x,
+                     double tol, int32_t maxIter, cfo_report* rep)
+{
+    int32_t* colour = (int32_t*)xcalloc((size_t)n, sizeof(int32_t));
+    const int32_t nc = cfo_colour_cells(n, rs, cols, colour);
+    double* rDinv = (double*)xcalloc((size_t)n, sizeof(double));
+    cfo_dic_factor(n, rs, cols, vals, colour, nc, rDinv);
+    double* Ax = (double*)xcalloc((size_t)n, sizeof(double));
+    double* r = (double*)xcalloc((size_t)n, sizeof(double));
+    double* z = (double*)xcalloc((size_t)n, sizeof(double));
+    double* p = (double*)xcalloc((size_t)n, sizeof(double));
+    double* Ap = (double*)xcalloc((size_t)n, sizeof(double));
+    cfo_spmv(n, rs, cols, vals, x, Ax);
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - Ax[i];
+    memset(rep, 0, sizeof *rep);
+    rep->initialResidual = inf_norm(n, r);
+    const double bnorm = smax(inf_norm(n, b), 1e-300);
+    if (rep->initialResidual / bnorm < tol)
+    {
+        rep->converged = 1;
+        rep->finalResidual = rep->initialResidual;
+        goto done;
+    }
+    cfo_dic_apply(n, rs, cols, vals, colour, nc, rDinv, r, z);
+    memcpy(p, z, sizeof(double) * (size_t)n);
+    double rz = sdot(n, r, z);
+    for (int it = 1; it <= maxIter; ++it)
+    {
+        cfo_spmv(n, rs, cols, vals, p, Ap);
+        const double pAp = sdot(n, p, Ap);
+        if (pAp <= 0 || fabs(rz) < 1e-300) break;
+        const double alpha = rz / pAp;
+        for (int64_t i = 0; i < n; ++i)
+        {
+            x[i] += alpha * p[i];
+            r[i] -= alpha * Ap[i];
+        }
+        rep->iterations = it;
+        rep->finalResidual = inf_norm(n, r);
+        if (rep->finalResidual / bnorm < tol)
+        {
+            rep->converged = 1;
+            break;
+        }
+        cfo_dic_apply(n, rs, cols, vals, colour, nc, rDinv, r, z);
+        const double rzNew = sdot(n, r, z);
+        const double beta = rzNew / rz;
+        rz = rzNew;
+        for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    }
+done:
+    free(colour); free(rDinv); free(Ax); free(r); free(z); free(p); free(Ap);
+    return 0;
+}
+
+/* The pressure matrix of one outer iteration for a given rAUf: the static
+ * part of fvm::laplacianFace (laplacianScheme.cpp:176-215, sign -1) with the
+ * optional reference cell, as CSR (Matrix.cpp:56-117).  rs: nC+1, cols and
+ * vals: room for nC + 2 nInt entries; returns nnz. */
+int64_t cfo_pressure_csr(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, const double* rAUf,
+                         int64_t* rs, int64_t* cols, double* vals)
+{
+    simple_ws w;
+    ws_init(&w, m, ctl->nu);
+    const int64_t nB = m->nF - m->nInt;
+    double* pc = (double*)xcalloc((size_t)nB, sizeof(double));
+    double* pk = (double*)xcalloc((size_t)nB, sizeof(double));
+    double* zero = (double*)xcalloc((size_t)m->nC, sizeof(double));
+    int64_t nnz = -1;
+    if (p_lin_table(m, &w, bc->pType, bc->pValue, pc, pk) == 0)
+    {
+        fvmat P;
+        build_peqn(&P, &w, ctl, pc, pk, rAUf, zero);
+        fvmat_build_csr(&P);
+        nnz = P.nnz;
+        memcpy(rs, P.rs, sizeof(int64_t) * (size_t)(m->nC + 1));
+        memcpy(cols, P.cols, sizeof(int64_t) * (size_t)nnz);
+        memcpy(vals, P.vals, sizeof(double) * (size_t)nnz);
+        fvmat_free(&P);
+    }
+    free(pc); free(pk); free(zero);
+    ws_free(&w);
+    return nnz;
 }

@@ -95,6 +95,8 @@ typedef struct cfo_controls
      * then diag += diag.  No counterpart in the reference. */
     int64_t pRefCell;
     double pRefValue;
+    /* pressure preconditioner: 0 Jacobi (the reference), 1 multicolour DIC */
+    int32_t pPrecond;
 } cfo_controls;
 
 typedef struct cfo_result
@@ -149,6 +151,16 @@ int cfo_solve_cg(int64_t n, const int64_t* rowStart, const int64_t* cols, const 
 int cfo_solve_bicgstab(int64_t n, const int64_t* rowStart, const int64_t* cols, const double* vals,
                        const double* b, double* x, double tol, int32_t maxIter, cfo_report* rep);
 
+/* Multicolour DIC (no reference counterpart): greedy colouring, factor,
+ * apply, and the PCG using it; see the definitions in cfo.c. */
+int cfo_colour_cells(int64_t n, const int64_t* rs, const int64_t* cols, int32_t* colour);
+int cfo_dic_factor(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const int32_t* colour,
+                   int32_t nColours, double* rDinv);
+void cfo_dic_apply(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const int32_t* colour,
+                   int32_t nColours, const double* rDinv, const double* r, double* z);
+int cfo_solve_dic_cg(int64_t n, const int64_t* rs, const int64_t* cols, const double* vals, const double* b,
+                     double* x, double tol, int32_t maxIter, cfo_report* rep);
+
 /* solveIncompressibleSimple (simpleSolver.cpp:33-394), laminar, steady.
  * U (nC*3), p (nC), phi (nF) are updated in place. */
 int cfo_simple(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, double* U, double* p,
@@ -164,6 +176,11 @@ int cfo_eqns(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, cons
 /* updatePhiInternal + correctBoundaryFlux (pressureCorrection.cpp:10-25,
  * volFields.cpp:294-306) */
 int cfo_flux_from_U(const cfo_mesh* m, const cfo_bcs* bc, const double* U, double* phi);
+
+/* The pressure matrix (static laplacianFace part + reference cell) for a
+ * given rAUf, as CSR; returns nnz. */
+int64_t cfo_pressure_csr(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, const double* rAUf,
+                         int64_t* rs, int64_t* cols, double* vals);
 
 const char* cfo_last_error(void);
 

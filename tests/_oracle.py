@@ -52,7 +52,7 @@ class Controls(C.Structure):
                 ("pRelaxStart", C.c_double), ("bodyForce", C.c_double * 3), ("nu", C.c_double),
                 ("div", C.c_int32), ("laplacianCorrected", C.c_int32), ("grad", C.c_int32),
                 ("blendCoeff", C.c_double), ("verbose", C.c_int32), ("pRefCell", C.c_int64),
-                ("pRefValue", C.c_double)]
+                ("pRefValue", C.c_double), ("pPrecond", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -204,6 +204,7 @@ class Case:
     u_face_values: dict = None
     p_ref_cell: int = -1
     p_ref_value: float = 0.0
+    p_precond: int = 0
 
     def controls(self, verbose=False):
         c = Controls()
@@ -227,6 +228,7 @@ class Case:
         c.verbose = int(verbose)
         c.pRefCell = self.p_ref_cell
         c.pRefValue = self.p_ref_value
+        c.pPrecond = self.p_precond
         return c
 
     def bcs(self):
@@ -264,6 +266,21 @@ class Case:
         _check(lib().cfo_simple(C.byref(m._c), C.byref(b), C.byref(ctl), _p(U), _p(p), _p(phi), C.byref(res)))
         return U, p, phi, res
 
+    def pressure_csr(self, rAUf):
+        m = self.mesh
+        rs = np.zeros(m.nC + 1, np.int64)
+        cols = np.zeros(m.nC + 2 * m.nInt, np.int64)
+        vals = np.zeros(m.nC + 2 * m.nInt)
+        b = self.bcs()
+        ctl = self.controls()
+        lib().cfo_pressure_csr.restype = C.c_int64
+        nnz = lib().cfo_pressure_csr(C.byref(m._c), C.byref(b), C.byref(ctl),
+                                     _p(np.ascontiguousarray(rAUf, np.float64)), _p(rs, _i64p), _p(cols, _i64p),
+                                     _p(vals))
+        if nnz < 0:
+            raise RuntimeError(lib().cfo_last_error().decode())
+        return rs, cols[:nnz].copy(), vals[:nnz].copy()
+
     def eqns(self, U, p, phi, xprobe):
         m = self.mesh
         nC, nF = m.nC, m.nF
@@ -297,10 +314,31 @@ def csr_from_triplets(n, rows, cols, vals, diag):
 def solve(method, rs, cols, vals, b, x0, tol, max_iter):
     x = np.array(x0, np.float64, copy=True)
     rep = Report()
-    fn = lib().cfo_solve_cg if method == "cg" else lib().cfo_solve_bicgstab
+    fn = {"cg": lib().cfo_solve_cg, "bicgstab": lib().cfo_solve_bicgstab, "dic": lib().cfo_solve_dic_cg}[method]
     _check(fn(C.c_int64(rs.size - 1), _p(rs, _i64p), _p(cols, _i64p), _p(vals),
               _p(np.ascontiguousarray(b, np.float64)), _p(x), C.c_double(tol), C.c_int32(max_iter), C.byref(rep)))
     return x, rep
+
+
+def dic(rs, cols, vals):
+    """Colouring and DIC factor of a CSR matrix; returns (colour, nColours, rDinv, apply)."""
+    rs = np.ascontiguousarray(rs, np.int64)
+    cols = np.ascontiguousarray(cols, np.int64)
+    vals = np.ascontiguousarray(vals, np.float64)
+    n = rs.size - 1
+    colour = np.zeros(n, np.int32)
+    nc = lib().cfo_colour_cells(C.c_int64(n), _p(rs, _i64p), _p(cols, _i64p), colour.ctypes.data_as(C.POINTER(C.c_int32)))
+    rDinv = np.zeros(n)
+    lib().cfo_dic_factor(C.c_int64(n), _p(rs, _i64p), _p(cols, _i64p), _p(vals),
+                         colour.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int32(nc), _p(rDinv))
+
+    def apply(r):
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros(n)
+        lib().cfo_dic_apply(C.c_int64(n), _p(rs, _i64p), _p(cols, _i64p), _p(vals),
+                            colour.ctypes.data_as(C.POINTER(C.c_int32)), C.c_int32(nc), _p(rDinv), _p(r), _p(z))
+        return z
+    return colour, nc, rDinv, apply
 
 
 # --------------------------------------------------------------------------

@@ -103,3 +103,34 @@ def test_sparse_solvers_match_reference(golden, fixture, method):
     assert abs(rep.iterations - int(g["iterations"])) <= 1
     assert rel(x, g["x"]) < 1e-9
     assert rep.initial_residual == float(g["initial"])
+
+
+def test_dic_factor_and_apply_bit_exact(golden):
+    """The multicolour DIC of the device pressure matrix equals the oracle's
+    restatement of the same definition (oracle/cfo.c) on the same matrix."""
+    g = golden("eqns_cavity.npz")
+    mesh, case = K.cavity_product(6, 5, 4)
+    case.upload(g["in_U"], g["in_p"], g["in_phi"])
+    oc = K.cavity_case(6, 5, 4)
+    out = case.probe_equations(K.controls_from(oc), g["in_xprobe"])
+    rs, cols, vals = oc.pressure_csr(out["rAUf"])
+    colour, nc, rdinv, apply = O.dic(rs, cols, vals)
+    r = np.random.default_rng(3).normal(size=mesh.n_cells)
+    z, rd, ncol = case.probe_dic(r)
+    assert ncol == nc == 2
+    assert np.array_equal(rd, rdinv)
+    assert np.array_equal(z, apply(r))
+
+
+@pytest.mark.parametrize("cells,jitter", [((12, 12, 12), 0.1), ((9, 7, 5), 0.0)])
+def test_simple_cavity_dic_matches_oracle(cells, jitter):
+    oc = K.cavity_case(*cells, jitter=jitter, iters=6, linear_tol=1e-10, nu=0.0025)
+    oc.p_ref_cell = 0
+    oc.p_precond = 1
+    U0, p0, phi0, r0 = oc.run()
+    mesh, case = K.cavity_product(*cells, jitter=jitter)
+    res = case.solve(K.controls_from(oc, p_preconditioner="DIC"))
+    U, p, phi = case.download()
+    assert res.iterations == r0.iterations
+    assert abs(res.p_inner_iterations - r0.pItersTotal) <= 2 * 6 * 2
+    assert rel(U, U0) < REL_TOL and rel(p, p0) < REL_TOL and rel(phi, phi0) < REL_TOL
