@@ -49,6 +49,14 @@ class _Result(C.Structure):
                 ("p_inner_iterations", C.c_int64), ("diverged", C.c_int32)]
 
 
+class _PoissonReport(C.Structure):
+    _fields_ = [("inner_iterations", C.c_int64), ("outer_iterations", C.c_int32), ("converged", C.c_int32),
+                ("true_rel_residual", C.c_double), ("device_ms", C.c_double), ("initial_rel_residual", C.c_double)]
+
+
+POISSON = {"jacobi64": 0, "dic64": 1, "ir32": 2}
+
+
 class _Report(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("initial_residual", C.c_double),
                 ("final_residual", C.c_double)]
@@ -138,6 +146,22 @@ class PolyMesh:
         h = C.c_void_p()
         _check(lib().cfg_mesh_block(_dp(mn), _dp(mx), C.c_int64(cells[0]), C.c_int64(cells[1]),
                                     C.c_int64(cells[2]), names, types, C.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self._counts()
+        return self
+
+    @classmethod
+    def from_cells(cls, points, cell_types, cell_offsets, cell_verts):
+        """The polyMesh the reference's gmsh reader builds from these volume
+        cells (4 tet, 5 hex, 6 prism; patches named after bounding-box planes)."""
+        pts = _f64(points).reshape(-1, 3)
+        ty = np.ascontiguousarray(cell_types, np.int32)
+        off = np.ascontiguousarray(cell_offsets, np.int64)
+        cv = np.ascontiguousarray(cell_verts, np.int64)
+        h = C.c_void_p()
+        _check(lib().cfg_mesh_from_cells(_dp(pts), C.c_int64(pts.shape[0]), ty.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         _ip(off), _ip(cv), C.c_int64(ty.size), C.byref(h)))
         self = cls.__new__(cls)
         self._h = h
         self._counts()
@@ -360,6 +384,23 @@ class SimpleCase:
         _check(lib().cfg_kernel_stats(self._h, _dp(out)))
         names = ("cg_spmv", "cg_update", "cg_p")
         return {n: (int(out[2 * i]), float(out[2 * i + 1])) for i, n in enumerate(names)}
+
+    # ---- the pressure-Poisson system on its own ----
+    def poisson_setup(self, ref_cell=-1):
+        """A = orthogonal laplacianFace(1) under the p conditions, pinned at ref_cell."""
+        _check(lib().cfg_poisson_setup(self._h, C.c_int64(ref_cell)))
+
+    def poisson_solve(self, b, method="dic64", tol=1e-8, x0=None, max_iter=20000, inner_max_iter=5000,
+                      inner_tol=1e-4):
+        """Returns (x, report dict); the residual test is |b - Ax|2/|b|2 in FP64."""
+        x = np.zeros(self.mesh.n_cells) if x0 is None else np.array(x0, np.float64, copy=True)
+        r = _PoissonReport()
+        _check(lib().cfg_poisson_solve(self._h, _dp(_f64(b)), _dp(x), C.c_int32(POISSON[method]), C.c_double(tol),
+                                       C.c_int32(max_iter), C.c_int32(inner_max_iter), C.c_double(inner_tol),
+                                       C.byref(r)))
+        return x, {"inner_iterations": r.inner_iterations, "outer_iterations": r.outer_iterations,
+                   "converged": bool(r.converged), "true_rel_residual": r.true_rel_residual,
+                   "device_ms": r.device_ms, "initial_rel_residual": r.initial_rel_residual}
 
     # ---- diagnostics ----
     def probe_equations(self, controls: SimpleControls, xprobe):

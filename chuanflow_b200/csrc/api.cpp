@@ -137,6 +137,25 @@ int cfg_mesh_block(const double mn[3], const double mx[3], int64_t nx, int64_t n
     });
 }
 
+int cfg_mesh_from_cells(const double* points, int64_t nP, const int32_t* types, const int64_t* cellOffsets,
+                        const int64_t* cellVerts, int64_t nCells, cfg_mesh** out)
+{
+    return guard([&] {
+        need(out && points && types && cellOffsets && cellVerts && nP > 0 && nCells > 0,
+             "cfg_mesh_from_cells: null argument");
+        std::vector<cfg::Vec> pts(static_cast<size_t>(nP));
+        for (int64_t i = 0; i < nP; ++i) pts[i] = {points[3 * i], points[3 * i + 1], points[3 * i + 2]};
+        std::vector<int32_t> ty(types, types + nCells);
+        std::vector<int64_t> off(cellOffsets, cellOffsets + nCells + 1);
+        need(off[0] == 0, "cfg_mesh_from_cells: cell_offsets[0] must be 0");
+        std::vector<int64_t> cv(cellVerts, cellVerts + off[nCells]);
+        for (int64_t v : cv) need(v >= 0 && v < nP, "cfg_mesh_from_cells: vertex index out of range");
+        auto m = std::make_unique<cfg_mesh>();
+        m->m = cfg::meshFromCells(pts, ty, off, cv);
+        *out = m.release();
+    });
+}
+
 int cfg_mesh_move_points(cfg_mesh* mesh, const double* points, int64_t nP)
 {
     return guard([&] {
@@ -418,6 +437,30 @@ int cfg_probe_dic(cfg_ctx* ctx, const double* r, double* z, double* rdinv, int32
         need(ctx && r && z && rdinv, "cfg_probe_dic: null argument");
         ctx->c->probeDIC(r, z, rdinv);
         if (n_colours) *n_colours = ctx->c->nColours();
+    });
+}
+
+int cfg_poisson_setup(cfg_ctx* ctx, int64_t ref_cell)
+{
+    return guard([&] {
+        need(ctx != nullptr, "cfg_poisson_setup: null context");
+        ctx->c->poissonSetup(ref_cell);
+    });
+}
+
+int cfg_poisson_solve(cfg_ctx* ctx, const double* b, double* x, int32_t method, double rel_tol, int32_t max_iter,
+                      int32_t inner_max_iter, double inner_rel_tol, cfg_poisson_report* report)
+{
+    return guard([&] {
+        need(ctx && b && x && report, "cfg_poisson_solve: null argument");
+        double out[6];
+        ctx->c->poissonSolve(b, x, method, rel_tol, max_iter, inner_max_iter, inner_rel_tol, out);
+        report->inner_iterations = static_cast<int64_t>(out[0]);
+        report->outer_iterations = static_cast<int32_t>(out[1]);
+        report->converged = static_cast<int32_t>(out[2]);
+        report->true_rel_residual = out[3];
+        report->device_ms = out[4];
+        report->initial_rel_residual = out[5];
     });
 }
 

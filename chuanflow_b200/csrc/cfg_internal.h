@@ -68,6 +68,12 @@ struct Mesh
     std::vector<Vec> skewVectors(const std::vector<double>& ow) const;
 };
 
+/// polyMesh from volume cells as the reference's gmsh reader builds it
+/// (types: 4 tet, 5 hex, 6 prism; boundary patches named after the
+/// bounding-box planes).
+Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& types,
+                   const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts);
+
 Mesh blockMesh(const Vec& mn, const Vec& mx, int64_t nx, int64_t ny, int64_t nz,
                const std::vector<std::string>& names, const std::vector<std::string>& types);
 

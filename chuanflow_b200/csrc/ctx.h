@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <string>
 #include <memory>
 #include <vector>
 
@@ -70,14 +71,33 @@ private:
     void solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, int64_t& inner);
     void solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner);
     void runCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-               cfg_solver_report* rep);
+               cfg_solver_report* rep, int normType = 0);
     void runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
                   cfg_solver_report* reps);
-    void launchCheck(const char* what);
+    void launchCheck(const char* what, int kernels = 1);
+    template <class F>
+    void launchChunk(const std::string& key, int n, F&& body);
     void dicSetup(const double* vals, const double* diag);
     void dicApply(const double* r, double* z);
     void runDICCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                  cfg_solver_report* rep);
+                  cfg_solver_report* rep, int normType = 0);
+    template <class T>
+    void dicSetupT(DDicT<T>& D, const double* vals, const T* diag);
+    template <class T>
+    void dicApplyT(const DDicT<T>& D, const T* r, T* z);
+    template <class T>
+    void dicCGT(const DDicT<T>& D, const T* vals, const T* diag, const T* b, T* x, T* r, T* p, T* Ap, T* z, double tol,
+                int maxIter, int normType, cfg_solver_report* rep);
+
+public:
+    /// The pressure-Poisson system of the mixed-precision study: the
+    /// orthogonal part of laplacianFace with unit face coefficient, the
+    /// patches' p conditions and an optional reference cell.
+    void poissonSetup(int64_t refCell);
+    void poissonSolve(const double* b, double* x, int method, double tol, int maxIter, int innerMax,
+                      double innerTol, double* out);
+
+private:
     void setNu(double nu);
     void checkMomentumBcs() const;
 
@@ -89,6 +109,7 @@ private:
     int GF_ = 0;       // grid of face kernels
     int GS_ = 0;       // grid of solver kernels (RPT rows per thread)
     int maxW_ = 0;     // longest matrix row
+    int nSlicesEntries_ = 0;  // matrix SELL entries
     int nSlices_ = 0;
     std::vector<void*> allocs_;
     DMesh dm_{};
@@ -117,6 +138,11 @@ private:
     bool needReference_ = true;
     // solver work
     double *cr_, *cp_, *cAp_, *cz_;
+    // mixed-precision Poisson solves
+    float *pVal32_ = nullptr, *pDiag32_ = nullptr, *r32_, *p32_, *Ap32_, *z32_, *e32_, *b32_;
+    DDicT<float> dic32_{};
+    double *pb64_ = nullptr, *px64_ = nullptr;
+    bool poissonReady_ = false;
     // multicolour DIC
     DDic dic_{};
     std::vector<DicPhase> dicPhase_;
@@ -130,6 +156,8 @@ private:
     Timing tm_{};
     int64_t launches_ = 0;
     bool ktime_ = false;
+    bool useGraphs_ = true;
+    std::map<std::string, cudaGraphExec_t> graphs_;
     std::vector<cudaEvent_t> kev_;  // 6 events per CG iteration of a chunk
 };
 

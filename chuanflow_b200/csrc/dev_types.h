@@ -86,11 +86,13 @@ struct SolveState
     double sMax[3];
     int it[3], done[3], conv[3], special[3];
     int allDone;
+    int normType;  // 0: |r|inf / |b|inf (the reference's test); 1: |r|2 / |b|2
     unsigned int ticket[8];
 };
 
 /// Multicolour DIC layout (see dic.cuh).
-struct DDic
+template <class T>
+struct DDicT
 {
     int nColours;
     const int* rows;      // cells grouped by colour, ascending within a colour
@@ -100,11 +102,12 @@ struct DDic
     const int* uStart;    // upper SELL
     const int* uCol;
     const int* uSrc;
-    double* lVal;
-    double* uVal;
-    double* rD;
-    double* rDinv;
+    T* lVal;
+    T* uVal;
+    T* rD;
+    T* rDinv;
 };
+using DDic = DDicT<double>;
 
 /// one colour: cnt rows starting at rows[off], slices starting at slice0
 struct DicPhase

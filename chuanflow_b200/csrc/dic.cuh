@@ -16,40 +16,46 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "solvers.cuh"
 
 namespace cfg
 {
 
+/// the colour layouts' values from the main matrix (T = float also rounds
+/// them to single precision)
+template <class T>
 __global__ void __launch_bounds__(TPB) k_dic_gather(int n, const int* __restrict__ src, const double* __restrict__ val,
-                                                    double* __restrict__ out)
+                                                    T* __restrict__ out)
 {
-    ROW_LOOP(e, n) out[e] = src[e] >= 0 ? val[src[e]] : 0.0;
+    ROW_LOOP(e, n) out[e] = src[e] >= 0 ? static_cast<T>(val[src[e]]) : T(0);
 }
 
 /// rD_i = a_ii - sum a_ij^2 / rD_j over the lower entries, one colour
-__global__ void __launch_bounds__(TPB) k_dic_factor(DDic D, DicPhase ph, const double* __restrict__ diag)
+template <class T>
+__global__ void __launch_bounds__(TPB) k_dic_factor(DDicT<T> D, DicPhase ph, const T* __restrict__ diag)
 {
     FOR_ROWS(t, ph.cnt)
     {
         const int i = D.rows[ph.off + t];
         const int sl = ph.slice0 + (t >> 5), lane = t & 31;
-        double d = diag[i];
+        T d = diag[i];
         for (int e = D.lStart[sl] + lane; e < D.lStart[sl + 1]; e += 32)
         {
             const int j = D.lCol[e];
             if (j < 0) break;
-            const double a = D.lVal[e];
+            const T a = D.lVal[e];
             d = d - a * a / D.rD[j];
         }
         D.rD[i] = d;
-        D.rDinv[i] = 1.0 / d;
+        D.rDinv[i] = T(1) / d;
     }
 }
 
 /// forward phase of one colour: z_i = rDinv_i (r_i - sum_lower a_ij z_j);
 /// the last colour's rows also contribute their r_i z_i partials
-__global__ void __launch_bounds__(TPB) k_dic_fwd(DDic D, DicPhase ph, const double* __restrict__ r, double* z,
-                                                 int last, double* partials, SolveState* st)
+template <class T>
+__global__ void __launch_bounds__(TPB) k_dic_fwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int last,
+                                                 double* partials, SolveState* st)
 {
     if (st->allDone) return;
     double sm[1] = {0.0};
@@ -57,17 +63,17 @@ __global__ void __launch_bounds__(TPB) k_dic_fwd(DDic D, DicPhase ph, const doub
     {
         const int i = D.rows[ph.off + t];
         const int sl = ph.slice0 + (t >> 5), lane = t & 31;
-        double s = 0.0;
+        T s = T(0);
         for (int e = D.lStart[sl] + lane; e < D.lStart[sl + 1]; e += 32)
         {
             const int j = D.lCol[e];
             if (j < 0) break;
             s += D.lVal[e] * z[j];
         }
-        const double ri = r[i];
-        const double zi = D.rDinv[i] * (ri - s);
+        const T ri = r[i];
+        const T zi = D.rDinv[i] * (ri - s);
         z[i] = zi;
-        sm[0] += ri * zi;
+        sm[0] += static_cast<double>(ri * zi);
     }
     if (!last) return;
     block_sum<1>(sm);
@@ -77,8 +83,9 @@ __global__ void __launch_bounds__(TPB) k_dic_fwd(DDic D, DicPhase ph, const doub
 /// backward phase of one colour: z_i -= rDinv_i sum_upper a_ij z_j, with
 /// the r_i z_i partials; `final` (the phase that runs last) also reduces
 /// all colours' partials into r.z and advances beta
-__global__ void __launch_bounds__(TPB) k_dic_bwd(DDic D, DicPhase ph, const double* __restrict__ r, double* z,
-                                                 int final, int nPartials, double* partials, SolveState* st)
+template <class T>
+__global__ void __launch_bounds__(TPB) k_dic_bwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int final,
+                                                 int nPartials, double* partials, SolveState* st)
 {
     if (st->allDone) return;
     double sm[1] = {0.0};
@@ -86,16 +93,16 @@ __global__ void __launch_bounds__(TPB) k_dic_bwd(DDic D, DicPhase ph, const doub
     {
         const int i = D.rows[ph.off + t];
         const int sl = ph.slice0 + (t >> 5), lane = t & 31;
-        double s = 0.0;
+        T s = T(0);
         for (int e = D.uStart[sl] + lane; e < D.uStart[sl + 1]; e += 32)
         {
             const int j = D.uCol[e];
             if (j < 0) break;
             s += D.uVal[e] * z[j];
         }
-        const double zi = z[i] - D.rDinv[i] * s;
+        const T zi = z[i] - D.rDinv[i] * s;
         z[i] = zi;
-        sm[0] += r[i] * zi;
+        sm[0] += static_cast<double>(r[i] * zi);
     }
     block_sum<1>(sm);
     if (threadIdx.x == 0) partials[ph.partialOff + blockIdx.x] = sm[0];
@@ -113,38 +120,46 @@ __global__ void __launch_bounds__(TPB) k_dic_bwd(DDic D, DicPhase ph, const doub
     }
 }
 
-/// x += alpha p; r -= alpha Ap; |r|inf test (Matrix.cpp:195-208), without z
-static __global__ void __launch_bounds__(TPB) k_cg_update_nz(int n, const double* __restrict__ p,
-                                                             const double* __restrict__ Ap, double* __restrict__ x,
-                                                             double* __restrict__ r, double* partials, SolveState* st)
+/// x += alpha p; r -= alpha Ap; residual test (Matrix.cpp:195-208), without z
+template <class T = double>
+__global__ void __launch_bounds__(TPB) k_cg_update_nz(int n, const T* __restrict__ p, const T* __restrict__ Ap,
+                                                      T* __restrict__ x, T* __restrict__ r, double* partials,
+                                                      SolveState* st)
 {
     if (st->allDone) return;
-    const double alpha = st->alpha[0];
+    const T alpha = static_cast<T>(st->alpha[0]);
     double mx[2] = {0.0, 0.0};
+    double sm[1] = {0.0};
     FOR_ROWS(c, n)
     {
         x[c] = x[c] + alpha * p[c];
-        const double ri = r[c] - alpha * Ap[c];
+        const T ri = r[c] - alpha * Ap[c];
         r[c] = ri;
-        if (isnan(ri)) mx[1] = 1.0;
-        mx[0] = smax(mx[0], fabs(ri));
+        if (isnan(static_cast<double>(ri))) mx[1] = 1.0;
+        mx[0] = smax(mx[0], fabs(static_cast<double>(ri)));
+        sm[0] += static_cast<double>(ri) * static_cast<double>(ri);
     }
     block_max<2>(mx);
+    __syncthreads();
+    block_sum<1>(sm);
     const int G = gridDim.x;
     if (threadIdx.x == 0)
     {
         partials[blockIdx.x] = mx[0];
         partials[G + blockIdx.x] = mx[1];
+        partials[2 * G + blockIdx.x] = sm[0];
     }
     if (!last_block(&st->ticket[0])) return;
-    double fm[2];
+    double fm[2], fs[1];
     final_max<2>(partials, G, fm);
+    __syncthreads();
+    final_sum<1>(partials + 2 * G, G, fs);
     if (threadIdx.x == 0)
     {
         st->ticket[0] = 0;
         const int it = st->it[0] + 1;
         st->it[0] = it;
-        const double fin = fm[1] > 0 ? NAN : fm[0];
+        const double fin = fm[1] > 0 ? NAN : resid_norm(st, fm[0], fs[0]);
         st->fin[0] = fin;
         if (fin / st->bnorm[0] < st->tol)
         {
@@ -165,11 +180,11 @@ static __global__ void __launch_bounds__(TPB) k_cg_update_nz(int n, const double
 }
 
 /// p = z + beta p
-static __global__ void __launch_bounds__(TPB) k_cg_pz(int n, const double* __restrict__ z, double* __restrict__ p,
-                                                      const SolveState* st)
+template <class T = double>
+__global__ void __launch_bounds__(TPB) k_cg_pz(int n, const T* __restrict__ z, T* __restrict__ p, const SolveState* st)
 {
     if (st->allDone) return;
-    const double beta = st->beta[0];
+    const T beta = static_cast<T>(st->beta[0]);
     FOR_ROWS(c, n) p[c] = z[c] + beta * p[c];
 }
 

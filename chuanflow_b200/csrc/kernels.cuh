@@ -329,10 +329,11 @@ __global__ void __launch_bounds__(TPB) k_grad_ls2(DMesh m, CV3P x, BcTab bc, CGr
 /// the row are loaded first and then all gathers issued, so a thread keeps W
 /// independent loads in flight instead of walking a dependent chain.  W = 0
 /// walks rows of any length.  Entries are added in order, skipping only the
-/// trailing pads, so the sum is the reference's.
-template <int W, int NC>
-__device__ __forceinline__ void spmv_row(const DMat& A, const double* __restrict__ val, int c,
-                                         const double* const (&x)[NC], double (&y)[NC])
+/// trailing pads, so the sum is the reference's.  T = float forms each
+/// product in single precision and accumulates in double.
+template <int W, int NC, class T = double>
+__device__ __forceinline__ void spmv_row(const DMat& A, const T* __restrict__ val, int c, const T* const (&x)[NC],
+                                         double (&y)[NC])
 {
 #pragma unroll
     for (int q = 0; q < NC; ++q) y[q] = 0.0;
@@ -341,24 +342,24 @@ __device__ __forceinline__ void spmv_row(const DMat& A, const double* __restrict
     if constexpr (W > 0)
     {
         int col[W];
-        double v[W];
+        T v[W];
 #pragma unroll
         for (int k = 0; k < W; ++k)
         {
             const int e = e0 + 32 * k;
             col[k] = e < e1 ? __ldg(A.col + e) : -1;
-            v[k] = e < e1 ? __ldg(val + e) : 0.0;
+            v[k] = e < e1 ? __ldg(val + e) : T(0);
         }
-        double xv[NC][W];
+        T xv[NC][W];
 #pragma unroll
         for (int k = 0; k < W; ++k)
 #pragma unroll
-            for (int q = 0; q < NC; ++q) xv[q][k] = col[k] >= 0 ? __ldg(x[q] + col[k]) : 0.0;
+            for (int q = 0; q < NC; ++q) xv[q][k] = col[k] >= 0 ? __ldg(x[q] + col[k]) : T(0);
 #pragma unroll
         for (int k = 0; k < W; ++k)
             if (col[k] >= 0)
 #pragma unroll
-                for (int q = 0; q < NC; ++q) y[q] += v[k] * xv[q][k];
+                for (int q = 0; q < NC; ++q) y[q] += static_cast<double>(v[k] * xv[q][k]);
     }
     else
     {
@@ -366,9 +367,9 @@ __device__ __forceinline__ void spmv_row(const DMat& A, const double* __restrict
         {
             const int col = A.col[e];
             if (col < 0) break;
-            const double v = val[e];
+            const T v = val[e];
 #pragma unroll
-            for (int q = 0; q < NC; ++q) y[q] += v * x[q][col];
+            for (int q = 0; q < NC; ++q) y[q] += static_cast<double>(v * x[q][col]);
         }
     }
 }

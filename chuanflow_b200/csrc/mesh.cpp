@@ -8,8 +8,10 @@
 // produces (src/3d/src/mesh/blockMesh.cpp:76-185), derived in closed form
 // instead of through a face map.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
 
 #include "cfg_internal.h"
 
@@ -120,8 +122,13 @@ void Mesh::finish()
 {
     const int64_t nF = nFaces(), nI = nInternal();
     if (static_cast<int64_t>(faceOffsets.size()) != nF + 1) fail(CFG_EMESH, "polyMesh: face offsets size");
+    // polyMesh.cpp:23 counts cells from the owners alone; a cell that owns
+    // no face (every face shared with lower-numbered cells, possible in
+    // element meshes) would then index past the cell arrays there, so the
+    // neighbours are counted too (identical whenever the reference is defined)
     nCells = 0;
     for (int64_t o : owner) nCells = std::max(nCells, o + 1);
+    for (int64_t nb : neighbour) nCells = std::max(nCells, nb + 1);
     for (int64_t f = 0; f < nF; ++f)
     {
         if (faceOffsets[f + 1] - faceOffsets[f] < 3) fail(CFG_EMESH, "polyMesh: face with fewer than 3 vertices");
@@ -298,6 +305,167 @@ std::vector<Vec> Mesh::skewVectors(const std::vector<double>& ow) const
         s[static_cast<size_t>(f)] = Cf[static_cast<size_t>(f)] - (co + (cn - co) * (1.0 - ow[static_cast<size_t>(f)]));
     }
     return s;
+}
+
+}  // namespace cfg
+
+namespace cfg
+{
+namespace
+{
+
+/// Local face rings of the gmsh volume elements (tet 4, hex 5, prism 6),
+/// in the order src/3d/src/mesh/gmshMesh.cpp:52-68 registers them.
+const std::vector<std::vector<int>>& faceRings(int type)
+{
+    static const std::vector<std::vector<int>> tet = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+    static const std::vector<std::vector<int>> hex = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4},
+                                                      {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}};
+    static const std::vector<std::vector<int>> prism = {{0, 1, 2}, {3, 4, 5}, {0, 1, 4, 3}, {1, 2, 5, 4}, {2, 0, 3, 5}};
+    static const std::vector<std::vector<int>> none;
+    switch (type)
+    {
+    case 4: return tet;
+    case 5: return hex;
+    case 6: return prism;
+    default: return none;
+    }
+}
+
+struct FaceKeyHash
+{
+    size_t operator()(const std::array<int64_t, 5>& k) const
+    {
+        uint64_t h = 1469598103934665603ULL;
+        for (int64_t v : k)
+        {
+            h ^= static_cast<uint64_t>(v) + 0x9E3779B97F4A7C15ULL;
+            h *= 1099511628211ULL;
+            h ^= h >> 31;
+        }
+        return static_cast<size_t>(h);
+    }
+};
+
+}  // namespace
+
+Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& types,
+                   const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts)
+{
+    // faces registered cell by cell in each element's ring order and
+    // deduplicated by their sorted vertices; the first registration keeps
+    // its vertex ring (gmshMesh.cpp:578-607)
+    struct Ref
+    {
+        int64_t v0, nv, cell0, cell1;
+    };
+    const int64_t nCells = static_cast<int64_t>(types.size());
+    std::vector<int64_t> ringVerts;
+    std::vector<Ref> refs;
+    std::unordered_map<std::array<int64_t, 5>, int64_t, FaceKeyHash> index;
+    index.reserve(static_cast<size_t>(4 * nCells));
+    for (int64_t c = 0; c < nCells; ++c)
+    {
+        const auto& rings = faceRings(types[static_cast<size_t>(c)]);
+        if (rings.empty()) fail(CFG_EMESH, "mesh: cell type " + std::to_string(types[c]) + " is not tet (4), hex (5) or prism (6)");
+        const int64_t* cv = cellVerts.data() + cellOffsets[c];
+        const int64_t need = types[c] == 4 ? 4 : (types[c] == 5 ? 8 : 6);
+        if (cellOffsets[c + 1] - cellOffsets[c] != need) fail(CFG_EMESH, "mesh: cell vertex count does not fit its type");
+        for (const auto& ring : rings)
+        {
+            std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
+            for (size_t k = 0; k < ring.size(); ++k) key[k] = cv[ring[k]];
+            std::sort(key.begin(), key.begin() + static_cast<long>(ring.size()));
+            auto it = index.find(key);
+            if (it == index.end())
+            {
+                index.emplace(key, static_cast<int64_t>(refs.size()));
+                refs.push_back({static_cast<int64_t>(ringVerts.size()), static_cast<int64_t>(ring.size()), c, -1});
+                for (int k : ring) ringVerts.push_back(cv[k]);
+            }
+            else
+            {
+                Ref& r = refs[static_cast<size_t>(it->second)];
+                if (r.cell1 != -1) fail(CFG_EMESH, "mesh: a face belongs to three cells: the mesh is not manifold");
+                r.cell1 = c;
+            }
+        }
+    }
+    // boundary faces named after the bounding-box plane they lie on
+    // (gmshMesh.cpp:636-667, the case of a file without surface groups)
+    Vec lo = points[0], hi = points[0];
+    for (const Vec& v : points)
+    {
+        lo.x = std::min(lo.x, v.x); hi.x = std::max(hi.x, v.x);
+        lo.y = std::min(lo.y, v.y); hi.y = std::max(hi.y, v.y);
+        lo.z = std::min(lo.z, v.z); hi.z = std::max(hi.z, v.z);
+    }
+    const double extent = std::max({hi.x - lo.x, hi.y - lo.y, hi.z - lo.z, 1e-300});
+    const double eps = 1e-9 * extent;
+    const char* planeNames[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+    auto comp = [](const Vec& v, int d) { return d == 0 ? v.x : (d == 1 ? v.y : v.z); };
+    auto planeOf = [&](const Ref& r) -> int {
+        for (int d = 0; d < 3; ++d)
+            for (int s = 0; s < 2; ++s)
+            {
+                const double lim = s ? comp(hi, d) : comp(lo, d);
+                bool on = true;
+                for (int64_t k = 0; k < r.nv; ++k)
+                    if (std::abs(comp(points[static_cast<size_t>(ringVerts[r.v0 + k])], d) - lim) > eps)
+                    {
+                        on = false;
+                        break;
+                    }
+                if (on) return 2 * d + s;
+            }
+        return -1;
+    };
+    Mesh m;
+    m.points = points;
+    std::vector<int> patchOfPlane(6, -1);
+    std::vector<std::vector<size_t>> patchFaces;
+    std::vector<size_t> internal;
+    for (size_t i = 0; i < refs.size(); ++i)
+    {
+        Ref& r = refs[i];
+        if (r.cell1 != -1)
+        {
+            if (r.cell0 > r.cell1) std::swap(r.cell0, r.cell1);
+            internal.push_back(i);
+            continue;
+        }
+        const int pl = planeOf(r);
+        if (pl < 0) fail(CFG_EMESH, "mesh: a boundary face lies on no bounding-box plane");
+        if (patchOfPlane[pl] < 0)
+        {
+            patchOfPlane[pl] = static_cast<int>(patchFaces.size());
+            patchFaces.emplace_back();
+            Mesh::Patch p;
+            p.name = planeNames[pl];
+            p.type = "wall";
+            m.patches.push_back(p);
+        }
+        patchFaces[patchOfPlane[pl]].push_back(i);
+    }
+    m.faceOffsets.push_back(0);
+    auto addFace = [&](const Ref& r) {
+        for (int64_t k = 0; k < r.nv; ++k) m.faceVerts.push_back(ringVerts[r.v0 + k]);
+        m.faceOffsets.push_back(static_cast<int64_t>(m.faceVerts.size()));
+        m.owner.push_back(r.cell0);
+    };
+    for (size_t i : internal)
+    {
+        addFace(refs[i]);
+        m.neighbour.push_back(refs[i].cell1);
+    }
+    for (size_t pi = 0; pi < patchFaces.size(); ++pi)
+    {
+        m.patches[pi].start = static_cast<int64_t>(m.owner.size());
+        m.patches[pi].size = static_cast<int64_t>(patchFaces[pi].size());
+        for (size_t i : patchFaces[pi]) addFace(refs[i]);
+    }
+    m.finish();
+    return m;
 }
 
 }  // namespace cfg

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 
@@ -522,6 +523,22 @@ __global__ void __launch_bounds__(TPB) k_explicit_op(DMat A, const double* __res
     }
 }
 
+__global__ void __launch_bounds__(TPB) k_fill(int n, double v, double* a)
+{
+    ROW_LOOP(i, n) a[i] = v;
+}
+
+__global__ void __launch_bounds__(TPB) k_to_float(int n, const double* __restrict__ a, float* __restrict__ b)
+{
+    ROW_LOOP(i, n) b[i] = static_cast<float>(a[i]);
+}
+
+/// x += e, e in single precision
+__global__ void __launch_bounds__(TPB) k_add_f32(int n, const float* __restrict__ e, double* __restrict__ x)
+{
+    ROW_LOOP(i, n) x[i] = x[i] + static_cast<double>(e[i]);
+}
+
 // ===========================================================================
 // host side
 // ===========================================================================
@@ -559,6 +576,7 @@ Ctx::Ctx(const Mesh& mesh, int device, cudaStream_t stream) : mesh_(mesh), devic
         CFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         ownStream_ = true;
     }
+    if (const char* g = std::getenv("CHUANFLOW_GRAPHS")) useGraphs_ = std::strcmp(g, "0") != 0;
     const size_t nP = mesh_.patches.size();
     uType_.assign(nP, CFG_BC_ZERO_GRADIENT);
     pType_.assign(nP, CFG_BC_ZERO_GRADIENT);
@@ -577,6 +595,7 @@ Ctx::~Ctx()
     if (scalHost_) cudaFreeHost(scalHost_);
     for (int i = 0; i < 16; ++i) cudaEventDestroy(tm_.ev[i]);
     for (auto& e : kev_) cudaEventDestroy(e);
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
     if (ownStream_) cudaStreamDestroy(stream_);
 }
 
@@ -852,6 +871,7 @@ void Ctx::buildDevice()
     d.cfCode = upload(cfCode);
     d.cfOther = upload(cfOther);
     d.mStart = upload(mStart);
+    nSlicesEntries_ = mStart[nSlices_];
     d.mCol = upload(mCol);
     d.mCode = upload(mCode);
 
@@ -1121,9 +1141,9 @@ void Ctx::refreshBc()
     bcDirty_ = false;
 }
 
-void Ctx::launchCheck(const char* what)
+void Ctx::launchCheck(const char* what, int kernels)
 {
-    ++launches_;
+    launches_ += kernels;
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) fail(CFG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -1216,14 +1236,67 @@ void dispatchW(int maxW, F&& f)
 }
 }  // namespace
 
+/// Enqueues body(0..n-1) -- n solver iterations -- on the stream.  The
+/// first time a (key, n) pair is seen the iterations are captured into a
+/// CUDA graph, which later calls replay: a chunk then costs one launch.
+/// key must name everything the kernels' arguments depend on.
+template <class F>
+void Ctx::launchChunk(const std::string& key, int n, F&& body)
+{
+    // Event-timed iterations stay eager: an event recorded during capture
+    // becomes a graph dependency, not a timestamp.
+    // The caller counts the chunk's kernels; counts taken inside body are
+    // dropped so eager and replayed chunks count alike.
+    const int64_t counted = launches_;
+    if (!useGraphs_ || ktime_)
+    {
+        for (int i = 0; i < n; ++i) body(i);
+        launches_ = counted;
+        return;
+    }
+    const std::string k = key + "#" + std::to_string(n) + (ktime_ ? "t" : "");
+    auto it = graphs_.find(k);
+    if (it == graphs_.end())
+    {
+        cudaGraph_t g = nullptr;
+        CFG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < n; ++i) body(i);
+        launches_ = counted;
+        CFG_CUDA(cudaStreamEndCapture(stream_, &g));
+        cudaGraphExec_t ge = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) fail(CFG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        it = graphs_.emplace(k, ge).first;
+    }
+    CFG_CUDA(cudaGraphLaunch(it->second, stream_));
+}
+
+namespace
+{
+std::string ptrKey(const char* kind, std::initializer_list<const void*> ps, int extra = 0)
+{
+    std::string s(kind);
+    char buf[32];
+    for (const void* p : ps)
+    {
+        std::snprintf(buf, sizeof buf, ":%p", p);
+        s += buf;
+    }
+    std::snprintf(buf, sizeof buf, ":%d", extra);
+    return s + buf;
+}
+}  // namespace
+
 void Ctx::runCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                cfg_solver_report* rep)
+                cfg_solver_report* rep, int normType)
 {
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
     SolveState init{};
     init.tol = tol;
     init.maxIter = maxIter;
     init.nComp = 1;
+    init.normType = normType;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     dispatchW(maxW_, [&](auto Wc) {
         constexpr int W = decltype(Wc)::value;
@@ -1252,21 +1325,20 @@ void Ctx::runCG(const double* vals, const double* diag, const double* b, double*
             itBefore = stHost_->it[0];
             if (stHost_->allDone || launched >= maxIter) break;
             const int n = std::min(chunk, maxIter - launched);
-            for (int k = 0; k < n; ++k)
-            {
+            launchChunk(ptrKey("cg", {vals, diag, x}, W), n, [&](int k) {
                 cudaEvent_t* ev = ktime_ ? &kev_[6 * k] : nullptr;
                 if (ev) CFG_CUDA(cudaEventRecord(ev[0], stream_));
                 k_cg_spmv<W><<<GS_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
                 if (ev) CFG_CUDA(cudaEventRecord(ev[1], stream_));
                 if (ev) CFG_CUDA(cudaEventRecord(ev[2], stream_));
-                k_cg_update<<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
+                k_cg_update<double><<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
                 if (ev) CFG_CUDA(cudaEventRecord(ev[3], stream_));
                 if (ev) CFG_CUDA(cudaEventRecord(ev[4], stream_));
-                k_cg_p<<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
+                k_cg_p<double><<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
                 if (ev) CFG_CUDA(cudaEventRecord(ev[5], stream_));
-                launches_ += 2;
-                launchCheck("cg_iter");
-            }
+                launchCheck("cg_iter", 0);
+            });
+            launches_ += 3 * n;
             launched += n;
             lastChunk = n;
             chunk = std::min(chunk * 2, 64);
@@ -1299,16 +1371,15 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
             CFG_CUDA(cudaStreamSynchronize(stream_));
             if (stHost_->allDone || launched >= maxIter) break;
             const int m = std::min(chunk, maxIter - launched);
-            for (int k = 0; k < m; ++k)
-            {
+            launchChunk(ptrKey("bicg", {vals, diag, x.c[0], x.c[1], x.c[2]}, W * 8 + NC), m, [&](int) {
                 k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, diag, br_, bp_, bv_, bz_, st_);
                 k_bi_spmv1<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
                 k_bi_s<NC><<<GS_, TPB, 0, stream_>>>(n, diag, x, bz_, br_, bv_, bs_, bsh_, partials_, st_);
                 k_bi_spmv2<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bt_, bs_, partials_, st_);
                 k_bi_x<NC><<<GS_, TPB, 0, stream_>>>(n, x, bsh_, bs_, bt_, br_, br0_, partials_, st_);
-                launches_ += 4;
-                launchCheck("bicg_iter");
-            }
+                launchCheck("bicg_iter", 0);
+            });
+            launches_ += 5 * m;
             launched += m;
             chunk = std::min(chunk * 2, 32);
         }
@@ -1326,62 +1397,64 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     }
 }
 
-void Ctx::dicSetup(const double* vals, const double* diag)
+namespace
 {
-    k_dic_gather<<<std::max(1, std::min((nLo_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nLo_, dic_.lSrc, vals,
-                                                                                           dic_.lVal);
-    k_dic_gather<<<std::max(1, std::min((nUp_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nUp_, dic_.uSrc, vals,
-                                                                                           dic_.uVal);
+inline int phaseGrid(const DicPhase& ph) { return std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)); }
+}  // namespace
+
+template <class T>
+void Ctx::dicSetupT(DDicT<T>& D, const double* vals, const T* diag)
+{
+    k_dic_gather<T><<<std::max(1, std::min((nLo_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nLo_, D.lSrc, vals, D.lVal);
+    k_dic_gather<T><<<std::max(1, std::min((nUp_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nUp_, D.uSrc, vals, D.uVal);
     launchCheck("dic_gather");
     for (const DicPhase& ph : dicPhase_)
     {
-        k_dic_factor<<<std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)), TPB, 0, stream_>>>(dic_, ph, diag);
+        k_dic_factor<T><<<phaseGrid(ph), TPB, 0, stream_>>>(D, ph, diag);
         launchCheck("dic_factor");
     }
 }
 
-void Ctx::dicApply(const double* r, double* z)
+template <class T>
+void Ctx::dicApplyT(const DDicT<T>& D, const T* r, T* z)
 {
-    const int C = dic_.nColours;
+    const int C = D.nColours;
     for (int c = 0; c < C; ++c)
-    {
-        const DicPhase& ph = dicPhase_[c];
-        k_dic_fwd<<<std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)), TPB, 0, stream_>>>(dic_, ph, r, z, c == C - 1,
-                                                                                           partials_, st_);
-    }
+        k_dic_fwd<T><<<phaseGrid(dicPhase_[c]), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == C - 1, partials_, st_);
     if (C == 1)
     {
         // no backward phase: a one-block final reduction of the forward partials
         const DicPhase none{0, 0, 0, dicPartials_ - 1};
-        k_dic_bwd<<<1, TPB, 0, stream_>>>(dic_, none, r, z, 1, dicPartials_, partials_, st_);
+        k_dic_bwd<T><<<1, TPB, 0, stream_>>>(D, none, r, z, 1, dicPartials_, partials_, st_);
     }
     for (int c = C - 2; c >= 0; --c)
-    {
-        const DicPhase& ph = dicPhase_[c];
-        k_dic_bwd<<<std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)), TPB, 0, stream_>>>(
-            dic_, ph, r, z, c == 0, c == 0 ? dicPartials_ - 1 : 0, partials_, st_);
-    }
-    launches_ += 2 * C;
-    launchCheck("dic_apply");
+        k_dic_bwd<T><<<phaseGrid(dicPhase_[c]), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == 0,
+                                                                   c == 0 ? dicPartials_ - 1 : 0, partials_, st_);
+    launchCheck("dic_apply", C == 1 ? 2 : 2 * C - 1);
 }
 
-/// PCG of Matrix.cpp:153-222 with z = M^-1 r from the multicolour DIC.
-void Ctx::runDICCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                   cfg_solver_report* rep)
+void Ctx::dicSetup(const double* vals, const double* diag) { dicSetupT<double>(dic_, vals, diag); }
+void Ctx::dicApply(const double* r, double* z) { dicApplyT<double>(dic_, r, z); }
+
+/// PCG of Matrix.cpp:153-222 with z = M^-1 r from the multicolour DIC, on
+/// values and vectors of type T; the DIC must be set up for these values.
+template <class T>
+void Ctx::dicCGT(const DDicT<T>& D, const T* vals, const T* diag, const T* b, T* x, T* r, T* p, T* Ap, T* z,
+                 double tol, int maxIter, int normType, cfg_solver_report* rep)
 {
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
     SolveState init{};
     init.tol = tol;
     init.maxIter = maxIter;
     init.nComp = 1;
+    init.normType = normType;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
-    dicSetup(vals, diag);
     dispatchW(maxW_, [&](auto Wc) {
         constexpr int W = decltype(Wc)::value;
-        k_cg_init<W><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
+        k_cg_init<W, T><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, r, p, partials_, st_);
         launchCheck("cg_init");
-        dicApply(cr_, cz_);
-        k_cg_pz<<<GS_, TPB, 0, stream_>>>(dm_.nC, cz_, cp_, st_);
+        dicApplyT<T>(D, r, z);
+        k_cg_pz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, z, p, st_);
         launchCheck("cg_pz");
         int launched = 0;
         int chunk = 8;
@@ -1391,15 +1464,14 @@ void Ctx::runDICCG(const double* vals, const double* diag, const double* b, doub
             CFG_CUDA(cudaStreamSynchronize(stream_));
             if (stHost_->allDone || launched >= maxIter) break;
             const int n = std::min(chunk, maxIter - launched);
-            for (int k = 0; k < n; ++k)
-            {
-                k_cg_spmv<W><<<GS_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
-                k_cg_update_nz<<<GS_, TPB, 0, stream_>>>(dm_.nC, cp_, cAp_, x, cr_, partials_, st_);
-                dicApply(cr_, cz_);
-                k_cg_pz<<<GS_, TPB, 0, stream_>>>(dm_.nC, cz_, cp_, st_);
-                launches_ += 3;
-                launchCheck("dic_cg_iter");
-            }
+            launchChunk(ptrKey("diccg", {vals, diag, x, r, p, Ap, z, D.lVal}, W), n, [&](int) {
+                k_cg_spmv<W, T><<<GS_, TPB, 0, stream_>>>(A, vals, p, Ap, partials_, st_);
+                k_cg_update_nz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, p, Ap, x, r, partials_, st_);
+                dicApplyT<T>(D, r, z);
+                k_cg_pz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, z, p, st_);
+                launchCheck("dic_cg_iter", 0);
+            });
+            launches_ += (3 + (D.nColours == 1 ? 2 : 2 * D.nColours - 1)) * static_cast<long>(n);
             launched += n;
             chunk = std::min(chunk * 2, 64);
         }
@@ -1408,6 +1480,13 @@ void Ctx::runDICCG(const double* vals, const double* diag, const double* b, doub
     rep->converged = stHost_->conv[0];
     rep->initial_residual = stHost_->init[0];
     rep->final_residual = stHost_->conv[0] && stHost_->it[0] == 0 ? stHost_->init[0] : stHost_->fin[0];
+}
+
+void Ctx::runDICCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                   cfg_solver_report* rep, int normType)
+{
+    dicSetup(vals, diag);
+    dicCGT<double>(dic_, vals, diag, b, x, cr_, cp_, cAp_, cz_, tol, maxIter, normType, rep);
 }
 
 /// fvMatrix::solve for the momentum equation (fvMatrix.cpp:73-129): x from
@@ -1856,6 +1935,135 @@ void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQ
         CFG_CUDA(cudaStreamSynchronize(stream_));
         for (int c = 0; c < nC; ++c) out[3 * static_cast<size_t>(c) + q] = t[c];
     }
+}
+
+void Ctx::poissonSetup(int64_t refCell)
+{
+    CFG_CUDA(cudaSetDevice(device_));
+    refreshBc();
+    const int nC = dm_.nC, nF = dm_.nF;
+    if (refCell >= nC) fail(CFG_EINVAL, "cfg_poisson_setup: reference cell beyond the last cell");
+    if (!poissonReady_)
+    {
+        const size_t nE = static_cast<size_t>(nSlicesEntries_);
+        pVal32_ = alloc<float>(nE);
+        pDiag32_ = alloc<float>(nC);
+        r32_ = alloc<float>(nC);
+        p32_ = alloc<float>(nC);
+        Ap32_ = alloc<float>(nC);
+        z32_ = alloc<float>(nC);
+        e32_ = alloc<float>(nC);
+        b32_ = alloc<float>(nC);
+        pb64_ = alloc<double>(nC);
+        px64_ = alloc<double>(nC);
+        dic32_.nColours = dic_.nColours;
+        dic32_.rows = dic_.rows;
+        dic32_.lStart = dic_.lStart;
+        dic32_.lCol = dic_.lCol;
+        dic32_.lSrc = dic_.lSrc;
+        dic32_.uStart = dic_.uStart;
+        dic32_.uCol = dic_.uCol;
+        dic32_.uSrc = dic_.uSrc;
+        dic32_.lVal = alloc<float>(nLo_);
+        dic32_.uVal = alloc<float>(nUp_);
+        dic32_.rD = alloc<float>(nC);
+        dic32_.rDinv = alloc<float>(nC);
+        poissonReady_ = true;
+    }
+    // unit face coefficient, no flux: laplacianFace(1) and the p conditions
+    k_fill<<<GF_, TPB, 0, stream_>>>(nF, 1.0, rAUf_);
+    CFG_CUDA(cudaMemsetAsync(fScratch_, 0, nF * sizeof(double), stream_));
+    CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
+    k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, fScratch_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_,
+                                          refCell >= 0 ? static_cast<int>(refCell) : -1, 0.0);
+    launchCheck("poisson_assemble");
+    const int nE = nSlicesEntries_;
+    k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, pVal_d_, pVal32_);
+    k_to_float<<<G_, TPB, 0, stream_>>>(nC, pDiag_, pDiag32_);
+    launchCheck("poisson_float");
+    dicSetupT<double>(dic_, pVal_d_, pDiag_);
+    dicSetupT<float>(dic32_, pVal_d_, pDiag32_);
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int maxIter, int innerMax, double innerTol,
+                       double* out)
+{
+    // out: inner iterations, outer iterations, converged, true |b-Ax|2/|b|2,
+    //      device ms, initial true relative residual
+    if (!poissonReady_) fail(CFG_EINVAL, "cfg_poisson_solve: call cfg_poisson_setup first");
+    CFG_CUDA(cudaSetDevice(device_));
+    const int nC = dm_.nC;
+    const DMat A{nC, dm_.mStart, dm_.mCol};
+    CFG_CUDA(cudaMemcpyAsync(pb64_, b, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(px64_, x, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    // true residual |b - A x|2 / |b|2 in FP64 (r left in cr_)
+    auto trueRel = [&]() {
+        SolveState s0{};
+        s0.normType = 1;
+        s0.maxIter = 0;
+        CFG_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+        dispatchW(maxW_, [&](auto Wc) {
+            constexpr int W = decltype(Wc)::value;
+            k_cg_init<W, double><<<GS_, TPB, 0, stream_>>>(A, pVal_d_, pDiag_, pb64_, px64_, cr_, cz_, partials_, st_);
+        });
+        launchCheck("true_residual");
+        CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        return stHost_->init[0] / stHost_->bnorm[0];
+    };
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    const double rel0 = trueRel();
+    CFG_CUDA(cudaEventRecord(tm_.ev[2], stream_));
+    int64_t inner = 0;
+    int outer = 0;
+    cfg_solver_report rep{};
+    if (method == 0)
+    {
+        runCG(pVal_d_, pDiag_, pb64_, px64_, tol, maxIter, &rep, 1);
+        inner = rep.iterations;
+        outer = 1;
+    }
+    else if (method == 1)
+    {
+        dicCGT<double>(dic_, pVal_d_, pDiag_, pb64_, px64_, cr_, cp_, cAp_, cz_, tol, maxIter, 1, &rep);
+        inner = rep.iterations;
+        outer = 1;
+    }
+    else if (method == 2)
+    {
+        // FP32 DIC-PCG corrections inside FP64 iterative refinement
+        double rel = rel0;
+        while (rel > tol && outer < 100 && inner < maxIter)
+        {
+            k_to_float<<<G_, TPB, 0, stream_>>>(nC, cr_, b32_);
+            CFG_CUDA(cudaMemsetAsync(e32_, 0, nC * sizeof(float), stream_));
+            dicCGT<float>(dic32_, pVal32_, pDiag32_, b32_, e32_, r32_, p32_, Ap32_, z32_, innerTol,
+                          std::min(innerMax, static_cast<int>(maxIter - inner)), 1, &rep);
+            inner += rep.iterations;
+            k_add_f32<<<G_, TPB, 0, stream_>>>(nC, e32_, px64_);
+            launchCheck("ir_update");
+            ++outer;
+            rel = trueRel();
+        }
+    }
+    else
+    {
+        fail(CFG_EINVAL, "cfg_poisson_solve: unknown method");
+    }
+    CFG_CUDA(cudaEventRecord(tm_.ev[3], stream_));
+    CFG_CUDA(cudaEventSynchronize(tm_.ev[3]));
+    float ms = 0;
+    CFG_CUDA(cudaEventElapsedTime(&ms, tm_.ev[2], tm_.ev[3]));
+    const double rel = trueRel();
+    CFG_CUDA(cudaMemcpyAsync(x, px64_, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    out[0] = static_cast<double>(inner);
+    out[1] = outer;
+    out[2] = rel <= tol ? 1.0 : 0.0;
+    out[3] = rel;
+    out[4] = ms;
+    out[5] = rel0;
 }
 
 }  // namespace cfg

@@ -12,38 +12,49 @@ namespace cfg
 {
 
 __device__ __forceinline__ double inv_diag_cg(double d) { return (fabs(d) > 1e-300) ? 1.0 / d : 1.0; }
+__device__ __forceinline__ float inv_diag_cg(float d) { return (fabs(static_cast<double>(d)) > 1e-300) ? 1.0f / d : 1.0f; }
 __device__ __forceinline__ double inv_diag_bicg(double d) { return (d > 1e-300) ? 1.0 / d : 1.0; }
 
+/// the residual norm of the stopping test from |r|inf and sum r^2
+__device__ __forceinline__ double resid_norm(const SolveState* st, double inf, double sumsq)
+{
+    return st->normType ? sqrt(sumsq) : inf;
+}
+
 // ------------------------------- CG ---------------------------------------
+// T is the type of the matrix values and vectors (double: the reference's
+// FP64 solve; float: the inner solves of the mixed-precision refinement).
+// Dot products and norms accumulate in double either way.
 
 /// r = b - A x; z = D^-1 r; p = z; initial residual, |b|, and r.z.
-template <int W>
-__global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __restrict__ val,
-                                                 const double* __restrict__ diag, const double* __restrict__ b,
-                                                 const double* __restrict__ x, double* __restrict__ r,
-                                                 double* __restrict__ p, double* partials, SolveState* st)
+template <int W, class T = double>
+__global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const T* __restrict__ val, const T* __restrict__ diag,
+                                                 const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r,
+                                                 T* __restrict__ p, double* partials, SolveState* st)
 {
     double mx[3] = {0.0, 0.0, 0.0};  // |r|, |b|, nan flag
-    double sm[1] = {0.0};            // r.z
-    const double* xs[1] = {x};
+    double sm[3] = {0.0, 0.0, 0.0};  // r.z, r.r, b.b
+    const T* xs[1] = {x};
     FOR_ROWS(c, A.n)
     {
         double y[1];
-        spmv_row<W, 1>(A, val, c, xs, y);
-        const double bi = b[c];
-        const double ri = bi - y[0];
+        spmv_row<W, 1, T>(A, val, c, xs, y);
+        const T bi = b[c];
+        const T ri = static_cast<T>(static_cast<double>(bi) - y[0]);
         r[c] = ri;
-        const double zi = inv_diag_cg(diag[c]) * ri;
+        const T zi = inv_diag_cg(diag[c]) * ri;
         p[c] = zi;
-        if (isnan(ri)) mx[2] = 1.0;
-        mx[0] = smax(mx[0], fabs(ri));
-        if (isnan(bi)) mx[2] = 1.0;
-        mx[1] = smax(mx[1], fabs(bi));
-        sm[0] += ri * zi;
+        if (isnan(static_cast<double>(ri))) mx[2] = 1.0;
+        mx[0] = smax(mx[0], fabs(static_cast<double>(ri)));
+        if (isnan(static_cast<double>(bi))) mx[2] = 1.0;
+        mx[1] = smax(mx[1], fabs(static_cast<double>(bi)));
+        sm[0] += static_cast<double>(ri * zi);
+        sm[1] += static_cast<double>(ri) * static_cast<double>(ri);
+        sm[2] += static_cast<double>(bi) * static_cast<double>(bi);
     }
     block_max<3>(mx);
     __syncthreads();
-    block_sum<1>(sm);
+    block_sum<3>(sm);
     const int G = gridDim.x;
     if (threadIdx.x == 0)
     {
@@ -51,17 +62,19 @@ __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __restric
         partials[G + blockIdx.x] = mx[1];
         partials[2 * G + blockIdx.x] = mx[2];
         partials[3 * G + blockIdx.x] = sm[0];
+        partials[4 * G + blockIdx.x] = sm[1];
+        partials[5 * G + blockIdx.x] = sm[2];
     }
     if (!last_block(&st->ticket[0])) return;
-    double fm[3], fs[1];
+    double fm[3], fs[3];
     final_max<3>(partials, G, fm);
     __syncthreads();
-    final_sum<1>(partials + 3 * G, G, fs);
+    final_sum<3>(partials + 3 * G, G, fs);
     if (threadIdx.x == 0)
     {
         st->ticket[0] = 0;
-        const double init = fm[2] > 0 ? NAN : fm[0];
-        const double bn = smax(fm[1], 1e-300);
+        const double init = fm[2] > 0 ? NAN : resid_norm(st, fm[0], fs[1]);
+        const double bn = smax(st->normType ? sqrt(fs[2]) : fm[1], 1e-300);
         st->init[0] = init;
         st->bnorm[0] = bn;
         st->it[0] = 0;
@@ -84,19 +97,20 @@ __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const double* __restric
 }
 
 /// Ap = A p and p.Ap; breakdown test and alpha (Matrix.cpp:187-194).
-template <int W>
-__global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const double* __restrict__ val, const double* __restrict__ p,
-                                                 double* __restrict__ Ap, double* partials, SolveState* st)
+template <int W, class T = double>
+__global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const T* __restrict__ val, const T* __restrict__ p,
+                                                 T* __restrict__ Ap, double* partials, SolveState* st)
 {
     if (st->allDone) return;
     double sm[1] = {0.0};
-    const double* xs[1] = {p};
+    const T* xs[1] = {p};
     FOR_ROWS(c, A.n)
     {
         double y[1];
-        spmv_row<W, 1>(A, val, c, xs, y);
-        Ap[c] = y[0];
-        sm[0] += p[c] * y[0];
+        spmv_row<W, 1, T>(A, val, c, xs, y);
+        const T ay = static_cast<T>(y[0]);
+        Ap[c] = ay;
+        sm[0] += static_cast<double>(p[c] * ay);
     }
     block_sum<1>(sm);
     if (threadIdx.x == 0) partials[blockIdx.x] = sm[0];
@@ -121,46 +135,49 @@ __global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const double* __restric
     }
 }
 
-/// x += alpha p; r -= alpha Ap; |r|inf test; z = D^-1 r; beta (Matrix.cpp:195-217).
-static __global__ void __launch_bounds__(TPB) k_cg_update(int n, const double* __restrict__ diag, const double* __restrict__ p,
-                                                   const double* __restrict__ Ap, double* __restrict__ x,
-                                                   double* __restrict__ r, double* partials, SolveState* st)
+/// x += alpha p; r -= alpha Ap; residual test; z = D^-1 r; beta (Matrix.cpp:195-217).
+template <class T = double>
+__global__ void __launch_bounds__(TPB) k_cg_update(int n, const T* __restrict__ diag, const T* __restrict__ p,
+                                                   const T* __restrict__ Ap, T* __restrict__ x, T* __restrict__ r,
+                                                   double* partials, SolveState* st)
 {
     if (st->allDone) return;
-    const double alpha = st->alpha[0];
+    const T alpha = static_cast<T>(st->alpha[0]);
     double mx[2] = {0.0, 0.0};
-    double sm[1] = {0.0};
+    double sm[2] = {0.0, 0.0};
     FOR_ROWS(c, n)
     {
         x[c] = x[c] + alpha * p[c];
-        const double ri = r[c] - alpha * Ap[c];
+        const T ri = r[c] - alpha * Ap[c];
         r[c] = ri;
-        if (isnan(ri)) mx[1] = 1.0;
-        mx[0] = smax(mx[0], fabs(ri));
-        const double zi = inv_diag_cg(diag[c]) * ri;
-        sm[0] += ri * zi;
+        if (isnan(static_cast<double>(ri))) mx[1] = 1.0;
+        mx[0] = smax(mx[0], fabs(static_cast<double>(ri)));
+        const T zi = inv_diag_cg(diag[c]) * ri;
+        sm[0] += static_cast<double>(ri * zi);
+        sm[1] += static_cast<double>(ri) * static_cast<double>(ri);
     }
     block_max<2>(mx);
     __syncthreads();
-    block_sum<1>(sm);
+    block_sum<2>(sm);
     const int G = gridDim.x;
     if (threadIdx.x == 0)
     {
         partials[blockIdx.x] = mx[0];
         partials[G + blockIdx.x] = mx[1];
         partials[2 * G + blockIdx.x] = sm[0];
+        partials[3 * G + blockIdx.x] = sm[1];
     }
     if (!last_block(&st->ticket[0])) return;
-    double fm[2], fs[1];
+    double fm[2], fs[2];
     final_max<2>(partials, G, fm);
     __syncthreads();
-    final_sum<1>(partials + 2 * G, G, fs);
+    final_sum<2>(partials + 2 * G, G, fs);
     if (threadIdx.x == 0)
     {
         st->ticket[0] = 0;
         const int it = st->it[0] + 1;
         st->it[0] = it;
-        const double fin = fm[1] > 0 ? NAN : fm[0];
+        const double fin = fm[1] > 0 ? NAN : resid_norm(st, fm[0], fs[1]);
         st->fin[0] = fin;
         if (fin / st->bnorm[0] < st->tol)
         {
@@ -186,11 +203,12 @@ static __global__ void __launch_bounds__(TPB) k_cg_update(int n, const double* _
 }
 
 /// p = z + beta p.
-static __global__ void __launch_bounds__(TPB) k_cg_p(int n, const double* __restrict__ diag, const double* __restrict__ r,
-                                              double* __restrict__ p, const SolveState* st)
+template <class T = double>
+__global__ void __launch_bounds__(TPB) k_cg_p(int n, const T* __restrict__ diag, const T* __restrict__ r,
+                                              T* __restrict__ p, const SolveState* st)
 {
     if (st->allDone) return;
-    const double beta = st->beta[0];
+    const T beta = static_cast<T>(st->beta[0]);
     FOR_ROWS(c, n) p[c] = inv_diag_cg(diag[c]) * r[c] + beta * p[c];
 }
 

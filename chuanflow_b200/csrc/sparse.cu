@@ -158,8 +158,8 @@ void Ctx::sparseSolve(int device, int64_t n64, const int64_t* rs, const int64_t*
                 for (int k = 0; k < m; ++k)
                 {
                     k_cg_spmv<W><<<GS, TPB, 0, s>>>(A, dVal, p, Ap, partials, st);
-                    k_cg_update<<<GS, TPB, 0, s>>>(n, dDiag, p, Ap, dx, r, partials, st);
-                    k_cg_p<<<GS, TPB, 0, s>>>(n, dDiag, r, p, st);
+                    k_cg_update<double><<<GS, TPB, 0, s>>>(n, dDiag, p, Ap, dx, r, partials, st);
+                    k_cg_p<double><<<GS, TPB, 0, s>>>(n, dDiag, r, p, st);
                 }
                 CFG_CUDA(cudaGetLastError());
                 launched += m;

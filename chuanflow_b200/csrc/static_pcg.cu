@@ -238,8 +238,8 @@ extern "C" int cfg_pcg_solve_static(int32_t device, int64_t n64, const int32_t* 
             for (int k = 0; k < m; ++k)
             {
                 k_static_cg_spmv<<<G, TPB, 0, s>>>(n, rowStart, cols, vals, p, Ap, partials, st);
-                k_cg_update<<<G, TPB, 0, s>>>(n, d, p, Ap, x, r, partials, st);
-                k_cg_p<<<G, TPB, 0, s>>>(n, d, r, p, st);
+                k_cg_update<double><<<G, TPB, 0, s>>>(n, d, p, Ap, x, r, partials, st);
+                k_cg_p<double><<<G, TPB, 0, s>>>(n, d, r, p, st);
             }
             CFG_CUDA(cudaGetLastError());
             launched += m;

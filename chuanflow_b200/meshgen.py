@@ -1,0 +1,52 @@
+"""Synthetic meshes of the study cases that the reference has no generator
+for: a seeded Delaunay tetrahedralisation of a jittered lattice.
+
+The tetrahedra come from scipy.spatial.Delaunay (library code, on the host);
+the polyMesh is then built by the library exactly as the reference's gmsh
+reader would build it from the same elements (cfg_mesh_from_cells)."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def jittered_lattice(n, jitter=0.1, seed=0, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """(n+1)^3 lattice points of the box, each moved by a seeded uniform
+    offset in [-jitter h, jitter h) along every axis it is free to move in:
+    boundary points stay on their planes (and edge points on their edges),
+    which also keeps Delaunay from leaving flat tetrahedra on the faces."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    g = [lo[a] + (hi[a] - lo[a]) * np.arange(n + 1) / n for a in range(3)]
+    z, y, x = np.meshgrid(g[2], g[1], g[0], indexing="ij")
+    pts = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    idx = np.stack(np.meshgrid(np.arange(n + 1), np.arange(n + 1), np.arange(n + 1), indexing="ij"), -1)
+    k, j, i = idx[..., 0].ravel(), idx[..., 1].ravel(), idx[..., 2].ravel()
+    free = np.stack([(i > 0) & (i < n), (j > 0) & (j < n), (k > 0) & (k < n)], 1)
+    h = (hi - lo) / n
+    rng = np.random.default_rng(seed)
+    pts += np.where(free, (rng.random(pts.shape) * 2.0 - 1.0) * jitter * h, 0.0)
+    return pts
+
+
+def delaunay_tets(points, min_volume_fraction=1e-9):
+    """Delaunay tetrahedra of the points, positively oriented, without the
+    flat ones Qhull may leave on planar boundaries."""
+    from scipy.spatial import Delaunay
+    tri = Delaunay(points)
+    t = np.ascontiguousarray(tri.simplices, np.int64)
+    p = points[t]
+    vol = np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0]) / 6.0
+    flip = vol < 0
+    t[flip, 0], t[flip, 1] = t[flip, 1].copy(), t[flip, 0].copy()
+    keep = np.abs(vol) > min_volume_fraction * np.abs(vol).mean()
+    return t[keep]
+
+
+def tet_mesh(n, jitter=0.1, seed=0):
+    """PolyMesh of the Delaunay tetrahedralisation of an (n+1)^3 jittered
+    lattice in the unit box (about 6 n^3 cells)."""
+    from ._capi import PolyMesh
+    pts = jittered_lattice(n, jitter, seed)
+    tets = delaunay_tets(pts)
+    off = np.arange(0, 4 * tets.shape[0] + 1, 4, dtype=np.int64)
+    return PolyMesh.from_cells(pts, np.full(tets.shape[0], 4, np.int32), off, tets.ravel()), pts, tets

@@ -141,6 +141,15 @@ int cfg_mesh_create(const double* points, int64_t n_points, const int64_t* face_
 int cfg_mesh_block(const double min[3], const double max[3], int64_t nx, int64_t ny, int64_t nz,
                    const char* const* side_names, const char* const* side_types, cfg_mesh** out);
 
+/* The polyMesh GmshMesh::fromFile builds from volume elements
+ * (src/3d/src/mesh/gmshMesh.cpp:578-760): tetrahedra (type 4), hexahedra (5)
+ * and prisms (6) with gmsh's local node order; faces recovered cell by cell
+ * and deduplicated, internal faces owned by the lower cell, boundary faces
+ * grouped into patches named after the bounding-box plane they lie on (the
+ * reader's rule for a file without surface groups), type "wall". */
+int cfg_mesh_from_cells(const double* points, int64_t n_points, const int32_t* cell_types,
+                        const int64_t* cell_offsets, const int64_t* cell_verts, int64_t n_cells, cfg_mesh** out);
+
 /* polyMesh::movePoints (polyMesh.cpp:320-329): same topology, new points,
  * geometry recomputed. */
 int cfg_mesh_move_points(cfg_mesh* mesh, const double* points, int64_t n_points);
@@ -226,6 +235,40 @@ int cfg_kernel_stats(const cfg_ctx* ctx, double out[6]);
 int cfg_sparse_solve(const cfg_ctx* ctx_or_null, int32_t device, int64_t n, const int64_t* row_start,
                      const int64_t* cols, const double* vals, const double* b, double* x, double tol,
                      int32_t max_iter, int32_t method, cfg_solver_report* report);
+
+/* ---- the pressure-Poisson solve on its own (no reference counterpart) ---- */
+
+enum cfg_poisson_method
+{
+    CFG_POISSON_JACOBI64 = 0,  /* FP64 Jacobi-PCG, the reference's solver */
+    CFG_POISSON_DIC64 = 1,     /* FP64 multicolour-DIC PCG */
+    CFG_POISSON_IR32 = 2       /* FP32 DIC-PCG corrections inside FP64 iterative refinement */
+};
+
+typedef struct cfg_poisson_report
+{
+    int64_t inner_iterations;   /* PCG iterations, summed over refinement steps */
+    int32_t outer_iterations;   /* refinement steps (1 for the FP64 methods) */
+    int32_t converged;
+    double true_rel_residual;   /* |b - A x|2 / |b|2 recomputed in FP64 */
+    double device_ms;           /* CUDA-event time of the solve on the context's stream */
+    double initial_rel_residual;
+} cfg_poisson_report;
+
+/* The context's pressure matrix set to the orthogonal part of laplacianFace
+ * with unit face coefficient (laplacianScheme.cpp:176-215, sign -1) under
+ * the patches' p conditions, plus a reference cell (-1: none) pinned as
+ * OpenFOAM's fvMatrix::setReference does; its FP32 copy and both DIC
+ * factors are prepared. */
+int cfg_poisson_setup(cfg_ctx* ctx, int64_t ref_cell);
+
+/* Solves that system for host b to |b - A x|2 / |b|2 <= rel_tol (FP64, true
+ * residual); x holds the initial guess and receives the solution.  For
+ * CFG_POISSON_IR32 each refinement step solves for the correction in FP32
+ * to inner_rel_tol (at most inner_max_iter iterations); max_iter bounds all
+ * PCG iterations. */
+int cfg_poisson_solve(cfg_ctx* ctx, const double* b, double* x, int32_t method, double rel_tol, int32_t max_iter,
+                      int32_t inner_max_iter, double inner_rel_tol, cfg_poisson_report* report);
 
 /* ---- diagnostics used by the parity tests (no reference counterpart) ----- */
 

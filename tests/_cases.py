@@ -230,3 +230,16 @@ def test_matrix(n, rng, symmetric):
             vals.append(rows[i][j])
         rs.append(len(cols))
     return np.array(rs, np.int64), np.array(cols, np.int64), np.array(vals, np.float64)
+
+
+def write_msh22(path, points, cells, cell_type=4):
+    """A gmsh 2.2 ASCII file of volume elements only (no surface groups), the
+    input of the reference's GmshMesh::fromFile."""
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(points))
+        for i, p in enumerate(points):
+            f.write("%d %.17g %.17g %.17g\n" % (i + 1, p[0], p[1], p[2]))
+        f.write("$EndNodes\n$Elements\n%d\n" % len(cells))
+        for e, c in enumerate(cells):
+            f.write("%d %d 2 1 1 %s\n" % (e + 1, cell_type, " ".join(str(int(v) + 1) for v in c)))
+        f.write("$EndElements\n")

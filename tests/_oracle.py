@@ -102,7 +102,11 @@ class OMesh:
         self.points = np.ascontiguousarray(self.points, dtype=np.float64).reshape(-1, 3)
         for k in ("face_offsets", "face_verts", "owner", "neighbour", "patch_start", "patch_size"):
             setattr(self, k, np.ascontiguousarray(getattr(self, k), dtype=np.int64))
-        self.nC = int(self.owner.max()) + 1 if self.owner.size else 0
+        # the reference counts cells from owners alone (polyMesh.cpp:23), which
+        # overruns its cell arrays when the last cell owns no face; count the
+        # neighbours too, as chuanflow_b200 does
+        self.nC = max(int(self.owner.max()) + 1 if self.owner.size else 0,
+                      int(self.neighbour.max()) + 1 if self.neighbour.size else 0)
         self.nF = self.owner.size
         self.nInt = self.neighbour.size
         self.V = np.zeros(self.nC)

@@ -10,6 +10,8 @@ Fixtures (small .npz files):
                            through its gmsh reader: addressing, geometry, weights,
                            and fvc::grad of its two test fields under all schemes
   mesh_hex41.npz           the orthogonal hex cube (tests/meshes/cubeHex_41.msh), same
+  mesh_delaunay.npz        a seeded Delaunay tetrahedralisation (chuanflow_b200.meshgen) written
+                           as gmsh 2.2 and read by the reference's gmsh reader
   simple_cavity.npz        jittered 6x5x4 lid-driven cavity: 3 SIMPLE iterations
   simple_channel.npz       10x6x5 inlet/outlet channel: 4 SIMPLE iterations
   eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
@@ -142,6 +144,19 @@ def main():
     mesh_npz("mesh_block_2x2x2.npz", "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\n")
     mesh_npz("mesh_tets22.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeTets_22.msh"; }}\n', grad_fields=True)
     mesh_npz("mesh_hex41.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeHex_41.msh"; }}\n', grad_fields=True)
+
+    sys.path.insert(0, ROOT)
+    from chuanflow_b200 import meshgen
+    pts = meshgen.jittered_lattice(6, 0.1, 5)
+    tets = meshgen.delaunay_tets(pts)
+    with tempfile.TemporaryDirectory() as td:
+        mp = os.path.join(td, "m.msh")
+        K.write_msh22(mp, pts, tets)
+        mesh_npz("mesh_delaunay.npz", f'mesh {{ format gmsh; file "{mp}"; }}\n')
+    d = dict(np.load(os.path.join(HERE, "mesh_delaunay.npz")))
+    d["tets"] = tets
+    d["lattice_points"] = pts
+    np.savez_compressed(os.path.join(HERE, "mesh_delaunay.npz"), **d)
 
     cav = K.cavity_case(6, 5, 4)
     simple_npz("simple_cavity.npz", cav, K.cavity_dict(6, 5, 4, iters=3), cav.mesh.points)

@@ -134,3 +134,30 @@ def test_simple_cavity_dic_matches_oracle(cells, jitter):
     assert res.iterations == r0.iterations
     assert abs(res.p_inner_iterations - r0.pItersTotal) <= 2 * 6 * 2
     assert rel(U, U0) < REL_TOL and rel(p, p0) < REL_TOL and rel(phi, phi0) < REL_TOL
+
+
+@pytest.mark.parametrize("method", ["jacobi64", "dic64", "ir32"])
+def test_poisson_solves_match_oracle(method):
+    """The pressure-Poisson study system (unit face coefficient, Neumann,
+    one reference cell) on a Delaunay tet mesh: every method reaches the
+    requested FP64 true residual and the oracle's FP64 solution."""
+    from chuanflow_b200 import meshgen
+    mesh, pts, tets = meshgen.tet_mesh(10, 0.1, 2)
+    import chuanflow_b200 as cf
+    case = cf.SimpleCase(mesh)
+    case.poisson_setup(ref_cell=0)
+    rng = np.random.default_rng(1)
+    b = rng.normal(size=mesh.n_cells)
+    b -= b.mean()
+    x, rep = case.poisson_solve(b, method, tol=1e-10)
+    assert rep["converged"] and rep["true_rel_residual"] <= 1e-10
+    a = mesh.addressing()
+    om = O.OMesh(a["points"], a["face_offsets"], a["face_verts"], a["owner"], a["neighbour"],
+                 [p[0] for p in mesh.patches], [p[1] for p in mesh.patches], [p[2] for p in mesh.patches],
+                 [p[3] for p in mesh.patches])
+    oc = O.Case(om, u_type=["fixedValue"] * mesh.n_patches, u_value=[(0, 0, 0)] * mesh.n_patches,
+                p_type=["zeroGradient"] * mesh.n_patches, p_value=[0] * mesh.n_patches, nu=1.0)
+    oc.p_ref_cell = 0
+    rs, cols, vals = oc.pressure_csr(np.ones(mesh.n_faces))
+    x0, r0 = O.solve("cg", rs, cols, vals, b, np.zeros(mesh.n_cells), 1e-15, 20000)
+    assert rel(x, x0) < 1e-7, rel(x, x0)

@@ -86,3 +86,39 @@ def test_mesh_errors_follow_reference():
     with pytest.raises(cf.CfgError, match="cell counts must be positive"):
         cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (0, 1, 1))
     assert nI == 1
+
+
+def test_mesh_from_cells_matches_reference_gmsh_reader(golden):
+    """The reference's gmsh reader on a Delaunay tetrahedralisation and
+    cfg_mesh_from_cells on the same elements give the same polyMesh."""
+    g = golden("mesh_delaunay.npz")
+    tets = g["tets"]
+    off = np.arange(0, 4 * tets.shape[0] + 1, 4)
+    m = cf.PolyMesh.from_cells(g["lattice_points"], np.full(tets.shape[0], 4, np.int32), off, tets.ravel())
+    a = m.addressing()
+    for k in ("face_offsets", "face_verts", "owner", "neighbour", "points"):
+        assert np.array_equal(a[k], g[k]), k
+    geo = m.geometry()
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(geo[k], g[k]), k
+    assert [p[0] for p in m.patches] == [str(x) for x in g["patch_names"]]
+
+
+def test_mesh_from_cells_hex_and_prism():
+    """A 2x1x1 hex pair and its prism split: face counts and volumes."""
+    pts = np.array([[x, y, z] for z in (0, 1) for y in (0, 1) for x in (0, 1, 2)], float)
+    P = lambda x, y, z: x + 3 * (y + 2 * z)
+    hexes = [[P(0, 0, 0), P(1, 0, 0), P(1, 1, 0), P(0, 1, 0), P(0, 0, 1), P(1, 0, 1), P(1, 1, 1), P(0, 1, 1)],
+             [P(1, 0, 0), P(2, 0, 0), P(2, 1, 0), P(1, 1, 0), P(1, 0, 1), P(2, 0, 1), P(2, 1, 1), P(1, 1, 1)]]
+    m = cf.PolyMesh.from_cells(pts, [5, 5], [0, 8, 16], np.ravel(hexes))
+    assert (m.n_cells, m.n_internal_faces, m.n_boundary_faces) == (2, 1, 10)
+    assert np.allclose(m.geometry()["V"], 1.0)
+    cube = np.array([[x, y, z] for z in (0, 1) for y in (0, 1) for x in (0, 1)], float)
+    Q = lambda x, y, z: x + 2 * (y + 2 * z)
+    prisms = [[Q(0, 0, 0), Q(1, 0, 0), Q(0, 1, 0), Q(0, 0, 1), Q(1, 0, 1), Q(0, 1, 1)],
+              [Q(1, 0, 0), Q(1, 1, 0), Q(0, 1, 0), Q(1, 0, 1), Q(1, 1, 1), Q(0, 1, 1)]]
+    m = cf.PolyMesh.from_cells(cube, [6, 6], [0, 6, 12], np.ravel(prisms))
+    assert (m.n_cells, m.n_internal_faces) == (2, 1)
+    assert np.allclose(m.geometry()["V"], 0.5)
+    with pytest.raises(cf.CfgError, match="not tet"):
+        cf.PolyMesh.from_cells(pts, [7], [0, 5], [0, 1, 2, 3, 4])
