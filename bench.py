@@ -7,7 +7,7 @@ A step is one SIMPLE outer iteration (momentum predictor with its non-
 orthogonal passes, predictor flux, pressure equation with its passes, flux
 correction, relaxed updates) over the whole 128^3 mesh, on fields that stay
 resident in HBM between steps.  N > 1 runs independent replicas, one per GPU
-(the path does not shard in the reference's sense), launched
+(one case per GPU: the SIMPLE loop is not split across GPUs), launched
 by torchrun; value is the whole job's cells*iterations / max-over-ranks time.
 
 The workload: 128^3 = 2,097,152 hex cells in the unit box, interior mesh
@@ -219,6 +219,9 @@ def main():
     ap.add_argument("--cpu-sample-cells", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--p-precond", default="Jacobi", choices=["Jacobi", "DIC"])
+    ap.add_argument("--profile", action="store_true",
+                    help="run --steps outer iterations from the initial state with no warm-up, timing or "
+                         "baselines: the command line the ncu captures run")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup()
     if args.impl == "reference":
@@ -230,6 +233,12 @@ def main():
     n = args.cells
     mesh, case, ctl = make_case(n, local, args.p_precond)
     ncell = mesh.n_cells
+    if args.profile:
+        for _ in range(args.steps):
+            r = case.solve(ctl)
+        print(json.dumps({"profile": workload_config(n)["workload"], "steps": args.steps,
+                          "u_inner": r.u_inner_iterations, "p_inner": r.p_inner_iterations}))
+        return
     for _ in range(max(3, args.warmup)):
         case.solve(ctl)
     # the state every leg starts from: the timed, end-to-end and kernel-timing
