@@ -107,7 +107,10 @@ private:
     bool ownStream_ = false;
     int G_ = 0;        // grid of row kernels
     int GF_ = 0;       // grid of face kernels
-    int GS_ = 0;       // grid of solver kernels (RPT rows per thread)
+    int GS_ = 0;       // grid of solver kernels (rowGrid(nC))
+    int sms_ = 0;
+    int rowBlocksPerSM_ = 4;  // 0: RPT rows per thread; k > 0: at most k blocks per SM
+    int rowGrid(int rows) const;
     int maxW_ = 0;     // longest matrix row
     int nSlicesEntries_ = 0;  // matrix SELL entries
     int nSlices_ = 0;

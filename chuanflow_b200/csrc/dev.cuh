@@ -75,34 +75,56 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket)
     return amLast;
 }
 
+/// The last block's pass over the per-block partials: for each of the NV
+/// arrays in turn, every thread loads FU of its values before the first
+/// add, so an array costs ceil(G / (FU * TPB)) memory latencies rather than
+/// G / TPB, without holding NV * FU values in registers.  Sums combine in a
+/// fixed order (pairwise within a thread, then the block tree), so a given
+/// grid size always gives the same bits.
+constexpr int FU = 8;
+
+__device__ __forceinline__ double partial_sum(const double* a, int G)
+{
+    double v = 0.0;
+    for (int b0 = threadIdx.x; b0 < G; b0 += FU * TPB)
+    {
+        double w[FU];
+#pragma unroll
+        for (int u = 0; u < FU; ++u) w[u] = b0 + u * TPB < G ? __ldcg(a + b0 + u * TPB) : 0.0;
+        v += ((w[0] + w[1]) + (w[2] + w[3])) + ((w[4] + w[5]) + (w[6] + w[7]));
+    }
+    return v;
+}
+static_assert(FU == 8, "partial_sum's pairwise tree is written for FU = 8");
+
+__device__ __forceinline__ double partial_max(const double* a, int G)
+{
+    double v = 0.0;
+    for (int b0 = threadIdx.x; b0 < G; b0 += FU * TPB)
+    {
+        double w[FU];
+#pragma unroll
+        for (int u = 0; u < FU; ++u) w[u] = b0 + u * TPB < G ? __ldcg(a + b0 + u * TPB) : 0.0;
+#pragma unroll
+        for (int u = 0; u < FU; ++u) v = (v < w[u]) ? w[u] : v;
+    }
+    return v;
+}
+
 /// Sum of NV partial arrays (layout q*G + block) in fixed order; thread 0.
 template <int NV>
 __device__ __forceinline__ void final_sum(const double* partials, int G, double (&v)[NV])
 {
-#pragma unroll
-    for (int q = 0; q < NV; ++q)
-    {
-        double a = 0.0;
-        for (int b = threadIdx.x; b < G; b += TPB) a += __ldcg(partials + q * G + b);
-        v[q] = a;
-    }
+#pragma unroll 1
+    for (int q = 0; q < NV; ++q) v[q] = partial_sum(partials + q * G, G);
     block_sum<NV>(v);
 }
 
 template <int NV>
 __device__ __forceinline__ void final_max(const double* partials, int G, double (&v)[NV])
 {
-#pragma unroll
-    for (int q = 0; q < NV; ++q)
-    {
-        double a = 0.0;
-        for (int b = threadIdx.x; b < G; b += TPB)
-        {
-            const double w = __ldcg(partials + q * G + b);
-            a = (a < w) ? w : a;
-        }
-        v[q] = a;
-    }
+#pragma unroll 1
+    for (int q = 0; q < NV; ++q) v[q] = partial_max(partials + q * G, G);
     block_max<NV>(v);
 }
 

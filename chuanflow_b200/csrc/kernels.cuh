@@ -374,14 +374,12 @@ __device__ __forceinline__ void spmv_row(const DMat& A, const T* __restrict__ va
     }
 }
 
-/// Rows handled per thread by the solver kernels: RPT rows TPB apart, so a
-/// warp's rows stay contiguous and each thread has two rows' loads in flight.
+/// The solver kernels' row loop: a grid-stride loop, so a warp's rows stay
+/// contiguous and the grid can be sized for the GPU rather than the system
+/// (fewer blocks means fewer per-block reduction epilogues and partials).
+/// RPT is the rows per thread of the default grid, ceil(n / (RPT * TPB)).
 constexpr int RPT = 2;
-#define FOR_ROWS(c, n)                                                                                \
-    _Pragma("unroll") for (int rr_ = 0; rr_ < ::cfg::RPT; ++rr_) if (const int c =                   \
-                                                                       (blockIdx.x * ::cfg::RPT + rr_) * \
-                                                                           ::cfg::TPB +             \
-                                                                       threadIdx.x;                 \
-                                                                   c < (n))
+#define FOR_ROWS(c, n) \
+    for (int c = blockIdx.x * ::cfg::TPB + threadIdx.x; c < (n); c += gridDim.x * ::cfg::TPB)
 
 }  // namespace cfg

@@ -614,7 +614,9 @@ void Ctx::buildDevice()
     int sms = 0;
     CFG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
     G_ = std::max(1, std::min((nC + TPB - 1) / TPB, sms * 8));
-    GS_ = std::max(1, (nC + RPT * TPB - 1) / (RPT * TPB));
+    sms_ = sms;
+    if (const char* e = std::getenv("CHUANFLOW_ROW_BLOCKS_PER_SM")) rowBlocksPerSM_ = std::max(0, std::atoi(e));
+    GS_ = rowGrid(nC);
     GF_ = std::max(1, std::min((nF + TPB - 1) / TPB, sms * 8));
 
     // ---- per-face geometry derived on the host in the reference's order ----
@@ -820,7 +822,7 @@ void Ctx::buildDevice()
                 uStart.push_back(static_cast<int>(uCol.size()));
             }
             slice += nSl;
-            pOff += std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB));
+            pOff += rowGrid(ph.cnt);
             dicPhase_.push_back(ph);
         }
         dicPartials_ = pOff + 1;
@@ -1397,10 +1399,12 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     }
 }
 
-namespace
+/// Blocks for a grid-stride row loop over `rows` rows.
+int Ctx::rowGrid(int rows) const
 {
-inline int phaseGrid(const DicPhase& ph) { return std::max(1, (ph.cnt + RPT * TPB - 1) / (RPT * TPB)); }
-}  // namespace
+    if (rowBlocksPerSM_ <= 0) return std::max(1, (rows + RPT * TPB - 1) / (RPT * TPB));
+    return std::max(1, std::min((rows + TPB - 1) / TPB, sms_ * rowBlocksPerSM_));
+}
 
 template <class T>
 void Ctx::dicSetupT(DDicT<T>& D, const double* vals, const T* diag)
@@ -1410,7 +1414,7 @@ void Ctx::dicSetupT(DDicT<T>& D, const double* vals, const T* diag)
     launchCheck("dic_gather");
     for (const DicPhase& ph : dicPhase_)
     {
-        k_dic_factor<T><<<phaseGrid(ph), TPB, 0, stream_>>>(D, ph, diag);
+        k_dic_factor<T><<<rowGrid(ph.cnt), TPB, 0, stream_>>>(D, ph, diag);
         launchCheck("dic_factor");
     }
 }
@@ -1420,7 +1424,7 @@ void Ctx::dicApplyT(const DDicT<T>& D, const T* r, T* z)
 {
     const int C = D.nColours;
     for (int c = 0; c < C; ++c)
-        k_dic_fwd<T><<<phaseGrid(dicPhase_[c]), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == C - 1, partials_, st_);
+        k_dic_fwd<T><<<rowGrid(dicPhase_[c].cnt), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == C - 1, partials_, st_);
     if (C == 1)
     {
         // no backward phase: a one-block final reduction of the forward partials
@@ -1428,7 +1432,7 @@ void Ctx::dicApplyT(const DDicT<T>& D, const T* r, T* z)
         k_dic_bwd<T><<<1, TPB, 0, stream_>>>(D, none, r, z, 1, dicPartials_, partials_, st_);
     }
     for (int c = C - 2; c >= 0; --c)
-        k_dic_bwd<T><<<phaseGrid(dicPhase_[c]), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == 0,
+        k_dic_bwd<T><<<rowGrid(dicPhase_[c].cnt), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == 0,
                                                                    c == 0 ? dicPartials_ - 1 : 0, partials_, st_);
     launchCheck("dic_apply", C == 1 ? 2 : 2 * C - 1);
 }
