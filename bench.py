@@ -43,13 +43,62 @@ SIDES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
 METRIC = "SIMPLE cell-iter/s at 2M cells; time to 1e-8 p-residual, learned vs plain PCG"
 
 
-def workload_config(n):
+def workload_config(n, precond="DIC"):
     return {"workload": f"lid-driven cavity {n}^3 hex ({n ** 3} cells), interior points jittered +-10% "
                         f"(seed {SEED}), Re 400, upwind/corrected/corrected, nonOrth 1, relaxU 0.7 relaxP 0.3 "
-                        f"pRelaxStart 0.02, pressure Jacobi-PCG tol 1e-8 maxIter 2000, pRefCell 0",
+                        f"pRelaxStart 0.02, pressure {precond}-PCG tol 1e-8 maxIter 2000, pRefCell 0",
             "cells": n ** 3, "step": "one SIMPLE outer iteration",
             "l2": "inputs larger than L2 (about 1.3 GB of fields, matrices and mesh resident in HBM)",
             "precision": "FP64 throughout"}
+
+
+KERNEL_NAMES = {
+    "cg_spmv": "k_cg_spmv (pressure PCG: SELL-32 SpMV + p.Ap)",
+    "cg_update": "k_cg_update (pressure PCG: x, r update + norms + r.z)",
+    "cg_p": "k_cg_p (pressure PCG: search direction)",
+    "bi_p": "k_bi_p (momentum BiCGStab, 3 components: p, z update)",
+    "bi_spmv1": "k_bi_spmv1 (momentum BiCGStab, 3 components: v = A z + r0.v)",
+    "bi_s": "k_bi_s (momentum BiCGStab, 3 components: x, s, s^ update + |s|)",
+    "bi_spmv2": "k_bi_spmv2 (momentum BiCGStab, 3 components: t = A s^ + t.t, t.s)",
+    "bi_x": "k_bi_x (momentum BiCGStab, 3 components: x, r update + |r| + r0.r)",
+    "dic_apply": "k_dic_fwd/k_dic_bwd (multicolour DIC z = M^-1 r, all colour phases)",
+}
+
+
+def kernel_bytes(N, F, s=8, i=4):
+    """Algorithmic bytes of one launch of each solver kernel: every array
+    counted once per read and once per write, gathers as one N-stream.
+    The three momentum components share one matrix read."""
+    spmv_sym = 3 * s * N + s * F + 2 * i * F       # x in, y out, diag + one coefficient per face, indices
+    spmv3 = 10 * s * N + 2 * s * F + 2 * i * F     # 3 x in, 3 y out, 3 dot partners, diag, both coefficients
+    return {"cg_spmv": spmv_sym, "cg_update": 7 * s * N, "cg_p": 4 * s * N,
+            "bi_p": 16 * s * N, "bi_spmv1": spmv3, "bi_s": 22 * s * N, "bi_spmv2": spmv3, "bi_x": 21 * s * N,
+            "dic_apply": 3 * s * N + 2 * (s * F + 2 * i * F)}
+
+
+def simple_step_bytes(N, F, Fb, n_orth, it_u, it_p, precond, s=8, i=4):
+    """Algorithmic bytes of one SIMPLE outer iteration: the fixed face and
+    cell passes plus the inner solves, per component-iteration of BiCGStab
+    (2 SpMVs with their own matrix read + 20 vector streams) and per PCG
+    iteration (SpMV + 11 streams; DIC adds both triangular sweeps)."""
+    Ft = F + Fb
+    grad_plain = Ft * (2 * i + 4 * s) + 5 * s * N
+    grad_corr = grad_plain + 2 * (Ft * (2 * i + 7 * s) + 8 * s * N)
+    corrector = Ft * (2 * i + 5 * s) + 5 * s * N
+    fixed = (2 * grad_corr + (n_orth + 1) * 3 * (grad_corr + corrector) + (n_orth + 1) * (grad_corr + corrector)
+             + Ft * (2 * i + 5 * s) + 8 * s * N          # momentum assembly
+             + Ft * (2 * i + 4 * s) + 3 * s * N          # pressure assembly
+             + Ft * (2 * i + 5 * s) + 3 * s * N          # predictor flux
+             + Ft * (2 * i + 9 * s) + 4 * s * N          # correctFluxes
+             + 21 * s * N                                # cell updates
+             + Ft * (i + s) + s * N)                     # divPhi
+    spmv_sym = 3 * s * N + s * F + 2 * i * F
+    spmv_asym1 = 3 * s * N + 2 * s * F + 2 * i * F
+    per_u = 2 * spmv_asym1 + 20 * s * N
+    per_p = spmv_sym + 11 * s * N
+    if precond == "DIC":
+        per_p += 2 * (s * F + 2 * i * F) + 3 * s * N
+    return fixed + it_u * per_u + it_p * per_p
 
 
 def make_case(n, device, precond="Jacobi"):
@@ -204,7 +253,8 @@ def main_reference(args, world, rank, dist):
            "cpu_baseline": {"value": v, "unit": "cell-iter/s", "cores": 1, "kind": kind,
                             "sample": f"one SIMPLE outer iteration of the {n}^3 case from rest (a step of the "
                                       f"timed loop); the reference has no pressure reference cell, so its "
-                                      f"pressure solve runs the unpinned system; {what}; {cpu_info()}"},
+                                      f"pressure solve runs the unpinned system with its only PCG, Jacobi (it has "
+                                      f"no DIC); {what}; {cpu_info()}"},
            "e2e": {"value": v, "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -218,7 +268,7 @@ def main():
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--cpu-sample-cells", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--p-precond", default="Jacobi", choices=["Jacobi", "DIC"])
+    ap.add_argument("--p-precond", default="DIC", choices=["Jacobi", "DIC"])
     ap.add_argument("--profile", action="store_true",
                     help="run --steps outer iterations from the initial state with no warm-up, timing or "
                          "baselines: the command line the ncu captures run")
@@ -236,7 +286,7 @@ def main():
     if args.profile:
         for _ in range(args.steps):
             r = case.solve(ctl)
-        print(json.dumps({"profile": workload_config(n)["workload"], "steps": args.steps,
+        print(json.dumps({"profile": workload_config(n, args.p_precond)["workload"], "steps": args.steps,
                           "u_inner": r.u_inner_iterations, "p_inner": r.p_inner_iterations}))
         return
     for _ in range(max(3, args.warmup)):
@@ -292,11 +342,7 @@ def main():
     kstats = case.kernel_stats()
     case.kernel_timing(False)
 
-    # ---- roofline of the dominant kernel: the pressure-PCG SpMV (+ p.Ap) ----
-    nI = mesh.n_internal_faces
-    s, i = 8, 4
-    alg_spmv = 3 * s * ncell + s * nI + 2 * i * nI          # SpMV symmetric LDU, FP64
-    alg_iter = alg_spmv + 11 * s * ncell                     # one Jacobi-PCG iteration
+    # ---- rooflines: every solver kernel, the dominant one, and the whole step ----
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -304,28 +350,41 @@ def main():
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    cnt, tot = kstats["cg_spmv"]
-    spmv_ms = tot / max(cnt, 1)
-    it_ms = sum(kstats[k][1] for k in kstats) / max(cnt, 1)
-    achieved = alg_spmv / (spmv_ms * 1e-3) / 1e9 if cnt else 0.0
+    alg = kernel_bytes(ncell, mesh.n_internal_faces)
+    kernels = {}
+    for k, (cnt, tot) in kstats.items():
+        if cnt:
+            us = tot / cnt * 1e3
+            kernels[k] = {"launches": cnt, "total_ms": tot, "avg_us": us, "alg_bytes": alg[k],
+                          "achieved_gbs": alg[k] / (us * 1e-6) / 1e9}
+    top = max(kernels, key=lambda k: kernels[k]["total_ms"])
+    kt = kernels[top]
     traffic = None
-    tp = os.environ.get("CFG_SPMV_TRAFFIC_BYTES")
+    tp = os.environ.get("CFG_TOP_KERNEL_TRAFFIC_BYTES")
     if tp:
         traffic = float(tp)
-    roof = {"kernel": "k_cg_spmv (pressure Jacobi-PCG: SELL-32 SpMV + p.Ap)", "bound": "hbm",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": peak_src, "traffic": traffic,
-            "algorithmic_bytes_per_launch": alg_spmv, "launches_timed": cnt, "avg_launch_us": spmv_ms * 1e3,
-            "pcg_iteration": {"algorithmic_bytes": alg_iter, "avg_us": it_ms * 1e3,
-                              "achieved_gbs": alg_iter / (it_ms * 1e-3) / 1e9 if cnt else 0.0}}
+    roof = {"kernel": KERNEL_NAMES[top], "bound": "hbm", "achieved": kt["achieved_gbs"], "peak": peak,
+            "unit": "GB/s", "frac": kt["achieved_gbs"] / peak, "peak_source": peak_src, "traffic": traffic,
+            "algorithmic_bytes_per_launch": kt["alg_bytes"], "launches_timed": kt["launches"],
+            "avg_launch_us": kt["avg_us"], "timing": "CUDA events around each launch over one outer iteration "
+                                                     "from the timed region's start state",
+            "kernels": kernels}
+    step_bytes = simple_step_bytes(ncell, mesh.n_internal_faces, mesh.n_boundary_faces, 1, u_inner / args.steps,
+                                   p_inner / args.steps, args.p_precond)
+    step_s = t_max / args.steps
+    simple_roof = {"bytes_per_step": step_bytes, "achieved_gbs": step_bytes / step_s / 1e9,
+                   "frac": step_bytes / step_s / 1e9 / peak, "peak": peak,
+                   "model": "per-kernel algorithmic bytes summed over the outer iteration with the measured inner "
+                            "iteration counts (BiCGStab 352 B/cell per component-iteration, PCG 160, DIC-PCG 280 "
+                            "B/cell per iteration at hex face counts) / device time per step"}
 
     out = {"metric": METRIC, "value": value, "unit": "cell-iter/s", "n_gpus": world, "steps": args.steps,
            "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": dict(workload_config(n), parallelism=f"replicas x{world}"),
+           "config": dict(workload_config(n, args.p_precond), parallelism=f"replicas x{world}"),
            "e2e": {"value": e2e, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
                    "steps": e2e_steps},
-           "gpu_launches": launches, "roofline": roof, "clocks": clk.summary(),
+           "gpu_launches": launches, "roofline": roof, "simple_roofline": simple_roof, "clocks": clk.summary(),
            "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": u_inner / args.steps,
                                          "pressure_pcg": p_inner / args.steps},
            "wall_s_timed": wall}

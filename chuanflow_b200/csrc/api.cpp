@@ -398,11 +398,11 @@ int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable)
     });
 }
 
-int cfg_kernel_stats(const cfg_ctx* ctx, double out[6])
+int cfg_kernel_stats(const cfg_ctx* ctx, double out[18])
 {
     return guard([&] {
         need(ctx && out, "cfg_kernel_stats: null argument");
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < cfg::Ctx::KS_COUNT; ++k)
         {
             out[2 * k] = ctx->c->kstat[k][0];
             out[2 * k + 1] = ctx->c->kstat[k][1];

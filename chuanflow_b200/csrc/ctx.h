@@ -52,10 +52,23 @@ public:
     double lastMs[8] = {0};
     int64_t lastLaunches = 0;
 
-    /// Per-kernel CUDA-event timing of the pressure-PCG kernels (opt-in):
-    /// kstat[k] = {launches, total ms} for k = spmv, update, p-update.
+    /// Per-kernel CUDA-event timing of the linear-solver kernels (opt-in):
+    /// kstat[k] = {launches, total ms} for the slots KS_*.
     void setKernelTiming(bool on);
-    double kstat[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    enum
+    {
+        KS_CG_SPMV,
+        KS_CG_UPDATE,
+        KS_CG_P,
+        KS_BI_P,
+        KS_BI_SPMV1,
+        KS_BI_S,
+        KS_BI_SPMV2,
+        KS_BI_X,
+        KS_DIC_APPLY,
+        KS_COUNT
+    };
+    double kstat[KS_COUNT][2] = {};
 
     const Mesh& mesh() const { return mesh_; }
 
@@ -161,7 +174,10 @@ private:
     bool ktime_ = false;
     bool useGraphs_ = true;
     std::map<std::string, cudaGraphExec_t> graphs_;
-    std::vector<cudaEvent_t> kev_;  // 6 events per CG iteration of a chunk
+    static constexpr int kEvPerIter = 6;  // events per solver iteration of a chunk (kernels + 1)
+    std::vector<cudaEvent_t> kev_;
+    void tmark(int k, int j);
+    void harvest(int ran, const int* slots, int nSlots);
 };
 
 }  // namespace cfg

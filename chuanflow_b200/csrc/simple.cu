@@ -1311,33 +1311,23 @@ void Ctx::runCG(const double* vals, const double* diag, const double* b, double*
         {
             CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
             CFG_CUDA(cudaStreamSynchronize(stream_));
-            if (ktime_ && lastChunk > 0)
+            if (lastChunk > 0)
             {
                 // only the iterations that ran (the rest returned on the done flag)
-                const int ran = std::min(lastChunk, std::max(0, stHost_->it[0] - itBefore));
-                for (int k = 0; k < ran; ++k)
-                    for (int q = 0; q < 3; ++q)
-                    {
-                        float ms = 0;
-                        CFG_CUDA(cudaEventElapsedTime(&ms, kev_[6 * k + 2 * q], kev_[6 * k + 2 * q + 1]));
-                        kstat[q][0] += 1;
-                        kstat[q][1] += ms;
-                    }
+                static const int slots[3] = {KS_CG_SPMV, KS_CG_UPDATE, KS_CG_P};
+                harvest(std::min(lastChunk, std::max(0, stHost_->it[0] - itBefore)), slots, 3);
             }
             itBefore = stHost_->it[0];
             if (stHost_->allDone || launched >= maxIter) break;
             const int n = std::min(chunk, maxIter - launched);
             launchChunk(ptrKey("cg", {vals, diag, x}, W), n, [&](int k) {
-                cudaEvent_t* ev = ktime_ ? &kev_[6 * k] : nullptr;
-                if (ev) CFG_CUDA(cudaEventRecord(ev[0], stream_));
+                tmark(k, 0);
                 k_cg_spmv<W><<<GS_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
-                if (ev) CFG_CUDA(cudaEventRecord(ev[1], stream_));
-                if (ev) CFG_CUDA(cudaEventRecord(ev[2], stream_));
+                tmark(k, 1);
                 k_cg_update<double><<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
-                if (ev) CFG_CUDA(cudaEventRecord(ev[3], stream_));
-                if (ev) CFG_CUDA(cudaEventRecord(ev[4], stream_));
+                tmark(k, 2);
                 k_cg_p<double><<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
-                if (ev) CFG_CUDA(cudaEventRecord(ev[5], stream_));
+                tmark(k, 3);
                 launchCheck("cg_iter", 0);
             });
             launches_ += 3 * n;
@@ -1367,22 +1357,41 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
         constexpr int NC = decltype(NCc)::value;
         k_bi_init<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, b, x, br_, br0_, bp_, bv_, partials_, st_);
         launchCheck("bicg_init");
+        int itBefore = 0, lastChunk = 0;
+        auto itMax = [&] {
+            int m = 0;
+            for (int q = 0; q < NC; ++q) m = std::max(m, stHost_->it[q]);
+            return m;
+        };
         for (int launched = 0, chunk = 4;;)
         {
             CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
             CFG_CUDA(cudaStreamSynchronize(stream_));
+            if (lastChunk > 0)
+            {
+                static const int slots[5] = {KS_BI_P, KS_BI_SPMV1, KS_BI_S, KS_BI_SPMV2, KS_BI_X};
+                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 5);
+            }
+            itBefore = itMax();
             if (stHost_->allDone || launched >= maxIter) break;
             const int m = std::min(chunk, maxIter - launched);
-            launchChunk(ptrKey("bicg", {vals, diag, x.c[0], x.c[1], x.c[2]}, W * 8 + NC), m, [&](int) {
+            launchChunk(ptrKey("bicg", {vals, diag, x.c[0], x.c[1], x.c[2]}, W * 8 + NC), m, [&](int k) {
+                tmark(k, 0);
                 k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, diag, br_, bp_, bv_, bz_, st_);
+                tmark(k, 1);
                 k_bi_spmv1<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
+                tmark(k, 2);
                 k_bi_s<NC><<<GS_, TPB, 0, stream_>>>(n, diag, x, bz_, br_, bv_, bs_, bsh_, partials_, st_);
+                tmark(k, 3);
                 k_bi_spmv2<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bt_, bs_, partials_, st_);
+                tmark(k, 4);
                 k_bi_x<NC><<<GS_, TPB, 0, stream_>>>(n, x, bsh_, bs_, bt_, br_, br0_, partials_, st_);
+                tmark(k, 5);
                 launchCheck("bicg_iter", 0);
             });
             launches_ += 5 * m;
             launched += m;
+            lastChunk = m;
             chunk = std::min(chunk * 2, 32);
         }
     };
@@ -1462,17 +1471,30 @@ void Ctx::dicCGT(const DDicT<T>& D, const T* vals, const T* diag, const T* b, T*
         launchCheck("cg_pz");
         int launched = 0;
         int chunk = 8;
+        int itBefore = 0, lastChunk = 0;
         for (;;)
         {
             CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
             CFG_CUDA(cudaStreamSynchronize(stream_));
+            if (lastChunk > 0)
+            {
+                static const int slots[4] = {KS_CG_SPMV, KS_CG_UPDATE, KS_DIC_APPLY, KS_CG_P};
+                harvest(std::min(lastChunk, std::max(0, stHost_->it[0] - itBefore)), slots, 4);
+            }
+            itBefore = stHost_->it[0];
             if (stHost_->allDone || launched >= maxIter) break;
             const int n = std::min(chunk, maxIter - launched);
-            launchChunk(ptrKey("diccg", {vals, diag, x, r, p, Ap, z, D.lVal}, W), n, [&](int) {
+            lastChunk = n;
+            launchChunk(ptrKey("diccg", {vals, diag, x, r, p, Ap, z, D.lVal}, W), n, [&](int k) {
+                tmark(k, 0);
                 k_cg_spmv<W, T><<<GS_, TPB, 0, stream_>>>(A, vals, p, Ap, partials_, st_);
+                tmark(k, 1);
                 k_cg_update_nz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, p, Ap, x, r, partials_, st_);
+                tmark(k, 2);
                 dicApplyT<T>(D, r, z);
+                tmark(k, 3);
                 k_cg_pz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, z, p, st_);
+                tmark(k, 4);
                 launchCheck("dic_cg_iter", 0);
             });
             launches_ += (3 + (D.nColours == 1 ? 2 : 2 * D.nColours - 1)) * static_cast<long>(n);
@@ -1530,11 +1552,32 @@ void Ctx::setKernelTiming(bool on)
 {
     if (on && kev_.empty())
     {
-        kev_.resize(6 * 64);
+        kev_.resize(kEvPerIter * 64);
         for (auto& e : kev_) CFG_CUDA(cudaEventCreate(&e));
     }
     ktime_ = on;
     for (auto& r : kstat) r[0] = r[1] = 0.0;
+}
+
+/// Event j of iteration k of the chunk being enqueued (kernel timing on).
+void Ctx::tmark(int k, int j)
+{
+    if (ktime_) CFG_CUDA(cudaEventRecord(kev_[kEvPerIter * k + j], stream_));
+}
+
+/// Adds the first `ran` iterations of the last timed chunk to kstat: the
+/// interval between events j and j+1 of an iteration is kernel slots[j].
+void Ctx::harvest(int ran, const int* slots, int nSlots)
+{
+    if (!ktime_) return;
+    for (int k = 0; k < ran; ++k)
+        for (int j = 0; j < nSlots; ++j)
+        {
+            float ms = 0;
+            CFG_CUDA(cudaEventElapsedTime(&ms, kev_[kEvPerIter * k + j], kev_[kEvPerIter * k + j + 1]));
+            kstat[slots[j]][0] += 1;
+            kstat[slots[j]][1] += ms;
+        }
 }
 
 void Ctx::setNu(double nu)

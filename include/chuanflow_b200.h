@@ -219,12 +219,15 @@ int cfg_simple_iterate(cfg_ctx* ctx, const cfg_simple_controls* controls, cfg_si
  * pressure solve, flux/update, continuity, other, total. */
 int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
 
-/* Opt-in CUDA-event timing of every pressure-PCG kernel launch on the
- * context's stream (no reference counterpart).  Enabling clears the counts;
- * cfg_kernel_stats gives {launches, total ms} for the SpMV + p.Ap kernel,
- * the x/r update + |r| + r.z kernel, and the search-direction update. */
+/* Opt-in CUDA-event timing of every linear-solver kernel launch on the
+ * context's stream (no reference counterpart); while it is on, solver
+ * iterations are launched one by one rather than as CUDA graphs.  Enabling
+ * clears the counts; cfg_kernel_stats gives {launches, total ms} for, in
+ * order: the PCG SpMV + p.Ap, the x/r update + norms + r.z, the
+ * search-direction update; the five BiCGStab kernels (p/z update, v = Az,
+ * s/s^ update, t = As^, x/r update); the whole DIC application z = M^-1 r. */
 int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable);
-int cfg_kernel_stats(const cfg_ctx* ctx, double out[6]);
+int cfg_kernel_stats(const cfg_ctx* ctx, double out[18]);
 
 /* ---- the linear-solver call surface ------------------------------------ */
 
