@@ -37,6 +37,15 @@
 #include "cf/fvm/PressureCorrection.h"
 #include "cf/fvm/SimpleSolver.h"
 
+// Built as cf_adapter_driver, the simple mode runs the same case through the
+// GPU drop-in (chuanflow_b200/adapter) instead of the reference's solver.
+#ifdef CFG_ADAPTER
+#include "cf_simple_gpu.h"
+#define SIMPLE_SOLVE cf::gpu::solveIncompressibleSimple
+#else
+#define SIMPLE_SOLVE solveIncompressibleSimple
+#endif
+
 using namespace cf;
 
 namespace
@@ -245,7 +254,7 @@ int modeSimple(int argc, char** argv)
     const SimpleControls ctl = readControls(caseDict);
 
     const auto t0 = std::chrono::steady_clock::now();
-    const SimpleResult res = solveIncompressibleSimple(mesh, U, p, phi, nu, schemes, ctl);
+    const SimpleResult res = SIMPLE_SOLVE(mesh, U, p, phi, nu, schemes, ctl);
     const auto t1 = std::chrono::steady_clock::now();
     const double secs = std::chrono::duration<double>(t1 - t0).count();
 
