@@ -24,7 +24,7 @@ namespace cfg
 /// the colour layouts' values from the main matrix (T = float also rounds
 /// them to single precision)
 template <class T>
-__global__ void __launch_bounds__(TPB) k_dic_gather(int n, const int* __restrict__ src, const double* __restrict__ val,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_gather(int n, const int* __restrict__ src, const double* __restrict__ val,
                                                     T* __restrict__ out)
 {
     ROW_LOOP(e, n) out[e] = src[e] >= 0 ? static_cast<T>(val[src[e]]) : T(0);
@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(TPB) k_dic_gather(int n, const int* __restrict
 
 /// rD_i = a_ii - sum a_ij^2 / rD_j over the lower entries, one colour
 template <class T>
-__global__ void __launch_bounds__(TPB) k_dic_factor(DDicT<T> D, DicPhase ph, const T* __restrict__ diag)
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_factor(DDicT<T> D, DicPhase ph, const T* __restrict__ diag)
 {
     FOR_ROWS(t, ph.cnt)
     {
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(TPB) k_dic_factor(DDicT<T> D, DicPhase ph, con
 /// forward phase of one colour: z_i = rDinv_i (r_i - sum_lower a_ij z_j);
 /// the last colour's rows also contribute their r_i z_i partials
 template <class T>
-__global__ void __launch_bounds__(TPB) k_dic_fwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int last,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_fwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int last,
                                                  double* partials, SolveState* st)
 {
     if (st->allDone) return;
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(TPB) k_dic_fwd(DDicT<T> D, DicPhase ph, const 
 /// the r_i z_i partials; `final` (the phase that runs last) also reduces
 /// all colours' partials into r.z and advances beta
 template <class T>
-__global__ void __launch_bounds__(TPB) k_dic_bwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int final,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_bwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int final,
                                                  int nPartials, double* partials, SolveState* st)
 {
     if (st->allDone) return;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(TPB) k_dic_bwd(DDicT<T> D, DicPhase ph, const 
 
 /// x += alpha p; r -= alpha Ap; residual test (Matrix.cpp:195-208), without z
 template <class T = double>
-__global__ void __launch_bounds__(TPB) k_cg_update_nz(int n, const T* __restrict__ p, const T* __restrict__ Ap,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_update_nz(int n, const T* __restrict__ p, const T* __restrict__ Ap,
                                                       T* __restrict__ x, T* __restrict__ r, double* partials,
                                                       SolveState* st)
 {
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(TPB) k_cg_update_nz(int n, const T* __restrict
 
 /// p = z + beta p
 template <class T = double>
-__global__ void __launch_bounds__(TPB) k_cg_pz(int n, const T* __restrict__ z, T* __restrict__ p, const SolveState* st)
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_pz(int n, const T* __restrict__ z, T* __restrict__ p, const SolveState* st)
 {
     if (st->allDone) return;
     const T beta = static_cast<T>(st->beta[0]);

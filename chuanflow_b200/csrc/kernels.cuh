@@ -379,6 +379,9 @@ __device__ __forceinline__ void spmv_row(const DMat& A, const T* __restrict__ va
 /// (fewer blocks means fewer per-block reduction epilogues and partials).
 /// RPT is the rows per thread of the default grid, ceil(n / (RPT * TPB)).
 constexpr int RPT = 2;
+/// Blocks per SM the solver kernels are compiled to fit (registers <= 64),
+/// so a grid of 4 blocks per SM runs in one wave.
+constexpr int kSolverMinBlocks = 4;
 #define FOR_ROWS(c, n) \
     for (int c = blockIdx.x * ::cfg::TPB + threadIdx.x; c < (n); c += gridDim.x * ::cfg::TPB)
 

@@ -28,7 +28,7 @@ __device__ __forceinline__ double resid_norm(const SolveState* st, double inf, d
 
 /// r = b - A x; z = D^-1 r; p = z; initial residual, |b|, and r.z.
 template <int W, class T = double>
-__global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const T* __restrict__ val, const T* __restrict__ diag,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_init(DMat A, const T* __restrict__ val, const T* __restrict__ diag,
                                                  const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r,
                                                  T* __restrict__ p, double* partials, SolveState* st)
 {
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(TPB) k_cg_init(DMat A, const T* __restrict__ v
 
 /// Ap = A p and p.Ap; breakdown test and alpha (Matrix.cpp:187-194).
 template <int W, class T = double>
-__global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const T* __restrict__ val, const T* __restrict__ p,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_spmv(DMat A, const T* __restrict__ val, const T* __restrict__ p,
                                                  T* __restrict__ Ap, double* partials, SolveState* st)
 {
     if (st->allDone) return;
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(TPB) k_cg_spmv(DMat A, const T* __restrict__ v
 
 /// x += alpha p; r -= alpha Ap; residual test; z = D^-1 r; beta (Matrix.cpp:195-217).
 template <class T = double>
-__global__ void __launch_bounds__(TPB) k_cg_update(int n, const T* __restrict__ diag, const T* __restrict__ p,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_update(int n, const T* __restrict__ diag, const T* __restrict__ p,
                                                    const T* __restrict__ Ap, T* __restrict__ x, T* __restrict__ r,
                                                    double* partials, SolveState* st)
 {
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(TPB) k_cg_update(int n, const T* __restrict__ 
 
 /// p = z + beta p.
 template <class T = double>
-__global__ void __launch_bounds__(TPB) k_cg_p(int n, const T* __restrict__ diag, const T* __restrict__ r,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_p(int n, const T* __restrict__ diag, const T* __restrict__ r,
                                               T* __restrict__ p, const SolveState* st)
 {
     if (st->allDone) return;
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(TPB) k_cg_p(int n, const T* __restrict__ diag,
 // stops on its own test exactly where the serial loop would.
 
 template <int W, int NC>
-__global__ void __launch_bounds__(TPB) k_bi_init(DMat A, const double* __restrict__ val, V3P b, V3P x, V3P r, V3P r0,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_init(DMat A, const double* __restrict__ val, V3P b, V3P x, V3P r, V3P r0,
                                                  V3P p, V3P v, double* partials, SolveState* st)
 {
     double mx[3 * NC];  // |r|, |b|, nan per comp
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(TPB) k_bi_init(DMat A, const double* __restric
 
 /// p = r + beta (p - omega v); z = p D^-1   (Matrix.cpp:262-272)
 template <int NC>
-__global__ void __launch_bounds__(TPB) k_bi_p(int n, const double* __restrict__ diag, V3P r, V3P p, V3P v, V3P z,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_p(int n, const double* __restrict__ diag, V3P r, V3P p, V3P v, V3P z,
                                               const SolveState* st)
 {
     if (st->allDone) return;
@@ -319,12 +319,24 @@ __global__ void __launch_bounds__(TPB) k_bi_p(int n, const double* __restrict__ 
     }
     FOR_ROWS(c, n)
     {
+        // every load of the row before its first store: the component
+        // arrays are not restrict-qualified, so a store would otherwise
+        // hold back the next component's loads
         const double id = inv_diag_bicg(diag[c]);
+        double rv[NC], pv[NC], vv[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q])
+            {
+                rv[q] = r.c[q][c];
+                pv[q] = p.c[q][c];
+                vv[q] = v.c[q][c];
+            }
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
             if (dn[q]) continue;
-            const double pi = r.c[q][c] + beta[q] * (p.c[q][c] - om[q] * v.c[q][c]);
+            const double pi = rv[q] + beta[q] * (pv[q] - om[q] * vv[q]);
             p.c[q][c] = pi;
             z.c[q][c] = pi * id;
         }
@@ -333,7 +345,7 @@ __global__ void __launch_bounds__(TPB) k_bi_p(int n, const double* __restrict__ 
 
 /// v = A z; r0.v; alpha (Matrix.cpp:273-276)
 template <int W, int NC>
-__global__ void __launch_bounds__(TPB) k_bi_spmv1(DMat A, const double* __restrict__ val, V3P z, V3P v, V3P r0,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv1(DMat A, const double* __restrict__ val, V3P z, V3P v, V3P r0,
                                                   double* partials, SolveState* st)
 {
     if (st->allDone) return;
@@ -345,13 +357,16 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv1(DMat A, const double* __restri
     for (int q = 0; q < NC; ++q) xs[q] = z.c[q];
     FOR_ROWS(c, A.n)
     {
+        double r0v[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) r0v[q] = r0.c[q][c];
         double y[NC];
         spmv_row<W, NC>(A, val, c, xs, y);
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
             v.c[q][c] = y[q];
-            sm[q] += r0.c[q][c] * y[q];
+            sm[q] += r0v[q] * y[q];
         }
     }
     block_sum<NC>(sm);
@@ -383,7 +398,7 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv1(DMat A, const double* __restri
 
 /// x += alpha z; s = r - alpha v; sh = s D^-1; |s|inf (Matrix.cpp:277-289)
 template <int NC>
-__global__ void __launch_bounds__(TPB) k_bi_s(int n, const double* __restrict__ diag, V3P x, V3P z, V3P r, V3P v,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_s(int n, const double* __restrict__ diag, V3P x, V3P z, V3P r, V3P v,
                                               V3P s, V3P sh, double* partials, SolveState* st)
 {
     if (st->allDone) return;
@@ -400,12 +415,22 @@ __global__ void __launch_bounds__(TPB) k_bi_s(int n, const double* __restrict__ 
     FOR_ROWS(c, n)
     {
         const double id = inv_diag_bicg(diag[c]);
+        double xv[NC], zv[NC], rv[NC], vv[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q])
+            {
+                xv[q] = x.c[q][c];
+                zv[q] = z.c[q][c];
+                rv[q] = r.c[q][c];
+                vv[q] = v.c[q][c];
+            }
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
             if (dn[q]) continue;
-            x.c[q][c] = x.c[q][c] + al[q] * z.c[q][c];
-            const double si = r.c[q][c] - al[q] * v.c[q][c];
+            x.c[q][c] = xv[q] + al[q] * zv[q];
+            const double si = rv[q] - al[q] * vv[q];
             s.c[q][c] = si;
             sh.c[q][c] = si * id;
             if (isnan(si)) mx[NC + q] = 1.0;
@@ -429,7 +454,7 @@ __global__ void __launch_bounds__(TPB) k_bi_s(int n, const double* __restrict__ 
 
 /// t = A sh; t.t and t.s; omega, or the tDenom breakdown exit (Matrix.cpp:290-300)
 template <int W, int NC>
-__global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restrict__ val, V3P sh, V3P t, V3P s,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv2(DMat A, const double* __restrict__ val, V3P sh, V3P t, V3P s,
                                                   double* partials, SolveState* st)
 {
     if (st->allDone) return;
@@ -441,6 +466,9 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restri
     for (int q = 0; q < NC; ++q) xs[q] = sh.c[q];
     FOR_ROWS(c, A.n)
     {
+        double sv[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) sv[q] = s.c[q][c];
         double y[NC];
         spmv_row<W, NC>(A, val, c, xs, y);
 #pragma unroll
@@ -448,7 +476,7 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restri
         {
             t.c[q][c] = y[q];
             sm[q] += y[q] * y[q];
-            sm[NC + q] += y[q] * s.c[q][c];
+            sm[NC + q] += y[q] * sv[q];
         }
     }
     block_sum<2 * NC>(sm);
@@ -489,7 +517,7 @@ __global__ void __launch_bounds__(TPB) k_bi_spmv2(DMat A, const double* __restri
 
 /// x += omega sh; r = s - omega t; |r|inf test; next r0.r (Matrix.cpp:301-315, :263-264)
 template <int NC>
-__global__ void __launch_bounds__(TPB) k_bi_x(int n, V3P x, V3P sh, V3P s, V3P t, V3P r, V3P r0, double* partials,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, V3P x, V3P sh, V3P s, V3P t, V3P r, V3P r0, double* partials,
                                               SolveState* st)
 {
     if (st->allDone) return;
@@ -506,16 +534,27 @@ __global__ void __launch_bounds__(TPB) k_bi_x(int n, V3P x, V3P sh, V3P s, V3P t
     }
     FOR_ROWS(c, n)
     {
+        double xv[NC], shv[NC], sv[NC], tv[NC], r0v[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q])
+            {
+                xv[q] = x.c[q][c];
+                shv[q] = sh.c[q][c];
+                sv[q] = s.c[q][c];
+                tv[q] = t.c[q][c];
+                r0v[q] = r0.c[q][c];
+            }
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
             if (dn[q]) continue;
-            x.c[q][c] = x.c[q][c] + om[q] * sh.c[q][c];
-            const double ri = s.c[q][c] - om[q] * t.c[q][c];
+            x.c[q][c] = xv[q] + om[q] * shv[q];
+            const double ri = sv[q] - om[q] * tv[q];
             r.c[q][c] = ri;
             if (isnan(ri)) mx[NC + q] = 1.0;
             mx[q] = smax(mx[q], fabs(ri));
-            sm[q] += r0.c[q][c] * ri;
+            sm[q] += r0v[q] * ri;
         }
     }
     block_max<2 * NC>(mx);
