@@ -203,6 +203,12 @@ class PolyMesh:
     def jitter_interior(self, fraction, seed):
         _check(lib().cfg_mesh_jitter_interior(self._h, C.c_double(fraction), C.c_uint64(seed)))
 
+    def device_order(self, order=None):
+        """The device numbering a context of this order uses, new -> original."""
+        out = np.zeros(self.n_cells, np.int64)
+        _check(lib().cfg_mesh_device_order(self._h, C.c_int32(CELL_ORDER[order]), _ip(out)))
+        return out
+
     def addressing(self):
         pts = np.zeros((self.n_points, 3))
         fo = np.zeros(self.n_faces + 1, np.int64)
@@ -310,13 +316,19 @@ class SolverReport:
     final_residual: float
 
 
+CELL_ORDER = {None: -1, "identity": 0, "colour": 1, "rcm": 2, "rcm-colour": 3}
+
+
 class SimpleCase:
     """U, p, phi and their boundary conditions on one device."""
 
-    def __init__(self, mesh: PolyMesh, device: int = 0, schemes: Schemes | None = None):
+    def __init__(self, mesh: PolyMesh, device: int = 0, schemes: Schemes | None = None, order: str | None = None):
+        """order: the device cell numbering ("identity", "colour", "rcm",
+        "rcm-colour"); None takes CHUANFLOW_CELL_ORDER, else "colour"."""
         self.mesh = mesh
         h = C.c_void_p()
-        _check(lib().cfg_ctx_create(mesh._h, C.c_int32(device), None, C.byref(h)))
+        _check(lib().cfg_ctx_create_ordered(mesh._h, C.c_int32(device), None, C.c_int32(CELL_ORDER[order]),
+                                            C.byref(h)))
         self._h = h
         self.set_schemes(schemes or Schemes())
 

@@ -295,22 +295,28 @@ int cfg_mesh_weights(const cfg_mesh* mesh, double* ow, double* skew)
     });
 }
 
-int cfg_mesh_device_order(const cfg_mesh* mesh, int64_t* newToOld)
+int cfg_mesh_device_order(const cfg_mesh* mesh, int32_t order, int64_t* newToOld)
 {
     return guard([&] {
         need(mesh && newToOld, "cfg_mesh_device_order: null argument");
-        for (int64_t c = 0; c < mesh->m.nCells; ++c) newToOld[c] = c;
+        const std::vector<int64_t> o = cfg::cellOrder(mesh->m, order);
+        std::copy(o.begin(), o.end(), newToOld);
+    });
+}
+
+int cfg_ctx_create_ordered(const cfg_mesh* mesh, int32_t device, void* stream, int32_t order, cfg_ctx** out)
+{
+    return guard([&] {
+        need(mesh && out, "cfg_ctx_create: null argument");
+        auto c = std::make_unique<cfg_ctx>();
+        c->c = std::make_unique<cfg::Ctx>(mesh->m, device, static_cast<cudaStream_t>(stream), order);
+        *out = c.release();
     });
 }
 
 int cfg_ctx_create(const cfg_mesh* mesh, int32_t device, void* stream, cfg_ctx** out)
 {
-    return guard([&] {
-        need(mesh && out, "cfg_ctx_create: null argument");
-        auto c = std::make_unique<cfg_ctx>();
-        c->c = std::make_unique<cfg::Ctx>(mesh->m, device, static_cast<cudaStream_t>(stream));
-        *out = c.release();
-    });
+    return cfg_ctx_create_ordered(mesh, device, stream, CFG_ORDER_DEFAULT, out);
 }
 
 void cfg_ctx_destroy(cfg_ctx* ctx) { delete ctx; }

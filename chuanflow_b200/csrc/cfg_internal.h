@@ -77,6 +77,19 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
 Mesh blockMesh(const Vec& mn, const Vec& mx, int64_t nx, int64_t ny, int64_t nz,
                const std::vector<std::string>& names, const std::vector<std::string>& types);
 
+/// Distinct cell neighbours across internal faces, ascending, as a CSR.
+struct CellGraph
+{
+    std::vector<int64_t> start, adj;
+};
+CellGraph cellGraph(const Mesh& M);
+/// First-fit colours in ascending cell order (no two neighbours alike).
+std::vector<int> greedyColours(const CellGraph& g, int* nColours);
+/// Reverse Cuthill-McKee order, new -> old.
+std::vector<int64_t> rcmOrder(const CellGraph& g);
+/// The device numbering of a cfg_cell_order mode, new -> old.
+std::vector<int64_t> cellOrder(const Mesh& M, int mode);
+
 }  // namespace cfg
 
 struct cfg_mesh

@@ -24,7 +24,7 @@ struct Timing
 class Ctx
 {
 public:
-    Ctx(const Mesh& mesh, int device, cudaStream_t stream);
+    Ctx(const Mesh& mesh, int device, cudaStream_t stream, int order = -1);
     ~Ctx();
 
     // boundary conditions and schemes
@@ -132,6 +132,14 @@ private:
 
     // boundary conditions (host)
     std::vector<int> uType_, pType_;
+    // device numbering: slot i holds original cell perm_[i]; inv_ = perm_^-1
+    int order_ = -1;
+    std::vector<int> perm_, inv_;
+    bool identityOrder_ = true;
+    std::vector<double> hostTmp_;
+    void toDevCells(double* dev, const double* host, int stride, int off);
+    void fromDevCells(double* host, const double* dev, int stride, int off);
+    int deviceCell(int64_t c) const;
     std::vector<Vec> uVal_;
     std::vector<double> pVal_;
     std::map<int64_t, Vec> uFace_;

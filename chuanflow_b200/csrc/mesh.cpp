@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <unordered_map>
 
@@ -466,6 +467,198 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
     }
     m.finish();
     return m;
+}
+
+}  // namespace cfg
+
+// ---------------------------------------------------------------------------
+// Device cell numbering (no reference counterpart: the reference keeps the
+// mesh's own order, and its only reordering is the domain decomposition's
+// coordinate median split, domainDecomposition.cpp:27-77).  Renumbering
+// changes where each cell's values sit in device memory, never the order of
+// any sum: per-cell face lists and matrix rows keep the original face and
+// column order, so results are bit-identical in every numbering.
+// ---------------------------------------------------------------------------
+namespace cfg
+{
+
+CellGraph cellGraph(const Mesh& M)
+{
+    const int64_t nC = M.nCells, nI = M.nInternal();
+    CellGraph g;
+    g.start.assign(static_cast<size_t>(nC) + 1, 0);
+    for (int64_t f = 0; f < nI; ++f)
+    {
+        ++g.start[M.owner[f] + 1];
+        ++g.start[M.neighbour[f] + 1];
+    }
+    for (int64_t c = 0; c < nC; ++c) g.start[c + 1] += g.start[c];
+    std::vector<int64_t> fill(g.start.begin(), g.start.end() - 1);
+    g.adj.resize(static_cast<size_t>(g.start[nC]));
+    for (int64_t f = 0; f < nI; ++f)
+    {
+        const int64_t o = M.owner[f], n = M.neighbour[f];
+        g.adj[fill[o]++] = n;
+        g.adj[fill[n]++] = o;
+    }
+    // distinct neighbours in ascending order (two faces may join one pair)
+    std::vector<int64_t> s2(static_cast<size_t>(nC) + 1, 0);
+    size_t w = 0;
+    for (int64_t c = 0; c < nC; ++c)
+    {
+        auto b = g.adj.begin() + g.start[c], e = g.adj.begin() + g.start[c + 1];
+        std::sort(b, e);
+        const auto u = std::unique(b, e);
+        for (auto it = b; it != u; ++it) g.adj[w++] = *it;
+        s2[c + 1] = static_cast<int64_t>(w);
+    }
+    g.adj.resize(w);
+    g.start.swap(s2);
+    return g;
+}
+
+std::vector<int> greedyColours(const CellGraph& g, int* nColours)
+{
+    const int64_t nC = static_cast<int64_t>(g.start.size()) - 1;
+    std::vector<int> colour(static_cast<size_t>(nC), -1), mark(static_cast<size_t>(nC) + 2, -1);
+    int nCol = 0;
+    for (int64_t c = 0; c < nC; ++c)
+    {
+        for (int64_t k = g.start[c]; k < g.start[c + 1]; ++k)
+        {
+            const int cj = colour[g.adj[k]];
+            if (cj >= 0) mark[cj] = static_cast<int>(c);
+        }
+        int col = 0;
+        while (mark[col] == c) ++col;
+        colour[c] = col;
+        nCol = std::max(nCol, col + 1);
+    }
+    if (nColours) *nColours = nCol;
+    return colour;
+}
+
+namespace
+{
+
+/// Breadth-first levels from `root` over cells not yet numbered; returns the
+/// eccentricity and leaves the last level in `last`.
+int bfsLevels(const CellGraph& g, int64_t root, const std::vector<char>& numbered, std::vector<int64_t>& stamp,
+              int64_t tag, std::vector<int64_t>& last)
+{
+    std::vector<int64_t> cur{root}, next;
+    stamp[root] = tag;
+    int ecc = 0;
+    for (;;)
+    {
+        next.clear();
+        for (int64_t u : cur)
+            for (int64_t k = g.start[u]; k < g.start[u + 1]; ++k)
+            {
+                const int64_t v = g.adj[k];
+                if (numbered[v] || stamp[v] == tag) continue;
+                stamp[v] = tag;
+                next.push_back(v);
+            }
+        if (next.empty()) break;
+        cur.swap(next);
+        ++ecc;
+    }
+    last = cur;
+    return ecc;
+}
+
+}  // namespace
+
+/// Reverse Cuthill-McKee (Cuthill & McKee 1969; reversed, George 1971).
+/// Each connected component starts from a pseudo-peripheral cell (George &
+/// Liu 1979, at most 8 rounds): the unnumbered cell of least (degree, index),
+/// moved to the least-(degree, index) cell of its farthest level while that
+/// increases the eccentricity.  Cells are numbered breadth-first, each
+/// cell's unnumbered neighbours by increasing (degree, index); the whole
+/// sequence is then reversed.  Returns new -> old.
+std::vector<int64_t> rcmOrder(const CellGraph& g)
+{
+    const int64_t nC = static_cast<int64_t>(g.start.size()) - 1;
+    auto deg = [&](int64_t c) { return g.start[c + 1] - g.start[c]; };
+    auto less = [&](int64_t a, int64_t b) { return deg(a) != deg(b) ? deg(a) < deg(b) : a < b; };
+    std::vector<int64_t> byDeg(static_cast<size_t>(nC));
+    for (int64_t c = 0; c < nC; ++c) byDeg[c] = c;
+    std::stable_sort(byDeg.begin(), byDeg.end(), less);
+    std::vector<char> numbered(static_cast<size_t>(nC), 0);
+    std::vector<int64_t> stamp(static_cast<size_t>(nC), -1), order, last, last2, nb;
+    order.reserve(static_cast<size_t>(nC));
+    int64_t tag = 0;
+    size_t scan = 0;
+    while (static_cast<int64_t>(order.size()) < nC)
+    {
+        while (numbered[byDeg[scan]]) ++scan;
+        int64_t root = byDeg[scan];
+        int ecc = bfsLevels(g, root, numbered, stamp, tag++, last);
+        for (int round = 0; round < 8; ++round)
+        {
+            int64_t cand = last[0];
+            for (int64_t v : last)
+                if (less(v, cand)) cand = v;
+            const int ecc2 = bfsLevels(g, cand, numbered, stamp, tag++, last2);
+            if (ecc2 <= ecc) break;
+            root = cand;
+            ecc = ecc2;
+            last.swap(last2);
+        }
+        size_t head = order.size();
+        order.push_back(root);
+        numbered[root] = 1;
+        while (head < order.size())
+        {
+            const int64_t u = order[head++];
+            nb.clear();
+            for (int64_t k = g.start[u]; k < g.start[u + 1]; ++k)
+                if (!numbered[g.adj[k]]) nb.push_back(g.adj[k]);
+            std::sort(nb.begin(), nb.end(), less);
+            for (int64_t v : nb)
+            {
+                numbered[v] = 1;
+                order.push_back(v);
+            }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+    return order;
+}
+
+int defaultCellOrder()
+{
+    if (const char* e = std::getenv("CHUANFLOW_CELL_ORDER"))
+    {
+        const std::string s(e);
+        if (s == "identity") return CFG_ORDER_IDENTITY;
+        if (s == "colour") return CFG_ORDER_COLOUR;
+        if (s == "rcm") return CFG_ORDER_RCM;
+        if (s == "rcm-colour") return CFG_ORDER_RCM_COLOUR;
+    }
+    return CFG_ORDER_COLOUR;
+}
+
+std::vector<int64_t> cellOrder(const Mesh& M, int mode)
+{
+    if (mode == CFG_ORDER_DEFAULT) mode = defaultCellOrder();
+    const int64_t nC = M.nCells;
+    std::vector<int64_t> order(static_cast<size_t>(nC));
+    for (int64_t c = 0; c < nC; ++c) order[c] = c;
+    if (mode == CFG_ORDER_IDENTITY) return order;
+    if (mode != CFG_ORDER_COLOUR && mode != CFG_ORDER_RCM && mode != CFG_ORDER_RCM_COLOUR)
+        fail(CFG_EINVAL, "unknown cell order " + std::to_string(mode));
+    const CellGraph g = cellGraph(M);
+    if (mode == CFG_ORDER_RCM || mode == CFG_ORDER_RCM_COLOUR) order = rcmOrder(g);
+    if (mode == CFG_ORDER_COLOUR || mode == CFG_ORDER_RCM_COLOUR)
+    {
+        // colour blocks, each in the base order: the colour of a cell is its
+        // greedy colour in the original numbering
+        const std::vector<int> colour = greedyColours(g, nullptr);
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return colour[a] < colour[b]; });
+    }
+    return order;
 }
 
 }  // namespace cfg

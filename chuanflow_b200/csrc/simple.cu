@@ -566,7 +566,8 @@ namespace
 inline double hdot(const Vec& a, const Vec& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 }
 
-Ctx::Ctx(const Mesh& mesh, int device, cudaStream_t stream) : mesh_(mesh), device_(device), stream_(stream)
+Ctx::Ctx(const Mesh& mesh, int device, cudaStream_t stream, int order)
+    : mesh_(mesh), device_(device), stream_(stream), order_(order)
 {
     if (mesh_.nCells >= (1LL << 30) || mesh_.nFaces() >= (1LL << 30))
         fail(CFG_EINVAL, "mesh too large for 32-bit device indices");
@@ -672,6 +673,18 @@ void Ctx::buildDevice()
         cz[c] = M.C[c].z;
     }
 
+    // ---- device numbering: slot i holds original cell perm_[i] ----
+    {
+        const std::vector<int64_t> o = cellOrder(M, order_);
+        perm_.assign(o.begin(), o.end());
+        inv_.assign(static_cast<size_t>(nC), 0);
+        for (int i = 0; i < nC; ++i) inv_[perm_[i]] = i;
+        identityOrder_ = true;
+        for (int i = 0; i < nC && identityOrder_; ++i) identityOrder_ = perm_[i] == i;
+    }
+    const std::vector<int>& perm = perm_;
+    const std::vector<int>& inv = inv_;
+
     // ---- cell -> face lists (ascending faces) and matrix rows ----
     std::vector<int> cnt(nC, 0), rowCnt(nC, 1);
     for (int f = 0; f < nF; ++f)
@@ -697,16 +710,17 @@ void Ctx::buildDevice()
             listF[cStart[n] + fill[n]++] = (f << 1) | 1;
         }
     }
+    // slices of 32 device slots; widths from the cells they hold
     std::vector<int> cfStart(nSlices_ + 1, 0), mStart(nSlices_ + 1, 0);
     for (int s = 0; s < nSlices_; ++s)
     {
         int w = 0, wm = 0;
         for (int l = 0; l < 32; ++l)
         {
-            const int c = 32 * s + l;
-            if (c >= nC) break;
-            w = std::max(w, cnt[c]);
-            wm = std::max(wm, rowCnt[c]);
+            const int i = 32 * s + l;
+            if (i >= nC) break;
+            w = std::max(w, cnt[perm[i]]);
+            wm = std::max(wm, rowCnt[perm[i]]);
         }
         cfStart[s + 1] = cfStart[s] + 32 * w;
         mStart[s + 1] = mStart[s] + 32 * wm;
@@ -714,10 +728,11 @@ void Ctx::buildDevice()
     }
     std::vector<int> cfCode(cfStart[nSlices_], -1), cfOther(cfStart[nSlices_], 0);
     std::vector<int> mCol(mStart[nSlices_], -1), mCode(mStart[nSlices_], -1);
-    std::vector<std::pair<int, int>> row;  // (col, code)
-    for (int c = 0; c < nC; ++c)
+    std::vector<std::pair<int, int>> row;  // (original col, code)
+    for (int i = 0; i < nC; ++i)
     {
-        const int s = c >> 5, l = c & 31;
+        const int c = perm[i];
+        const int s = i >> 5, l = i & 31;
         row.clear();
         row.push_back({c, -2});
         for (int k = 0; k < cnt[c]; ++k)
@@ -729,7 +744,7 @@ void Ctx::buildDevice()
             if (f < nI)
             {
                 const int other = (code & 1) ? own[f] : nbr[f];
-                cfOther[e] = other;
+                cfOther[e] = inv[other];
                 row.push_back({other, code});
             }
             else
@@ -737,36 +752,24 @@ void Ctx::buildDevice()
                 cfOther[e] = f - nI;
             }
         }
-        // CSR column order (Matrix.cpp:72-76); entries with equal columns
-        // (two faces between the same cells) stay separate, in face order
+        // CSR column order of the original numbering (Matrix.cpp:72-76);
+        // entries with equal columns (two faces between the same cells) stay
+        // separate, in face order
         std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
         for (size_t k = 0; k < row.size(); ++k)
         {
             const int e = mStart[s] + 32 * static_cast<int>(k) + l;
-            mCol[e] = row[k].first;
+            mCol[e] = inv[row[k].first];
             mCode[e] = row[k].second;
         }
     }
 
     // ---- multicolour DIC layouts (dic.cuh) ----
     {
-        std::vector<int> colour(nC, -1), mark(nC + 2, -1);
         int nCol = 0;
-        for (int c = 0; c < nC; ++c)
-        {
-            const int s0 = c >> 5, l0 = c & 31;
-            for (int k = 0;; ++k)
-            {
-                const int e = mStart[s0] + 32 * k + l0;
-                if (e >= mStart[s0 + 1] || mCol[e] < 0) break;
-                const int j = mCol[e];
-                if (j != c && colour[j] >= 0) mark[colour[j]] = c;
-            }
-            int col = 0;
-            while (mark[col] == c) ++col;
-            colour[c] = col;
-            nCol = std::max(nCol, col + 1);
-        }
+        const std::vector<int> colourOrig = greedyColours(cellGraph(M), &nCol);
+        std::vector<int> colour(nC);
+        for (int i = 0; i < nC; ++i) colour[i] = colourOrig[perm[i]];
         nColours_ = nCol;
         std::vector<int> rows;
         std::vector<int> lStart{0}, uStart{0}, lCol, lSrc, uCol, uSrc;
@@ -842,8 +845,13 @@ void Ctx::buildDevice()
         nUp_ = static_cast<int>(uCol.size());
     }
 
-    d.own = upload(own);
-    d.nbr = upload(nbr);
+    {
+        std::vector<int> ownN(nF), nbrN(std::max(nI, 1));
+        for (int f = 0; f < nF; ++f) ownN[f] = inv[own[f]];
+        for (int f = 0; f < nI; ++f) nbrN[f] = inv[nbr[f]];
+        d.own = upload(ownN);
+        d.nbr = upload(nbrN);
+    }
     d.sfx = upload(sfx);
     d.sfy = upload(sfy);
     d.sfz = upload(sfz);
@@ -861,11 +869,16 @@ void Ctx::buildDevice()
     d.cvx = upload(cvx);
     d.cvy = upload(cvy);
     d.cvz = upload(cvz);
-    d.V = upload(M.V);
-    d.lscale = upload(lscale);
-    d.cx = upload(cx);
-    d.cy = upload(cy);
-    d.cz = upload(cz);
+    auto permuted = [&](const std::vector<double>& a) {
+        std::vector<double> b(static_cast<size_t>(nC));
+        for (int i = 0; i < nC; ++i) b[i] = a[perm[i]];
+        return b;
+    };
+    d.V = upload(permuted(M.V));
+    d.lscale = upload(permuted(lscale));
+    d.cx = upload(permuted(cx));
+    d.cy = upload(permuted(cy));
+    d.cz = upload(permuted(cz));
     d.fcx = upload(fcx);
     d.fcy = upload(fcy);
     d.fcz = upload(fcz);
@@ -1658,38 +1671,57 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
     }
 }
 
+/// A host cell array in the original numbering (element c at
+/// host[c * stride + off]) copied into device slot order.
+void Ctx::toDevCells(double* dev, const double* host, int stride, int off)
+{
+    const int nC = dm_.nC;
+    if (identityOrder_ && stride == 1)
+    {
+        CFG_CUDA(cudaMemcpyAsync(dev, host + off, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        return;
+    }
+    hostTmp_.resize(static_cast<size_t>(nC));
+    for (int i = 0; i < nC; ++i) hostTmp_[i] = host[static_cast<size_t>(perm_[i]) * stride + off];
+    CFG_CUDA(cudaMemcpyAsync(dev, hostTmp_.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+/// The inverse of toDevCells.
+void Ctx::fromDevCells(double* host, const double* dev, int stride, int off)
+{
+    const int nC = dm_.nC;
+    if (identityOrder_ && stride == 1)
+    {
+        CFG_CUDA(cudaMemcpyAsync(host + off, dev, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        return;
+    }
+    hostTmp_.resize(static_cast<size_t>(nC));
+    CFG_CUDA(cudaMemcpyAsync(hostTmp_.data(), dev, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    for (int i = 0; i < nC; ++i) host[static_cast<size_t>(perm_[i]) * stride + off] = hostTmp_[i];
+}
+
+int Ctx::deviceCell(int64_t c) const { return c < 0 ? -1 : inv_[static_cast<size_t>(c)]; }
+
 void Ctx::upload(const double* U, const double* p, const double* phi)
 {
-    const int nC = dm_.nC, nF = dm_.nF;
+    const int nF = dm_.nF;
     if (U)
-    {
-        std::vector<double> t(static_cast<size_t>(nC));
-        for (int q = 0; q < 3; ++q)
-        {
-            for (int c = 0; c < nC; ++c) t[c] = U[3 * static_cast<size_t>(c) + q];
-            CFG_CUDA(cudaMemcpyAsync(U_.c[q], t.data(), nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
-            CFG_CUDA(cudaStreamSynchronize(stream_));
-        }
-    }
-    if (p) CFG_CUDA(cudaMemcpyAsync(p_, p, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        for (int q = 0; q < 3; ++q) toDevCells(U_.c[q], U, 3, q);
+    if (p) toDevCells(p_, p, 1, 0);
     if (phi) CFG_CUDA(cudaMemcpyAsync(phi_, phi, nF * sizeof(double), cudaMemcpyHostToDevice, stream_));
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Ctx::download(double* U, double* p, double* phi)
 {
-    const int nC = dm_.nC, nF = dm_.nF;
+    const int nF = dm_.nF;
     if (U)
-    {
-        std::vector<double> t(static_cast<size_t>(nC));
-        for (int q = 0; q < 3; ++q)
-        {
-            CFG_CUDA(cudaMemcpyAsync(t.data(), U_.c[q], nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-            CFG_CUDA(cudaStreamSynchronize(stream_));
-            for (int c = 0; c < nC; ++c) U[3 * static_cast<size_t>(c) + q] = t[c];
-        }
-    }
-    if (p) CFG_CUDA(cudaMemcpyAsync(p, p_, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        for (int q = 0; q < 3; ++q) fromDevCells(U, U_.c[q], 3, q);
+    if (p) fromDevCells(p, p_, 1, 0);
     if (phi) CFG_CUDA(cudaMemcpyAsync(phi, phi_, nF * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -1740,7 +1772,7 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
     const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
     const bool doAdjust = needReference_ && nFreeUFaces_ > 0;
     if (ctl.p_ref_cell >= nC) fail(CFG_EINVAL, "p_ref_cell beyond the last cell");
-    const int refCell = ctl.p_ref_cell >= 0 ? static_cast<int>(ctl.p_ref_cell) : -1;
+    const int refCell = deviceCell(ctl.p_ref_cell);
     double contLag1 = INFINITY, contLag2 = INFINITY;
     launches_ = 0;
     for (int k = 0; k < 8; ++k) lastMs[k] = 0.0;
@@ -1851,20 +1883,25 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
     const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
     const DMat A{nC, dm_.mStart, dm_.mCol};
     double* o = out;
-    auto d2h = [&](const double* src, size_t n) {
-        CFG_CUDA(cudaMemcpyAsync(o, src, n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    // cell arrays back in the original numbering, face arrays as they are
+    auto d2hC = [&](const double* src) {
+        fromDevCells(o, src, 1, 0);
+        o += nC;
+    };
+    auto d2hF = [&](const double* src) {
+        CFG_CUDA(cudaMemcpyAsync(o, src, nF * sizeof(double), cudaMemcpyDeviceToHost, stream_));
         CFG_CUDA(cudaStreamSynchronize(stream_));
-        o += n;
+        o += nF;
     };
     CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
     double* xp = cr_;
-    CFG_CUDA(cudaMemcpyAsync(xp, xprobe, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    toDevCells(xp, xprobe, 1, 0);
     {
         const double* xs[1] = {p_};
         V3P g[1] = {gPn_};
         gradCells(xs, 1, pb, gs, true, g);
     }
-    for (int q = 0; q < 3; ++q) d2h(gPn_.c[q], nC);
+    for (int q = 0; q < 3; ++q) d2hC(gPn_.c[q]);
     MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_), mVal_,
                uDiag_, uBase_};
     k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
@@ -1884,20 +1921,20 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
         for (int q = 0; q < 3; ++q)
             CFG_CUDA(cudaMemcpyAsync(uRhs_.c[q], uBase_.c[q], nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     }
-    for (int q = 0; q < 3; ++q) d2h(uDiag_, nC);
+    for (int q = 0; q < 3; ++q) d2hC(uDiag_);
     for (int pass = 0; pass < 2; ++pass)
         for (int q = 0; q < 3; ++q)
         {
             k_explicit_op<<<G_, TPB, 0, stream_>>>(A, mVal_, uDiag_, uRhs_.c[q], pass ? xp : ux_.c[0], cAp_);
             launchCheck("explicit_op");
-            d2h(cAp_, nC);
+            d2hC(cAp_);
         }
     k_hfree<<<G_, TPB, 0, stream_>>>(dm_, uDiag_, cv(U_), cv(ux_), 1.0, Hf_, rAUr_);
     launchCheck("hfree");
     k_face_interp<<<GF_, TPB, 0, stream_>>>(dm_, rAUr_, rAUf_);
     launchCheck("face_interp");
-    d2h(rAUf_, nF);
-    const int refCell = ctl.p_ref_cell >= 0 && ctl.p_ref_cell < nC ? static_cast<int>(ctl.p_ref_cell) : -1;
+    d2hF(rAUf_);
+    const int refCell = ctl.p_ref_cell >= 0 && ctl.p_ref_cell < nC ? deviceCell(ctl.p_ref_cell) : -1;
     k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, phi_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_, refCell,
                                           ctl.p_ref_value);
     launchCheck("assemble_p");
@@ -1906,7 +1943,7 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
     CFG_CUDA(cudaStreamSynchronize(stream_));
     k_divphi<<<G_, TPB, 0, stream_>>>(dm_, phi_, cAp_);
     launchCheck("divphi");
-    d2h(cAp_, nC);
+    d2hC(cAp_);
     *o++ = hostScal[S_CONT];
     // pressure equation rhs = base + corrector(x = 0)
     CFG_CUDA(cudaMemsetAsync(px_, 0, nC * sizeof(double), stream_));
@@ -1923,24 +1960,24 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
     {
         CFG_CUDA(cudaMemcpyAsync(pRhs_, pBase_, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     }
-    d2h(pDiag_, nC);
+    d2hC(pDiag_);
     for (int pass = 0; pass < 2; ++pass)
     {
         k_explicit_op<<<G_, TPB, 0, stream_>>>(A, pVal_d_, pDiag_, pRhs_, pass ? xp : px_, cAp_);
         launchCheck("explicit_op");
-        d2h(cAp_, nC);
+        d2hC(cAp_);
     }
     {
         const double* xs[1] = {xp};
         V3P g[1] = {gPF_};
         gradCells(xs, 1, pb, gs, true, g);
     }
-    for (int q = 0; q < 3; ++q) d2h(gPF_.c[q], nC);
+    for (int q = 0; q < 3; ++q) d2hC(gPF_.c[q]);
     CFG_CUDA(cudaMemcpyAsync(fScratch_, phi_, nF * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     k_correct_flux<<<GF_, TPB, 0, stream_>>>(dm_, xp, cv(gPF_), rAUf_, pc_, pk_, schemes_.laplacian_corrected,
                                              fScratch_);
     launchCheck("correct_flux");
-    d2h(fScratch_, nF);
+    d2hF(fScratch_);
 }
 
 void Ctx::probeDIC(const double* r, double* z, double* rDinv)
@@ -1953,11 +1990,10 @@ void Ctx::probeDIC(const double* r, double* z, double* rDinv)
     init.maxIter = 1;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     dicSetup(pVal_d_, pDiag_);
-    CFG_CUDA(cudaMemcpyAsync(cr_, r, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    toDevCells(cr_, r, 1, 0);
     dicApply(cr_, cz_);
-    CFG_CUDA(cudaMemcpyAsync(z, cz_, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    CFG_CUDA(cudaMemcpyAsync(rDinv, dic_.rDinv, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    CFG_CUDA(cudaStreamSynchronize(stream_));
+    fromDevCells(z, cz_, 1, 0);
+    fromDevCells(rDinv, dic_.rDinv, 1, 0);
 }
 
 void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQuirk, double* out)
@@ -1968,20 +2004,14 @@ void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQ
     double* x = cr_;
     double* k = bScratch_;
     double* c0 = bScratch_ + nB;
-    CFG_CUDA(cudaMemcpyAsync(x, data, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    toDevCells(x, data, 1, 0);
     CFG_CUDA(cudaMemcpyAsync(k, bvals, nB * sizeof(double), cudaMemcpyHostToDevice, stream_));
     CFG_CUDA(cudaMemsetAsync(c0, 0, nB * sizeof(double), stream_));
     const BcTab bt{{c0, c0, c0}, {k, k, k}};
     const double* xs[1] = {x};
     V3P g[1] = {gPF_};
     gradCells(xs, 1, bt, scheme, volQuirk != 0, g);
-    std::vector<double> t(nC);
-    for (int q = 0; q < 3; ++q)
-    {
-        CFG_CUDA(cudaMemcpyAsync(t.data(), gPF_.c[q], nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-        CFG_CUDA(cudaStreamSynchronize(stream_));
-        for (int c = 0; c < nC; ++c) out[3 * static_cast<size_t>(c) + q] = t[c];
-    }
+    for (int q = 0; q < 3; ++q) fromDevCells(out, gPF_.c[q], 3, q);
 }
 
 void Ctx::poissonSetup(int64_t refCell)
@@ -2022,7 +2052,7 @@ void Ctx::poissonSetup(int64_t refCell)
     CFG_CUDA(cudaMemsetAsync(fScratch_, 0, nF * sizeof(double), stream_));
     CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
     k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, fScratch_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_,
-                                          refCell >= 0 ? static_cast<int>(refCell) : -1, 0.0);
+                                          deviceCell(refCell), 0.0);
     launchCheck("poisson_assemble");
     const int nE = nSlicesEntries_;
     k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, pVal_d_, pVal32_);
@@ -2042,8 +2072,8 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
     CFG_CUDA(cudaSetDevice(device_));
     const int nC = dm_.nC;
     const DMat A{nC, dm_.mStart, dm_.mCol};
-    CFG_CUDA(cudaMemcpyAsync(pb64_, b, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
-    CFG_CUDA(cudaMemcpyAsync(px64_, x, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    toDevCells(pb64_, b, 1, 0);
+    toDevCells(px64_, x, 1, 0);
     // true residual |b - A x|2 / |b|2 in FP64 (r left in cr_)
     auto trueRel = [&]() {
         SolveState s0{};
@@ -2103,8 +2133,7 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
     float ms = 0;
     CFG_CUDA(cudaEventElapsedTime(&ms, tm_.ev[2], tm_.ev[3]));
     const double rel = trueRel();
-    CFG_CUDA(cudaMemcpyAsync(x, px64_, nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    CFG_CUDA(cudaStreamSynchronize(stream_));
+    fromDevCells(x, px64_, 1, 0);
     out[0] = static_cast<double>(inner);
     out[1] = outer;
     out[2] = rel <= tol ? 1.0 : 0.0;

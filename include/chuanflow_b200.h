@@ -177,15 +177,33 @@ int cfg_mesh_geometry(const cfg_mesh* mesh, double* cell_volumes, double* cell_c
                       double* delta_coeff);
 /* makeInternalOwnerWeights / makeFaceSkewVectors (src/3d/src/discrete/interpolate.cpp:28-48) */
 int cfg_mesh_weights(const cfg_mesh* mesh, double* owner_weights, double* skew);
-/* The cell order the device arrays are laid out in (new -> original); the
- * identity unless the mesh was renumbered (no reference counterpart). */
-int cfg_mesh_device_order(const cfg_mesh* mesh, int64_t* new_to_old);
+/* Device cell numbering (no reference counterpart; the reference keeps the
+ * mesh order).  A context lays its cell arrays out in one of these orders;
+ * every per-cell sum keeps the original face and column order, so results
+ * are identical in all of them, and fields cross the ABI in the original
+ * order.  COLOUR: cells grouped by their greedy first-fit colour (computed in
+ * ascending original order), so each multicolour-DIC sweep reads contiguous
+ * rows.  RCM: reverse Cuthill-McKee from a pseudo-peripheral cell, for
+ * locality on unstructured meshes.  DEFAULT: the environment variable
+ * CHUANFLOW_CELL_ORDER (identity | colour | rcm | rcm-colour), else COLOUR. */
+enum cfg_cell_order
+{
+    CFG_ORDER_DEFAULT = -1,
+    CFG_ORDER_IDENTITY = 0,
+    CFG_ORDER_COLOUR = 1,
+    CFG_ORDER_RCM = 2,
+    CFG_ORDER_RCM_COLOUR = 3
+};
+/* The numbering of `order` as new -> original cell index. */
+int cfg_mesh_device_order(const cfg_mesh* mesh, int32_t order, int64_t* new_to_old);
 
 /* ---- case context on one device ------------------------------------------ */
 
 /* Uploads the mesh to `device` and allocates the case state there. `stream`
  * is a cudaStream_t (NULL = a stream created and owned by the context). */
 int cfg_ctx_create(const cfg_mesh* mesh, int32_t device, void* stream, cfg_ctx** out);
+/* cfg_ctx_create with an explicit device cell numbering (cfg_cell_order). */
+int cfg_ctx_create_ordered(const cfg_mesh* mesh, int32_t device, void* stream, int32_t order, cfg_ctx** out);
 void cfg_ctx_destroy(cfg_ctx* ctx);
 
 /* volVectorField::setPatchValue / volScalarField::setPatchValue

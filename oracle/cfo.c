@@ -1783,3 +1783,183 @@ int64_t cfo_pressure_csr(const cfo_mesh* m, const cfo_bcs* bc, const cfo_control
     ws_free(&w);
     return nnz;
 }
+
+/* ------------------------------------------------------------------------
+ * Device cell numbering (the library's cellOrder, no reference counterpart):
+ * restated here so the permutation is checked element for element.
+ *   adjacency: distinct neighbours across internal faces, ascending;
+ *   colours:   first fit in ascending cell order (cfo_colour_cells);
+ *   RCM:       per component, root = unnumbered cell of least (degree,
+ *              index), moved at most 8 times to the least-(degree, index)
+ *              cell of its farthest BFS level while the eccentricity grows;
+ *              breadth-first numbering with neighbours by (degree, index);
+ *              the whole sequence reversed;
+ *   modes:     0 identity, 1 colour blocks of the identity, 2 RCM,
+ *              3 colour blocks of the RCM order (stable).
+ * ------------------------------------------------------------------------ */
+static const int64_t* g_ord_deg;
+
+static int ord_less(int64_t a, int64_t b)
+{
+    return g_ord_deg[a] != g_ord_deg[b] ? g_ord_deg[a] < g_ord_deg[b] : a < b;
+}
+
+static int ord_cmp(const void* pa, const void* pb)
+{
+    const int64_t a = *(const int64_t*)pa, b = *(const int64_t*)pb;
+    return ord_less(a, b) ? -1 : (ord_less(b, a) ? 1 : 0);
+}
+
+static int i64_cmp(const void* pa, const void* pb)
+{
+    const int64_t a = *(const int64_t*)pa, b = *(const int64_t*)pb;
+    return a < b ? -1 : (a > b ? 1 : 0);
+}
+
+/* BFS levels from root over unnumbered cells; eccentricity returned, the
+ * farthest level left in last[0..*nLast) */
+static int ord_bfs(int64_t nC, const int64_t* rs, const int64_t* adj, int64_t root, const char* numbered,
+                   int64_t* stamp, int64_t tag, int64_t* last, int64_t* nLast, int64_t* buf)
+{
+    int64_t* cur = buf;
+    int64_t* next = buf + nC;
+    int64_t nCur = 1, nNext;
+    cur[0] = root;
+    stamp[root] = tag;
+    int ecc = 0;
+    for (;;)
+    {
+        nNext = 0;
+        for (int64_t a = 0; a < nCur; ++a)
+        {
+            const int64_t u = cur[a];
+            for (int64_t k = rs[u]; k < rs[u + 1]; ++k)
+            {
+                const int64_t v = adj[k];
+                if (numbered[v] || stamp[v] == tag) continue;
+                stamp[v] = tag;
+                next[nNext++] = v;
+            }
+        }
+        if (nNext == 0) break;
+        int64_t* t = cur;
+        cur = next;
+        next = t;
+        nCur = nNext;
+        ++ecc;
+    }
+    memcpy(last, cur, (size_t)nCur * sizeof(int64_t));
+    *nLast = nCur;
+    return ecc;
+}
+
+int cfo_cell_order(int64_t nC, int64_t nInt, const int64_t* own, const int64_t* nbr, int32_t mode,
+                   int64_t* newToOld)
+{
+    for (int64_t c = 0; c < nC; ++c) newToOld[c] = c;
+    if (mode == 0) return 0;
+    int64_t* rs = (int64_t*)xcalloc((size_t)(nC + 1), sizeof(int64_t));
+    for (int64_t f = 0; f < nInt; ++f)
+    {
+        ++rs[own[f] + 1];
+        ++rs[nbr[f] + 1];
+    }
+    for (int64_t c = 0; c < nC; ++c) rs[c + 1] += rs[c];
+    int64_t* fill = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+    int64_t* adj = (int64_t*)xcalloc((size_t)rs[nC] + 1, sizeof(int64_t));
+    for (int64_t c = 0; c < nC; ++c) fill[c] = rs[c];
+    for (int64_t f = 0; f < nInt; ++f)
+    {
+        adj[fill[own[f]]++] = nbr[f];
+        adj[fill[nbr[f]]++] = own[f];
+    }
+    int64_t w = 0, s0 = 0;
+    for (int64_t c = 0; c < nC; ++c)
+    {
+        const int64_t b = s0, e = rs[c + 1];
+        qsort(adj + b, (size_t)(e - b), sizeof(int64_t), i64_cmp);
+        for (int64_t k = b; k < e; ++k)
+            if (k == b || adj[k] != adj[k - 1]) adj[w++] = adj[k];
+        s0 = e;
+        rs[c + 1] = w;
+    }
+    if (mode == 2 || mode == 3)
+    {
+        int64_t* deg = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        for (int64_t c = 0; c < nC; ++c) deg[c] = rs[c + 1] - rs[c];
+        g_ord_deg = deg;
+        int64_t* byDeg = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        for (int64_t c = 0; c < nC; ++c) byDeg[c] = c;
+        qsort(byDeg, (size_t)nC, sizeof(int64_t), ord_cmp);
+        char* numbered = (char*)xcalloc((size_t)nC + 1, 1);
+        int64_t* stamp = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        for (int64_t c = 0; c < nC; ++c) stamp[c] = -1;
+        int64_t* last = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        int64_t* last2 = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        int64_t* buf = (int64_t*)xcalloc((size_t)(2 * nC) + 2, sizeof(int64_t));
+        int64_t* nb = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        int64_t* order = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        int64_t nOrd = 0, scan = 0, tag = 0, nLast = 0, nLast2 = 0;
+        while (nOrd < nC)
+        {
+            while (numbered[byDeg[scan]]) ++scan;
+            int64_t root = byDeg[scan];
+            int ecc = ord_bfs(nC, rs, adj, root, numbered, stamp, tag++, last, &nLast, buf);
+            for (int round = 0; round < 8; ++round)
+            {
+                int64_t cand = last[0];
+                for (int64_t a = 0; a < nLast; ++a)
+                    if (ord_less(last[a], cand)) cand = last[a];
+                const int ecc2 = ord_bfs(nC, rs, adj, cand, numbered, stamp, tag++, last2, &nLast2, buf);
+                if (ecc2 <= ecc) break;
+                root = cand;
+                ecc = ecc2;
+                memcpy(last, last2, (size_t)nLast2 * sizeof(int64_t));
+                nLast = nLast2;
+            }
+            int64_t head = nOrd;
+            order[nOrd++] = root;
+            numbered[root] = 1;
+            while (head < nOrd)
+            {
+                const int64_t u = order[head++];
+                int64_t m = 0;
+                for (int64_t k = rs[u]; k < rs[u + 1]; ++k)
+                    if (!numbered[adj[k]]) nb[m++] = adj[k];
+                qsort(nb, (size_t)m, sizeof(int64_t), ord_cmp);
+                for (int64_t a = 0; a < m; ++a)
+                {
+                    numbered[nb[a]] = 1;
+                    order[nOrd++] = nb[a];
+                }
+            }
+        }
+        for (int64_t i = 0; i < nC; ++i) newToOld[i] = order[nC - 1 - i];
+        free(deg);
+        free(byDeg);
+        free(numbered);
+        free(stamp);
+        free(last);
+        free(last2);
+        free(buf);
+        free(nb);
+        free(order);
+    }
+    if (mode == 1 || mode == 3)
+    {
+        int32_t* colour = (int32_t*)xcalloc((size_t)nC + 1, sizeof(int32_t));
+        const int32_t nCol = cfo_colour_cells(nC, rs, adj, colour);
+        int64_t* tmp = (int64_t*)xcalloc((size_t)nC + 1, sizeof(int64_t));
+        int64_t t = 0;
+        for (int32_t col = 0; col < nCol; ++col)
+            for (int64_t i = 0; i < nC; ++i)
+                if (colour[newToOld[i]] == col) tmp[t++] = newToOld[i];
+        memcpy(newToOld, tmp, (size_t)nC * sizeof(int64_t));
+        free(colour);
+        free(tmp);
+    }
+    free(rs);
+    free(fill);
+    free(adj);
+    return 0;
+}

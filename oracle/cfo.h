@@ -184,6 +184,11 @@ int64_t cfo_pressure_csr(const cfo_mesh* m, const cfo_bcs* bc, const cfo_control
 
 const char* cfo_last_error(void);
 
+/* the library's device cell numbering (new -> old) for mode 0 identity,
+ * 1 colour blocks, 2 reverse Cuthill-McKee, 3 colour blocks of RCM */
+int cfo_cell_order(int64_t nC, int64_t nInt, const int64_t* own, const int64_t* nbr, int32_t mode,
+                   int64_t* newToOld);
+
 #ifdef __cplusplus
 }
 #endif

@@ -112,14 +112,14 @@ simple
 """
 
 
-def cavity_product(nx, ny, nz, jitter=0.1, seed=7, device=0, schemes=None):
+def cavity_product(nx, ny, nz, jitter=0.1, seed=7, device=0, schemes=None, order=None):
     """The same cavity through chuanflow_b200 (mesh, BCs, initial flux)."""
     import chuanflow_b200 as cf
     mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (nx, ny, nz),
                              {s: (n, "wall") for s, n in zip(SIDES, CAVITY_NAMES)})
     if jitter:
         mesh.jitter_interior(jitter, seed)
-    case = cf.SimpleCase(mesh, device, schemes)
+    case = cf.SimpleCase(mesh, device, schemes, order=order)
     for n in CAVITY_NAMES:
         case.set_patch_bc("U", n, "fixedValue", (1.0, 0, 0) if n == "lid" else (0, 0, 0))
         case.set_patch_bc("p", n, "zeroGradient", 0.0)

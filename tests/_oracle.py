@@ -350,6 +350,17 @@ def dic(rs, cols, vals):
 # sources by oracle/Makefile)
 # --------------------------------------------------------------------------
 
+def cell_order(n_cells, owner, neighbour, mode):
+    """The restated device cell numbering (new -> old); mode 0..3 =
+    identity, colour, rcm, rcm-colour."""
+    own = np.ascontiguousarray(owner, np.int64)
+    nbr = np.ascontiguousarray(neighbour, np.int64)
+    out = np.zeros(n_cells, np.int64)
+    _check(lib().cfo_cell_order(C.c_int64(n_cells), C.c_int64(nbr.size), _p(own, _i64p), _p(nbr, _i64p),
+                                C.c_int32(mode), _p(out, _i64p)))
+    return out
+
+
 def have_ref():
     return os.path.exists(REF_DRIVER)
 

@@ -44,11 +44,13 @@ def test_gradients_bit_exact(golden, fixture):
             assert np.array_equal(got, g[f"grad_vol_{s}_{fname}"]), (fixture, fname, s, "vol")
 
 
-def test_equations_bit_exact(golden):
+@pytest.mark.parametrize("order", ["identity", "colour", "rcm", "rcm-colour"])
+def test_equations_bit_exact(golden, order):
     """Momentum and pressure assembly, gradients, rAUf, div(phi), continuity
-    and the flux correction of one outer iteration equal the reference's."""
+    and the flux correction of one outer iteration equal the reference's, in
+    every device cell numbering."""
     g = golden("eqns_cavity.npz")
-    mesh, case = K.cavity_product(6, 5, 4)
+    mesh, case = K.cavity_product(6, 5, 4, order=order)
     assert np.array_equal(mesh.addressing()["points"], g["points"])
     case.upload(g["in_U"], g["in_p"], g["in_phi"])
     ctl = K.controls_from(K.cavity_case(6, 5, 4))
@@ -105,11 +107,13 @@ def test_sparse_solvers_match_reference(golden, fixture, method):
     assert rep.initial_residual == float(g["initial"])
 
 
-def test_dic_factor_and_apply_bit_exact(golden):
+@pytest.mark.parametrize("order", ["identity", "colour", "rcm-colour"])
+def test_dic_factor_and_apply_bit_exact(golden, order):
     """The multicolour DIC of the device pressure matrix equals the oracle's
-    restatement of the same definition (oracle/cfo.c) on the same matrix."""
+    restatement of the same definition (oracle/cfo.c) on the same matrix, in
+    any device cell numbering."""
     g = golden("eqns_cavity.npz")
-    mesh, case = K.cavity_product(6, 5, 4)
+    mesh, case = K.cavity_product(6, 5, 4, order=order)
     case.upload(g["in_U"], g["in_p"], g["in_phi"])
     oc = K.cavity_case(6, 5, 4)
     out = case.probe_equations(K.controls_from(oc), g["in_xprobe"])
@@ -136,15 +140,16 @@ def test_simple_cavity_dic_matches_oracle(cells, jitter):
     assert rel(U, U0) < REL_TOL and rel(p, p0) < REL_TOL and rel(phi, phi0) < REL_TOL
 
 
+@pytest.mark.parametrize("order", ["colour", "rcm-colour"])
 @pytest.mark.parametrize("method", ["jacobi64", "dic64", "ir32"])
-def test_poisson_solves_match_oracle(method):
+def test_poisson_solves_match_oracle(method, order):
     """The pressure-Poisson study system (unit face coefficient, Neumann,
     one reference cell) on a Delaunay tet mesh: every method reaches the
     requested FP64 true residual and the oracle's FP64 solution."""
     from chuanflow_b200 import meshgen
     mesh, pts, tets = meshgen.tet_mesh(10, 0.1, 2)
     import chuanflow_b200 as cf
-    case = cf.SimpleCase(mesh)
+    case = cf.SimpleCase(mesh, order=order)
     case.poisson_setup(ref_cell=0)
     rng = np.random.default_rng(1)
     b = rng.normal(size=mesh.n_cells)

@@ -122,3 +122,49 @@ def test_mesh_from_cells_hex_and_prism():
     assert np.allclose(m.geometry()["V"], 0.5)
     with pytest.raises(cf.CfgError, match="not tet"):
         cf.PolyMesh.from_cells(pts, [7], [0, 5], [0, 1, 2, 3, 4])
+
+
+ORDERS = ("identity", "colour", "rcm", "rcm-colour")
+
+
+@pytest.mark.parametrize("source", ["block", "mesh_tets22.npz", "mesh_hex41.npz", "mesh_delaunay.npz"])
+def test_device_cell_order_matches_restatement(golden, source):
+    """The device numbering (colour blocks, reverse Cuthill-McKee and both)
+    is a permutation equal element for element to the oracle's restatement;
+    colour blocks are contiguous and no two neighbours share a colour."""
+    if source == "block":
+        m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (7, 5, 4))
+    else:
+        g = golden(source)
+        pats = [(str(n), str(t), int(s), int(z)) for n, t, s, z in
+                zip(g["patch_names"], g["patch_types"], g["patch_start"], g["patch_size"])]
+        m = cf.PolyMesh(g["points"], g["face_offsets"], g["face_verts"], g["owner"], g["neighbour"], pats)
+    a = m.addressing()
+    for mode, name in enumerate(ORDERS):
+        got = m.device_order(name)
+        assert np.array_equal(np.sort(got), np.arange(m.n_cells)), name
+        assert np.array_equal(got, O.cell_order(m.n_cells, a["owner"], a["neighbour"], mode)), name
+    # colours along the colour-block order: non-decreasing, proper
+    own, nbr = a["owner"][:m.n_internal_faces], a["neighbour"]
+    col = np.full(m.n_cells, -1)
+    for c in range(m.n_cells):
+        used = {col[x] for x in np.concatenate([nbr[own == c], own[nbr == c]]) if col[x] >= 0}
+        k = 0
+        while k in used:
+            k += 1
+        col[c] = k
+    assert np.all(col[own] != col[nbr])
+    blocks = col[m.device_order("colour")]
+    assert np.all(np.diff(blocks) >= 0)
+
+
+def test_rcm_reduces_bandwidth_of_shuffled_mesh(golden):
+    """Reverse Cuthill-McKee on the Delaunay mesh (cells in qhull's order)
+    shrinks the matrix bandwidth max|i - j| over neighbour pairs."""
+    g = golden("mesh_delaunay.npz")
+    own, nbr = g["owner"][:g["neighbour"].size], g["neighbour"]
+    n = int(max(own.max(), nbr.max())) + 1
+    perm = O.cell_order(n, own, nbr, 2)
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    assert np.abs(inv[own] - inv[nbr]).max() < np.abs(own - nbr).max()
