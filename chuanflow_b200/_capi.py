@@ -324,7 +324,7 @@ class SimpleCase:
 
     def __init__(self, mesh: PolyMesh, device: int = 0, schemes: Schemes | None = None, order: str | None = None):
         """order: the device cell numbering ("identity", "colour", "rcm",
-        "rcm-colour"); None takes CHUANFLOW_CELL_ORDER, else "colour"."""
+        "rcm-colour"); None takes CHUANFLOW_CELL_ORDER, else "identity"."""
         self.mesh = mesh
         h = C.c_void_p()
         _check(lib().cfg_ctx_create_ordered(mesh._h, C.c_int32(device), None, C.c_int32(CELL_ORDER[order]),

@@ -637,7 +637,7 @@ int defaultCellOrder()
         if (s == "rcm") return CFG_ORDER_RCM;
         if (s == "rcm-colour") return CFG_ORDER_RCM_COLOUR;
     }
-    return CFG_ORDER_COLOUR;
+    return CFG_ORDER_IDENTITY;
 }
 
 std::vector<int64_t> cellOrder(const Mesh& M, int mode)

@@ -184,8 +184,10 @@ int cfg_mesh_weights(const cfg_mesh* mesh, double* owner_weights, double* skew);
  * order.  COLOUR: cells grouped by their greedy first-fit colour (computed in
  * ascending original order), so each multicolour-DIC sweep reads contiguous
  * rows.  RCM: reverse Cuthill-McKee from a pseudo-peripheral cell, for
- * locality on unstructured meshes.  DEFAULT: the environment variable
- * CHUANFLOW_CELL_ORDER (identity | colour | rcm | rcm-colour), else COLOUR. */
+ * locality on meshes whose cells come in no spatial order.  DEFAULT: the
+ * environment variable CHUANFLOW_CELL_ORDER (identity | colour | rcm |
+ * rcm-colour), else IDENTITY (measured fastest on block and Delaunay meshes,
+ * whose own order is already local). */
 enum cfg_cell_order
 {
     CFG_ORDER_DEFAULT = -1,
