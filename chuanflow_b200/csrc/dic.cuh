@@ -30,8 +30,34 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_gather(int n, con
     ROW_LOOP(e, n) out[e] = src[e] >= 0 ? static_cast<T>(val[src[e]]) : T(0);
 }
 
+/// One row's entries of a colour slice (lane `lane`, entries e0 + 32k below
+/// e1): columns and values loaded for all W slots first, then the gathered
+/// x_j, so a row costs one index latency and one gather latency however
+/// many entries it has.  Pads (column -1) come after a row's last entry.
+/// W = 0 walks the list entry by entry.
+template <int W, class T>
+struct DicRow
+{
+    int col[W > 0 ? W : 1];
+    T val[W > 0 ? W : 1];
+    T x[W > 0 ? W : 1];
+    __device__ __forceinline__ void load(const int* __restrict__ cols, const T* __restrict__ vals, int e0, int e1,
+                                         const T* __restrict__ xs)
+    {
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+        {
+            const int e = e0 + 32 * k;
+            col[k] = e < e1 ? __ldg(cols + e) : -1;
+            val[k] = e < e1 ? __ldg(vals + e) : T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k) x[k] = col[k] >= 0 ? xs[col[k]] : T(0);
+    }
+};
+
 /// rD_i = a_ii - sum a_ij^2 / rD_j over the lower entries, one colour
-template <class T>
+template <int W, class T>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_factor(DDicT<T> D, DicPhase ph, const T* __restrict__ diag)
 {
     FOR_ROWS(t, ph.cnt)
@@ -39,12 +65,24 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_factor(DDicT<T> D
         const int i = D.rows[ph.off + t];
         const int sl = ph.slice0 + (t >> 5), lane = t & 31;
         T d = diag[i];
-        for (int e = D.lStart[sl] + lane; e < D.lStart[sl + 1]; e += 32)
+        const int e0 = D.lStart[sl] + lane, e1 = D.lStart[sl + 1];
+        if constexpr (W > 0)
         {
-            const int j = D.lCol[e];
-            if (j < 0) break;
-            const T a = D.lVal[e];
-            d = d - a * a / D.rD[j];
+            DicRow<W, T> rw;
+            rw.load(D.lCol, D.lVal, e0, e1, D.rD);
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                if (rw.col[k] >= 0) d = d - rw.val[k] * rw.val[k] / rw.x[k];
+        }
+        else
+        {
+            for (int e = e0; e < e1; e += 32)
+            {
+                const int j = D.lCol[e];
+                if (j < 0) break;
+                const T a = D.lVal[e];
+                d = d - a * a / D.rD[j];
+            }
         }
         D.rD[i] = d;
         D.rDinv[i] = T(1) / d;
@@ -53,7 +91,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_factor(DDicT<T> D
 
 /// forward phase of one colour: z_i = rDinv_i (r_i - sum_lower a_ij z_j);
 /// the last colour's rows also contribute their r_i z_i partials
-template <class T>
+template <int W, class T>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_fwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int last,
                                                  double* partials, SolveState* st)
 {
@@ -64,11 +102,23 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_fwd(DDicT<T> D, D
         const int i = D.rows[ph.off + t];
         const int sl = ph.slice0 + (t >> 5), lane = t & 31;
         T s = T(0);
-        for (int e = D.lStart[sl] + lane; e < D.lStart[sl + 1]; e += 32)
+        const int e0 = D.lStart[sl] + lane, e1 = D.lStart[sl + 1];
+        if constexpr (W > 0)
         {
-            const int j = D.lCol[e];
-            if (j < 0) break;
-            s += D.lVal[e] * z[j];
+            DicRow<W, T> rw;
+            rw.load(D.lCol, D.lVal, e0, e1, z);
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                if (rw.col[k] >= 0) s += rw.val[k] * rw.x[k];
+        }
+        else
+        {
+            for (int e = e0; e < e1; e += 32)
+            {
+                const int j = D.lCol[e];
+                if (j < 0) break;
+                s += D.lVal[e] * z[j];
+            }
         }
         const T ri = r[i];
         const T zi = D.rDinv[i] * (ri - s);
@@ -83,7 +133,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_fwd(DDicT<T> D, D
 /// backward phase of one colour: z_i -= rDinv_i sum_upper a_ij z_j, with
 /// the r_i z_i partials; `final` (the phase that runs last) also reduces
 /// all colours' partials into r.z and advances beta
-template <class T>
+template <int W, class T>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_bwd(DDicT<T> D, DicPhase ph, const T* __restrict__ r, T* z, int final,
                                                  int nPartials, double* partials, SolveState* st)
 {
@@ -94,11 +144,23 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_dic_bwd(DDicT<T> D, D
         const int i = D.rows[ph.off + t];
         const int sl = ph.slice0 + (t >> 5), lane = t & 31;
         T s = T(0);
-        for (int e = D.uStart[sl] + lane; e < D.uStart[sl + 1]; e += 32)
+        const int e0 = D.uStart[sl] + lane, e1 = D.uStart[sl + 1];
+        if constexpr (W > 0)
         {
-            const int j = D.uCol[e];
-            if (j < 0) break;
-            s += D.uVal[e] * z[j];
+            DicRow<W, T> rw;
+            rw.load(D.uCol, D.uVal, e0, e1, z);
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                if (rw.col[k] >= 0) s += rw.val[k] * rw.x[k];
+        }
+        else
+        {
+            for (int e = e0; e < e1; e += 32)
+            {
+                const int j = D.uCol[e];
+                if (j < 0) break;
+                s += D.uVal[e] * z[j];
+            }
         }
         const T zi = z[i] - D.rDinv[i] * s;
         z[i] = zi;

@@ -1434,28 +1434,35 @@ void Ctx::dicSetupT(DDicT<T>& D, const double* vals, const T* diag)
     k_dic_gather<T><<<std::max(1, std::min((nLo_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nLo_, D.lSrc, vals, D.lVal);
     k_dic_gather<T><<<std::max(1, std::min((nUp_ + TPB - 1) / TPB, 4096)), TPB, 0, stream_>>>(nUp_, D.uSrc, vals, D.uVal);
     launchCheck("dic_gather");
-    for (const DicPhase& ph : dicPhase_)
-    {
-        k_dic_factor<T><<<rowGrid(ph.cnt), TPB, 0, stream_>>>(D, ph, diag);
-        launchCheck("dic_factor");
-    }
+    dispatchW(maxW_, [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        for (const DicPhase& ph : dicPhase_)
+        {
+            k_dic_factor<W, T><<<rowGrid(ph.cnt), TPB, 0, stream_>>>(D, ph, diag);
+            launchCheck("dic_factor");
+        }
+    });
 }
 
 template <class T>
 void Ctx::dicApplyT(const DDicT<T>& D, const T* r, T* z)
 {
     const int C = D.nColours;
-    for (int c = 0; c < C; ++c)
-        k_dic_fwd<T><<<rowGrid(dicPhase_[c].cnt), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == C - 1, partials_, st_);
-    if (C == 1)
-    {
-        // no backward phase: a one-block final reduction of the forward partials
-        const DicPhase none{0, 0, 0, dicPartials_ - 1};
-        k_dic_bwd<T><<<1, TPB, 0, stream_>>>(D, none, r, z, 1, dicPartials_, partials_, st_);
-    }
-    for (int c = C - 2; c >= 0; --c)
-        k_dic_bwd<T><<<rowGrid(dicPhase_[c].cnt), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == 0,
-                                                                   c == 0 ? dicPartials_ - 1 : 0, partials_, st_);
+    dispatchW(maxW_, [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        for (int c = 0; c < C; ++c)
+            k_dic_fwd<W, T><<<rowGrid(dicPhase_[c].cnt), TPB, 0, stream_>>>(D, dicPhase_[c], r, z, c == C - 1,
+                                                                            partials_, st_);
+        if (C == 1)
+        {
+            // no backward phase: a one-block final reduction of the forward partials
+            const DicPhase none{0, 0, 0, dicPartials_ - 1};
+            k_dic_bwd<W, T><<<1, TPB, 0, stream_>>>(D, none, r, z, 1, dicPartials_, partials_, st_);
+        }
+        for (int c = C - 2; c >= 0; --c)
+            k_dic_bwd<W, T><<<rowGrid(dicPhase_[c].cnt), TPB, 0, stream_>>>(
+                D, dicPhase_[c], r, z, c == 0, c == 0 ? dicPartials_ - 1 : 0, partials_, st_);
+    });
     launchCheck("dic_apply", C == 1 ? 2 : 2 * C - 1);
 }
 
