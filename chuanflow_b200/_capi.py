@@ -13,7 +13,7 @@ _SO = os.path.join(_HERE, "libchuanflow_b200.so")
 BC = {"fixedValue": 0, "zeroGradient": 1, "fixedGradient": 2, "symmetry": 3, "outlet": 4, "wall": 5,
       "empty": 6}
 GRAD = {"linear": 0, "corrected": 1, "leastSquares": 2}
-DIV = {"upwind": 0, "linear": 1, "blend": 2}
+DIV = {"upwind": 0, "linear": 1, "blend": 2, "linearUpwind": 3}
 PRECOND = {"Jacobi": 0, "DIC": 1}
 
 _f64p = C.POINTER(C.c_double)

@@ -37,18 +37,18 @@ int bcType(const std::string& s)
 
 cfg_schemes toSchemes(const Schemes& s)
 {
+    // names the reference does not know select its defaults, as its own
+    // string tests do (divScheme.cpp:18, laplacianScheme.cpp:71,
+    // gradScheme.cpp:251-275); "linearUpwind" is this library's extension
     cfg_schemes out{};
-    if (s.div == "upwind") out.div = CFG_DIV_UPWIND;
-    else if (s.div == "linear") out.div = CFG_DIV_LINEAR;
-    else if (s.div == "blend") out.div = CFG_DIV_BLEND;
-    else throw Error("chuanflow_b200: div scheme '" + s.div + "' is not on the GPU path");
-    if (s.laplacian == "corrected") out.laplacian_corrected = 1;
-    else if (s.laplacian == "none") out.laplacian_corrected = 0;
-    else throw Error("chuanflow_b200: laplacian scheme '" + s.laplacian + "' is not on the GPU path");
-    if (s.grad == "linear") out.grad = CFG_GRAD_LINEAR;
-    else if (s.grad == "corrected") out.grad = CFG_GRAD_CORRECTED;
-    else if (s.grad == "leastSquares") out.grad = CFG_GRAD_LEAST_SQUARES;
-    else throw Error("chuanflow_b200: grad scheme '" + s.grad + "' is not on the GPU path");
+    out.div = s.div == "linear" ? CFG_DIV_LINEAR
+              : s.div == "blend" ? CFG_DIV_BLEND
+              : s.div == "linearUpwind" ? CFG_DIV_LINEAR_UPWIND
+                                        : CFG_DIV_UPWIND;
+    out.laplacian_corrected = s.laplacian == "corrected" ? 1 : 0;
+    out.grad = s.grad == "leastSquares" ? CFG_GRAD_LEAST_SQUARES
+               : s.grad == "corrected" ? CFG_GRAD_CORRECTED
+                                       : CFG_GRAD_LINEAR;
     out.blend_coeff = s.blendCoeff;
     return out;
 }

@@ -349,7 +349,7 @@ int cfg_set_schemes(cfg_ctx* ctx, const cfg_schemes* s)
 {
     return guard([&] {
         need(ctx && s, "cfg_set_schemes: null argument");
-        need(s->div >= 0 && s->div <= 2 && s->grad >= 0 && s->grad <= 2, "cfg_set_schemes: unknown scheme");
+        need(s->div >= 0 && s->div <= CFG_DIV_LINEAR_UPWIND && s->grad >= 0 && s->grad <= 2, "cfg_set_schemes: unknown scheme");
         ctx->c->setSchemes(*s);
     });
 }
@@ -572,7 +572,11 @@ CaseSpec parseCase(const char* path)
     {
         const cfg::Dict& s = d.dict("schemes");
         const std::string div = s.wordOr("div", "upwind");
-        cs.schemes.div = div == "linear" ? CFG_DIV_LINEAR : (div == "blend" ? CFG_DIV_BLEND : CFG_DIV_UPWIND);
+        // unknown names fall back to upwind, as fvm::div's alpha selection does
+        cs.schemes.div = div == "linear" ? CFG_DIV_LINEAR
+                         : div == "blend" ? CFG_DIV_BLEND
+                         : div == "linearUpwind" ? CFG_DIV_LINEAR_UPWIND
+                                                 : CFG_DIV_UPWIND;
         cs.schemes.laplacian_corrected = s.wordOr("laplacian", "corrected") == "corrected";
         const std::string g = s.wordOr("grad", "corrected");
         cs.schemes.grad =

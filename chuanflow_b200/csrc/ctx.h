@@ -88,6 +88,7 @@ private:
     void runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
                   cfg_solver_report* reps);
     void launchCheck(const char* what, int kernels = 1);
+    int linUpwindGrad(const BcTab& ub, int gradScheme);
     template <class F>
     void launchChunk(const std::string& key, int n, F&& body);
     void dicSetup(const double* vals, const double* diag);

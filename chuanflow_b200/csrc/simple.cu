@@ -46,9 +46,11 @@ struct MomArgs
     const double* phi;
     const double* gamma;
     BcTab ub;
-    double alpha;  // 0 upwind, 1 linear, blendCoeff for blend
+    double alpha;  // 0 upwind (and linear-upwind), 1 linear, blendCoeff for blend
     double force[3];
     CV3P gPn;
+    int linUpwind;  // add the linear-upwind deferred correction from gUc
+    CGrad3 gUc;     // grad of each U component, when linUpwind
     double* mVal;
     double* uDiag;
     V3P base;
@@ -119,6 +121,40 @@ __global__ void __launch_bounds__(TPB) k_assemble_U(DMesh m, MomArgs a)
         r0 += ((a.force[0] + 0.0) - a.gPn.c[0][c]) * v;
         r1 += ((a.force[1] + 0.0) - a.gPn.c[1][c]) * v;
         r2 += ((a.force[2] + 0.0) - a.gPn.c[2][c]) * v;
+        if (a.linUpwind)
+        {
+            // linear-upwind deferred correction: -phi_f (grad U)_u.(Cf - C_u)
+            // on the owner row, + on the neighbour row, in face order
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+            for (int e = e0; e < e1; e += 32)
+            {
+                const int code = m.cfCode[e];
+                if (code < 0) break;
+                const int f = code >> 1, side = code & 1;
+                if (f >= m.nI) continue;
+                const double p = a.phi[f];
+                const int u = p >= 0 ? m.own[f] : m.nbr[f];
+                const double dx = m.fcx[f] - m.cx[u], dy = m.fcy[f] - m.cy[u], dz = m.fcz[f] - m.cz[u];
+                const double k0 = p * (a.gUc.g[0].c[0][u] * dx + a.gUc.g[0].c[1][u] * dy + a.gUc.g[0].c[2][u] * dz);
+                const double k1 = p * (a.gUc.g[1].c[0][u] * dx + a.gUc.g[1].c[1][u] * dy + a.gUc.g[1].c[2][u] * dz);
+                const double k2 = p * (a.gUc.g[2].c[0][u] * dx + a.gUc.g[2].c[1][u] * dy + a.gUc.g[2].c[2][u] * dz);
+                if (side)
+                {
+                    s0 = s0 + k0;
+                    s1 = s1 + k1;
+                    s2 = s2 + k2;
+                }
+                else
+                {
+                    s0 = s0 - k0;
+                    s1 = s1 - k1;
+                    s2 = s2 - k2;
+                }
+            }
+            r0 += s0;
+            r1 += s1;
+            r2 += s2;
+        }
         a.uDiag[c] = diag;
         a.base.c[0][c] = r0;
         a.base.c[1][c] = r1;
@@ -1156,6 +1192,18 @@ void Ctx::refreshBc()
     bcDirty_ = false;
 }
 
+/// With linear-upwind convection, fvc::grad of the three U components (the
+/// iterate the momentum equation is assembled from) into gA_, gB_, Hf_,
+/// which the momentum solve only overwrites after assembly; returns 1 then.
+int Ctx::linUpwindGrad(const BcTab& ub, int gradScheme)
+{
+    if (schemes_.div != CFG_DIV_LINEAR_UPWIND) return 0;
+    const double* xs[3] = {U_.c[0], U_.c[1], U_.c[2]};
+    V3P g[3] = {gA_, gB_, Hf_};
+    gradCells(xs, 3, ub, gradScheme, true, g);
+    return 1;
+}
+
 void Ctx::launchCheck(const char* what, int kernels)
 {
     launches_ += kernels;
@@ -1794,7 +1842,8 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
             gradCells(xs, 1, pb, gs, true, g);
         }
         MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
-                   mVal_, uDiag_, uBase_};
+                   linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_};
+        ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
         k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
         launchCheck("assemble_U");
         solveMomentum(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, res.u_inner_iterations);
@@ -1909,8 +1958,9 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
         gradCells(xs, 1, pb, gs, true, g);
     }
     for (int q = 0; q < 3; ++q) d2hC(gPn_.c[q]);
-    MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_), mVal_,
-               uDiag_, uBase_};
+    MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
+               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_};
+    ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
     k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
     launchCheck("assemble_U");
     // one pass with maxIter 0: rhs = base + corrector(x = 0)

@@ -51,7 +51,12 @@ enum cfg_bc_type
 };
 
 enum cfg_grad_scheme { CFG_GRAD_LINEAR = 0, CFG_GRAD_CORRECTED = 1, CFG_GRAD_LEAST_SQUARES = 2 };
-enum cfg_div_scheme { CFG_DIV_UPWIND = 0, CFG_DIV_LINEAR = 1, CFG_DIV_BLEND = 2 };
+/* upwind, linear and blend as fvm::div (src/3d/src/discrete/divScheme.cpp:11-62);
+ * LINEAR_UPWIND is this library's extension (no reference counterpart): the
+ * upwind matrix plus a deferred correction phi_f (grad U)_u.(Cf - C_u) of the
+ * upwind cell's gradient (the case's grad scheme, U's conditions) on the
+ * right-hand side, evaluated on the iterate each equation is assembled from */
+enum cfg_div_scheme { CFG_DIV_UPWIND = 0, CFG_DIV_LINEAR = 1, CFG_DIV_BLEND = 2, CFG_DIV_LINEAR_UPWIND = 3 };
 enum cfg_lin_method { CFG_SOLVE_CG = 0, CFG_SOLVE_BICGSTAB = 1 };
 /* pressure preconditioner: the reference's Jacobi PCG, or this library's
  * multicolour DIC (no reference counterpart) */

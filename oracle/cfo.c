@@ -1353,15 +1353,55 @@ int cfo_flux_from_U(const cfo_mesh* m, const cfo_bcs* bc, const double* U, doubl
 }
 
 /* the momentum equation of one outer iteration (simpleSolver.cpp:67-112) */
+/* Linear-upwind convection (this library's extension; the reference's
+ * fvm::div knows upwind, linear and blend only, divScheme.cpp:18): the
+ * face value is the upwind cell's value extrapolated along its gradient,
+ * U_f = U_u + (grad U)_u . (Cf - C_u), u the upwind cell of phi_f >= 0 ->
+ * owner.  The matrix keeps the upwind part; the extrapolation, evaluated on
+ * the iterate the equation is assembled from with fvc::grad of each
+ * component under U's conditions and the case's grad scheme, is a deferred
+ * correction: -phi_f d_f on the owner's right-hand side, +phi_f d_f on the
+ * neighbour's, summed per cell in face order and added after the other
+ * right-hand-side terms. */
+static void linear_upwind_rhs(fvmat* U, const simple_ws* w, const cfo_controls* ctl, const double* uc,
+                              const double* uk, const double* phi, const double* Ucur)
+{
+    const cfo_mesh* m = w->g.m;
+    const int64_t nC = m->nC, nB = m->nF - m->nInt;
+    double* comp = (double*)xcalloc((size_t)nC, sizeof(double));
+    double* g = (double*)xcalloc((size_t)(3 * nC), sizeof(double));
+    double* s = (double*)xcalloc((size_t)nC, sizeof(double));
+    for (int q = 0; q < 3; ++q)
+    {
+        for (int64_t c = 0; c < nC; ++c) comp[c] = Ucur[3 * c + q];
+        vol_grad(w, comp, uc + q * nB, uk + q * nB, ctl->grad, g);
+        memset(s, 0, sizeof(double) * (size_t)nC);
+        for (int64_t f = 0; f < m->nInt; ++f)
+        {
+            const int64_t o = m->own[f], nb = m->nbr[f];
+            const double p = phi[f];
+            const int64_t u = p >= 0 ? o : nb;
+            const v3 d = vsub(ld(m->Cf, f), ld(m->C, u));
+            const double corr = p * vdot(ld(g, u), d);
+            s[o] = s[o] - corr;
+            s[nb] = s[nb] + corr;
+        }
+        for (int64_t c = 0; c < nC; ++c) U->rhs[q * nC + c] += s[c];
+    }
+    free(comp);
+    free(g);
+    free(s);
+}
+
 static int build_ueqn(fvmat* U, const simple_ws* w, const cfo_controls* ctl, const double* uc, const double* uk,
-                      const double* phi, const double* gradPn)
+                      const double* phi, const double* gradPn, const double* Ucur)
 {
     const cfo_mesh* m = w->g.m;
     const int64_t nB = m->nF - m->nInt;
     fvmat_init(U, 3, m->nC, 4 * m->nInt, nB);
     memcpy(U->bc_c, uc, sizeof(double) * (size_t)(3 * nB));
     memcpy(U->bc_k, uk, sizeof(double) * (size_t)(3 * nB));
-    fvm_div(U, &w->g, phi, ctl->div, ctl->blendCoeff, 1);
+    fvm_div(U, &w->g, phi, ctl->div == CFO_DIV_LINEAR_UPWIND ? CFO_DIV_UPWIND : ctl->div, ctl->blendCoeff, 1);
     fvm_laplacian(U, &w->g, w->gammaU, ctl->laplacianCorrected, -1);
     for (int64_t c = 0; c < m->nC; ++c)
     {
@@ -1369,6 +1409,7 @@ static int build_ueqn(fvmat* U, const simple_ws* w, const cfo_controls* ctl, con
         const v3 rhs = vmul(vsub(vadd(f0, V3(0, 0, 0)), ld(gradPn, c)), m->V[c]);
         for (int q = 0; q < 3; ++q) U->rhs[q * m->nC + c] += vcomp(rhs, q);
     }
+    if (ctl->div == CFO_DIV_LINEAR_UPWIND) linear_upwind_rhs(U, w, ctl, uc, uk, phi, Ucur);
     return 0;
 }
 
@@ -1444,7 +1485,7 @@ int cfo_simple(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, do
     {
         vol_grad(&w, p, pc, pk, ctl->grad, gradPn);
         fvmat UE;
-        build_ueqn(&UE, &w, ctl, uc, uk, phi, gradPn);
+        build_ueqn(&UE, &w, ctl, uc, uk, phi, gradPn, U);
         g_innerSum = 0;
         const cfo_report uRep = fvmat_solve(&UE, &w.g, ctl->linearTol, ctl->linearMaxIter, ctl->nonOrthCorrectors, ctl->grad);
         res->uItersTotal += g_innerSum;
@@ -1580,7 +1621,7 @@ int cfo_eqns(const cfo_mesh* m, const cfo_bcs* bc, const cfo_controls* ctl, cons
     }
     vol_grad(&w, p, pc, pk, ctl->grad, gradPn);
     fvmat UE;
-    build_ueqn(&UE, &w, ctl, uc, uk, phi, gradPn);
+    build_ueqn(&UE, &w, ctl, uc, uk, phi, gradPn, U);
     fvmat_solve(&UE, &w.g, ctl->linearTol, 0, 0, ctl->grad);
     for (int q = 0; q < 3; ++q)
     {

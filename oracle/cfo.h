@@ -43,7 +43,8 @@ enum cfo_div
 {
     CFO_DIV_UPWIND = 0,
     CFO_DIV_LINEAR = 1,
-    CFO_DIV_BLEND = 2
+    CFO_DIV_BLEND = 2,
+    CFO_DIV_LINEAR_UPWIND = 3 /* this library's extension, no reference counterpart */
 };
 
 typedef struct cfo_mesh

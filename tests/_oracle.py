@@ -22,7 +22,7 @@ REF_DRIVER = os.path.join(ORACLE_DIR, "_ref", "cf_ref_driver")
 BC = {"fixedValue": 0, "zeroGradient": 1, "fixedGradient": 2, "symmetry": 3, "outlet": 4,
       "wall": 5, "empty": 6}
 GRAD = {"linear": 0, "corrected": 1, "leastSquares": 2}
-DIV = {"upwind": 0, "linear": 1, "blend": 2}
+DIV = {"upwind": 0, "linear": 1, "blend": 2, "linearUpwind": 3}
 
 _f64p = C.POINTER(C.c_double)
 _i64p = C.POINTER(C.c_int64)

@@ -40,16 +40,34 @@ def test_adapter_reproduces_reference_channel(golden):
         assert rel(a, b) < REL_TOL, (name, rel(a, b))
 
 
-@pytest.mark.skipif(not os.path.exists(DRIVER), reason="oracle/_ref/cf_adapter_driver not built")
-def test_adapter_rejects_what_the_gpu_path_lacks():
-    """A scheme the GPU path does not carry is a cf::Error, as the
-    reference's own unknown-scheme errors are; the driver exits non-zero."""
-    text = ("block { min (0 0 0); max (1 1 1); cells (3 3 3); }\nnu 0.01;\n"
-            "schemes { ddt steady; div QUICK; laplacian corrected; grad corrected; }\n"
-            "simple { maxIterations 1; }\n")
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "cf_ref_driver")
+
+
+def run_driver(exe, text, points):
     with tempfile.TemporaryDirectory() as td:
         cp = os.path.join(td, "case.dict")
         open(cp, "w").write(text)
-        r = subprocess.run([DRIVER, "simple", cp, td], capture_output=True, text=True, timeout=300)
-    assert r.returncode != 0
-    assert "chuanflow_b200" in r.stderr, r.stderr[-2000:]
+        pp = os.path.join(td, "points.f64")
+        np.ascontiguousarray(points).tofile(pp)
+        r = subprocess.run([exe, "simple", cp, td, pp], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        return (np.fromfile(os.path.join(td, "U.f64")).reshape(-1, 3), np.fromfile(os.path.join(td, "p.f64")),
+                np.fromfile(os.path.join(td, "phi.f64")), open(os.path.join(td, "result.txt")).read().split())
+
+
+@pytest.mark.skipif(not (os.path.exists(DRIVER) and os.path.exists(REF_DRIVER)), reason="drivers not built")
+def test_adapter_follows_reference_scheme_defaults():
+    """Scheme names the reference does not know select its defaults (upwind
+    convection, Gauss linear gradients, no laplacian correction); the adapter
+    does the same, run live against the reference driver on one case."""
+    import _cases as K
+    g = K.channel_case(8, 5, 4)
+    text = K.channel_dict(8, 5, 4, iters=4).replace(
+        "schemes { ddt steady; div upwind; laplacian corrected; grad corrected; }",
+        "schemes { ddt steady; div QUICK; laplacian uncorrected; grad fancy; }")
+    assert "div QUICK" in text
+    Ur, pr, phir, rr = run_driver(REF_DRIVER, text, g.mesh.points)
+    Ua, pa, phia, ra = run_driver(DRIVER, text, g.mesh.points)
+    assert int(ra[0]) == int(rr[0])
+    for a, b, name in ((Ua, Ur, "U"), (pa, pr, "p"), (phia, phir, "phi")):
+        assert rel(a, b) < REL_TOL, (name, rel(a, b))
