@@ -16,6 +16,7 @@ or running it without a CUDA device, raises.
 from ._capi import (  # noqa: F401
     BC,
     DIV,
+    Batch,
     GRAD,
     CfgError,
     PolyMesh,
@@ -32,5 +33,5 @@ from ._capi import (  # noqa: F401
     solve_cg,
 )
 
-__all__ = ["BC", "DIV", "GRAD", "CfgError", "PolyMesh", "Schemes", "SimpleCase", "SimpleControls",
+__all__ = ["BC", "Batch", "DIV", "GRAD", "CfgError", "PolyMesh", "Schemes", "SimpleCase", "SimpleControls",
            "SimpleResult", "SolverReport", "inspect_case_file", "lib", "lib_path", "run_case_file", "solve_bicgstab", "solve_cg"]

@@ -499,3 +499,82 @@ def run_case_file(path, device=0):
     return SimpleResult(r.iterations, bool(r.converged), r.final_continuity_error, r.final_momentum_residual,
                         r.last_dp, r.last_continuity_corrected, r.u_inner_iterations, r.p_inner_iterations,
                         bool(r.diverged)), counts
+
+
+# ---- detail blocks and batches --------------------------------------------
+
+class DetailMeasure(C.Structure):
+    _fields_ = [("cells", C.c_int64), ("sweeps", C.c_int32), ("converged", C.c_int32), ("diverged", C.c_int32),
+                ("dp_pa", C.c_double), ("imposed_q", C.c_double), ("flux_in", C.c_double),
+                ("flux_out", C.c_double), ("inlet_area", C.c_double), ("plug_speed", C.c_double),
+                ("device_ms", C.c_double), ("u_inner_iterations", C.c_int64), ("p_inner_iterations", C.c_int64),
+                ("status", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _detail_setup(self, inlet_shape="flat", rho=1.0):
+    """DetailBlock's constructor on this case's mesh (inlet/outlet patches by
+    type, cross-sections, inlet profile flat | parabolic | power1over7)."""
+    _check(lib().cfg_detail_setup(self._h, inlet_shape.encode(), C.c_double(rho)))
+
+
+def _detail_loss(self, q, controls):
+    """DetailBlock::lossAt(q): boundary conditions of rate q, SIMPLE from the
+    current fields, the measured drop (dict of BlockMeasure's fields)."""
+    c = controls._c()
+    m = DetailMeasure()
+    _check(lib().cfg_detail_loss(self._h, C.c_double(q), C.byref(c), C.byref(m)))
+    return m.as_dict()
+
+
+SimpleCase.detail_setup = _detail_setup
+SimpleCase.detail_loss = _detail_loss
+
+
+class Batch:
+    """Detail-block cases evaluated together, one stream each."""
+
+    CANDIDATES = [(1, 0), (4, 2), (8, 1), (8, 2), (16, 1), (32, 1)]
+
+    def __init__(self, cases):
+        self.cases = list(cases)
+        arr = (C.c_void_p * len(self.cases))(*[c._h.value for c in self.cases])
+        h = C.c_void_p()
+        _check(lib().cfg_batch_create(C.c_int32(len(self.cases)), arr, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.cfg_batch_destroy(h)
+            self._h = None
+
+    def set_schedule(self, workers, row_blocks_per_sm=0):
+        _check(lib().cfg_batch_set_schedule(self._h, C.c_int32(workers), C.c_int32(row_blocks_per_sm)))
+
+    def _args(self, q, controls):
+        n = len(self.cases)
+        qa = _f64(q)
+        if isinstance(controls, SimpleControls):
+            controls = [controls] * n
+        ca = (_Controls * n)(*[c._c() for c in controls])
+        return qa, ca
+
+    def loss(self, q, controls):
+        """One coupling pass; returns (list of measure dicts, wall ms)."""
+        qa, ca = self._args(q, controls)
+        out = (DetailMeasure * len(self.cases))()
+        ms = C.c_double()
+        _check(lib().cfg_batch_loss(self._h, _dp(qa), ca, out, C.byref(ms)))
+        return [m.as_dict() for m in out], ms.value
+
+    def autotune(self, q, controls):
+        """Runs one pass per candidate schedule and keeps the fastest;
+        returns ((workers, row_blocks_per_sm), {candidate: ms})."""
+        qa, ca = self._args(q, controls)
+        w, r = C.c_int32(), C.c_int32()
+        t = np.zeros(len(self.CANDIDATES))
+        _check(lib().cfg_batch_autotune(self._h, _dp(qa), ca, C.byref(w), C.byref(r), _dp(t)))
+        return (w.value, r.value), dict(zip(self.CANDIDATES, t.tolist()))

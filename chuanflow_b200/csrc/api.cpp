@@ -1,6 +1,7 @@
 // The extern "C" boundary: status codes, the per-thread error message, and
 // the case-file runner.
 #include <array>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -695,3 +696,91 @@ int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* resul
 }
 
 }  // extern "C"
+
+// ---- detail blocks and batches ----
+
+int cfg_detail_setup(cfg_ctx* ctx, const char* shape, double rho)
+{
+    return guard([&] {
+        need(ctx && shape, "cfg_detail_setup: null argument");
+        ctx->c->detailSetup(shape, rho);
+    });
+}
+
+int cfg_detail_loss(cfg_ctx* ctx, double q, const cfg_simple_controls* controls, cfg_detail_measure* out)
+{
+    return guard([&] {
+        need(ctx && controls && out, "cfg_detail_loss: null argument");
+        ctx->c->detailLoss(q, *controls, *out);
+        if (out->status != CFG_OK)
+            cfg::fail(out->status, !std::isfinite(out->dp_pa)
+                                       ? std::string("detailBlock: non-finite pressure drop")
+                                       : "detailBlock: the detailed region reports a non-positive drop (" +
+                                             std::to_string(out->dp_pa) + " Pa) at " + std::to_string(q) +
+                                             " m3/s");
+    });
+}
+
+int cfg_batch_create(int32_t n, cfg_ctx* const* blocks, cfg_batch** out)
+{
+    return guard([&] {
+        need(n > 0 && blocks && out, "cfg_batch_create: null argument or empty batch");
+        auto b = std::make_unique<cfg_batch>();
+        for (int32_t i = 0; i < n; ++i)
+        {
+            need(blocks[i] != nullptr, "cfg_batch_create: null block");
+            for (int32_t j = 0; j < i; ++j) need(blocks[j] != blocks[i], "cfg_batch_create: a block appears twice");
+            b->blocks.push_back(blocks[i]->c.get());
+        }
+        *out = b.release();
+    });
+}
+
+void cfg_batch_destroy(cfg_batch* batch) { delete batch; }
+
+int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t rowBlocks)
+{
+    return guard([&] {
+        need(batch && workers > 0 && rowBlocks >= 0, "cfg_batch_set_schedule: bad argument");
+        batch->workers = workers;
+        batch->rowBlocks = rowBlocks;
+    });
+}
+
+int cfg_batch_loss(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, cfg_detail_measure* out,
+                   double* wallMs)
+{
+    return guard([&] {
+        need(batch && q && controls && out, "cfg_batch_loss: null argument");
+        cfg::batchPass(*batch, q, controls, out, wallMs);
+    });
+}
+
+int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
+                       int32_t* rowBlocks, double* times)
+{
+    return guard([&] {
+        need(batch && q && controls && workers && rowBlocks, "cfg_batch_autotune: null argument");
+        static const int cand[][2] = {{1, 0}, {4, 2}, {8, 1}, {8, 2}, {16, 1}, {32, 1}};
+        std::vector<cfg_detail_measure> m(batch->blocks.size());
+        double best = 0;
+        int bi = 0;
+        for (int k = 0; k < 6; ++k)
+        {
+            batch->workers = cand[k][0];
+            batch->rowBlocks = cand[k][1];
+            double ms = 0;
+            cfg::batchPass(*batch, q, controls, m.data(), &ms);
+            if (times) times[k] = ms;
+            if (k == 0 || ms < best)
+            {
+                best = ms;
+                bi = k;
+            }
+        }
+        batch->workers = cand[bi][0];
+        batch->rowBlocks = cand[bi][1];
+        *workers = batch->workers;
+        *rowBlocks = batch->rowBlocks;
+    });
+}

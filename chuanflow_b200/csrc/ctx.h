@@ -21,6 +21,12 @@ struct Timing
     int64_t launches;
 };
 
+struct DetailState;
+struct DetailDeleter
+{
+    void operator()(DetailState* d) const;
+};
+
 class Ctx
 {
 public:
@@ -37,6 +43,13 @@ public:
     void download(double* U, double* p, double* phi);
     void initFlux(const double* u0);
     void iterate(const cfg_simple_controls& ctl, cfg_simple_result& res);
+
+    /// DetailBlock (src/coupling/src/coupledNetwork.cpp): inlet/outlet
+    /// patches, cross-sections and the inlet profile, then lossAt(q).
+    void detailSetup(const std::string& shape, double rho);
+    void detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out);
+    /// Solver grid of at most k blocks per SM (0: the context's own).
+    void setRowBlocks(int k);
 
     // diagnostics used by the parity tests
     void probeEquations(const cfg_simple_controls& ctl, const double* xprobe, double* out);
@@ -124,6 +137,8 @@ private:
     int GS_ = 0;       // grid of solver kernels (rowGrid(nC))
     int sms_ = 0;
     int rowBlocksPerSM_ = 4;  // 0: RPT rows per thread; k > 0: at most k blocks per SM
+    int initRowBlocks_ = 4, initGS_ = 0, initDicPartials_ = 1;
+    std::unique_ptr<DetailState, DetailDeleter> detail_;
     int rowGrid(int rows) const;
     int maxW_ = 0;     // longest matrix row
     int nSlicesEntries_ = 0;  // matrix SELL entries
@@ -195,3 +210,16 @@ struct cfg_ctx
 {
     std::unique_ptr<cfg::Ctx> c;
 };
+
+struct cfg_batch
+{
+    std::vector<cfg::Ctx*> blocks;
+    int workers = 1;
+    int rowBlocks = 0;  // 0: each block's own solver grid
+};
+
+namespace cfg
+{
+void batchPass(cfg_batch& b, const double* q, const cfg_simple_controls* ctl, cfg_detail_measure* out,
+               double* wallMs);
+}

@@ -1,0 +1,412 @@
+// Detail blocks of a coupled 1D-3D network and their batched evaluation.
+//
+// DetailBlock (src/coupling/src/coupledNetwork.cpp:462-620, 644-767,
+// 768-877, 878-926, 1080-1152, 1154-1195) is a 3D duct region between one
+// inlet and one outlet patch: lossAt(q) writes the inlet rate q (flat, or a
+// parabolic / 1/7-power section profile normalised to carry q exactly),
+// runs SIMPLE from the region's previous state, and measures the pressure
+// drop as rho times the difference of the volume-weighted mean kinematic
+// pressure of the first and last cross-sections.  The reference evaluates a
+// network's blocks one after another (coupledNetwork.cpp:1454-1487); here a
+// batch runs them concurrently, one CUDA stream per block, with a schedule
+// (concurrent workers, solver grid per block) chosen by measurement.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <limits>
+#include <thread>
+
+#include "ctx.h"
+#include "kernels.cuh"
+
+namespace cfg
+{
+
+namespace
+{
+
+/// Volume-weighted pressure sums of the first and last cross-section and
+/// the flux sums of the inlet and outlet patches: block b of 4 reduces list
+/// b in a fixed order.  out = {pV0, V0, pV1, V1, phiIn, phiOut}.
+__global__ void __launch_bounds__(TPB) k_detail_measure(const int* __restrict__ first, int nFirst,
+                                                        const int* __restrict__ last, int nLast, int inStart, int nIn,
+                                                        int outStart, int nOut, const double* __restrict__ V,
+                                                        const double* __restrict__ p, const double* __restrict__ phi,
+                                                        double* out)
+{
+    double s[2] = {0.0, 0.0};
+    const int b = blockIdx.x;
+    if (b < 2)
+    {
+        const int* list = b == 0 ? first : last;
+        const int n = b == 0 ? nFirst : nLast;
+        for (int k = threadIdx.x; k < n; k += TPB)
+        {
+            const int c = list[k];
+            s[0] += p[c] * V[c];
+            s[1] += V[c];
+        }
+    }
+    else
+    {
+        const int st = b == 2 ? inStart : outStart;
+        const int n = b == 2 ? nIn : nOut;
+        for (int k = threadIdx.x; k < n; k += TPB) s[0] += phi[st + k];
+    }
+    block_sum<2>(s);
+    if (threadIdx.x != 0) return;
+    if (b < 2)
+    {
+        out[2 * b] = s[0];
+        out[2 * b + 1] = s[1];
+    }
+    else
+    {
+        out[2 + b] = s[0];
+    }
+}
+
+Vec patchArea(const Mesh& M, int patch)
+{
+    const auto& pt = M.patches[static_cast<size_t>(patch)];
+    Vec s{0, 0, 0};
+    for (int64_t f = pt.start; f < pt.start + pt.size; ++f) s = s + M.Sf[static_cast<size_t>(f)];
+    return s;
+}
+
+double comp(const Vec& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+double hdot(const Vec& a, const Vec& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+}  // namespace
+
+struct DetailState
+{
+    int inlet = -1, outlet = -1, axis = 0, flowSign = 1;
+    double inletArea = 0, rho = 1;
+    std::vector<int64_t> inletFaces;
+    std::vector<double> inletWeights;  // empty: flat
+    std::vector<int> first, last;      // device slots of the first and last cross-section
+    int* dFirst = nullptr;
+    int* dLast = nullptr;
+    double* dOut = nullptr;
+    double* hOut = nullptr;
+};
+
+void Ctx::detailSetup(const std::string& shape, double rho)
+{
+    CFG_CUDA(cudaSetDevice(device_));
+    const Mesh& M = mesh_;
+    if (!(rho > 0)) fail(CFG_EINVAL, "detailBlock: nu and rho must be positive");
+    std::unique_ptr<DetailState> d(new DetailState());
+    d->rho = rho;
+    const int nP = static_cast<int>(M.patches.size());
+    for (int pi = 0; pi < nP; ++pi)
+    {
+        const std::string& t = M.patches[static_cast<size_t>(pi)].type;
+        if (t == "inlet" && d->inlet < 0) d->inlet = pi;
+        else if (t == "outlet" && d->outlet < 0) d->outlet = pi;
+    }
+    if (d->inlet < 0 || d->outlet < 0)
+        fail(CFG_ESETUP, "detailBlock: the detailed region needs one patch of type inlet and one of type outlet");
+    const Vec inSf = patchArea(M, d->inlet), outSf = patchArea(M, d->outlet);
+    d->inletArea = std::sqrt(hdot(inSf, inSf));
+    if (!(d->inletArea > 0)) fail(CFG_ESETUP, "detailBlock: the inlet patch has no area");
+    const Vec sum = inSf + outSf;
+    if (std::sqrt(hdot(sum, sum)) > 1e-6 * d->inletArea)
+        fail(CFG_ESETUP, "detailBlock: the inlet and outlet patches are not opposed");
+    const Vec nrm{inSf.x / d->inletArea, inSf.y / d->inletArea, inSf.z / d->inletArea};
+    d->axis = 0;
+    if (std::abs(nrm.y) > std::abs(comp(nrm, d->axis))) d->axis = 1;
+    if (std::abs(nrm.z) > std::abs(comp(nrm, d->axis))) d->axis = 2;
+    d->flowSign = comp(nrm, d->axis) < 0 ? 1 : -1;
+
+    // bounding box of the points (polyMesh::minX / maxX)
+    Vec lo = M.points[0], hi = M.points[0];
+    for (const Vec& p : M.points)
+    {
+        lo = Vec{std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z)};
+        hi = Vec{std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z)};
+    }
+
+    // cross-sections in the order the flow meets them (buildSections): cells
+    // by (axial centre, index), grouped while within 1e-9 of the extent
+    {
+        const int64_t nC = M.nCells;
+        const int ax = d->axis;
+        std::vector<int64_t> order(static_cast<size_t>(nC));
+        for (int64_t c = 0; c < nC; ++c) order[c] = c;
+        auto coord = [&](int64_t c) { return comp(M.C[static_cast<size_t>(c)], ax); };
+        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+            const double ka = coord(a), kb = coord(b);
+            if (ka != kb) return ka < kb;
+            return a < b;
+        });
+        if (d->flowSign < 0) std::reverse(order.begin(), order.end());
+        const double band = 1e-9 * std::max(std::abs(comp(hi, ax) - comp(lo, ax)), 1e-30);
+        std::vector<std::pair<size_t, size_t>> groups;
+        size_t g = 0;
+        while (g < order.size())
+        {
+            const double anchor = coord(order[g]);
+            size_t h = g + 1;
+            while (h < order.size() && std::abs(coord(order[h]) - anchor) <= band) ++h;
+            groups.push_back({g, h});
+            g = h;
+        }
+        if (groups.size() < 2)
+            fail(CFG_ESETUP, "detailBlock: the detailed region has fewer than two cross-sections to measure a drop between");
+        for (size_t k = groups.front().first; k < groups.front().second; ++k)
+            d->first.push_back(inv_[static_cast<size_t>(order[k])]);
+        for (size_t k = groups.back().first; k < groups.back().second; ++k)
+            d->last.push_back(inv_[static_cast<size_t>(order[k])]);
+    }
+
+    // the inlet profile (buildInletProfile)
+    if (shape != "flat")
+    {
+        if (shape != "parabolic" && shape != "power1over7")
+            fail(CFG_ESETUP, "detailBlock: the inlet profile '" + shape +
+                                 "' is not one this block can write (flat, parabolic, power1over7)");
+        int bounds[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int pi = 0; pi < nP; ++pi)
+        {
+            if (M.patches[static_cast<size_t>(pi)].type != "wall") continue;
+            const Vec sf = patchArea(M, pi);
+            if (!(std::sqrt(hdot(sf, sf)) > 0)) continue;
+            int k = 0;
+            for (int c = 1; c < 3; ++c)
+                if (std::abs(comp(sf, c)) > std::abs(comp(sf, k))) k = c;
+            if (k == d->axis) continue;
+            bounds[k][comp(sf, k) < 0 ? 0 : 1] = 1;
+        }
+        std::vector<int> axes;
+        for (int k = 0; k < 3; ++k)
+            if (k != d->axis && bounds[k][0] && bounds[k][1]) axes.push_back(k);
+        if (axes.empty())
+            fail(CFG_ESETUP, "detailBlock: the inlet profile '" + shape +
+                                 "' has no wall-confined transverse direction to vary along");
+        for (int k : axes)
+            if (!(comp(hi, k) > comp(lo, k)))
+                fail(CFG_ESETUP, "detailBlock: the inlet section has no extent to spread a profile over");
+        const auto& pin = M.patches[static_cast<size_t>(d->inlet)];
+        std::vector<double> w(static_cast<size_t>(pin.size), 0.0);
+        double wMin = std::numeric_limits<double>::max();
+        for (int64_t j = 0; j < pin.size; ++j)
+        {
+            const Vec& fc = M.Cf[static_cast<size_t>(pin.start + j)];
+            double value = 1.0;
+            for (int k : axes)
+            {
+                const double mid = 0.5 * (comp(hi, k) + comp(lo, k));
+                const double half = 0.5 * (comp(hi, k) - comp(lo, k));
+                const double eta = (comp(fc, k) - mid) / half;
+                value *= shape == "parabolic" ? (1.0 - eta * eta) : std::pow(1.0 - std::abs(eta), 1.0 / 7.0);
+            }
+            w[static_cast<size_t>(j)] = value;
+            wMin = std::min(wMin, value);
+        }
+        if (!(wMin > 0))
+            fail(CFG_ESETUP, "detailBlock: the inlet profile writes a zero or reversed weight on a face");
+        double sumWA = 0, sumA = 0;
+        for (int64_t j = 0; j < pin.size; ++j)
+        {
+            const double a = M.magSf[static_cast<size_t>(pin.start + j)];
+            sumWA += w[static_cast<size_t>(j)] * a;
+            sumA += a;
+        }
+        if (!(sumA > 0) || !(sumWA > 0)) fail(CFG_ESETUP, "detailBlock: the inlet section integrates to no area");
+        if (std::abs(sumA - d->inletArea) > 1e-9 * d->inletArea)
+            fail(CFG_ESETUP, "detailBlock: the inlet patch's face areas do not add to its area vector");
+        const double norm = sumWA / sumA;
+        for (int64_t j = 0; j < pin.size; ++j)
+        {
+            d->inletFaces.push_back(pin.start + j);
+            d->inletWeights.push_back(w[static_cast<size_t>(j)] / norm);
+        }
+    }
+    d->dFirst = upload(d->first);
+    d->dLast = upload(d->last);
+    d->dOut = alloc<double>(8);
+    CFG_CUDA(cudaMallocHost(&d->hOut, 8 * sizeof(double)));
+    detail_.reset(d.release());
+}
+
+void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out)
+{
+    if (!detail_) fail(CFG_EINVAL, "cfg_detail_loss: call cfg_detail_setup first");
+    if (!(q > 0)) fail(CFG_EINVAL, "detailBlock: asked for the drop of a detailed region at a non-positive rate");
+    CFG_CUDA(cudaSetDevice(device_));
+    DetailState& d = *detail_;
+    const Mesh& M = mesh_;
+    // applyBoundary (coupledNetwork.cpp:878-926)
+    double inletU[3] = {0, 0, 0};
+    inletU[d.axis] = d.flowSign * q / d.inletArea;
+    const double zero[3] = {0, 0, 0};
+    const int nP = static_cast<int>(M.patches.size());
+    for (int pi = 0; pi < nP; ++pi)
+    {
+        const std::string& t = M.patches[static_cast<size_t>(pi)].type;
+        if (pi == d.inlet)
+        {
+            setPatchBC('U', pi, CFG_BC_FIXED_VALUE, inletU);
+            setPatchBC('p', pi, CFG_BC_ZERO_GRADIENT, zero);
+        }
+        else if (pi == d.outlet)
+        {
+            setPatchBC('U', pi, CFG_BC_ZERO_GRADIENT, zero);
+            setPatchBC('p', pi, CFG_BC_FIXED_VALUE, zero);
+        }
+        else if (t == "wall")
+        {
+            setPatchBC('U', pi, CFG_BC_FIXED_VALUE, zero);
+            setPatchBC('p', pi, CFG_BC_ZERO_GRADIENT, zero);
+        }
+        else
+        {
+            setPatchBC('U', pi, CFG_BC_ZERO_GRADIENT, zero);
+            setPatchBC('p', pi, CFG_BC_ZERO_GRADIENT, zero);
+        }
+    }
+    clearFaceValuesU();
+    if (!d.inletWeights.empty())
+    {
+        std::vector<double> vals(3 * d.inletFaces.size());
+        for (size_t j = 0; j < d.inletFaces.size(); ++j)
+            for (int k = 0; k < 3; ++k) vals[3 * j + k] = inletU[k] * d.inletWeights[j];
+        setFaceValuesU(static_cast<int64_t>(d.inletFaces.size()), d.inletFaces.data(), vals.data());
+    }
+    initFlux(nullptr);  // phi.correctBoundaryFlux(U)
+    cfg_simple_result res{};
+    iterate(ctl, res);
+    // measure (coupledNetwork.cpp:1154-1195)
+    const auto& pin = M.patches[static_cast<size_t>(d.inlet)];
+    const auto& pout = M.patches[static_cast<size_t>(d.outlet)];
+    k_detail_measure<<<4, TPB, 0, stream_>>>(d.dFirst, static_cast<int>(d.first.size()), d.dLast,
+                                             static_cast<int>(d.last.size()), static_cast<int>(pin.start),
+                                             static_cast<int>(pin.size), static_cast<int>(pout.start),
+                                             static_cast<int>(pout.size), dm_.V, p_, phi_, d.dOut);
+    launchCheck("detail_measure");
+    CFG_CUDA(cudaMemcpyAsync(d.hOut, d.dOut, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    const double* h = d.hOut;
+    const double p0 = h[1] > 0 ? h[0] / h[1] : 0.0, p1 = h[3] > 0 ? h[2] / h[3] : 0.0;
+    out = cfg_detail_measure{};
+    out.cells = M.nCells;
+    out.sweeps = res.iterations;
+    out.converged = res.converged;
+    out.diverged = res.diverged;
+    out.dp_pa = d.rho * p0 - d.rho * p1;
+    out.imposed_q = q;
+    out.flux_in = -h[4];
+    out.flux_out = h[5];
+    out.inlet_area = d.inletArea;
+    out.plug_speed = q / d.inletArea;
+    out.device_ms = lastMs[7];
+    out.u_inner_iterations = res.u_inner_iterations;
+    out.p_inner_iterations = res.p_inner_iterations;
+    // lossAt's own checks of the measured drop (coupledNetwork.cpp:1146-1151)
+    if (!std::isfinite(out.dp_pa)) out.status = CFG_ENUMERIC;
+    else if (out.dp_pa <= 0) out.status = CFG_ENUMERIC;
+}
+
+void Ctx::setRowBlocks(int k)
+{
+    // the solver grid, for blocks that share the GPU: never larger than the
+    // grid the partial buffers were sized for
+    if (k <= 0) k = initRowBlocks_;
+    if (k == rowBlocksPerSM_) return;
+    const int keep = rowBlocksPerSM_;
+    rowBlocksPerSM_ = k;
+    int pOff = 0;
+    for (const DicPhase& ph : dicPhase_) pOff += rowGrid(ph.cnt);
+    if (rowGrid(dm_.nC) > initGS_ || pOff + 1 > initDicPartials_)
+    {
+        rowBlocksPerSM_ = keep;  // larger than the partial buffers allow
+        return;
+    }
+    GS_ = rowGrid(dm_.nC);
+    pOff = 0;
+    for (DicPhase& ph : dicPhase_)
+    {
+        ph.partialOff = pOff;
+        pOff += rowGrid(ph.cnt);
+    }
+    dicPartials_ = pOff + 1;
+    for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
+    graphs_.clear();
+}
+
+}  // namespace cfg
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+
+namespace cfg
+{
+
+void DetailDeleter::operator()(DetailState* d) const
+{
+    if (d && d->hOut) cudaFreeHost(d->hOut);
+    delete d;
+}
+
+/// One coupling pass: every block's lossAt at its own rate.  Blocks are
+/// taken largest first by `workers` host threads, each block on its own
+/// context stream, so up to `workers` blocks run on the GPU at once.
+void batchPass(cfg_batch& b, const double* q, const cfg_simple_controls* ctl, cfg_detail_measure* out,
+               double* wallMs)
+{
+    const int n = static_cast<int>(b.blocks.size());
+    std::vector<int> order(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return b.blocks[x]->mesh().nCells > b.blocks[y]->mesh().nCells; });
+    for (cfg::Ctx* c : b.blocks) c->setRowBlocks(b.rowBlocks);
+    std::atomic<int> next{0};
+    std::vector<std::string> errs(static_cast<size_t>(n));
+    std::vector<int> codes(static_cast<size_t>(n), CFG_OK);
+    auto work = [&]() {
+        for (;;)
+        {
+            const int k = next.fetch_add(1);
+            if (k >= n) return;
+            const int i = order[k];
+            try
+            {
+                // a non-positive or non-finite drop is reported in
+                // out[i].status; the pass goes on with the other blocks
+                b.blocks[i]->detailLoss(q[i], ctl[i], out[i]);
+            }
+            catch (const Error& e)
+            {
+                errs[i] = e.what();
+                codes[i] = e.code;
+            }
+            catch (const std::exception& e)
+            {
+                errs[i] = e.what();
+                codes[i] = CFG_EINVAL;
+            }
+        }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    const int w = std::max(1, std::min(b.workers, n));
+    if (w == 1)
+    {
+        work();
+    }
+    else
+    {
+        std::vector<std::thread> th;
+        for (int t = 0; t < w; ++t) th.emplace_back(work);
+        for (auto& t : th) t.join();
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    if (wallMs) *wallMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    for (int i = 0; i < n; ++i)
+        if (codes[i] != CFG_OK) fail(codes[i], "block " + std::to_string(i) + ": " + errs[i]);
+}
+
+}  // namespace cfg

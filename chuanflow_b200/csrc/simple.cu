@@ -654,6 +654,8 @@ void Ctx::buildDevice()
     sms_ = sms;
     if (const char* e = std::getenv("CHUANFLOW_ROW_BLOCKS_PER_SM")) rowBlocksPerSM_ = std::max(0, std::atoi(e));
     GS_ = rowGrid(nC);
+    initRowBlocks_ = rowBlocksPerSM_;
+    initGS_ = GS_;
     GF_ = std::max(1, std::min((nF + TPB - 1) / TPB, sms * 8));
 
     // ---- per-face geometry derived on the host in the reference's order ----
@@ -865,6 +867,7 @@ void Ctx::buildDevice()
             dicPhase_.push_back(ph);
         }
         dicPartials_ = pOff + 1;
+        initDicPartials_ = dicPartials_;
         dic_.nColours = nCol;
         dic_.rows = upload(rows);
         dic_.lStart = upload(lStart);

@@ -50,3 +50,35 @@ def tet_mesh(n, jitter=0.1, seed=0):
     tets = delaunay_tets(pts)
     off = np.arange(0, 4 * tets.shape[0] + 1, 4, dtype=np.int64)
     return PolyMesh.from_cells(pts, np.full(tets.shape[0], 4, np.int32), off, tets.ravel()), pts, tets
+
+
+CHANNEL_SIDES = {"xmin": ("inlet", "inlet"), "xmax": ("outlet", "outlet"), "ymin": ("bottom", "wall"),
+                 "ymax": ("top", "wall"), "zmin": ("front", "wall"), "zmax": ("back", "wall")}
+SHAPES = ("flat", "parabolic", "power1over7")
+
+
+def channel_block(cells, aspect, H=0.1):
+    """A straight square duct L x H x H (L = aspect H) of about `cells`
+    cubic hex cells along x: inlet at xmin, outlet at xmax, four walls."""
+    from ._capi import PolyMesh
+    ny = max(2, int(round((cells / aspect) ** (1.0 / 3.0))))
+    nx = max(2, int(round(cells / (ny * ny))))
+    return PolyMesh.block((0.0, 0.0, 0.0), (H * nx / ny, H, H), (nx, ny, ny), CHANNEL_SIDES)
+
+
+def detail_block_set(n=64, seed=2024, cells_min=2_000, cells_max=200_000):
+    """The batched detail-block workload: n ducts with cell counts drawn
+    log-uniformly in [cells_min, cells_max], aspect ratios uniform in
+    [5, 20], inlet profiles cycling flat / parabolic / power1over7, mean
+    inlet speeds uniform in [0.05, 0.5] m/s; even-numbered blocks laminar
+    (nu 1e-4), odd-numbered ones marked for k-epsilon at Re_H ~ 2e4.
+    Seeded numpy draws.  Returns a list of dicts."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        cells = float(np.exp(rng.uniform(np.log(cells_min), np.log(cells_max))))
+        aspect = float(rng.uniform(5.0, 20.0))
+        speed = float(rng.uniform(0.05, 0.5))
+        out.append({"cells": cells, "aspect": aspect, "shape": SHAPES[i % 3], "speed": speed,
+                    "laminar": i % 2 == 0})
+    return out

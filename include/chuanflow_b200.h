@@ -353,6 +353,66 @@ int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* resul
  * of the mesh counts, every patch's U/p conditions, schemes and controls. */
 int cfg_case_inspect(const char* path, char* out, size_t size);
 
+/* ---- detail blocks of a coupled 1D-3D network ------------------------- */
+
+/* BlockMeasure (src/coupling/include/cf/coupling/CoupledNetwork.h:327-357),
+ * the part a laminar block reports, plus inner-solver statistics */
+typedef struct cfg_detail_measure
+{
+    int64_t cells;
+    int32_t sweeps;       /* SIMPLE outer iterations of this lossAt */
+    int32_t converged;
+    int32_t diverged;
+    double dp_pa;         /* rho * (volume-weighted p of the first cross-section - the last) */
+    double imposed_q;     /* m3/s */
+    double flux_in;       /* -sum phi over the inlet patch */
+    double flux_out;      /* sum phi over the outlet patch */
+    double inlet_area;
+    double plug_speed;
+    double device_ms;     /* device time of the SIMPLE iterations */
+    int64_t u_inner_iterations;
+    int64_t p_inner_iterations;
+    int32_t status;       /* CFG_OK, or CFG_ENUMERIC for a non-finite or non-positive drop,
+                           * the two results lossAt rejects (coupledNetwork.cpp:1146-1151) */
+} cfg_detail_measure;
+
+/* DetailBlock's constructor (coupledNetwork.cpp:462-620, 644-877): the first
+ * patch of type "inlet" and of type "outlet" (opposed, equal areas), the flow
+ * axis from the inlet area vector, the cross-sections (cells by axial centre,
+ * grouped within 1e-9 of the extent) and the inlet profile "flat",
+ * "parabolic" or "power1over7" (normalised to carry the rate exactly). */
+int cfg_detail_setup(cfg_ctx* ctx, const char* inlet_shape, double rho);
+/* DetailBlock::lossAt(q) (coupledNetwork.cpp:1080-1152, 878-926,
+ * 1154-1195) for a laminar block: the boundary conditions of rate q, SIMPLE
+ * with `controls` from the block's current fields (a coupling pass warm
+ * starts), and the measured drop.  Returns CFG_ENUMERIC, with `out` filled,
+ * when the drop is non-finite or non-positive, where lossAt raises. */
+int cfg_detail_loss(cfg_ctx* ctx, double q, const cfg_simple_controls* controls, cfg_detail_measure* out);
+
+/* A batch of detail-block contexts on one device (no reference counterpart:
+ * solveCoupled1d3d evaluates its blocks one after another,
+ * coupledNetwork.cpp:1454-1487).  The contexts stay owned by the caller and
+ * must each have their own stream (the default of cfg_ctx_create). */
+typedef struct cfg_batch cfg_batch;
+int cfg_batch_create(int32_t n, cfg_ctx* const* blocks, cfg_batch** out);
+void cfg_batch_destroy(cfg_batch* batch);
+/* The schedule: `workers` blocks in flight at once (1 = one after another),
+ * each block's solver kernels on a grid of at most `row_blocks_per_sm`
+ * blocks per SM (0 = the context's own grid). */
+int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t row_blocks_per_sm);
+/* One coupling pass: lossAt(q[i]) of every block i with controls[i]; wall_ms
+ * (may be NULL) is the pass's host wall time.  A block whose drop lossAt
+ * would reject reports it in out[i].status; the pass still completes. */
+int cfg_batch_loss(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, cfg_detail_measure* out,
+                   double* wall_ms);
+/* Chooses the schedule by measurement: runs one pass per candidate (each a
+ * real pass, warm-starting the blocks) and keeps the fastest; the chosen
+ * schedule and each candidate's time are returned (times: n_candidates
+ * doubles, may be NULL).  Candidates (workers, row blocks per SM): (1,0),
+ * (4,2), (8,1), (8,2), (16,1), (32,1). */
+int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
+                       int32_t* row_blocks_per_sm, double* times);
+
 #ifdef __cplusplus
 }
 #endif
