@@ -536,7 +536,7 @@ SimpleCase.detail_loss = _detail_loss
 class Batch:
     """Detail-block cases evaluated together, one stream each."""
 
-    CANDIDATES = [(1, 0), (4, 2), (8, 1), (8, 2), (16, 1), (32, 1)]
+    CANDIDATES = [(1, 0), (4, 2), (8, 1), (16, 1), (32, 1), (64, 1)]
 
     def __init__(self, cases):
         self.cases = list(cases)
@@ -569,6 +569,12 @@ class Batch:
         ms = C.c_double()
         _check(lib().cfg_batch_loss(self._h, _dp(qa), ca, out, C.byref(ms)))
         return [m.as_dict() for m in out], ms.value
+
+    def save(self):
+        _check(lib().cfg_batch_save(self._h))
+
+    def restore(self):
+        _check(lib().cfg_batch_restore(self._h))
 
     def autotune(self, q, controls):
         """Runs one pass per candidate schedule and keeps the fastest;

@@ -756,17 +756,37 @@ int cfg_batch_loss(cfg_batch* batch, const double* q, const cfg_simple_controls*
     });
 }
 
+int cfg_batch_save(cfg_batch* batch)
+{
+    return guard([&] {
+        need(batch, "cfg_batch_save: null argument");
+        for (cfg::Ctx* c : batch->blocks) c->saveState();
+    });
+}
+
+int cfg_batch_restore(cfg_batch* batch)
+{
+    return guard([&] {
+        need(batch, "cfg_batch_restore: null argument");
+        for (cfg::Ctx* c : batch->blocks) c->restoreState();
+    });
+}
+
 int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
                        int32_t* rowBlocks, double* times)
 {
     return guard([&] {
         need(batch && q && controls && workers && rowBlocks, "cfg_batch_autotune: null argument");
-        static const int cand[][2] = {{1, 0}, {4, 2}, {8, 1}, {8, 2}, {16, 1}, {32, 1}};
+        static const int cand[][2] = {{1, 0}, {4, 2}, {8, 1}, {16, 1}, {32, 1}, {64, 1}};
         std::vector<cfg_detail_measure> m(batch->blocks.size());
         double best = 0;
         int bi = 0;
+        // every candidate runs the same pass from the same saved fields; the
+        // chosen one then runs it for real
+        for (cfg::Ctx* c : batch->blocks) c->saveState();
         for (int k = 0; k < 6; ++k)
         {
+            for (cfg::Ctx* c : batch->blocks) c->restoreState();
             batch->workers = cand[k][0];
             batch->rowBlocks = cand[k][1];
             double ms = 0;
@@ -778,8 +798,10 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
                 bi = k;
             }
         }
+        for (cfg::Ctx* c : batch->blocks) c->restoreState();
         batch->workers = cand[bi][0];
         batch->rowBlocks = cand[bi][1];
+        cfg::batchPass(*batch, q, controls, m.data(), nullptr);
         *workers = batch->workers;
         *rowBlocks = batch->rowBlocks;
     });

@@ -50,6 +50,10 @@ public:
     void detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out);
     /// Solver grid of at most k blocks per SM (0: the context's own).
     void setRowBlocks(int k);
+    /// A device-side copy of U, p, phi, and its return (for schedule trials
+    /// on identical work).
+    void saveState();
+    void restoreState();
 
     // diagnostics used by the parity tests
     void probeEquations(const cfg_simple_controls& ctl, const double* xprobe, double* out);
@@ -139,6 +143,7 @@ private:
     int rowBlocksPerSM_ = 4;  // 0: RPT rows per thread; k > 0: at most k blocks per SM
     int initRowBlocks_ = 4, initGS_ = 0, initDicPartials_ = 1;
     std::unique_ptr<DetailState, DetailDeleter> detail_;
+    double* saved_ = nullptr;
     int rowGrid(int rows) const;
     int maxW_ = 0;     // longest matrix row
     int nSlicesEntries_ = 0;  // matrix SELL entries

@@ -310,6 +310,30 @@ void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measur
     else if (out.dp_pa <= 0) out.status = CFG_ENUMERIC;
 }
 
+void Ctx::saveState()
+{
+    CFG_CUDA(cudaSetDevice(device_));
+    const size_t nC = static_cast<size_t>(dm_.nC), nF = static_cast<size_t>(dm_.nF);
+    if (!saved_) saved_ = alloc<double>(4 * nC + nF);
+    for (int q = 0; q < 3; ++q)
+        CFG_CUDA(cudaMemcpyAsync(saved_ + q * nC, U_.c[q], nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(saved_ + 3 * nC, p_, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(saved_ + 4 * nC, phi_, nF * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::restoreState()
+{
+    if (!saved_) fail(CFG_EINVAL, "restoreState: nothing saved");
+    CFG_CUDA(cudaSetDevice(device_));
+    const size_t nC = static_cast<size_t>(dm_.nC), nF = static_cast<size_t>(dm_.nF);
+    for (int q = 0; q < 3; ++q)
+        CFG_CUDA(cudaMemcpyAsync(U_.c[q], saved_ + q * nC, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(p_, saved_ + 3 * nC, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaMemcpyAsync(phi_, saved_ + 4 * nC, nF * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Ctx::setRowBlocks(int k)
 {
     // the solver grid, for blocks that share the GPU: never larger than the

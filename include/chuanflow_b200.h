@@ -405,11 +405,16 @@ int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t row_blocks
  * would reject reports it in out[i].status; the pass still completes. */
 int cfg_batch_loss(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, cfg_detail_measure* out,
                    double* wall_ms);
-/* Chooses the schedule by measurement: runs one pass per candidate (each a
- * real pass, warm-starting the blocks) and keeps the fastest; the chosen
- * schedule and each candidate's time are returned (times: n_candidates
- * doubles, may be NULL).  Candidates (workers, row blocks per SM): (1,0),
- * (4,2), (8,1), (8,2), (16,1), (32,1). */
+/* A device-side copy of every block's U, p, phi, and its return: passes
+ * repeated from the same fields (the same work under another schedule). */
+int cfg_batch_save(cfg_batch* batch);
+int cfg_batch_restore(cfg_batch* batch);
+/* Chooses the schedule by measurement: every candidate runs the same pass
+ * from the blocks' current fields (saved and restored around each), the
+ * fastest is kept and then runs that pass for real; the chosen schedule and
+ * each candidate's wall time are returned (times: 6 doubles, may be NULL).
+ * Candidates (workers, row blocks per SM): (1,0), (4,2), (8,1), (16,1),
+ * (32,1), (64,1). */
 int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
                        int32_t* row_blocks_per_sm, double* times);
 
