@@ -529,6 +529,23 @@ def _detail_loss(self, q, controls):
     return m.as_dict()
 
 
+def _turbulence_setup(self, model="kEpsilon", intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=1e-4):
+    """RansModel::create for this case (model kEpsilon | laminar): call after
+    the velocity conditions are set; advanced once per SIMPLE iteration."""
+    _check(lib().cfg_turbulence_setup(self._h, model.encode(), C.c_double(intensity), C.c_double(length_scale),
+                                      C.c_double(relaxation), C.c_double(nu)))
+
+
+def _turbulence_fields(self):
+    """k, epsilon, nut (cells) and nu + nut on faces."""
+    n, f = self.mesh.n_cells, self.mesh.n_faces
+    k, e, nut, nuf = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(f)
+    _check(lib().cfg_turbulence_fields(self._h, _dp(k), _dp(e), _dp(nut), _dp(nuf)))
+    return {"k": k, "eps": e, "nut": nut, "nuEffFace": nuf}
+
+
+SimpleCase.turbulence_setup = _turbulence_setup
+SimpleCase.turbulence_fields = _turbulence_fields
 SimpleCase.detail_setup = _detail_setup
 SimpleCase.detail_loss = _detail_loss
 

@@ -806,3 +806,23 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
         *rowBlocks = batch->rowBlocks;
     });
 }
+
+// ---- RANS turbulence ----
+
+int cfg_turbulence_setup(cfg_ctx* ctx, const char* model, double intensity, double lengthScale, double relaxation,
+                         double nu)
+{
+    return guard([&] {
+        need(ctx && model, "cfg_turbulence_setup: null argument");
+        ctx->c->refreshBcPublic();
+        ctx->c->turbulenceSetup(model, intensity, lengthScale, relaxation, nu);
+    });
+}
+
+int cfg_turbulence_fields(cfg_ctx* ctx, double* k, double* eps, double* nut, double* nuEffFace)
+{
+    return guard([&] {
+        need(ctx, "cfg_turbulence_fields: null argument");
+        ctx->c->turbulenceFields(k, eps, nut, nuEffFace);
+    });
+}

@@ -26,6 +26,11 @@ struct DetailDeleter
 {
     void operator()(DetailState* d) const;
 };
+struct TurbState;
+struct TurbDeleter
+{
+    void operator()(TurbState* t) const;
+};
 
 class Ctx
 {
@@ -50,6 +55,16 @@ public:
     void detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out);
     /// Solver grid of at most k blocks per SM (0: the context's own).
     void setRowBlocks(int k);
+
+    /// RANS model ("laminar" removes it), advanced once per SIMPLE outer
+    /// iteration; the case's boundary conditions must be set first (the
+    /// initial k and epsilon scale with the inlet velocity).
+    void turbulenceSetup(const std::string& model, double intensity, double lengthScale, double relaxation,
+                         double nu);
+    void turbulenceFields(double* k, double* eps, double* nut, double* nuEffFace);
+    bool hasTurbulence() const { return static_cast<bool>(turb_); }
+    void refreshBcPublic() { refreshBc(); }
+    int64_t lastTurbInner = 0;
     /// A device-side copy of U, p, phi, and its return (for schedule trials
     /// on identical work).
     void saveState();
@@ -143,6 +158,10 @@ private:
     int rowBlocksPerSM_ = 4;  // 0: RPT rows per thread; k > 0: at most k blocks per SM
     int initRowBlocks_ = 4, initGS_ = 0, initDicPartials_ = 1;
     std::unique_ptr<DetailState, DetailDeleter> detail_;
+    std::unique_ptr<TurbState, TurbDeleter> turb_;
+    void turbCorrect(int64_t& inner);
+    void turbRefreshNut();
+    void turbSolveScalar(double sigma, bool isK, double* field, double floorV, int64_t& inner);
     double* saved_ = nullptr;
     int rowGrid(int rows) const;
     int maxW_ = 0;     // longest matrix row

@@ -385,4 +385,57 @@ constexpr int kSolverMinBlocks = 4;
 #define FOR_ROWS(c, n) \
     for (int c = blockIdx.x * ::cfg::TPB + threadIdx.x; c < (n); c += gridDim.x * ::cfg::TPB)
 
+inline CV3P cv(const V3P& v) { return CV3P{{v.c[0], v.c[1], v.c[2]}}; }
+
+/// The non-orthogonal corrector of assembleLaplacian (laplacianScheme.cpp:217-263):
+/// rhs = base + sum over faces in order of +-gamma_f (cfVec . grad_f), with
+/// grad_f the owner-weighted face interpolation of the cell gradients.
+template <int NC>
+__global__ void __launch_bounds__(TPB) k_corrector(DMesh m, const double* __restrict__ gamma, CGrad3 g, CV3P base,
+                                                   V3P rhs)
+{
+    ROW_LOOP(c, m.nC)
+    {
+        const int sl = c >> 5, lane = c & 31;
+        double r[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) r[q] = base.c[q][c];
+        const int e1 = m.cfStart[sl + 1];
+        for (int e = m.cfStart[sl] + lane; e < e1; e += 32)
+        {
+            const int code = m.cfCode[e];
+            if (code < 0) break;
+            const int f = code >> 1, side = code & 1;
+            const double cvx = m.cvx[f], cvy = m.cvy[f], cvz = m.cvz[f], gm = gamma[f];
+            if (f < m.nI)
+            {
+                const int other = m.cfOther[e];
+                const int o = side ? other : c, n = side ? c : other;
+                const double w = m.ow[f], w1 = 1.0 - w;
+#pragma unroll
+                for (int q = 0; q < NC; ++q)
+                {
+                    const double gx = g.g[q].c[0][o] * w + g.g[q].c[0][n] * w1;
+                    const double gy = g.g[q].c[1][o] * w + g.g[q].c[1][n] * w1;
+                    const double gz = g.g[q].c[2][o] * w + g.g[q].c[2][n] * w1;
+                    const double corr = gm * (cvx * gx + cvy * gy + cvz * gz);
+                    r[q] = side ? r[q] + (-corr) : r[q] + corr;
+                }
+            }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < NC; ++q)
+                {
+                    const double corr =
+                        gm * (cvx * g.g[q].c[0][c] + cvy * g.g[q].c[1][c] + cvz * g.g[q].c[2][c]);
+                    r[q] = r[q] + corr;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q) rhs.c[q][c] = r[q];
+    }
+}
+
 }  // namespace cfg

@@ -286,56 +286,6 @@ __global__ void __launch_bounds__(TPB) k_divphi(DMesh m, const double* __restric
     }
 }
 
-/// The non-orthogonal corrector of assembleLaplacian (laplacianScheme.cpp:217-263):
-/// rhs = base + sum over faces in order of +-gamma_f (cfVec . grad_f), with
-/// grad_f the owner-weighted face interpolation of the cell gradients.
-template <int NC>
-__global__ void __launch_bounds__(TPB) k_corrector(DMesh m, const double* __restrict__ gamma, CGrad3 g, CV3P base,
-                                                   V3P rhs)
-{
-    ROW_LOOP(c, m.nC)
-    {
-        const int sl = c >> 5, lane = c & 31;
-        double r[NC];
-#pragma unroll
-        for (int q = 0; q < NC; ++q) r[q] = base.c[q][c];
-        const int e1 = m.cfStart[sl + 1];
-        for (int e = m.cfStart[sl] + lane; e < e1; e += 32)
-        {
-            const int code = m.cfCode[e];
-            if (code < 0) break;
-            const int f = code >> 1, side = code & 1;
-            const double cvx = m.cvx[f], cvy = m.cvy[f], cvz = m.cvz[f], gm = gamma[f];
-            if (f < m.nI)
-            {
-                const int other = m.cfOther[e];
-                const int o = side ? other : c, n = side ? c : other;
-                const double w = m.ow[f], w1 = 1.0 - w;
-#pragma unroll
-                for (int q = 0; q < NC; ++q)
-                {
-                    const double gx = g.g[q].c[0][o] * w + g.g[q].c[0][n] * w1;
-                    const double gy = g.g[q].c[1][o] * w + g.g[q].c[1][n] * w1;
-                    const double gz = g.g[q].c[2][o] * w + g.g[q].c[2][n] * w1;
-                    const double corr = gm * (cvx * gx + cvy * gy + cvz * gz);
-                    r[q] = side ? r[q] + (-corr) : r[q] + corr;
-                }
-            }
-            else
-            {
-#pragma unroll
-                for (int q = 0; q < NC; ++q)
-                {
-                    const double corr =
-                        gm * (cvx * g.g[q].c[0][c] + cvy * g.g[q].c[1][c] + cvz * g.g[q].c[2][c]);
-                    r[q] = r[q] + corr;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < NC; ++q) rhs.c[q][c] = r[q];
-    }
-}
 
 /// rAU = V / aDiag and the pressure-free blend Hfree (simpleSolver.cpp:123-172).
 __global__ void __launch_bounds__(TPB) k_hfree(DMesh m, const double* __restrict__ uDiag, CV3P U, CV3P x,
@@ -1195,15 +1145,16 @@ void Ctx::refreshBc()
     bcDirty_ = false;
 }
 
-/// With linear-upwind convection, fvc::grad of the three U components (the
-/// iterate the momentum equation is assembled from) into gA_, gB_, Hf_,
-/// which the momentum solve only overwrites after assembly; returns 1 then.
+/// With linear-upwind convection, the gradient of the three U components
+/// (the iterate the momentum equation is assembled from; internal faces by
+/// the bounded owner weight, as makeFaceValueFn) into gA_, gB_, Hf_, which
+/// the momentum solve only overwrites after assembly; returns 1 then.
 int Ctx::linUpwindGrad(const BcTab& ub, int gradScheme)
 {
     if (schemes_.div != CFG_DIV_LINEAR_UPWIND) return 0;
     const double* xs[3] = {U_.c[0], U_.c[1], U_.c[2]};
     V3P g[3] = {gA_, gB_, Hf_};
-    gradCells(xs, 3, ub, gradScheme, true, g);
+    gradCells(xs, 3, ub, gradScheme, false, g);
     return 1;
 }
 
@@ -1214,10 +1165,6 @@ void Ctx::launchCheck(const char* what, int kernels)
     if (e != cudaSuccess) fail(CFG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-namespace
-{
-CV3P cv(const V3P& v) { return CV3P{{v.c[0], v.c[1], v.c[2]}}; }
-}  // namespace
 
 /// fvc::grad of NC cell fields into gA_ (NC = 1) or gA_/gB_/... (see callers):
 /// scheme linear | corrected | leastSquares; volQuirk selects the
@@ -1820,8 +1767,9 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
     CFG_CUDA(cudaSetDevice(device_));
     refreshBc();
     checkMomentumBcs();
-    setNu(ctl.nu);
+    if (!turb_) setNu(ctl.nu);  // with a RANS model the model's nu + nut is the diffusivity
     std::memset(&res, 0, sizeof res);
+    lastTurbInner = 0;
     const int nC = dm_.nC;
     const int gs = schemes_.grad;
     const double alpha = schemes_.div == CFG_DIV_BLEND ? schemes_.blend_coeff : (schemes_.div == CFG_DIV_LINEAR ? 1.0 : 0.0);
@@ -1837,6 +1785,7 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
     CFG_CUDA(cudaEventRecord(tm_.ev[0], stream_));
     for (int iter = 1; iter <= ctl.max_iterations; ++iter)
     {
+        if (turb_) turbCorrect(lastTurbInner);  // simpleSolver.cpp:52
         CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
         // ---- momentum ----
         {

@@ -353,6 +353,23 @@ int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* resul
  * of the mesh counts, every patch's U/p conditions, schemes and controls. */
 int cfg_case_inspect(const char* path, char* out, size_t size);
 
+/* ---- RANS turbulence -------------------------------------------------------- */
+
+/* RansModel::create + KEpsilon (src/3d/src/turbulence/turbulenceModel.cpp,
+ * kEpsilon.cpp, wallFunction.cpp): model "kEpsilon" (standard constants,
+ * Spalding wall functions on patches of type "wall", k and epsilon fixed on
+ * patches of type "inlet") or "laminar" (removes a model).  Set up after the
+ * velocity conditions: the initial k = 1.5 (U_inlet intensity)^2 and
+ * epsilon = Cmu^0.25 k^1.5 / L (L = length_scale, or 7% of the box diagonal
+ * when length_scale <= 0).  The model is then advanced once per SIMPLE outer
+ * iteration and supplies nu + nut on faces to the momentum equation
+ * (simpleSolver.cpp:52, :97); `nu` is the molecular viscosity. */
+int cfg_turbulence_setup(cfg_ctx* ctx, const char* model, double intensity, double length_scale, double relaxation,
+                         double nu);
+/* k, epsilon, nut (nCells, original order) and nu + nut on faces (nFaces);
+ * any pointer may be NULL. */
+int cfg_turbulence_fields(cfg_ctx* ctx, double* k, double* eps, double* nut, double* nu_eff_face);
+
 /* ---- detail blocks of a coupled 1D-3D network ------------------------- */
 
 /* BlockMeasure (src/coupling/include/cf/coupling/CoupledNetwork.h:327-357),

@@ -1358,11 +1358,13 @@ int cfo_flux_from_U(const cfo_mesh* m, const cfo_bcs* bc, const double* U, doubl
  * face value is the upwind cell's value extrapolated along its gradient,
  * U_f = U_u + (grad U)_u . (Cf - C_u), u the upwind cell of phi_f >= 0 ->
  * owner.  The matrix keeps the upwind part; the extrapolation, evaluated on
- * the iterate the equation is assembled from with fvc::grad of each
+ * the iterate the equation is assembled from with the gradient of each
  * component under U's conditions and the case's grad scheme, is a deferred
  * correction: -phi_f d_f on the owner's right-hand side, +phi_f d_f on the
  * neighbour's, summed per cell in face order and added after the other
- * right-hand-side terms. */
+ * right-hand-side terms.  The gradient interpolates internal faces with the
+ * bounded owner weight (makeFaceValueFn, interpolate.cpp), as the
+ * reference's strain rate of U does (turbulenceModel.cpp:197-211). */
 static void linear_upwind_rhs(fvmat* U, const simple_ws* w, const cfo_controls* ctl, const double* uc,
                               const double* uk, const double* phi, const double* Ucur)
 {
@@ -1371,10 +1373,12 @@ static void linear_upwind_rhs(fvmat* U, const simple_ws* w, const cfo_controls* 
     double* comp = (double*)xcalloc((size_t)nC, sizeof(double));
     double* g = (double*)xcalloc((size_t)(3 * nC), sizeof(double));
     double* s = (double*)xcalloc((size_t)nC, sizeof(double));
+    double* bv = (double*)xcalloc((size_t)nB + 1, sizeof(double));
     for (int q = 0; q < 3; ++q)
     {
         for (int64_t c = 0; c < nC; ++c) comp[c] = Ucur[3 * c + q];
-        vol_grad(w, comp, uc + q * nB, uk + q * nB, ctl->grad, g);
+        for (int64_t b = 0; b < nB; ++b) bv[b] = uc[q * nB + b] * comp[m->own[m->nInt + b]] + uk[q * nB + b];
+        grad_any(&w->g, comp, bv, ctl->grad, 0, g);
         memset(s, 0, sizeof(double) * (size_t)nC);
         for (int64_t f = 0; f < m->nInt; ++f)
         {
@@ -1391,6 +1395,7 @@ static void linear_upwind_rhs(fvmat* U, const simple_ws* w, const cfo_controls* 
     free(comp);
     free(g);
     free(s);
+    free(bv);
 }
 
 static int build_ueqn(fvmat* U, const simple_ws* w, const cfo_controls* ctl, const double* uc, const double* uk,

@@ -12,6 +12,7 @@
 //   grad   <case.dict> <out> <points|-> <T.f64> <bvals.f64>
 //                                                     fvc::grad, both overloads
 //   simple <case.dict> <out> [points|-] [statedir]    solveIncompressibleSimple
+//   rans   <case.dict> <out> [points|-]               the same with the case's RANS model
 //   eqns   <case.dict> <out> <points|-> <statedir>    UEqn / pEqn assembly probes
 //   solve  <out> <n> <trip.i64> <tripv.f64> <diag.f64> <b.f64> <x0.f64> <cg|bicgstab> <tol> <maxIter>
 //
@@ -36,6 +37,7 @@
 #include "cf/fvm/MeshLoader.h"
 #include "cf/fvm/PressureCorrection.h"
 #include "cf/fvm/SimpleSolver.h"
+#include "cf/turbulence/TurbulenceModel.h"
 
 // Built as cf_adapter_driver, the simple mode runs the same case through the
 // GPU drop-in (chuanflow_b200/adapter) instead of the reference's solver.
@@ -231,6 +233,44 @@ int modeGrad(int argc, char** argv)
     return 0;
 }
 
+/// simple with the case's turbulence{} block: the model is created after the
+/// boundary conditions and the initial flux (simpleFoamApp.cpp:93-102) and
+/// advanced inside solveIncompressibleSimple; k, the dissipation, nut and
+/// the wall layer are dumped next to U, p and phi.
+int modeRans(int argc, char** argv)
+{
+    const Dictionary caseDict = Dictionary::parseFile(argv[2]);
+    const std::string out = argv[3];
+    polyMesh mesh = loadMesh(caseDict, argv[2], argc > 4 ? argv[4] : "");
+    const scalar nu = caseDict.getScalar("nu");
+    volVectorField U(mesh, "U");
+    volScalarField p(mesh, "p");
+    surfaceScalarField phi(mesh, "phi", 0.0);
+    applyPatches(caseDict, mesh, U, p);
+    phi.correctBoundaryFlux(U);
+    const Schemes schemes = loadSchemes(caseDict);
+    const SimpleControls ctl = readControls(caseDict);
+    const TurbulenceConfig cfg = TurbulenceConfig::fromCase(caseDict);
+    std::unique_ptr<RansModel> turb = RansModel::create(mesh, U, phi, nu, schemes, cfg);
+    const auto t0 = std::chrono::steady_clock::now();
+    const SimpleResult res = solveIncompressibleSimple(mesh, U, p, phi, nu, schemes, ctl, turb.get());
+    const auto t1 = std::chrono::steady_clock::now();
+    writeVec(out + "/U.f64", U.internalField());
+    writeSca(out + "/p.f64", p.internalField());
+    writeSca(out + "/phi.f64", phi.values());
+    writeSca(out + "/k.f64", turb->k());
+    writeSca(out + "/eps.f64", turb->dissipation());
+    writeSca(out + "/nut.f64", turb->nut());
+    writeSca(out + "/nuEffFace.f64", turb->nuEffFace());
+    writeSca(out + "/wallUTau.f64", turb->wallUTau());
+    writeSca(out + "/wallYPlus.f64", turb->wallYPlus());
+    std::ofstream r(out + "/result.txt");
+    r << std::setprecision(17) << res.iterations << " " << res.finalContinuityError << " "
+      << res.finalMomentumResidual << " " << (res.converged ? 1 : 0) << " "
+      << std::chrono::duration<double>(t1 - t0).count() << " " << mesh.nCells() << "\n";
+    return 0;
+}
+
 int modeSimple(int argc, char** argv)
 {
     const Dictionary caseDict = Dictionary::parseFile(argv[2]);
@@ -396,6 +436,7 @@ int main(int argc, char** argv)
         if (mode == "mesh" && argc >= 4) return modeMesh(argc, argv);
         if (mode == "grad" && argc >= 7) return modeGrad(argc, argv);
         if (mode == "simple" && argc >= 4) return modeSimple(argc, argv);
+        if (mode == "rans" && argc >= 4) return modeRans(argc, argv);
         if (mode == "eqns" && argc >= 6) return modeEqns(argc, argv);
         if (mode == "solve" && argc >= 12) return modeSolve(argc, argv);
         std::cerr << "cf_ref_driver: bad arguments for mode " << mode << "\n";

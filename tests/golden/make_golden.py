@@ -16,6 +16,8 @@ Fixtures (small .npz files):
   simple_channel.npz       10x6x5 inlet/outlet channel: 4 SIMPLE iterations
   eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
   solve_cg.npz, solve_bicgstab.npz   one CSR solve each
+  rans_channel.npz         12x5x5 orthogonal channel at Re_H 2e4 with the reference's k-epsilon:
+                           5 SIMPLE iterations (U, p, phi, k, epsilon, nut, nu + nut on faces)
 """
 import os
 import subprocess
@@ -115,6 +117,22 @@ def eqns_npz(name, dict_text, points, state):
         print("wrote", name)
 
 
+def rans_npz(name, text, points):
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(text)
+        pp = os.path.join(td, "points.f64")
+        np.ascontiguousarray(points).tofile(pp)
+        O.ref_run(["rans", cp, td, pp])
+        res = open(os.path.join(td, "result.txt")).read().split()
+        out = {"points": points, "dict": np.array(text), "iterations": int(res[0]),
+               "U": O.read(os.path.join(td, "U.f64"), shape=(-1, 3))}
+        for k in ("p", "phi", "k", "eps", "nut", "nuEffFace", "wallUTau", "wallYPlus"):
+            out[k] = O.read(os.path.join(td, k + ".f64"))
+        np.savez_compressed(os.path.join(HERE, name), **out)
+        print("wrote", name, res[:4])
+
+
 def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
     n = rs.size - 1
     rows = np.repeat(np.arange(n), np.diff(rs))
@@ -162,6 +180,9 @@ def main():
     simple_npz("simple_cavity.npz", cav, K.cavity_dict(6, 5, 4, iters=3), cav.mesh.points)
     ch = K.channel_case(10, 6, 5)
     simple_npz("simple_channel.npz", ch, K.channel_dict(10, 6, 5, iters=4), ch.mesh.points)
+
+    rc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0)
+    rans_npz("rans_channel.npz", K.rans_channel_dict(), rc.mesh.points)
 
     rng = np.random.default_rng(11)
     m = cav.mesh

@@ -1,0 +1,50 @@
+"""The device k-epsilon model (RansModel + KEpsilon + Spalding wall
+functions) inside SIMPLE against the reference's own run of the same
+channel at Re_H 2e4 (tests/golden/rans_channel.npz, made by the compiled
+reference).  The wall functions evaluate exp and pow on the device, so the
+bar is relative, not bit-for-bit."""
+import numpy as np
+import pytest
+
+import _cases as K
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-6  # relative L2 of every field after the fixture's iterations (FP64)
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def test_kepsilon_channel_matches_reference(golden):
+    import chuanflow_b200 as cf
+    g = golden("rans_channel.npz")
+    mesh, case = K.rans_channel_product()
+    assert np.array_equal(mesh.addressing()["points"], g["points"])
+    oc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0, nu=2.5e-6, iters=int(g["iterations"]),
+                         non_orth=1)
+    res = case.solve(K.controls_from(oc))
+    assert res.iterations == int(g["iterations"])
+    U, p, phi = case.download()
+    t = case.turbulence_fields()
+    for a, b, name in ((U, g["U"], "U"), (p, g["p"], "p"), (phi, g["phi"], "phi"), (t["k"], g["k"], "k"),
+                       (t["eps"], g["eps"], "eps"), (t["nut"], g["nut"], "nut"),
+                       (t["nuEffFace"], g["nuEffFace"], "nuEffFace")):
+        assert rel(a, b) < REL_TOL, (name, rel(a, b))
+
+
+def test_turbulence_setup_errors():
+    import chuanflow_b200 as cf
+    mesh, case = K.channel_product(6, 3, 3)
+    with pytest.raises(cf.CfgError, match="kOmega"):
+        case.turbulence_setup("kOmegaSST")
+    with pytest.raises(cf.CfgError, match="relaxation"):
+        case.turbulence_setup("kEpsilon", relaxation=1.5)
+    with pytest.raises(cf.CfgError, match="no turbulence"):
+        case.turbulence_fields()
+    case.turbulence_setup("kEpsilon", nu=1e-3)
+    case.turbulence_setup("laminar")
+    with pytest.raises(cf.CfgError, match="no turbulence"):
+        case.turbulence_fields()

@@ -79,7 +79,7 @@ def test_linear_upwind_equations_bit_exact():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("grad", ["corrected", "leastSquares"])
+@pytest.mark.parametrize("grad", ["linear", "corrected", "leastSquares"])
 def test_linear_upwind_simple_matches_oracle(grad):
     """SIMPLE iterations of the jittered channel with linear-upwind
     convection against the oracle's run of the same case."""
