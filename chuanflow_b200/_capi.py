@@ -544,6 +544,13 @@ def _turbulence_fields(self):
     return {"k": k, "eps": e, "nut": nut, "nuEffFace": nuf}
 
 
+def _detail_turbulence(self, model="kEpsilon", intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=1e-4):
+    """The detail block's RANS model, created at its first lossAt."""
+    _check(lib().cfg_detail_turbulence(self._h, model.encode(), C.c_double(intensity), C.c_double(length_scale),
+                                       C.c_double(relaxation), C.c_double(nu)))
+
+
+SimpleCase.detail_turbulence = _detail_turbulence
 SimpleCase.turbulence_setup = _turbulence_setup
 SimpleCase.turbulence_fields = _turbulence_fields
 SimpleCase.detail_setup = _detail_setup
@@ -553,7 +560,7 @@ SimpleCase.detail_loss = _detail_loss
 class Batch:
     """Detail-block cases evaluated together, one stream each."""
 
-    CANDIDATES = [(1, 0), (4, 2), (8, 1), (16, 1), (32, 1), (64, 1)]
+    CANDIDATES = [(1, 0), (8, 1), (16, 1), (16, -1), (32, -1), (64, -1)]
 
     def __init__(self, cases):
         self.cases = list(cases)

@@ -721,6 +721,15 @@ int cfg_detail_loss(cfg_ctx* ctx, double q, const cfg_simple_controls* controls,
     });
 }
 
+int cfg_detail_turbulence(cfg_ctx* ctx, const char* model, double intensity, double lengthScale, double relaxation,
+                          double nu)
+{
+    return guard([&] {
+        need(ctx && model, "cfg_detail_turbulence: null argument");
+        ctx->c->detailTurbulence(model, intensity, lengthScale, relaxation, nu);
+    });
+}
+
 int cfg_batch_create(int32_t n, cfg_ctx* const* blocks, cfg_batch** out)
 {
     return guard([&] {
@@ -741,7 +750,7 @@ void cfg_batch_destroy(cfg_batch* batch) { delete batch; }
 int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t rowBlocks)
 {
     return guard([&] {
-        need(batch && workers > 0 && rowBlocks >= 0, "cfg_batch_set_schedule: bad argument");
+        need(batch && workers > 0 && rowBlocks >= -1, "cfg_batch_set_schedule: bad argument");
         batch->workers = workers;
         batch->rowBlocks = rowBlocks;
     });
@@ -777,7 +786,7 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
 {
     return guard([&] {
         need(batch && q && controls && workers && rowBlocks, "cfg_batch_autotune: null argument");
-        static const int cand[][2] = {{1, 0}, {4, 2}, {8, 1}, {16, 1}, {32, 1}, {64, 1}};
+        static const int cand[][2] = {{1, 0}, {8, 1}, {16, 1}, {16, -1}, {32, -1}, {64, -1}};
         std::vector<cfg_detail_measure> m(batch->blocks.size());
         double best = 0;
         int bi = 0;

@@ -53,6 +53,8 @@ public:
     /// patches, cross-sections and the inlet profile, then lossAt(q).
     void detailSetup(const std::string& shape, double rho);
     void detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out);
+    void detailTurbulence(const std::string& model, double intensity, double lengthScale, double relaxation,
+                          double nu);
     /// Solver grid of at most k blocks per SM (0: the context's own).
     void setRowBlocks(int k);
 
@@ -163,6 +165,9 @@ private:
     void turbRefreshNut();
     void turbSolveScalar(double sigma, bool isK, double* field, double floorV, int64_t& inner);
     double* saved_ = nullptr;
+    double* savedT_ = nullptr;
+    bool savedTurb_ = false;
+    void turbCopy(double* buf, bool save);
     int rowGrid(int rows) const;
     int maxW_ = 0;     // longest matrix row
     int nSlicesEntries_ = 0;  // matrix SELL entries

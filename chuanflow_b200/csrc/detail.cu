@@ -84,6 +84,10 @@ struct DetailState
 {
     int inlet = -1, outlet = -1, axis = 0, flowSign = 1;
     double inletArea = 0, rho = 1;
+    // the block's RANS model, created at its first lossAt (after the inlet
+    // velocity it scales with is written), as coupledNetwork.cpp:1112-1113
+    std::string turbModel = "laminar";
+    double turbIntensity = 0.05, turbLength = -1, turbRelax = 0.7, turbNu = 1e-4;
     std::vector<int64_t> inletFaces;
     std::vector<double> inletWeights;  // empty: flat
     std::vector<int> first, last;      // device slots of the first and last cross-section
@@ -277,6 +281,8 @@ void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measur
         setFaceValuesU(static_cast<int64_t>(d.inletFaces.size()), d.inletFaces.data(), vals.data());
     }
     initFlux(nullptr);  // phi.correctBoundaryFlux(U)
+    if (!turb_ && d.turbModel != "laminar")
+        turbulenceSetup(d.turbModel, d.turbIntensity, d.turbLength, d.turbRelax, d.turbNu);
     cfg_simple_result res{};
     iterate(ctl, res);
     // measure (coupledNetwork.cpp:1154-1195)
@@ -310,6 +316,20 @@ void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measur
     else if (out.dp_pa <= 0) out.status = CFG_ENUMERIC;
 }
 
+void Ctx::detailTurbulence(const std::string& model, double intensity, double lengthScale, double relaxation,
+                           double nu)
+{
+    if (!detail_) fail(CFG_EINVAL, "cfg_detail_turbulence: call cfg_detail_setup first");
+    if (model != "laminar" && model != "kEpsilon")
+        fail(CFG_ESETUP, "turbulence: model '" + model + "' is not on the GPU path (laminar | kEpsilon)");
+    detail_->turbModel = model;
+    detail_->turbIntensity = intensity;
+    detail_->turbLength = lengthScale;
+    detail_->turbRelax = relaxation;
+    detail_->turbNu = nu;
+    if (model == "laminar" && turb_) turbulenceSetup("laminar", 0, 0, 1, nu);
+}
+
 void Ctx::saveState()
 {
     CFG_CUDA(cudaSetDevice(device_));
@@ -319,6 +339,12 @@ void Ctx::saveState()
         CFG_CUDA(cudaMemcpyAsync(saved_ + q * nC, U_.c[q], nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CFG_CUDA(cudaMemcpyAsync(saved_ + 3 * nC, p_, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CFG_CUDA(cudaMemcpyAsync(saved_ + 4 * nC, phi_, nF * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    savedTurb_ = turb_ != nullptr;
+    if (savedTurb_)
+    {
+        if (!savedT_) savedT_ = alloc<double>(3 * nC);
+        turbCopy(savedT_, true);
+    }
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -331,6 +357,7 @@ void Ctx::restoreState()
         CFG_CUDA(cudaMemcpyAsync(U_.c[q], saved_ + q * nC, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CFG_CUDA(cudaMemcpyAsync(p_, saved_ + 3 * nC, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     CFG_CUDA(cudaMemcpyAsync(phi_, saved_ + 4 * nC, nF * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    if (savedTurb_ && turb_) turbCopy(savedT_, false);
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -387,7 +414,13 @@ void batchPass(cfg_batch& b, const double* q, const cfg_simple_controls* ctl, cf
     for (int i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(),
                      [&](int x, int y) { return b.blocks[x]->mesh().nCells > b.blocks[y]->mesh().nCells; });
-    for (cfg::Ctx* c : b.blocks) c->setRowBlocks(b.rowBlocks);
+    // rowBlocks < 0: by size, so a large block on the critical path keeps a
+    // wide grid while small ones share the SMs (1 block per SM per 32k cells,
+    // at most 4)
+    for (cfg::Ctx* c : b.blocks)
+        c->setRowBlocks(b.rowBlocks >= 0 ? b.rowBlocks
+                                         : static_cast<int>(std::min<int64_t>(4, std::max<int64_t>(
+                                                                                  1, c->mesh().nCells / 32768))));
     std::atomic<int> next{0};
     std::vector<std::string> errs(static_cast<size_t>(n));
     std::vector<int> codes(static_cast<size_t>(n), CFG_OK);

@@ -578,6 +578,17 @@ void Ctx::turbCorrect(int64_t& inner)
     turbRefreshNut();
 }
 
+/// k, epsilon and nut to (save) or from a device buffer of 3 nCells
+void Ctx::turbCopy(double* buf, bool save)
+{
+    TurbState& t = *turb_;
+    const size_t n = static_cast<size_t>(dm_.nC);
+    double* f[3] = {t.k, t.eps, t.nut};
+    for (int i = 0; i < 3; ++i)
+        CFG_CUDA(cudaMemcpyAsync(save ? buf + i * n : f[i], save ? f[i] : buf + i * n, n * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, stream_));
+}
+
 void Ctx::turbulenceFields(double* k, double* eps, double* nut, double* nuEffFace)
 {
     if (!turb_) fail(CFG_EINVAL, "cfg_turbulence_fields: no turbulence model set up");

@@ -406,6 +406,12 @@ int cfg_detail_setup(cfg_ctx* ctx, const char* inlet_shape, double rho);
  * when the drop is non-finite or non-positive, where lossAt raises. */
 int cfg_detail_loss(cfg_ctx* ctx, double q, const cfg_simple_controls* controls, cfg_detail_measure* out);
 
+/* DetailBlock's TurbulenceConfig (coupledNetwork.cpp:1112-1113): the block's
+ * RANS model ("laminar" or "kEpsilon", see cfg_turbulence_setup), created at
+ * its first lossAt after the inlet velocity is written. */
+int cfg_detail_turbulence(cfg_ctx* ctx, const char* model, double intensity, double length_scale, double relaxation,
+                          double nu);
+
 /* A batch of detail-block contexts on one device (no reference counterpart:
  * solveCoupled1d3d evaluates its blocks one after another,
  * coupledNetwork.cpp:1454-1487).  The contexts stay owned by the caller and
@@ -415,7 +421,8 @@ int cfg_batch_create(int32_t n, cfg_ctx* const* blocks, cfg_batch** out);
 void cfg_batch_destroy(cfg_batch* batch);
 /* The schedule: `workers` blocks in flight at once (1 = one after another),
  * each block's solver kernels on a grid of at most `row_blocks_per_sm`
- * blocks per SM (0 = the context's own grid). */
+ * blocks per SM (0 = the context's own grid; -1 = by block size, one per
+ * 32k cells between 1 and 4). */
 int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t row_blocks_per_sm);
 /* One coupling pass: lossAt(q[i]) of every block i with controls[i]; wall_ms
  * (may be NULL) is the pass's host wall time.  A block whose drop lossAt
@@ -430,8 +437,8 @@ int cfg_batch_restore(cfg_batch* batch);
  * from the blocks' current fields (saved and restored around each), the
  * fastest is kept and then runs that pass for real; the chosen schedule and
  * each candidate's wall time are returned (times: 6 doubles, may be NULL).
- * Candidates (workers, row blocks per SM): (1,0), (4,2), (8,1), (16,1),
- * (32,1), (64,1). */
+ * Candidates (workers, row blocks per SM): (1,0), (8,1), (16,1), (16,-1),
+ * (32,-1), (64,-1). */
 int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
                        int32_t* row_blocks_per_sm, double* times);
 

@@ -165,3 +165,32 @@ def test_batch_matches_blocks_alone():
             assert np.array_equal(u, v)
     sched, times = b.autotune(q, ctl)
     assert sched in cf.Batch.CANDIDATES and len(times) == len(cf.Batch.CANDIDATES)
+
+
+def test_rans_blocks_batch_and_restore():
+    """k-epsilon detail blocks in a batch: the model is created at the first
+    lossAt, a pass repeated from restored fields (velocity, pressure, flux,
+    k, epsilon, nut) gives the same bits, and the drop is finite."""
+    import chuanflow_b200 as cf
+    from chuanflow_b200 import meshgen
+    cases = []
+    for cells, aspect, shape in ((1500, 6.0, "flat"), (3000, 9.0, "power1over7")):
+        c = cf.SimpleCase(meshgen.channel_block(cells, aspect))
+        c.detail_setup(shape)
+        c.detail_turbulence("kEpsilon", nu=0.3 * 0.1 / 2e4)
+        cases.append(c)
+    b = cf.Batch(cases)
+    b.set_schedule(2, 1)
+    ctl = cf.SimpleControls(max_iterations=2, relax_u=0.7, relax_p=0.3, p_relax_start=0.02, non_orth_correctors=1,
+                            linear_tol=1e-8, nu=0.3 * 0.1 / 2e4, p_preconditioner="DIC")
+    q = [0.3 * 0.01, 0.2 * 0.01]
+    b.loss(q, ctl)
+    b.save()
+    r1, _ = b.loss(q, ctl)
+    t1 = [c.turbulence_fields()["k"] for c in cases]
+    b.restore()
+    r2, _ = b.loss(q, ctl)
+    t2 = [c.turbulence_fields()["k"] for c in cases]
+    for x, y, a, bb in zip(r1, r2, t1, t2):
+        assert x["dp_pa"] == y["dp_pa"] and np.isfinite(x["dp_pa"])
+        assert np.array_equal(a, bb)
