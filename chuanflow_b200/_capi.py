@@ -54,7 +54,7 @@ class _PoissonReport(C.Structure):
                 ("true_rel_residual", C.c_double), ("device_ms", C.c_double), ("initial_rel_residual", C.c_double)]
 
 
-POISSON = {"jacobi64": 0, "dic64": 1, "ir32": 2}
+POISSON = {"jacobi64": 0, "dic64": 1, "ir32": 2, "fcg_mpnn": 3}
 
 
 class _Report(C.Structure):
@@ -550,6 +550,58 @@ def _detail_turbulence(self, model="kEpsilon", intensity=0.05, length_scale=-1.0
                                        C.c_double(relaxation), C.c_double(nu)))
 
 
+def _mpnn_create(self, layers=4, seed=1):
+    """The learned pressure preconditioner on this case's pressure matrix."""
+    _check(lib().cfg_mpnn_create(self._h, C.c_int32(layers), C.c_uint64(seed)))
+
+
+def _mpnn_weights(self, set=None):
+    """The FP32 master weights (after setting `set`, when given)."""
+    n = C.c_int64()
+    _check(lib().cfg_mpnn_params(self._h, C.byref(n)))
+    out = np.zeros(n.value, np.float32)
+    src = None if set is None else np.ascontiguousarray(set, np.float32)
+    _check(lib().cfg_mpnn_weights(self._h, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                  None if src is None else src.ctypes.data_as(C.POINTER(C.c_float)), n))
+    return out
+
+
+def _mpnn_loss_grad(self, r):
+    n = C.c_int64()
+    _check(lib().cfg_mpnn_params(self._h, C.byref(n)))
+    g = np.zeros(n.value, np.float32)
+    loss = C.c_double()
+    _check(lib().cfg_mpnn_loss_grad(self._h, _dp(_f64(r)), C.byref(loss), g.ctypes.data_as(C.POINTER(C.c_float))))
+    return loss.value, g
+
+
+def _mpnn_apply(self, r):
+    z = np.zeros(self.mesh.n_cells)
+    _check(lib().cfg_mpnn_apply(self._h, _dp(_f64(r)), _dp(z)))
+    return z
+
+
+def _mpnn_train(self, samples, epochs=1, lr=1e-3):
+    """Adam over residual samples (rows); returns the per-epoch mean losses."""
+    s = np.ascontiguousarray(samples, np.float64)
+    losses = np.zeros(epochs)
+    _check(lib().cfg_mpnn_train(self._h, _dp(s), C.c_int32(s.shape[0]), C.c_int32(epochs), C.c_float(lr),
+                                _dp(losses)))
+    return losses
+
+
+def _poisson_residual(self, b, x):
+    r = np.zeros(self.mesh.n_cells)
+    _check(lib().cfg_poisson_residual(self._h, _dp(_f64(b)), _dp(_f64(x)), _dp(r)))
+    return r
+
+
+SimpleCase.mpnn_create = _mpnn_create
+SimpleCase.mpnn_weights = _mpnn_weights
+SimpleCase.mpnn_loss_grad = _mpnn_loss_grad
+SimpleCase.mpnn_apply = _mpnn_apply
+SimpleCase.mpnn_train = _mpnn_train
+SimpleCase.poisson_residual = _poisson_residual
 SimpleCase.detail_turbulence = _detail_turbulence
 SimpleCase.turbulence_setup = _turbulence_setup
 SimpleCase.turbulence_fields = _turbulence_fields

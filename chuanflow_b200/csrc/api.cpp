@@ -835,3 +835,61 @@ int cfg_turbulence_fields(cfg_ctx* ctx, double* k, double* eps, double* nut, dou
         ctx->c->turbulenceFields(k, eps, nut, nuEffFace);
     });
 }
+
+// ---- learned pressure preconditioner ----
+
+int cfg_mpnn_create(cfg_ctx* ctx, int32_t layers, uint64_t seed)
+{
+    return guard([&] {
+        need(ctx, "cfg_mpnn_create: null argument");
+        ctx->c->mpnnCreate(layers, seed);
+    });
+}
+
+int cfg_mpnn_params(const cfg_ctx* ctx, int64_t* n)
+{
+    return guard([&] {
+        need(ctx && n, "cfg_mpnn_params: null argument");
+        *n = ctx->c->mpnnParams();
+    });
+}
+
+int cfg_mpnn_weights(cfg_ctx* ctx, float* get, const float* set, int64_t n)
+{
+    return guard([&] {
+        need(ctx, "cfg_mpnn_weights: null argument");
+        ctx->c->mpnnWeights(get, set, n);
+    });
+}
+
+int cfg_mpnn_loss_grad(cfg_ctx* ctx, const double* r, double* loss, float* grad)
+{
+    return guard([&] {
+        need(ctx && r && loss, "cfg_mpnn_loss_grad: null argument");
+        *loss = ctx->c->mpnnLossGradHost(r, grad);
+    });
+}
+
+int cfg_mpnn_apply(cfg_ctx* ctx, const double* r, double* z)
+{
+    return guard([&] {
+        need(ctx && r && z, "cfg_mpnn_apply: null argument");
+        ctx->c->mpnnApplyHost(r, z);
+    });
+}
+
+int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t nSamples, int32_t epochs, float lr, double* losses)
+{
+    return guard([&] {
+        need(ctx && samples, "cfg_mpnn_train: null argument");
+        ctx->c->mpnnTrainHost(samples, nSamples, epochs, lr, losses);
+    });
+}
+
+int cfg_poisson_residual(cfg_ctx* ctx, const double* b, const double* x, double* r)
+{
+    return guard([&] {
+        need(ctx && b && x && r, "cfg_poisson_residual: null argument");
+        ctx->c->poissonResidual(b, x, r);
+    });
+}

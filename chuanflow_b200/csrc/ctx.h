@@ -5,6 +5,7 @@
 
 #include <map>
 #include <string>
+#include <algorithm>
 #include <memory>
 #include <vector>
 
@@ -25,6 +26,11 @@ struct DetailState;
 struct DetailDeleter
 {
     void operator()(DetailState* d) const;
+};
+struct MpnnState;
+struct MpnnDeleter
+{
+    void operator()(MpnnState* m) const;
 };
 struct TurbState;
 struct TurbDeleter
@@ -65,8 +71,19 @@ public:
                          double nu);
     void turbulenceFields(double* k, double* eps, double* nut, double* nuEffFace);
     bool hasTurbulence() const { return static_cast<bool>(turb_); }
+
+    /// The learned pressure preconditioner (mpnn.cu) on the context's
+    /// pressure matrix (the Poisson system or the last SIMPLE equation).
+    void mpnnCreate(int layers, uint64_t seed);
+    void mpnnWeights(float* get, const float* set, int64_t n);
+    int mpnnParams() const;
+    double mpnnLossGradHost(const double* r, float* grad);
+    void mpnnApplyHost(const double* r, double* z);
+    void mpnnTrainHost(const double* samples, int nSamples, int epochs, float lr, double* losses);
+    void poissonResidual(const double* b, const double* x, double* r);
     void refreshBcPublic() { refreshBc(); }
     int64_t lastTurbInner = 0;
+    int64_t lastFallbackIters = 0;
     /// A device-side copy of U, p, phi, and its return (for schedule trials
     /// on identical work).
     void saveState();
@@ -161,6 +178,19 @@ private:
     int initRowBlocks_ = 4, initGS_ = 0, initDicPartials_ = 1;
     std::unique_ptr<DetailState, DetailDeleter> detail_;
     std::unique_ptr<TurbState, TurbDeleter> turb_;
+    std::unique_ptr<MpnnState, MpnnDeleter> mpnn_;
+    void mpnnApply(const double* vals, const double* diag, const double* r, double* z);
+    double mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z);
+    void mpnnAdam(float lr);
+    void mpnnMatrix(const double** vals, const double** diag) const;
+    void mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses);
+    void mpnnFcg(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                 int window, int64_t* out);
+    void fcgSpmv(const double* vals, const double* x, double* y);
+    void fcgDots(int np, const double* const* a, const double* const* b, double* out);
+    const double** fcgPtrs_ = nullptr;
+    double* fcgOut_ = nullptr;
+    unsigned* fcgTicket_ = nullptr;
     void turbCorrect(int64_t& inner);
     void turbRefreshNut();
     void turbSolveScalar(double sigma, bool isK, double* field, double floorV, int64_t& inner);
@@ -232,6 +262,30 @@ private:
     void tmark(int k, int j);
     void harvest(int ran, const int* slots, int nSlots);
 };
+
+}  // namespace cfg
+
+namespace cfg
+{
+
+/// device memory owned by the context (zeroed), released in its destructor
+template <class T>
+T* Ctx::alloc(size_t n)
+{
+    void* p = nullptr;
+    CFG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    allocs_.push_back(p);
+    CFG_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), stream_));
+    return static_cast<T*>(p);
+}
+
+template <class T>
+T* Ctx::upload(const std::vector<T>& v)
+{
+    T* p = alloc<T>(v.size());
+    if (!v.empty()) CFG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    return p;
+}
 
 }  // namespace cfg
 

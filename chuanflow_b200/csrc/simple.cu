@@ -529,24 +529,6 @@ __global__ void __launch_bounds__(TPB) k_add_f32(int n, const float* __restrict_
 // host side
 // ===========================================================================
 
-template <class T>
-T* Ctx::alloc(size_t n)
-{
-    void* p = nullptr;
-    CFG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
-    allocs_.push_back(p);
-    CFG_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(T), stream_));
-    return static_cast<T*>(p);
-}
-
-template <class T>
-T* Ctx::upload(const std::vector<T>& v)
-{
-    T* p = alloc<T>(v.size());
-    if (!v.empty()) CFG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
-    return p;
-}
-
 namespace
 {
 inline double hdot(const Vec& a, const Vec& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
@@ -2133,6 +2115,16 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
             rel = trueRel();
         }
     }
+    else if (method == 3)
+    {
+        // flexible CG with the learned preconditioner, DIC-PCG when it stalls
+        if (!mpnn_) fail(CFG_EINVAL, "cfg_poisson_solve: fcg_mpnn needs cfg_mpnn_create");
+        int64_t o[3];
+        mpnnFcg(pVal_d_, pDiag_, pb64_, px64_, tol, maxIter, 25, o);
+        inner = o[0] + o[1];
+        outer = 1 + static_cast<int>(o[2]);
+        lastFallbackIters = o[1];
+    }
     else
     {
         fail(CFG_EINVAL, "cfg_poisson_solve: unknown method");
@@ -2150,5 +2142,9 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
     out[4] = ms;
     out[5] = rel0;
 }
+
+// the FP64 DIC-PCG is also the fallback of the learned preconditioner (mpnn.cu)
+template void Ctx::dicCGT<double>(const DDicT<double>&, const double*, const double*, const double*, double*, double*,
+                                  double*, double*, double*, double, int, int, cfg_solver_report*);
 
 }  // namespace cfg

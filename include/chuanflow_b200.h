@@ -270,7 +270,9 @@ enum cfg_poisson_method
 {
     CFG_POISSON_JACOBI64 = 0,  /* FP64 Jacobi-PCG, the reference's solver */
     CFG_POISSON_DIC64 = 1,     /* FP64 multicolour-DIC PCG */
-    CFG_POISSON_IR32 = 2       /* FP32 DIC-PCG corrections inside FP64 iterative refinement */
+    CFG_POISSON_IR32 = 2,      /* FP32 DIC-PCG corrections inside FP64 iterative refinement */
+    CFG_POISSON_FCG_MPNN = 3   /* flexible CG with the learned preconditioner (cfg_mpnn_create),
+                                * FP64 DIC-PCG from its iterate when it stalls */
 };
 
 typedef struct cfg_poisson_report
@@ -369,6 +371,30 @@ int cfg_turbulence_setup(cfg_ctx* ctx, const char* model, double intensity, doub
 /* k, epsilon, nut (nCells, original order) and nu + nut on faces (nFaces);
  * any pointer may be NULL. */
 int cfg_turbulence_fields(cfg_ctx* ctx, double* k, double* eps, double* nut, double* nu_eff_face);
+
+/* ---- learned pressure preconditioner (no reference counterpart) ------------ */
+
+/* A message-passing network on the cell-face graph of the context's pressure
+ * matrix (the cfg_poisson_setup system, else the last SIMPLE pressure
+ * equation): z = r/diag + s (wout . h), h from `layers` residual layers of
+ * width 32 with one-hop messages weighted by -a_ij/a_ii, s = rms(r).  FP32
+ * master weights, BF16 in use, FP32 activations; trained on the device.
+ * Parameters: 64 + layers * 2080 + 32 floats. */
+int cfg_mpnn_create(cfg_ctx* ctx, int32_t layers, uint64_t seed);
+int cfg_mpnn_params(const cfg_ctx* ctx, int64_t* n);
+/* FP32 master weights: get and/or set (either may be NULL). */
+int cfg_mpnn_weights(cfg_ctx* ctx, float* get, const float* set, int64_t n);
+/* loss |A M(r) - r|^2 / |r|^2 of one residual sample and its gradient with
+ * respect to the (BF16-rounded) weights; grad may be NULL. */
+int cfg_mpnn_loss_grad(cfg_ctx* ctx, const double* r, double* loss, float* grad);
+/* z = M(r) */
+int cfg_mpnn_apply(cfg_ctx* ctx, const double* r, double* z);
+/* Adam (lr) over n_samples residual samples (n_samples x nCells, original
+ * order), `epochs` passes; losses[epoch] = mean loss (may be NULL). */
+int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t n_samples, int32_t epochs, float lr, double* losses);
+/* r = b - A x on the cfg_poisson_setup system (training samples from the
+ * plain solver's iterates). */
+int cfg_poisson_residual(cfg_ctx* ctx, const double* b, const double* x, double* r);
 
 /* ---- detail blocks of a coupled 1D-3D network ------------------------- */
 

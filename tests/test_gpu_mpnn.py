@@ -1,0 +1,95 @@
+"""The learned pressure preconditioner: the device forward and backward
+kernels against the FP64 PyTorch restatement (tests/_mpnn_ref.py) on the
+same BF16 weights, training on the device from the plain solver's
+residuals, and the gain of the trained network in flexible CG."""
+import numpy as np
+import pytest
+
+import _cases as K
+import _mpnn_ref as R
+import _oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def poisson_case(n=8):
+    import chuanflow_b200 as cf
+    mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (n, n, n))
+    mesh.jitter_interior(0.15, 3)
+    case = cf.SimpleCase(mesh)
+    for p in mesh.patches:
+        case.set_patch_bc("U", p[0], "fixedValue", (0, 0, 0))
+        case.set_patch_bc("p", p[0], "zeroGradient", 0.0)
+    case.poisson_setup(ref_cell=0)
+    return mesh, case
+
+
+def oracle_csr(mesh):
+    a = mesh.addressing()
+    om = O.OMesh(a["points"], a["face_offsets"], a["face_verts"], a["owner"], a["neighbour"],
+                 [p[0] for p in mesh.patches], [p[1] for p in mesh.patches], [p[2] for p in mesh.patches],
+                 [p[3] for p in mesh.patches])
+    oc = O.Case(om, u_type=["fixedValue"] * mesh.n_patches, u_value=[(0, 0, 0)] * mesh.n_patches,
+                p_type=["zeroGradient"] * mesh.n_patches, p_value=[0] * mesh.n_patches, nu=1.0)
+    oc.p_ref_cell = 0
+    return oc.pressure_csr(np.ones(mesh.n_faces))
+
+
+@pytest.mark.parametrize("layers", [1, 4])
+def test_mpnn_gradient_matches_fp64_autograd(layers):
+    """Loss and every weight's gradient against FP64 autograd on the same
+    (BF16-exact) weights: FP32 activations and accumulation bound the gap."""
+    mesh, case = poisson_case(8)
+    case.mpnn_create(layers, seed=5)
+    rng = np.random.default_rng(7)
+    w = R.bf16_round(rng.normal(size=R.n_params(layers)).astype(np.float32) * 0.2)
+    case.mpnn_weights(set=w)
+    r = rng.normal(size=mesh.n_cells)
+    loss, g = case.mpnn_loss_grad(r)
+    rs, cols, vals = oracle_csr(mesh)
+    loss0, g0, z0 = R.loss_and_grad(rs, cols, vals, r, w, layers)
+    assert abs(loss - loss0) <= 1e-5 * abs(loss0), (loss, loss0)
+    assert np.linalg.norm(g - g0) <= 2e-4 * np.linalg.norm(g0), np.linalg.norm(g - g0) / np.linalg.norm(g0)
+    z = case.mpnn_apply(r)
+    assert np.linalg.norm(z - z0) <= 1e-5 * np.linalg.norm(z0)
+
+
+def test_untrained_network_is_jacobi():
+    mesh, case = poisson_case(6)
+    case.mpnn_create(4, seed=1)
+    r = np.random.default_rng(2).normal(size=mesh.n_cells)
+    rs, cols, vals = oracle_csr(mesh)
+    n = mesh.n_cells
+    rows = np.repeat(np.arange(n), np.diff(rs))
+    d = np.zeros(n)
+    np.add.at(d, rows[rows == cols], vals[rows == cols])
+    assert np.array_equal(case.mpnn_apply(r), r / d)
+
+
+def test_trained_network_gains_in_flexible_cg():
+    """Trained on residuals of the plain Jacobi-PCG's iterates, the network
+    lowers its training loss, and flexible CG with it needs fewer
+    iterations to the same FP64 true residual than with the untrained
+    (Jacobi) network; both reach the DIC-PCG solution."""
+    mesh, case = poisson_case(16)
+    rng = np.random.default_rng(11)
+    samples = []
+    for k in range(6):
+        b = rng.normal(size=mesh.n_cells)
+        b -= b.mean()
+        for it in (0, 5, 20, 60):
+            x, _ = case.poisson_solve(b, "jacobi64", tol=1e-14, max_iter=max(it, 1)) if it else (np.zeros_like(b), None)
+            samples.append(case.poisson_residual(b, x))
+    samples = np.array(samples)
+    case.mpnn_create(4, seed=3)
+    b = rng.normal(size=mesh.n_cells)
+    b -= b.mean()
+    x0, r0 = case.poisson_solve(b, "fcg_mpnn", tol=1e-8)
+    losses = case.mpnn_train(samples, epochs=40, lr=2e-3)
+    assert losses[-1] < 0.8 * losses[0], losses
+    x1, r1 = case.poisson_solve(b, "fcg_mpnn", tol=1e-8)
+    xd, rd = case.poisson_solve(b, "dic64", tol=1e-12)
+    assert r0["converged"] and r1["converged"]
+    assert r1["inner_iterations"] < r0["inner_iterations"], (r1, r0)
+    for x in (x0, x1):
+        assert np.linalg.norm(x - xd) <= 1e-6 * np.linalg.norm(xd)
