@@ -19,6 +19,7 @@ from ._capi import (  # noqa: F401
     Batch,
     GRAD,
     CfgError,
+    PisoControls,
     PolyMesh,
     Schemes,
     SimpleCase,
@@ -33,5 +34,5 @@ from ._capi import (  # noqa: F401
     solve_cg,
 )
 
-__all__ = ["BC", "Batch", "DIV", "GRAD", "CfgError", "PolyMesh", "Schemes", "SimpleCase", "SimpleControls",
+__all__ = ["BC", "Batch", "DIV", "GRAD", "CfgError", "PisoControls", "PolyMesh", "Schemes", "SimpleCase", "SimpleControls",
            "SimpleResult", "SolverReport", "inspect_case_file", "lib", "lib_path", "run_case_file", "solve_bicgstab", "solve_cg"]

@@ -596,6 +596,57 @@ def _poisson_residual(self, b, x):
     return r
 
 
+class _PisoControls(C.Structure):
+    _fields_ = [("dt", C.c_double), ("correctors", C.c_int32), ("continuity_tol", C.c_double),
+                ("linear_tol", C.c_double), ("linear_max_iter", C.c_int32), ("non_orth_correctors", C.c_int32),
+                ("body_force", C.c_double * 3), ("nu", C.c_double), ("p_precond", C.c_int32)]
+
+
+class _PisoResult(C.Structure):
+    _fields_ = [("correctors_used", C.c_int32), ("converged", C.c_int32), ("diverged", C.c_int32),
+                ("predicted_continuity_error", C.c_double), ("continuity_error", C.c_double),
+                ("pressure_correction_max", C.c_double), ("u_inner_iterations", C.c_int64),
+                ("p_inner_iterations", C.c_int64), ("device_ms", C.c_double)]
+
+
+@dataclass
+class PisoControls:
+    """PisoControls (src/3d/include/cf/fvm/PisoSolver.h) + nu and the GPU
+    pressure preconditioner."""
+    dt: float = 0.01
+    correctors: int = 2
+    continuity_tol: float = 1e-10
+    linear_tol: float = 1e-8
+    linear_max_iter: int = 2000
+    non_orth_correctors: int = 2
+    body_force: tuple = (0.0, 0.0, 0.0)
+    nu: float = 1e-4
+    p_preconditioner: str = "Jacobi"
+
+    def _c(self):
+        c = _PisoControls()
+        c.dt = self.dt
+        c.correctors = self.correctors
+        c.continuity_tol = self.continuity_tol
+        c.linear_tol = self.linear_tol
+        c.linear_max_iter = self.linear_max_iter
+        c.non_orth_correctors = self.non_orth_correctors
+        for i in range(3):
+            c.body_force[i] = self.body_force[i]
+        c.nu = self.nu
+        c.p_precond = PRECOND[self.p_preconditioner]
+        return c
+
+
+def _piso_step(self, controls):
+    """One transient PISO step of the device fields (dict of PisoStepResult)."""
+    c = controls._c()
+    r = _PisoResult()
+    _check(lib().cfg_piso_step(self._h, C.byref(c), C.byref(r)))
+    return {k: getattr(r, k) for k, _ in r._fields_}
+
+
+SimpleCase.piso_step = _piso_step
 SimpleCase.mpnn_create = _mpnn_create
 SimpleCase.mpnn_weights = _mpnn_weights
 SimpleCase.mpnn_loss_grad = _mpnn_loss_grad

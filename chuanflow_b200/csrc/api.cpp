@@ -893,3 +893,13 @@ int cfg_poisson_residual(cfg_ctx* ctx, const double* b, const double* x, double*
         ctx->c->poissonResidual(b, x, r);
     });
 }
+
+// ---- PISO ----
+
+int cfg_piso_step(cfg_ctx* ctx, const cfg_piso_controls* controls, cfg_piso_result* result)
+{
+    return guard([&] {
+        need(ctx && controls && result, "cfg_piso_step: null argument");
+        ctx->c->pisoStep(*controls, *result);
+    });
+}

@@ -54,6 +54,8 @@ public:
     void download(double* U, double* p, double* phi);
     void initFlux(const double* u0);
     void iterate(const cfg_simple_controls& ctl, cfg_simple_result& res);
+    /// one transient PISO step (pisoSolver.cpp)
+    void pisoStep(const cfg_piso_controls& ctl, cfg_piso_result& res);
 
     /// DetailBlock (src/coupling/src/coupledNetwork.cpp): inlet/outlet
     /// patches, cross-sections and the inlet profile, then lossAt(q).
@@ -133,7 +135,8 @@ private:
     void refreshBc();
     void gradCells(const double* const* x, int nComp, const BcTab& bc, int scheme, bool volQuirk, V3P* out);
     void solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, int64_t& inner);
-    void solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner);
+    void solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner,
+                       const double* x0 = nullptr);
     void runCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
                cfg_solver_report* rep, int normType = 0);
     void runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
@@ -195,6 +198,7 @@ private:
     void turbRefreshNut();
     void turbSolveScalar(double sigma, bool isK, double* field, double floorV, int64_t& inner);
     double* saved_ = nullptr;
+    V3P uOld_{};
     double* savedT_ = nullptr;
     bool savedTurb_ = false;
     void turbCopy(double* buf, bool save);

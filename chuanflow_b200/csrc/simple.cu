@@ -54,6 +54,8 @@ struct MomArgs
     double* mVal;
     double* uDiag;
     V3P base;
+    double dt;  // > 0: fvm::ddt(U, uOld, dt) first (divScheme.cpp:80-93)
+    CV3P uOld;
 };
 
 __device__ __forceinline__ void div_weights(double p, double alpha, double ow, double& wPo, double& wNo)
@@ -77,6 +79,15 @@ __global__ void __launch_bounds__(TPB) k_assemble_U(DMesh m, MomArgs a)
         const int e0 = m.cfStart[sl] + lane, e1 = m.cfStart[sl + 1];
         double diag = 0.0;
         double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+        if (a.dt > 0)
+        {
+            // the implicit Euler term, assembled before every face term
+            const double at = m.V[c] / a.dt;
+            diag = at;
+            r0 = at * a.uOld.c[0][c];
+            r1 = at * a.uOld.c[1][c];
+            r2 = at * a.uOld.c[2][c];
+        }
         for (int e = e0; e < e1; e += 32)  // convection
         {
             const int code = m.cfCode[e];
@@ -523,6 +534,41 @@ __global__ void __launch_bounds__(TPB) k_to_float(int n, const double* __restric
 __global__ void __launch_bounds__(TPB) k_add_f32(int n, const float* __restrict__ e, double* __restrict__ x)
 {
     ROW_LOOP(i, n) x[i] = x[i] + static_cast<double>(e[i]);
+}
+
+/// PISO's pressure-free response (pisoSolver.cpp:118-139): rAU = V/aDiag and
+/// HbyA = rAU (H(U) + V grad p^n) / V with H(U) = rhs - (A U - aDiag U), the
+/// explicit operator of the momentum equation (fvMatrix.cpp:131-146)
+template <int W>
+__global__ void __launch_bounds__(TPB) k_piso_hbya(DMat A, const double* __restrict__ val,
+                                                   const double* __restrict__ diag, CV3P rhs, CV3P U, CV3P gPn,
+                                                   const double* __restrict__ V, double* __restrict__ rAU, V3P H)
+{
+    const double* xs[3] = {U.c[0], U.c[1], U.c[2]};
+    ROW_LOOP(c, A.n)
+    {
+        double y[3];
+        spmv_row<W, 3>(A, val, c, xs, y);
+        const double d = diag[c], v = V[c];
+        const double r = v / smax(d, 1e-300);
+        rAU[c] = r;
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+            const double h = rhs.c[q][c] - (y[q] - d * U.c[q][c]);
+            H.c[q][c] = r * (h + v * gPn.c[q][c]) / v;
+        }
+    }
+}
+
+/// U = HbyA - rAU grad p (pisoSolver.cpp:202-206)
+__global__ void __launch_bounds__(TPB) k_piso_update(int n, CV3P H, const double* __restrict__ rAU, CV3P gP, V3P U)
+{
+    ROW_LOOP(c, n)
+    {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) U.c[q][c] = H.c[q][c] - rAU[c] * gP.c[q][c];
+    }
 }
 
 // ===========================================================================
@@ -1629,10 +1675,12 @@ void Ctx::checkMomentumBcs() const
     }
 }
 
-void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner)
+void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, int precond, int64_t& inner,
+                        const double* x0)
 {
     const int n = dm_.nC;
-    CFG_CUDA(cudaMemsetAsync(px_, 0, n * sizeof(double), stream_));
+    if (x0) CFG_CUDA(cudaMemcpyAsync(px_, x0, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    else CFG_CUDA(cudaMemsetAsync(px_, 0, n * sizeof(double), stream_));
     const bool corr = schemes_.laplacian_corrected != 0;
     const int passes = corr ? std::max(1, nonOrth + 1) : 1;
     const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
@@ -1776,7 +1824,7 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
             gradCells(xs, 1, pb, gs, true, g);
         }
         MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
-                   linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_};
+                   linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, 0.0, CV3P{}};
         ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
         k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
         launchCheck("assemble_U");
@@ -1855,6 +1903,104 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
     lastLaunches = launches_;
 }
 
+/// solveTransientIncompressiblePiso (pisoSolver.cpp:13-237), one time step
+void Ctx::pisoStep(const cfg_piso_controls& ctl, cfg_piso_result& res)
+{
+    CFG_CUDA(cudaSetDevice(device_));
+    if (!(ctl.dt > 0)) fail(CFG_EINVAL, "PISO: non-positive time step");
+    if (turb_) fail(CFG_ESETUP, "PISO: a RANS model with a time step is not on the GPU path");
+    refreshBc();
+    checkMomentumBcs();
+    setNu(ctl.nu);
+    std::memset(&res, 0, sizeof res);
+    const int nC = dm_.nC;
+    const int gs = schemes_.grad;
+    const double alpha = schemes_.div == CFG_DIV_BLEND ? schemes_.blend_coeff : (schemes_.div == CFG_DIV_LINEAR ? 1.0 : 0.0);
+    const BcTab ub{{uc_[0], uc_[1], uc_[2]}, {uk_[0], uk_[1], uk_[2]}};
+    const BcTab hb{{hc_[0], hc_[1], hc_[2]}, {hk_[0], hk_[1], hk_[2]}};
+    const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
+    if (!uOld_.c[0])
+        for (int q = 0; q < 3; ++q) uOld_.c[q] = alloc<double>(nC);
+    launches_ = 0;
+    CFG_CUDA(cudaEventRecord(tm_.ev[0], stream_));
+    CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
+    {
+        const double* xs[1] = {p_};
+        V3P g[1] = {gPn_};
+        gradCells(xs, 1, pb, gs, true, g);
+    }
+    for (int q = 0; q < 3; ++q)
+        CFG_CUDA(cudaMemcpyAsync(uOld_.c[q], U_.c[q], nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
+               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, ctl.dt, cv(uOld_)};
+    ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
+    k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
+    launchCheck("assemble_U");
+    solveMomentum(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, res.u_inner_iterations);
+    for (int q = 0; q < 3; ++q)
+        CFG_CUDA(cudaMemcpyAsync(U_.c[q], ux_.c[q], nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    const DMat A{nC, dm_.mStart, dm_.mCol};
+    auto hbya = [&]() {
+        dispatchW(maxW_, [&](auto Wc) {
+            constexpr int W = decltype(Wc)::value;
+            k_piso_hbya<W><<<G_, TPB, 0, stream_>>>(A, mVal_, uDiag_, cv(uRhs_), cv(U_), cv(gPn_), dm_.V, rAUr_, Hf_);
+        });
+        launchCheck("piso_hbya");
+    };
+    hbya();
+    k_face_interp<<<GF_, TPB, 0, stream_>>>(dm_, rAUr_, rAUf_);
+    launchCheck("face_interp");
+    for (int corr = 1; corr <= ctl.correctors; ++corr)
+    {
+        if (corr > 1) hbya();
+        CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
+        k_flux<<<GF_, TPB, 0, stream_>>>(dm_, cv(Hf_), hb, nullptr, phi_);
+        launchCheck("flux");
+        k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, phi_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_, -1, 0.0);
+        launchCheck("assemble_p");
+        solvePressure(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, ctl.p_precond,
+                      res.p_inner_iterations, p_);
+        k_pstep<<<G_, TPB, 0, stream_>>>(nC, px_, p_, scal_);
+        launchCheck("pstep");
+        CFG_CUDA(cudaMemcpyAsync(p_, px_, nC * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        {
+            const double* xs[1] = {p_};
+            V3P g[1] = {gPF_};
+            gradCells(xs, 1, pb, gs, true, g);
+        }
+        k_piso_update<<<G_, TPB, 0, stream_>>>(nC, cv(Hf_), rAUr_, cv(gPF_), U_);
+        launchCheck("piso_update");
+        k_correct_flux<<<GF_, TPB, 0, stream_>>>(dm_, p_, cv(gPF_), rAUf_, pc_, pk_, schemes_.laplacian_corrected,
+                                                 phi_);
+        launchCheck("correct_flux");
+        k_continuity<<<G_, TPB, 0, stream_>>>(dm_, phi_, scal_, S_CONT_AFTER);
+        launchCheck("continuity");
+        CFG_CUDA(cudaMemcpyAsync(scalHost_, scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        const double* S = scalHost_;
+        res.predicted_continuity_error = S[S_CONT];
+        res.continuity_error = S[S_CONT_AFTER];
+        res.pressure_correction_max = S[S_PSTEP];
+        res.correctors_used = corr;
+        if (!std::isfinite(res.continuity_error) || !std::isfinite(res.pressure_correction_max))
+        {
+            res.diverged = 1;
+            break;
+        }
+        if (res.continuity_error < ctl.continuity_tol)
+        {
+            res.converged = 1;
+            break;
+        }
+    }
+    CFG_CUDA(cudaEventRecord(tm_.ev[1], stream_));
+    CFG_CUDA(cudaEventSynchronize(tm_.ev[1]));
+    float ms = 0;
+    CFG_CUDA(cudaEventElapsedTime(&ms, tm_.ev[0], tm_.ev[1]));
+    res.device_ms = ms;
+    lastLaunches = launches_;
+}
+
 void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, double* out)
 {
     // the equations of one outer iteration built from the current fields,
@@ -1893,7 +2039,7 @@ void Ctx::probeEquations(const cfg_simple_controls& ctl, const double* xprobe, d
     }
     for (int q = 0; q < 3; ++q) d2hC(gPn_.c[q]);
     MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
-               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_};
+               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, 0.0, CV3P{}};
     ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
     k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
     launchCheck("assemble_U");

@@ -238,6 +238,41 @@ int cfg_fields_init_flux(cfg_ctx* ctx, const double* u0);
  * to controls->max_iterations outer iterations on the device fields. */
 int cfg_simple_iterate(cfg_ctx* ctx, const cfg_simple_controls* controls, cfg_simple_result* result);
 
+/* PisoControls (src/3d/include/cf/fvm/PisoSolver.h:13-40) plus the
+ * viscosity and the GPU pressure preconditioner */
+typedef struct cfg_piso_controls
+{
+    double dt;
+    int32_t correctors;          /* 2 */
+    double continuity_tol;       /* 1e-10 */
+    double linear_tol;           /* 1e-8 */
+    int32_t linear_max_iter;     /* 2000 */
+    int32_t non_orth_correctors; /* 2 */
+    double body_force[3];
+    double nu;
+    int32_t p_precond;           /* cfg_precond */
+} cfg_piso_controls;
+
+/* PisoStepResult (PisoSolver.h:42-50) */
+typedef struct cfg_piso_result
+{
+    int32_t correctors_used;
+    int32_t converged;
+    int32_t diverged;
+    double predicted_continuity_error;
+    double continuity_error;
+    double pressure_correction_max;
+    int64_t u_inner_iterations;
+    int64_t p_inner_iterations;
+    double device_ms;
+} cfg_piso_result;
+
+/* solveTransientIncompressiblePiso (PisoSolver.h:92-100,
+ * src/3d/src/solvers/pisoSolver.cpp:13-237), laminar: one implicit-Euler
+ * time step of the device fields (momentum once, then the correctors, each
+ * solving the full pressure from the previous iterate). */
+int cfg_piso_step(cfg_ctx* ctx, const cfg_piso_controls* controls, cfg_piso_result* result);
+
 /* Wall time (ms) of the device work of the last cfg_simple_iterate call,
  * measured with CUDA events on the context's stream, and the launch count.
  * kernel_ms[0..7] split it by family: gradient, assembly, momentum solve,

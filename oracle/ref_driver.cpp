@@ -13,6 +13,7 @@
 //                                                     fvc::grad, both overloads
 //   simple <case.dict> <out> [points|-] [statedir]    solveIncompressibleSimple
 //   rans   <case.dict> <out> [points|-]               the same with the case's RANS model
+//   piso   <case.dict> <out> [points|-]               transient PISO steps (piso{} block)
 //   eqns   <case.dict> <out> <points|-> <statedir>    UEqn / pEqn assembly probes
 //   solve  <out> <n> <trip.i64> <tripv.f64> <diag.f64> <b.f64> <x0.f64> <cg|bicgstab> <tol> <maxIter>
 //
@@ -36,6 +37,7 @@
 #include "cf/fvm/FvMatrix.h"
 #include "cf/fvm/MeshLoader.h"
 #include "cf/fvm/PressureCorrection.h"
+#include "cf/fvm/PisoSolver.h"
 #include "cf/fvm/SimpleSolver.h"
 #include "cf/turbulence/TurbulenceModel.h"
 
@@ -271,6 +273,43 @@ int modeRans(int argc, char** argv)
     return 0;
 }
 
+/// transient PISO: the case's piso{} block (dt, correctors, continuityTol,
+/// nonOrthCorrectors, linearTol, linearMaxIter, steps) from rest
+int modePiso(int argc, char** argv)
+{
+    const Dictionary caseDict = Dictionary::parseFile(argv[2]);
+    const std::string out = argv[3];
+    polyMesh mesh = loadMesh(caseDict, argv[2], argc > 4 ? argv[4] : "");
+    const scalar nu = caseDict.getScalar("nu");
+    volVectorField U(mesh, "U");
+    volScalarField p(mesh, "p");
+    surfaceScalarField phi(mesh, "phi", 0.0);
+    applyPatches(caseDict, mesh, U, p);
+    phi.correctBoundaryFlux(U);
+    const Schemes schemes = loadSchemes(caseDict);
+    PisoControls ctl;
+    const Dictionary& pd = caseDict.getDict("piso");
+    ctl.dt = pd.getScalar("dt");
+    ctl.correctors = static_cast<int>(pd.getScalarOr("correctors", ctl.correctors));
+    ctl.continuityTol = pd.getScalarOr("continuityTol", ctl.continuityTol);
+    ctl.nonOrthCorrectors = static_cast<int>(pd.getScalarOr("nonOrthCorrectors", ctl.nonOrthCorrectors));
+    ctl.linearTol = pd.getScalarOr("linearTol", ctl.linearTol);
+    ctl.linearMaxIter = static_cast<int>(pd.getScalarOr("linearMaxIter", ctl.linearMaxIter));
+    const int steps = static_cast<int>(pd.getScalarOr("steps", 1));
+    std::ofstream r(out + "/result.txt");
+    r << std::setprecision(17);
+    for (int s = 0; s < steps; ++s)
+    {
+        const PisoStepResult res = solveTransientIncompressiblePiso(mesh, U, p, phi, nu, schemes, ctl);
+        r << res.correctorsUsed << " " << res.predictedContinuityError << " " << res.continuityError << " "
+          << res.pressureCorrectionMax << " " << (res.converged ? 1 : 0) << "\n";
+    }
+    writeVec(out + "/U.f64", U.internalField());
+    writeSca(out + "/p.f64", p.internalField());
+    writeSca(out + "/phi.f64", phi.values());
+    return 0;
+}
+
 int modeSimple(int argc, char** argv)
 {
     const Dictionary caseDict = Dictionary::parseFile(argv[2]);
@@ -437,6 +476,7 @@ int main(int argc, char** argv)
         if (mode == "grad" && argc >= 7) return modeGrad(argc, argv);
         if (mode == "simple" && argc >= 4) return modeSimple(argc, argv);
         if (mode == "rans" && argc >= 4) return modeRans(argc, argv);
+        if (mode == "piso" && argc >= 4) return modePiso(argc, argv);
         if (mode == "eqns" && argc >= 6) return modeEqns(argc, argv);
         if (mode == "solve" && argc >= 12) return modeSolve(argc, argv);
         std::cerr << "cf_ref_driver: bad arguments for mode " << mode << "\n";

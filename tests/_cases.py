@@ -260,3 +260,9 @@ def rans_channel_product(nx=12, ny=5, nz=5):
     case.init_flux()
     case.turbulence_setup("kEpsilon", intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=2.5e-6)
     return mesh, case
+
+
+def piso_channel_dict(nx=16, ny=6, nz=6, dt=0.05, steps=4):
+    """The jittered channel (nu 1e-3) stepped by the reference's PISO."""
+    return channel_dict(nx, ny, nz, nu=1e-3, iters=1) + (
+        f"piso {{ dt {dt!r}; correctors 2; nonOrthCorrectors 1; linearTol 1e-10; steps {steps}; }}\n")

@@ -16,6 +16,7 @@ Fixtures (small .npz files):
   simple_channel.npz       10x6x5 inlet/outlet channel: 4 SIMPLE iterations
   eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
   solve_cg.npz, solve_bicgstab.npz   one CSR solve each
+  piso_channel.npz         16x6x6 jittered channel: 4 transient PISO steps (dt 0.05, 2 correctors)
   rans_channel.npz         12x5x5 orthogonal channel at Re_H 2e4 with the reference's k-epsilon:
                            5 SIMPLE iterations (U, p, phi, k, epsilon, nut, nu + nut on faces)
 """
@@ -133,6 +134,21 @@ def rans_npz(name, text, points):
         print("wrote", name, res[:4])
 
 
+def piso_npz(name, text, points):
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(text)
+        pp = os.path.join(td, "points.f64")
+        np.ascontiguousarray(points).tofile(pp)
+        O.ref_run(["piso", cp, td, pp])
+        steps = np.loadtxt(os.path.join(td, "result.txt"), ndmin=2)
+        out = {"points": points, "dict": np.array(text), "steps": steps,
+               "U": O.read(os.path.join(td, "U.f64"), shape=(-1, 3)), "p": O.read(os.path.join(td, "p.f64")),
+               "phi": O.read(os.path.join(td, "phi.f64"))}
+        np.savez_compressed(os.path.join(HERE, name), **out)
+        print("wrote", name, steps[-1])
+
+
 def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
     n = rs.size - 1
     rows = np.repeat(np.arange(n), np.diff(rs))
@@ -181,6 +197,8 @@ def main():
     ch = K.channel_case(10, 6, 5)
     simple_npz("simple_channel.npz", ch, K.channel_dict(10, 6, 5, iters=4), ch.mesh.points)
 
+    pc = K.channel_case(16, 6, 6)
+    piso_npz("piso_channel.npz", K.piso_channel_dict(), pc.mesh.points)
     rc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0)
     rans_npz("rans_channel.npz", K.rans_channel_dict(), rc.mesh.points)
 
