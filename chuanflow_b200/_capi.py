@@ -167,6 +167,20 @@ class PolyMesh:
         self._counts()
         return self
 
+    @classmethod
+    def read_gmsh(cls, path, patch_types=None):
+        """GmshMesh::fromFile: an ASCII .msh 2.2 / 4.x file; patch_types maps
+        physical-group names to boundary types (others "wall")."""
+        pt = patch_types or {}
+        names = (C.c_char_p * max(1, len(pt)))(*[k.encode() for k in pt])
+        types = (C.c_char_p * max(1, len(pt)))(*[v.encode() for v in pt.values()])
+        h = C.c_void_p()
+        _check(lib().cfg_mesh_read_gmsh(str(path).encode(), C.c_int32(len(pt)), names, types, C.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self._counts()
+        return self
+
     def _counts(self):
         c = np.zeros(5, np.int64)
         _check(lib().cfg_mesh_counts(self._h, _ip(c)))

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <string>
 
 #include "cfg_internal.h"
@@ -153,6 +155,19 @@ int cfg_mesh_from_cells(const double* points, int64_t nP, const int32_t* types, 
         for (int64_t v : cv) need(v >= 0 && v < nP, "cfg_mesh_from_cells: vertex index out of range");
         auto m = std::make_unique<cfg_mesh>();
         m->m = cfg::meshFromCells(pts, ty, off, cv);
+        *out = m.release();
+    });
+}
+
+int cfg_mesh_read_gmsh(const char* path, int32_t nTypes, const char* const* names, const char* const* types,
+                       cfg_mesh** out)
+{
+    return guard([&] {
+        need(path && out && (nTypes == 0 || (names && types)), "cfg_mesh_read_gmsh: null argument");
+        std::map<std::string, std::string> pt;
+        for (int32_t i = 0; i < nTypes; ++i) pt[names[i]] = types[i];
+        auto m = std::make_unique<cfg_mesh>();
+        m->m = cfg::readGmsh(path, pt);
         *out = m.release();
     });
 }
@@ -502,8 +517,49 @@ CaseSpec parseCase(const char* path)
 {
     const cfg::Dict d = cfg::Dict::parseFile(path);
     CaseSpec cs;
-    // mesh: block{} (BlockMesh::fromDict, blockMesh.cpp:191-223)
-    if (!d.has("block")) cfg::fail(CFG_ESETUP, "case: only block {} meshes are read from a case file");
+    // mesh: block{} (BlockMesh::fromDict, blockMesh.cpp:191-223) or mesh{} of a
+    // gmsh file (meshLoader.cpp:14-59)
+    const bool hasBlock = d.has("block"), hasFile = d.has("mesh");
+    if (hasBlock && hasFile) cfg::fail(CFG_ESETUP, "case: block {} and mesh {} are mutually exclusive");
+    if (!hasBlock && !hasFile) cfg::fail(CFG_ESETUP, "case: no mesh; add a block {} or a mesh {} section");
+    if (hasFile)
+    {
+        const cfg::Dict& md = d.dict("mesh");
+        const std::string format = md.wordOr("format", "gmsh");
+        if (format != "gmsh") cfg::fail(CFG_ESETUP, "mesh: format '" + format + "' is unknown (gmsh is supported)");
+        std::string file = md.word("file");
+        if (!file.empty() && file[0] != '/')
+        {
+            // a relative file not found from the working directory is looked
+            // up beside the case dictionary
+            std::FILE* probe = std::fopen(file.c_str(), "rb");
+            if (probe) std::fclose(probe);
+            else
+            {
+                const std::string dir(path);
+                const size_t slash = dir.find_last_of('/');
+                if (slash != std::string::npos)
+                {
+                    const std::string beside = dir.substr(0, slash + 1) + file;
+                    std::FILE* p2 = std::fopen(beside.c_str(), "rb");
+                    if (p2)
+                    {
+                        std::fclose(p2);
+                        file = beside;
+                    }
+                }
+            }
+        }
+        std::map<std::string, std::string> patchTypes;
+        if (md.has("patches"))
+        {
+            const cfg::Dict& ps = md.dict("patches");
+            for (const auto& name : ps.keys()) patchTypes[name] = ps.dict(name).wordOr("type", "wall");
+        }
+        cs.mesh = cfg::readGmsh(file, patchTypes);
+    }
+    else
+    {
     const cfg::Dict& b = d.dict("block");
     const auto mn = b.numbers("min"), mx = b.numbers("max"), nc = b.numbers("cells");
     if (mn.size() != 3 || mx.size() != 3 || nc.size() != 3)
@@ -520,6 +576,7 @@ CaseSpec parseCase(const char* path)
         }
     cs.mesh = cfg::blockMesh({mn[0], mn[1], mn[2]}, {mx[0], mx[1], mx[2]}, static_cast<int64_t>(nc[0]),
                              static_cast<int64_t>(nc[1]), static_cast<int64_t>(nc[2]), names, types);
+    }
     const cfg::Mesh& M = cs.mesh;
     const size_t nP = M.patches.size();
     // the fields' defaults: every patch zeroGradient (volFields.cpp:46-50)

@@ -4,7 +4,10 @@
 
 #include <cstdint>
 #include <stdexcept>
+#include <array>
+#include <map>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "chuanflow_b200.h"
@@ -73,6 +76,31 @@ struct Mesh
 /// bounding-box planes).
 Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& types,
                    const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts);
+
+/// sorted vertex key of a face (unused slots -1) -> physical-group name
+struct FaceKeyHash
+{
+    size_t operator()(const std::array<int64_t, 5>& k) const
+    {
+        uint64_t h = 1469598103934665603ULL;
+        for (int64_t v : k)
+        {
+            h ^= static_cast<uint64_t>(v) + 0x9E3779B97F4A7C15ULL;
+            h *= 1099511628211ULL;
+            h ^= h >> 31;
+        }
+        return static_cast<size_t>(h);
+    }
+};
+using SurfaceNames = std::unordered_map<std::array<int64_t, 5>, std::string, FaceKeyHash>;
+/// the same with boundary faces named by their surface element's physical
+/// group when there is one, and patch types from `patchTypes` (else "wall")
+Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& types,
+                   const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts,
+                   const SurfaceNames& surfaceNames, const std::map<std::string, std::string>& patchTypes);
+
+/// GmshMesh::fromFile (gmshMesh.cpp:534-776): ASCII .msh 2.2 or 4.x
+Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>& patchTypes);
 
 Mesh blockMesh(const Vec& mn, const Vec& mx, int64_t nx, int64_t ny, int64_t nz,
                const std::vector<std::string>& names, const std::vector<std::string>& types);

@@ -1,0 +1,459 @@
+// GmshMesh::fromFile (src/3d/src/mesh/gmshMesh.cpp:534-776): ASCII .msh 2.2
+// and 4.x with first-order tetrahedra, hexahedra and prisms; boundary faces
+// named by the physical groups of the surface elements (a quad face also by
+// one of its triangles), else by the bounding-box plane they lie on.
+//
+// The file is read into memory once and tokenised row by row in place
+// (string views, strtol/strtod), so a multi-million-element file parses at
+// memory speed instead of through one std::string per token.  The reading
+// rules follow the reference: the section layout and header checks, the
+// 4.x node blocks with or without tag lists, per-block element tags, node
+// tags renumbered densely in ascending order, and its error messages.
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <string_view>
+#include <unordered_map>
+#include <vector>
+
+#include "cfg_internal.h"
+
+namespace cfg
+{
+namespace
+{
+
+using Row = std::vector<std::string_view>;
+
+int nodesPerElement(int type)
+{
+    switch (type)
+    {
+    case 1: return 2;
+    case 2: return 3;
+    case 3: return 4;
+    case 4: return 4;
+    case 5: return 8;
+    case 6: return 6;
+    case 7: return 5;
+    default: return 0;
+    }
+}
+
+long toInt(std::string_view t, const char* where)
+{
+    std::string s(t);
+    char* end = nullptr;
+    errno = 0;
+    const long v = std::strtol(s.c_str(), &end, 10);
+    if (end == s.c_str() || errno) fail(CFG_EMESH, "gmsh: expected an integer but found '" + s + "' in " + where);
+    return v;
+}
+
+double toDouble(std::string_view t, const char* where)
+{
+    std::string s(t);
+    char* end = nullptr;
+    const double v = std::strtod(s.c_str(), &end);
+    if (end == s.c_str()) fail(CFG_EMESH, "gmsh: expected a number but found '" + s + "' in " + where);
+    return v;
+}
+
+bool isIntegerToken(std::string_view t) { return t.find_first_of(".eE") == std::string_view::npos; }
+
+/// the non-empty rows of one $Name ... $EndName section
+class Section
+{
+public:
+    Section() = default;
+    Section(std::vector<Row> rows, std::string where) : rows_(std::move(rows)), where_(std::move(where)) {}
+    bool found() const { return !rows_.empty(); }
+    bool atEnd() const { return pos_ >= rows_.size(); }
+    const Row& take()
+    {
+        if (atEnd())
+            fail(CFG_EMESH, "gmsh: truncated file: " + where_ + " ends after " + std::to_string(rows_.size()) + " rows");
+        return rows_[pos_++];
+    }
+    bool takeSingleInt(long& v)
+    {
+        if (atEnd() || rows_[pos_].size() != 1 || !isIntegerToken(rows_[pos_][0])) return false;
+        v = toInt(rows_[pos_][0], where_.c_str());
+        ++pos_;
+        return true;
+    }
+
+private:
+    std::vector<Row> rows_;
+    size_t pos_ = 0;
+    std::string where_;
+};
+
+struct File
+{
+    std::string text;
+    std::vector<std::pair<size_t, size_t>> lines;  // [begin, end) of every line
+
+    Row tokens(size_t li) const
+    {
+        Row r;
+        const char* s = text.data() + lines[li].first;
+        const char* e = text.data() + lines[li].second;
+        while (s < e)
+        {
+            while (s < e && (*s == ' ' || *s == '\t' || *s == '\r' || *s == '\v' || *s == '\f')) ++s;
+            const char* b = s;
+            while (s < e && !(*s == ' ' || *s == '\t' || *s == '\r' || *s == '\v' || *s == '\f')) ++s;
+            if (s > b) r.emplace_back(b, static_cast<size_t>(s - b));
+        }
+        return r;
+    }
+
+    std::string_view first(size_t li) const
+    {
+        const char* s = text.data() + lines[li].first;
+        const char* e = text.data() + lines[li].second;
+        while (s < e && std::isspace(static_cast<unsigned char>(*s))) ++s;
+        const char* b = s;
+        while (s < e && !std::isspace(static_cast<unsigned char>(*s))) ++s;
+        return std::string_view(b, static_cast<size_t>(s - b));
+    }
+
+    Section section(const std::string& name, const std::string& path, bool required) const
+    {
+        const std::string begin = "$" + name, end = "$End" + name;
+        for (size_t i = 0; i < lines.size(); ++i)
+        {
+            if (first(i) != begin) continue;
+            for (size_t j = i + 1; j < lines.size(); ++j)
+            {
+                if (first(j) != end) continue;
+                std::vector<Row> rows;
+                rows.reserve(j - i - 1);
+                for (size_t k = i + 1; k < j; ++k)
+                {
+                    Row t = tokens(k);
+                    if (!t.empty()) rows.push_back(std::move(t));
+                }
+                return Section(std::move(rows), begin + " in " + path);
+            }
+            fail(CFG_EMESH, "gmsh: section " + begin + " in " + path + " is not terminated");
+        }
+        if (required) fail(CFG_EMESH, "gmsh: " + path + " has no " + begin + " section");
+        return Section();
+    }
+};
+
+struct Element
+{
+    int type;
+    long physical;
+    std::vector<int64_t> nodes;
+};
+
+}  // namespace
+
+Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>& patchTypes)
+{
+    File f;
+    {
+        std::FILE* fp = std::fopen(path.c_str(), "rb");
+        if (!fp) fail(CFG_EMESH, "gmsh: cannot open " + path);
+        std::fseek(fp, 0, SEEK_END);
+        const long size = std::ftell(fp);
+        std::fseek(fp, 0, SEEK_SET);
+        f.text.resize(static_cast<size_t>(std::max(size, 0L)));
+        const size_t got = size > 0 ? std::fread(&f.text[0], 1, static_cast<size_t>(size), fp) : 0;
+        std::fclose(fp);
+        if (got != f.text.size()) fail(CFG_EMESH, "gmsh: cannot read " + path);
+        size_t b = 0;
+        for (size_t i = 0; i <= f.text.size(); ++i)
+            if (i == f.text.size() || f.text[i] == '\n')
+            {
+                if (i < f.text.size() || i > b) f.lines.push_back({b, i});
+                b = i + 1;
+            }
+    }
+
+    Section fmt = f.section("MeshFormat", path, true);
+    const Row& fv = fmt.take();
+    if (fv.size() < 2) fail(CFG_EMESH, "gmsh: malformed $MeshFormat in " + path);
+    const double version = toDouble(fv[0], "$MeshFormat");
+    if (toInt(fv[1], "$MeshFormat") != 0)
+        fail(CFG_EMESH, "gmsh: " + path + " is a binary .msh; write it with Mesh.Binary = 0");
+    if (!(std::abs(version - 2.2) < 1e-9 || version >= 4.0))
+        fail(CFG_EMESH, "gmsh: format '" + std::string(fv[0]) + "' is not supported (ASCII 2.2 and 4.1 are)");
+
+    // physical names of surfaces (dim 2)
+    std::map<long, std::string> physicalNames;
+    {
+        Section s = f.section("PhysicalNames", path, false);
+        if (s.found())
+        {
+            const long n = toInt(s.take()[0], "$PhysicalNames");
+            for (long i = 0; i < n; ++i)
+            {
+                const Row& t = s.take();
+                if (t.size() < 3) fail(CFG_EMESH, "gmsh: malformed $PhysicalNames entry");
+                const long dim = toInt(t[0], "$PhysicalNames");
+                const long tag = toInt(t[1], "$PhysicalNames");
+                std::string name;
+                for (size_t k = 2; k < t.size(); ++k) name += std::string(t[k]);
+                name.erase(std::remove(name.begin(), name.end(), '"'), name.end());
+                if (name.empty()) fail(CFG_EMESH, "gmsh: physical group " + std::to_string(tag) + " has no name");
+                if (dim == 2) physicalNames[tag] = name;
+            }
+        }
+    }
+
+    // nodes, renumbered densely in ascending tag order
+    std::vector<Vec> points;
+    std::unordered_map<long, int64_t> tagIndex;
+    {
+        Section sec = f.section("Nodes", path, true);
+        if (!sec.found()) fail(CFG_EMESH, "gmsh: " + path + " has an empty $Nodes section");
+        std::vector<std::pair<long, Vec>> rec;
+        long declared = 0;
+        auto coords = [&](const Row& t) {
+            if (t.size() < 3) fail(CFG_EMESH, "gmsh: malformed node coordinate in $Nodes");
+            return Vec{toDouble(t[0], "$Nodes"), toDouble(t[1], "$Nodes"), toDouble(t[2], "$Nodes")};
+        };
+        if (version < 3.0)
+        {
+            declared = toInt(sec.take()[0], "$Nodes");
+            rec.reserve(static_cast<size_t>(std::max(declared, 0L)));
+            for (long i = 0; i < declared; ++i)
+            {
+                const Row& t = sec.take();
+                if (t.size() < 4) fail(CFG_EMESH, "gmsh: malformed node line in " + path);
+                rec.push_back({toInt(t[0], "$Nodes"), Vec{toDouble(t[1], "$Nodes"), toDouble(t[2], "$Nodes"),
+                                                         toDouble(t[3], "$Nodes")}});
+            }
+        }
+        else
+        {
+            const Row h = sec.take();
+            if (h.size() < 4) fail(CFG_EMESH, "gmsh: malformed $Nodes header in " + path);
+            const long blocks = toInt(h[0], "$Nodes header");
+            declared = toInt(h[1], "$Nodes header");
+            const long firstTag = toInt(h[2], "$Nodes header");
+            for (long b = 0; b < blocks; ++b)
+            {
+                const Row bh = sec.take();
+                if (bh.size() < 4) fail(CFG_EMESH, "gmsh: malformed $Nodes block header in " + path);
+                const long num = toInt(bh[3], "$Nodes block");
+                if (num <= 0) continue;
+                const bool documented = bh.size() >= 6;
+                const long minTag = documented ? toInt(bh[4], "$Nodes block") : firstTag;
+                const long maxTag = documented ? toInt(bh[5], "$Nodes block") : firstTag;
+                std::vector<long> tags;
+                std::vector<Vec> xyz;
+                if (documented)
+                {
+                    for (long i = 0; i < num; ++i) xyz.push_back(coords(sec.take()));
+                    if (minTag != maxTag)
+                    {
+                        long v = 0;
+                        while (static_cast<long>(tags.size()) < num && sec.takeSingleInt(v)) tags.push_back(v);
+                    }
+                    if (tags.empty())
+                        for (long i = 0; i < num; ++i) tags.push_back(minTag + i);
+                }
+                else
+                {
+                    long v = 0;
+                    while (static_cast<long>(tags.size()) < num && sec.takeSingleInt(v)) tags.push_back(v);
+                    const bool tagged = static_cast<long>(tags.size()) == num;
+                    for (long i = 0; i < num; ++i) xyz.push_back(coords(sec.take()));
+                    if (!tagged) tags.assign(static_cast<size_t>(num), 0);
+                }
+                for (size_t i = 0; i < xyz.size(); ++i) rec.push_back({tags[i], xyz[i]});
+            }
+        }
+        if (static_cast<long>(rec.size()) != declared)
+            fail(CFG_EMESH, "gmsh: $Nodes declares " + std::to_string(declared) + " nodes, " +
+                                std::to_string(rec.size()) + " were read from " + path +
+                                " (unsupported node layout?)");
+        // untagged nodes take the smallest unused positive tags in file order
+        bool anyUntagged = false;
+        for (const auto& r : rec) anyUntagged = anyUntagged || r.first <= 0;
+        if (anyUntagged)
+        {
+            std::set<long> used;
+            for (const auto& r : rec)
+                if (r.first > 0) used.insert(r.first);
+            long cand = 1;
+            for (auto& r : rec)
+            {
+                if (r.first > 0) continue;
+                while (used.count(cand)) ++cand;
+                r.first = cand;
+                used.insert(cand);
+            }
+        }
+        std::stable_sort(rec.begin(), rec.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        points.reserve(rec.size());
+        tagIndex.reserve(rec.size());
+        for (const auto& r : rec)
+        {
+            if (!tagIndex.emplace(r.first, static_cast<int64_t>(points.size())).second)
+                fail(CFG_EMESH, "gmsh: duplicate node tag " + std::to_string(r.first) + " in " + path);
+            points.push_back(r.second);
+        }
+    }
+
+    // entity -> physical tag of surfaces (4.x)
+    std::map<long, long> entityPhysical;
+    if (version >= 3.0)
+    {
+        Section en = f.section("EntityNames", path, false);
+        if (en.found())
+        {
+            const long n = toInt(en.take()[0], "$EntityNames");
+            for (long i = 0; i < n; ++i)
+            {
+                const Row& t = en.take();
+                if (t.size() < 4) fail(CFG_EMESH, "gmsh: malformed $EntityNames entry");
+                if (toInt(t[0], "$EntityNames") == 2) entityPhysical[toInt(t[1], "$EntityNames")] = toInt(t[2], "$EntityNames");
+            }
+        }
+        Section es = f.section("Entities", path, false);
+        if (es.found())
+        {
+            const Row h = es.take();
+            if (h.size() < 4) fail(CFG_EMESH, "gmsh: malformed $Entities header");
+            for (int dim = 0; dim < 4; ++dim)
+            {
+                const long n = toInt(h[static_cast<size_t>(dim)], "$Entities");
+                for (long i = 0; i < n; ++i)
+                {
+                    const Row& t = es.take();
+                    if (dim != 2) continue;
+                    if (t.size() < 8) fail(CFG_EMESH, "gmsh: malformed $Entities surface line");
+                    const long tag = toInt(t[0], "$Entities");
+                    const long nPhys = toInt(t[7], "$Entities");
+                    if (nPhys > 0)
+                    {
+                        if (t.size() < 9) fail(CFG_EMESH, "gmsh: malformed $Entities surface line");
+                        entityPhysical[tag] = toInt(t[8], "$Entities");
+                    }
+                }
+            }
+        }
+    }
+
+    // elements: volumes into cells, surfaces into physical names
+    std::vector<int32_t> types;
+    std::vector<int64_t> offsets{0}, verts;
+    SurfaceNames surfaceNames;
+    {
+        Section sec = f.section("Elements", path, true);
+        if (!sec.found()) fail(CFG_EMESH, "gmsh: " + path + " has an empty $Elements section");
+        auto add = [&](int type, long physical, const Row& t, size_t first, int npn) {
+            int64_t nodes[8];
+            for (int k = 0; k < npn; ++k)
+            {
+                const long tag = toInt(t[first + static_cast<size_t>(k)], "$Elements");
+                const auto it = tagIndex.find(tag);
+                if (it == tagIndex.end())
+                    fail(CFG_EMESH, "gmsh: an element refers to node " + std::to_string(tag) +
+                                        ", which $Nodes does not define");
+                nodes[k] = it->second;
+            }
+            if (std::unique(nodes, nodes + npn) != nodes + npn)
+                fail(CFG_EMESH, "gmsh: element " + std::to_string(type) + " repeats a node");
+            if (type == 2 || type == 3)
+            {
+                const auto nit = physicalNames.find(physical);
+                if (nit == physicalNames.end()) return;
+                std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
+                for (int k = 0; k < npn; ++k) key[static_cast<size_t>(k)] = nodes[k];
+                std::sort(key.begin(), key.begin() + npn);
+                surfaceNames.emplace(key, nit->second);
+            }
+            else if (type == 4 || type == 5 || type == 6)
+            {
+                types.push_back(type);
+                verts.insert(verts.end(), nodes, nodes + npn);
+                offsets.push_back(static_cast<int64_t>(verts.size()));
+            }
+            else if (type == 7)
+            {
+                fail(CFG_EMESH, "gmsh: pyramid elements are not supported");
+            }
+        };
+        if (version < 3.0)
+        {
+            const long declared = toInt(sec.take()[0], "$Elements");
+            for (long i = 0; i < declared; ++i)
+            {
+                const Row& t = sec.take();
+                if (t.size() < 3) fail(CFG_EMESH, "gmsh: malformed element line in " + path);
+                const int type = static_cast<int>(toInt(t[1], "$Elements"));
+                const int npn = nodesPerElement(type);
+                if (npn <= 0)
+                    fail(CFG_EMESH, "gmsh: element type " + std::to_string(type) + " in " + path +
+                                        " is not a first-order element; mesh with Linear order");
+                const long nTags = toInt(t[2], "$Elements");
+                if (static_cast<long>(t.size()) < 3 + nTags + npn)
+                    fail(CFG_EMESH, "gmsh: truncated element line in " + path);
+                const long physical = nTags > 0 ? toInt(t[3], "$Elements") : 0;
+                add(type, physical, t, static_cast<size_t>(3 + nTags), npn);
+            }
+        }
+        else
+        {
+            const Row h = sec.take();
+            if (h.size() < 4) fail(CFG_EMESH, "gmsh: malformed $Elements header in " + path);
+            const long blocks = toInt(h[0], "$Elements header");
+            const long declared = toInt(h[1], "$Elements header");
+            long read = 0;
+            for (long b = 0; b < blocks; ++b)
+            {
+                const Row bh = sec.take();
+                if (bh.size() < 4) fail(CFG_EMESH, "gmsh: malformed $Elements block header in " + path);
+                const long entityTag = toInt(bh[1], "$Elements block");
+                const int type = static_cast<int>(toInt(bh[2], "$Elements block"));
+                const long num = toInt(bh[3], "$Elements block");
+                const int npn = nodesPerElement(type);
+                if (npn <= 0)
+                    fail(CFG_EMESH, "gmsh: element type " + std::to_string(type) + " in " + path +
+                                        " is not a first-order element; mesh with Linear order");
+                const auto pit = entityPhysical.find(entityTag);
+                const long physical = pit != entityPhysical.end() ? pit->second : 0;
+                bool tagged = false;
+                for (long i = 0; i < num; ++i, ++read)
+                {
+                    const Row& t = sec.take();
+                    const long width = static_cast<long>(t.size());
+                    if (i == 0)
+                    {
+                        if (width == npn + 1) tagged = true;
+                        else if (width != npn)
+                            fail(CFG_EMESH, "gmsh: element line with " + std::to_string(width) + " entries, expected " +
+                                                std::to_string(npn) + " or " + std::to_string(npn + 1));
+                    }
+                    else if (width != npn + (tagged ? 1 : 0))
+                    {
+                        fail(CFG_EMESH, "gmsh: inconsistent element line width in " + path);
+                    }
+                    add(type, physical, t, tagged ? 1 : 0, npn);
+                }
+            }
+            if (read != declared)
+                fail(CFG_EMESH, "gmsh: $Elements declares " + std::to_string(declared) + " elements, " +
+                                    std::to_string(read) + " were read from " + path +
+                                    " (unsupported element layout?)");
+        }
+    }
+    if (types.empty()) fail(CFG_EMESH, "gmsh: " + path + " has no volume elements");
+    return meshFromCells(points, types, offsets, verts, surfaceNames, patchTypes);
+}
+
+}  // namespace cfg

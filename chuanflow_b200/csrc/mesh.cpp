@@ -333,25 +333,17 @@ const std::vector<std::vector<int>>& faceRings(int type)
     }
 }
 
-struct FaceKeyHash
-{
-    size_t operator()(const std::array<int64_t, 5>& k) const
-    {
-        uint64_t h = 1469598103934665603ULL;
-        for (int64_t v : k)
-        {
-            h ^= static_cast<uint64_t>(v) + 0x9E3779B97F4A7C15ULL;
-            h *= 1099511628211ULL;
-            h ^= h >> 31;
-        }
-        return static_cast<size_t>(h);
-    }
-};
-
 }  // namespace
 
 Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& types,
                    const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts)
+{
+    return meshFromCells(points, types, cellOffsets, cellVerts, {}, {});
+}
+
+Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& types,
+                   const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts,
+                   const SurfaceNames& surfaceNames, const std::map<std::string, std::string>& patchTypes)
 {
     // faces registered cell by cell in each element's ring order and
     // deduplicated by their sorted vertices; the first registration keeps
@@ -421,11 +413,43 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
             }
         return -1;
     };
+    // the physical-group name of a boundary face: its own surface element,
+    // or for a quad face one of the triangles a triangulated surface split
+    // it into (gmshMesh.cpp:617-634)
+    auto nameOf = [&](const Ref& r) -> const std::string* {
+        std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
+        for (int64_t k = 0; k < r.nv; ++k) key[k] = ringVerts[r.v0 + k];
+        std::sort(key.begin(), key.begin() + r.nv);
+        auto it = surfaceNames.find(key);
+        if (it != surfaceNames.end()) return &it->second;
+        if (r.nv == 4)
+            for (int skip = 0; skip < 4; ++skip)
+            {
+                std::array<int64_t, 5> tri{-1, -1, -1, -1, -1};
+                int t = 0;
+                for (int k = 0; k < 4; ++k)
+                    if (k != skip) tri[t++] = ringVerts[r.v0 + k];
+                std::sort(tri.begin(), tri.begin() + 3);
+                auto jt = surfaceNames.find(tri);
+                if (jt != surfaceNames.end()) return &jt->second;
+            }
+        return nullptr;
+    };
     Mesh m;
     m.points = points;
-    std::vector<int> patchOfPlane(6, -1);
     std::vector<std::vector<size_t>> patchFaces;
     std::vector<size_t> internal;
+    auto patchIndex = [&](const std::string& name) {
+        for (size_t p = 0; p < m.patches.size(); ++p)
+            if (m.patches[p].name == name) return p;
+        Mesh::Patch p;
+        p.name = name;
+        const auto t = patchTypes.find(name);
+        p.type = t != patchTypes.end() ? t->second : "wall";
+        m.patches.push_back(p);
+        patchFaces.emplace_back();
+        return m.patches.size() - 1;
+    };
     for (size_t i = 0; i < refs.size(); ++i)
     {
         Ref& r = refs[i];
@@ -435,18 +459,20 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
             internal.push_back(i);
             continue;
         }
-        const int pl = planeOf(r);
-        if (pl < 0) fail(CFG_EMESH, "mesh: a boundary face lies on no bounding-box plane");
-        if (patchOfPlane[pl] < 0)
+        const std::string* named = surfaceNames.empty() ? nullptr : nameOf(r);
+        std::string name;
+        if (named)
         {
-            patchOfPlane[pl] = static_cast<int>(patchFaces.size());
-            patchFaces.emplace_back();
-            Mesh::Patch p;
-            p.name = planeNames[pl];
-            p.type = "wall";
-            m.patches.push_back(p);
+            name = *named;
         }
-        patchFaces[patchOfPlane[pl]].push_back(i);
+        else
+        {
+            const int pl = planeOf(r);
+            if (pl < 0)
+                fail(CFG_EMESH, "mesh: a boundary face belongs to no physical group and lies on no bounding-box plane");
+            name = planeNames[pl];
+        }
+        patchFaces[patchIndex(name)].push_back(i);
     }
     m.faceOffsets.push_back(0);
     auto addFace = [&](const Ref& r) {
@@ -461,7 +487,7 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
     }
     for (size_t pi = 0; pi < patchFaces.size(); ++pi)
     {
-        m.patches[pi].start = static_cast<int64_t>(m.owner.size());
+        m.patches[pi].start = static_cast<int64_t>(m.owner.size());  // in order of first appearance
         m.patches[pi].size = static_cast<int64_t>(patchFaces[pi].size());
         for (size_t i : patchFaces[pi]) addFace(refs[i]);
     }

@@ -155,6 +155,14 @@ int cfg_mesh_block(const double min[3], const double max[3], int64_t nx, int64_t
 int cfg_mesh_from_cells(const double* points, int64_t n_points, const int32_t* cell_types,
                         const int64_t* cell_offsets, const int64_t* cell_verts, int64_t n_cells, cfg_mesh** out);
 
+/* GmshMesh::fromFile (src/3d/include/cf/fvm/GmshMesh.h:11-37,
+ * src/3d/src/mesh/gmshMesh.cpp:534-776): an ASCII .msh 2.2 or 4.x file of
+ * first-order tetrahedra, hexahedra and prisms; boundary faces named by the
+ * physical groups of the surface elements (else by bounding-box plane);
+ * patch types from names[i] -> types[i] (others "wall"). */
+int cfg_mesh_read_gmsh(const char* path, int32_t n_types, const char* const* names, const char* const* types,
+                       cfg_mesh** out);
+
 /* polyMesh::movePoints (polyMesh.cpp:320-329): same topology, new points,
  * geometry recomputed. */
 int cfg_mesh_move_points(cfg_mesh* mesh, const double* points, int64_t n_points);

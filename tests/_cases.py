@@ -266,3 +266,66 @@ def piso_channel_dict(nx=16, ny=6, nz=6, dt=0.05, steps=4):
     """The jittered channel (nu 1e-3) stepped by the reference's PISO."""
     return channel_dict(nx, ny, nz, nu=1e-3, iters=1) + (
         f"piso {{ dt {dt!r}; correctors 2; nonOrthCorrectors 1; linearTol 1e-10; steps {steps}; }}\n")
+
+
+def hex_box_cells(n):
+    """An n^3 hex box in the unit cube as gmsh volume elements (0-based
+    nodes) plus its boundary quads grouped by side: (points, hexes, sides)."""
+    g = np.linspace(0.0, 1.0, n + 1)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    idx = lambda i, j, k: (i * (n + 1) + j) * (n + 1) + k
+    hexes = []
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                hexes.append([idx(i, j, k), idx(i + 1, j, k), idx(i + 1, j + 1, k), idx(i, j + 1, k),
+                              idx(i, j, k + 1), idx(i + 1, j, k + 1), idx(i + 1, j + 1, k + 1), idx(i, j + 1, k + 1)])
+    sides = {"xmin": [], "xmax": [], "ymin": [], "ymax": [], "zmin": [], "zmax": []}
+    for a in range(n):
+        for b in range(n):
+            sides["xmin"].append([idx(0, a, b), idx(0, a + 1, b), idx(0, a + 1, b + 1), idx(0, a, b + 1)])
+            sides["xmax"].append([idx(n, a, b), idx(n, a + 1, b), idx(n, a + 1, b + 1), idx(n, a, b + 1)])
+            sides["ymin"].append([idx(a, 0, b), idx(a + 1, 0, b), idx(a + 1, 0, b + 1), idx(a, 0, b + 1)])
+            sides["ymax"].append([idx(a, n, b), idx(a + 1, n, b), idx(a + 1, n, b + 1), idx(a, n, b + 1)])
+            sides["zmin"].append([idx(a, b, 0), idx(a + 1, b, 0), idx(a + 1, b + 1, 0), idx(a, b + 1, 0)])
+            sides["zmax"].append([idx(a, b, n), idx(a + 1, b, n), idx(a + 1, b + 1, n), idx(a, b + 1, n)])
+    return pts, np.array(hexes), sides
+
+
+def write_msh22_groups(path, points, hexes, groups):
+    """gmsh 2.2 ASCII with physical surface groups: groups = [(name, quads,
+    as_triangles)]; a group written as triangles splits each quad in two."""
+    lines = []
+    for g, (name, quads, tri) in enumerate(groups):
+        for q in quads:
+            if tri:
+                lines.append((2, g + 1, [q[0], q[1], q[2]]))
+                lines.append((2, g + 1, [q[0], q[2], q[3]]))
+            else:
+                lines.append((3, g + 1, list(q)))
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$PhysicalNames\n%d\n" % (len(groups) + 1))
+        for g, (name, _, _) in enumerate(groups):
+            f.write('2 %d "%s"\n' % (g + 1, name))
+        f.write('3 %d "fluid"\n$EndPhysicalNames\n$Nodes\n%d\n' % (len(groups) + 1, len(points)))
+        for i, p in enumerate(points):
+            f.write("%d %.17g %.17g %.17g\n" % (i + 1, p[0], p[1], p[2]))
+        f.write("$EndNodes\n$Elements\n%d\n" % (len(lines) + len(hexes)))
+        e = 0
+        for t, g, nodes in lines:
+            e += 1
+            f.write("%d %d 2 %d %d %s\n" % (e, t, g, g, " ".join(str(int(v) + 1) for v in nodes)))
+        for c in hexes:
+            e += 1
+            f.write("%d 5 2 %d %d %s\n" % (e, len(groups) + 1, len(groups) + 1, " ".join(str(int(v) + 1) for v in c)))
+        f.write("$EndElements\n")
+
+
+def grouped_box_file(path, n=3):
+    """The 3^3 box with physical groups: inlet (xmin, quads), outlet (xmax,
+    triangles), walls (y and z sides, quads)."""
+    pts, hexes, sides = hex_box_cells(n)
+    groups = [("inlet", sides["xmin"], False), ("outlet", sides["xmax"], True),
+              ("walls", sides["ymin"] + sides["ymax"] + sides["zmin"] + sides["zmax"], False)]
+    write_msh22_groups(path, pts, hexes, groups)

@@ -10,6 +10,8 @@ Fixtures (small .npz files):
                            through its gmsh reader: addressing, geometry, weights,
                            and fvc::grad of its two test fields under all schemes
   mesh_hex41.npz           the orthogonal hex cube (tests/meshes/cubeHex_41.msh), same
+  mesh_groups.npz          a 3^3 hex box with physical surface groups (one written as triangles),
+                           read by the reference's gmsh reader with patch types from the case
   mesh_delaunay.npz        a seeded Delaunay tetrahedralisation (chuanflow_b200.meshgen) written
                            as gmsh 2.2 and read by the reference's gmsh reader
   simple_cavity.npz        jittered 6x5x4 lid-driven cavity: 3 SIMPLE iterations
@@ -191,6 +193,12 @@ def main():
     d["tets"] = tets
     d["lattice_points"] = pts
     np.savez_compressed(os.path.join(HERE, "mesh_delaunay.npz"), **d)
+
+    with tempfile.TemporaryDirectory() as td:
+        mp = os.path.join(td, "box.msh")
+        K.grouped_box_file(mp)
+        mesh_npz("mesh_groups.npz", f'mesh {{ format gmsh; file "{mp}"; patches {{ inlet {{ type inlet; }} '
+                                    f'outlet {{ type outlet; }} }} }}\n')
 
     cav = K.cavity_case(6, 5, 4)
     simple_npz("simple_cavity.npz", cav, K.cavity_dict(6, 5, 4, iters=3), cav.mesh.points)

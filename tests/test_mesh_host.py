@@ -2,6 +2,8 @@
 blockMesh addressing, geometry, weights and the interior jitter, bit-for-bit
 against the reference (fixtures) and the oracle, plus the reference's mesh
 errors.  CPU only."""
+import os
+
 import numpy as np
 import pytest
 
@@ -168,3 +170,59 @@ def test_rcm_reduces_bandwidth_of_shuffled_mesh(golden):
     inv = np.empty(n, np.int64)
     inv[perm] = np.arange(n)
     assert np.abs(inv[own] - inv[nbr]).max() < np.abs(own - nbr).max()
+
+
+REF_MESHES = "/root/reference/tests/meshes"
+
+
+def check_fixture(m, g):
+    a = m.addressing()
+    for k in ("face_offsets", "face_verts", "owner", "neighbour", "points"):
+        assert np.array_equal(a[k], g[k]), k
+    geo = m.geometry()
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(geo[k], g[k]), k
+    pats = [(str(n), str(t), int(s), int(z)) for n, t, s, z in
+            zip(g["patch_names"], g["patch_types"], g["patch_start"], g["patch_size"])]
+    assert m.patches == pats
+
+
+def test_read_gmsh_physical_groups_match_reference(golden, tmp_path):
+    """Physical surface groups (one written as triangles over quad faces)
+    and patch types, against the reference's GmshMesh::fromFile."""
+    p = tmp_path / "box.msh"
+    K.grouped_box_file(str(p))
+    m = cf.PolyMesh.read_gmsh(p, {"inlet": "inlet", "outlet": "outlet"})
+    check_fixture(m, golden("mesh_groups.npz"))
+
+
+def test_read_gmsh_delaunay_matches_reference(golden, tmp_path):
+    g = golden("mesh_delaunay.npz")
+    p = tmp_path / "d.msh"
+    K.write_msh22(str(p), g["lattice_points"], g["tets"])
+    check_fixture(cf.PolyMesh.read_gmsh(p), g)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_MESHES), reason="the reference's test meshes are not present")
+@pytest.mark.parametrize("name,fixture", [("cubeTets_22.msh", "mesh_tets22.npz"), ("cubeHex_41.msh", "mesh_hex41.npz")])
+def test_read_gmsh_reference_test_meshes(golden, name, fixture):
+    """The reference's own .msh test files (formats 2.2 and 4.1), read here
+    where they are present, against its reader's output."""
+    check_fixture(cf.PolyMesh.read_gmsh(os.path.join(REF_MESHES, name)), golden(fixture))
+
+
+def test_read_gmsh_errors(tmp_path):
+    with pytest.raises(cf.CfgError, match="cannot open"):
+        cf.PolyMesh.read_gmsh(tmp_path / "missing.msh")
+    p = tmp_path / "bin.msh"
+    p.write_text("$MeshFormat\n2.2 1 8\n$EndMeshFormat\n")
+    with pytest.raises(cf.CfgError, match="binary"):
+        cf.PolyMesh.read_gmsh(p)
+    p.write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n5\n1 0 0 0\n2 1 0 0\n3 0 1 0\n4 0 0 1\n5 1 1 1\n"
+                 "$EndNodes\n$Elements\n1\n1 7 2 1 1 1 2 3 4 5\n$EndElements\n")
+    with pytest.raises(cf.CfgError, match="pyramid"):
+        cf.PolyMesh.read_gmsh(p)
+    p.write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n1\n1 0 0 0\n$EndNodes\n$Elements\n1\n"
+                 "1 4 2 1 1 1 2 3 4\n$EndElements\n")
+    with pytest.raises(cf.CfgError, match="node 2"):
+        cf.PolyMesh.read_gmsh(p)
