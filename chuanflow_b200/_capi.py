@@ -181,6 +181,18 @@ class PolyMesh:
         self._counts()
         return self
 
+    def write_vtu(self, path, fields=None, binary=True):
+        """VtkWriter: cell fields {name: array (n) or (n, 3)}; binary=False
+        writes the reference's ASCII file."""
+        fields = fields or {}
+        arrs = [np.ascontiguousarray(v, np.float64) for v in fields.values()]
+        n = len(arrs)
+        names = (C.c_char_p * max(1, n))(*[k.encode() for k in fields])
+        comps = (C.c_int32 * max(1, n))(*[1 if a.ndim == 1 else 3 for a in arrs])
+        ptrs = (C.POINTER(C.c_double) * max(1, n))(*[_dp(a) for a in arrs])
+        _check(lib().cfg_mesh_write_vtu(self._h, str(path).encode(), C.c_int32(n), names, comps, ptrs,
+                                        C.c_int32(int(binary))))
+
     def _counts(self):
         c = np.zeros(5, np.int64)
         _check(lib().cfg_mesh_counts(self._h, _ip(c)))
@@ -660,6 +672,12 @@ def _piso_step(self, controls):
     return {k: getattr(r, k) for k, _ in r._fields_}
 
 
+def _write_vtu(self, path, binary=True):
+    """The case's fields (p, k/epsilon/nut with a RANS model, U) as .vtu."""
+    _check(lib().cfg_write_vtu(self._h, str(path).encode(), C.c_int32(int(binary))))
+
+
+SimpleCase.write_vtu = _write_vtu
 SimpleCase.piso_step = _piso_step
 SimpleCase.mpnn_create = _mpnn_create
 SimpleCase.mpnn_weights = _mpnn_weights

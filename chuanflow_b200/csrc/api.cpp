@@ -960,3 +960,42 @@ int cfg_piso_step(cfg_ctx* ctx, const cfg_piso_controls* controls, cfg_piso_resu
         ctx->c->pisoStep(*controls, *result);
     });
 }
+
+// ---- VTK output ----
+
+int cfg_write_vtu(cfg_ctx* ctx, const char* path, int32_t binary)
+{
+    return guard([&] {
+        need(ctx && path, "cfg_write_vtu: null argument");
+        cfg::Ctx& c = *ctx->c;
+        const cfg::Mesh& M = c.mesh();
+        const size_t nC = static_cast<size_t>(M.nCells);
+        std::vector<cfg::VtuField> f;
+        f.push_back({"p", 1, std::vector<double>(nC)});
+        f.push_back({"U", 3, std::vector<double>(3 * nC)});
+        c.download(f[1].data.data(), f[0].data.data(), nullptr);
+        if (c.hasTurbulence())
+        {
+            f.insert(f.begin() + 1, {{"k", 1, std::vector<double>(nC)}, {"epsilon", 1, std::vector<double>(nC)},
+                                     {"nut", 1, std::vector<double>(nC)}});
+            c.turbulenceFields(f[1].data.data(), f[2].data.data(), f[3].data.data(), nullptr);
+        }
+        cfg::writeVtu(M, path, f, binary != 0);
+    });
+}
+
+int cfg_mesh_write_vtu(const cfg_mesh* mesh, const char* path, int32_t n_fields, const char* const* names,
+                       const int32_t* n_comp, const double* const* data, int32_t binary)
+{
+    return guard([&] {
+        need(mesh && path && (n_fields == 0 || (names && n_comp && data)), "cfg_mesh_write_vtu: null argument");
+        const size_t nC = static_cast<size_t>(mesh->m.nCells);
+        std::vector<cfg::VtuField> f;
+        for (int32_t i = 0; i < n_fields; ++i)
+        {
+            need(n_comp[i] == 1 || n_comp[i] == 3, "cfg_mesh_write_vtu: fields have 1 or 3 components");
+            f.push_back({names[i], n_comp[i], std::vector<double>(data[i], data[i] + nC * n_comp[i])});
+        }
+        cfg::writeVtu(mesh->m, path, f, binary != 0);
+    });
+}

@@ -99,6 +99,17 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
                    const std::vector<int64_t>& cellOffsets, const std::vector<int64_t>& cellVerts,
                    const SurfaceNames& surfaceNames, const std::map<std::string, std::string>& patchTypes);
 
+/// a cell field for writeVtu: nComp 1 or 3, cell-major, original order
+struct VtuField
+{
+    std::string name;
+    int nComp;
+    std::vector<double> data;
+};
+/// VtkWriter::write (vtkWrite.cpp:33-131): scalars then vectors, each in the
+/// order given; binary = raw appended arrays instead of ASCII
+void writeVtu(const Mesh& M, const std::string& path, const std::vector<VtuField>& fields, bool binary);
+
 /// GmshMesh::fromFile (gmshMesh.cpp:534-776): ASCII .msh 2.2 or 4.x
 Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>& patchTypes);
 

@@ -398,6 +398,19 @@ int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* resul
  * of the mesh counts, every patch's U/p conditions, schemes and controls. */
 int cfg_case_inspect(const char* path, char* out, size_t size);
 
+/* ---- output ----------------------------------------------------------------- */
+
+/* VtkWriter (src/3d/include/cf/fvm/VtkWriter.h, src/3d/src/io/vtkWrite.cpp:33-131):
+ * a .vtu of the mesh, every cell a polyhedron, with cell fields -- the
+ * scalars in the order given, then the vectors.  binary = 0 writes the
+ * reference's ASCII file byte for byte; 1 writes the same arrays raw in an
+ * appended block (plus the polyhedron face offsets). */
+int cfg_mesh_write_vtu(const cfg_mesh* mesh, const char* path, int32_t n_fields, const char* const* names,
+                       const int32_t* n_comp, const double* const* data, int32_t binary);
+/* the context's fields (original order): p, then k, epsilon, nut when a RANS
+ * model is set up, then U */
+int cfg_write_vtu(cfg_ctx* ctx, const char* path, int32_t binary);
+
 /* ---- RANS turbulence -------------------------------------------------------- */
 
 /* RansModel::create + KEpsilon (src/3d/src/turbulence/turbulenceModel.cpp,

@@ -14,6 +14,7 @@
 //   simple <case.dict> <out> [points|-] [statedir]    solveIncompressibleSimple
 //   rans   <case.dict> <out> [points|-]               the same with the case's RANS model
 //   piso   <case.dict> <out> [points|-]               transient PISO steps (piso{} block)
+//   vtk    <case.dict> <out.vtu> <points|-> <p.f64> <U.f64>   VtkWriter
 //   eqns   <case.dict> <out> <points|-> <statedir>    UEqn / pEqn assembly probes
 //   solve  <out> <n> <trip.i64> <tripv.f64> <diag.f64> <b.f64> <x0.f64> <cg|bicgstab> <tol> <maxIter>
 //
@@ -39,6 +40,7 @@
 #include "cf/fvm/PressureCorrection.h"
 #include "cf/fvm/PisoSolver.h"
 #include "cf/fvm/SimpleSolver.h"
+#include "cf/fvm/VtkWriter.h"
 #include "cf/turbulence/TurbulenceModel.h"
 
 // Built as cf_adapter_driver, the simple mode runs the same case through the
@@ -310,6 +312,24 @@ int modePiso(int argc, char** argv)
     return 0;
 }
 
+/// VtkWriter on the case's mesh with cell fields p (scalar) and U (vector)
+/// read from raw FP64 files
+int modeVtk(int argc, char** argv)
+{
+    const Dictionary caseDict = Dictionary::parseFile(argv[2]);
+    polyMesh mesh = loadMesh(caseDict, argv[2], argv[4]);
+    const auto pv = readRaw<double>(argv[5]);
+    const auto uv = readRaw<double>(argv[6]);
+    Field<scalar> p(pv.begin(), pv.end());
+    Field<Vector> U(static_cast<std::size_t>(mesh.nCells()));
+    for (std::size_t c = 0; c < U.size(); ++c) U[c] = Vector{uv[3 * c], uv[3 * c + 1], uv[3 * c + 2]};
+    VtkWriter w(mesh);
+    w.addCellScalar("p", p);
+    w.addCellVector("U", U);
+    w.write(argv[3]);
+    return 0;
+}
+
 int modeSimple(int argc, char** argv)
 {
     const Dictionary caseDict = Dictionary::parseFile(argv[2]);
@@ -477,6 +497,7 @@ int main(int argc, char** argv)
         if (mode == "simple" && argc >= 4) return modeSimple(argc, argv);
         if (mode == "rans" && argc >= 4) return modeRans(argc, argv);
         if (mode == "piso" && argc >= 4) return modePiso(argc, argv);
+        if (mode == "vtk" && argc >= 7) return modeVtk(argc, argv);
         if (mode == "eqns" && argc >= 6) return modeEqns(argc, argv);
         if (mode == "solve" && argc >= 12) return modeSolve(argc, argv);
         std::cerr << "cf_ref_driver: bad arguments for mode " << mode << "\n";

@@ -19,6 +19,8 @@ Fixtures (small .npz files):
   eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
   solve_cg.npz, solve_bicgstab.npz   one CSR solve each
   piso_channel.npz         16x6x6 jittered channel: 4 transient PISO steps (dt 0.05, 2 correctors)
+  vtk_cavity.npz           the reference's VtkWriter output (ASCII .vtu) of a jittered 3x3x2 cavity
+                           with random p and U
   rans_channel.npz         12x5x5 orthogonal channel at Re_H 2e4 with the reference's k-epsilon:
                            5 SIMPLE iterations (U, p, phi, k, epsilon, nut, nu + nut on faces)
 """
@@ -151,6 +153,25 @@ def piso_npz(name, text, points):
         print("wrote", name, steps[-1])
 
 
+def vtk_npz(name, case_text, points, p, U):
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(case_text)
+        pp = os.path.join(td, "points.f64")
+        if points is None:
+            pp = "-"
+        else:
+            np.ascontiguousarray(points).tofile(pp)
+        np.ascontiguousarray(p).tofile(os.path.join(td, "p.f64"))
+        np.ascontiguousarray(U).tofile(os.path.join(td, "U.f64"))
+        out = os.path.join(td, "out.vtu")
+        O.ref_run(["vtk", cp, out, pp, os.path.join(td, "p.f64"), os.path.join(td, "U.f64")])
+        data = np.frombuffer(open(out, "rb").read(), np.uint8)
+        np.savez_compressed(os.path.join(HERE, name), text=data, p=p, U=U,
+                            points=np.zeros((0, 3)) if points is None else points, dict=np.array(case_text))
+        print("wrote", name, data.size, "bytes")
+
+
 def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
     n = rs.size - 1
     rows = np.repeat(np.arange(n), np.diff(rs))
@@ -199,6 +220,11 @@ def main():
         K.grouped_box_file(mp)
         mesh_npz("mesh_groups.npz", f'mesh {{ format gmsh; file "{mp}"; patches {{ inlet {{ type inlet; }} '
                                     f'outlet {{ type outlet; }} }} }}\n')
+
+    vc = K.cavity_case(3, 3, 2)
+    rv = np.random.default_rng(4)
+    vtk_npz("vtk_cavity.npz", K.cavity_dict(3, 3, 2), vc.mesh.points, rv.normal(size=vc.mesh.nC),
+            rv.normal(size=(vc.mesh.nC, 3)))
 
     cav = K.cavity_case(6, 5, 4)
     simple_npz("simple_cavity.npz", cav, K.cavity_dict(6, 5, 4, iters=3), cav.mesh.points)

@@ -48,3 +48,26 @@ def test_turbulence_setup_errors():
     case.turbulence_setup("laminar")
     with pytest.raises(cf.CfgError, match="no turbulence"):
         case.turbulence_fields()
+
+
+def test_case_vtu_carries_the_device_fields(tmp_path):
+    """cfg_write_vtu of a k-epsilon case: p, k, epsilon, nut and U as the
+    device holds them (binary arrays read back)."""
+    import re
+    mesh, case = K.rans_channel_product(8, 4, 4)
+    import chuanflow_b200 as cf
+    case.solve(cf.SimpleControls(max_iterations=2, relax_u=0.9, relax_p=0.03, p_relax_start=0.02,
+                                 non_orth_correctors=1, linear_tol=1e-8, nu=2.5e-6))
+    out = tmp_path / "c.vtu"
+    case.write_vtu(out, binary=True)
+    head, data = out.read_bytes().split(b'<AppendedData encoding="raw">\n_', 1)
+    got = {}
+    for mt in re.finditer(rb'<DataArray type="Float64" Name="(\w+)"[^>]*offset="(\d+)"', head):
+        off = int(mt.group(2))
+        n = int(np.frombuffer(data[off:off + 8], np.uint64)[0])
+        got[mt.group(1).decode()] = np.frombuffer(data[off + 8:off + 8 + n], np.float64)
+    U, p, _ = case.download()
+    t = case.turbulence_fields()
+    assert list(got) == ["p", "k", "epsilon", "nut", "U"]
+    assert np.array_equal(got["p"], p) and np.array_equal(got["U"].reshape(-1, 3), U)
+    assert np.array_equal(got["k"], t["k"]) and np.array_equal(got["nut"], t["nut"])

@@ -226,3 +226,41 @@ def test_read_gmsh_errors(tmp_path):
                  "1 4 2 1 1 1 2 3 4\n$EndElements\n")
     with pytest.raises(cf.CfgError, match="node 2"):
         cf.PolyMesh.read_gmsh(p)
+
+
+def test_vtu_ascii_is_the_reference_writers_file(golden, tmp_path):
+    """VtkWriter's ASCII .vtu (polyhedra, face stream, p and U), byte for byte."""
+    g = golden("vtk_cavity.npz")
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (3, 3, 2), {s: (n, "wall") for s, n in zip(K.SIDES, K.CAVITY_NAMES)})
+    m.jitter_interior(0.1, 7)
+    assert np.array_equal(m.addressing()["points"], g["points"])
+    out = tmp_path / "a.vtu"
+    m.write_vtu(out, {"p": g["p"], "U": g["U"]}, binary=False)
+    assert out.read_bytes() == g["text"].tobytes()
+
+
+def test_vtu_binary_holds_the_same_arrays(golden, tmp_path):
+    """The appended binary form: the same points, connectivity, offsets,
+    face stream and fields, read back raw."""
+    g = golden("vtk_cavity.npz")
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (3, 3, 2), {s: (n, "wall") for s, n in zip(K.SIDES, K.CAVITY_NAMES)})
+    m.jitter_interior(0.1, 7)
+    out = tmp_path / "b.vtu"
+    m.write_vtu(out, {"p": g["p"], "U": g["U"]}, binary=True)
+    raw = out.read_bytes()
+    head, data = raw.split(b'<AppendedData encoding="raw">\n_', 1)
+    import re
+    arrays = {}
+    for mt in re.finditer(rb'<DataArray type="(\w+)"(?: Name="(\w+)")?[^>]*offset="(\d+)"', head):
+        typ, name, off = mt.group(1).decode(), (mt.group(2) or b"points").decode(), int(mt.group(3))
+        nbytes = int(np.frombuffer(data[off:off + 8], np.uint64)[0])
+        dt = {"Float64": np.float64, "Int64": np.int64, "UInt8": np.uint8}[typ]
+        arrays[name] = np.frombuffer(data[off + 8:off + 8 + nbytes], dt)
+    assert np.array_equal(arrays["points"].reshape(-1, 3), g["points"])
+    assert np.array_equal(arrays["p"], g["p"]) and np.array_equal(arrays["U"].reshape(-1, 3), g["U"])
+    text = g["text"].tobytes().decode()
+    conn = re.search(r'Name="connectivity" format="ascii">\n(.*?)</DataArray>', text, re.S).group(1).split()
+    assert np.array_equal(arrays["connectivity"], np.array(conn, np.int64))
+    faces = re.search(r'Name="faces" format="ascii">\n(.*?)</DataArray>', text, re.S).group(1).split()
+    assert np.array_equal(arrays["faces"], np.array(faces, np.int64))
+    assert np.all(arrays["types"] == 42) and arrays["types"].size == m.n_cells
