@@ -19,6 +19,10 @@ Fixtures (small .npz files):
   eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
   solve_cg.npz, solve_bicgstab.npz   one CSR solve each
   piso_channel.npz         16x6x6 jittered channel: 4 transient PISO steps (dt 0.05, 2 correctors)
+  simple_channel40.npz     the 16,000-cell channel: 20 reference iterations, and 20 with linear-upwind,
+                           Gauss linear and DIC-PCG by the C restatement (checksums, samples)
+  simple_cavity128.npz     the 2M-cell bench cavity (pinned, so by the C restatement): checksums and
+                           4096 seeded cell/face samples after one outer iteration
   vtk_cavity.npz           the reference's VtkWriter output (ASCII .vtu) of a jittered 3x3x2 cavity
                            with random p and U
   rans_channel.npz         12x5x5 orthogonal channel at Re_H 2e4 with the reference's k-epsilon:
@@ -172,6 +176,63 @@ def vtk_npz(name, case_text, points, p, U):
         print("wrote", name, data.size, "bytes")
 
 
+def cavity128_npz(name, n=128, iters=1):
+    """The 2M-cell jittered cavity of bench.py (pressure reference cell 0,
+    which the reference lacks, so the oracle's C restatement runs it): the
+    scalar results, field checksums and 4096 seeded cell and face samples
+    after `iters` outer iterations from rest."""
+    m = K._block((0, 0, 0), (1, 1, 1), (n, n, n), K.CAVITY_NAMES, ["wall"] * 6, 0.1, 7)
+    case = O.Case(m, u_type=["fixedValue"] * 6,
+                  u_value=[(1.0, 0, 0) if nm == "lid" else (0, 0, 0) for nm in m.patch_names],
+                  p_type=["zeroGradient"] * 6, p_value=[0] * 6, nu=1.0 / 400.0, max_iterations=iters,
+                  linear_tol=1e-8, non_orth=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02)
+    case.p_ref_cell = 0
+    U, p, phi, r = case.run()
+    rng = np.random.default_rng(2024)
+    cells = np.sort(rng.choice(m.nC, 4096, replace=False))
+    faces = np.sort(rng.choice(m.nF, 4096, replace=False))
+    np.savez_compressed(os.path.join(HERE, name), n=n, iters=iters, iterations=r.iterations,
+                        continuity=r.finalContinuityError, momentum=r.finalMomentumResidual,
+                        u_inner=r.uItersTotal, p_inner=r.pItersTotal, U_sum=U.sum(0), p_sum=p.sum(),
+                        phi_abs_sum=np.abs(phi).sum(), cells=cells, faces=faces, U_cells=U[cells],
+                        p_cells=p[cells], phi_faces=phi[faces], points_sum=m.points.sum(0))
+    print("wrote", name, r.iterations, r.uItersTotal, r.pItersTotal)
+
+
+def channel40_npz(name, iters=20):
+    """The 40x20x20 channel (2 x 0.1 x 0.1 m, inlet 0.1 m/s, nu 1e-4, the
+    reference's stable relaxation 0.9 / 0.03 / pRelaxStart 0.02, nonOrth 2):
+    the reference's own run, checksums and seeded samples; and the same case
+    with linear-upwind convection, Gauss linear gradients and DIC-PCG by the
+    C restatement (no reference counterpart)."""
+    text = K.channel_dict(40, 20, 20, nu=1e-4, iters=iters, L=(2.0, 0.1, 0.1))
+    m = K._block((0, 0, 0), (2.0, 0.1, 0.1), (40, 20, 20), K.CHANNEL_NAMES, K.CHANNEL_TYPES, 0.0, 0)
+    rng = np.random.default_rng(40)
+    cells = np.sort(rng.choice(m.nC, 2048, replace=False))
+    faces = np.sort(rng.choice(m.nF, 2048, replace=False))
+    out = {"cells": cells, "faces": faces, "iters": iters}
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(text)
+        O.ref_run(["simple", cp, td])
+        res = open(os.path.join(td, "result.txt")).read().split()
+        U = O.read(os.path.join(td, "U.f64"), shape=(-1, 3))
+        p = O.read(os.path.join(td, "p.f64"))
+        phi = O.read(os.path.join(td, "phi.f64"))
+    out.update(ref_iterations=int(res[0]), ref_continuity=float(res[1]), ref_U_sum=U.sum(0), ref_p_sum=p.sum(),
+               ref_U_cells=U[cells], ref_p_cells=p[cells], ref_phi_faces=phi[faces])
+    c = O.Case(m, u_type=["fixedValue", "zeroGradient"] + ["fixedValue"] * 4,
+               u_value=[(0.1, 0, 0)] + [(0, 0, 0)] * 5, p_type=["zeroGradient", "fixedValue"] + ["zeroGradient"] * 4,
+               p_value=[0] * 6, nu=1e-4, max_iterations=iters, linear_tol=1e-8, non_orth=2, relax_u=0.7,
+               relax_p=0.3, p_relax_start=0.02, div="linearUpwind", grad="linear")
+    c.p_precond = 1
+    U, p, phi, r = c.run()
+    out.update(lu_iterations=r.iterations, lu_continuity=r.finalContinuityError, lu_U_sum=U.sum(0),
+               lu_p_sum=p.sum(), lu_U_cells=U[cells], lu_p_cells=p[cells], lu_phi_faces=phi[faces])
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print("wrote", name, res[:2], r.iterations)
+
+
 def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
     n = rs.size - 1
     rows = np.repeat(np.arange(n), np.diff(rs))
@@ -220,6 +281,9 @@ def main():
         K.grouped_box_file(mp)
         mesh_npz("mesh_groups.npz", f'mesh {{ format gmsh; file "{mp}"; patches {{ inlet {{ type inlet; }} '
                                     f'outlet {{ type outlet; }} }} }}\n')
+
+    channel40_npz("simple_channel40.npz")
+    cavity128_npz("simple_cavity128.npz")
 
     vc = K.cavity_case(3, 3, 2)
     rv = np.random.default_rng(4)

@@ -166,3 +166,80 @@ def test_poisson_solves_match_oracle(method, order):
     rs, cols, vals = oc.pressure_csr(np.ones(mesh.n_faces))
     x0, r0 = O.solve("cg", rs, cols, vals, b, np.zeros(mesh.n_cells), 1e-15, 20000)
     assert rel(x, x0) < 1e-7, rel(x, x0)
+
+
+def test_full_size_cavity_matches_oracle_checksums(golden):
+    """The 2M-cell jittered cavity of bench.py (128^3, pressure reference cell
+    0) after one outer iteration from rest, against the C restatement's run
+    (the reference itself has no reference cell): inner iteration counts,
+    continuity, field checksums and 4096 seeded cell and face samples."""
+    import bench
+    g = golden("simple_cavity128.npz")
+    mesh, case, ctl = bench.make_case(int(g["n"]), 0, "Jacobi")
+    assert np.array_equal(mesh.addressing()["points"].sum(0), g["points_sum"])
+    ctl.max_iterations = int(g["iters"])
+    r = case.solve(ctl)
+    U, p, phi = case.download()
+    assert r.iterations == int(g["iterations"])
+    assert abs(r.final_continuity_error - float(g["continuity"])) <= 1e-6 * abs(float(g["continuity"]))
+    # checksums relative to the sums of magnitudes (the recirculating flow's
+    # signed sums nearly cancel)
+    assert np.all(np.abs(U.sum(0) - g["U_sum"]) <= REL_TOL * np.abs(U).sum(0))
+    assert abs(p.sum() - g["p_sum"]) <= REL_TOL * np.abs(p).sum()
+    assert abs(np.abs(phi).sum() - g["phi_abs_sum"]) <= REL_TOL * g["phi_abs_sum"]
+    assert rel(U[g["cells"]], g["U_cells"]) < REL_TOL
+    assert rel(p[g["cells"]], g["p_cells"]) < REL_TOL
+    assert rel(phi[g["faces"]], g["phi_faces"]) < REL_TOL
+    # the inner counts: the solves stop where a 2M-term dot product crosses
+    # the tolerance, so a different summation order moves them a little
+    assert abs(r.u_inner_iterations - int(g["u_inner"])) <= 0.1 * int(g["u_inner"])
+    assert abs(r.p_inner_iterations - int(g["p_inner"])) <= 0.1 * int(g["p_inner"])
+
+
+def channel40_product(schemes=None):
+    import chuanflow_b200 as cf
+    mesh = cf.PolyMesh.block((0, 0, 0), (2.0, 0.1, 0.1), (40, 20, 20),
+                             {s: (n, t) for s, n, t in zip(K.SIDES, K.CHANNEL_NAMES, K.CHANNEL_TYPES)})
+    case = cf.SimpleCase(mesh, 0, schemes)
+    case.set_patch_bc("U", "inlet", "fixedValue", (0.1, 0, 0))
+    case.set_patch_bc("p", "inlet", "zeroGradient", 0.0)
+    case.set_patch_bc("U", "outlet", "zeroGradient", (0, 0, 0))
+    case.set_patch_bc("p", "outlet", "fixedValue", 0.0)
+    for n in ("bottom", "top", "front", "back"):
+        case.set_patch_bc("U", n, "fixedValue", (0, 0, 0))
+        case.set_patch_bc("p", n, "zeroGradient", 0.0)
+    case.init_flux()
+    return mesh, case
+
+
+def test_config1_channel_matches_reference(golden):
+    """The 16,000-cell channel (40x20x20, 2 x 0.1 x 0.1 m, Re 100) for 20
+    iterations at the reference's stable relaxation, against its own run."""
+    import chuanflow_b200 as cf
+    g = golden("simple_channel40.npz")
+    mesh, case = channel40_product()
+    ctl = cf.SimpleControls(max_iterations=int(g["iters"]), relax_u=0.9, relax_p=0.03, p_relax_start=0.02,
+                            non_orth_correctors=2, linear_tol=1e-10, nu=1e-4)
+    r = case.solve(ctl)
+    U, p, phi = case.download()
+    assert r.iterations == int(g["ref_iterations"])
+    assert abs(r.final_continuity_error - float(g["ref_continuity"])) <= 1e-6 * float(g["ref_continuity"])
+    assert rel(U[g["cells"]], g["ref_U_cells"]) < REL_TOL and rel(p[g["cells"]], g["ref_p_cells"]) < REL_TOL
+    assert rel(phi[g["faces"]], g["ref_phi_faces"]) < REL_TOL
+    assert np.all(np.abs(U.sum(0) - g["ref_U_sum"]) <= REL_TOL * np.abs(U).sum(0))
+
+
+def test_config1_linear_upwind_dic_matches_oracle(golden):
+    """The same channel as the workload names it -- linear-upwind convection,
+    Gauss linear gradients, relaxation 0.7 / 0.3, DIC-PCG to 1e-8 -- against
+    the C restatement (no reference counterpart)."""
+    import chuanflow_b200 as cf
+    g = golden("simple_channel40.npz")
+    mesh, case = channel40_product(cf.Schemes(div="linearUpwind", grad="linear"))
+    ctl = cf.SimpleControls(max_iterations=int(g["iters"]), relax_u=0.7, relax_p=0.3, p_relax_start=0.02,
+                            non_orth_correctors=2, linear_tol=1e-8, nu=1e-4, p_preconditioner="DIC")
+    r = case.solve(ctl)
+    U, p, phi = case.download()
+    assert r.iterations == int(g["lu_iterations"])
+    assert rel(U[g["cells"]], g["lu_U_cells"]) < REL_TOL and rel(p[g["cells"]], g["lu_p_cells"]) < REL_TOL
+    assert rel(phi[g["faces"]], g["lu_phi_faces"]) < REL_TOL
