@@ -21,6 +21,7 @@ Neumann pressure system, made inconsistent by its own boundary
 non-orthogonal correction, drives p to ~1e12 in the first iteration.
 """
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -259,6 +260,89 @@ def main_reference(args, world, rank, dist):
     print(json.dumps(out), flush=True)
 
 
+def main_transient(args, world, rank, local, dist):
+    """The learned preconditioner in a transient run: a 2D-extruded channel
+    (nx x nx/4 x 4 hex cells) with a square obstacle of a quarter of the
+    height, Re 200 on the obstacle, implicit-Euler PISO at CFL 0.5.  The
+    first 75% of the steps run with DIC-PCG pressure and keep (a spread of)
+    the residuals their pressure solves start from; the network trains on
+    them; the last 25% then run twice from the same fields -- DIC-PCG, and
+    flexible CG with the network (warm-started from the previous pressure,
+    DIC fallback) -- to the same 1e-8 test."""
+    import chuanflow_b200 as cf
+    from chuanflow_b200 import meshgen
+    nx = args.transient_nx
+    ny = nx // 4
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "obstacle.msh")
+        ncell, h = meshgen.obstacle_channel_msh(path, nx, ny, 4)
+        mesh = cf.PolyMesh.read_gmsh(path, {"inlet": "inlet", "outlet": "outlet"})
+    case = cf.SimpleCase(mesh, local)
+    for name, _, _, _ in mesh.patches:
+        if name == "inlet":
+            case.set_patch_bc("U", name, "fixedValue", (1.0, 0, 0))
+            case.set_patch_bc("p", name, "zeroGradient", 0.0)
+        elif name == "outlet":
+            case.set_patch_bc("U", name, "zeroGradient", 0.0)
+            case.set_patch_bc("p", name, "fixedValue", 0.0)
+        elif name in ("walls", "obstacle"):
+            case.set_patch_bc("U", name, "fixedValue", (0, 0, 0))
+            case.set_patch_bc("p", name, "zeroGradient", 0.0)
+        else:
+            case.set_patch_bc("U", name, "zeroGradient", 0.0)
+            case.set_patch_bc("p", name, "zeroGradient", 0.0)
+    case.init_flux()
+    nu = 1.0 * 0.25 / 200.0
+    dt = 0.5 * h / 1.0
+    ctl = cf.PisoControls(dt=dt, correctors=2, continuity_tol=1e-10, linear_tol=1e-8, non_orth_correctors=0, nu=nu,
+                          p_preconditioner="DIC")
+    steps = args.transient_steps
+    n_train = (3 * steps) // 4
+    every = max(1, n_train // 32)
+    case.mpnn_create(4, seed=3)
+    t0 = time.perf_counter()
+    for s in range(n_train):
+        case.mpnn_collect(2 if s == 0 else (1 if s % every == 0 else 0), 64)
+        case.piso_step(ctl)
+    case.mpnn_collect(0, 64)
+    sim_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    losses = case.mpnn_train_collected(args.train_epochs, 2e-3)
+    train_s = time.perf_counter() - t0
+    batch = cf.Batch([case])
+    batch.save()
+    legs = {}
+    for name, pre in (("dic64", "DIC"), ("learned_fcg", "MPNN")):
+        batch.restore()
+        c2 = dataclasses.replace(ctl, p_preconditioner=pre)
+        ms, pit, fin = [], 0, None
+        for s in range(n_train, steps):
+            r = case.piso_step(c2)
+            ms.append(r["device_ms"])
+            pit += r["p_inner_iterations"]
+            fin = r
+        U, p, phi = case.download()
+        legs[name] = {"ms_per_step": statistics.mean(ms), "pressure_iterations_per_step": pit / max(1, len(ms)),
+                      "continuity_last": fin["continuity_error"], "U": U}
+    dU = float(np.linalg.norm(legs["learned_fcg"]["U"] - legs["dic64"]["U"]) / np.linalg.norm(legs["dic64"]["U"]))
+    for v in legs.values():
+        v.pop("U")
+    if rank == 0:
+        out = {"metric": "transient obstacle channel: device ms per PISO step, learned FCG vs DIC-PCG pressure",
+               "value": legs["learned_fcg"]["ms_per_step"], "unit": "ms", "n_gpus": world,
+               "steps": steps - n_train, "warmup": n_train, "higher_is_better": False, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64 (network: bf16 weights, f32 activations)", "data": "synthetic",
+               "config": {"workload": f"2D-extruded channel {nx}x{ny}x4 hex with a square obstacle (blockage 0.25), "
+                                      f"{ncell} cells, Re 200 on the obstacle, implicit Euler PISO (2 correctors) "
+                                      f"at CFL 0.5 (dt {dt:g}), {steps} steps: the first {n_train} with DIC-PCG "
+                                      f"generate the training residuals, the rest are timed twice from the same "
+                                      f"fields", "cells": ncell},
+               "legs": legs, "rel_L2_U_learned_vs_dic": dU, "simulation_s_training_steps": sim_s,
+               "train_s": train_s, "train_loss_first": float(losses[0]), "train_loss_last": float(losses[-1]),
+               "speedup_learned_vs_dic": legs["dic64"]["ms_per_step"] / legs["learned_fcg"]["ms_per_step"]}
+        print(json.dumps(out), flush=True)
+
+
 def main_blocks(args, world, rank, local, dist):
     """Detail blocks of a coupled 1D-3D network: N straight ducts with cell
     counts log-uniform in [2e3, 2e5], aspect 5-20, inlet profiles flat /
@@ -424,16 +508,23 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run --steps outer iterations from the initial state with no warm-up, timing or "
                          "baselines: the command line the ncu captures run")
-    ap.add_argument("--workload", default="simple", choices=["simple", "poisson", "blocks"],
+    ap.add_argument("--workload", default="simple", choices=["simple", "poisson", "blocks", "transient"],
                     help="simple: the 2M-cell SIMPLE cavity (the headline); poisson: the ~4M-tet "
                          "pressure-Poisson solve, FP64 DIC-PCG vs FP32-in-FP64 refinement; blocks: 64 detail "
                          "blocks of a coupled network, one coupling pass per step, batched vs one after another")
     ap.add_argument("--blocks", type=int, default=64, help="blocks: number of detail blocks")
+    ap.add_argument("--transient-steps", type=int, default=2000, help="transient: PISO steps in all")
+    ap.add_argument("--transient-nx", type=int, default=800, help="transient: cells along the channel")
     ap.add_argument("--tet-n", type=int, default=84, help="poisson: lattice intervals per axis (6 n^3 tets)")
     ap.add_argument("--no-learned", action="store_true", help="poisson: skip the learned preconditioner")
     ap.add_argument("--train-epochs", type=int, default=30, help="poisson: training epochs of the network")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup()
+    if args.workload == "transient":
+        main_transient(args, world, rank, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     if args.workload == "blocks":
         main_blocks(args, world, rank, local, dist)
         if dist is not None:

@@ -14,7 +14,7 @@ BC = {"fixedValue": 0, "zeroGradient": 1, "fixedGradient": 2, "symmetry": 3, "ou
       "empty": 6}
 GRAD = {"linear": 0, "corrected": 1, "leastSquares": 2}
 DIV = {"upwind": 0, "linear": 1, "blend": 2, "linearUpwind": 3}
-PRECOND = {"Jacobi": 0, "DIC": 1}
+PRECOND = {"Jacobi": 0, "DIC": 1, "MPNN": 2}
 
 _f64p = C.POINTER(C.c_double)
 _i64p = C.POINTER(C.c_int64)
@@ -679,6 +679,22 @@ def _write_vtu(self, path, binary=True):
 
 SimpleCase.write_vtu = _write_vtu
 SimpleCase.piso_step = _piso_step
+def _mpnn_collect(self, on=1, max_samples=64):
+    """Keep (1) / stop keeping (0) / drop and keep (2) the residuals later
+    pressure solves start from; returns the count kept."""
+    n = C.c_int32()
+    _check(lib().cfg_mpnn_collect(self._h, C.c_int32(int(on)), C.c_int32(max_samples), C.byref(n)))
+    return n.value
+
+
+def _mpnn_train_collected(self, epochs=10, lr=1e-3):
+    losses = np.zeros(epochs)
+    _check(lib().cfg_mpnn_train_collected(self._h, C.c_int32(epochs), C.c_float(lr), _dp(losses)))
+    return losses
+
+
+SimpleCase.mpnn_collect = _mpnn_collect
+SimpleCase.mpnn_train_collected = _mpnn_train_collected
 SimpleCase.mpnn_create = _mpnn_create
 SimpleCase.mpnn_weights = _mpnn_weights
 SimpleCase.mpnn_loss_grad = _mpnn_loss_grad

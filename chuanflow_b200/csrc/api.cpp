@@ -999,3 +999,20 @@ int cfg_mesh_write_vtu(const cfg_mesh* mesh, const char* path, int32_t n_fields,
         cfg::writeVtu(mesh->m, path, f, binary != 0);
     });
 }
+
+int cfg_mpnn_collect(cfg_ctx* ctx, int32_t on, int32_t maxSamples, int32_t* n)
+{
+    return guard([&] {
+        need(ctx, "cfg_mpnn_collect: null argument");
+        ctx->c->mpnnCollect(on, maxSamples);
+        if (n) *n = ctx->c->mpnnCollected();
+    });
+}
+
+int cfg_mpnn_train_collected(cfg_ctx* ctx, int32_t epochs, float lr, double* losses)
+{
+    return guard([&] {
+        need(ctx, "cfg_mpnn_train_collected: null argument");
+        ctx->c->mpnnTrainCollected(epochs, lr, losses);
+    });
+}

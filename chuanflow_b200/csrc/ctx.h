@@ -82,6 +82,10 @@ public:
     double mpnnLossGradHost(const double* r, float* grad);
     void mpnnApplyHost(const double* r, double* z);
     void mpnnTrainHost(const double* samples, int nSamples, int epochs, float lr, double* losses);
+    /// residuals the pressure solves start from, kept as training samples
+    void mpnnCollect(int mode, int maxSamples);
+    int mpnnCollected() const { return static_cast<int>(collected_.size()); }
+    void mpnnTrainCollected(int epochs, float lr, double* losses);
     void poissonResidual(const double* b, const double* x, double* r);
     void refreshBcPublic() { refreshBc(); }
     int64_t lastTurbInner = 0;
@@ -188,7 +192,12 @@ private:
     void mpnnMatrix(const double** vals, const double** diag) const;
     void mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses);
     void mpnnFcg(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                 int window, int64_t* out);
+                 int window, int64_t* out, int normType);
+    double fcgNorm(const double* v, int normType);
+    void mpnnResidualHost(const double* vals, const double* b, const double* x, double* rHost);
+    bool collectOn_ = false;
+    int collectMax_ = 0;
+    std::vector<std::vector<double>> collected_;
     void fcgSpmv(const double* vals, const double* x, double* y);
     void fcgDots(int np, const double* const* a, const double* const* b, double* out);
     const double** fcgPtrs_ = nullptr;

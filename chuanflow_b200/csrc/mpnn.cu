@@ -388,6 +388,15 @@ __global__ void __launch_bounds__(TPB) k_fcg_dots(int n, const double* const* a,
     }
 }
 
+/// max |a| (non-negative, order-free) into out
+__global__ void __launch_bounds__(TPB) k_fcg_absmax(int n, const double* __restrict__ a, double* out)
+{
+    double v[1] = {0.0};
+    FOR_ROWS(c, n) v[0] = smax(v[0], fabs(a[c]));
+    block_max<1>(v);
+    if (threadIdx.x == 0) atomic_max_nonneg(out, v[0]);
+}
+
 /// y = x + a p (x may alias y)
 __global__ void __launch_bounds__(TPB) k_fcg_axpy(int n, double a, const double* __restrict__ p, double* y)
 {
@@ -640,6 +649,22 @@ void Ctx::mpnnTrainHost(const double* samples, int nSamples, int epochs, float l
     mpnnTrain(d, nSamples, epochs, lr, losses);
 }
 
+void Ctx::mpnnCollect(int mode, int maxSamples)
+{
+    if (mode == 2) collected_.clear();
+    collectOn_ = mode != 0;
+    collectMax_ = std::max(0, maxSamples);
+}
+
+void Ctx::mpnnTrainCollected(int epochs, float lr, double* losses)
+{
+    if (collected_.empty()) fail(CFG_EINVAL, "mpnn: no collected samples");
+    const size_t n = static_cast<size_t>(dm_.nC);
+    std::vector<double> all(collected_.size() * n);
+    for (size_t k = 0; k < collected_.size(); ++k) std::copy(collected_[k].begin(), collected_[k].end(), all.begin() + k * n);
+    mpnnTrainHost(all.data(), static_cast<int>(collected_.size()), epochs, lr, losses);
+}
+
 void Ctx::poissonResidual(const double* b, const double* x, double* r)
 {
     if (!poissonReady_) fail(CFG_EINVAL, "cfg_poisson_residual: call cfg_poisson_setup first");
@@ -670,7 +695,7 @@ void Ctx::fcgDots(int np, const double* const* a, const double* const* b, double
     if (!fcgPtrs_)
     {
         fcgPtrs_ = alloc<const double*>(6);
-        fcgOut_ = alloc<double>(4);
+        fcgOut_ = alloc<double>(8);
         fcgTicket_ = alloc<unsigned>(1);
         CFG_CUDA(cudaMemsetAsync(fcgTicket_, 0, sizeof(unsigned), stream_));
     }
@@ -690,8 +715,37 @@ void Ctx::fcgDots(int np, const double* const* a, const double* const* b, double
 /// residual has not fallen by 10% over the last `window` iterations the
 /// solve continues from the current x with FP64 DIC-PCG (the fallback).
 /// out: {network iterations, fallback iterations, fell back}
+/// the stopping norm: |v|2 (normType 1) or |v|inf (0, the reference's test)
+double Ctx::fcgNorm(const double* v, int normType)
+{
+    if (normType == 1)
+    {
+        double d[1];
+        const double* a[1] = {v};
+        fcgDots(1, a, a, d);
+        return std::sqrt(d[0]);
+    }
+    CFG_CUDA(cudaMemsetAsync(fcgOut_ + 3, 0, sizeof(double), stream_));
+    k_fcg_absmax<<<GS_, TPB, 0, stream_>>>(dm_.nC, v, fcgOut_ + 3);
+    launchCheck("fcg_absmax");
+    double h;
+    CFG_CUDA(cudaMemcpyAsync(&h, fcgOut_ + 3, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    return h;
+}
+
+void Ctx::mpnnResidualHost(const double* vals, const double* b, const double* x, double* rHost)
+{
+    const int n = dm_.nC;
+    fcgSpmv(vals, x, cAp_);
+    CFG_CUDA(cudaMemcpyAsync(cz_, b, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, -1.0, cAp_, cz_);
+    launchCheck("mpnn_residual");
+    fromDevCells(rHost, cz_, 1, 0);
+}
+
 void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                  int window, int64_t* out)
+                  int window, int64_t* out, int normType)
 {
     const int n = dm_.nC;
     double* r = cr_;
@@ -703,12 +757,9 @@ void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, doubl
     k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, -1.0, q, r);
     launchCheck("fcg_r0");
     double d3[3];
-    {
-        const double* a[2] = {b, r};
-        fcgDots(2, a, a, d3);
-    }
-    const double bn = std::sqrt(d3[0]);
-    double rn = std::sqrt(d3[1]);
+    if (!fcgPtrs_) fcgDots(1, &b, &b, d3);  // allocates the scalar buffers
+    const double bn = std::max(fcgNorm(b, normType), normType == 1 ? 0.0 : 1e-300);
+    double rn = fcgNorm(r, normType);
     std::vector<double> hist{rn};
     int it = 0;
     out[0] = out[1] = out[2] = 0;
@@ -729,11 +780,7 @@ void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, doubl
         k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, -alpha, q, r);
         launchCheck("fcg_update", 2);
         ++it;
-        {
-            const double* aa[1] = {r};
-            fcgDots(1, aa, aa, d3);
-        }
-        rn = std::sqrt(d3[0]);
+        rn = fcgNorm(r, normType);
         hist.push_back(rn);
         if (rn / bn <= tol) break;
         if (static_cast<int>(hist.size()) > window && rn > 0.9 * hist[hist.size() - 1 - window])
@@ -754,7 +801,8 @@ void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, doubl
     if (fallback && it < maxIter)
     {
         cfg_solver_report rep{};
-        dicCGT<double>(dic_, vals, diag, b, x, cr_, cp_, cAp_, cz_, tol, maxIter - it, 1, &rep);
+        if (normType == 0) dicSetup(vals, diag);  // the SIMPLE/PISO matrix of this solve
+        dicCGT<double>(dic_, vals, diag, b, x, cr_, cp_, cAp_, cz_, tol, maxIter - it, normType, &rep);
         out[1] = rep.iterations;
         out[2] = 1;
     }

@@ -1699,8 +1699,24 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
         {
             CFG_CUDA(cudaMemcpyAsync(pRhs_, pBase_, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
         }
+        if (collectOn_ && pass == 0 && static_cast<int>(collected_.size()) < collectMax_)
+        {
+            // a training sample of the learned preconditioner: the residual
+            // this solve starts from
+            std::vector<double> r(static_cast<size_t>(n));
+            mpnnResidualHost(pVal_d_, pRhs_, px_, r.data());
+            collected_.push_back(std::move(r));
+        }
         cfg_solver_report rep;
         if (precond == CFG_PRECOND_DIC) runDICCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
+        else if (precond == CFG_PRECOND_MPNN)
+        {
+            if (!mpnn_) fail(CFG_ESETUP, "pressure: the learned preconditioner needs cfg_mpnn_create");
+            int64_t o[3];
+            mpnnFcg(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, 25, o, 0);
+            rep.iterations = static_cast<int32_t>(o[0] + o[1]);
+            lastFallbackIters += o[1];
+        }
         else runCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
         inner += rep.iterations;
     }
@@ -2266,7 +2282,7 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
         // flexible CG with the learned preconditioner, DIC-PCG when it stalls
         if (!mpnn_) fail(CFG_EINVAL, "cfg_poisson_solve: fcg_mpnn needs cfg_mpnn_create");
         int64_t o[3];
-        mpnnFcg(pVal_d_, pDiag_, pb64_, px64_, tol, maxIter, 25, o);
+        mpnnFcg(pVal_d_, pDiag_, pb64_, px64_, tol, maxIter, 25, o, 1);
         inner = o[0] + o[1];
         outer = 1 + static_cast<int>(o[2]);
         lastFallbackIters = o[1];

@@ -82,3 +82,69 @@ def detail_block_set(n=64, seed=2024, cells_min=2_000, cells_max=200_000):
         out.append({"cells": cells, "aspect": aspect, "shape": SHAPES[i % 3], "speed": speed,
                     "laminar": i % 2 == 0})
     return out
+
+
+def obstacle_channel_msh(path, nx=800, ny=200, nz=4, H=1.0, blockage=0.25, x_center=1.0):
+    """A 2D-extruded channel of cubic hex cells (h = H/ny; L = nx h, depth
+    nz h) with a square obstacle of side blockage*H centred at x_center on
+    the axis, written as a gmsh 2.2 file with physical surfaces inlet
+    (xmin), outlet (xmax), walls (y sides), obstacle, front and back (z
+    sides).  Returns (n cells, cell size h)."""
+    h = H / ny
+    ns = int(round(blockage * ny))
+    j0 = (ny - ns) // 2
+    i0 = int(round(x_center / h)) - ns // 2
+    inside = np.zeros((nx, ny), bool)
+    inside[i0:i0 + ns, j0:j0 + ns] = True
+    nid = lambda i, j, k: (k * (ny + 1) + j) * (nx + 1) + i + 1  # 1-based
+    I, J, Kk = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    order = np.argsort(nid(I, J, Kk).ravel())
+    pts = np.stack([I.ravel() * h, J.ravel() * h, Kk.ravel() * h], 1)[order]
+    ci, cj, ck = np.nonzero(np.broadcast_to(~inside[:, :, None], (nx, ny, nz)))
+    hexes = np.stack([nid(ci, cj, ck), nid(ci + 1, cj, ck), nid(ci + 1, cj + 1, ck), nid(ci, cj + 1, ck),
+                      nid(ci, cj, ck + 1), nid(ci + 1, cj, ck + 1), nid(ci + 1, cj + 1, ck + 1),
+                      nid(ci, cj + 1, ck + 1)], 1)
+    quads = {name: [] for name in ("inlet", "outlet", "walls", "obstacle", "front", "back")}
+    jj, kk = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+    jj, kk = jj.ravel(), kk.ravel()
+    quads["inlet"] = np.stack([nid(0, jj, kk), nid(0, jj + 1, kk), nid(0, jj + 1, kk + 1), nid(0, jj, kk + 1)], 1)
+    quads["outlet"] = np.stack([nid(nx, jj, kk), nid(nx, jj + 1, kk), nid(nx, jj + 1, kk + 1),
+                                nid(nx, jj, kk + 1)], 1)
+    ii, kk2 = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+    ii, kk2 = ii.ravel(), kk2.ravel()
+    quads["walls"] = np.concatenate([
+        np.stack([nid(ii, 0, kk2), nid(ii + 1, 0, kk2), nid(ii + 1, 0, kk2 + 1), nid(ii, 0, kk2 + 1)], 1),
+        np.stack([nid(ii, ny, kk2), nid(ii + 1, ny, kk2), nid(ii + 1, ny, kk2 + 1), nid(ii, ny, kk2 + 1)], 1)])
+    ob = []
+    for k in range(nz):
+        for j in range(j0, j0 + ns):
+            ob.append([nid(i0, j, k), nid(i0, j + 1, k), nid(i0, j + 1, k + 1), nid(i0, j, k + 1)])
+            ob.append([nid(i0 + ns, j, k), nid(i0 + ns, j + 1, k), nid(i0 + ns, j + 1, k + 1), nid(i0 + ns, j, k + 1)])
+        for i in range(i0, i0 + ns):
+            ob.append([nid(i, j0, k), nid(i + 1, j0, k), nid(i + 1, j0, k + 1), nid(i, j0, k + 1)])
+            ob.append([nid(i, j0 + ns, k), nid(i + 1, j0 + ns, k), nid(i + 1, j0 + ns, k + 1), nid(i, j0 + ns, k + 1)])
+    quads["obstacle"] = np.array(ob)
+    fi, fj = np.nonzero(~inside)
+    quads["front"] = np.stack([nid(fi, fj, 0), nid(fi + 1, fj, 0), nid(fi + 1, fj + 1, 0), nid(fi, fj + 1, 0)], 1)
+    quads["back"] = np.stack([nid(fi, fj, nz), nid(fi + 1, fj, nz), nid(fi + 1, fj + 1, nz), nid(fi, fj + 1, nz)], 1)
+    names = list(quads)
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$PhysicalNames\n%d\n" % (len(names) + 1))
+        for g, name in enumerate(names):
+            f.write('2 %d "%s"\n' % (g + 1, name))
+        f.write('3 %d "fluid"\n$EndPhysicalNames\n$Nodes\n%d\n' % (len(names) + 1, len(pts)))
+        np.savetxt(f, np.column_stack([np.arange(1, len(pts) + 1), pts]), fmt="%d %.17g %.17g %.17g")
+        nq = sum(len(q) for q in quads.values())
+        f.write("$EndNodes\n$Elements\n%d\n" % (nq + len(hexes)))
+        e = 1
+        for g, name in enumerate(names):
+            q = np.asarray(quads[name])
+            rows = np.column_stack([np.arange(e, e + len(q)), np.full(len(q), 3), np.full(len(q), 2),
+                                    np.full(len(q), g + 1), np.full(len(q), g + 1), q])
+            np.savetxt(f, rows, fmt="%d")
+            e += len(q)
+        rows = np.column_stack([np.arange(e, e + len(hexes)), np.full(len(hexes), 5), np.full(len(hexes), 2),
+                                np.full(len(hexes), len(names) + 1), np.full(len(hexes), len(names) + 1), hexes])
+        np.savetxt(f, rows, fmt="%d")
+        f.write("$EndElements\n")
+    return int(len(hexes)), h

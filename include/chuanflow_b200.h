@@ -60,7 +60,9 @@ enum cfg_div_scheme { CFG_DIV_UPWIND = 0, CFG_DIV_LINEAR = 1, CFG_DIV_BLEND = 2,
 enum cfg_lin_method { CFG_SOLVE_CG = 0, CFG_SOLVE_BICGSTAB = 1 };
 /* pressure preconditioner: the reference's Jacobi PCG, or this library's
  * multicolour DIC (no reference counterpart) */
-enum cfg_precond { CFG_PRECOND_JACOBI = 0, CFG_PRECOND_DIC = 1 };
+enum cfg_precond { CFG_PRECOND_JACOBI = 0, CFG_PRECOND_DIC = 1, CFG_PRECOND_MPNN = 2 };
+/* CFG_PRECOND_MPNN: flexible CG with the learned preconditioner (cfg_mpnn_*),
+ * the reference's infinity-norm test, FP64 DIC-PCG when it stalls */
 
 /* Schemes (src/3d/include/cf/fvm/FvMatrix.h:30-38) */
 typedef struct cfg_schemes
@@ -448,6 +450,12 @@ int cfg_mpnn_apply(cfg_ctx* ctx, const double* r, double* z);
 /* Adam (lr) over n_samples residual samples (n_samples x nCells, original
  * order), `epochs` passes; losses[epoch] = mean loss (may be NULL). */
 int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t n_samples, int32_t epochs, float lr, double* losses);
+/* Keep (on = 1) up to max_samples of the residuals the SIMPLE / PISO
+ * pressure solves start from (b - A x0 of their first pass, original
+ * order) as training samples; on = 2 first drops those kept; on = 0 stops.
+ * cfg_mpnn_train_collected trains on them; n returns how many are kept. */
+int cfg_mpnn_collect(cfg_ctx* ctx, int32_t on, int32_t max_samples, int32_t* n);
+int cfg_mpnn_train_collected(cfg_ctx* ctx, int32_t epochs, float lr, double* losses);
 /* r = b - A x on the cfg_poisson_setup system (training samples from the
  * plain solver's iterates). */
 int cfg_poisson_residual(cfg_ctx* ctx, const double* b, const double* x, double* r);

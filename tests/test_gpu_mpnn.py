@@ -93,3 +93,45 @@ def test_trained_network_gains_in_flexible_cg():
     assert r1["inner_iterations"] < r0["inner_iterations"], (r1, r0)
     for x in (x0, x1):
         assert np.linalg.norm(x - xd) <= 1e-6 * np.linalg.norm(xd)
+
+
+def test_learned_pressure_in_piso_steps(tmp_path):
+    """Residuals kept from the DIC-PCG pressure solves of PISO steps train
+    the network; steps with the network's flexible CG (DIC fallback) from
+    the same fields reach the same flow as DIC-PCG steps."""
+    import chuanflow_b200 as cf
+    from chuanflow_b200 import meshgen
+    path = tmp_path / "o.msh"
+    n, h = meshgen.obstacle_channel_msh(str(path), 80, 20, 2)
+    mesh = cf.PolyMesh.read_gmsh(path, {"inlet": "inlet", "outlet": "outlet"})
+    case = cf.SimpleCase(mesh)
+    bcs = {"inlet": ("fixedValue", (1.0, 0, 0), "zeroGradient"), "outlet": ("zeroGradient", 0.0, "fixedValue"),
+           "walls": ("fixedValue", (0, 0, 0), "zeroGradient"), "obstacle": ("fixedValue", (0, 0, 0), "zeroGradient"),
+           "front": ("zeroGradient", 0.0, "zeroGradient"), "back": ("zeroGradient", 0.0, "zeroGradient")}
+    for name, (ut, uv, pt) in bcs.items():
+        case.set_patch_bc("U", name, ut, uv)
+        case.set_patch_bc("p", name, pt, 0.0)
+    case.init_flux()
+    ctl = cf.PisoControls(dt=0.5 * h, correctors=2, linear_tol=1e-8, non_orth_correctors=0, nu=0.25 / 200,
+                          p_preconditioner="DIC")
+    case.mpnn_create(4, seed=3)
+    for s in range(24):
+        case.mpnn_collect(2 if s == 0 else 1, 48)
+        case.piso_step(ctl)
+    kept = case.mpnn_collect(0, 48)
+    assert kept == 48
+    losses = case.mpnn_train_collected(20, 2e-3)
+    assert losses[-1] < losses[0]
+    b = cf.Batch([case])
+    b.save()
+    for _ in range(6):
+        case.piso_step(ctl)
+    U0, p0, _ = case.download()
+    b.restore()
+    import dataclasses
+    c2 = dataclasses.replace(ctl, p_preconditioner="MPNN")
+    for _ in range(6):
+        r = case.piso_step(c2)
+        assert not r["diverged"]
+    U1, p1, _ = case.download()
+    assert np.linalg.norm(U1 - U0) <= 1e-6 * np.linalg.norm(U0)

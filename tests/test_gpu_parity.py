@@ -178,6 +178,7 @@ def test_full_size_cavity_matches_oracle_checksums(golden):
     mesh, case, ctl = bench.make_case(int(g["n"]), 0, "Jacobi")
     assert np.array_equal(mesh.addressing()["points"].sum(0), g["points_sum"])
     ctl.max_iterations = int(g["iters"])
+    ctl.linear_tol = float(g["linear_tol"])
     r = case.solve(ctl)
     U, p, phi = case.download()
     assert r.iterations == int(g["iterations"])
