@@ -66,7 +66,7 @@ KERNEL_NAMES = {
 }
 
 
-MEASURED_TRAFFIC = {"bi_spmv2": 314.3e6, "cg_spmv": 204.9e6}
+MEASURED_TRAFFIC = {"bi_spmv2": 314.3e6}
 
 
 def kernel_bytes(N, F, s=8, i=4):
@@ -623,9 +623,8 @@ def main():
                           "achieved_gbs": alg[k] / (us * 1e-6) / 1e9}
     top = max(kernels, key=lambda k: kernels[k]["total_ms"])
     kt = kernels[top]
-    # DRAM bytes per launch from one ncu capture of this workload (128^3):
-    # profiles/k_bi_spmv2_128cube_memory.md and the earlier pressure-SpMV
-    # capture; null for a kernel without one
+    # DRAM bytes per launch from one ncu capture of this workload (128^3,
+    # profiles/k_bi_spmv2_128cube_memory.md); null for a kernel without one
     traffic = MEASURED_TRAFFIC.get(top) if n == 128 else None
     roof = {"kernel": KERNEL_NAMES[top], "bound": "hbm", "achieved": kt["achieved_gbs"], "peak": peak,
             "unit": "GB/s", "frac": kt["achieved_gbs"] / peak, "peak_source": peak_src, "traffic": traffic,
