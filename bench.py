@@ -59,14 +59,14 @@ KERNEL_NAMES = {
     "cg_p": "k_cg_p (pressure PCG: search direction)",
     "bi_p": "k_bi_p (momentum BiCGStab, 3 components: p, z update)",
     "bi_spmv1": "k_bi_spmv1 (momentum BiCGStab, 3 components: v = A z + r0.v)",
-    "bi_s": "k_bi_s (momentum BiCGStab, 3 components: x, s, s^ update + |s|)",
+    "bi_s": "k_bi_s (momentum BiCGStab, 3 components: s, s^ update + |s|)",
     "bi_spmv2": "k_bi_spmv2 (momentum BiCGStab, 3 components: t = A s^ + t.t, t.s)",
-    "bi_x": "k_bi_x (momentum BiCGStab, 3 components: x, r update + |r| + r0.r)",
+    "bi_x": "k_bi_x (momentum BiCGStab, 3 components: x += alpha z + omega s^, r update + |r| + r0.r)",
     "dic_apply": "k_dic_fwd/k_dic_bwd (multicolour DIC z = M^-1 r, all colour phases)",
 }
 
 
-MEASURED_TRAFFIC = {"bi_spmv2": 314.3e6}
+MEASURED_TRAFFIC = {}
 
 
 def kernel_bytes(N, F, s=8, i=4):
@@ -76,7 +76,7 @@ def kernel_bytes(N, F, s=8, i=4):
     spmv_sym = 3 * s * N + s * F + 2 * i * F       # x in, y out, diag + one coefficient per face, indices
     spmv3 = 10 * s * N + 2 * s * F + 2 * i * F     # 3 x in, 3 y out, 3 dot partners, diag, both coefficients
     return {"cg_spmv": spmv_sym, "cg_update": 7 * s * N, "cg_p": 4 * s * N,
-            "bi_p": 16 * s * N, "bi_spmv1": spmv3, "bi_s": 22 * s * N, "bi_spmv2": spmv3, "bi_x": 21 * s * N,
+            "bi_p": 16 * s * N, "bi_spmv1": spmv3, "bi_s": 13 * s * N, "bi_spmv2": spmv3, "bi_x": 24 * s * N,
             "dic_apply": 3 * s * N + 2 * (s * F + 2 * i * F)}
 
 

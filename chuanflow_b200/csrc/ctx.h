@@ -260,6 +260,7 @@ private:
     std::vector<DicPhase> dicPhase_;
     int nColours_ = 0, nLo_ = 0, nUp_ = 0, dicPartials_ = 1;
     V3P br_, br0_, bp_, bv_, bs_, bsh_, bt_, bz_;
+    double* bInvD_ = nullptr;  // BiCGStab's Jacobi inverse diagonal
     double* partials_;
     SolveState* st_;
     SolveState* stHost_;

@@ -83,7 +83,6 @@ struct SolveState
     double bnorm[3], init[3], fin[3];
     double rho[3], alpha[3], omega[3], beta[3];
     double rz[3], pAp[3];
-    double sMax[3];
     int it[3], done[3], conv[3], special[3];
     int allDone;
     int normType;  // 0: |r|inf / |b|inf (the reference's test); 1: |r|2 / |b|2

@@ -374,6 +374,53 @@ __device__ __forceinline__ void spmv_row(const DMat& A, const T* __restrict__ va
     }
 }
 
+/// One row of y = A x where the NC values of x at a column are formed by
+/// `gather(col, xv)` from several arrays, in the same entry order and with
+/// the same skipping as spmv_row.
+template <int W, int NC, class Gather>
+__device__ __forceinline__ void spmv_row_gather(const DMat& A, const double* __restrict__ val, int c, double (&y)[NC],
+                                                Gather gather)
+{
+#pragma unroll
+    for (int q = 0; q < NC; ++q) y[q] = 0.0;
+    const int sl = c >> 5, lane = c & 31;
+    const int e0 = __ldg(A.start + sl) + lane, e1 = __ldg(A.start + sl + 1);
+    if constexpr (W > 0)
+    {
+        int col[W];
+        double v[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+        {
+            const int e = e0 + 32 * k;
+            col[k] = e < e1 ? __ldg(A.col + e) : -1;
+            v[k] = e < e1 ? __ldg(val + e) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if (col[k] >= 0)
+            {
+                double xv[NC];
+                gather(col[k], xv);
+#pragma unroll
+                for (int q = 0; q < NC; ++q) y[q] += v[k] * xv[q];
+            }
+    }
+    else
+    {
+        for (int e = e0; e < e1; e += 32)
+        {
+            const int col = A.col[e];
+            if (col < 0) break;
+            const double v = val[e];
+            double xv[NC];
+            gather(col, xv);
+#pragma unroll
+            for (int q = 0; q < NC; ++q) y[q] += v * xv[q];
+        }
+    }
+}
+
 /// The solver kernels' row loop: a grid-stride loop, so a warp's rows stay
 /// contiguous and the grid can be sized for the GPU rather than the system
 /// (fewer blocks means fewer per-block reduction epilogues and partials).

@@ -952,6 +952,7 @@ void Ctx::buildDevice()
     v3(bsh_, nC);
     v3(bt_, nC);
     v3(bz_, nC);
+    bInvD_ = alloc<double>(nC);
     gU_ = alloc<double>(nF);
     fScratch_ = alloc<double>(nF);
     bScratch_ = alloc<double>(2 * static_cast<size_t>(nB));
@@ -1394,7 +1395,7 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     auto loop = [&](auto Wc, auto NCc) {
         constexpr int W = decltype(Wc)::value;
         constexpr int NC = decltype(NCc)::value;
-        k_bi_init<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, b, x, br_, br0_, bp_, bv_, partials_, st_);
+        k_bi_init<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, diag, bInvD_, b, x, br_, br0_, bp_, bv_, partials_, st_);
         launchCheck("bicg_init");
         int itBefore = 0, lastChunk = 0;
         auto itMax = [&] {
@@ -1408,27 +1409,25 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
             CFG_CUDA(cudaStreamSynchronize(stream_));
             if (lastChunk > 0)
             {
-                static const int slots[5] = {KS_BI_P, KS_BI_SPMV1, KS_BI_S, KS_BI_SPMV2, KS_BI_X};
-                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 5);
+                static const int slots[4] = {KS_BI_P, KS_BI_SPMV1, KS_BI_SPMV2, KS_BI_X};
+                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 4);
             }
             itBefore = itMax();
             if (stHost_->allDone || launched >= maxIter) break;
             const int m = std::min(chunk, maxIter - launched);
             launchChunk(ptrKey("bicg", {vals, diag, x.c[0], x.c[1], x.c[2]}, W * 8 + NC), m, [&](int k) {
                 tmark(k, 0);
-                k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, diag, br_, bp_, bv_, bz_, st_);
+                k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, bInvD_, br_, bp_, bv_, bz_, st_);
                 tmark(k, 1);
                 k_bi_spmv1<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
                 tmark(k, 2);
-                k_bi_s<NC><<<GS_, TPB, 0, stream_>>>(n, diag, x, bz_, br_, bv_, bs_, bsh_, partials_, st_);
+                k_bi_spmv2<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bInvD_, br_, bv_, bt_, partials_, st_);
                 tmark(k, 3);
-                k_bi_spmv2<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bt_, bs_, partials_, st_);
+                k_bi_x<NC><<<GS_, TPB, 0, stream_>>>(n, bInvD_, x, bz_, bv_, bt_, br_, br0_, partials_, st_);
                 tmark(k, 4);
-                k_bi_x<NC><<<GS_, TPB, 0, stream_>>>(n, x, bsh_, bs_, bt_, br_, br0_, partials_, st_);
-                tmark(k, 5);
                 launchCheck("bicg_iter", 0);
             });
-            launches_ += 5 * m;
+            launches_ += 4 * m;
             launched += m;
             lastChunk = m;
             chunk = std::min(chunk * 2, 32);

@@ -220,8 +220,9 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_cg_p(int n, const T* 
 // stops on its own test exactly where the serial loop would.
 
 template <int W, int NC>
-__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_init(DMat A, const double* __restrict__ val, V3P b, V3P x, V3P r, V3P r0,
-                                                 V3P p, V3P v, double* partials, SolveState* st)
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_init(DMat A, const double* __restrict__ val,
+                                                 const double* __restrict__ diag, double* __restrict__ invD, V3P b,
+                                                 V3P x, V3P r, V3P r0, V3P p, V3P v, double* partials, SolveState* st)
 {
     double mx[3 * NC];  // |r|, |b|, nan per comp
     double sm[NC];      // r.r
@@ -234,6 +235,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_init(DMat A, const
     for (int q = 0; q < NC; ++q) xs[q] = x.c[q];
     FOR_ROWS(c, A.n)
     {
+        invD[c] = inv_diag_bicg(diag[c]);  // invD of Matrix.cpp:229-236
         double y[NC];
         spmv_row<W, NC>(A, val, c, xs, y);
 #pragma unroll
@@ -304,8 +306,8 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_init(DMat A, const
 
 /// p = r + beta (p - omega v); z = p D^-1   (Matrix.cpp:262-272)
 template <int NC>
-__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_p(int n, const double* __restrict__ diag, V3P r, V3P p, V3P v, V3P z,
-                                              const SolveState* st)
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_p(int n, const double* __restrict__ invD, V3P r, V3P p, V3P v,
+                                              V3P z, const SolveState* st)
 {
     if (st->allDone) return;
     double beta[NC], om[NC];
@@ -322,7 +324,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_p(int n, const dou
         // every load of the row before its first store: the component
         // arrays are not restrict-qualified, so a store would otherwise
         // hold back the next component's loads
-        const double id = inv_diag_bicg(diag[c]);
+        const double id = invD[c];
         double rv[NC], pv[NC], vv[NC];
 #pragma unroll
         for (int q = 0; q < NC; ++q)
@@ -396,87 +398,41 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv1(DMat A, cons
     }
 }
 
-/// x += alpha z; s = r - alpha v; sh = s D^-1; |s|inf (Matrix.cpp:277-289)
-template <int NC>
-__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_s(int n, const double* __restrict__ diag, V3P x, V3P z, V3P r, V3P v,
-                                              V3P s, V3P sh, double* partials, SolveState* st)
-{
-    if (st->allDone) return;
-    double al[NC];
-    int dn[NC];
-    double mx[2 * NC];
-#pragma unroll
-    for (int q = 0; q < NC; ++q)
-    {
-        dn[q] = st->done[q];
-        al[q] = st->alpha[q];
-        mx[q] = mx[NC + q] = 0.0;
-    }
-    FOR_ROWS(c, n)
-    {
-        const double id = inv_diag_bicg(diag[c]);
-        double xv[NC], zv[NC], rv[NC], vv[NC];
-#pragma unroll
-        for (int q = 0; q < NC; ++q)
-            if (!dn[q])
-            {
-                xv[q] = x.c[q][c];
-                zv[q] = z.c[q][c];
-                rv[q] = r.c[q][c];
-                vv[q] = v.c[q][c];
-            }
-#pragma unroll
-        for (int q = 0; q < NC; ++q)
-        {
-            if (dn[q]) continue;
-            x.c[q][c] = xv[q] + al[q] * zv[q];
-            const double si = rv[q] - al[q] * vv[q];
-            s.c[q][c] = si;
-            sh.c[q][c] = si * id;
-            if (isnan(si)) mx[NC + q] = 1.0;
-            mx[q] = smax(mx[q], fabs(si));
-        }
-    }
-    block_max<2 * NC>(mx);
-    const int G = gridDim.x;
-    if (threadIdx.x == 0)
-#pragma unroll
-        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = mx[q];
-    if (!last_block(&st->ticket[0])) return;
-    double fm[2 * NC];
-    final_max<2 * NC>(partials, G, fm);
-    if (threadIdx.x == 0)
-    {
-        st->ticket[0] = 0;
-        for (int q = 0; q < NC; ++q) st->sMax[q] = fm[NC + q] > 0 ? NAN : fm[q];
-    }
-}
-
-/// t = A sh; t.t and t.s; omega, or the tDenom breakdown exit (Matrix.cpp:290-300)
+/// t = A sh with sh = (r - alpha v) D^-1 formed per column as the row is
+/// read; t.t and t.s; omega, or the tDenom breakdown exit (Matrix.cpp:
+/// 277-300).  s and sh are never stored: every reader forms them from r, v
+/// and invD with the same two operations, so each value is the reference's,
+/// and the separate s pass and its two stores disappear.  The |s|inf that
+/// the breakdown exit reports is taken by k_bi_x, in that case only.
 template <int W, int NC>
-__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv2(DMat A, const double* __restrict__ val, V3P sh, V3P t, V3P s,
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv2(DMat A, const double* __restrict__ val,
+                                                  const double* __restrict__ invD, V3P r, V3P v, V3P t,
                                                   double* partials, SolveState* st)
 {
     if (st->allDone) return;
+    double al[NC];
     double sm[2 * NC];
 #pragma unroll
-    for (int q = 0; q < 2 * NC; ++q) sm[q] = 0.0;
-    const double* xs[NC];
-#pragma unroll
-    for (int q = 0; q < NC; ++q) xs[q] = sh.c[q];
+    for (int q = 0; q < NC; ++q)
+    {
+        al[q] = st->alpha[q];
+        sm[q] = sm[NC + q] = 0.0;
+    }
     FOR_ROWS(c, A.n)
     {
-        double sv[NC];
-#pragma unroll
-        for (int q = 0; q < NC; ++q) sv[q] = s.c[q][c];
         double y[NC];
-        spmv_row<W, NC>(A, val, c, xs, y);
+        spmv_row_gather<W, NC>(A, val, c, y, [&](int col, double (&xv)[NC]) {
+            const double id = __ldg(invD + col);
+#pragma unroll
+            for (int q = 0; q < NC; ++q) xv[q] = (__ldg(r.c[q] + col) - al[q] * __ldg(v.c[q] + col)) * id;
+        });
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
+            const double si = r.c[q][c] - al[q] * v.c[q][c];
             t.c[q][c] = y[q];
             sm[q] += y[q] * y[q];
-            sm[NC + q] += y[q] * sv[q];
+            sm[NC + q] += y[q] * si;
         }
     }
     block_sum<2 * NC>(sm);
@@ -498,10 +454,10 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv2(DMat A, cons
                 const double tDenom = fs[q];
                 if (tDenom < 1e-300)
                 {
-                    // r = s; the iteration counts and ends here
+                    // r = s and the iteration counts; k_bi_x applies this
+                    // iteration's x += alpha z and reports |s|inf
+                    st->special[q] = 1;
                     st->it[q] = st->it[q] + 1;
-                    st->fin[q] = st->sMax[q];
-                    st->conv[q] = st->fin[q] / st->bnorm[q] < st->tol;
                     st->done[q] = 1;
                 }
                 else
@@ -515,46 +471,55 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv2(DMat A, cons
     }
 }
 
-/// x += omega sh; r = s - omega t; |r|inf test; next r0.r (Matrix.cpp:301-315, :263-264)
+/// x = (x + alpha z) + omega sh; r = s - omega t; |r|inf test; next r0.r
+/// (Matrix.cpp:280-282, 301-315, 263-264), with s = r - alpha v and sh = s
+/// invD formed as in k_bi_spmv2.  A component that broke down in k_bi_spmv2
+/// takes only its x + alpha z, and its |s|inf becomes the final residual.
 template <int NC>
-__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, V3P x, V3P sh, V3P s, V3P t, V3P r, V3P r0, double* partials,
-                                              SolveState* st)
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, const double* __restrict__ invD, V3P x, V3P z,
+                                              V3P v, V3P t, V3P r, V3P r0, double* partials, SolveState* st)
 {
-    if (st->allDone) return;
-    double om[NC];
-    int dn[NC];
+    if (st->allDone && !(st->special[0] | st->special[1] | st->special[2])) return;
+    double om[NC], al[NC];
+    int dn[NC], sp[NC];
     double mx[2 * NC], sm[NC];
 #pragma unroll
     for (int q = 0; q < NC; ++q)
     {
         dn[q] = st->done[q];
+        sp[q] = st->special[q];
         om[q] = st->omega[q];
+        al[q] = st->alpha[q];
         mx[q] = mx[NC + q] = 0.0;
         sm[q] = 0.0;
     }
     FOR_ROWS(c, n)
     {
-        double xv[NC], shv[NC], sv[NC], tv[NC], r0v[NC];
-#pragma unroll
-        for (int q = 0; q < NC; ++q)
-            if (!dn[q])
-            {
-                xv[q] = x.c[q][c];
-                shv[q] = sh.c[q][c];
-                sv[q] = s.c[q][c];
-                tv[q] = t.c[q][c];
-                r0v[q] = r0.c[q][c];
-            }
+        const double id = invD[c];
+        // one component at a time: its loads, then its two stores
 #pragma unroll
         for (int q = 0; q < NC; ++q)
         {
-            if (dn[q]) continue;
-            x.c[q][c] = xv[q] + om[q] * shv[q];
-            const double ri = sv[q] - om[q] * tv[q];
+            if (dn[q])
+            {
+                if (sp[q])
+                {
+                    x.c[q][c] = x.c[q][c] + al[q] * z.c[q][c];
+                    const double si = r.c[q][c] - al[q] * v.c[q][c];
+                    if (isnan(si)) mx[NC + q] = 1.0;
+                    mx[q] = smax(mx[q], fabs(si));
+                }
+                continue;
+            }
+            const double xv = x.c[q][c], zv = z.c[q][c], rv = r.c[q][c];
+            const double vv = v.c[q][c], tv = t.c[q][c], r0v = r0.c[q][c];
+            const double si = rv - al[q] * vv;
+            x.c[q][c] = (xv + al[q] * zv) + om[q] * (si * id);
+            const double ri = si - om[q] * tv;
             r.c[q][c] = ri;
             if (isnan(ri)) mx[NC + q] = 1.0;
             mx[q] = smax(mx[q], fabs(ri));
-            sm[q] += r0v[q] * ri;
+            sm[q] += r0v * ri;
         }
     }
     block_max<2 * NC>(mx);
@@ -579,7 +544,12 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, V3P x, V3
         int all = 1;
         for (int q = 0; q < NC; ++q)
         {
-            if (!st->done[q])
+            if (st->special[q])
+            {
+                st->fin[q] = fm[NC + q] > 0 ? NAN : fm[q];
+                st->conv[q] = st->fin[q] / st->bnorm[q] < st->tol;
+            }
+            else if (!st->done[q])
             {
                 const int it = st->it[q] + 1;
                 st->it[q] = it;
@@ -603,6 +573,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, V3P x, V3
             }
             all &= st->done[q];
         }
+        for (int q = 0; q < 3; ++q) st->special[q] = 0;
         st->allDone = all;
     }
 }

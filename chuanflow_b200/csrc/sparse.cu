@@ -167,32 +167,30 @@ void Ctx::sparseSolve(int device, int64_t n64, const int64_t* rs, const int64_t*
         }
         else
         {
-            V3P r{}, r0{}, p{}, v{}, sv{}, sh{}, t{}, z{}, bb{}, xx{};
+            V3P r{}, r0{}, p{}, v{}, t{}, z{}, bb{}, xx{};
             for (int q = 0; q < 3; ++q)
             {
                 r.c[q] = buf.get<double>(n);
                 r0.c[q] = buf.get<double>(n);
                 p.c[q] = buf.get<double>(n);
                 v.c[q] = buf.get<double>(n);
-                sv.c[q] = buf.get<double>(n);
-                sh.c[q] = buf.get<double>(n);
                 t.c[q] = buf.get<double>(n);
                 z.c[q] = buf.get<double>(n);
                 bb.c[q] = db;
                 xx.c[q] = dx;
             }
-            k_bi_init<W, 1><<<GS, TPB, 0, s>>>(A, dVal, bb, xx, r, r0, p, v, partials, st);
+            double* invD = buf.get<double>(n);
+            k_bi_init<W, 1><<<GS, TPB, 0, s>>>(A, dVal, dDiag, invD, bb, xx, r, r0, p, v, partials, st);
             CFG_CUDA(cudaGetLastError());
             for (int launched = 0, chunk = 4; !poll() && launched < maxIter; chunk = std::min(2 * chunk, 32))
             {
                 const int m = std::min(chunk, maxIter - launched);
                 for (int k = 0; k < m; ++k)
                 {
-                    k_bi_p<1><<<GS, TPB, 0, s>>>(n, dDiag, r, p, v, z, st);
+                    k_bi_p<1><<<GS, TPB, 0, s>>>(n, invD, r, p, v, z, st);
                     k_bi_spmv1<W, 1><<<GS, TPB, 0, s>>>(A, dVal, z, v, r0, partials, st);
-                    k_bi_s<1><<<GS, TPB, 0, s>>>(n, dDiag, xx, z, r, v, sv, sh, partials, st);
-                    k_bi_spmv2<W, 1><<<GS, TPB, 0, s>>>(A, dVal, sh, t, sv, partials, st);
-                    k_bi_x<1><<<GS, TPB, 0, s>>>(n, xx, sh, sv, t, r, r0, partials, st);
+                    k_bi_spmv2<W, 1><<<GS, TPB, 0, s>>>(A, dVal, invD, r, v, t, partials, st);
+                    k_bi_x<1><<<GS, TPB, 0, s>>>(n, invD, xx, z, v, t, r, r0, partials, st);
                 }
                 CFG_CUDA(cudaGetLastError());
                 launched += m;
