@@ -59,8 +59,7 @@ KERNEL_NAMES = {
     "cg_p": "k_cg_p (pressure PCG: search direction)",
     "bi_p": "k_bi_p (momentum BiCGStab, 3 components: p, z update)",
     "bi_spmv1": "k_bi_spmv1 (momentum BiCGStab, 3 components: v = A z + r0.v)",
-    "bi_s": "k_bi_s (momentum BiCGStab, 3 components: s, s^ update + |s|)",
-    "bi_spmv2": "k_bi_spmv2 (momentum BiCGStab, 3 components: t = A s^ + t.t, t.s)",
+    "bi_spmv2": "k_bi_spmv2 (momentum BiCGStab, 3 components: t = A s^, s^ formed per column, + t.t, t.s)",
     "bi_x": "k_bi_x (momentum BiCGStab, 3 components: x += alpha z + omega s^, r update + |r| + r0.r)",
     "dic_apply": "k_dic_fwd/k_dic_bwd (multicolour DIC z = M^-1 r, all colour phases)",
 }
@@ -74,9 +73,16 @@ def kernel_bytes(N, F, s=8, i=4):
     counted once per read and once per write, gathers as one N-stream.
     The three momentum components share one matrix read."""
     spmv_sym = 3 * s * N + s * F + 2 * i * F       # x in, y out, diag + one coefficient per face, indices
-    spmv3 = 10 * s * N + 2 * s * F + 2 * i * F     # 3 x in, 3 y out, 3 dot partners, diag, both coefficients
+    mat3 = s * N + 2 * s * F + 2 * i * F           # diag + both coefficients + indices, shared by 3 components
     return {"cg_spmv": spmv_sym, "cg_update": 7 * s * N, "cg_p": 4 * s * N,
-            "bi_p": 16 * s * N, "bi_spmv1": spmv3, "bi_s": 13 * s * N, "bi_spmv2": spmv3, "bi_x": 24 * s * N,
+            # r, p, v, invD in; p, z out
+            "bi_p": 16 * s * N,
+            # z in (gathered), v out, r0 in
+            "bi_spmv1": 9 * s * N + mat3,
+            # r, v, invD in (gathered); t out
+            "bi_spmv2": 10 * s * N + mat3,
+            # x, z, r, v, t, r0, invD in; x, r out
+            "bi_x": 25 * s * N,
             "dic_apply": 3 * s * N + 2 * (s * F + 2 * i * F)}
 
 

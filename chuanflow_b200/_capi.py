@@ -418,9 +418,9 @@ class SimpleCase:
         _check(lib().cfg_kernel_timing(self._h, C.c_int32(int(enable))))
 
     def kernel_stats(self):
-        out = np.zeros(18)
+        out = np.zeros(16)
         _check(lib().cfg_kernel_stats(self._h, _dp(out)))
-        names = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_s", "bi_spmv2", "bi_x", "dic_apply")
+        names = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_spmv2", "bi_x", "dic_apply")
         return {n: (int(out[2 * i]), float(out[2 * i + 1])) for i, n in enumerate(names)}
 
     # ---- the pressure-Poisson system on its own ----

@@ -420,7 +420,7 @@ int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable)
     });
 }
 
-int cfg_kernel_stats(const cfg_ctx* ctx, double out[18])
+int cfg_kernel_stats(const cfg_ctx* ctx, double out[16])
 {
     return guard([&] {
         need(ctx && out, "cfg_kernel_stats: null argument");

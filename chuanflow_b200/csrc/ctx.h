@@ -119,7 +119,6 @@ public:
         KS_CG_P,
         KS_BI_P,
         KS_BI_SPMV1,
-        KS_BI_S,
         KS_BI_SPMV2,
         KS_BI_X,
         KS_DIC_APPLY,

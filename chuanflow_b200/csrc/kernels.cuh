@@ -341,25 +341,31 @@ __device__ __forceinline__ void spmv_row(const DMat& A, const T* __restrict__ va
     const int e0 = __ldg(A.start + sl) + lane, e1 = __ldg(A.start + sl + 1);
     if constexpr (W > 0)
     {
-        int col[W];
-        T v[W];
+        // entries in groups of at most 8 (wide rows stay in registers)
+        constexpr int CH = W > 8 ? 8 : W;
 #pragma unroll
-        for (int k = 0; k < W; ++k)
+        for (int k0 = 0; k0 < W; k0 += CH)
         {
-            const int e = e0 + 32 * k;
-            col[k] = e < e1 ? __ldg(A.col + e) : -1;
-            v[k] = e < e1 ? __ldg(val + e) : T(0);
+            int col[CH];
+            T v[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+            {
+                const int e = e0 + 32 * (k0 + k);
+                col[k] = (k0 + k < W && e < e1) ? __ldg(A.col + e) : -1;
+                v[k] = (k0 + k < W && e < e1) ? __ldg(val + e) : T(0);
+            }
+            T xv[NC][CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+#pragma unroll
+                for (int q = 0; q < NC; ++q) xv[q][k] = col[k] >= 0 ? __ldg(x[q] + col[k]) : T(0);
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+                if (col[k] >= 0)
+#pragma unroll
+                    for (int q = 0; q < NC; ++q) y[q] += static_cast<double>(v[k] * xv[q][k]);
         }
-        T xv[NC][W];
-#pragma unroll
-        for (int k = 0; k < W; ++k)
-#pragma unroll
-            for (int q = 0; q < NC; ++q) xv[q][k] = col[k] >= 0 ? __ldg(x[q] + col[k]) : T(0);
-#pragma unroll
-        for (int k = 0; k < W; ++k)
-            if (col[k] >= 0)
-#pragma unroll
-                for (int q = 0; q < NC; ++q) y[q] += static_cast<double>(v[k] * xv[q][k]);
     }
     else
     {
@@ -387,24 +393,31 @@ __device__ __forceinline__ void spmv_row_gather(const DMat& A, const double* __r
     const int e0 = __ldg(A.start + sl) + lane, e1 = __ldg(A.start + sl + 1);
     if constexpr (W > 0)
     {
-        int col[W];
-        double v[W];
+        // entries in groups of at most 8, so that the gathers of wide rows
+        // stay in registers; the sum still runs in entry order
+        constexpr int CH = W > 8 ? 8 : W;
 #pragma unroll
-        for (int k = 0; k < W; ++k)
+        for (int k0 = 0; k0 < W; k0 += CH)
         {
-            const int e = e0 + 32 * k;
-            col[k] = e < e1 ? __ldg(A.col + e) : -1;
-            v[k] = e < e1 ? __ldg(val + e) : 0.0;
-        }
+            int col[CH];
+            double v[CH];
 #pragma unroll
-        for (int k = 0; k < W; ++k)
-            if (col[k] >= 0)
+            for (int k = 0; k < CH; ++k)
             {
-                double xv[NC];
-                gather(col[k], xv);
-#pragma unroll
-                for (int q = 0; q < NC; ++q) y[q] += v[k] * xv[q];
+                const int e = e0 + 32 * (k0 + k);
+                col[k] = (k0 + k < W && e < e1) ? __ldg(A.col + e) : -1;
+                v[k] = (k0 + k < W && e < e1) ? __ldg(val + e) : 0.0;
             }
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+                if (col[k] >= 0)
+                {
+                    double xv[NC];
+                    gather(col[k], xv);
+#pragma unroll
+                    for (int q = 0; q < NC; ++q) y[q] += v[k] * xv[q];
+                }
+        }
     }
     else
     {

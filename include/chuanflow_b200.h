@@ -294,10 +294,10 @@ int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
  * iterations are launched one by one rather than as CUDA graphs.  Enabling
  * clears the counts; cfg_kernel_stats gives {launches, total ms} for, in
  * order: the PCG SpMV + p.Ap, the x/r update + norms + r.z, the
- * search-direction update; the five BiCGStab kernels (p/z update, v = Az,
- * s/s^ update, t = As^, x/r update); the whole DIC application z = M^-1 r. */
+ * search-direction update; the four BiCGStab kernels (p/z update, v = Az,
+ * t = As^, x/r update); the whole DIC application z = M^-1 r. */
 int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable);
-int cfg_kernel_stats(const cfg_ctx* ctx, double out[18]);
+int cfg_kernel_stats(const cfg_ctx* ctx, double out[16]);
 
 /* ---- the linear-solver call surface ------------------------------------ */
 
