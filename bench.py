@@ -517,6 +517,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="run --steps outer iterations from the initial state with no warm-up, timing or "
                          "baselines: the command line the ncu captures run")
+    ap.add_argument("--profile-warm", type=int, default=0,
+                    help="with --profile: outer iterations run before the profiler range opens")
     ap.add_argument("--workload", default="simple", choices=["simple", "poisson", "blocks", "transient"],
                     help="simple: the 2M-cell SIMPLE cavity (the headline); poisson: the ~4M-tet "
                          "pressure-Poisson solve, FP64 DIC-PCG vs FP32-in-FP64 refinement; blocks: 64 detail "
@@ -554,10 +556,20 @@ def main():
     mesh, case, ctl = make_case(n, local, args.p_precond)
     ncell = mesh.n_cells
     if args.profile:
+        import torch
+        # --profile-warm W outer iterations first, outside the profiler range
+        # (ncu --profile-from-start off captures only the --steps after them)
+        for _ in range(args.profile_warm):
+            case.solve(ctl)
+        torch.cuda.synchronize(local)
+        torch.cuda.profiler.start()
         for _ in range(args.steps):
             r = case.solve(ctl)
+        torch.cuda.synchronize(local)
+        torch.cuda.profiler.stop()
         print(json.dumps({"profile": workload_config(n, args.p_precond)["workload"], "steps": args.steps,
-                          "u_inner": r.u_inner_iterations, "p_inner": r.p_inner_iterations}))
+                          "warm": args.profile_warm, "u_inner": r.u_inner_iterations,
+                          "p_inner": r.p_inner_iterations}))
         return
     for _ in range(max(3, args.warmup)):
         case.solve(ctl)
