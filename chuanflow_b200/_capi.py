@@ -389,10 +389,18 @@ class SimpleCase:
                                        _dp(_f64(p)) if p is not None else None,
                                        _dp(_f64(phi)) if phi is not None else None))
 
-    def download(self):
-        U = np.zeros((self.mesh.n_cells, 3))
-        p = np.zeros(self.mesh.n_cells)
-        phi = np.zeros(self.mesh.n_faces)
+    def download(self, U=None, p=None, phi=None):
+        """U (n_cells x 3), p and phi; given arrays (C-contiguous float64 of
+        those shapes, e.g. pinned buffers) are filled in place."""
+        def out(a, shape):
+            if a is None:
+                return np.empty(shape)
+            if a.dtype != np.float64 or a.shape != shape or not a.flags.c_contiguous or not a.flags.writeable:
+                raise ValueError(f"download: expected a writeable C-contiguous float64 array of shape {shape}")
+            return a
+        U = out(U, (self.mesh.n_cells, 3))
+        p = out(p, (self.mesh.n_cells,))
+        phi = out(phi, (self.mesh.n_faces,))
         _check(lib().cfg_fields_download(self._h, _dp(U), _dp(p), _dp(phi)))
         return U, p, phi
 

@@ -226,6 +226,12 @@ private:
     std::vector<double> hostTmp_;
     void toDevCells(double* dev, const double* host, int stride, int off);
     void fromDevCells(double* host, const double* dev, int stride, int off);
+    // whole cell fields of nc = 1 or 3 interleaved components: one copy of the
+    // host array through ioStage_, transposed and renumbered on the device
+    void cellsToDev(double* const* dev, int nc, const double* host);
+    void cellsFromDev(double* host, const double* const* dev, int nc);
+    double* ioStage_ = nullptr;  // 3 nC doubles
+    int* dPerm_ = nullptr;       // perm_ on the device; null for the identity
     int deviceCell(int64_t c) const;
     std::vector<Vec> uVal_;
     std::vector<double> pVal_;

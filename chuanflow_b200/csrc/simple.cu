@@ -697,6 +697,8 @@ void Ctx::buildDevice()
         for (int i = 0; i < nC; ++i) inv_[perm_[i]] = i;
         identityOrder_ = true;
         for (int i = 0; i < nC && identityOrder_; ++i) identityOrder_ = perm_[i] == i;
+        ioStage_ = alloc<double>(3 * static_cast<size_t>(nC));
+        dPerm_ = identityOrder_ ? nullptr : upload(perm_);
     }
     const std::vector<int>& perm = perm_;
     const std::vector<int>& inv = inv_;
@@ -1756,12 +1758,86 @@ void Ctx::fromDevCells(double* host, const double* dev, int stride, int off)
 
 int Ctx::deviceCell(int64_t c) const { return c < 0 ? -1 : inv_[static_cast<size_t>(c)]; }
 
+/// dev[q][i] = aos[perm[i] nc + q]: interleaved original-order cell values to
+/// device-numbered component arrays (perm null: the identity)
+__global__ void k_cells_scatter(int n, int nc, const int* __restrict__ perm, const double* __restrict__ aos,
+                                double* d0, double* d1, double* d2)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const size_t o = static_cast<size_t>(perm ? perm[i] : i) * nc;
+        d0[i] = aos[o];
+        if (nc == 3)
+        {
+            d1[i] = aos[o + 1];
+            d2[i] = aos[o + 2];
+        }
+    }
+}
+
+/// The inverse of k_cells_scatter.
+__global__ void k_cells_gather(int n, int nc, const int* __restrict__ perm, double* __restrict__ aos,
+                               const double* s0, const double* s1, const double* s2)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const size_t o = static_cast<size_t>(perm ? perm[i] : i) * nc;
+        aos[o] = s0[i];
+        if (nc == 3)
+        {
+            aos[o + 1] = s1[i];
+            aos[o + 2] = s2[i];
+        }
+    }
+}
+
+void Ctx::cellsToDev(double* const* dev, int nc, const double* host)
+{
+    const int nC = dm_.nC;
+    if (nc == 1 && identityOrder_)
+    {
+        CFG_CUDA(cudaMemcpyAsync(dev[0], host, nC * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        return;
+    }
+    CFG_CUDA(cudaMemcpyAsync(ioStage_, host, static_cast<size_t>(nC) * nc * sizeof(double), cudaMemcpyHostToDevice,
+                             stream_));
+    k_cells_scatter<<<GS_, TPB, 0, stream_>>>(nC, nc, dPerm_, ioStage_, dev[0], nc == 3 ? dev[1] : nullptr,
+                                              nc == 3 ? dev[2] : nullptr);
+    launchCheck("cells_scatter");
+}
+
+void Ctx::cellsFromDev(double* host, const double* const* dev, int nc)
+{
+    const int nC = dm_.nC;
+    if (nc == 1 && identityOrder_)
+    {
+        CFG_CUDA(cudaMemcpyAsync(host, dev[0], nC * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        return;
+    }
+    k_cells_gather<<<GS_, TPB, 0, stream_>>>(nC, nc, dPerm_, ioStage_, dev[0], nc == 3 ? dev[1] : nullptr,
+                                             nc == 3 ? dev[2] : nullptr);
+    launchCheck("cells_gather");
+    CFG_CUDA(cudaMemcpyAsync(host, ioStage_, static_cast<size_t>(nC) * nc * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
+}
+
+/// Fields in: one host-to-device copy per field (from the caller's buffers,
+/// pinned or not), then the device transposes and renumbers.  The stage is
+/// shared, so each field's scatter runs before the next copy overwrites it
+/// (both are ordered on the context's stream).
 void Ctx::upload(const double* U, const double* p, const double* phi)
 {
     const int nF = dm_.nF;
     if (U)
-        for (int q = 0; q < 3; ++q) toDevCells(U_.c[q], U, 3, q);
-    if (p) toDevCells(p_, p, 1, 0);
+    {
+        double* const d[3] = {U_.c[0], U_.c[1], U_.c[2]};
+        cellsToDev(d, 3, U);
+    }
+    if (p)
+    {
+        double* const d[1] = {p_};
+        cellsToDev(d, 1, p);
+    }
     if (phi) CFG_CUDA(cudaMemcpyAsync(phi_, phi, nF * sizeof(double), cudaMemcpyHostToDevice, stream_));
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -1770,8 +1846,15 @@ void Ctx::download(double* U, double* p, double* phi)
 {
     const int nF = dm_.nF;
     if (U)
-        for (int q = 0; q < 3; ++q) fromDevCells(U, U_.c[q], 3, q);
-    if (p) fromDevCells(p, p_, 1, 0);
+    {
+        const double* const s[3] = {U_.c[0], U_.c[1], U_.c[2]};
+        cellsFromDev(U, s, 3);
+    }
+    if (p)
+    {
+        const double* const s[1] = {p_};
+        cellsFromDev(p, s, 1);
+    }
     if (phi) CFG_CUDA(cudaMemcpyAsync(phi, phi_, nF * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
