@@ -5,8 +5,7 @@
 #include <string>
 #include <vector>
 
-#include "cf/common/Error.h"
-#include "chuanflow_b200.h"
+#include "cf_gpu_common.h"
 
 namespace cf
 {
@@ -15,13 +14,8 @@ namespace gpu
 namespace
 {
 
-void check(int status, const char* what)
-{
-    if (status == CFG_OK) return;
-    char buf[1024];
-    cfg_last_error(buf, sizeof buf);
-    throw Error(std::string("chuanflow_b200 ") + what + ": " + buf);
-}
+using detail::check;
+using detail::toSchemes;
 
 int bcType(const std::string& s)
 {
@@ -33,24 +27,6 @@ int bcType(const std::string& s)
     if (s == "wall") return CFG_BC_WALL;
     if (s == "empty") return CFG_BC_EMPTY;
     throw Error("chuanflow_b200: unknown patch bc type '" + s + "'");
-}
-
-cfg_schemes toSchemes(const Schemes& s)
-{
-    // names the reference does not know select its defaults, as its own
-    // string tests do (divScheme.cpp:18, laplacianScheme.cpp:71,
-    // gradScheme.cpp:251-275); "linearUpwind" is this library's extension
-    cfg_schemes out{};
-    out.div = s.div == "linear" ? CFG_DIV_LINEAR
-              : s.div == "blend" ? CFG_DIV_BLEND
-              : s.div == "linearUpwind" ? CFG_DIV_LINEAR_UPWIND
-                                        : CFG_DIV_UPWIND;
-    out.laplacian_corrected = s.laplacian == "corrected" ? 1 : 0;
-    out.grad = s.grad == "leastSquares" ? CFG_GRAD_LEAST_SQUARES
-               : s.grad == "corrected" ? CFG_GRAD_CORRECTED
-                                       : CFG_GRAD_LINEAR;
-    out.blend_coeff = s.blendCoeff;
-    return out;
 }
 
 }  // namespace
@@ -160,21 +136,7 @@ SimpleResult SimpleSession::solve(volVectorField& U, volScalarField& p, surfaceS
     }
     check(cfg_fields_upload(c_, u.data(), p.internalField().data(), phi.values().data()), "cfg_fields_upload");
 
-    cfg_simple_controls cc{};
-    cc.max_iterations = ctl.maxIterations;
-    cc.continuity_tol = ctl.continuityTol;
-    cc.pcorr_tol = ctl.pcorrTol;
-    cc.momentum_tol = ctl.momentumTol;
-    cc.linear_tol = ctl.linearTol;
-    cc.linear_max_iter = ctl.linearMaxIter;
-    cc.non_orth_correctors = ctl.nonOrthCorrectors;
-    cc.relax_u = ctl.relaxU;
-    cc.relax_p = ctl.relaxP;
-    cc.p_relax_start = ctl.pRelaxStart;
-    cc.body_force[0] = ctl.bodyForce.x;
-    cc.body_force[1] = ctl.bodyForce.y;
-    cc.body_force[2] = ctl.bodyForce.z;
-    cc.nu = nu;
+    cfg_simple_controls cc = detail::toControls(ctl, nu);
     cc.p_precond = opt_.dicPressure ? CFG_PRECOND_DIC : CFG_PRECOND_JACOBI;
     cc.verbose = opt_.verbose ? 1 : 0;
     cc.p_ref_cell = opt_.pRefCell;

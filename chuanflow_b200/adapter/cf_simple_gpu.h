@@ -46,6 +46,10 @@ public:
     SimpleResult solve(volVectorField& U, volScalarField& p, surfaceScalarField& phi, scalar nu,
                        const Schemes& schemes, const SimpleControls& ctl);
 
+    /// The session's C ABI context (owned by the session), for the calls
+    /// this class does not wrap: detail blocks, batches, turbulence.
+    cfg_ctx* context() const { return c_; }
+
 private:
     const polyMesh& mesh_;
     Options opt_;

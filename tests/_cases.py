@@ -329,3 +329,35 @@ def grouped_box_file(path, n=3):
     groups = [("inlet", sides["xmin"], False), ("outlet", sides["xmax"], True),
               ("walls", sides["ymin"] + sides["ymax"] + sides["zmin"] + sides["zmax"], False)]
     write_msh22_groups(path, pts, hexes, groups)
+
+
+def _duct_block(L, W, H, cells):
+    walls = "\n".join(f"        {s} {{ name w{k}; type wall; }}" for k, s in enumerate(("ymin", "ymax", "zmin", "zmax")))
+    return (f"block\n    {{\n        min (0 0 0);\n        max ({L!r} {W!r} {H!r});\n"
+            f"        cells ({cells[0]} {cells[1]} {cells[2]});\n"
+            f"        xmin {{ name inlet; type inlet; }}\n        xmax {{ name outlet; type outlet; }}\n{walls}\n    }}")
+
+
+def coupled_network_dict(passes=6, sweeps=60, turbulent=False):
+    """The coupled-network case of oracle/coupled_driver.cpp: a rate of 2e-3
+    m3/s through Src -In- J1 -{X1 || X2 || X3}- J2 -Out- Snk, every X a
+    detailed duct block (three sections, the three inlet profiles) warm
+    started pass after pass, `sweeps` SIMPLE iterations per lossAt.  With
+    `turbulent`, X3 is a k-epsilon block at a low viscosity."""
+    blocks = [("X1", (1.0, 0.1, 0.1), (24, 6, 6), 1e-4, "parabolic", ""),
+              ("X2", (0.8, 0.08, 0.1), (20, 5, 6), 1e-4, "flat", ""),
+              ("X3", (0.6, 0.1, 0.12), (16, 6, 7), 1e-4, "power1over7", "")]
+    if turbulent:
+        blocks[2] = ("X3", (1.0, 0.1, 0.1), (12, 5, 5), 2.5e-6, "flat",
+                     "turbulence { model kEpsilon; intensity 0.05; relaxation 0.7; }")
+    body = "\n".join(f"    {n}\n    {{\n    {_duct_block(*g, c)}\n        nu {nu!r}; rho 800; shape {sh}; "
+                     f"resistance 10000;\n        {tb}\n    }}" for n, g, c, nu, sh, tb in blocks)
+    return f"""network {{ qIn 0.002; pOut 100000; rho 800; mu 0.08; rIn 10000; rOut 10000; }}
+coupling {{ maxOuterIterations {passes}; relax 1; tolerance 1e-9; accelerate no; }}
+schemes {{ ddt steady; div upwind; laplacian corrected; grad corrected; }}
+simple {{ maxIterations {sweeps}; relaxU 0.7; relaxP 0.3; pRelaxStart 0.02; nonOrthCorrectors 1; linearTol 1e-10; continuityTol 1e-7; }}
+blocks
+{{
+{body}
+}}
+"""

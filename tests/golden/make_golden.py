@@ -27,6 +27,12 @@ Fixtures (small .npz files):
                            with random p and U
   rans_channel.npz         12x5x5 orthogonal channel at Re_H 2e4 with the reference's k-epsilon:
                            5 SIMPLE iterations (U, p, phi, k, epsilon, nut, nu + nut on faces)
+  coupled_laminar.npz      the reference's solveCoupled1d3d over three laminar DetailBlocks in
+                           parallel (oracle/_ref/cf_coupled_driver): per pass and edge q, drop,
+                           coefficient, sweeps
+  coupled_kepsilon.npz     the same with the third block a k-epsilon duct
+
+`python tests/golden/make_golden.py coupled` rebuilds only the two coupled fixtures.
 """
 import os
 import subprocess
@@ -258,9 +264,31 @@ def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
         print("wrote", name, rep[:4])
 
 
+def coupled_npz(name, text):
+    """solveCoupled1d3d with the reference's DetailBlock partners."""
+    drv = os.path.join(ROOT, "oracle", "_ref", "cf_coupled_driver")
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(text)
+        subprocess.run([drv, cp, td], check=True, stdout=subprocess.DEVNULL)
+        lines = open(os.path.join(td, "history.txt")).read().split("\n")
+    rows = [list(map(float, ln.split())) for ln in lines if ln and not ln.startswith("result")]
+    res = [ln for ln in lines if ln.startswith("result")][0].split()[1:]
+    np.savez_compressed(os.path.join(HERE, name), dict=np.array(text), history=np.array(rows),
+                        iterations=int(res[0]), converged=int(res[1]), residual=float(res[2]))
+
+
+def coupled_fixtures():
+    coupled_npz("coupled_laminar.npz", K.coupled_network_dict())
+    coupled_npz("coupled_kepsilon.npz", K.coupled_network_dict(turbulent=True))
+
+
 def main():
     if not O.have_ref():
         sys.exit("oracle/_ref/cf_ref_driver missing: run `make -C oracle` where the reference is present")
+    if sys.argv[1:] == ["coupled"]:
+        coupled_fixtures()
+        return
     mesh_npz("mesh_block_2x2x2.npz", "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\n")
     mesh_npz("mesh_tets22.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeTets_22.msh"; }}\n', grad_fields=True)
     mesh_npz("mesh_hex41.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeHex_41.msh"; }}\n', grad_fields=True)
@@ -318,6 +346,7 @@ def main():
     solve_npz("solve_cg.npz", "cg", rs, cols, vals, b, np.zeros(n), 1e-10, 500)
     rs, cols, vals = K.test_matrix(n, rng, symmetric=False)
     solve_npz("solve_bicgstab.npz", "bicgstab", rs, cols, vals, b, np.zeros(n), 1e-10, 500)
+    coupled_fixtures()
 
 
 if __name__ == "__main__":

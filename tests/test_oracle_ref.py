@@ -3,6 +3,7 @@ reference: bit-for-bit against the golden fixtures the reference produced,
 and, where the reference driver is built (oracle/_ref), against fresh runs
 of the reference on cases the fixtures do not cover.  CPU only."""
 import os
+import subprocess
 import tempfile
 
 import numpy as np
@@ -183,3 +184,21 @@ def test_jitter_and_blockmesh_match_fresh_reference():
         assert np.array_equal(getattr(case.mesh, k), r[k])
     for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
         assert np.array_equal(getattr(case.mesh, k), r[k]), k
+
+
+COUPLED = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "cf_coupled_driver")
+
+
+@pytest.mark.skipif(not os.path.exists(COUPLED), reason="oracle/_ref/cf_coupled_driver not built")
+def test_coupled_fixture_matches_fresh_reference(golden):
+    """The reference's coupled interface over its own DetailBlocks, rerun
+    here, gives the laminar fixture's history to the last bit."""
+    g = golden("coupled_laminar.npz")
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(str(g["dict"]))
+        subprocess.run([COUPLED, cp, td], check=True, stdout=subprocess.DEVNULL, timeout=300)
+        lines = open(os.path.join(td, "history.txt")).read().split("\n")
+    rows = np.array([list(map(float, ln.split())) for ln in lines if ln and not ln.startswith("result")])
+    assert np.array_equal(rows, g["history"])
