@@ -563,15 +563,21 @@ def _detail_loss(self, q, controls):
     return m.as_dict()
 
 
-def _turbulence_setup(self, model="kEpsilon", intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=1e-4):
-    """RansModel::create for this case (model kEpsilon | laminar): call after
-    the velocity conditions are set; advanced once per SIMPLE iteration."""
+def _turbulence_setup(self, model="kEpsilon", intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=1e-4,
+                      c_des=0.61, re_onset=0.0, onset_width=-1.0, gamma_rate=4.0):
+    """RansModel::create for this case (model kEpsilon | kOmegaSST | des |
+    gammaTransition | laminar): call after the velocity conditions are set;
+    advanced once per SIMPLE iteration.  c_des (des) and re_onset,
+    onset_width, gamma_rate (gammaTransition) are TurbulenceConfig's."""
+    _check(lib().cfg_turbulence_params(self._h, C.c_double(c_des), C.c_double(re_onset), C.c_double(onset_width),
+                                       C.c_double(gamma_rate)))
     _check(lib().cfg_turbulence_setup(self._h, model.encode(), C.c_double(intensity), C.c_double(length_scale),
                                       C.c_double(relaxation), C.c_double(nu)))
 
 
 def _turbulence_fields(self):
-    """k, epsilon, nut (cells) and nu + nut on faces."""
+    """k, the dissipation variable (key "eps": epsilon, or omega for
+    kOmegaSST), nut (cells) and nu + nut on faces."""
     n, f = self.mesh.n_cells, self.mesh.n_faces
     k, e, nut, nuf = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(f)
     _check(lib().cfg_turbulence_fields(self._h, _dp(k), _dp(e), _dp(nut), _dp(nuf)))

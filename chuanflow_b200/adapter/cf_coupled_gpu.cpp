@@ -34,6 +34,7 @@ GpuDetailBlock::GpuDetailBlock(polyMesh mesh, scalar nu, scalar rho, const Schem
     const cfg_schemes sc = detail::toSchemes(schemes);
     check(cfg_set_schemes(c, &sc), "cfg_set_schemes");
     check(cfg_detail_setup(c, inletShape.c_str(), rho), "cfg_detail_setup");
+    check(cfg_turbulence_params(c, turb.cDES, turb.reOnset, turb.onsetWidth, turb.gammaRate), "cfg_turbulence_params");
     if (turb.model != "laminar")
         check(cfg_detail_turbulence(c, turb.model.c_str(), turb.intensity, turb.lengthScale, turb.relaxation, nu),
               "cfg_detail_turbulence");

@@ -34,8 +34,9 @@ namespace gpu
 {
 
 /// A detailed region on the device.  Covers the DetailBlock configurations
-/// of a Newtonian, steady, incompressible region: laminar or k-epsilon, inlet
-/// profile "flat", "parabolic" or "power1over7".  A case that declares
+/// of a Newtonian, steady, incompressible region: laminar or one of the RANS
+/// models kEpsilon, kOmegaSST, des, gammaTransition; inlet profile "flat",
+/// "parabolic" or "power1over7".  A case that declares
 /// anything else (a rheology, phases, a compressible or thermal region, an
 /// Euler ddt) is refused at construction with cf::Error.  The probe range of
 /// DetailBlock only feeds diagnostics that solveCoupled1d3d does not read and

@@ -885,6 +885,14 @@ int cfg_turbulence_setup(cfg_ctx* ctx, const char* model, double intensity, doub
     });
 }
 
+int cfg_turbulence_params(cfg_ctx* ctx, double c_des, double re_onset, double onset_width, double gamma_rate)
+{
+    return guard([&] {
+        need(ctx, "cfg_turbulence_params: null argument");
+        ctx->c->turbulenceParams(c_des, re_onset, onset_width, gamma_rate);
+    });
+}
+
 int cfg_turbulence_fields(cfg_ctx* ctx, double* k, double* eps, double* nut, double* nuEffFace)
 {
     return guard([&] {
@@ -976,7 +984,9 @@ int cfg_write_vtu(cfg_ctx* ctx, const char* path, int32_t binary)
         c.download(f[1].data.data(), f[0].data.data(), nullptr);
         if (c.hasTurbulence())
         {
-            f.insert(f.begin() + 1, {{"k", 1, std::vector<double>(nC)}, {"epsilon", 1, std::vector<double>(nC)},
+            // the dissipation variable under the model's own name
+            const char* dn = c.turbulenceModelName() == "kOmegaSST" ? "omega" : "epsilon";
+            f.insert(f.begin() + 1, {{"k", 1, std::vector<double>(nC)}, {dn, 1, std::vector<double>(nC)},
                                      {"nut", 1, std::vector<double>(nC)}});
             c.turbulenceFields(f[1].data.data(), f[2].data.data(), f[3].data.data(), nullptr);
         }

@@ -72,7 +72,9 @@ public:
     void turbulenceSetup(const std::string& model, double intensity, double lengthScale, double relaxation,
                          double nu);
     void turbulenceFields(double* k, double* eps, double* nut, double* nuEffFace);
+    void turbulenceParams(double cDES, double reOnset, double onsetWidth, double gammaRate);
     bool hasTurbulence() const { return static_cast<bool>(turb_); }
+    std::string turbulenceModelName() const;
 
     /// The learned pressure preconditioner (mpnn.cu) on the context's
     /// pressure matrix (the Poisson system or the last SIMPLE equation).
@@ -204,7 +206,11 @@ private:
     unsigned* fcgTicket_ = nullptr;
     void turbCorrect(int64_t& inner);
     void turbRefreshNut();
-    void turbSolveScalar(double sigma, bool isK, double* field, double floorV, int64_t& inner);
+    void turbSolveScalar(const double* bc, const double* bk, const double* sigCell, double sigma, bool wallOverride,
+                         const double* src2, double* field, double floorV, bool clamp01, int64_t& inner);
+    double turbURef();
+    // the model options of TurbulenceConfig beyond cfg_turbulence_setup's
+    double turbCDES_ = 0.61, turbReOnset_ = 0.0, turbOnsetWidth_ = -1.0, turbGammaRate_ = 4.0;
     double* saved_ = nullptr;
     V3P uOld_{};
     double* savedT_ = nullptr;

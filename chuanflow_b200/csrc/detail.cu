@@ -320,8 +320,10 @@ void Ctx::detailTurbulence(const std::string& model, double intensity, double le
                            double nu)
 {
     if (!detail_) fail(CFG_EINVAL, "cfg_detail_turbulence: call cfg_detail_setup first");
-    if (model != "laminar" && model != "kEpsilon")
-        fail(CFG_ESETUP, "turbulence: model '" + model + "' is not on the GPU path (laminar | kEpsilon)");
+    if (model != "laminar" && model != "kEpsilon" && model != "kOmegaSST" && model != "des" &&
+        model != "gammaTransition")
+        fail(CFG_ESETUP, "turbulence: model '" + model +
+                             "' is not on the GPU path (laminar | kEpsilon | kOmegaSST | des | gammaTransition)");
     detail_->turbModel = model;
     detail_->turbIntensity = intensity;
     detail_->turbLength = lengthScale;
@@ -342,7 +344,7 @@ void Ctx::saveState()
     savedTurb_ = turb_ != nullptr;
     if (savedTurb_)
     {
-        if (!savedT_) savedT_ = alloc<double>(3 * nC);
+        if (!savedT_) savedT_ = alloc<double>(4 * nC);
         turbCopy(savedT_, true);
     }
     CFG_CUDA(cudaStreamSynchronize(stream_));

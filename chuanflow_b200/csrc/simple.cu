@@ -1202,6 +1202,9 @@ void Ctx::launchCheck(const char* what, int kernels)
 /// volScalarField overload's internal face value for the linear scheme.
 void Ctx::gradCells(const double* const* x, int nComp, const BcTab& bc, int scheme, bool volQuirk, V3P* out)
 {
+    // the kernels come in one- and three-field forms; any other count would
+    // leave output pointers unset
+    if (nComp != 1 && nComp != 3) fail(CFG_EINVAL, "gradCells: one or three fields per call");
     CV3P xs{{x[0], nComp > 1 ? x[1] : x[0], nComp > 2 ? x[2] : x[0]}};
     Grad3 o{};
     for (int q = 0; q < nComp; ++q) o.g[q] = out[q];

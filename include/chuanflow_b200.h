@@ -415,19 +415,28 @@ int cfg_write_vtu(cfg_ctx* ctx, const char* path, int32_t binary);
 
 /* ---- RANS turbulence -------------------------------------------------------- */
 
-/* RansModel::create + KEpsilon (src/3d/src/turbulence/turbulenceModel.cpp,
- * kEpsilon.cpp, wallFunction.cpp): model "kEpsilon" (standard constants,
- * Spalding wall functions on patches of type "wall", k and epsilon fixed on
- * patches of type "inlet") or "laminar" (removes a model).  Set up after the
- * velocity conditions: the initial k = 1.5 (U_inlet intensity)^2 and
- * epsilon = Cmu^0.25 k^1.5 / L (L = length_scale, or 7% of the box diagonal
+/* RansModel::create (src/3d/src/turbulence/turbulenceModel.cpp:54-104,
+ * wallFunction.cpp) with model "kEpsilon" (kEpsilon.cpp), "kOmegaSST"
+ * (kOmegaSST.cpp: Menter 2003 blend with the shortest-path cell wall
+ * distance), "des" (desModel.cpp: the shielded length on k-epsilon) or
+ * "gammaTransition" (transitionModel.cpp: k-epsilon with an intermittency
+ * equation), or "laminar" (removes a model).  Spalding wall functions on
+ * patches of type "wall"; k and the dissipation variable fixed on patches of
+ * type "inlet".  Set up after the velocity conditions: the initial k = 1.5
+ * (U_inlet intensity)^2 and epsilon = Cmu^0.25 k^1.5 / L, or for kOmegaSST
+ * omega = k^0.5 / (Cmu^0.25 L) (L = length_scale, or 7% of the box diagonal
  * when length_scale <= 0).  The model is then advanced once per SIMPLE outer
  * iteration and supplies nu + nut on faces to the momentum equation
  * (simpleSolver.cpp:52, :97); `nu` is the molecular viscosity. */
 int cfg_turbulence_setup(cfg_ctx* ctx, const char* model, double intensity, double length_scale, double relaxation,
                          double nu);
-/* k, epsilon, nut (nCells, original order) and nu + nut on faces (nFaces);
- * any pointer may be NULL. */
+/* TurbulenceConfig's model options (TurbulenceModel.h:50-59), taken by the
+ * next cfg_turbulence_setup (or detail-block model) of this context: C_DES
+ * (des, default 0.61), reOnset, onsetWidth and gammaRate (gammaTransition;
+ * defaults 0, -1 = 5% of the onset distance, 4). */
+int cfg_turbulence_params(cfg_ctx* ctx, double c_des, double re_onset, double onset_width, double gamma_rate);
+/* k, the dissipation variable (epsilon; omega for kOmegaSST), nut (nCells,
+ * original order) and nu + nut on faces (nFaces); any pointer may be NULL. */
 int cfg_turbulence_fields(cfg_ctx* ctx, double* k, double* eps, double* nut, double* nu_eff_face);
 
 /* ---- learned pressure preconditioner (no reference counterpart) ------------ */

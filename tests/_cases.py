@@ -245,20 +245,25 @@ def write_msh22(path, points, cells, cell_type=4):
         f.write("$EndElements\n")
 
 
-def rans_channel_dict(nx=12, ny=5, nz=5, iters=5):
-    """The orthogonal channel at Re_H = 0.5 * 0.1 / 2.5e-6 = 2e4 with the
-    reference's k-epsilon (5% intensity, the automatic length scale); on the
-    jittered 5x5 section the reference's own k-epsilon diverges."""
+RANS_OPTIONS = {"kEpsilon": "", "kOmegaSST": "", "des": "C_DES 0.61; ",
+                "gammaTransition": "reOnset 20000; gammaRate 4; "}
+
+
+def rans_channel_dict(nx=12, ny=5, nz=5, iters=5, model="kEpsilon"):
+    """The orthogonal channel at Re_H = 0.5 * 0.1 / 2.5e-6 = 2e4 with one of
+    the reference's RANS models (5% intensity, the automatic length scale);
+    on the jittered 5x5 section the reference's own k-epsilon diverges."""
     t = channel_dict(nx, ny, nz, nu=2.5e-6, iters=iters, non_orth=1, L=(1.0, 0.1, 0.1))
     t = t.replace("inlet  { U (0.1 0 0);", "inlet  { U (0.5 0 0);")
-    return t + "turbulence { model kEpsilon; intensity 0.05; relaxation 0.7; }\n"
+    return t + f"turbulence {{ model {model}; {RANS_OPTIONS[model]}intensity 0.05; relaxation 0.7; }}\n"
 
 
-def rans_channel_product(nx=12, ny=5, nz=5):
+def rans_channel_product(nx=12, ny=5, nz=5, model="kEpsilon"):
     mesh, case = channel_product(nx, ny, nz, jitter=0.0, L=(1.0, 0.1, 0.1))
     case.set_patch_bc("U", "inlet", "fixedValue", (0.5, 0, 0))
     case.init_flux()
-    case.turbulence_setup("kEpsilon", intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=2.5e-6)
+    case.turbulence_setup(model, intensity=0.05, length_scale=-1.0, relaxation=0.7, nu=2.5e-6, c_des=0.61,
+                          re_onset=20000.0, gamma_rate=4.0)
     return mesh, case
 
 

@@ -31,8 +31,11 @@ Fixtures (small .npz files):
                            parallel (oracle/_ref/cf_coupled_driver): per pass and edge q, drop,
                            coefficient, sweeps
   coupled_kepsilon.npz     the same with the third block a k-epsilon duct
+  rans_sst.npz, rans_des.npz, rans_transition.npz   the rans_channel case with the reference's
+                           k-omega SST, DES and gamma-transition models
 
-`python tests/golden/make_golden.py coupled` rebuilds only the two coupled fixtures.
+`python tests/golden/make_golden.py coupled` (or `rans`) rebuilds only the coupled (or the
+three extra RANS) fixtures.
 """
 import os
 import subprocess
@@ -278,6 +281,12 @@ def coupled_npz(name, text):
                         iterations=int(res[0]), converged=int(res[1]), residual=float(res[2]))
 
 
+def rans_fixtures():
+    rc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0)
+    for model, name in (("kOmegaSST", "rans_sst"), ("des", "rans_des"), ("gammaTransition", "rans_transition")):
+        rans_npz(name + ".npz", K.rans_channel_dict(model=model), rc.mesh.points)
+
+
 def coupled_fixtures():
     coupled_npz("coupled_laminar.npz", K.coupled_network_dict())
     coupled_npz("coupled_kepsilon.npz", K.coupled_network_dict(turbulent=True))
@@ -288,6 +297,9 @@ def main():
         sys.exit("oracle/_ref/cf_ref_driver missing: run `make -C oracle` where the reference is present")
     if sys.argv[1:] == ["coupled"]:
         coupled_fixtures()
+        return
+    if sys.argv[1:] == ["rans"]:
+        rans_fixtures()
         return
     mesh_npz("mesh_block_2x2x2.npz", "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\n")
     mesh_npz("mesh_tets22.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeTets_22.msh"; }}\n', grad_fields=True)
@@ -329,6 +341,7 @@ def main():
     piso_npz("piso_channel.npz", K.piso_channel_dict(), pc.mesh.points)
     rc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0)
     rans_npz("rans_channel.npz", K.rans_channel_dict(), rc.mesh.points)
+    rans_fixtures()
 
     rng = np.random.default_rng(11)
     m = cav.mesh

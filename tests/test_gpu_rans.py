@@ -1,8 +1,9 @@
-"""The device k-epsilon model (RansModel + KEpsilon + Spalding wall
-functions) inside SIMPLE against the reference's own run of the same
-channel at Re_H 2e4 (tests/golden/rans_channel.npz, made by the compiled
-reference).  The wall functions evaluate exp and pow on the device, so the
-bar is relative, not bit-for-bit."""
+"""The device RANS models (RansModel with KEpsilon, KOmegaSST, DesModel and
+TransitionModel, Spalding wall functions) inside SIMPLE against the
+reference's own runs of the same channel at Re_H 2e4 (tests/golden/rans_*.npz,
+made by the compiled reference).  The wall functions and the SST blend
+evaluate exp, pow, tanh and cbrt on the device, so the bar is relative, not
+bit-for-bit."""
 import numpy as np
 import pytest
 
@@ -18,10 +19,12 @@ def rel(a, b):
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
 
 
-def test_kepsilon_channel_matches_reference(golden):
+@pytest.mark.parametrize("fixture,model", [("rans_channel.npz", "kEpsilon"), ("rans_sst.npz", "kOmegaSST"),
+                                           ("rans_des.npz", "des"), ("rans_transition.npz", "gammaTransition")])
+def test_rans_channel_matches_reference(golden, fixture, model):
     import chuanflow_b200 as cf
-    g = golden("rans_channel.npz")
-    mesh, case = K.rans_channel_product()
+    g = golden(fixture)
+    mesh, case = K.rans_channel_product(model=model)
     assert np.array_equal(mesh.addressing()["points"], g["points"])
     oc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0, nu=2.5e-6, iters=int(g["iterations"]),
                          non_orth=1)
@@ -38,8 +41,12 @@ def test_kepsilon_channel_matches_reference(golden):
 def test_turbulence_setup_errors():
     import chuanflow_b200 as cf
     mesh, case = K.channel_product(6, 3, 3)
-    with pytest.raises(cf.CfgError, match="kOmega"):
-        case.turbulence_setup("kOmegaSST")
+    with pytest.raises(cf.CfgError, match="not on the GPU path"):
+        case.turbulence_setup("spalartAllmaras")
+    with pytest.raises(cf.CfgError, match="reOnset"):
+        case.turbulence_setup("gammaTransition", re_onset=0.0)
+    with pytest.raises(cf.CfgError, match="C_DES"):
+        case.turbulence_setup("des", c_des=0.0)
     with pytest.raises(cf.CfgError, match="relaxation"):
         case.turbulence_setup("kEpsilon", relaxation=1.5)
     with pytest.raises(cf.CfgError, match="no turbulence"):
