@@ -204,10 +204,11 @@ private:
     const double** fcgPtrs_ = nullptr;
     double* fcgOut_ = nullptr;
     unsigned* fcgTicket_ = nullptr;
-    void turbCorrect(int64_t& inner);
+    void turbCorrect(int64_t& inner, double dt = 0.0);
     void turbRefreshNut();
     void turbSolveScalar(const double* bc, const double* bk, const double* sigCell, double sigma, bool wallOverride,
-                         const double* src2, double* field, double floorV, bool clamp01, int64_t& inner);
+                         const double* src2, double* field, double floorV, bool clamp01, double dt,
+                         int64_t& inner);
     double turbURef();
     // the model options of TurbulenceConfig beyond cfg_turbulence_setup's
     double turbCDES_ = 0.61, turbReOnset_ = 0.0, turbOnsetWidth_ = -1.0, turbGammaRate_ = 4.0;

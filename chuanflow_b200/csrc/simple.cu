@@ -2009,10 +2009,13 @@ void Ctx::pisoStep(const cfg_piso_controls& ctl, cfg_piso_result& res)
 {
     CFG_CUDA(cudaSetDevice(device_));
     if (!(ctl.dt > 0)) fail(CFG_EINVAL, "PISO: non-positive time step");
-    if (turb_) fail(CFG_ESETUP, "PISO: a RANS model with a time step is not on the GPU path");
     refreshBc();
     checkMomentumBcs();
-    setNu(ctl.nu);
+    // the RANS model advances first, with the step's dt, and hands the
+    // momentum equation nu + nut on faces (pisoSolver.cpp:29-30)
+    lastTurbInner = 0;
+    if (turb_) turbCorrect(lastTurbInner, ctl.dt);
+    else setNu(ctl.nu);
     std::memset(&res, 0, sizeof res);
     const int nC = dm_.nC;
     const int gs = schemes_.grad;

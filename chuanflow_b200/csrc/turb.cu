@@ -219,14 +219,16 @@ __global__ void __launch_bounds__(TPB) k_turb_src_e(int n, const double* __restr
     }
 }
 
-/// a scalar transport equation div(phi,T) - laplacianFace(gamma,T) + Sp T =
-/// src, in the reference's term order per cell (fvm::div, laplacianFace,
-/// then the source and the implicit Sp)
+/// a scalar transport equation [ddt(T)] + div(phi,T) - laplacianFace(gamma,T)
+/// + Sp T = src, in the reference's term order per cell (fvm::ddt when dt >
+/// 0, divScheme.cpp:64-77; fvm::div; laplacianFace; then the source and the
+/// implicit Sp)
 __global__ void __launch_bounds__(TPB) k_assemble_S(DMesh m, const double* __restrict__ phi,
                                                     const double* __restrict__ gamma, const double* __restrict__ bc,
                                                     const double* __restrict__ bk, double alpha,
                                                     const double* __restrict__ sp, const double* __restrict__ src,
-                                                    const double* __restrict__ src2, double* __restrict__ val,
+                                                    const double* __restrict__ src2, double dt,
+                                                    const double* __restrict__ old, double* __restrict__ val,
                                                     double* __restrict__ diagOut, double* __restrict__ base)
 {
     ROW_LOOP(c, m.nC)
@@ -234,6 +236,12 @@ __global__ void __launch_bounds__(TPB) k_assemble_S(DMesh m, const double* __res
         const int sl = c >> 5, lane = c & 31;
         const int e0 = m.cfStart[sl] + lane, e1 = m.cfStart[sl + 1];
         double diag = 0.0, r = 0.0;
+        if (dt > 0)
+        {
+            const double a = m.V[c] / dt;
+            diag = a;
+            r = a * old[c];
+        }
         for (int e = e0; e < e1; e += 32)  // convection
         {
             const int code = m.cfCode[e];
@@ -903,7 +911,7 @@ void Ctx::turbRefreshNut()
 /// nu + nutWall sigma[owner] unless `wallOverride` is off (the plain
 /// harmonic face gamma of the intermittency).
 void Ctx::turbSolveScalar(const double* bc, const double* bk, const double* sigCell, double sigma, bool wallOverride,
-                          const double* src2, double* field, double floorV, bool clamp01, int64_t& inner)
+                          const double* src2, double* field, double floorV, bool clamp01, double dt, int64_t& inner)
 {
     TurbState& t = *turb_;
     const int nC = dm_.nC;
@@ -919,7 +927,10 @@ void Ctx::turbSolveScalar(const double* bc, const double* bk, const double* sigC
     double* x = ux_.c[0];
     double* base = uBase_.c[0];
     double* rhs = uRhs_.c[0];
-    k_assemble_S<<<G_, TPB, 0, stream_>>>(dm_, phi_, t.gammaF, bc, bk, alpha, t.sp, t.src, src2, mVal_, uDiag_, base);
+    // the old field of a time step is the field itself: it changes only at
+    // the relaxation below
+    k_assemble_S<<<G_, TPB, 0, stream_>>>(dm_, phi_, t.gammaF, bc, bk, alpha, t.sp, t.src, src2, dt, field, mVal_,
+                                         uDiag_, base);
     launchCheck("turb_assemble");
     CFG_CUDA(cudaMemsetAsync(x, 0, nC * sizeof(double), stream_));
     const bool corr = schemes_.laplacian_corrected != 0;
@@ -948,8 +959,9 @@ void Ctx::turbSolveScalar(const double* bc, const double* bk, const double* sigC
     launchCheck("turb_relax");
 }
 
-/// RansModel::correctTurbulence for the model in hand.
-void Ctx::turbCorrect(int64_t& inner)
+/// RansModel::correctTurbulence(dt) for the model in hand (dt = 0 in
+/// SIMPLE, the step's dt in PISO, pisoSolver.cpp:29).
+void Ctx::turbCorrect(int64_t& inner, double dt)
 {
     TurbState& t = *turb_;
     const int nC = dm_.nC;
@@ -987,23 +999,23 @@ void Ctx::turbCorrect(int64_t& inner)
         k_sst_k_coefs<<<G_, TPB, 0, stream_>>>(nC, dm_.V, t.k, t.eps, t.y, CGrad3{{cv(gA_), cv(Hf_), cv(Hf_)}},
                                                t.prod, t.nut, t.nu, t.sig, t.gammaC, t.sp, t.src);
         launchCheck("sst_k_coefs");
-        turbSolveScalar(t.kc, t.kk, t.sig, 0.0, true, nullptr, t.k, kFloor, false, inner);
+        turbSolveScalar(t.kc, t.kk, t.sig, 0.0, true, nullptr, t.k, kFloor, false, dt, inner);
         gradWK();  // with the new k
         k_sst_w_coefs<<<G_, TPB, 0, stream_>>>(nC, dm_.V, t.k, t.eps, t.y, CGrad3{{cv(gA_), cv(Hf_), cv(Hf_)}},
                                                t.strain, t.nut, t.nu, t.sig, t.gammaC, t.sp, t.src, t.src2);
         launchCheck("sst_w_coefs");
-        turbSolveScalar(t.ec, t.ek, t.sig, 0.0, true, t.src2, t.eps, kDissFloor, false, inner);
+        turbSolveScalar(t.ec, t.ek, t.sig, 0.0, true, t.src2, t.eps, kDissFloor, false, dt, inner);
     }
     else
     {
         // k
         k_turb_src_k<<<G_, TPB, 0, stream_>>>(nC, dm_.V, t.k, t.eps, t.prod, t.sp, t.src);
         launchCheck("turb_src_k");
-        turbSolveScalar(t.kc, t.kk, nullptr, 1.0 / kSigmaK, true, nullptr, t.k, kFloor, false, inner);
+        turbSolveScalar(t.kc, t.kk, nullptr, 1.0 / kSigmaK, true, nullptr, t.k, kFloor, false, dt, inner);
         // epsilon, with the new k
         k_turb_src_e<<<G_, TPB, 0, stream_>>>(nC, dm_.V, t.k, t.eps, t.prod, t.sp, t.src);
         launchCheck("turb_src_e");
-        turbSolveScalar(t.ec, t.ek, nullptr, 1.0 / kSigmaE, true, nullptr, t.eps, kDissFloor, false, inner);
+        turbSolveScalar(t.ec, t.ek, nullptr, 1.0 / kSigmaE, true, nullptr, t.eps, kDissFloor, false, dt, inner);
         if (t.model == TM_TRANSITION)
         {
             // the intermittency (TransitionModel::solveGamma): sigma 1, the
@@ -1011,7 +1023,7 @@ void Ctx::turbCorrect(int64_t& inner)
             const double amp = t.rate * turbURef() / t.onsetX;
             k_trans_src<<<G_, TPB, 0, stream_>>>(nC, dm_.V, t.cx, t.gam, amp, t.onsetX, t.width, t.sp, t.src);
             launchCheck("trans_src");
-            turbSolveScalar(t.gc, t.gk, nullptr, 1.0, false, nullptr, t.gam, 0.0, true, inner);
+            turbSolveScalar(t.gc, t.gk, nullptr, 1.0, false, nullptr, t.gam, 0.0, true, dt, inner);
         }
     }
     if (t.nW > 0)

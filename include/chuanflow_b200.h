@@ -278,9 +278,11 @@ typedef struct cfg_piso_result
 } cfg_piso_result;
 
 /* solveTransientIncompressiblePiso (PisoSolver.h:92-100,
- * src/3d/src/solvers/pisoSolver.cpp:13-237), laminar: one implicit-Euler
- * time step of the device fields (momentum once, then the correctors, each
- * solving the full pressure from the previous iterate). */
+ * src/3d/src/solvers/pisoSolver.cpp:13-237): one implicit-Euler time step of
+ * the device fields (momentum once, then the correctors, each solving the
+ * full pressure from the previous iterate).  With a RANS model set up
+ * (cfg_turbulence_setup) the model advances first with the step's dt and
+ * supplies nu + nut on faces (pisoSolver.cpp:29-30); otherwise laminar. */
 int cfg_piso_step(cfg_ctx* ctx, const cfg_piso_controls* controls, cfg_piso_result* result);
 
 /* Wall time (ms) of the device work of the last cfg_simple_iterate call,

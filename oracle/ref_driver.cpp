@@ -13,7 +13,8 @@
 //                                                     fvc::grad, both overloads
 //   simple <case.dict> <out> [points|-] [statedir]    solveIncompressibleSimple
 //   rans   <case.dict> <out> [points|-]               the same with the case's RANS model
-//   piso   <case.dict> <out> [points|-]               transient PISO steps (piso{} block)
+//   piso   <case.dict> <out> [points|-]               transient PISO steps (piso{} block), with the
+//                                                     case's RANS model when it has a turbulence{}
 //   vtk    <case.dict> <out.vtu> <points|-> <p.f64> <U.f64>   VtkWriter
 //   eqns   <case.dict> <out> <points|-> <statedir>    UEqn / pEqn assembly probes
 //   solve  <out> <n> <trip.i64> <tripv.f64> <diag.f64> <b.f64> <x0.f64> <cg|bicgstab> <tol> <maxIter>
@@ -29,6 +30,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -298,17 +300,28 @@ int modePiso(int argc, char** argv)
     ctl.linearTol = pd.getScalarOr("linearTol", ctl.linearTol);
     ctl.linearMaxIter = static_cast<int>(pd.getScalarOr("linearMaxIter", ctl.linearMaxIter));
     const int steps = static_cast<int>(pd.getScalarOr("steps", 1));
+    // a case with a turbulence{} block steps its RANS model with the flow
+    std::unique_ptr<RansModel> turb;
+    if (caseDict.has("turbulence"))
+        turb = RansModel::create(mesh, U, phi, nu, schemes, TurbulenceConfig::fromCase(caseDict));
     std::ofstream r(out + "/result.txt");
     r << std::setprecision(17);
     for (int s = 0; s < steps; ++s)
     {
-        const PisoStepResult res = solveTransientIncompressiblePiso(mesh, U, p, phi, nu, schemes, ctl);
+        const PisoStepResult res = solveTransientIncompressiblePiso(mesh, U, p, phi, nu, schemes, ctl, turb.get());
         r << res.correctorsUsed << " " << res.predictedContinuityError << " " << res.continuityError << " "
           << res.pressureCorrectionMax << " " << (res.converged ? 1 : 0) << "\n";
     }
     writeVec(out + "/U.f64", U.internalField());
     writeSca(out + "/p.f64", p.internalField());
     writeSca(out + "/phi.f64", phi.values());
+    if (turb)
+    {
+        writeSca(out + "/k.f64", turb->k());
+        writeSca(out + "/eps.f64", turb->dissipation());
+        writeSca(out + "/nut.f64", turb->nut());
+        writeSca(out + "/nuEffFace.f64", turb->nuEffFace());
+    }
     return 0;
 }
 

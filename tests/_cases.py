@@ -267,6 +267,12 @@ def rans_channel_product(nx=12, ny=5, nz=5, model="kEpsilon"):
     return mesh, case
 
 
+def piso_rans_dict(model, dt=0.05, steps=4):
+    """The RANS channel stepped by PISO with its model (pisoSolver.cpp:29)."""
+    return rans_channel_dict(model=model, iters=1) + (
+        f"piso {{ dt {dt!r}; correctors 2; nonOrthCorrectors 1; linearTol 1e-10; steps {steps}; }}\n")
+
+
 def piso_channel_dict(nx=16, ny=6, nz=6, dt=0.05, steps=4):
     """The jittered channel (nu 1e-3) stepped by the reference's PISO."""
     return channel_dict(nx, ny, nz, nu=1e-3, iters=1) + (

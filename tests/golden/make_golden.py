@@ -33,6 +33,8 @@ Fixtures (small .npz files):
   coupled_kepsilon.npz     the same with the third block a k-epsilon duct
   rans_sst.npz, rans_des.npz, rans_transition.npz   the rans_channel case with the reference's
                            k-omega SST, DES and gamma-transition models
+  piso_rans_keps.npz, piso_rans_sst.npz   the same channel stepped by the reference's PISO
+                           (4 steps, dt 0.05) with k-epsilon and with k-omega SST
 
 `python tests/golden/make_golden.py coupled` (or `rans`) rebuilds only the coupled (or the
 three extra RANS) fixtures.
@@ -162,6 +164,9 @@ def piso_npz(name, text, points):
         out = {"points": points, "dict": np.array(text), "steps": steps,
                "U": O.read(os.path.join(td, "U.f64"), shape=(-1, 3)), "p": O.read(os.path.join(td, "p.f64")),
                "phi": O.read(os.path.join(td, "phi.f64"))}
+        for k in ("k", "eps", "nut", "nuEffFace"):  # a case with a RANS model
+            if os.path.exists(os.path.join(td, k + ".f64")):
+                out[k] = O.read(os.path.join(td, k + ".f64"))
         np.savez_compressed(os.path.join(HERE, name), **out)
         print("wrote", name, steps[-1])
 
@@ -285,6 +290,8 @@ def rans_fixtures():
     rc = K.channel_case(12, 5, 5, L=(1.0, 0.1, 0.1), jitter=0.0)
     for model, name in (("kOmegaSST", "rans_sst"), ("des", "rans_des"), ("gammaTransition", "rans_transition")):
         rans_npz(name + ".npz", K.rans_channel_dict(model=model), rc.mesh.points)
+    for model, name in (("kEpsilon", "piso_rans_keps"), ("kOmegaSST", "piso_rans_sst")):
+        piso_npz(name + ".npz", K.piso_rans_dict(model), rc.mesh.points)
 
 
 def coupled_fixtures():
