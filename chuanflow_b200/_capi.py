@@ -54,7 +54,7 @@ class _PoissonReport(C.Structure):
                 ("true_rel_residual", C.c_double), ("device_ms", C.c_double), ("initial_rel_residual", C.c_double)]
 
 
-POISSON = {"jacobi64": 0, "dic64": 1, "ir32": 2, "fcg_mpnn": 3}
+POISSON = {"jacobi64": 0, "dic64": 1, "ir32": 2, "fcg_mpnn": 3, "fcg_amg": 4, "fcg_amg_mpnn": 5}
 
 
 class _Report(C.Structure):
@@ -447,6 +447,21 @@ class SimpleCase:
         return x, {"inner_iterations": r.inner_iterations, "outer_iterations": r.outer_iterations,
                    "converged": bool(r.converged), "true_rel_residual": r.true_rel_residual,
                    "device_ms": r.device_ms, "initial_rel_residual": r.initial_rel_residual}
+
+    def poisson_amg_setup(self):
+        """The FP32 aggregation-AMG hierarchy of the Poisson system: levels,
+        rows per level, host structure and device value set-up times."""
+        out = np.zeros(11)
+        _check(lib().cfg_poisson_amg_setup(self._h, _dp(out)))
+        nl = int(out[0])
+        return {"levels": nl, "rows": [int(v) for v in out[1:1 + min(nl, 8)]], "structure_ms": float(out[9]),
+                "values_ms": float(out[10])}
+
+    def poisson_amg_apply(self, r):
+        """One V-cycle z = V(r) of that hierarchy (FP32 inside, FP64 in and out)."""
+        z = np.zeros(self.mesh.n_cells)
+        _check(lib().cfg_poisson_amg_apply(self._h, _dp(_f64(r)), _dp(z)))
+        return z
 
     # ---- diagnostics ----
     def probe_equations(self, controls: SimpleControls, xprobe):

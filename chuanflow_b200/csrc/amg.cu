@@ -1,0 +1,806 @@
+// Aggregation-AMG preconditioner for the pressure equation, in FP32 inside
+// the FP64 flexible CG (no reference counterpart: the reference solves its
+// pressure with Jacobi-PCG, Matrix.cpp:153-222).
+//
+// Structure (host, once per mesh): plain aggregation of the matrix graph in
+// device numbering.  Phase 1 visits rows in order and makes a row whose
+// neighbours are all free the root of an aggregate of itself and those
+// neighbours; phase 2 puts every row left over into the aggregate of its
+// first aggregated neighbour.  The coarse operator is the Galerkin product
+// P^T A P with the piecewise-constant P, so every coarse entry is a plain
+// sum of fine entries: the host lists, per coarse entry, the fine entries it
+// sums (in a fixed order), and the device forms the values with one gather
+// kernel per level.  Levels stop at <= 128 rows, whose operator is inverted
+// densely on the host (diagonally regularised when singular, as a pure
+// Neumann system is).
+//
+// V-cycle (device, FP32 vectors and values): per level one kernel does the
+// first damped-Jacobi sweep from zero and the residual, one sums the
+// residual over each aggregate, and after the coarse solve one kernel adds
+// the coarse correction (scaled by s > 1, which makes up for the piecewise
+// constant interpolation) and does the last Jacobi sweep.  The finest level
+// reads the FCG residual in FP64 and writes z in FP64.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <numeric>
+#include <utility>
+#include <vector>
+
+#include "ctx.h"
+#include "kernels.cuh"
+
+namespace cfg
+{
+
+struct AmgLevel
+{
+    int n = 0;
+    // levels >= 1 below the coarsest: CSR operator, diagonal position per row
+    int *rs = nullptr, *cols = nullptr, *dpos = nullptr;
+    float* val = nullptr;
+    float* dinv = nullptr;
+    // to the next level: the aggregate of each row, each aggregate's rows,
+    // and per next-level entry the entries of this level it sums
+    int* agg = nullptr;
+    int *ms = nullptr, *mem = nullptr;
+    int *gs = nullptr, *gl = nullptr;
+    int nnzNext = 0;
+    // work vectors: rhs, first sweep, residual, output
+    float *b = nullptr, *x = nullptr, *r = nullptr, *xo = nullptr;
+};
+
+/// Device scalars of the device-resident flexible CG (amgFcg)
+struct FcgState
+{
+    double tol, bn, pq, alpha, beta, rn;
+    int it, maxIter, done, conv;
+    unsigned int ticket[4];
+};
+
+struct AmgState
+{
+    ~AmgState()
+    {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+        if (stHost) cudaFreeHost(stHost);
+    }
+    std::vector<std::pair<std::pair<const void*, int>, cudaGraphExec_t>> graphs;  // (values, chunk) -> graph
+    FcgState* st = nullptr;
+    FcgState* stHost = nullptr;
+    std::vector<AmgLevel> lv;
+    int nc = 0;                  // rows of the coarsest level (dense inverse)
+    float* dense = nullptr;      // nc x nc inverse
+    std::vector<int> hrs, hcols;  // coarsest CSR on the host
+    bool valuesReady = false;
+    double setupMs = 0, valuesMs = 0;
+};
+
+void AmgDeleter::operator()(AmgState* a) const { delete a; }
+
+namespace
+{
+
+constexpr float kOmega = 0.67f;   // damped Jacobi
+constexpr float kScale = 1.8f;    // coarse-correction scaling
+constexpr int kDenseMax = 128;
+
+/// one SELL row of the finest operator: sum over its entries of val * f(col).
+/// W bounds the row length at compile time: all columns and values of the
+/// row are loaded before the first gather (W = 0 walks any length).
+template <int W, class F>
+__device__ __forceinline__ float sell_row(const DMat& A, const float* __restrict__ val, int c, F f)
+{
+    const int sl = c >> 5, lane = c & 31;
+    const int e0 = __ldg(A.start + sl) + lane, e1 = __ldg(A.start + sl + 1);
+    float s = 0.0f;
+    if constexpr (W > 0)
+    {
+        int col[W];
+        float v[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+        {
+            const int e = e0 + 32 * k;
+            col[k] = e < e1 ? __ldg(A.col + e) : -1;
+            v[k] = e < e1 ? __ldg(val + e) : 0.0f;
+        }
+        float g[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) g[k] = col[k] >= 0 ? f(col[k]) : 0.0f;
+#pragma unroll
+        for (int k = 0; k < W; ++k) s += v[k] * g[k];
+    }
+    else
+    {
+        for (int e = e0; e < e1; e += 32)
+        {
+            const int col = __ldg(A.col + e);
+            if (col < 0) break;
+            s += __ldg(val + e) * f(col);
+        }
+    }
+    return s;
+}
+
+/// a CSR row of a coarse level summed by a group of G lanes (rows there are
+/// long and few): lane l of the group takes entries l, l + G, ...; the
+/// group's lanes hold the sum after the shuffle tree
+template <int G, class F>
+__device__ __forceinline__ float group_row(const int* __restrict__ rs, const int* __restrict__ cols,
+                                           const float* __restrict__ val, int i, int l, F f)
+{
+    float s = 0.0f;
+    if (i >= 0)
+        for (int e = __ldg(rs + i) + l; e < __ldg(rs + i + 1); e += G) s += __ldg(val + e) * f(__ldg(cols + e));
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+constexpr int kGroup = 8;
+
+/// finest level, first sweep and residual: x = w D^-1 b, r = b - A x
+template <int W>
+__global__ void __launch_bounds__(TPB) k_amg_pre0(const int* __restrict__ stop, DMat A, const float* __restrict__ val,
+                                                  const float* __restrict__ dinv, const double* __restrict__ b,
+                                                  float* __restrict__ x, float* __restrict__ r)
+{
+    if (stop && *stop) return;
+    FOR_ROWS(c, A.n)
+    {
+        const float bc = static_cast<float>(b[c]);
+        x[c] = kOmega * dinv[c] * bc;
+        const float s =
+            sell_row<W>(A, val, c, [&](int j) { return kOmega * __ldg(dinv + j) * static_cast<float>(__ldg(b + j)); });
+        r[c] = bc - s;
+    }
+}
+
+/// coarse level, the same on CSR
+__global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, int n, const int* __restrict__ rs,
+                                                 const int* __restrict__ cols, const float* __restrict__ val,
+                                                 const float* __restrict__ dinv, const float* __restrict__ b,
+                                                 float* __restrict__ x, float* __restrict__ r)
+{
+    if (stop && *stop) return;
+    const int l = threadIdx.x % kGroup;
+    const int stride = gridDim.x * (TPB / kGroup);
+    // whole warps iterate together (the shuffle needs every lane)
+    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup - 0; ; i0 += stride)
+    {
+        const int base = i0 - (threadIdx.x % 32) / kGroup;  // the warp's first row this round
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        const float s = group_row<kGroup>(rs, cols, val, i, l, [&](int j) { return kOmega * __ldg(dinv + j) * __ldg(b + j); });
+        if (i >= 0 && l == 0)
+        {
+            const float bi = b[i];
+            x[i] = kOmega * dinv[i] * bi;
+            r[i] = bi - s;
+        }
+    }
+}
+
+/// the residual summed over each aggregate: the next level's right-hand side
+__global__ void __launch_bounds__(TPB) k_amg_restrict(const int* __restrict__ stop, int nc, const int* __restrict__ ms,
+                                                      const int* __restrict__ mem, const float* __restrict__ r,
+                                                      float* __restrict__ bc)
+{
+    if (stop && *stop) return;
+    FOR_ROWS(I, nc)
+    {
+        float s = 0.0f;
+        for (int k = ms[I]; k < ms[I + 1]; ++k) s += r[mem[k]];
+        bc[I] = s;
+    }
+}
+
+/// finest level: y = x + s P xc, then z = y + w D^-1 (b - A y), in FP64
+/// out; inside the device FCG (st given) also z.q and, in the block that
+/// finishes last, beta = -z.q / p.q
+template <int W>
+__global__ void __launch_bounds__(TPB) k_amg_post0(const int* __restrict__ stop, DMat A, const float* __restrict__ val,
+                                                   const float* __restrict__ dinv, const double* __restrict__ b,
+                                                   const float* __restrict__ x, const float* __restrict__ xc,
+                                                   const int* __restrict__ agg, double* __restrict__ z,
+                                                   const double* __restrict__ q, double* partials, FcgState* st)
+{
+    if (stop && *stop) return;
+    const bool dot = q != nullptr;  // inside the FCG iteration
+    double zq[1] = {0.0};
+    FOR_ROWS(c, A.n)
+    {
+        const float y = x[c] + kScale * xc[agg[c]];
+        const float s =
+            sell_row<W>(A, val, c, [&](int j) { return __ldg(x + j) + kScale * __ldg(xc + __ldg(agg + j)); });
+        const double zc = static_cast<double>(y + kOmega * dinv[c] * (static_cast<float>(b[c]) - s));
+        z[c] = zc;
+        if (dot) zq[0] += zc * q[c];
+    }
+    if (!dot) return;
+    block_sum<1>(zq);
+    if (threadIdx.x == 0) partials[blockIdx.x] = zq[0];
+    if (!last_block(&st->ticket[2])) return;
+    double f[1];
+    final_sum<1>(partials, gridDim.x, f);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[2] = 0;
+        st->beta = -f[0] / st->pq;
+    }
+}
+
+/// coarse level, the same on CSR
+__global__ void __launch_bounds__(TPB) k_amg_post(const int* __restrict__ stop, int n, const int* __restrict__ rs,
+                                                  const int* __restrict__ cols, const float* __restrict__ val,
+                                                  const float* __restrict__ dinv, const float* __restrict__ b,
+                                                  const float* __restrict__ x, const float* __restrict__ xc,
+                                                  const int* __restrict__ agg, float* __restrict__ xo)
+{
+    if (stop && *stop) return;
+    const int l = threadIdx.x % kGroup;
+    const int stride = gridDim.x * (TPB / kGroup);
+    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup; ; i0 += stride)
+    {
+        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        const float s =
+            group_row<kGroup>(rs, cols, val, i, l, [&](int j) { return __ldg(x + j) + kScale * __ldg(xc + __ldg(agg + j)); });
+        if (i >= 0 && l == 0) xo[i] = x[i] + kScale * xc[agg[i]] + kOmega * dinv[i] * (b[i] - s);
+    }
+}
+
+/// the coarsest solve: x = M^-1 b with the dense inverse (one block)
+__global__ void __launch_bounds__(kDenseMax) k_amg_dense(const int* __restrict__ stop, int n,
+                                                         const float* __restrict__ m, const float* __restrict__ b,
+                                                         float* __restrict__ x)
+{
+    if (stop && *stop) return;
+    const int i = threadIdx.x;
+    if (i >= n) return;
+    float s = 0.0f;
+    for (int j = 0; j < n; ++j) s += m[i * n + j] * b[j];
+    x[i] = s;
+}
+
+/// next-level entries as sums of this level's: FP64 sums of FP64 (finest,
+/// SELL) or FP32 values, stored in FP32
+__global__ void __launch_bounds__(TPB) k_amg_galerkin(int nnz, const int* __restrict__ gs, const int* __restrict__ gl,
+                                                      const double* __restrict__ fineD, const float* __restrict__ fineF,
+                                                      float* __restrict__ out)
+{
+    FOR_ROWS(e, nnz)
+    {
+        double s = 0.0;
+        for (int k = gs[e]; k < gs[e + 1]; ++k) s += fineD ? fineD[gl[k]] : static_cast<double>(fineF[gl[k]]);
+        out[e] = static_cast<float>(s);
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_amg_dinv(int n, const int* __restrict__ dpos, const float* __restrict__ val,
+                                                  float* __restrict__ dinv)
+{
+    FOR_ROWS(i, n)
+    {
+        const float d = val[dpos[i]];
+        dinv[i] = d != 0.0f ? 1.0f / d : 1.0f;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_amg_dinv0(int n, const double* __restrict__ diag, float* __restrict__ dinv)
+{
+    FOR_ROWS(i, n) dinv[i] = diag[i] != 0.0 ? static_cast<float>(1.0 / diag[i]) : 1.0f;
+}
+
+/// a host CSR pattern whose entries remember where their values live
+struct Pattern
+{
+    int n = 0;
+    std::vector<int> rs, cols, pos;
+};
+
+/// plain aggregation (the two phases of the file comment)
+int aggregate(const Pattern& A, std::vector<int>& agg)
+{
+    agg.assign(static_cast<size_t>(A.n), -1);
+    int na = 0;
+    for (int i = 0; i < A.n; ++i)
+    {
+        if (agg[i] >= 0) continue;
+        bool free = true;
+        for (int e = A.rs[i]; e < A.rs[i + 1] && free; ++e) free = agg[A.cols[e]] < 0;
+        if (!free) continue;
+        for (int e = A.rs[i]; e < A.rs[i + 1]; ++e) agg[A.cols[e]] = na;
+        agg[i] = na++;
+    }
+    for (int i = 0; i < A.n; ++i)
+    {
+        if (agg[i] >= 0) continue;
+        for (int e = A.rs[i]; e < A.rs[i + 1]; ++e)
+            if (agg[A.cols[e]] >= 0 && A.cols[e] != i)
+            {
+                agg[i] = agg[A.cols[e]];
+                break;
+            }
+        if (agg[i] < 0) agg[i] = na++;
+    }
+    return na;
+}
+
+}  // namespace
+
+/// The hierarchy's structure from the device pressure pattern.
+void Ctx::amgSetup()
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<AmgState> a(new AmgState());
+    const int n0 = dm_.nC;
+    // the finest pattern from the SELL slices, entries in row order
+    Pattern P;
+    {
+        std::vector<int> start(static_cast<size_t>(nSlices_) + 1), col(static_cast<size_t>(nSlicesEntries_));
+        CFG_CUDA(cudaMemcpyAsync(start.data(), dm_.mStart, start.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaMemcpyAsync(col.data(), dm_.mCol, col.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        P.n = n0;
+        P.rs.assign(static_cast<size_t>(n0) + 1, 0);
+        for (int c = 0; c < n0; ++c)
+        {
+            const int sl = c >> 5, lane = c & 31;
+            for (int e = start[sl] + lane; e < start[sl + 1]; e += 32)
+            {
+                if (col[e] < 0) break;
+                P.cols.push_back(col[e]);
+                P.pos.push_back(e);
+            }
+            P.rs[c + 1] = static_cast<int>(P.cols.size());
+        }
+    }
+    while (true)
+    {
+        AmgLevel L;
+        L.n = P.n;
+        // the finest level always aggregates (it reads FP64 in and out)
+        if (P.n <= kDenseMax && !a->lv.empty())
+        {
+            a->nc = P.n;
+            a->hrs = P.rs;
+            a->hcols = P.cols;
+            L.b = alloc<float>(P.n);
+            L.x = alloc<float>(P.n);
+            a->lv.push_back(L);
+            break;
+        }
+        std::vector<int> agg;
+        const int na = aggregate(P, agg);
+        if (na > P.n * 9 / 10 || na > 0x3fffffff)
+            fail(CFG_ESETUP, "amg: the aggregation stopped coarsening above " + std::to_string(kDenseMax) + " rows");
+        // members of each aggregate, in row order
+        std::vector<int> ms(static_cast<size_t>(na) + 1, 0), mem(static_cast<size_t>(P.n));
+        for (int i = 0; i < P.n; ++i) ++ms[agg[i] + 1];
+        for (int I = 0; I < na; ++I) ms[I + 1] += ms[I];
+        {
+            std::vector<int> fill(ms.begin(), ms.end() - 1);
+            for (int i = 0; i < P.n; ++i) mem[fill[agg[i]]++] = i;
+        }
+        // the coarse pattern and, per coarse entry, the fine entries it sums
+        Pattern C;
+        C.n = na;
+        C.rs.assign(static_cast<size_t>(na) + 1, 0);
+        std::vector<int> gs{0}, gl;
+        std::vector<std::pair<int, int>> row;  // (coarse column, fine entry index)
+        for (int I = 0; I < na; ++I)
+        {
+            row.clear();
+            for (int k = ms[I]; k < ms[I + 1]; ++k)
+            {
+                const int i = mem[k];
+                for (int e = P.rs[i]; e < P.rs[i + 1]; ++e) row.push_back({agg[P.cols[e]], e});
+            }
+            std::stable_sort(row.begin(), row.end(),
+                             [](const std::pair<int, int>& x, const std::pair<int, int>& y) { return x.first < y.first; });
+            for (size_t k = 0; k < row.size(); ++k)
+            {
+                if (k == 0 || row[k].first != row[k - 1].first)
+                {
+                    if (k > 0) gs.push_back(static_cast<int>(gl.size()));
+                    C.cols.push_back(row[k].first);
+                }
+                gl.push_back(P.pos[row[k].second]);
+            }
+            if (!row.empty()) gs.push_back(static_cast<int>(gl.size()));
+            C.rs[I + 1] = static_cast<int>(C.cols.size());
+        }
+        C.pos.resize(C.cols.size());
+        std::iota(C.pos.begin(), C.pos.end(), 0);
+        L.agg = upload(agg);
+        L.ms = upload(ms);
+        L.mem = upload(mem);
+        L.gs = upload(gs);
+        L.gl = upload(gl);
+        L.nnzNext = static_cast<int>(C.cols.size());
+        if (!a->lv.empty())
+        {
+            std::vector<int> dpos(static_cast<size_t>(P.n), -1);
+            for (int i = 0; i < P.n; ++i)
+                for (int e = P.rs[i]; e < P.rs[i + 1]; ++e)
+                    if (P.cols[e] == i) dpos[i] = e;
+            L.rs = upload(P.rs);
+            L.cols = upload(P.cols);
+            L.dpos = upload(dpos);
+            L.val = alloc<float>(P.cols.size());
+        }
+        L.dinv = alloc<float>(P.n);
+        L.b = alloc<float>(P.n);
+        L.x = alloc<float>(P.n);
+        L.r = alloc<float>(P.n);
+        L.xo = alloc<float>(P.n);
+        a->lv.push_back(L);
+        P = std::move(C);
+    }
+    // the coarsest level's CSR operator (for the Galerkin values and its inverse)
+    {
+        AmgLevel& L = a->lv.back();
+        L.val = alloc<float>(std::max<size_t>(P.cols.size(), 1));
+        a->dense = alloc<float>(static_cast<size_t>(P.n) * P.n);
+    }
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    a->setupMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    amg_.reset(a.release());
+}
+
+/// The hierarchy's values from the finest operator (FP64 SELL values and
+/// diagonal): Galerkin sums level by level, inverse diagonals, and the
+/// coarsest level's dense inverse (on the host).
+void Ctx::amgValues(const double* vals, const double* diag, const float* vals32)
+{
+    if (!amg_) amgSetup();
+    AmgState& a = *amg_;
+    const auto t0 = std::chrono::steady_clock::now();
+    amgVals32_ = vals32;
+    k_amg_dinv0<<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, a.lv[0].dinv);
+    for (size_t l = 0; l + 1 < a.lv.size(); ++l)
+    {
+        const AmgLevel& L = a.lv[l];
+        AmgLevel& N = a.lv[l + 1];
+        const int g = std::max(1, std::min((L.nnzNext + TPB - 1) / TPB, sms_ * 8));
+        k_amg_galerkin<<<g, TPB, 0, stream_>>>(L.nnzNext, L.gs, L.gl, l == 0 ? vals : nullptr, l == 0 ? nullptr : L.val,
+                                               N.val);
+        if (l + 2 < a.lv.size())
+            k_amg_dinv<<<std::max(1, std::min((N.n + TPB - 1) / TPB, sms_ * 8)), TPB, 0, stream_>>>(N.n, N.dpos, N.val,
+                                                                                                N.dinv);
+        launchCheck("amg_galerkin", 2);
+    }
+    // dense inverse of the coarsest operator, Gauss-Jordan with partial
+    // pivoting; a singular operator (pure Neumann) gets a small diagonal shift
+    {
+        const int n = a.nc;
+        std::vector<float> v(a.hcols.size());
+        if (!v.empty())
+            CFG_CUDA(cudaMemcpyAsync(v.data(), a.lv.back().val, v.size() * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        std::vector<double> m(static_cast<size_t>(n) * n, 0.0), inv(static_cast<size_t>(n) * n, 0.0);
+        double dmax = 0;
+        for (int i = 0; i < n; ++i)
+            for (int e = a.hrs[i]; e < a.hrs[i + 1]; ++e)
+            {
+                m[static_cast<size_t>(i) * n + a.hcols[e]] += v[e];
+                if (a.hcols[e] == i) dmax = std::max(dmax, std::abs(static_cast<double>(v[e])));
+            }
+        for (int i = 0; i < n; ++i)
+        {
+            m[static_cast<size_t>(i) * n + i] += 1e-6 * dmax;
+            inv[static_cast<size_t>(i) * n + i] = 1.0;
+        }
+        for (int c = 0; c < n; ++c)
+        {
+            int piv = c;
+            for (int i = c + 1; i < n; ++i)
+                if (std::abs(m[static_cast<size_t>(i) * n + c]) > std::abs(m[static_cast<size_t>(piv) * n + c])) piv = i;
+            if (piv != c)
+                for (int j = 0; j < n; ++j)
+                {
+                    std::swap(m[static_cast<size_t>(c) * n + j], m[static_cast<size_t>(piv) * n + j]);
+                    std::swap(inv[static_cast<size_t>(c) * n + j], inv[static_cast<size_t>(piv) * n + j]);
+                }
+            const double d = m[static_cast<size_t>(c) * n + c];
+            if (!(std::abs(d) > 0)) fail(CFG_ENUMERIC, "amg: singular coarsest operator");
+            for (int j = 0; j < n; ++j)
+            {
+                m[static_cast<size_t>(c) * n + j] /= d;
+                inv[static_cast<size_t>(c) * n + j] /= d;
+            }
+            for (int i = 0; i < n; ++i)
+            {
+                if (i == c) continue;
+                const double f = m[static_cast<size_t>(i) * n + c];
+                if (f == 0) continue;
+                for (int j = 0; j < n; ++j)
+                {
+                    m[static_cast<size_t>(i) * n + j] -= f * m[static_cast<size_t>(c) * n + j];
+                    inv[static_cast<size_t>(i) * n + j] -= f * inv[static_cast<size_t>(c) * n + j];
+                }
+            }
+        }
+        std::vector<float> invf(inv.begin(), inv.end());
+        if (!invf.empty())
+            CFG_CUDA(cudaMemcpyAsync(a.dense, invf.data(), invf.size() * sizeof(float), cudaMemcpyHostToDevice, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+    }
+    a.valuesReady = true;
+    a.valuesMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+/// z = V-cycle(r), r and z in FP64 on device cells.  Inside the device FCG
+/// every kernel stops once the solve is done (st->done) and the finest
+/// post-smoothing also forms z.q and beta.
+void Ctx::amgApply(const double* r, double* z)
+{
+    amgCycle(r, z, nullptr, nullptr);
+}
+
+void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
+{
+    AmgState& a = *amg_;
+    if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
+    const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
+    const int L = static_cast<int>(a.lv.size());
+    const int* stop = st ? &st->done : nullptr;
+    auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
+    // a group of kGroup lanes per coarse row
+    auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
+    const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
+    // down
+    for (int l = 0; l + 1 < L; ++l)
+    {
+        AmgLevel& V = a.lv[l];
+        AmgLevel& N = a.lv[l + 1];
+        if (l == 0)
+        {
+            if (Wsel == 7) k_amg_pre0<7><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, V.r);
+            else if (Wsel == 16) k_amg_pre0<16><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, V.r);
+            else k_amg_pre0<0><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, V.r);
+        }
+        else
+            k_amg_pre<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
+        k_amg_restrict<<<grid(N.n), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
+    }
+    k_amg_dense<<<1, kDenseMax, 0, stream_>>>(stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
+    // up: each level corrects with the next level's output
+    for (int l = L - 2; l >= 0; --l)
+    {
+        AmgLevel& V = a.lv[l];
+        const float* xc = (l + 1 == L - 1) ? a.lv[l + 1].x : a.lv[l + 1].xo;
+        if (l == 0)
+        {
+            if (Wsel == 7)
+                k_amg_post0<7><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, xc, V.agg, z, q, partials_, st);
+            else if (Wsel == 16)
+                k_amg_post0<16><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, xc, V.agg, z, q, partials_,
+                                                          st);
+            else
+                k_amg_post0<0><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, xc, V.agg, z, q, partials_, st);
+        }
+        else
+            k_amg_post<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, xc, V.agg, V.xo);
+    }
+    launchCheck("amg_vcycle", 3 * (L - 1) + 1);
+}
+
+namespace
+{
+
+/// r = b - A x, |r|2 and |b|2; the solve is done at once when |r|/|b| <= tol
+template <int W>
+__global__ void __launch_bounds__(TPB) k_fcgd_init(DMat A, const double* __restrict__ val, const double* __restrict__ b,
+                                                   const double* __restrict__ x, double* __restrict__ r,
+                                                   double* partials, FcgState* st)
+{
+    double s[2] = {0.0, 0.0};
+    const double* xs[1] = {x};
+    FOR_ROWS(c, A.n)
+    {
+        double y[1];
+        spmv_row<W, 1>(A, val, c, xs, y);
+        const double bc = b[c], rc = bc - y[0];
+        r[c] = rc;
+        s[0] += rc * rc;
+        s[1] += bc * bc;
+    }
+    block_sum<2>(s);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = s[0];
+        partials[G + blockIdx.x] = s[1];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double f[2];
+    final_sum<2>(partials, G, f);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        st->rn = sqrt(f[0]);
+        st->bn = sqrt(f[1]);
+        st->it = 0;
+        st->conv = !(st->bn > 0) || st->rn / st->bn <= st->tol;
+        st->done = st->conv || st->maxIter <= 0;
+    }
+}
+
+/// q = A p with p.r and p.q; alpha = p.r / p.q, or done on a breakdown
+template <int W>
+__global__ void __launch_bounds__(TPB) k_fcgd_spmv(DMat A, const double* __restrict__ val, const double* __restrict__ p,
+                                                   const double* __restrict__ r, double* __restrict__ q,
+                                                   double* partials, FcgState* st)
+{
+    if (st->done) return;
+    double s[2] = {0.0, 0.0};
+    const double* xs[1] = {p};
+    FOR_ROWS(c, A.n)
+    {
+        double y[1];
+        spmv_row<W, 1>(A, val, c, xs, y);
+        q[c] = y[0];
+        const double pc = p[c];
+        s[0] += pc * r[c];
+        s[1] += pc * y[0];
+    }
+    block_sum<2>(s);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+    {
+        partials[blockIdx.x] = s[0];
+        partials[G + blockIdx.x] = s[1];
+    }
+    if (!last_block(&st->ticket[0])) return;
+    double f[2];
+    final_sum<2>(partials, G, f);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        if (!(f[1] > 0)) st->done = 1;
+        else
+        {
+            st->pq = f[1];
+            st->alpha = f[0] / f[1];
+        }
+    }
+}
+
+/// x += alpha p, r -= alpha q, |r|2 and the stopping test
+__global__ void __launch_bounds__(TPB) k_fcgd_update(int n, const double* __restrict__ p, const double* __restrict__ q,
+                                                     double* __restrict__ x, double* __restrict__ r, double* partials,
+                                                     FcgState* st)
+{
+    if (st->done) return;
+    const double al = st->alpha;
+    double s[1] = {0.0};
+    FOR_ROWS(c, n)
+    {
+        x[c] = x[c] + al * p[c];
+        const double rc = r[c] - al * q[c];
+        r[c] = rc;
+        s[0] += rc * rc;
+    }
+    block_sum<1>(s);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s[0];
+    if (!last_block(&st->ticket[1])) return;
+    double f[1];
+    final_sum<1>(partials, gridDim.x, f);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[1] = 0;
+        st->it = st->it + 1;
+        st->rn = sqrt(f[0]);
+        if (st->rn / st->bn <= st->tol)
+        {
+            st->conv = 1;
+            st->done = 1;
+        }
+        else if (st->it >= st->maxIter || !(st->rn == st->rn))
+        {
+            st->done = 1;
+        }
+    }
+}
+
+/// p = z + beta p (beta = 0 gives p = z)
+__global__ void __launch_bounds__(TPB) k_fcgd_p(int n, const double* __restrict__ z, double* __restrict__ p,
+                                                const FcgState* st, int first)
+{
+    if (st->done) return;
+    const double be = first ? 0.0 : st->beta;
+    FOR_ROWS(c, n) p[c] = first ? z[c] : z[c] + be * p[c];
+}
+
+}  // namespace
+
+/// Flexible CG (FCG(1): alpha = p.r / p.q, beta = -z.q / p.q) with the AMG
+/// V-cycle as preconditioner, to |b - A x|2 / |b|2 <= tol, with every scalar
+/// on the device: the host polls the state once per chunk of iterations,
+/// and each chunk is a CUDA graph captured once.  out: {iterations,
+/// converged}.
+void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int64_t* out)
+{
+    AmgState& a = *amg_;
+    const int n = dm_.nC;
+    const DMat A{n, dm_.mStart, dm_.mCol};
+    double* r = cr_;
+    double* z = cz_;
+    double* p = cp_;
+    double* q = cAp_;
+    if (!a.st)
+    {
+        a.st = alloc<FcgState>(1);
+        CFG_CUDA(cudaMallocHost(&a.stHost, sizeof(FcgState)));
+    }
+    FcgState init{};
+    init.tol = tol;
+    init.maxIter = maxIter;
+    CFG_CUDA(cudaMemcpyAsync(a.st, &init, sizeof(FcgState), cudaMemcpyHostToDevice, stream_));
+    auto spmvInit = [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        k_fcgd_init<W><<<GS_, TPB, 0, stream_>>>(A, vals, b, x, r, partials_, a.st);
+    };
+    const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
+    if (Wsel == 7) spmvInit(std::integral_constant<int, 7>{});
+    else if (Wsel == 16) spmvInit(std::integral_constant<int, 16>{});
+    else spmvInit(std::integral_constant<int, 0>{});
+    launchCheck("fcgd_init");
+    amgCycle(r, z, nullptr, a.st);
+    k_fcgd_p<<<GS_, TPB, 0, stream_>>>(n, z, p, a.st, 1);
+    launchCheck("fcgd_p0");
+    auto iteration = [&]() {
+        if (Wsel == 7) k_fcgd_spmv<7><<<GS_, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
+        else if (Wsel == 16) k_fcgd_spmv<16><<<GS_, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
+        else k_fcgd_spmv<0><<<GS_, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
+        k_fcgd_update<<<GS_, TPB, 0, stream_>>>(n, p, q, x, r, partials_, a.st);
+        amgCycle(r, z, q, a.st);
+        k_fcgd_p<<<GS_, TPB, 0, stream_>>>(n, z, p, a.st, 0);
+        launchCheck("fcgd_iter", 3);
+    };
+    for (int launched = 0, chunk = 8;;)
+    {
+        CFG_CUDA(cudaMemcpyAsync(a.stHost, a.st, sizeof(FcgState), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        if (a.stHost->done || launched >= maxIter) break;
+        const int m = std::min(chunk, maxIter - launched);
+        const std::pair<const void*, int> key{vals, m};
+        cudaGraphExec_t ge = nullptr;
+        for (auto& g : a.graphs)
+            if (g.first == key) ge = g.second;
+        if (!ge && useGraphs_)
+        {
+            cudaGraph_t g = nullptr;
+            CFG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < m; ++k) iteration();
+            CFG_CUDA(cudaStreamEndCapture(stream_, &g));
+            const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) fail(CFG_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+            a.graphs.push_back({key, ge});
+        }
+        if (ge) CFG_CUDA(cudaGraphLaunch(ge, stream_));
+        else
+            for (int k = 0; k < m; ++k) iteration();
+        launched += m;
+        chunk = std::min(chunk * 2, 32);
+    }
+    out[0] = a.stHost->it;
+    out[1] = a.stHost->conv;
+}
+
+void Ctx::amgInfo(double* out)
+{
+    // out: levels, rows of each of up to 8 levels, setup ms, values ms
+    for (int k = 0; k < 11; ++k) out[k] = 0;
+    if (!amg_) return;
+    out[0] = static_cast<double>(amg_->lv.size());
+    for (size_t l = 0; l < amg_->lv.size() && l < 8; ++l) out[1 + l] = amg_->lv[l].n;
+    out[9] = amg_->setupMs;
+    out[10] = amg_->valuesMs;
+}
+
+}  // namespace cfg

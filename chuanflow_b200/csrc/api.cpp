@@ -486,6 +486,22 @@ int cfg_poisson_solve(cfg_ctx* ctx, const double* b, double* x, int32_t method, 
     });
 }
 
+int cfg_poisson_amg_setup(cfg_ctx* ctx, double out[11])
+{
+    return guard([&] {
+        need(ctx && out, "cfg_poisson_amg_setup: null argument");
+        ctx->c->poissonAmg(out);
+    });
+}
+
+int cfg_poisson_amg_apply(cfg_ctx* ctx, const double* r, double* z)
+{
+    return guard([&] {
+        need(ctx && r && z, "cfg_poisson_amg_apply: null argument");
+        ctx->c->poissonAmgApply(r, z);
+    });
+}
+
 int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t scheme, int32_t volQuirk, double* out)
 {
     return guard([&] {

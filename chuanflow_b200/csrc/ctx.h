@@ -37,6 +37,12 @@ struct TurbDeleter
 {
     void operator()(TurbState* t) const;
 };
+struct AmgState;
+struct FcgState;
+struct AmgDeleter
+{
+    void operator()(AmgState* a) const;
+};
 
 class Ctx
 {
@@ -169,6 +175,9 @@ public:
     void poissonSetup(int64_t refCell);
     void poissonSolve(const double* b, double* x, int method, double tol, int maxIter, int innerMax,
                       double innerTol, double* out);
+    /// the AMG hierarchy for the Poisson system's current values
+    void poissonAmg(double* out);
+    void poissonAmgApply(const double* r, double* z);
 
 private:
     void setNu(double nu);
@@ -187,13 +196,23 @@ private:
     std::unique_ptr<DetailState, DetailDeleter> detail_;
     std::unique_ptr<TurbState, TurbDeleter> turb_;
     std::unique_ptr<MpnnState, MpnnDeleter> mpnn_;
+    // aggregation AMG in FP32 (amg.cu)
+    std::unique_ptr<AmgState, AmgDeleter> amg_;
+    const float* amgVals32_ = nullptr;
+    void amgSetup();
+    void amgValues(const double* vals, const double* diag, const float* vals32);
+    void amgApply(const double* r, double* z);
+    void amgCycle(const double* r, double* z, const double* q, FcgState* st);
+    void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int64_t* out);
+    void amgInfo(double* out);
+    bool amgFresh_ = false;  // the hierarchy's values match the Poisson system
     void mpnnApply(const double* vals, const double* diag, const double* r, double* z);
     double mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z);
     void mpnnAdam(float lr);
     void mpnnMatrix(const double** vals, const double** diag) const;
     void mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses);
     void mpnnFcg(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                 int window, int64_t* out, int normType);
+                 int window, int64_t* out, int normType, int pc = 0);
     double fcgNorm(const double* v, int normType);
     void mpnnResidualHost(const double* vals, const double* b, const double* x, double* rHost);
     bool collectOn_ = false;

@@ -745,13 +745,32 @@ void Ctx::mpnnResidualHost(const double* vals, const double* b, const double* x,
 }
 
 void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
-                  int window, int64_t* out, int normType)
+                  int window, int64_t* out, int normType, int pc)
 {
     const int n = dm_.nC;
     double* r = cr_;
     double* z = cz_;
     double* p = cp_;
     double* q = cAp_;
+    // the preconditioner: the network (pc 0), an AMG V-cycle (1), or the
+    // V-cycle with the network applied to the residual it leaves (2)
+    auto precond = [&](const double* rr, double* zz) {
+        if (pc == 0)
+        {
+            mpnnApply(vals, diag, rr, zz);
+            return;
+        }
+        amgApply(rr, zz);
+        if (pc != 2) return;
+        double* t = bt_.c[0];
+        double* w = bt_.c[1];
+        fcgSpmv(vals, zz, t);
+        k_fcg_p<<<GS_, TPB, 0, stream_>>>(n, rr, -1.0, t);  // t = r - A z
+        launchCheck("amg_mpnn_residual");
+        mpnnApply(vals, diag, t, w);
+        k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, 1.0, w, zz);  // z += N(r - A z)
+        launchCheck("amg_mpnn_correct");
+    };
     fcgSpmv(vals, x, q);
     CFG_CUDA(cudaMemcpyAsync(r, b, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, -1.0, q, r);
@@ -764,7 +783,7 @@ void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, doubl
     int it = 0;
     out[0] = out[1] = out[2] = 0;
     if (!(bn > 0) || rn / bn <= tol) return;
-    mpnnApply(vals, diag, r, z);
+    precond(r, z);
     CFG_CUDA(cudaMemcpyAsync(p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     bool fallback = false;
     while (it < maxIter)
@@ -788,7 +807,7 @@ void Ctx::mpnnFcg(const double* vals, const double* diag, const double* b, doubl
             fallback = true;
             break;
         }
-        mpnnApply(vals, diag, r, z);
+        precond(r, z);
         {
             const double* aa[1] = {z};
             const double* bq[1] = {q};

@@ -2301,7 +2301,29 @@ void Ctx::poissonSetup(int64_t refCell)
     launchCheck("poisson_float");
     dicSetupT<double>(dic_, pVal_d_, pDiag_);
     dicSetupT<float>(dic32_, pVal_d_, pDiag32_);
+    amgFresh_ = false;
     CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Ctx::poissonAmg(double* out)
+{
+    if (!poissonReady_) fail(CFG_EINVAL, "cfg_poisson_amg_setup: call cfg_poisson_setup first");
+    CFG_CUDA(cudaSetDevice(device_));
+    amgValues(pVal_d_, pDiag_, pVal32_);
+    amgFresh_ = true;
+    amgInfo(out);
+}
+
+void Ctx::poissonAmgApply(const double* r, double* z)
+{
+    if (!amgFresh_)
+    {
+        double info[11];
+        poissonAmg(info);
+    }
+    toDevCells(cr_, r, 1, 0);
+    amgApply(cr_, cz_);
+    fromDevCells(z, cz_, 1, 0);
 }
 
 void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int maxIter, int innerMax, double innerTol,
@@ -2330,6 +2352,13 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
         CFG_CUDA(cudaStreamSynchronize(stream_));
         return stHost_->init[0] / stHost_->bnorm[0];
     };
+    // the AMG hierarchy is set up outside the timed solve, as the DIC
+    // factors are (cfg_poisson_amg_setup reports what it costs)
+    if ((method == 4 || method == 5) && !amgFresh_)
+    {
+        double info[11];
+        poissonAmg(info);
+    }
     CFG_CUDA(cudaStreamSynchronize(stream_));
     const double rel0 = trueRel();
     CFG_CUDA(cudaEventRecord(tm_.ev[2], stream_));
@@ -2371,6 +2400,26 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
         if (!mpnn_) fail(CFG_EINVAL, "cfg_poisson_solve: fcg_mpnn needs cfg_mpnn_create");
         int64_t o[3];
         mpnnFcg(pVal_d_, pDiag_, pb64_, px64_, tol, maxIter, 25, o, 1);
+        inner = o[0] + o[1];
+        outer = 1 + static_cast<int>(o[2]);
+        lastFallbackIters = o[1];
+    }
+    else if (method == 4)
+    {
+        // flexible CG with the FP32 AMG V-cycle, every scalar on the device
+        int64_t o[2];
+        amgFcg(pVal_d_, pb64_, px64_, tol, maxIter, o);
+        inner = o[0];
+        outer = 1;
+    }
+    else if (method == 5)
+    {
+        // the same with the learned correction after each V-cycle (host
+        // driven: the network's application is its own launch sequence);
+        // DIC-PCG when it stalls
+        if (!mpnn_) fail(CFG_EINVAL, "cfg_poisson_solve: fcg_amg_mpnn needs cfg_mpnn_create");
+        int64_t o[3];
+        mpnnFcg(pVal_d_, pDiag_, pb64_, px64_, tol, maxIter, 25, o, 1, 2);
         inner = o[0] + o[1];
         outer = 1 + static_cast<int>(o[2]);
         lastFallbackIters = o[1];

@@ -318,8 +318,12 @@ enum cfg_poisson_method
     CFG_POISSON_JACOBI64 = 0,  /* FP64 Jacobi-PCG, the reference's solver */
     CFG_POISSON_DIC64 = 1,     /* FP64 multicolour-DIC PCG */
     CFG_POISSON_IR32 = 2,      /* FP32 DIC-PCG corrections inside FP64 iterative refinement */
-    CFG_POISSON_FCG_MPNN = 3   /* flexible CG with the learned preconditioner (cfg_mpnn_create),
+    CFG_POISSON_FCG_MPNN = 3,  /* flexible CG with the learned preconditioner (cfg_mpnn_create),
                                 * FP64 DIC-PCG from its iterate when it stalls */
+    CFG_POISSON_FCG_AMG = 4,   /* FP64 flexible CG preconditioned by an FP32 aggregation-AMG
+                                * V-cycle (same fallback) */
+    CFG_POISSON_FCG_AMG_MPNN = 5 /* the same with the learned network correcting what each
+                                  * V-cycle leaves: z = V(r) + N(r - A V(r)) */
 };
 
 typedef struct cfg_poisson_report
@@ -346,6 +350,15 @@ int cfg_poisson_setup(cfg_ctx* ctx, int64_t ref_cell);
  * PCG iterations. */
 int cfg_poisson_solve(cfg_ctx* ctx, const double* b, double* x, int32_t method, double rel_tol, int32_t max_iter,
                       int32_t inner_max_iter, double inner_rel_tol, cfg_poisson_report* report);
+/* The aggregation-AMG hierarchy of the cfg_poisson_setup system, built (or
+ * refreshed for new values) here rather than inside the first AMG solve:
+ * out[0] levels, out[1..8] rows per level, out[9] host structure set-up ms
+ * (plain aggregation, Galerkin gather lists; once per mesh), out[10] value
+ * set-up ms (device Galerkin sums and the coarsest dense inverse). */
+int cfg_poisson_amg_setup(cfg_ctx* ctx, double out[11]);
+/* One V-cycle of that hierarchy, z = V(r) (host vectors, original order):
+ * the preconditioner as CFG_POISSON_FCG_AMG applies it, for tests. */
+int cfg_poisson_amg_apply(cfg_ctx* ctx, const double* r, double* z);
 
 /* ---- diagnostics used by the parity tests (no reference counterpart) ----- */
 
