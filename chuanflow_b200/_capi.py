@@ -14,7 +14,7 @@ BC = {"fixedValue": 0, "zeroGradient": 1, "fixedGradient": 2, "symmetry": 3, "ou
       "empty": 6}
 GRAD = {"linear": 0, "corrected": 1, "leastSquares": 2}
 DIV = {"upwind": 0, "linear": 1, "blend": 2, "linearUpwind": 3}
-PRECOND = {"Jacobi": 0, "DIC": 1, "MPNN": 2}
+PRECOND = {"Jacobi": 0, "DIC": 1, "MPNN": 2, "AMG": 3}
 
 _f64p = C.POINTER(C.c_double)
 _i64p = C.POINTER(C.c_int64)

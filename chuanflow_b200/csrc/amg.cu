@@ -53,8 +53,9 @@ struct AmgLevel
 /// Device scalars of the device-resident flexible CG (amgFcg)
 struct FcgState
 {
-    double tol, bn, pq, alpha, beta, rn;
+    double tol, bn, pq, alpha, beta, rn, init;
     int it, maxIter, done, conv;
+    int normType;  // 1: |r|2 / |b|2 <= tol; 0: |r|inf / max(|b|inf, 1e-300) < tol (the reference's test)
     unsigned int ticket[4];
 };
 
@@ -65,7 +66,8 @@ struct AmgState
         for (auto& g : graphs) cudaGraphExecDestroy(g.second);
         if (stHost) cudaFreeHost(stHost);
     }
-    std::vector<std::pair<std::pair<const void*, int>, cudaGraphExec_t>> graphs;  // (values, chunk) -> graph
+    // (values, solution vector, chunk) -> graph
+    std::vector<std::pair<std::pair<std::pair<const void*, const void*>, int>, cudaGraphExec_t>> graphs;
     FcgState* st = nullptr;
     FcgState* stHost = nullptr;
     std::vector<AmgLevel> lv;
@@ -597,6 +599,7 @@ __global__ void __launch_bounds__(TPB) k_fcgd_init(DMat A, const double* __restr
                                                    const double* __restrict__ x, double* __restrict__ r,
                                                    double* partials, FcgState* st)
 {
+    const bool inf = st->normType == 0;
     double s[2] = {0.0, 0.0};
     const double* xs[1] = {x};
     FOR_ROWS(c, A.n)
@@ -605,10 +608,19 @@ __global__ void __launch_bounds__(TPB) k_fcgd_init(DMat A, const double* __restr
         spmv_row<W, 1>(A, val, c, xs, y);
         const double bc = b[c], rc = bc - y[0];
         r[c] = rc;
-        s[0] += rc * rc;
-        s[1] += bc * bc;
+        if (inf)
+        {
+            s[0] = smax(s[0], fabs(rc));
+            s[1] = smax(s[1], fabs(bc));
+        }
+        else
+        {
+            s[0] += rc * rc;
+            s[1] += bc * bc;
+        }
     }
-    block_sum<2>(s);
+    if (inf) block_max<2>(s);
+    else block_sum<2>(s);
     const int G = gridDim.x;
     if (threadIdx.x == 0)
     {
@@ -617,14 +629,25 @@ __global__ void __launch_bounds__(TPB) k_fcgd_init(DMat A, const double* __restr
     }
     if (!last_block(&st->ticket[0])) return;
     double f[2];
-    final_sum<2>(partials, G, f);
+    if (inf) final_max<2>(partials, G, f);
+    else final_sum<2>(partials, G, f);
     if (threadIdx.x == 0)
     {
         st->ticket[0] = 0;
-        st->rn = sqrt(f[0]);
-        st->bn = sqrt(f[1]);
         st->it = 0;
-        st->conv = !(st->bn > 0) || st->rn / st->bn <= st->tol;
+        if (inf)
+        {
+            st->rn = f[0];
+            st->bn = smax(f[1], 1e-300);
+            st->conv = st->rn / st->bn < st->tol;
+        }
+        else
+        {
+            st->rn = sqrt(f[0]);
+            st->bn = sqrt(f[1]);
+            st->conv = !(st->bn > 0) || st->rn / st->bn <= st->tol;
+        }
+        st->init = st->rn;
         st->done = st->conv || st->maxIter <= 0;
     }
 }
@@ -675,6 +698,7 @@ __global__ void __launch_bounds__(TPB) k_fcgd_update(int n, const double* __rest
                                                      FcgState* st)
 {
     if (st->done) return;
+    const bool inf = st->normType == 0;
     const double al = st->alpha;
     double s[1] = {0.0};
     FOR_ROWS(c, n)
@@ -682,19 +706,21 @@ __global__ void __launch_bounds__(TPB) k_fcgd_update(int n, const double* __rest
         x[c] = x[c] + al * p[c];
         const double rc = r[c] - al * q[c];
         r[c] = rc;
-        s[0] += rc * rc;
+        s[0] = inf ? smax(s[0], fabs(rc)) : s[0] + rc * rc;
     }
-    block_sum<1>(s);
+    if (inf) block_max<1>(s);
+    else block_sum<1>(s);
     if (threadIdx.x == 0) partials[blockIdx.x] = s[0];
     if (!last_block(&st->ticket[1])) return;
     double f[1];
-    final_sum<1>(partials, gridDim.x, f);
+    if (inf) final_max<1>(partials, gridDim.x, f);
+    else final_sum<1>(partials, gridDim.x, f);
     if (threadIdx.x == 0)
     {
         st->ticket[1] = 0;
         st->it = st->it + 1;
-        st->rn = sqrt(f[0]);
-        if (st->rn / st->bn <= st->tol)
+        st->rn = inf ? f[0] : sqrt(f[0]);
+        if (inf ? st->rn / st->bn < st->tol : st->rn / st->bn <= st->tol)
         {
             st->conv = 1;
             st->done = 1;
@@ -718,11 +744,12 @@ __global__ void __launch_bounds__(TPB) k_fcgd_p(int n, const double* __restrict_
 }  // namespace
 
 /// Flexible CG (FCG(1): alpha = p.r / p.q, beta = -z.q / p.q) with the AMG
-/// V-cycle as preconditioner, to |b - A x|2 / |b|2 <= tol, with every scalar
-/// on the device: the host polls the state once per chunk of iterations,
-/// and each chunk is a CUDA graph captured once.  out: {iterations,
-/// converged}.
-void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int64_t* out)
+/// V-cycle as preconditioner, to |b - A x|2 / |b|2 <= tol (normType 1) or
+/// the reference's |r|inf test (0), with every scalar on the device: the
+/// host polls the state once per chunk of iterations, and each chunk is a
+/// CUDA graph captured once.
+void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,
+                 cfg_solver_report* rep)
 {
     AmgState& a = *amg_;
     const int n = dm_.nC;
@@ -739,6 +766,7 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
     FcgState init{};
     init.tol = tol;
     init.maxIter = maxIter;
+    init.normType = normType;
     CFG_CUDA(cudaMemcpyAsync(a.st, &init, sizeof(FcgState), cudaMemcpyHostToDevice, stream_));
     auto spmvInit = [&](auto Wc) {
         constexpr int W = decltype(Wc)::value;
@@ -767,7 +795,7 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
         CFG_CUDA(cudaStreamSynchronize(stream_));
         if (a.stHost->done || launched >= maxIter) break;
         const int m = std::min(chunk, maxIter - launched);
-        const std::pair<const void*, int> key{vals, m};
+        const std::pair<std::pair<const void*, const void*>, int> key{{vals, x}, m};
         cudaGraphExec_t ge = nullptr;
         for (auto& g : a.graphs)
             if (g.first == key) ge = g.second;
@@ -788,8 +816,10 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
         launched += m;
         chunk = std::min(chunk * 2, 32);
     }
-    out[0] = a.stHost->it;
-    out[1] = a.stHost->conv;
+    rep->iterations = a.stHost->it;
+    rep->converged = a.stHost->conv;
+    rep->initial_residual = a.stHost->init;
+    rep->final_residual = a.stHost->rn;
 }
 
 void Ctx::amgInfo(double* out)

@@ -694,7 +694,8 @@ CaseSpec parseCase(const char* path)
     if (d.has("gpu"))
     {
         const cfg::Dict& g = d.dict("gpu");
-        c.p_precond = g.wordOr("pPreconditioner", "Jacobi") == "DIC" ? CFG_PRECOND_DIC : CFG_PRECOND_JACOBI;
+        const std::string pp = g.wordOr("pPreconditioner", "Jacobi");
+        c.p_precond = pp == "DIC" ? CFG_PRECOND_DIC : (pp == "AMG" ? CFG_PRECOND_AMG : CFG_PRECOND_JACOBI);
         c.p_ref_cell = static_cast<int64_t>(g.numberOr("pRefCell", -1));
         c.p_ref_value = g.numberOr("pRefValue", 0.0);
         c.verbose = static_cast<int32_t>(g.numberOr("verbose", 1));

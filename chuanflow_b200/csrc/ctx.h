@@ -203,7 +203,8 @@ private:
     void amgValues(const double* vals, const double* diag, const float* vals32);
     void amgApply(const double* r, double* z);
     void amgCycle(const double* r, double* z, const double* q, FcgState* st);
-    void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int64_t* out);
+    void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,
+                cfg_solver_report* rep);
     void amgInfo(double* out);
     bool amgFresh_ = false;  // the hierarchy's values match the Poisson system
     void mpnnApply(const double* vals, const double* diag, const double* r, double* z);

@@ -1721,6 +1721,20 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
             rep.iterations = static_cast<int32_t>(o[0] + o[1]);
             lastFallbackIters += o[1];
         }
+        else if (precond == CFG_PRECOND_AMG)
+        {
+            // the FP32 AMG hierarchy follows this outer iteration's matrix
+            if (pass == 0)
+            {
+                const int nE = nSlicesEntries_;
+                if (!pVal32_) pVal32_ = alloc<float>(static_cast<size_t>(nE));
+                k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, pVal_d_, pVal32_);
+                launchCheck("amg_float");
+                amgValues(pVal_d_, pDiag_, pVal32_);
+                amgFresh_ = false;  // the Poisson system, if any, must refresh its own
+            }
+            amgFcg(pVal_d_, pRhs_, px_, tol, maxIter, 0, &rep);
+        }
         else runCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
         inner += rep.iterations;
     }
@@ -2407,9 +2421,8 @@ void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int m
     else if (method == 4)
     {
         // flexible CG with the FP32 AMG V-cycle, every scalar on the device
-        int64_t o[2];
-        amgFcg(pVal_d_, pb64_, px64_, tol, maxIter, o);
-        inner = o[0];
+        amgFcg(pVal_d_, pb64_, px64_, tol, maxIter, 1, &rep);
+        inner = rep.iterations;
         outer = 1;
     }
     else if (method == 5)

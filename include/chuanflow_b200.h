@@ -60,9 +60,12 @@ enum cfg_div_scheme { CFG_DIV_UPWIND = 0, CFG_DIV_LINEAR = 1, CFG_DIV_BLEND = 2,
 enum cfg_lin_method { CFG_SOLVE_CG = 0, CFG_SOLVE_BICGSTAB = 1 };
 /* pressure preconditioner: the reference's Jacobi PCG, or this library's
  * multicolour DIC (no reference counterpart) */
-enum cfg_precond { CFG_PRECOND_JACOBI = 0, CFG_PRECOND_DIC = 1, CFG_PRECOND_MPNN = 2 };
+enum cfg_precond { CFG_PRECOND_JACOBI = 0, CFG_PRECOND_DIC = 1, CFG_PRECOND_MPNN = 2, CFG_PRECOND_AMG = 3 };
 /* CFG_PRECOND_MPNN: flexible CG with the learned preconditioner (cfg_mpnn_*),
- * the reference's infinity-norm test, FP64 DIC-PCG when it stalls */
+ * the reference's infinity-norm test, FP64 DIC-PCG when it stalls.
+ * CFG_PRECOND_AMG: FP64 flexible CG, device-resident, preconditioned by an
+ * FP32 aggregation-AMG V-cycle rebuilt from each outer iteration's matrix
+ * (hierarchy structure once per context), the reference's infinity-norm test */
 
 /* Schemes (src/3d/include/cf/fvm/FvMatrix.h:30-38) */
 typedef struct cfg_schemes

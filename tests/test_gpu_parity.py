@@ -140,6 +140,22 @@ def test_simple_cavity_dic_matches_oracle(cells, jitter):
     assert rel(U, U0) < REL_TOL and rel(p, p0) < REL_TOL and rel(phi, phi0) < REL_TOL
 
 
+def test_simple_cavity_amg_pressure_matches_oracle():
+    """SIMPLE with the FP32-AMG flexible-CG pressure solve against the
+    oracle's DIC run: the pressure solves stop at the same 1e-10 infinity-norm
+    test, so the outer iterations agree to the SIMPLE bar."""
+    oc = K.cavity_case(10, 9, 8, jitter=0.1, iters=6, linear_tol=1e-10, nu=0.0025)
+    oc.p_ref_cell = 0
+    oc.p_precond = 1
+    U0, p0, phi0, r0 = oc.run()
+    mesh, case = K.cavity_product(10, 9, 8, jitter=0.1)
+    res = case.solve(K.controls_from(oc, p_preconditioner="AMG"))
+    U, p, phi = case.download()
+    assert res.iterations == r0.iterations
+    assert res.p_inner_iterations * 2 < r0.pItersTotal, (res.p_inner_iterations, r0.pItersTotal)
+    assert rel(U, U0) < REL_TOL and rel(p, p0) < REL_TOL and rel(phi, phi0) < REL_TOL
+
+
 @pytest.mark.parametrize("order", ["colour", "rcm-colour"])
 @pytest.mark.parametrize("method", ["jacobi64", "dic64", "ir32"])
 def test_poisson_solves_match_oracle(method, order):
