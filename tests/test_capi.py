@@ -103,6 +103,9 @@ def test_case_file_defaults_and_gpu_block(tmp_path):
     assert s["simple"] == [200.0, 1e-6, 0.0, 0.0, 1e-7, 2000.0, 2.0, 0.7, 0.3, 0.0]
     assert s["schemes"] == [0.0, 1.0, 1.0, 0.9]
     assert s["gpu"] == [0.0, 3.0, 1.5]
+    for word, code in (("DIC", 1.0), ("AMG", 3.0)):
+        s = cf.inspect_case_file(write(tmp_path, text.replace("gpu {", f"gpu {{ pPreconditioner {word};")))
+        assert s["gpu"] == [code, 3.0, 1.5]
 
 
 @pytest.mark.parametrize("text,msg", [
