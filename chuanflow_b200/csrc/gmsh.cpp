@@ -19,6 +19,7 @@
 #include <set>
 #include <string>
 #include <string_view>
+#include <charconv>
 #include <unordered_map>
 #include <vector>
 
@@ -29,7 +30,20 @@ namespace cfg
 namespace
 {
 
-using Row = std::vector<std::string_view>;
+/// the tokens of one row: a view into its section's flat token array
+class Row
+{
+public:
+    Row() = default;
+    Row(const std::string_view* b, size_t n) : b_(b), n_(n) {}
+    size_t size() const { return n_; }
+    bool empty() const { return n_ == 0; }
+    const std::string_view& operator[](size_t i) const { return b_[i]; }
+
+private:
+    const std::string_view* b_ = nullptr;
+    size_t n_ = 0;
+};
 
 int nodesPerElement(int type)
 {
@@ -48,6 +62,15 @@ int nodesPerElement(int type)
 
 long toInt(std::string_view t, const char* where)
 {
+    {
+        // the common case without a copy: the whole token is the number
+        long v = 0;
+        const char* b = t.data();
+        const char* e = b + t.size();
+        if (b < e && *b == '+') ++b;
+        const auto r = std::from_chars(b, e, v);
+        if (r.ec == std::errc() && r.ptr == e) return v;
+    }
     std::string s(t);
     char* end = nullptr;
     errno = 0;
@@ -58,6 +81,15 @@ long toInt(std::string_view t, const char* where)
 
 double toDouble(std::string_view t, const char* where)
 {
+    {
+        // from_chars rounds correctly, as strtod does
+        double v = 0;
+        const char* b = t.data();
+        const char* e = b + t.size();
+        if (b < e && *b == '+') ++b;
+        const auto r = std::from_chars(b, e, v);
+        if (r.ec == std::errc() && r.ptr == e) return v;
+    }
     std::string s(t);
     char* end = nullptr;
     const double v = std::strtod(s.c_str(), &end);
@@ -72,7 +104,17 @@ class Section
 {
 public:
     Section() = default;
-    Section(std::vector<Row> rows, std::string where) : rows_(std::move(rows)), where_(std::move(where)) {}
+    /// rows over `tokens` (kept here, so the rows' views stay valid)
+    Section(std::vector<std::string_view> tokens, const std::vector<size_t>& start, std::string where)
+        : tok_(std::move(tokens)), where_(std::move(where))
+    {
+        rows_.reserve(start.empty() ? 0 : start.size() - 1);
+        for (size_t k = 0; k + 1 < start.size(); ++k) rows_.emplace_back(tok_.data() + start[k], start[k + 1] - start[k]);
+    }
+    Section(Section&&) = default;
+    Section& operator=(Section&&) = default;
+    Section(const Section&) = delete;
+    Section& operator=(const Section&) = delete;
     bool found() const { return !rows_.empty(); }
     bool atEnd() const { return pos_ >= rows_.size(); }
     const Row& take()
@@ -90,6 +132,7 @@ public:
     }
 
 private:
+    std::vector<std::string_view> tok_;
     std::vector<Row> rows_;
     size_t pos_ = 0;
     std::string where_;
@@ -100,9 +143,10 @@ struct File
     std::string text;
     std::vector<std::pair<size_t, size_t>> lines;  // [begin, end) of every line
 
-    Row tokens(size_t li) const
+    /// appends the tokens of line li; returns how many
+    size_t tokens(size_t li, std::vector<std::string_view>& out) const
     {
-        Row r;
+        const size_t before = out.size();
         const char* s = text.data() + lines[li].first;
         const char* e = text.data() + lines[li].second;
         while (s < e)
@@ -110,9 +154,9 @@ struct File
             while (s < e && (*s == ' ' || *s == '\t' || *s == '\r' || *s == '\v' || *s == '\f')) ++s;
             const char* b = s;
             while (s < e && !(*s == ' ' || *s == '\t' || *s == '\r' || *s == '\v' || *s == '\f')) ++s;
-            if (s > b) r.emplace_back(b, static_cast<size_t>(s - b));
+            if (s > b) out.emplace_back(b, static_cast<size_t>(s - b));
         }
-        return r;
+        return out.size() - before;
     }
 
     std::string_view first(size_t li) const
@@ -134,14 +178,12 @@ struct File
             for (size_t j = i + 1; j < lines.size(); ++j)
             {
                 if (first(j) != end) continue;
-                std::vector<Row> rows;
-                rows.reserve(j - i - 1);
+                std::vector<std::string_view> tok;
+                std::vector<size_t> start{0};
+                start.reserve(j - i);
                 for (size_t k = i + 1; k < j; ++k)
-                {
-                    Row t = tokens(k);
-                    if (!t.empty()) rows.push_back(std::move(t));
-                }
-                return Section(std::move(rows), begin + " in " + path);
+                    if (tokens(k, tok) > 0) start.push_back(tok.size());  // empty lines make no row
+                return Section(std::move(tok), start, begin + " in " + path);
             }
             fail(CFG_EMESH, "gmsh: section " + begin + " in " + path + " is not terminated");
         }

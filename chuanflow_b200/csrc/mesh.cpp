@@ -355,8 +355,16 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
     const int64_t nCells = static_cast<int64_t>(types.size());
     std::vector<int64_t> ringVerts;
     std::vector<Ref> refs;
-    std::unordered_map<std::array<int64_t, 5>, int64_t, FaceKeyHash> index;
-    index.reserve(static_cast<size_t>(4 * nCells));
+    // open addressing over the sorted vertex keys (no allocation per face):
+    // the table holds face indices, the keys sit beside the faces
+    std::vector<std::array<int64_t, 5>> keys;
+    size_t cap = 16;
+    while (cap < static_cast<size_t>(8 * std::max<int64_t>(nCells, 1))) cap <<= 1;
+    std::vector<int64_t> table(cap, -1);
+    const FaceKeyHash hasher;
+    ringVerts.reserve(static_cast<size_t>(4 * 4 * nCells));
+    refs.reserve(static_cast<size_t>(4 * nCells));
+    keys.reserve(static_cast<size_t>(4 * nCells));
     for (int64_t c = 0; c < nCells; ++c)
     {
         const auto& rings = faceRings(types[static_cast<size_t>(c)]);
@@ -369,21 +377,37 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
             std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
             for (size_t k = 0; k < ring.size(); ++k) key[k] = cv[ring[k]];
             std::sort(key.begin(), key.begin() + static_cast<long>(ring.size()));
-            auto it = index.find(key);
-            if (it == index.end())
+            size_t h = hasher(key) & (cap - 1);
+            while (table[h] >= 0 && keys[static_cast<size_t>(table[h])] != key) h = (h + 1) & (cap - 1);
+            if (table[h] < 0)
             {
-                index.emplace(key, static_cast<int64_t>(refs.size()));
+                table[h] = static_cast<int64_t>(refs.size());
+                keys.push_back(key);
                 refs.push_back({static_cast<int64_t>(ringVerts.size()), static_cast<int64_t>(ring.size()), c, -1});
                 for (int k : ring) ringVerts.push_back(cv[k]);
+                if (2 * refs.size() > cap)
+                {
+                    // keep the load under one half: rebuild at twice the size
+                    cap <<= 1;
+                    table.assign(cap, -1);
+                    for (size_t i = 0; i < refs.size(); ++i)
+                    {
+                        size_t g = hasher(keys[i]) & (cap - 1);
+                        while (table[g] >= 0) g = (g + 1) & (cap - 1);
+                        table[g] = static_cast<int64_t>(i);
+                    }
+                }
             }
             else
             {
-                Ref& r = refs[static_cast<size_t>(it->second)];
+                Ref& r = refs[static_cast<size_t>(table[h])];
                 if (r.cell1 != -1) fail(CFG_EMESH, "mesh: a face belongs to three cells: the mesh is not manifold");
                 r.cell1 = c;
             }
         }
     }
+    std::vector<int64_t>().swap(table);
+    std::vector<std::array<int64_t, 5>>().swap(keys);
     // boundary faces named after the bounding-box plane they lie on
     // (gmshMesh.cpp:636-667, the case of a file without surface groups)
     Vec lo = points[0], hi = points[0];

@@ -9,6 +9,7 @@
 //
 // Modes (all take the case dictionary the reference app would read):
 //   mesh   <case.dict> <out> [points.f64]             addressing + geometry
+//   meshtime <case.dict>                              seconds to load the case's mesh, cells, faces
 //   grad   <case.dict> <out> <points|-> <T.f64> <bvals.f64>
 //                                                     fvc::grad, both overloads
 //   simple <case.dict> <out> [points|-] [statedir]    solveIncompressibleSimple
@@ -197,6 +198,17 @@ void loadState(const std::string& dir, volVectorField& U, volScalarField& p, sur
         U.internalField()[i] = {u[3 * i], u[3 * i + 1], u[3 * i + 2]};
     for (std::size_t i = 0; i < p.internalField().size(); ++i) p.internalField()[i] = pp[i];
     for (std::size_t i = 0; i < phi.values().size(); ++i) phi.values()[i] = ph[i];
+}
+
+/// the reference's mesh loading alone, timed (reader throughput)
+int modeMeshTime(int argc, char** argv)
+{
+    const Dictionary dict = Dictionary::parseFile(argv[2]);
+    const auto t0 = std::chrono::steady_clock::now();
+    const polyMesh mesh = MeshLoader::fromCase(dict, argv[2]);
+    const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::cout << std::setprecision(6) << s << " " << mesh.nCells() << " " << mesh.nFaces() << "\n";
+    return 0;
 }
 
 int modeMesh(int argc, char** argv)
@@ -506,6 +518,7 @@ int main(int argc, char** argv)
     {
         const std::string mode = argv[1];
         if (mode == "mesh" && argc >= 4) return modeMesh(argc, argv);
+        if (mode == "meshtime" && argc >= 3) return modeMeshTime(argc, argv);
         if (mode == "grad" && argc >= 7) return modeGrad(argc, argv);
         if (mode == "simple" && argc >= 4) return modeSimple(argc, argv);
         if (mode == "rans" && argc >= 4) return modeRans(argc, argv);
