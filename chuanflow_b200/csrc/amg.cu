@@ -799,6 +799,8 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
         cudaGraphExec_t ge = nullptr;
         for (auto& g : a.graphs)
             if (g.first == key) ge = g.second;
+        // every chunk counts its kernels once, replayed or eager
+        const int64_t counted = launches_;
         if (!ge && useGraphs_)
         {
             cudaGraph_t g = nullptr;
@@ -813,6 +815,7 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
         if (ge) CFG_CUDA(cudaGraphLaunch(ge, stream_));
         else
             for (int k = 0; k < m; ++k) iteration();
+        launches_ = counted + static_cast<int64_t>(m) * (3 + 3 * (static_cast<int>(a.lv.size()) - 1) + 1);
         launched += m;
         chunk = std::min(chunk * 2, 32);
     }
