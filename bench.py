@@ -329,7 +329,7 @@ def main_transient(args, world, rank, local, dist):
     batch = cf.Batch([case])
     batch.save()
     legs = {}
-    for name, pre in (("dic64", "DIC"), ("learned_fcg", "MPNN")):
+    for name, pre in (("dic64", "DIC"), ("amg32", "AMG"), ("learned_fcg", "MPNN")):
         batch.restore()
         c2 = dataclasses.replace(ctl, p_preconditioner=pre)
         ms, pit, fin = [], 0, None
@@ -342,6 +342,7 @@ def main_transient(args, world, rank, local, dist):
         legs[name] = {"ms_per_step": statistics.mean(ms), "pressure_iterations_per_step": pit / max(1, len(ms)),
                       "continuity_last": fin["continuity_error"], "U": U}
     dU = float(np.linalg.norm(legs["learned_fcg"]["U"] - legs["dic64"]["U"]) / np.linalg.norm(legs["dic64"]["U"]))
+    dUa = float(np.linalg.norm(legs["amg32"]["U"] - legs["dic64"]["U"]) / np.linalg.norm(legs["dic64"]["U"]))
     for v in legs.values():
         v.pop("U")
     if rank == 0:
@@ -354,9 +355,11 @@ def main_transient(args, world, rank, local, dist):
                                       f"at CFL 0.5 (dt {dt:g}), {steps} steps: the first {n_train} with DIC-PCG "
                                       f"generate the training residuals, the rest are timed twice from the same "
                                       f"fields", "cells": ncell},
-               "legs": legs, "rel_L2_U_learned_vs_dic": dU, "simulation_s_training_steps": sim_s,
+               "legs": legs, "rel_L2_U_learned_vs_dic": dU, "rel_L2_U_amg32_vs_dic": dUa,
+               "simulation_s_training_steps": sim_s,
                "train_s": train_s, "train_loss_first": float(losses[0]), "train_loss_last": float(losses[-1]),
-               "speedup_learned_vs_dic": legs["dic64"]["ms_per_step"] / legs["learned_fcg"]["ms_per_step"]}
+               "speedup_learned_vs_dic": legs["dic64"]["ms_per_step"] / legs["learned_fcg"]["ms_per_step"],
+               "speedup_amg32_vs_dic": legs["dic64"]["ms_per_step"] / legs["amg32"]["ms_per_step"]}
         print(json.dumps(out), flush=True)
 
 
