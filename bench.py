@@ -267,7 +267,9 @@ def main_reference(args, world, rank, dist):
     v = n ** 3 * steps / secs
     out = {"metric": METRIC, "impl": "reference", "value": v, "unit": "cell-iter/s", "n_gpus": args.gpus,
            "steps": steps, "warmup": 0, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(n),
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           # the same config object as the B200 line; the reference's own solver choice is in the sample
+           "config": dict(workload_config(n, args.p_precond), parallelism="reference CPU, one core"),
            "cpu_baseline": {"value": v, "unit": "cell-iter/s", "cores": 1, "kind": kind,
                             "sample": f"one SIMPLE outer iteration of the {n}^3 case from rest (a step of the "
                                       f"timed loop); the reference has no pressure reference cell, so its "
