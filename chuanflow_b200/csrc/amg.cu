@@ -83,8 +83,8 @@ void AmgDeleter::operator()(AmgState* a) const { delete a; }
 namespace
 {
 
-constexpr float kOmega = 0.67f;   // damped Jacobi
-constexpr float kScale = 1.8f;    // coarse-correction scaling
+constexpr float kOmega = 0.8f;    // damped Jacobi
+constexpr float kScale = 2.0f;    // coarse-correction scaling
 constexpr int kDenseMax = 128;
 
 /// one SELL row of the finest operator: sum over its entries of val * f(col).

@@ -2,13 +2,13 @@
 the aggregation-AMG V-cycle the GPU applies as the pressure preconditioner
 (no reference counterpart).  Same aggregation (rows in order, entries in
 row order), Galerkin sums in FP64 stored in FP32, FP32 damped Jacobi with
-w = 0.67, coarse correction scaled by 1.8, coarsest level (<= 128 rows)
+w = 0.8, coarse correction scaled by 2.0, coarsest level (<= 128 rows)
 inverted densely with a 1e-6 max|diag| shift."""
 import numpy as np
 import scipy.sparse as sp
 
-OMEGA = np.float32(0.67)
-SCALE = np.float32(1.8)
+OMEGA = np.float32(0.8)
+SCALE = np.float32(2.0)
 DENSE_MAX = 128
 
 
