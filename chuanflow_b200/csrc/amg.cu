@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, i
     const int l = threadIdx.x % kGroup;
     const int stride = gridDim.x * (TPB / kGroup);
     // whole warps iterate together (the shuffle needs every lane)
-    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup - 0; ; i0 += stride)
+    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
     {
         const int base = i0 - (threadIdx.x % 32) / kGroup;  // the warp's first row this round
         if (base >= n) break;
