@@ -2,9 +2,12 @@
 // libchuanflow_b200.so.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
+#include <exception>
 #include <stdexcept>
 #include <array>
+#include <thread>
 #include <map>
 #include <string>
 #include <unordered_map>
@@ -26,6 +29,39 @@ struct Error : std::runtime_error
 
 /// Sets the calling thread's message for cfg_last_error (api.cpp).
 void setLastError(const std::string& msg);
+
+/// Runs fn(begin, end) over [0, n) in contiguous chunks of at least
+/// `minChunk` items on the host's threads.  Chunks must be independent;
+/// if any throw, the exception of the lowest such chunk is rethrown, which
+/// is the one a serial loop would have met first.
+template <class F>
+void parallelChunks(int64_t n, int64_t minChunk, F&& fn)
+{
+    const int64_t hw = std::max<int64_t>(1, std::thread::hardware_concurrency());
+    const int64_t t = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 32), n / std::max<int64_t>(1, minChunk)));
+    if (t == 1)
+    {
+        if (n > 0) fn(int64_t(0), n);
+        return;
+    }
+    std::vector<std::exception_ptr> err(static_cast<size_t>(t));
+    std::vector<std::thread> th;
+    th.reserve(static_cast<size_t>(t));
+    for (int64_t k = 0; k < t; ++k)
+        th.emplace_back([&, k] {
+            try
+            {
+                fn(n * k / t, n * (k + 1) / t);
+            }
+            catch (...)
+            {
+                err[static_cast<size_t>(k)] = std::current_exception();
+            }
+        });
+    for (auto& x : th) x.join();
+    for (const auto& e : err)
+        if (e) std::rethrow_exception(e);
+}
 
 struct Vec
 {

@@ -123,6 +123,10 @@ public:
             fail(CFG_EMESH, "gmsh: truncated file: " + where_ + " ends after " + std::to_string(rows_.size()) + " rows");
         return rows_[pos_++];
     }
+    size_t remaining() const { return rows_.size() - pos_; }
+    /// row k after the current one, not consumed (k < remaining())
+    const Row& peek(size_t k) const { return rows_[pos_ + k]; }
+    void skip(size_t n) { pos_ += n; }
     bool takeSingleInt(long& v)
     {
         if (atEnd() || rows_[pos_].size() != 1 || !isIntegerToken(rows_[pos_][0])) return false;
@@ -142,6 +146,7 @@ struct File
 {
     std::string text;
     std::vector<std::pair<size_t, size_t>> lines;  // [begin, end) of every line
+    std::vector<size_t> marks;                     // the lines whose first token starts with '$'
 
     /// appends the tokens of line li; returns how many
     size_t tokens(size_t li, std::vector<std::string_view>& out) const
@@ -171,18 +176,50 @@ struct File
 
     Section section(const std::string& name, const std::string& path, bool required) const
     {
+        // only the '$' lines can open or close a section
         const std::string begin = "$" + name, end = "$End" + name;
-        for (size_t i = 0; i < lines.size(); ++i)
+        for (size_t mi = 0; mi < marks.size(); ++mi)
         {
+            const size_t i = marks[mi];
             if (first(i) != begin) continue;
-            for (size_t j = i + 1; j < lines.size(); ++j)
+            for (size_t mj = mi + 1; mj < marks.size(); ++mj)
             {
+                const size_t j = marks[mj];
                 if (first(j) != end) continue;
-                std::vector<std::string_view> tok;
-                std::vector<size_t> start{0};
-                start.reserve(j - i);
-                for (size_t k = i + 1; k < j; ++k)
-                    if (tokens(k, tok) > 0) start.push_back(tok.size());  // empty lines make no row
+                // lines tokenized in parallel chunks, then joined in order
+                const int64_t nl = static_cast<int64_t>(j - i - 1);
+                const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(64, nl / 8192));
+                std::vector<std::vector<std::string_view>> ptok(static_cast<size_t>(parts));
+                std::vector<std::vector<size_t>> pend(static_cast<size_t>(parts));
+                parallelChunks(parts, 1, [&](int64_t pb, int64_t pe) {
+                    for (int64_t q = pb; q < pe; ++q)
+                    {
+                        auto& tq = ptok[static_cast<size_t>(q)];
+                        auto& eq = pend[static_cast<size_t>(q)];
+                        const size_t lb = i + 1 + static_cast<size_t>(nl * q / parts);
+                        const size_t le = i + 1 + static_cast<size_t>(nl * (q + 1) / parts);
+                        eq.reserve(le - lb);
+                        for (size_t k = lb; k < le; ++k)
+                            if (tokens(k, tq) > 0) eq.push_back(tq.size());  // empty lines make no row
+                    }
+                });
+                std::vector<size_t> tokBase(static_cast<size_t>(parts) + 1, 0), rowBase(static_cast<size_t>(parts) + 1, 0);
+                for (size_t q = 0; q < static_cast<size_t>(parts); ++q)
+                {
+                    tokBase[q + 1] = tokBase[q] + ptok[q].size();
+                    rowBase[q + 1] = rowBase[q] + pend[q].size();
+                }
+                std::vector<std::string_view> tok(tokBase.back());
+                std::vector<size_t> start(rowBase.back() + 1, 0);
+                parallelChunks(parts, 1, [&](int64_t pb, int64_t pe) {
+                    for (int64_t q = pb; q < pe; ++q)
+                    {
+                        const size_t u = static_cast<size_t>(q);
+                        std::copy(ptok[u].begin(), ptok[u].end(), tok.begin() + static_cast<long>(tokBase[u]));
+                        for (size_t r = 0; r < pend[u].size(); ++r) start[rowBase[u] + r + 1] = tokBase[u] + pend[u][r];
+                        std::vector<std::string_view>().swap(ptok[u]);
+                    }
+                });
                 return Section(std::move(tok), start, begin + " in " + path);
             }
             fail(CFG_EMESH, "gmsh: section " + begin + " in " + path + " is not terminated");
@@ -215,12 +252,21 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
         std::fclose(fp);
         if (got != f.text.size()) fail(CFG_EMESH, "gmsh: cannot read " + path);
         size_t b = 0;
-        for (size_t i = 0; i <= f.text.size(); ++i)
-            if (i == f.text.size() || f.text[i] == '\n')
+        const char* t = f.text.data();
+        const size_t n = f.text.size();
+        while (b <= n)
+        {
+            const void* nl = b < n ? std::memchr(t + b, '\n', n - b) : nullptr;
+            const size_t i = nl ? static_cast<size_t>(static_cast<const char*>(nl) - t) : n;
+            if (i < n || i > b)
             {
-                if (i < f.text.size() || i > b) f.lines.push_back({b, i});
-                b = i + 1;
+                size_t k = b;
+                while (k < i && std::isspace(static_cast<unsigned char>(t[k]))) ++k;
+                if (k < i && t[k] == '$') f.marks.push_back(f.lines.size());
+                f.lines.push_back({b, i});
             }
+            b = i + 1;
+        }
     }
 
     Section fmt = f.section("MeshFormat", path, true);
@@ -256,7 +302,21 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
 
     // nodes, renumbered densely in ascending tag order
     std::vector<Vec> points;
-    std::unordered_map<long, int64_t> tagIndex;
+    // node tag -> dense index: the sorted tags, searched unless they run 1..n
+    std::vector<long> sortedTags;
+    bool denseTags = true;
+    auto tagIndex = [&](long tag, int64_t& index) {
+        if (denseTags)
+        {
+            if (tag < 1 || tag > static_cast<long>(sortedTags.size())) return false;
+            index = tag - 1;
+            return true;
+        }
+        const auto it = std::lower_bound(sortedTags.begin(), sortedTags.end(), tag);
+        if (it == sortedTags.end() || *it != tag) return false;
+        index = static_cast<int64_t>(it - sortedTags.begin());
+        return true;
+    };
     {
         Section sec = f.section("Nodes", path, true);
         if (!sec.found()) fail(CFG_EMESH, "gmsh: " + path + " has an empty $Nodes section");
@@ -269,14 +329,19 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
         if (version < 3.0)
         {
             declared = toInt(sec.take()[0], "$Nodes");
-            rec.reserve(static_cast<size_t>(std::max(declared, 0L)));
-            for (long i = 0; i < declared; ++i)
-            {
-                const Row& t = sec.take();
-                if (t.size() < 4) fail(CFG_EMESH, "gmsh: malformed node line in " + path);
-                rec.push_back({toInt(t[0], "$Nodes"), Vec{toDouble(t[1], "$Nodes"), toDouble(t[2], "$Nodes"),
-                                                         toDouble(t[3], "$Nodes")}});
-            }
+            const long avail = std::max(0L, std::min(declared, static_cast<long>(sec.remaining())));
+            rec.resize(static_cast<size_t>(avail));
+            parallelChunks(avail, 1 << 14, [&](int64_t b, int64_t e) {
+                for (int64_t i = b; i < e; ++i)
+                {
+                    const Row& t = sec.peek(static_cast<size_t>(i));
+                    if (t.size() < 4) fail(CFG_EMESH, "gmsh: malformed node line in " + path);
+                    rec[static_cast<size_t>(i)] = {toInt(t[0], "$Nodes"), Vec{toDouble(t[1], "$Nodes"), toDouble(t[2], "$Nodes"),
+                                                                            toDouble(t[3], "$Nodes")}};
+                }
+            });
+            sec.skip(static_cast<size_t>(avail));
+            if (avail < declared) sec.take();  // the truncation error
         }
         else
         {
@@ -298,7 +363,13 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
                 std::vector<Vec> xyz;
                 if (documented)
                 {
-                    for (long i = 0; i < num; ++i) xyz.push_back(coords(sec.take()));
+                    const long avail = std::min(num, static_cast<long>(sec.remaining()));
+                    xyz.resize(static_cast<size_t>(avail));
+                    parallelChunks(avail, 1 << 14, [&](int64_t b, int64_t e) {
+                        for (int64_t i = b; i < e; ++i) xyz[static_cast<size_t>(i)] = coords(sec.peek(static_cast<size_t>(i)));
+                    });
+                    sec.skip(static_cast<size_t>(avail));
+                    if (avail < num) sec.take();  // the truncation error
                     if (minTag != maxTag)
                     {
                         long v = 0;
@@ -341,11 +412,13 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
         }
         std::stable_sort(rec.begin(), rec.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
         points.reserve(rec.size());
-        tagIndex.reserve(rec.size());
+        sortedTags.reserve(rec.size());
         for (const auto& r : rec)
         {
-            if (!tagIndex.emplace(r.first, static_cast<int64_t>(points.size())).second)
+            if (!sortedTags.empty() && sortedTags.back() == r.first)
                 fail(CFG_EMESH, "gmsh: duplicate node tag " + std::to_string(r.first) + " in " + path);
+            denseTags = denseTags && r.first == static_cast<long>(sortedTags.size()) + 1;
+            sortedTags.push_back(r.first);
             points.push_back(r.second);
         }
     }
@@ -397,57 +470,78 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
     {
         Section sec = f.section("Elements", path, true);
         if (!sec.found()) fail(CFG_EMESH, "gmsh: " + path + " has an empty $Elements section");
-        auto add = [&](int type, long physical, const Row& t, size_t first, int npn) {
+        // rows decode independently (in parallel); their cells and surface
+        // names are then committed in file order
+        struct Decoded
+        {
+            int type, npn;
+            long physical;
             int64_t nodes[8];
+        };
+        auto decode = [&](int type, long physical, const Row& t, size_t first, int npn, Decoded& d) {
+            d.type = type;
+            d.npn = npn;
+            d.physical = physical;
             for (int k = 0; k < npn; ++k)
             {
                 const long tag = toInt(t[first + static_cast<size_t>(k)], "$Elements");
-                const auto it = tagIndex.find(tag);
-                if (it == tagIndex.end())
+                if (!tagIndex(tag, d.nodes[k]))
                     fail(CFG_EMESH, "gmsh: an element refers to node " + std::to_string(tag) +
                                         ", which $Nodes does not define");
-                nodes[k] = it->second;
             }
-            if (std::unique(nodes, nodes + npn) != nodes + npn)
+            if (std::unique(d.nodes, d.nodes + npn) != d.nodes + npn)
                 fail(CFG_EMESH, "gmsh: element " + std::to_string(type) + " repeats a node");
-            if (type == 2 || type == 3)
+            if (type == 7) fail(CFG_EMESH, "gmsh: pyramid elements are not supported");
+        };
+        auto commit = [&](const std::vector<Decoded>& dec) {
+            for (const Decoded& d : dec)
             {
-                const auto nit = physicalNames.find(physical);
-                if (nit == physicalNames.end()) return;
-                std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
-                for (int k = 0; k < npn; ++k) key[static_cast<size_t>(k)] = nodes[k];
-                std::sort(key.begin(), key.begin() + npn);
-                surfaceNames.emplace(key, nit->second);
-            }
-            else if (type == 4 || type == 5 || type == 6)
-            {
-                types.push_back(type);
-                verts.insert(verts.end(), nodes, nodes + npn);
-                offsets.push_back(static_cast<int64_t>(verts.size()));
-            }
-            else if (type == 7)
-            {
-                fail(CFG_EMESH, "gmsh: pyramid elements are not supported");
+                if (d.type == 2 || d.type == 3)
+                {
+                    const auto nit = physicalNames.find(d.physical);
+                    if (nit == physicalNames.end()) continue;
+                    // a triangle or quad: npn is 3 or 4 here
+                    std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
+                    for (int k = 0; k < d.npn; ++k) key[static_cast<size_t>(k)] = d.nodes[k];
+                    std::sort(key.begin(), key.begin() + (d.type == 2 ? 3 : 4));
+                    surfaceNames.emplace(key, nit->second);
+                }
+                else if (d.type == 4 || d.type == 5 || d.type == 6)
+                {
+                    types.push_back(d.type);
+                    verts.insert(verts.end(), d.nodes, d.nodes + d.npn);
+                    offsets.push_back(static_cast<int64_t>(verts.size()));
+                }
             }
         };
         if (version < 3.0)
         {
             const long declared = toInt(sec.take()[0], "$Elements");
-            for (long i = 0; i < declared; ++i)
-            {
-                const Row& t = sec.take();
-                if (t.size() < 3) fail(CFG_EMESH, "gmsh: malformed element line in " + path);
-                const int type = static_cast<int>(toInt(t[1], "$Elements"));
-                const int npn = nodesPerElement(type);
-                if (npn <= 0)
-                    fail(CFG_EMESH, "gmsh: element type " + std::to_string(type) + " in " + path +
-                                        " is not a first-order element; mesh with Linear order");
-                const long nTags = toInt(t[2], "$Elements");
-                if (static_cast<long>(t.size()) < 3 + nTags + npn)
-                    fail(CFG_EMESH, "gmsh: truncated element line in " + path);
-                const long physical = nTags > 0 ? toInt(t[3], "$Elements") : 0;
-                add(type, physical, t, static_cast<size_t>(3 + nTags), npn);
-            }
+            const long avail = std::max(0L, std::min(declared, static_cast<long>(sec.remaining())));
+            std::vector<Decoded> dec(static_cast<size_t>(avail));
+            parallelChunks(avail, 1 << 13, [&](int64_t b, int64_t e) {
+                for (int64_t i = b; i < e; ++i)
+                {
+                    const Row& t = sec.peek(static_cast<size_t>(i));
+                    if (t.size() < 3) fail(CFG_EMESH, "gmsh: malformed element line in " + path);
+                    const int type = static_cast<int>(toInt(t[1], "$Elements"));
+                    const int npn = nodesPerElement(type);
+                    if (npn <= 0)
+                        fail(CFG_EMESH, "gmsh: element type " + std::to_string(type) + " in " + path +
+                                            " is not a first-order element; mesh with Linear order");
+                    const long nTags = toInt(t[2], "$Elements");
+                    if (static_cast<long>(t.size()) < 3 + nTags + npn)
+                        fail(CFG_EMESH, "gmsh: truncated element line in " + path);
+                    const long physical = nTags > 0 ? toInt(t[3], "$Elements") : 0;
+                    decode(type, physical, t, static_cast<size_t>(3 + nTags), npn, dec[static_cast<size_t>(i)]);
+                }
+            });
+            sec.skip(static_cast<size_t>(avail));
+            if (avail < declared) sec.take();  // the truncation error
+            types.reserve(dec.size());
+            offsets.reserve(dec.size() + 1);
+            verts.reserve(8 * dec.size());
+            commit(dec);
         }
         else
         {
@@ -469,24 +563,31 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
                                         " is not a first-order element; mesh with Linear order");
                 const auto pit = entityPhysical.find(entityTag);
                 const long physical = pit != entityPhysical.end() ? pit->second : 0;
+                const long avail = std::max(0L, std::min(num, static_cast<long>(sec.remaining())));
+                // the first line fixes whether the lines carry the element tag
                 bool tagged = false;
-                for (long i = 0; i < num; ++i, ++read)
+                if (avail > 0)
                 {
-                    const Row& t = sec.take();
-                    const long width = static_cast<long>(t.size());
-                    if (i == 0)
-                    {
-                        if (width == npn + 1) tagged = true;
-                        else if (width != npn)
-                            fail(CFG_EMESH, "gmsh: element line with " + std::to_string(width) + " entries, expected " +
-                                                std::to_string(npn) + " or " + std::to_string(npn + 1));
-                    }
-                    else if (width != npn + (tagged ? 1 : 0))
-                    {
-                        fail(CFG_EMESH, "gmsh: inconsistent element line width in " + path);
-                    }
-                    add(type, physical, t, tagged ? 1 : 0, npn);
+                    const long width = static_cast<long>(sec.peek(0).size());
+                    if (width == npn + 1) tagged = true;
+                    else if (width != npn)
+                        fail(CFG_EMESH, "gmsh: element line with " + std::to_string(width) + " entries, expected " +
+                                            std::to_string(npn) + " or " + std::to_string(npn + 1));
                 }
+                std::vector<Decoded> dec(static_cast<size_t>(avail));
+                parallelChunks(avail, 1 << 13, [&](int64_t lo, int64_t hi) {
+                    for (int64_t i = lo; i < hi; ++i)
+                    {
+                        const Row& t = sec.peek(static_cast<size_t>(i));
+                        if (static_cast<long>(t.size()) != npn + (tagged ? 1 : 0))
+                            fail(CFG_EMESH, "gmsh: inconsistent element line width in " + path);
+                        decode(type, physical, t, tagged ? 1 : 0, npn, dec[static_cast<size_t>(i)]);
+                    }
+                });
+                sec.skip(static_cast<size_t>(avail));
+                read += avail;
+                if (avail < num) sec.take();  // the truncation error
+                commit(dec);
             }
             if (read != declared)
                 fail(CFG_EMESH, "gmsh: $Elements declares " + std::to_string(declared) + " elements, " +

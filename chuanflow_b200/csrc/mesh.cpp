@@ -353,61 +353,76 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
         int64_t v0, nv, cell0, cell1;
     };
     const int64_t nCells = static_cast<int64_t>(types.size());
+    const int64_t nPoints = static_cast<int64_t>(points.size());
     std::vector<int64_t> ringVerts;
     std::vector<Ref> refs;
-    // open addressing over the sorted vertex keys (no allocation per face):
-    // the table holds face indices, the keys sit beside the faces
-    std::vector<std::array<int64_t, 5>> keys;
-    size_t cap = 16;
-    while (cap < static_cast<size_t>(8 * std::max<int64_t>(nCells, 1))) cap <<= 1;
-    std::vector<int64_t> table(cap, -1);
-    const FaceKeyHash hasher;
-    ringVerts.reserve(static_cast<size_t>(4 * 4 * nCells));
-    refs.reserve(static_cast<size_t>(4 * nCells));
-    keys.reserve(static_cast<size_t>(4 * nCells));
+    // every registration is filed under its smallest vertex: a first pass
+    // counts the registrations per vertex, the second scans that vertex's
+    // few earlier faces for the same key (faces of nearby cells share
+    // nearby vertices, so the buckets are visited almost in order)
+    std::vector<int64_t> bucket(static_cast<size_t>(nPoints) + 1, 0);
     for (int64_t c = 0; c < nCells; ++c)
     {
         const auto& rings = faceRings(types[static_cast<size_t>(c)]);
         if (rings.empty()) fail(CFG_EMESH, "mesh: cell type " + std::to_string(types[c]) + " is not tet (4), hex (5) or prism (6)");
-        const int64_t* cv = cellVerts.data() + cellOffsets[c];
         const int64_t need = types[c] == 4 ? 4 : (types[c] == 5 ? 8 : 6);
         if (cellOffsets[c + 1] - cellOffsets[c] != need) fail(CFG_EMESH, "mesh: cell vertex count does not fit its type");
+        const int64_t* cv = cellVerts.data() + cellOffsets[c];
+        for (int64_t k = 0; k < need; ++k)
+            if (cv[k] < 0 || cv[k] >= nPoints) fail(CFG_EMESH, "mesh: cell vertex out of range");
         for (const auto& ring : rings)
         {
-            std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
+            int64_t lo = cv[ring[0]];
+            for (size_t k = 1; k < ring.size(); ++k) lo = std::min(lo, cv[ring[k]]);
+            ++bucket[static_cast<size_t>(lo) + 1];
+        }
+    }
+    for (int64_t v = 0; v < nPoints; ++v) bucket[v + 1] += bucket[v];
+    struct Slot
+    {
+        int64_t k1, k2, k3, face;  // the sorted key after its smallest vertex (-1 padded)
+    };
+    std::vector<Slot> slots(static_cast<size_t>(bucket[nPoints]));
+    std::vector<int64_t> fill(bucket.begin(), bucket.end() - 1);
+    ringVerts.reserve(static_cast<size_t>(4 * 4 * nCells));
+    refs.reserve(static_cast<size_t>(4 * nCells));
+    for (int64_t c = 0; c < nCells; ++c)
+    {
+        const auto& rings = faceRings(types[static_cast<size_t>(c)]);
+        const int64_t* cv = cellVerts.data() + cellOffsets[c];
+        for (const auto& ring : rings)
+        {
+            std::array<int64_t, 4> key{-1, -1, -1, -1};
             for (size_t k = 0; k < ring.size(); ++k) key[k] = cv[ring[k]];
             std::sort(key.begin(), key.begin() + static_cast<long>(ring.size()));
-            size_t h = hasher(key) & (cap - 1);
-            while (table[h] >= 0 && keys[static_cast<size_t>(table[h])] != key) h = (h + 1) & (cap - 1);
-            if (table[h] < 0)
+            const size_t b = static_cast<size_t>(key[0]);
+            int64_t found = -1;
+            for (int64_t q = bucket[b]; q < fill[b]; ++q)
             {
-                table[h] = static_cast<int64_t>(refs.size());
-                keys.push_back(key);
+                const Slot& sl = slots[static_cast<size_t>(q)];
+                if (sl.k1 == key[1] && sl.k2 == key[2] && sl.k3 == key[3])
+                {
+                    found = sl.face;
+                    break;
+                }
+            }
+            if (found < 0)
+            {
+                slots[static_cast<size_t>(fill[b]++)] = {key[1], key[2], key[3], static_cast<int64_t>(refs.size())};
                 refs.push_back({static_cast<int64_t>(ringVerts.size()), static_cast<int64_t>(ring.size()), c, -1});
                 for (int k : ring) ringVerts.push_back(cv[k]);
-                if (2 * refs.size() > cap)
-                {
-                    // keep the load under one half: rebuild at twice the size
-                    cap <<= 1;
-                    table.assign(cap, -1);
-                    for (size_t i = 0; i < refs.size(); ++i)
-                    {
-                        size_t g = hasher(keys[i]) & (cap - 1);
-                        while (table[g] >= 0) g = (g + 1) & (cap - 1);
-                        table[g] = static_cast<int64_t>(i);
-                    }
-                }
             }
             else
             {
-                Ref& r = refs[static_cast<size_t>(table[h])];
+                Ref& r = refs[static_cast<size_t>(found)];
                 if (r.cell1 != -1) fail(CFG_EMESH, "mesh: a face belongs to three cells: the mesh is not manifold");
                 r.cell1 = c;
             }
         }
     }
-    std::vector<int64_t>().swap(table);
-    std::vector<std::array<int64_t, 5>>().swap(keys);
+    std::vector<Slot>().swap(slots);
+    std::vector<int64_t>().swap(fill);
+    std::vector<int64_t>().swap(bucket);
     // boundary faces named after the bounding-box plane they lie on
     // (gmshMesh.cpp:636-667, the case of a file without surface groups)
     Vec lo = points[0], hi = points[0];
@@ -498,6 +513,10 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
         }
         patchFaces[patchIndex(name)].push_back(i);
     }
+    m.faceOffsets.reserve(refs.size() + 1);
+    m.faceVerts.reserve(ringVerts.size());
+    m.owner.reserve(refs.size());
+    m.neighbour.reserve(internal.size());
     m.faceOffsets.push_back(0);
     auto addFace = [&](const Ref& r) {
         for (int64_t k = 0; k < r.nv; ++k) m.faceVerts.push_back(ringVerts[r.v0 + k]);
