@@ -119,6 +119,12 @@ Mesh blockMesh(const Vec& mn, const Vec& mx, int64_t nx, int64_t ny, int64_t nz,
     return m;
 }
 
+namespace
+{
+/// faces (or cells) per thread chunk in the geometry loops
+constexpr int64_t kFaceChunk = 1 << 15;
+}  // namespace
+
 void Mesh::finish()
 {
     const int64_t nF = nFaces(), nI = nInternal();
@@ -130,16 +136,18 @@ void Mesh::finish()
     nCells = 0;
     for (int64_t o : owner) nCells = std::max(nCells, o + 1);
     for (int64_t nb : neighbour) nCells = std::max(nCells, nb + 1);
-    for (int64_t f = 0; f < nF; ++f)
-    {
-        if (faceOffsets[f + 1] - faceOffsets[f] < 3) fail(CFG_EMESH, "polyMesh: face with fewer than 3 vertices");
-        if (owner[f] < 0) fail(CFG_EMESH, "polyMesh: negative owner");
-        for (int64_t q = faceOffsets[f]; q < faceOffsets[f + 1]; ++q)
-            if (faceVerts[q] < 0 || faceVerts[q] >= static_cast<int64_t>(points.size()))
-                fail(CFG_EMESH, "polyMesh: face vertex out of range");
-        if (f < nI && (neighbour[f] < 0 || neighbour[f] >= nCells))
-            fail(CFG_EMESH, "polyMesh: neighbour out of range at face " + std::to_string(f));
-    }
+    parallelChunks(nF, kFaceChunk, [&](int64_t fb, int64_t fe) {
+        for (int64_t f = fb; f < fe; ++f)
+        {
+            if (faceOffsets[f + 1] - faceOffsets[f] < 3) fail(CFG_EMESH, "polyMesh: face with fewer than 3 vertices");
+            if (owner[f] < 0) fail(CFG_EMESH, "polyMesh: negative owner");
+            for (int64_t q = faceOffsets[f]; q < faceOffsets[f + 1]; ++q)
+                if (faceVerts[q] < 0 || faceVerts[q] >= static_cast<int64_t>(points.size()))
+                    fail(CFG_EMESH, "polyMesh: face vertex out of range");
+            if (f < nI && (neighbour[f] < 0 || neighbour[f] >= nCells))
+                fail(CFG_EMESH, "polyMesh: neighbour out of range at face " + std::to_string(f));
+        }
+    });
     // face -> patch, patches must cover every boundary face exactly once
     // (polyMesh.cpp:35-61)
     facePatch.assign(static_cast<size_t>(nF), -1);
@@ -168,8 +176,12 @@ void Mesh::calcGeometry()
     Sf.assign(static_cast<size_t>(nF), Vec{});
     auto P = [&](int64_t v) -> const Vec& { return points[static_cast<size_t>(v)]; };
 
+    // Per-face and per-cell steps run on the host's threads; the sums over
+    // a cell's faces stay serial, in face order, so every value is the one
+    // the serial loops give.
     // fan-triangle area vectors and face centroids
-    for (int64_t f = 0; f < nF; ++f)
+    parallelChunks(nF, kFaceChunk, [&](int64_t fb, int64_t fe) {
+    for (int64_t f = fb; f < fe; ++f)
     {
         const int64_t* vs = faceVerts.data() + faceOffsets[f];
         const int64_t nv = faceOffsets[f + 1] - faceOffsets[f];
@@ -201,6 +213,7 @@ void Mesh::calcGeometry()
             Cf[static_cast<size_t>(f)] = c / static_cast<double>(nv);
         }
     }
+    });
 
     // provisional cell centres (mean of face centres), used only to orient
     std::vector<Vec> est(static_cast<size_t>(nCells));
@@ -219,23 +232,28 @@ void Mesh::calcGeometry()
     }
     for (size_t c = 0; c < est.size(); ++c)
         if (cnt[c] > 0) est[c] = est[c] / static_cast<double>(cnt[c]);
-    for (int64_t f = 0; f < nF; ++f)
-    {
-        const size_t o = static_cast<size_t>(owner[f]);
-        const Vec dd = f < nI ? est[static_cast<size_t>(neighbour[f])] - est[o] : Cf[static_cast<size_t>(f)] - est[o];
-        Vec& sf = Sf[static_cast<size_t>(f)];
-        const double side = dot(sf, dd);
-        const double tol = 1e-12 * mag(sf) * mag(dd);
-        if (side < -tol) sf = Vec{-sf.x, -sf.y, -sf.z};
-    }
     magSf.resize(static_cast<size_t>(nF));
-    for (int64_t f = 0; f < nF; ++f) magSf[static_cast<size_t>(f)] = mag(Sf[static_cast<size_t>(f)]);
+    parallelChunks(nF, kFaceChunk, [&](int64_t fb, int64_t fe) {
+        for (int64_t f = fb; f < fe; ++f)
+        {
+            const size_t o = static_cast<size_t>(owner[f]);
+            const Vec dd = f < nI ? est[static_cast<size_t>(neighbour[f])] - est[o] : Cf[static_cast<size_t>(f)] - est[o];
+            Vec& sf = Sf[static_cast<size_t>(f)];
+            const double side = dot(sf, dd);
+            const double tol = 1e-12 * mag(sf) * mag(dd);
+            if (side < -tol) sf = Vec{-sf.x, -sf.y, -sf.z};
+            magSf[static_cast<size_t>(f)] = mag(sf);
+        }
+    });
 
     // volumes and centroids through the divergence theorem over fan tets
     V.assign(static_cast<size_t>(nCells), 0.0);
     C.assign(static_cast<size_t>(nCells), Vec{});
     std::vector<Vec> moment(static_cast<size_t>(nCells));
-    for (int64_t f = 0; f < nF; ++f)
+    std::vector<double> faceV(static_cast<size_t>(nF));
+    std::vector<Vec> faceM(static_cast<size_t>(nF));
+    parallelChunks(nF, kFaceChunk, [&](int64_t fb, int64_t fe) {
+    for (int64_t f = fb; f < fe; ++f)
     {
         const int64_t* vs = faceVerts.data() + faceOffsets[f];
         const int64_t nv = faceOffsets[f + 1] - faceOffsets[f];
@@ -251,32 +269,42 @@ void Mesh::calcGeometry()
         }
         for (int64_t i = 1; i + 1 < nv; ++i) raw = raw + cross(P(vs[i]) - v0, P(vs[i + 1]) - v0);
         const double s = dot(raw, Sf[static_cast<size_t>(f)]) >= 0 ? 1.0 : -1.0;
-        const size_t o = static_cast<size_t>(owner[f]);
-        V[o] += s * fv;
-        moment[o] = moment[o] + fm * s;
-        if (f < nI)
-        {
-            const size_t nb = static_cast<size_t>(neighbour[f]);
-            V[nb] -= s * fv;
-            moment[nb] = moment[nb] - fm * s;
-        }
+        faceV[static_cast<size_t>(f)] = s * fv;
+        faceM[static_cast<size_t>(f)] = fm * s;
     }
-    for (size_t c = 0; c < V.size(); ++c)
-    {
-        C[c] = moment[c] / V[c];
-        V[c] = std::abs(V[c]);
-        if (!(V[c] > 0)) fail(CFG_EMESH, "polyMesh: degenerate cell volume for cell " + std::to_string(c));
-    }
-    d.resize(static_cast<size_t>(nF));
-    invDist.resize(static_cast<size_t>(nF));
+    });
     for (int64_t f = 0; f < nF; ++f)
     {
         const size_t o = static_cast<size_t>(owner[f]);
-        d[static_cast<size_t>(f)] = f < nI ? C[static_cast<size_t>(neighbour[f])] - C[o] : Cf[static_cast<size_t>(f)] - C[o];
-        const double dm = mag(d[static_cast<size_t>(f)]);
-        if (!(dm > 0)) fail(CFG_EMESH, "polyMesh: zero owner-neighbour distance at face " + std::to_string(f));
-        invDist[static_cast<size_t>(f)] = 1.0 / dm;
+        V[o] += faceV[static_cast<size_t>(f)];
+        moment[o] = moment[o] + faceM[static_cast<size_t>(f)];
+        if (f < nI)
+        {
+            const size_t nb = static_cast<size_t>(neighbour[f]);
+            V[nb] -= faceV[static_cast<size_t>(f)];
+            moment[nb] = moment[nb] - faceM[static_cast<size_t>(f)];
+        }
     }
+    parallelChunks(nCells, kFaceChunk, [&](int64_t cb, int64_t ce) {
+        for (int64_t c = cb; c < ce; ++c)
+        {
+            C[c] = moment[c] / V[c];
+            V[c] = std::abs(V[c]);
+            if (!(V[c] > 0)) fail(CFG_EMESH, "polyMesh: degenerate cell volume for cell " + std::to_string(c));
+        }
+    });
+    d.resize(static_cast<size_t>(nF));
+    invDist.resize(static_cast<size_t>(nF));
+    parallelChunks(nF, kFaceChunk, [&](int64_t fb, int64_t fe) {
+        for (int64_t f = fb; f < fe; ++f)
+        {
+            const size_t o = static_cast<size_t>(owner[f]);
+            d[static_cast<size_t>(f)] = f < nI ? C[static_cast<size_t>(neighbour[f])] - C[o] : Cf[static_cast<size_t>(f)] - C[o];
+            const double dm = mag(d[static_cast<size_t>(f)]);
+            if (!(dm > 0)) fail(CFG_EMESH, "polyMesh: zero owner-neighbour distance at face " + std::to_string(f));
+            invDist[static_cast<size_t>(f)] = 1.0 / dm;
+        }
+    });
 }
 
 std::vector<double> Mesh::ownerWeights() const
@@ -356,11 +384,12 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
     const int64_t nPoints = static_cast<int64_t>(points.size());
     std::vector<int64_t> ringVerts;
     std::vector<Ref> refs;
-    // every registration is filed under its smallest vertex: a first pass
-    // counts the registrations per vertex, the second scans that vertex's
-    // few earlier faces for the same key (faces of nearby cells share
-    // nearby vertices, so the buckets are visited almost in order)
-    std::vector<int64_t> bucket(static_cast<size_t>(nPoints) + 1, 0);
+    // every registration (cell c, ring k) is filed under its smallest
+    // vertex.  Threads own ranges of vertices: each walks all registrations
+    // in order, files those of its own vertices and finds for each the
+    // first registration with the same key in that vertex's short bucket.
+    // A serial walk then numbers the faces in order of first registration.
+    std::vector<int64_t> regStart(static_cast<size_t>(nCells) + 1, 0);
     for (int64_t c = 0; c < nCells; ++c)
     {
         const auto& rings = faceRings(types[static_cast<size_t>(c)]);
@@ -370,59 +399,87 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
         const int64_t* cv = cellVerts.data() + cellOffsets[c];
         for (int64_t k = 0; k < need; ++k)
             if (cv[k] < 0 || cv[k] >= nPoints) fail(CFG_EMESH, "mesh: cell vertex out of range");
-        for (const auto& ring : rings)
-        {
-            int64_t lo = cv[ring[0]];
-            for (size_t k = 1; k < ring.size(); ++k) lo = std::min(lo, cv[ring[k]]);
-            ++bucket[static_cast<size_t>(lo) + 1];
-        }
+        regStart[c + 1] = regStart[c] + static_cast<int64_t>(rings.size());
     }
-    for (int64_t v = 0; v < nPoints; ++v) bucket[v + 1] += bucket[v];
-    struct Slot
+    const int64_t nReg = regStart[nCells];
+    // first[r]: the earliest registration with r's key (r itself if none)
+    std::vector<int64_t> first(static_cast<size_t>(nReg));
     {
-        int64_t k1, k2, k3, face;  // the sorted key after its smallest vertex (-1 padded)
-    };
-    std::vector<Slot> slots(static_cast<size_t>(bucket[nPoints]));
-    std::vector<int64_t> fill(bucket.begin(), bucket.end() - 1);
+        std::vector<int64_t> bucket(static_cast<size_t>(nPoints) + 1, 0);
+        const int64_t hw = std::max<int64_t>(1, std::thread::hardware_concurrency());
+        const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(hw, 32), nReg / (1 << 16)));
+        auto forOwn = [&](int64_t part, auto&& fn) {
+            const int64_t vlo = nPoints * part / parts, vhi = nPoints * (part + 1) / parts;
+            for (int64_t c = 0; c < nCells; ++c)
+            {
+                const int64_t* cv = cellVerts.data() + cellOffsets[c];
+                int64_t r = regStart[c];
+                for (const auto& ring : faceRings(types[static_cast<size_t>(c)]))
+                {
+                    int64_t lo = cv[ring[0]];
+                    for (size_t k = 1; k < ring.size(); ++k) lo = std::min(lo, cv[ring[k]]);
+                    if (lo >= vlo && lo < vhi) fn(r, cv, ring, lo);
+                    ++r;
+                }
+            }
+        };
+        parallelChunks(parts, 1, [&](int64_t pb, int64_t pe) {
+            for (int64_t part = pb; part < pe; ++part)
+                forOwn(part, [&](int64_t, const int64_t*, const std::vector<int>&, int64_t lo) { ++bucket[static_cast<size_t>(lo) + 1]; });
+        });
+        for (int64_t v = 0; v < nPoints; ++v) bucket[v + 1] += bucket[v];
+        struct Slot
+        {
+            int64_t k1, k2, k3, reg;  // the sorted key after its smallest vertex (-1 padded)
+        };
+        std::vector<Slot> slots(static_cast<size_t>(bucket[nPoints]));
+        std::vector<int64_t> fill(bucket.begin(), bucket.end() - 1);
+        parallelChunks(parts, 1, [&](int64_t pb, int64_t pe) {
+            for (int64_t part = pb; part < pe; ++part)
+                forOwn(part, [&](int64_t r, const int64_t* cv, const std::vector<int>& ring, int64_t lo) {
+                    std::array<int64_t, 4> key{-1, -1, -1, -1};
+                    for (size_t k = 0; k < ring.size(); ++k) key[k] = cv[ring[k]];
+                    std::sort(key.begin(), key.begin() + static_cast<long>(ring.size()));
+                    const size_t b = static_cast<size_t>(lo);
+                    for (int64_t q = bucket[b]; q < fill[b]; ++q)
+                    {
+                        const Slot& sl = slots[static_cast<size_t>(q)];
+                        if (sl.k1 == key[1] && sl.k2 == key[2] && sl.k3 == key[3])
+                        {
+                            first[static_cast<size_t>(r)] = sl.reg;
+                            return;
+                        }
+                    }
+                    slots[static_cast<size_t>(fill[b]++)] = {key[1], key[2], key[3], r};
+                    first[static_cast<size_t>(r)] = r;
+                });
+        });
+    }
     ringVerts.reserve(static_cast<size_t>(4 * 4 * nCells));
     refs.reserve(static_cast<size_t>(4 * nCells));
     for (int64_t c = 0; c < nCells; ++c)
     {
-        const auto& rings = faceRings(types[static_cast<size_t>(c)]);
         const int64_t* cv = cellVerts.data() + cellOffsets[c];
-        for (const auto& ring : rings)
+        int64_t r = regStart[c];
+        for (const auto& ring : faceRings(types[static_cast<size_t>(c)]))
         {
-            std::array<int64_t, 4> key{-1, -1, -1, -1};
-            for (size_t k = 0; k < ring.size(); ++k) key[k] = cv[ring[k]];
-            std::sort(key.begin(), key.begin() + static_cast<long>(ring.size()));
-            const size_t b = static_cast<size_t>(key[0]);
-            int64_t found = -1;
-            for (int64_t q = bucket[b]; q < fill[b]; ++q)
+            const int64_t f0 = first[static_cast<size_t>(r)];
+            if (f0 == r)
             {
-                const Slot& sl = slots[static_cast<size_t>(q)];
-                if (sl.k1 == key[1] && sl.k2 == key[2] && sl.k3 == key[3])
-                {
-                    found = sl.face;
-                    break;
-                }
-            }
-            if (found < 0)
-            {
-                slots[static_cast<size_t>(fill[b]++)] = {key[1], key[2], key[3], static_cast<int64_t>(refs.size())};
+                first[static_cast<size_t>(r)] = ~static_cast<int64_t>(refs.size());  // now the face index
                 refs.push_back({static_cast<int64_t>(ringVerts.size()), static_cast<int64_t>(ring.size()), c, -1});
                 for (int k : ring) ringVerts.push_back(cv[k]);
             }
             else
             {
-                Ref& r = refs[static_cast<size_t>(found)];
-                if (r.cell1 != -1) fail(CFG_EMESH, "mesh: a face belongs to three cells: the mesh is not manifold");
-                r.cell1 = c;
+                Ref& fr = refs[static_cast<size_t>(~first[static_cast<size_t>(f0)])];
+                if (fr.cell1 != -1) fail(CFG_EMESH, "mesh: a face belongs to three cells: the mesh is not manifold");
+                fr.cell1 = c;
             }
+            ++r;
         }
     }
-    std::vector<Slot>().swap(slots);
-    std::vector<int64_t>().swap(fill);
-    std::vector<int64_t>().swap(bucket);
+    std::vector<int64_t>().swap(first);
     // boundary faces named after the bounding-box plane they lie on
     // (gmshMesh.cpp:636-667, the case of a file without surface groups)
     Vec lo = points[0], hi = points[0];
