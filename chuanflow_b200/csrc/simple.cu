@@ -2240,7 +2240,6 @@ void Ctx::probeDIC(const double* r, double* z, double* rDinv)
     // the DIC of the pressure matrix last assembled (by probeEquations or an
     // outer iteration): factor, then one application to r
     CFG_CUDA(cudaSetDevice(device_));
-    const int nC = dm_.nC;
     SolveState init{};
     init.maxIter = 1;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
@@ -2255,7 +2254,7 @@ void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQ
 {
     // fvc::grad of one cell field with fixed boundary face values
     CFG_CUDA(cudaSetDevice(device_));
-    const int nC = dm_.nC, nB = dm_.nB;
+    const int nB = dm_.nB;
     double* x = cr_;
     double* k = bScratch_;
     double* c0 = bScratch_ + nB;
