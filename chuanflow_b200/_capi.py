@@ -193,6 +193,19 @@ class PolyMesh:
         _check(lib().cfg_mesh_write_vtu(self._h, str(path).encode(), C.c_int32(n), names, comps, ptrs,
                                         C.c_int32(int(binary))))
 
+    def write_hdf5(self, path, fields=None):
+        """writeFieldsHdf5: /points, /owner, /neighbour and /fields/<name>
+        for cell fields {name: array (n_cells,)}."""
+        fields = fields or {}
+        arrs = [np.ascontiguousarray(v, np.float64) for v in fields.values()]
+        for k, a in zip(fields, arrs):
+            if a.shape != (self.n_cells,):
+                raise CfgError(1, "hdf5: field '%s' size mismatch (expected %d cells)" % (k, self.n_cells))
+        n = len(arrs)
+        names = (C.c_char_p * max(1, n))(*[k.encode() for k in fields])
+        ptrs = (C.POINTER(C.c_double) * max(1, n))(*[_dp(a) for a in arrs])
+        _check(lib().cfg_mesh_write_hdf5(self._h, str(path).encode(), C.c_int32(n), names, ptrs))
+
     def _counts(self):
         c = np.zeros(5, np.int64)
         _check(lib().cfg_mesh_counts(self._h, _ip(c)))
@@ -706,7 +719,14 @@ def _write_vtu(self, path, binary=True):
     _check(lib().cfg_write_vtu(self._h, str(path).encode(), C.c_int32(int(binary))))
 
 
+def _write_hdf5(self, path):
+    """The case's cell fields as HDF5: /fields/p, k/epsilon (omega)/nut with
+    a RANS model, Ux, Uy, Uz, beside the mesh's points, owner, neighbour."""
+    _check(lib().cfg_write_hdf5(self._h, str(path).encode()))
+
+
 SimpleCase.write_vtu = _write_vtu
+SimpleCase.write_hdf5 = _write_hdf5
 SimpleCase.piso_step = _piso_step
 def _mpnn_collect(self, on=1, max_samples=64):
     """Keep (1) / stop keeping (0) / drop and keep (2) the residuals later

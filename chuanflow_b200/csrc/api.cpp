@@ -1011,6 +1011,52 @@ int cfg_write_vtu(cfg_ctx* ctx, const char* path, int32_t binary)
     });
 }
 
+int cfg_write_hdf5(cfg_ctx* ctx, const char* path)
+{
+    return guard([&] {
+        need(ctx && path, "cfg_write_hdf5: null argument");
+        cfg::Ctx& c = *ctx->c;
+        const cfg::Mesh& M = c.mesh();
+        const size_t nC = static_cast<size_t>(M.nCells);
+        std::vector<double> p(nC), U(3 * nC), k, eps, nut;
+        c.download(U.data(), p.data(), nullptr);
+        std::vector<std::pair<std::string, const double*>> f{{"p", p.data()}};
+        if (c.hasTurbulence())
+        {
+            k.resize(nC);
+            eps.resize(nC);
+            nut.resize(nC);
+            c.turbulenceFields(k.data(), eps.data(), nut.data(), nullptr);
+            f.push_back({"k", k.data()});
+            f.push_back({c.turbulenceModelName() == "kOmegaSST" ? "omega" : "epsilon", eps.data()});
+            f.push_back({"nut", nut.data()});
+        }
+        // U is cell-major (x y z per cell); the datasets are one component each
+        std::vector<double> Uc(3 * nC);
+        for (size_t i = 0; i < nC; ++i)
+            for (size_t q = 0; q < 3; ++q) Uc[q * nC + i] = U[3 * i + q];
+        f.push_back({"Ux", Uc.data()});
+        f.push_back({"Uy", Uc.data() + nC});
+        f.push_back({"Uz", Uc.data() + 2 * nC});
+        cfg::writeHdf5(M, path, f);
+    });
+}
+
+int cfg_mesh_write_hdf5(const cfg_mesh* mesh, const char* path, int32_t n_fields, const char* const* names,
+                        const double* const* data)
+{
+    return guard([&] {
+        need(mesh && path && n_fields >= 0 && (n_fields == 0 || (names && data)), "cfg_mesh_write_hdf5: null argument");
+        std::vector<std::pair<std::string, const double*>> f;
+        for (int32_t i = 0; i < n_fields; ++i)
+        {
+            need(names[i] && (data[i] || mesh->m.nCells == 0), "cfg_mesh_write_hdf5: null field");
+            f.push_back({names[i], data[i]});
+        }
+        cfg::writeHdf5(mesh->m, path, f);
+    });
+}
+
 int cfg_mesh_write_vtu(const cfg_mesh* mesh, const char* path, int32_t n_fields, const char* const* names,
                        const int32_t* n_comp, const double* const* data, int32_t binary)
 {

@@ -145,6 +145,10 @@ struct VtuField
 /// VtkWriter::write (vtkWrite.cpp:33-131): scalars then vectors, each in the
 /// order given; binary = raw appended arrays instead of ASCII
 void writeVtu(const Mesh& M, const std::string& path, const std::vector<VtuField>& fields, bool binary);
+/// writeFieldsHdf5's file (hdf5Write.cpp:38-95): /points, /owner,
+/// /neighbour and /fields/<name> (one f64 per cell), by this library's own
+/// HDF5 encoder (hdf5.cpp)
+void writeHdf5(const Mesh& M, const std::string& path, const std::vector<std::pair<std::string, const double*>>& fields);
 
 /// GmshMesh::fromFile (gmshMesh.cpp:534-776): ASCII .msh 2.2 or 4.x
 Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>& patchTypes);

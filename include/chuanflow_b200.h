@@ -431,6 +431,21 @@ int cfg_mesh_write_vtu(const cfg_mesh* mesh, const char* path, int32_t n_fields,
  * model is set up, then U */
 int cfg_write_vtu(cfg_ctx* ctx, const char* path, int32_t binary);
 
+/* writeFieldsHdf5 (src/3d/include/cf/fvm/Hdf5Writer.h:25, src/3d/src/io/hdf5Write.cpp:38-95):
+ * an HDF5 file holding /points (n_points x 3 f64), /owner and /neighbour
+ * (int64) and one 1-D f64 dataset of n_cells values per field under
+ * /fields.  The reference writes it through the HDF5 C library and fails
+ * without one; this library encodes the file format itself (superblock 0,
+ * symbol-table groups, version-1 object headers, contiguous datasets), so
+ * no HDF5 library is needed.  Field names must be non-empty, distinct and
+ * free of '/'; at most 256 fields. */
+int cfg_mesh_write_hdf5(const cfg_mesh* mesh, const char* path, int32_t n_fields, const char* const* names,
+                        const double* const* data);
+/* the context's cell fields (original order) as /fields/p, then k, epsilon
+ * (omega for k-omega SST) and nut when a RANS model is set up, then Ux, Uy,
+ * Uz */
+int cfg_write_hdf5(cfg_ctx* ctx, const char* path);
+
 /* ---- RANS turbulence -------------------------------------------------------- */
 
 /* RansModel::create (src/3d/src/turbulence/turbulenceModel.cpp:54-104,

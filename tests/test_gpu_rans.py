@@ -78,3 +78,25 @@ def test_case_vtu_carries_the_device_fields(tmp_path):
     assert list(got) == ["p", "k", "epsilon", "nut", "U"]
     assert np.array_equal(got["p"], p) and np.array_equal(got["U"].reshape(-1, 3), U)
     assert np.array_equal(got["k"], t["k"]) and np.array_equal(got["nut"], t["nut"])
+
+
+def test_case_hdf5_carries_the_device_fields(tmp_path):
+    """cfg_write_hdf5 of a k-omega SST case: /fields/p, k, omega, nut and
+    Ux, Uy, Uz as the device holds them, beside the mesh datasets."""
+    from _hdf5_read import read
+    mesh, case = K.rans_channel_product(8, 4, 4, model="kOmegaSST")
+    import chuanflow_b200 as cf
+    case.solve(cf.SimpleControls(max_iterations=2, relax_u=0.9, relax_p=0.03, p_relax_start=0.02,
+                                 non_orth_correctors=1, linear_tol=1e-8, nu=2.5e-6))
+    out = tmp_path / "c.h5"
+    case.write_hdf5(out)
+    data, listing = read(out)
+    U, p, _ = case.download()
+    t = case.turbulence_fields()
+    assert listing["/fields/"] == ["Ux", "Uy", "Uz", "k", "nut", "omega", "p"]
+    assert np.array_equal(data["/fields/p"], p)
+    for q, c in enumerate("xyz"):
+        assert np.array_equal(data["/fields/U" + c], U[:, q])
+    assert np.array_equal(data["/fields/k"], t["k"]) and np.array_equal(data["/fields/nut"], t["nut"])
+    assert np.array_equal(data["/fields/omega"], t["eps"])
+    assert np.array_equal(data["/points"], mesh.addressing()["points"])
