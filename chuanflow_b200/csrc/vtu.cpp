@@ -26,19 +26,31 @@ struct Topo
 Topo topology(const Mesh& M)
 {
     const int64_t nC = M.nCells, nF = M.nFaces(), nI = M.nInternal();
-    std::vector<std::vector<int64_t>> cells(static_cast<size_t>(nC));
+    // each cell's faces in ascending face order (polyMesh::cells)
+    std::vector<int64_t> cStart(static_cast<size_t>(nC) + 1, 0), cFaces;
     for (int64_t f = 0; f < nF; ++f)
     {
-        cells[static_cast<size_t>(M.owner[f])].push_back(f);
-        if (f < nI) cells[static_cast<size_t>(M.neighbour[f])].push_back(f);
+        ++cStart[static_cast<size_t>(M.owner[f]) + 1];
+        if (f < nI) ++cStart[static_cast<size_t>(M.neighbour[f]) + 1];
     }
-    Topo t;
-    t.offsets.reserve(static_cast<size_t>(nC));
-    std::vector<int64_t> verts;
-    for (const auto& cell : cells)
+    for (int64_t c = 0; c < nC; ++c) cStart[c + 1] += cStart[c];
+    cFaces.resize(static_cast<size_t>(cStart[nC]));
     {
+        std::vector<int64_t> fill(cStart.begin(), cStart.end() - 1);
+        for (int64_t f = 0; f < nF; ++f)
+        {
+            cFaces[static_cast<size_t>(fill[static_cast<size_t>(M.owner[f])]++)] = f;
+            if (f < nI) cFaces[static_cast<size_t>(fill[static_cast<size_t>(M.neighbour[f])]++)] = f;
+        }
+    }
+    // a cell's vertices in the order its faces first visit them; cells are
+    // independent, so two parallel passes: sizes, then the arrays at their
+    // prefix offsets
+    auto cellVerts = [&](int64_t c, std::vector<int64_t>& verts) {
         verts.clear();
-        for (int64_t f : cell)
+        for (int64_t q = cStart[c]; q < cStart[c + 1]; ++q)
+        {
+            const int64_t f = cFaces[static_cast<size_t>(q)];
             for (int64_t k = M.faceOffsets[f]; k < M.faceOffsets[f + 1]; ++k)
             {
                 const int64_t v = M.faceVerts[k];
@@ -46,16 +58,51 @@ Topo topology(const Mesh& M)
                 for (int64_t w : verts) seen = seen || w == v;
                 if (!seen) verts.push_back(v);
             }
-        t.conn.insert(t.conn.end(), verts.begin(), verts.end());
-        t.offsets.push_back(static_cast<int64_t>(t.conn.size()));
-        t.faces.push_back(static_cast<int64_t>(cell.size()));
-        for (int64_t f : cell)
-        {
-            t.faces.push_back(M.faceOffsets[f + 1] - M.faceOffsets[f]);
-            for (int64_t k = M.faceOffsets[f]; k < M.faceOffsets[f + 1]; ++k) t.faces.push_back(M.faceVerts[k]);
         }
-        t.faceOffsets.push_back(static_cast<int64_t>(t.faces.size()));
+    };
+    constexpr int64_t kChunk = 1 << 14;
+    std::vector<int64_t> nConn(static_cast<size_t>(nC) + 1, 0), nFaceStream(static_cast<size_t>(nC) + 1, 0);
+    parallelChunks(nC, kChunk, [&](int64_t cb, int64_t ce) {
+        std::vector<int64_t> verts;
+        for (int64_t c = cb; c < ce; ++c)
+        {
+            cellVerts(c, verts);
+            nConn[c + 1] = static_cast<int64_t>(verts.size());
+            int64_t len = 1;
+            for (int64_t q = cStart[c]; q < cStart[c + 1]; ++q)
+            {
+                const int64_t f = cFaces[static_cast<size_t>(q)];
+                len += 1 + M.faceOffsets[f + 1] - M.faceOffsets[f];
+            }
+            nFaceStream[c + 1] = len;
+        }
+    });
+    for (int64_t c = 0; c < nC; ++c)
+    {
+        nConn[c + 1] += nConn[c];
+        nFaceStream[c + 1] += nFaceStream[c];
     }
+    Topo t;
+    t.conn.resize(static_cast<size_t>(nConn[nC]));
+    t.faces.resize(static_cast<size_t>(nFaceStream[nC]));
+    t.offsets.assign(nConn.begin() + 1, nConn.end());
+    t.faceOffsets.assign(nFaceStream.begin() + 1, nFaceStream.end());
+    parallelChunks(nC, kChunk, [&](int64_t cb, int64_t ce) {
+        std::vector<int64_t> verts;
+        for (int64_t c = cb; c < ce; ++c)
+        {
+            cellVerts(c, verts);
+            std::copy(verts.begin(), verts.end(), t.conn.begin() + nConn[c]);
+            int64_t w = nFaceStream[c];
+            t.faces[static_cast<size_t>(w++)] = cStart[c + 1] - cStart[c];
+            for (int64_t q = cStart[c]; q < cStart[c + 1]; ++q)
+            {
+                const int64_t f = cFaces[static_cast<size_t>(q)];
+                t.faces[static_cast<size_t>(w++)] = M.faceOffsets[f + 1] - M.faceOffsets[f];
+                for (int64_t k = M.faceOffsets[f]; k < M.faceOffsets[f + 1]; ++k) t.faces[static_cast<size_t>(w++)] = M.faceVerts[k];
+            }
+        }
+    });
     return t;
 }
 

@@ -361,3 +361,49 @@ def test_read_gmsh_reports_the_first_bad_row(tmp_path):
     p.write_text("\n".join(lines))
     with pytest.raises(cf.CfgError, match="inconsistent element line width"):
         cf.PolyMesh.read_gmsh(p)
+
+
+def _vtu_arrays(raw):
+    import re
+    head, data = raw.split(b'<AppendedData encoding="raw">\n_', 1)
+    arrays = {}
+    for mt in re.finditer(rb'<DataArray type="(\w+)"(?: Name="(\w+)")?[^>]*offset="(\d+)"', head):
+        typ, name, off = mt.group(1).decode(), (mt.group(2) or b"points").decode(), int(mt.group(3))
+        nbytes = int(np.frombuffer(data[off:off + 8], np.uint64)[0])
+        dt = {"Float64": np.float64, "Int64": np.int64, "UInt8": np.uint8}[typ]
+        arrays[name] = np.frombuffer(data[off + 8:off + 8 + nbytes], dt)
+    return arrays
+
+
+def test_vtu_polyhedra_of_a_large_mesh(tmp_path):
+    """Cells split over the writer's threads (32^3 cells): connectivity in
+    first-visit order over each cell's ascending faces, and the face
+    stream, as polyMesh::cells gives them."""
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (32, 32, 32))
+    m.jitter_interior(0.1, 3)
+    out = tmp_path / "big.vtu"
+    m.write_vtu(out, {}, binary=True)
+    arr = _vtu_arrays(out.read_bytes())
+    a = m.addressing()
+    fo, fv, own, nbr = a["face_offsets"], a["face_verts"], a["owner"], a["neighbour"][:m.n_internal_faces]
+    cells = [[] for _ in range(m.n_cells)]
+    for f in range(m.n_faces):
+        cells[own[f]].append(f)
+        if f < m.n_internal_faces:
+            cells[nbr[f]].append(f)
+    conn, offs, faces, foffs = [], [], [], []
+    for cf_ in cells:
+        seen = []
+        for f in cf_:
+            for v in fv[fo[f]:fo[f + 1]]:
+                if v not in seen:
+                    seen.append(v)
+        conn += seen
+        offs.append(len(conn))
+        faces.append(len(cf_))
+        for f in cf_:
+            faces.append(fo[f + 1] - fo[f])
+            faces += list(fv[fo[f]:fo[f + 1]])
+        foffs.append(len(faces))
+    assert np.array_equal(arr["connectivity"], conn) and np.array_equal(arr["offsets"], offs)
+    assert np.array_equal(arr["faces"], faces) and np.array_equal(arr["faceoffsets"], foffs)
