@@ -120,3 +120,22 @@ def test_case_file_defaults_and_gpu_block(tmp_path):
 def test_case_file_errors(tmp_path, text, msg):
     with pytest.raises(cf.CfgError, match=re.escape(msg)):
         cf.inspect_case_file(write(tmp_path, text))
+
+
+def test_writers_refuse_null_arguments():
+    """The output entry points report a null mesh, path or field as
+    CFG_EINVAL through the status and the error channel, never a crash."""
+    import ctypes as C
+    lib = cf.lib()
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (2, 2, 2))
+    one = (C.c_char_p * 1)(b"p")
+    assert lib.cfg_mesh_write_hdf5(None, b"x.h5", 0, None, None) == 1
+    assert lib.cfg_mesh_write_hdf5(m._h, None, 0, None, None) == 1
+    assert lib.cfg_mesh_write_hdf5(m._h, b"x.h5", 1, one, None) == 1
+    assert lib.cfg_mesh_write_hdf5(m._h, b"x.h5", 1, one, (C.POINTER(C.c_double) * 1)()) == 1
+    assert lib.cfg_mesh_write_hdf5(m._h, b"x.h5", -1, None, None) == 1
+    buf = C.create_string_buffer(256)
+    lib.cfg_last_error(buf, 256)
+    assert b"cfg_mesh_write_hdf5" in buf.value
+    assert lib.cfg_write_hdf5(None, b"x.h5") == 1
+    assert lib.cfg_mesh_write_vtu(None, b"x.vtu", 0, None, None, None, 1) == 1
