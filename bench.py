@@ -24,6 +24,7 @@ import argparse
 import dataclasses
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -214,8 +215,18 @@ def barrier(dist):
         dist.barrier()
 
 
+def pinned_core():
+    """The core the CPU baseline runs on: the first one this process may use
+    (the reference is serial), when taskset is there to pin it."""
+    try:
+        return min(os.sched_getaffinity(0)) if shutil.which("taskset") else None
+    except (AttributeError, OSError, ValueError):
+        return None
+
+
 def run_reference_cpu(n, points, timeout=3600):
-    """One SIMPLE outer iteration of the reference's own build on this host."""
+    """One SIMPLE outer iteration of the reference's own build on this host,
+    pinned to one core."""
     drv = os.path.join(ROOT, "oracle", "_ref", "cf_ref_driver")
     with tempfile.TemporaryDirectory() as td:
         cp = os.path.join(td, "case.dict")
@@ -223,7 +234,9 @@ def run_reference_cpu(n, points, timeout=3600):
         pp = os.path.join(td, "points.f64")
         np.ascontiguousarray(points).tofile(pp)
         if os.path.exists(drv):
-            r = subprocess.run([drv, "simple", cp, td, pp], capture_output=True, text=True, timeout=timeout)
+            core = pinned_core()
+            pin = ["taskset", "-c", str(core)] if core is not None else []
+            r = subprocess.run(pin + [drv, "simple", cp, td, pp], capture_output=True, text=True, timeout=timeout)
             if r.returncode != 0:
                 raise RuntimeError(r.stderr)
             res = open(os.path.join(td, "result.txt")).read().split()
@@ -242,13 +255,18 @@ def run_reference_cpu(n, points, timeout=3600):
 
 
 def cpu_info():
+    """The CPU model, the host's core count and the core the baseline ran on."""
+    model = "unknown"
     try:
         for ln in open("/proc/cpuinfo"):
             if ln.startswith("model name"):
-                return ln.split(":", 1)[1].strip()
+                model = ln.split(":", 1)[1].strip()
+                break
     except OSError:
         pass
-    return "unknown"
+    core = pinned_core()
+    where = f"pinned to core {core}" if core is not None else "unpinned"
+    return f"{model}, {os.cpu_count()} host cores, {where}"
 
 
 def main_reference(args, world, rank, dist):
