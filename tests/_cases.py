@@ -304,6 +304,28 @@ def hex_box_cells(n):
     return pts, np.array(hexes), sides
 
 
+def write_msh_box(path, pts, hexes, tags, fmt):
+    """The box as gmsh 2.2 or 4.1 ASCII, nodes written under `tags`; a
+    vertex index past the points becomes a tag past the last one."""
+    def tag(v):
+        return int(tags[v]) if v < len(tags) else int(max(tags)) + 1 + int(v) - len(tags)
+
+    with open(path, "w") as f:
+        if fmt == "2.2":
+            f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(pts))
+            f.writelines("%d %.17g %.17g %.17g\n" % (t, *p) for t, p in zip(tags, pts))
+            f.write("$EndNodes\n$Elements\n%d\n" % len(hexes))
+            f.writelines("%d 5 2 1 1 %s\n" % (e + 1, " ".join(str(tag(v)) for v in c)) for e, c in enumerate(hexes))
+        else:
+            f.write("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n$Nodes\n1 %d %d %d\n3 1 0 %d\n"
+                    % (len(pts), min(tags), max(tags), len(pts)))
+            f.writelines("%d\n" % t for t in tags)
+            f.writelines("%.17g %.17g %.17g\n" % tuple(p) for p in pts)
+            f.write("$EndNodes\n$Elements\n1 %d 1 %d\n3 1 5 %d\n" % (len(hexes), len(hexes), len(hexes)))
+            f.writelines("%d %s\n" % (e + 1, " ".join(str(tag(v)) for v in c)) for e, c in enumerate(hexes))
+        f.write("$EndElements\n")
+
+
 def write_msh22_groups(path, points, hexes, groups):
     """gmsh 2.2 ASCII with physical surface groups: groups = [(name, quads,
     as_triangles)]; a group written as triangles splits each quad in two."""

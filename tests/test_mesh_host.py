@@ -272,28 +272,6 @@ def _hex_box_rows(n):
     return pts, hexes
 
 
-def _write_msh(path, pts, hexes, tags, fmt):
-    """The box as gmsh 2.2 or 4.1 ASCII, nodes written under `tags`; a
-    vertex index past the points becomes a tag past the last one."""
-    def tag(v):
-        return int(tags[v]) if v < len(tags) else int(max(tags)) + 1 + int(v) - len(tags)
-
-    with open(path, "w") as f:
-        if fmt == "2.2":
-            f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(pts))
-            f.writelines("%d %.17g %.17g %.17g\n" % (t, *p) for t, p in zip(tags, pts))
-            f.write("$EndNodes\n$Elements\n%d\n" % len(hexes))
-            f.writelines("%d 5 2 1 1 %s\n" % (e + 1, " ".join(str(tag(v)) for v in c)) for e, c in enumerate(hexes))
-        else:
-            f.write("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n$Nodes\n1 %d %d %d\n3 1 0 %d\n"
-                    % (len(pts), min(tags), max(tags), len(pts)))
-            f.writelines("%d\n" % t for t in tags)
-            f.writelines("%.17g %.17g %.17g\n" % tuple(p) for p in pts)
-            f.write("$EndNodes\n$Elements\n1 %d 1 %d\n3 1 5 %d\n" % (len(hexes), len(hexes), len(hexes)))
-            f.writelines("%d %s\n" % (e + 1, " ".join(str(tag(v)) for v in c)) for e, c in enumerate(hexes))
-        f.write("$EndElements\n")
-
-
 @pytest.mark.parametrize("fmt", ["2.2", "4.1"])
 @pytest.mark.parametrize("sparse_tags", [False, True])
 def test_read_gmsh_large_file_is_its_cells(tmp_path, fmt, sparse_tags):
@@ -305,7 +283,7 @@ def test_read_gmsh_large_file_is_its_cells(tmp_path, fmt, sparse_tags):
     if sparse_tags:
         tags = np.random.default_rng(3).permutation(len(pts)) * 3 + 7
     p = tmp_path / "box.msh"
-    _write_msh(str(p), pts, hexes, tags, fmt)
+    K.write_msh_box(str(p), pts, hexes, tags, fmt)
     m = cf.PolyMesh.read_gmsh(p)
     # the reader renumbers nodes in ascending tag order
     order = np.argsort(tags, kind="stable")
@@ -330,7 +308,7 @@ def test_read_gmsh_reports_the_first_bad_row(tmp_path):
     def write(mutate, fmt="2.2"):
         h = hexes.copy()
         mutate(h)
-        _write_msh(str(p), pts, h, tags, fmt)
+        K.write_msh_box(str(p), pts, h, tags, fmt)
 
     def undefined_late(h):  # row 20000 names node len(pts) + 5 (undefined); row 26000 repeats one
         h[20000, 0] = len(pts) + 4
@@ -348,13 +326,13 @@ def test_read_gmsh_reports_the_first_bad_row(tmp_path):
         with pytest.raises(cf.CfgError, match="repeats a node"):
             cf.PolyMesh.read_gmsh(p)
     # a declared count above the rows present
-    _write_msh(str(p), pts, hexes, tags, "2.2")
+    K.write_msh_box(str(p), pts, hexes, tags, "2.2")
     text = p.read_text().replace("$Elements\n%d\n" % len(hexes), "$Elements\n%d\n" % (len(hexes) + 1))
     p.write_text(text)
     with pytest.raises(cf.CfgError, match="truncated"):
         cf.PolyMesh.read_gmsh(p)
     # a 4.1 element line of another width after the first
-    _write_msh(str(p), pts, hexes, tags, "4.1")
+    K.write_msh_box(str(p), pts, hexes, tags, "4.1")
     lines = p.read_text().split("\n")
     k = lines.index("$Elements") + 3 + 17000
     lines[k] = lines[k] + " 1"

@@ -202,3 +202,51 @@ def test_coupled_fixture_matches_fresh_reference(golden):
         lines = open(os.path.join(td, "history.txt")).read().split("\n")
     rows = np.array([list(map(float, ln.split())) for ln in lines if ln and not ln.startswith("result")])
     assert np.array_equal(rows, g["history"])
+
+
+@ref
+def test_large_grouped_gmsh_file_matches_fresh_reference(tmp_path):
+    """A 26^3 hex box with physical groups (the outlet as triangles over its
+    quad faces), large enough that the product's reader splits its rows over
+    threads, read by the reference's own gmsh reader and by the product's:
+    addressing, patches and geometry bit for bit."""
+    cf = pytest.importorskip("chuanflow_b200")
+    mp = tmp_path / "box.msh"
+    K.grouped_box_file(str(mp), n=26)
+    cp = tmp_path / "case.dict"
+    cp.write_text(f'mesh {{ format gmsh; file "{mp}"; patches {{ inlet {{ type inlet; }} '
+                  f'outlet {{ type outlet; }} }} }}\n')
+    r = O.ref_mesh(str(cp))
+    m = cf.PolyMesh.read_gmsh(mp, {"inlet": "inlet", "outlet": "outlet"})
+    assert m.n_cells == 26 ** 3
+    a, g = m.addressing(), m.geometry()
+    for k in ("face_offsets", "face_verts", "owner", "points"):
+        assert np.array_equal(a[k], r[k]), k
+    assert np.array_equal(a["neighbour"][:m.n_internal_faces], r["neighbour"])
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(g[k], r[k]), k
+    assert [(n, t, s, z) for n, t, s, z in m.patches] == [(p[0], p[1], int(p[2]), int(p[3])) for p in r["patches"]]
+
+
+@ref
+@pytest.mark.parametrize("fmt", ["2.2", "4.1"])
+def test_large_plane_named_gmsh_file_matches_fresh_reference(tmp_path, fmt):
+    """A 30^3 hex box without surface groups, node tags sparse and shuffled,
+    in both formats: boundary faces named after the bounding-box planes by
+    both readers alike."""
+    cf = pytest.importorskip("chuanflow_b200")
+    pts, hexes, _ = K.hex_box_cells(30)
+    tags = np.random.default_rng(5).permutation(len(pts)) * 2 + 3
+    mp = tmp_path / "box.msh"
+    K.write_msh_box(str(mp), pts, hexes, tags, fmt)
+    cp = tmp_path / "case.dict"
+    cp.write_text(f'mesh {{ format gmsh; file "{mp}"; }}\n')
+    r = O.ref_mesh(str(cp))
+    m = cf.PolyMesh.read_gmsh(mp)
+    a, g = m.addressing(), m.geometry()
+    for k in ("face_offsets", "face_verts", "owner", "points"):
+        assert np.array_equal(a[k], r[k]), k
+    assert np.array_equal(a["neighbour"][:m.n_internal_faces], r["neighbour"])
+    for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
+        assert np.array_equal(g[k], r[k]), k
+    assert [(n, t, s, z) for n, t, s, z in m.patches] == [(p[0], p[1], int(p[2]), int(p[3])) for p in r["patches"]]
