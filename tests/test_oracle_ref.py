@@ -250,3 +250,27 @@ def test_large_plane_named_gmsh_file_matches_fresh_reference(tmp_path, fmt):
     for k in ("V", "C", "Cf", "Sf", "magSf", "d", "invDist"):
         assert np.array_equal(g[k], r[k]), k
     assert [(n, t, s, z) for n, t, s, z in m.patches] == [(p[0], p[1], int(p[2]), int(p[3])) for p in r["patches"]]
+
+
+@ref
+def test_large_ascii_vtu_is_the_reference_writers_file(tmp_path):
+    """VtkWriter's ASCII .vtu of a jittered 28^3 cavity (its polyhedra built
+    on the product writer's threads), byte for byte against the reference's
+    writer run here."""
+    cf = pytest.importorskip("chuanflow_b200")
+    n = (28, 28, 28)
+    m = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), n, {s: (nm, "wall") for s, nm in zip(K.SIDES, K.CAVITY_NAMES)})
+    m.jitter_interior(0.1, 11)
+    rng = np.random.default_rng(8)
+    p, U = rng.normal(size=m.n_cells), rng.normal(size=(m.n_cells, 3))
+    cp = tmp_path / "case.dict"
+    cp.write_text(K.cavity_dict(*n))
+    pts = tmp_path / "points.f64"
+    m.addressing()["points"].tofile(pts)
+    p.tofile(tmp_path / "p.f64")
+    U.tofile(tmp_path / "U.f64")
+    ref_out = tmp_path / "ref.vtu"
+    O.ref_run(["vtk", str(cp), str(ref_out), str(pts), str(tmp_path / "p.f64"), str(tmp_path / "U.f64")])
+    out = tmp_path / "a.vtu"
+    m.write_vtu(out, {"p": p, "U": U}, binary=False)
+    assert out.read_bytes() == ref_out.read_bytes()
