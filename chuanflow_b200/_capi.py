@@ -536,6 +536,13 @@ def solve_bicgstab(row_start, cols, vals, b, x0, tol, max_iter, device=0):
     return _sparse(1, row_start, cols, vals, b, x0, tol, max_iter, device)
 
 
+def _number_or_word(x):
+    try:
+        return float(x)
+    except ValueError:
+        return x
+
+
 def inspect_case_file(path):
     """Host-only parse of a case file: a dict of what the runner would use."""
     buf = C.create_string_buffer(1 << 16)
@@ -547,20 +554,27 @@ def inspect_case_file(path):
             out["patches"][v[0]] = {"type": v[1], "start": int(v[2]), "size": int(v[3]), "U_type": int(v[5]),
                                     "U": tuple(float(x) for x in v[6:9]), "p_type": int(v[10]), "p": float(v[11])}
         else:
-            out[k] = [float(x) if any(ch in x for ch in ".e") or x.lstrip("-").isdigit() else x for x in v]
+            out[k] = [_number_or_word(x) for x in v]
     return out
 
 
-def run_case_file(path, device=0):
-    """A chflow-simple-foam case file end to end; returns (result, U, p, phi)."""
+def run_case_file(path, device=0, fields=False):
+    """A chflow-simple-foam case file end to end; returns (result, counts),
+    or with fields=True (result, counts, (U, p, phi)): the case is then run
+    a second time into buffers sized by the first run's counts."""
     counts = np.zeros(5, np.int64)
     r = _Result()
-    # two calls: the first sizes the fields
     _check(lib().cfg_run_case_file(str(path).encode(), C.c_int32(device), C.byref(r), _ip(counts), None, None,
                                    None))
-    return SimpleResult(r.iterations, bool(r.converged), r.final_continuity_error, r.final_momentum_residual,
-                        r.last_dp, r.last_continuity_corrected, r.u_inner_iterations, r.p_inner_iterations,
-                        bool(r.diverged)), counts
+    res = lambda: SimpleResult(r.iterations, bool(r.converged), r.final_continuity_error, r.final_momentum_residual,
+                               r.last_dp, r.last_continuity_corrected, r.u_inner_iterations, r.p_inner_iterations,
+                               bool(r.diverged))
+    if not fields:
+        return res(), counts
+    U, p, phi = np.zeros((int(counts[1]), 3)), np.zeros(int(counts[1])), np.zeros(int(counts[2]))
+    _check(lib().cfg_run_case_file(str(path).encode(), C.c_int32(device), C.byref(r), _ip(counts), _dp(U), _dp(p),
+                                   _dp(phi)))
+    return res(), counts, (U, p, phi)
 
 
 # ---- detail blocks and batches --------------------------------------------

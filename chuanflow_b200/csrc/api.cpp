@@ -527,6 +527,10 @@ struct CaseSpec
     double u0[3] = {0, 0, 0};
     cfg_schemes schemes{CFG_DIV_UPWIND, 1, CFG_GRAD_CORRECTED, 0.9};
     cfg_simple_controls ctl{};
+    // turbulence{} (TurbulenceConfig, TurbulenceModel.h:50-59 defaults)
+    std::string turbModel = "laminar";
+    double turbIntensity = 0.05, turbLength = -1, turbRelax = 0.7;
+    double cDES = 0.61, reOnset = 0, onsetWidth = -1, gammaRate = 4.0;
 };
 
 CaseSpec parseCase(const char* path)
@@ -690,6 +694,26 @@ CaseSpec parseCase(const char* path)
             for (int i = 0; i < 3; ++i) c.body_force[i] = f[i];
         }
     }
+    // turbulence{} (TurbulenceConfig::fromCase, turbulenceModel.cpp:41-56):
+    // a missing block means laminar
+    if (d.has("turbulence"))
+    {
+        const cfg::Dict& t = d.dict("turbulence");
+        cs.turbModel = t.wordOr("model", cs.turbModel);
+        cs.turbIntensity = t.numberOr("intensity", cs.turbIntensity);
+        cs.turbLength = t.numberOr("lengthScale", cs.turbLength);
+        cs.turbRelax = t.numberOr("relaxation", cs.turbRelax);
+        cs.cDES = t.numberOr("C_DES", cs.cDES);
+        cs.reOnset = t.numberOr("reOnset", cs.reOnset);
+        cs.onsetWidth = t.numberOr("onsetWidth", cs.onsetWidth);
+        cs.gammaRate = t.numberOr("gammaRate", cs.gammaRate);
+        if (!(cs.turbIntensity >= 0)) cfg::fail(CFG_ESETUP, "turbulence: intensity must be non-negative");
+        if (!(cs.turbRelax > 0 && cs.turbRelax <= 1)) cfg::fail(CFG_ESETUP, "turbulence: relaxation must be in (0, 1]");
+        const std::string& m = cs.turbModel;
+        if (m != "laminar" && m != "kEpsilon" && m != "kOmegaSST" && m != "des" && m != "gammaTransition")
+            cfg::fail(CFG_ESETUP, "turbulence: unknown model '" + m +
+                                      "' (laminar | kEpsilon | kOmegaSST | des | gammaTransition)");
+    }
     // gpu{}: settings the reference does not have; defaults reproduce it
     if (d.has("gpu"))
     {
@@ -734,6 +758,8 @@ int cfg_case_inspect(const char* path, char* out, size_t size)
         add("force %.17g %.17g %.17g\nnu %.17g\n", c.body_force[0], c.body_force[1], c.body_force[2], c.nu);
         add("gpu %d %lld %.17g\n", c.p_precond, static_cast<long long>(c.p_ref_cell), c.p_ref_value);
         if (cs.hasU0) add("initialU %.17g %.17g %.17g\n", cs.u0[0], cs.u0[1], cs.u0[2]);
+        add("turbulence %s %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", cs.turbModel.c_str(), cs.turbIntensity,
+            cs.turbLength, cs.turbRelax, cs.cDES, cs.reOnset, cs.onsetWidth, cs.gammaRate);
         std::snprintf(out, size, "%s", s.c_str());
     });
 }
@@ -756,6 +782,12 @@ int cfg_run_case_file(const char* path, int32_t device, cfg_simple_result* resul
         ctx.initFlux(nullptr);
         if (cs.hasU0) ctx.initFlux(cs.u0);
         ctx.setSchemes(cs.schemes);
+        // the RANS model, created after the initial flux (simpleFoamApp.cpp:93-102)
+        if (cs.turbModel != "laminar")
+        {
+            ctx.turbulenceParams(cs.cDES, cs.reOnset, cs.onsetWidth, cs.gammaRate);
+            ctx.turbulenceSetup(cs.turbModel.c_str(), cs.turbIntensity, cs.turbLength, cs.turbRelax, cs.ctl.nu);
+        }
         ctx.iterate(cs.ctl, *result);
         if (counts)
         {

@@ -139,3 +139,19 @@ def test_writers_refuse_null_arguments():
     assert b"cfg_mesh_write_hdf5" in buf.value
     assert lib.cfg_write_hdf5(None, b"x.h5") == 1
     assert lib.cfg_mesh_write_vtu(None, b"x.vtu", 0, None, None, None, 1) == 1
+
+
+def test_case_file_turbulence_block(tmp_path):
+    """turbulence{} as TurbulenceConfig::fromCase reads it (its defaults when
+    keys are missing, laminar without the block) and its refusals."""
+    base = "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\nnu 1;\n"
+    out = cf.inspect_case_file(write(tmp_path, base))
+    assert out["turbulence"] == ["laminar", 0.05, -1.0, 0.7, 0.61, 0.0, -1.0, 4.0]
+    out = cf.inspect_case_file(write(tmp_path, base + "turbulence { model des; intensity 0.02; lengthScale 0.01; "
+                                                     "relaxation 0.5; C_DES 0.65; }\n"))
+    assert out["turbulence"] == ["des", 0.02, 0.01, 0.5, 0.65, 0.0, -1.0, 4.0]
+    for text, msg in (("turbulence { model kOmega; }", "unknown model 'kOmega'"),
+                      ("turbulence { model kEpsilon; relaxation 0; }", "relaxation must be in (0, 1]"),
+                      ("turbulence { model kEpsilon; intensity -1; }", "intensity must be non-negative")):
+        with pytest.raises(cf.CfgError, match=re.escape(msg)):
+            cf.inspect_case_file(write(tmp_path, base + text + "\n"))

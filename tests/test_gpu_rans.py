@@ -100,3 +100,17 @@ def test_case_hdf5_carries_the_device_fields(tmp_path):
     assert np.array_equal(data["/fields/k"], t["k"]) and np.array_equal(data["/fields/nut"], t["nut"])
     assert np.array_equal(data["/fields/omega"], t["eps"])
     assert np.array_equal(data["/points"], mesh.addressing()["points"])
+
+
+@pytest.mark.parametrize("fixture", ["rans_channel.npz", "rans_sst.npz", "rans_des.npz", "rans_transition.npz"])
+def test_case_file_with_turbulence_matches_reference(golden, tmp_path, fixture):
+    """cfg_run_case_file on the fixture's own case file, turbulence{} block
+    included, as the reference's simpleFoam app reads it: the same fields."""
+    import chuanflow_b200 as cf
+    g = golden(fixture)
+    path = tmp_path / "case.dict"
+    path.write_text(str(g["dict"]))
+    res, counts, (U, p, phi) = cf.run_case_file(path, fields=True)
+    assert res.iterations == int(g["iterations"])
+    for a, b, name in ((U, g["U"], "U"), (p, g["p"], "p"), (phi, g["phi"], "phi")):
+        assert rel(a, b) < REL_TOL, (name, rel(a, b))
