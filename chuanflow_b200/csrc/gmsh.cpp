@@ -410,7 +410,8 @@ Mesh readGmsh(const std::string& path, const std::map<std::string, std::string>&
                 used.insert(cand);
             }
         }
-        std::stable_sort(rec.begin(), rec.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        const auto byTag = [](const auto& a, const auto& b) { return a.first < b.first; };
+        if (!std::is_sorted(rec.begin(), rec.end(), byTag)) std::stable_sort(rec.begin(), rec.end(), byTag);
         points.reserve(rec.size());
         sortedTags.reserve(rec.size());
         for (const auto& r : rec)
