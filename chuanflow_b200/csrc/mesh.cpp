@@ -480,72 +480,98 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
         }
     }
     std::vector<int64_t>().swap(first);
-    // boundary faces named after the bounding-box plane they lie on
-    // (gmshMesh.cpp:636-667, the case of a file without surface groups)
-    Vec lo = points[0], hi = points[0];
-    for (const Vec& v : points)
+    // ---- boundary faces to patches ----
+    // A boundary face takes the physical-group name of a surface element on
+    // it, else the name of the bounding-box plane it lies in: within 1e-9 of
+    // the box's largest extent of that plane.  Every point is on one side of
+    // a box plane, so the face vertex farthest from it decides, and each
+    // face's per-axis coordinate range is enough: fmax - lo <= eps puts it
+    // in a low plane, hi - fmin <= eps in a high one.  Planes are tried in
+    // the order low x, high x, low y, high y, low z, high z.
+    double lo[3] = {points[0].x, points[0].y, points[0].z};
+    double hi[3] = {lo[0], lo[1], lo[2]};
     {
-        lo.x = std::min(lo.x, v.x); hi.x = std::max(hi.x, v.x);
-        lo.y = std::min(lo.y, v.y); hi.y = std::max(hi.y, v.y);
-        lo.z = std::min(lo.z, v.z); hi.z = std::max(hi.z, v.z);
-    }
-    const double extent = std::max({hi.x - lo.x, hi.y - lo.y, hi.z - lo.z, 1e-300});
-    const double eps = 1e-9 * extent;
-    const char* planeNames[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
-    auto comp = [](const Vec& v, int d) { return d == 0 ? v.x : (d == 1 ? v.y : v.z); };
-    auto planeOf = [&](const Ref& r) -> int {
-        for (int d = 0; d < 3; ++d)
-            for (int s = 0; s < 2; ++s)
+        const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(32, nPoints / (1 << 16)));
+        std::vector<std::array<double, 6>> part(static_cast<size_t>(parts));
+        parallelChunks(parts, 1, [&](int64_t pb, int64_t pe) {
+            for (int64_t q = pb; q < pe; ++q)
             {
-                const double lim = s ? comp(hi, d) : comp(lo, d);
-                bool on = true;
-                for (int64_t k = 0; k < r.nv; ++k)
-                    if (std::abs(comp(points[static_cast<size_t>(ringVerts[r.v0 + k])], d) - lim) > eps)
+                auto& box = part[static_cast<size_t>(q)];
+                box = {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]};
+                for (int64_t i = nPoints * q / parts; i < nPoints * (q + 1) / parts; ++i)
+                {
+                    const double x[3] = {points[i].x, points[i].y, points[i].z};
+                    for (int d = 0; d < 3; ++d)
                     {
-                        on = false;
-                        break;
+                        box[d] = std::min(box[d], x[d]);
+                        box[3 + d] = std::max(box[3 + d], x[d]);
                     }
-                if (on) return 2 * d + s;
+                }
             }
+        });
+        for (const auto& box : part)
+            for (int d = 0; d < 3; ++d)
+            {
+                lo[d] = std::min(lo[d], box[d]);
+                hi[d] = std::max(hi[d], box[3 + d]);
+            }
+    }
+    const double eps = 1e-9 * std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-300});
+    static const char* const kPlane[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+    auto boxPlane = [&](const Ref& r) -> int {
+        double fmin[3], fmax[3];
+        for (int64_t k = 0; k < r.nv; ++k)
+        {
+            const Vec& v = points[static_cast<size_t>(ringVerts[r.v0 + k])];
+            const double x[3] = {v.x, v.y, v.z};
+            for (int d = 0; d < 3; ++d)
+            {
+                fmin[d] = k ? std::min(fmin[d], x[d]) : x[d];
+                fmax[d] = k ? std::max(fmax[d], x[d]) : x[d];
+            }
+        }
+        for (int d = 0; d < 3; ++d)
+        {
+            if (fmax[d] - lo[d] <= eps) return 2 * d;
+            if (hi[d] - fmin[d] <= eps) return 2 * d + 1;
+        }
         return -1;
     };
-    // the physical-group name of a boundary face: its own surface element,
-    // or for a quad face one of the triangles a triangulated surface split
-    // it into (gmshMesh.cpp:617-634)
-    auto nameOf = [&](const Ref& r) -> const std::string* {
-        std::array<int64_t, 5> key{-1, -1, -1, -1, -1};
-        for (int64_t k = 0; k < r.nv; ++k) key[k] = ringVerts[r.v0 + k];
+    // the group of a face: a surface element with the face's vertex set, or
+    // for a quad one with the vertex set left when one ring vertex (0, then
+    // 1, 2, 3) is dropped -- a triangulated surface splits quads in two
+    auto surfaceGroup = [&](const Ref& r) -> const std::string* {
+        std::array<int64_t, 5> key;
+        key.fill(-1);
+        std::copy(ringVerts.begin() + r.v0, ringVerts.begin() + r.v0 + r.nv, key.begin());
         std::sort(key.begin(), key.begin() + r.nv);
-        auto it = surfaceNames.find(key);
-        if (it != surfaceNames.end()) return &it->second;
-        if (r.nv == 4)
-            for (int skip = 0; skip < 4; ++skip)
+        if (const auto it = surfaceNames.find(key); it != surfaceNames.end()) return &it->second;
+        if (r.nv != 4) return nullptr;
+        for (int drop = 0; drop < 4; ++drop)
+        {
+            const int64_t gone = ringVerts[r.v0 + drop];
+            std::array<int64_t, 5> tri;
+            tri.fill(-1);
+            bool dropped = false;
+            for (int k = 0, t = 0; k < 4; ++k)
             {
-                std::array<int64_t, 5> tri{-1, -1, -1, -1, -1};
-                int t = 0;
-                for (int k = 0; k < 4; ++k)
-                    if (k != skip) tri[t++] = ringVerts[r.v0 + k];
-                std::sort(tri.begin(), tri.begin() + 3);
-                auto jt = surfaceNames.find(tri);
-                if (jt != surfaceNames.end()) return &jt->second;
+                if (!dropped && key[k] == gone)
+                {
+                    dropped = true;
+                    continue;
+                }
+                tri[t++] = key[k];
             }
+            if (const auto it = surfaceNames.find(tri); it != surfaceNames.end()) return &it->second;
+        }
         return nullptr;
     };
     Mesh m;
     m.points = points;
+    // patches in order of their first face
     std::vector<std::vector<size_t>> patchFaces;
+    std::unordered_map<std::string, size_t> patchOf;
     std::vector<size_t> internal;
-    auto patchIndex = [&](const std::string& name) {
-        for (size_t p = 0; p < m.patches.size(); ++p)
-            if (m.patches[p].name == name) return p;
-        Mesh::Patch p;
-        p.name = name;
-        const auto t = patchTypes.find(name);
-        p.type = t != patchTypes.end() ? t->second : "wall";
-        m.patches.push_back(p);
-        patchFaces.emplace_back();
-        return m.patches.size() - 1;
-    };
     for (size_t i = 0; i < refs.size(); ++i)
     {
         Ref& r = refs[i];
@@ -555,20 +581,33 @@ Mesh meshFromCells(const std::vector<Vec>& points, const std::vector<int32_t>& t
             internal.push_back(i);
             continue;
         }
-        const std::string* named = surfaceNames.empty() ? nullptr : nameOf(r);
+        const std::string* group = surfaceNames.empty() ? nullptr : surfaceGroup(r);
         std::string name;
-        if (named)
-        {
-            name = *named;
-        }
+        if (group) name = *group;
         else
         {
-            const int pl = planeOf(r);
-            if (pl < 0)
-                fail(CFG_EMESH, "mesh: a boundary face belongs to no physical group and lies on no bounding-box plane");
-            name = planeNames[pl];
+            const int plane = boxPlane(r);
+            if (plane < 0)
+            {
+                std::string list;
+                for (int64_t k = 0; k < r.nv; ++k) list += " " + std::to_string(ringVerts[r.v0 + k]);
+                fail(CFG_EMESH, "gmsh: boundary face with nodes" + list +
+                                    " belongs to no physical group and lies on no bounding-box plane; give every "
+                                    "boundary surface a physical group in Gmsh");
+            }
+            name = kPlane[plane];
         }
-        patchFaces[patchIndex(name)].push_back(i);
+        auto [it, added] = patchOf.emplace(name, m.patches.size());
+        if (added)
+        {
+            Mesh::Patch p;
+            p.name = name;
+            const auto t = patchTypes.find(name);
+            p.type = t != patchTypes.end() ? t->second : "wall";
+            m.patches.push_back(p);
+            patchFaces.emplace_back();
+        }
+        patchFaces[it->second].push_back(i);
     }
     m.faceOffsets.reserve(refs.size() + 1);
     m.faceVerts.reserve(ringVerts.size());

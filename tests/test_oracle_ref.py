@@ -3,6 +3,7 @@ reference: bit-for-bit against the golden fixtures the reference produced,
 and, where the reference driver is built (oracle/_ref), against fresh runs
 of the reference on cases the fixtures do not cover.  CPU only."""
 import os
+import re
 import subprocess
 import tempfile
 
@@ -274,3 +275,85 @@ def test_large_ascii_vtu_is_the_reference_writers_file(tmp_path):
     out = tmp_path / "a.vtu"
     m.write_vtu(out, {"p": p, "U": U}, binary=False)
     assert out.read_bytes() == ref_out.read_bytes()
+
+
+_MSH_HEAD = "$MeshFormat\n2.2 0 8\n$EndMeshFormat\n"
+_NODES5 = "$Nodes\n5\n1 0 0 0\n2 1 0 0\n3 0 1 0\n4 0 0 1\n5 1 1 1\n$EndNodes\n"
+_TET = "1 4 2 1 1 1 2 3 4"
+_MSH41_HEAD = "$MeshFormat\n4.1 0 8\n$EndMeshFormat\n"
+_NODES41 = ("$Nodes\n1 4 1 4\n3 1 0 4\n1\n2\n3\n4\n0 0 0\n1 0 0\n0 1 0\n0 0 1\n$EndNodes\n")
+
+# malformed (and a few unusual but valid) files: both readers must agree on
+# the outcome, and on the message when they refuse the file
+GMSH_CASES = {
+    "binary": "$MeshFormat\n2.2 1 8\n$EndMeshFormat\n",
+    "version": "$MeshFormat\n3.0 0 8\n$EndMeshFormat\n",
+    "no_format_fields": "$MeshFormat\n2.2\n$EndMeshFormat\n",
+    "no_nodes": _MSH_HEAD + "$Elements\n1\n" + _TET + "\n$EndElements\n",
+    "unterminated": _MSH_HEAD + "$Nodes\n1\n1 0 0 0\n",
+    "empty_nodes": _MSH_HEAD + "$Nodes\n$EndNodes\n$Elements\n1\n" + _TET + "\n$EndElements\n",
+    "nodes_ran_out": _MSH_HEAD + "$Nodes\n6\n1 0 0 0\n2 1 0 0\n$EndNodes\n",
+    "short_node_row": _MSH_HEAD + "$Nodes\n2\n1 0 0 0\n2 1 0\n$EndNodes\n",
+    "bad_tag": _MSH_HEAD + "$Nodes\n1\nx1 0 0 0\n$EndNodes\n",
+    "bad_coordinate": _MSH_HEAD + "$Nodes\n1\n1 0 abc 0\n$EndNodes\n",
+    "duplicate_tag": _MSH_HEAD + "$Nodes\n3\n1 0 0 0\n2 1 0 0\n2 0 1 0\n$EndNodes\n",
+    "unknown_node": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 4 2 1 1 1 2 3 9\n$EndElements\n",
+    "second_order": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 11 2 1 1 1 2 3 4 5 1 2 3 4 5\n$EndElements\n",
+    "short_element": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 4 2 1 1 1 2 3\n$EndElements\n",
+    "element_row": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 4\n$EndElements\n",
+    "pyramid": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 7 2 1 1 1 2 3 4 5\n$EndElements\n",
+    "repeated_node": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 4 2 1 1 1 2 2 4\n$EndElements\n",
+    "no_volumes": _MSH_HEAD + _NODES5 + "$Elements\n1\n1 2 2 1 1 1 2 3\n$EndElements\n",
+    # a node error in row 1 and a layout error in row 2: layout comes first
+    "layout_before_nodes": _MSH_HEAD + _NODES5 + "$Elements\n2\n1 4 2 1 1 1 2 3 9\n2 4 2 1 1 1 2\n$EndElements\n",
+    "elements_ran_out": _MSH_HEAD + _NODES5 + "$Elements\n3\n" + _TET + "\n$EndElements\n",
+    "unnamed_group": _MSH_HEAD + '$PhysicalNames\n1\n2 1 ""\n$EndPhysicalNames\n' + _NODES5,
+    "group_row": _MSH_HEAD + "$PhysicalNames\n1\n2 1\n$EndPhysicalNames\n" + _NODES5,
+    "one_tet": _MSH_HEAD + _NODES5 + "$Elements\n1\n" + _TET + "\n$EndElements\n",
+    "two_tets_shuffled_tags": _MSH_HEAD + "$Nodes\n5\n50 0 0 0\n7 1 0 0\n30 0 1 0\n4 0 0 1\n9 1 1 1\n$EndNodes\n"
+                              "$Elements\n2\n1 4 0 50 7 30 4\n2 4 0 7 30 4 9\n$EndElements\n",
+    "v41_tet": _MSH41_HEAD + _NODES41 + "$Elements\n1 1 1 1\n3 1 4 1\n1 1 2 3 4\n$EndElements\n",
+    "v41_untagged_width": _MSH41_HEAD + _NODES41 + "$Elements\n1 1 1 1\n3 1 4 1\n1 2 3 4\n$EndElements\n",
+    "v41_width": _MSH41_HEAD + _NODES41 + "$Elements\n1 1 1 1\n3 1 4 1\n1 2 3\n$EndElements\n",
+    "v41_width_changed": _MSH41_HEAD + _NODES41 + "$Elements\n1 2 1 2\n3 1 4 2\n1 1 2 3 4\n1 2 3 4\n$EndElements\n",
+    "v41_count": _MSH41_HEAD + _NODES41 + "$Elements\n1 2 1 1\n3 1 4 1\n1 1 2 3 4\n$EndElements\n",
+    "v41_nodes_header": _MSH41_HEAD + "$Nodes\n1 4\n$EndNodes\n",
+    "v41_node_block": _MSH41_HEAD + "$Nodes\n1 4 1 4\n3 1\n$EndNodes\n",
+    "v41_node_count": _MSH41_HEAD + "$Nodes\n1 5 1 5\n3 1 0 4\n1\n2\n3\n4\n0 0 0\n1 0 0\n0 1 0\n0 0 1\n$EndNodes\n",
+    # a block whose tag rows are missing: its nodes take the free tags
+    "v41_untagged_nodes": _MSH41_HEAD + "$Nodes\n1 4 1 4\n3 1 0 4\n0 0 0\n1 0 0\n0 1 0\n0 0 1\n$EndNodes\n"
+                          "$Elements\n1 1 1 1\n3 1 4 1\n1 1 2 3 4\n$EndElements\n",
+    "v41_entities": _MSH41_HEAD + "$Entities\n0 0 1 0\n1 0 0 0 1 1\n$EndEntities\n" + _NODES41,
+    "v41_elements_header": _MSH41_HEAD + _NODES41 + "$Elements\n1 1\n$EndElements\n",
+}
+
+
+@ref
+@pytest.mark.parametrize("case", sorted(GMSH_CASES))
+def test_gmsh_reader_outcomes_match_reference(tmp_path, case):
+    """The product's gmsh reader and the reference's own, on small malformed
+    or unusual files: the same refusal message, or the same mesh."""
+    cf = pytest.importorskip("chuanflow_b200")
+    mp = tmp_path / "m.msh"
+    mp.write_text(GMSH_CASES[case])
+    cp = tmp_path / "case.dict"
+    cp.write_text(f'mesh {{ format gmsh; file "{mp}"; }}\n')
+    try:
+        r = O.ref_mesh(str(cp))
+        ref_err = None
+    except RuntimeError as e:
+        # cfFatal prefixes the reference's source file:line
+        r, ref_err = None, re.sub(r"^\S+:\d+ ", "", str(e).split("cf_ref_driver: ", 1)[-1])
+    try:
+        m = cf.PolyMesh.read_gmsh(mp)
+        err = None
+    except cf.CfgError as e:
+        m, err = None, str(e).split("] ", 1)[-1]
+    assert (ref_err is None) == (err is None), (ref_err, err)
+    if err is not None:
+        assert err == ref_err
+        return
+    a = m.addressing()
+    for k in ("face_offsets", "face_verts", "owner", "points"):
+        assert np.array_equal(a[k], r[k]), k
+    assert [(n, t, s, z) for n, t, s, z in m.patches] == [(p[0], p[1], int(p[2]), int(p[3])) for p in r["patches"]]
