@@ -135,6 +135,37 @@ def make_case(n, device, precond="Jacobi"):
     return mesh, case, ctl
 
 
+def _splitmix64(x):
+    """splitmix64 over a uint64 array (numpy wraps on overflow)."""
+    x = x + np.uint64(0x9E3779B97F4A7C15)
+    z = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def cavity_points(n, fraction=JITTER, seed=SEED):
+    """The points of the jittered n^3 unit-box cavity, computed in numpy
+    with the same IEEE operations as BlockMesh::create's coordAt
+    (blockMesh.cpp:52-57) and cfg_mesh_jitter_interior (every interior point
+    moves by (2u - 1) fraction h per axis, u = splitmix64(seed *
+    0x100000001B3 ^ (3 point + axis)) >> 11 over 2^53), so the reference arm
+    needs no product library to build the same mesh."""
+    c = 0.0 + (1.0 - 0.0) * np.arange(n + 1, dtype=np.float64) / float(n)
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    pts = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    inner = np.arange(1, n)
+    k, j, i = np.meshgrid(inner, inner, inner, indexing="ij")
+    pid = (i + (n + 1) * (j + (n + 1) * k)).ravel().astype(np.uint64)
+    s0 = np.uint64((seed * 0x100000001B3) & ((1 << 64) - 1))
+    h = (1.0 - 0.0) / float(n)
+    with np.errstate(over="ignore"):
+        for a in range(3):
+            r = _splitmix64(s0 ^ (pid * np.uint64(3) + np.uint64(a)))
+            u = (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+            pts[pid.astype(np.int64), a] += (u * 2.0 - 1.0) * fraction * h
+    return pts
+
+
 def case_dict(n):
     sides = "\n".join(f"    {s} {{ name {nm}; type wall; }}" for s, nm in zip(SIDES, NAMES))
     pats = "\n".join(f"    {nm} {{ U ({'1' if nm == 'lid' else '0'} 0 0); }}" for nm in NAMES)

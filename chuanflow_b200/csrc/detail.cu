@@ -78,6 +78,126 @@ Vec patchArea(const Mesh& M, int patch)
 double comp(const Vec& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
 double hdot(const Vec& a, const Vec& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
+/// The box of the mesh points (polyMesh::minX / maxX).
+struct Box
+{
+    double lo[3], hi[3];
+};
+
+Box pointBox(const Mesh& M)
+{
+    Box b{{M.points[0].x, M.points[0].y, M.points[0].z}, {M.points[0].x, M.points[0].y, M.points[0].z}};
+    for (const Vec& p : M.points)
+    {
+        const double x[3] = {p.x, p.y, p.z};
+        for (int k = 0; k < 3; ++k)
+        {
+            b.lo[k] = std::min(b.lo[k], x[k]);
+            b.hi[k] = std::max(b.hi[k], x[k]);
+        }
+    }
+    return b;
+}
+
+/// The cells of the first and the last cross-section the flow meets.  Cells
+/// are ranked by (axial centre, index) and taken in flow order; a section is
+/// a run of cells whose centres lie within `band` of the run's first one
+/// (DetailBlock::buildSections, coupledNetwork.cpp:644-667).
+void endSections(const Mesh& M, int axis, int flowSign, double band, std::vector<int64_t>& first,
+                 std::vector<int64_t>& last)
+{
+    const size_t n = static_cast<size_t>(M.nCells);
+    std::vector<std::pair<double, int64_t>> rank(n);
+    for (size_t c = 0; c < n; ++c) rank[c] = {comp(M.C[c], axis), static_cast<int64_t>(c)};
+    std::sort(rank.begin(), rank.end());
+    // position i in flow order
+    auto at = [&](size_t i) -> const std::pair<double, int64_t>& { return rank[flowSign > 0 ? i : n - 1 - i]; };
+    size_t runs = 0, lastStart = 0;
+    for (size_t i = 0; i < n;)
+    {
+        const double anchor = at(i).first;
+        size_t j = i + 1;
+        while (j < n && std::abs(at(j).first - anchor) <= band) ++j;
+        if (runs == 0)
+            for (size_t k = i; k < j; ++k) first.push_back(at(k).second);
+        lastStart = i;
+        ++runs;
+        i = j;
+    }
+    if (runs < 2)
+        fail(CFG_ESETUP, "detailBlock: the detailed region has fewer than two cross-sections to measure a drop between");
+    for (size_t k = lastStart; k < n; ++k) last.push_back(at(k).second);
+}
+
+/// Bit k set: wall patches close the section on both sides across axis k
+/// (each wall counted on the axis its area vector points along most).
+unsigned wallBoundedAxes(const Mesh& M, int flowAxis)
+{
+    unsigned low = 0, high = 0;
+    for (int pi = 0; pi < static_cast<int>(M.patches.size()); ++pi)
+    {
+        if (M.patches[static_cast<size_t>(pi)].type != "wall") continue;
+        const Vec a = patchArea(M, pi);
+        if (!(std::sqrt(hdot(a, a)) > 0)) continue;
+        const double s[3] = {a.x, a.y, a.z};
+        int k = 0;
+        if (std::abs(s[1]) > std::abs(s[k])) k = 1;
+        if (std::abs(s[2]) > std::abs(s[k])) k = 2;
+        (s[k] < 0 ? low : high) |= 1u << k;
+    }
+    return low & high & ~(1u << flowAxis);
+}
+
+/// Per-face weights of a shaped inlet profile (parabolic or 1/7 power in the
+/// normalised transverse coordinate of each bounded axis, the axes'
+/// factors multiplied in ascending axis order), scaled so the weighted
+/// section area equals the section area: the rate written stays the rate
+/// given (DetailBlock::buildInletProfile, coupledNetwork.cpp:768-877).
+std::vector<double> profileWeights(const Mesh& M, int inlet, double inletArea, unsigned axes, bool parabolic,
+                                   const Box& box, const std::string& shape)
+{
+    double mid[3], half[3];
+    for (int k = 0; k < 3; ++k)
+    {
+        if (!(axes >> k & 1u)) continue;
+        if (!(box.hi[k] > box.lo[k]))
+            fail(CFG_ESETUP, "detailBlock: the inlet section has no extent to spread a profile over");
+        mid[k] = 0.5 * (box.hi[k] + box.lo[k]);
+        half[k] = 0.5 * (box.hi[k] - box.lo[k]);
+    }
+    const auto& pin = M.patches[static_cast<size_t>(inlet)];
+    std::vector<double> w(static_cast<size_t>(pin.size));
+    double sumA = 0, sumWA = 0;
+    double least = std::numeric_limits<double>::max();
+    for (int64_t j = 0; j < pin.size; ++j)
+    {
+        const Vec& fc = M.Cf[static_cast<size_t>(pin.start + j)];
+        const double x[3] = {fc.x, fc.y, fc.z};
+        double f = 1.0;
+        for (int k = 0; k < 3; ++k)
+        {
+            if (!(axes >> k & 1u)) continue;
+            const double eta = (x[k] - mid[k]) / half[k];
+            f *= parabolic ? 1.0 - eta * eta : std::pow(1.0 - std::abs(eta), 1.0 / 7.0);
+        }
+        least = std::min(least, f);
+        w[static_cast<size_t>(j)] = f;
+    }
+    if (!(least > 0)) fail(CFG_ESETUP, "detailBlock: the inlet profile '" + shape + "' writes a zero or reversed weight on a face");
+    for (int64_t j = 0; j < pin.size; ++j)
+    {
+        const double a = M.magSf[static_cast<size_t>(pin.start + j)];
+        sumWA += w[static_cast<size_t>(j)] * a;
+        sumA += a;
+    }
+    if (!(sumA > 0) || !(sumWA > 0)) fail(CFG_ESETUP, "detailBlock: the inlet section integrates to no area");
+    if (std::abs(sumA - inletArea) > 1e-9 * inletArea)
+        fail(CFG_ESETUP, "detailBlock: the inlet patch's face areas do not add to its area vector");
+    const double mean = sumWA / sumA;
+    for (double& x : w) x = x / mean;
+    return w;
+}
+
 }  // namespace
 
 struct DetailState
@@ -125,109 +245,25 @@ void Ctx::detailSetup(const std::string& shape, double rho)
     if (std::abs(nrm.z) > std::abs(comp(nrm, d->axis))) d->axis = 2;
     d->flowSign = comp(nrm, d->axis) < 0 ? 1 : -1;
 
-    // bounding box of the points (polyMesh::minX / maxX)
-    Vec lo = M.points[0], hi = M.points[0];
-    for (const Vec& p : M.points)
+    const Box box = pointBox(M);
     {
-        lo = Vec{std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z)};
-        hi = Vec{std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z)};
+        std::vector<int64_t> c0, c1;
+        endSections(M, d->axis, d->flowSign, 1e-9 * std::max(std::abs(box.hi[d->axis] - box.lo[d->axis]), 1e-30), c0, c1);
+        for (int64_t c : c0) d->first.push_back(inv_[static_cast<size_t>(c)]);
+        for (int64_t c : c1) d->last.push_back(inv_[static_cast<size_t>(c)]);
     }
-
-    // cross-sections in the order the flow meets them (buildSections): cells
-    // by (axial centre, index), grouped while within 1e-9 of the extent
-    {
-        const int64_t nC = M.nCells;
-        const int ax = d->axis;
-        std::vector<int64_t> order(static_cast<size_t>(nC));
-        for (int64_t c = 0; c < nC; ++c) order[c] = c;
-        auto coord = [&](int64_t c) { return comp(M.C[static_cast<size_t>(c)], ax); };
-        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
-            const double ka = coord(a), kb = coord(b);
-            if (ka != kb) return ka < kb;
-            return a < b;
-        });
-        if (d->flowSign < 0) std::reverse(order.begin(), order.end());
-        const double band = 1e-9 * std::max(std::abs(comp(hi, ax) - comp(lo, ax)), 1e-30);
-        std::vector<std::pair<size_t, size_t>> groups;
-        size_t g = 0;
-        while (g < order.size())
-        {
-            const double anchor = coord(order[g]);
-            size_t h = g + 1;
-            while (h < order.size() && std::abs(coord(order[h]) - anchor) <= band) ++h;
-            groups.push_back({g, h});
-            g = h;
-        }
-        if (groups.size() < 2)
-            fail(CFG_ESETUP, "detailBlock: the detailed region has fewer than two cross-sections to measure a drop between");
-        for (size_t k = groups.front().first; k < groups.front().second; ++k)
-            d->first.push_back(inv_[static_cast<size_t>(order[k])]);
-        for (size_t k = groups.back().first; k < groups.back().second; ++k)
-            d->last.push_back(inv_[static_cast<size_t>(order[k])]);
-    }
-
-    // the inlet profile (buildInletProfile)
     if (shape != "flat")
     {
         if (shape != "parabolic" && shape != "power1over7")
             fail(CFG_ESETUP, "detailBlock: the inlet profile '" + shape +
                                  "' is not one this block can write (flat, parabolic, power1over7)");
-        int bounds[3][2] = {{0, 0}, {0, 0}, {0, 0}};
-        for (int pi = 0; pi < nP; ++pi)
-        {
-            if (M.patches[static_cast<size_t>(pi)].type != "wall") continue;
-            const Vec sf = patchArea(M, pi);
-            if (!(std::sqrt(hdot(sf, sf)) > 0)) continue;
-            int k = 0;
-            for (int c = 1; c < 3; ++c)
-                if (std::abs(comp(sf, c)) > std::abs(comp(sf, k))) k = c;
-            if (k == d->axis) continue;
-            bounds[k][comp(sf, k) < 0 ? 0 : 1] = 1;
-        }
-        std::vector<int> axes;
-        for (int k = 0; k < 3; ++k)
-            if (k != d->axis && bounds[k][0] && bounds[k][1]) axes.push_back(k);
-        if (axes.empty())
+        const unsigned axes = wallBoundedAxes(M, d->axis);
+        if (!axes)
             fail(CFG_ESETUP, "detailBlock: the inlet profile '" + shape +
                                  "' has no wall-confined transverse direction to vary along");
-        for (int k : axes)
-            if (!(comp(hi, k) > comp(lo, k)))
-                fail(CFG_ESETUP, "detailBlock: the inlet section has no extent to spread a profile over");
+        d->inletWeights = profileWeights(M, d->inlet, d->inletArea, axes, shape == "parabolic", box, shape);
         const auto& pin = M.patches[static_cast<size_t>(d->inlet)];
-        std::vector<double> w(static_cast<size_t>(pin.size), 0.0);
-        double wMin = std::numeric_limits<double>::max();
-        for (int64_t j = 0; j < pin.size; ++j)
-        {
-            const Vec& fc = M.Cf[static_cast<size_t>(pin.start + j)];
-            double value = 1.0;
-            for (int k : axes)
-            {
-                const double mid = 0.5 * (comp(hi, k) + comp(lo, k));
-                const double half = 0.5 * (comp(hi, k) - comp(lo, k));
-                const double eta = (comp(fc, k) - mid) / half;
-                value *= shape == "parabolic" ? (1.0 - eta * eta) : std::pow(1.0 - std::abs(eta), 1.0 / 7.0);
-            }
-            w[static_cast<size_t>(j)] = value;
-            wMin = std::min(wMin, value);
-        }
-        if (!(wMin > 0))
-            fail(CFG_ESETUP, "detailBlock: the inlet profile writes a zero or reversed weight on a face");
-        double sumWA = 0, sumA = 0;
-        for (int64_t j = 0; j < pin.size; ++j)
-        {
-            const double a = M.magSf[static_cast<size_t>(pin.start + j)];
-            sumWA += w[static_cast<size_t>(j)] * a;
-            sumA += a;
-        }
-        if (!(sumA > 0) || !(sumWA > 0)) fail(CFG_ESETUP, "detailBlock: the inlet section integrates to no area");
-        if (std::abs(sumA - d->inletArea) > 1e-9 * d->inletArea)
-            fail(CFG_ESETUP, "detailBlock: the inlet patch's face areas do not add to its area vector");
-        const double norm = sumWA / sumA;
-        for (int64_t j = 0; j < pin.size; ++j)
-        {
-            d->inletFaces.push_back(pin.start + j);
-            d->inletWeights.push_back(w[static_cast<size_t>(j)] / norm);
-        }
+        for (int64_t j = 0; j < pin.size; ++j) d->inletFaces.push_back(pin.start + j);
     }
     d->dFirst = upload(d->first);
     d->dLast = upload(d->last);

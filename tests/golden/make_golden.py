@@ -52,7 +52,8 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 import _oracle as O  # noqa: E402
 import _cases as K  # noqa: E402
 
-REF_MESHES = "/root/reference/tests/meshes"
+# the reference source tree this script reads the reference's test meshes from
+REF_MESHES = os.path.join(os.environ.get("CHUANFLOW_REFERENCE", "/root/reference"), "tests", "meshes")
 
 
 def mesh_npz(name, case_text, points=None, grad_fields=False):

@@ -172,7 +172,19 @@ def test_rcm_reduces_bandwidth_of_shuffled_mesh(golden):
     assert np.abs(inv[own] - inv[nbr]).max() < np.abs(own - nbr).max()
 
 
-REF_MESHES = "/root/reference/tests/meshes"
+def _reference_tree():
+    """The reference source tree: CHUANFLOW_REFERENCE, else the one
+    oracle/Makefile built its driver from (oracle/_ref/REFERENCE_PATH);
+    empty when neither is there, and the tests that need it skip."""
+    env = os.environ.get("CHUANFLOW_REFERENCE")
+    if env:
+        return env
+    rec = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "REFERENCE_PATH")
+    return open(rec).read().strip() if os.path.exists(rec) else ""
+
+
+REF_MESHES = os.path.join(_reference_tree(), "tests", "meshes") if _reference_tree() else ""
 
 
 def check_fixture(m, g):
