@@ -14,11 +14,18 @@ The workload: 128^3 = 2,097,152 hex cells in the unit box, interior mesh
 points jittered by a seeded uniform +-10% of the cell size, lid (ymax)
 U = (1 0 0), other walls no-slip, nu = 1/400 (Re 400), schemes upwind /
 corrected / corrected, 1 non-orthogonal corrector, relaxU 0.7, relaxP 0.3,
-pRelaxStart 0.02, pressure Jacobi-PCG to 1e-8 (infinity norm relative to the
-right-hand side, the reference's test) with at most 2000 iterations, and a
-pressure reference cell (cell 0) -- without it the reference's singular
-Neumann pressure system, made inconsistent by its own boundary
-non-orthogonal correction, drives p to ~1e12 in the first iteration.
+pRelaxStart 0.02, momentum by the reference's Jacobi-BiCGStab, pressure to
+1e-8 (infinity norm relative to the right-hand side, the reference's test)
+with at most 2000 iterations by FP64 flexible CG preconditioned with an FP32
+aggregation-AMG V-cycle (--p-precond; the line's `variant` runs the same
+steps with FP64 multicolour DIC-PCG), and a pressure reference cell (cell 0)
+-- without it the reference's singular Neumann pressure system, made
+inconsistent by its own boundary non-orthogonal correction, drives p to
+~1e12 in the first iteration.
+
+Every leg counts the outer iterations that diverged (simpleSolver.cpp:360-364:
+non-finite continuity, pressure step or fields); the JSON line carries them
+and the run exits 1 when any did.
 """
 import argparse
 import dataclasses
@@ -43,6 +50,10 @@ NU = 1.0 / 400.0
 NAMES = ["left", "right", "bottom", "lid", "front", "back"]
 SIDES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
 METRIC = "SIMPLE cell-iter/s at 2M cells; time to 1e-8 p-residual, learned vs plain PCG"
+REFERENCE_ARM = ("the reference's CPU SIMPLE (its own sources) on the same mesh and settings, one outer iteration "
+                 "from rest as a bounded sample (a whole 128^3 iteration takes minutes on one core); the reference "
+                 "has no pressure reference cell and no DIC or AMG, so it solves its singular Neumann pressure "
+                 "system with Jacobi-PCG to the same 1e-8 / 2000-iteration limits; one core, pinned")
 
 
 def workload_config(n, precond="DIC"):
@@ -52,7 +63,9 @@ def workload_config(n, precond="DIC"):
                         f"pRelaxStart 0.02, pressure {solve} tol 1e-8 (|r|inf/|b|inf) maxIter 2000, pRefCell 0",
             "cells": n ** 3, "step": "one SIMPLE outer iteration",
             "l2": "inputs larger than L2 (about 1.3 GB of fields, matrices and mesh resident in HBM)",
-            "precision": ("FP64, the pressure preconditioner FP32" if precond == "AMG" else "FP64 throughout")}
+            "precision": ("FP64, the pressure preconditioner FP32" if precond == "AMG" else "FP64 throughout"),
+            "parallelism": "one case per GPU (replicas); the reference arm on one host core",
+            "reference_arm": REFERENCE_ARM}
 
 
 KERNEL_NAMES = {
@@ -71,28 +84,34 @@ MEASURED_TRAFFIC = {"bi_spmv2": 334e6}
 
 
 def kernel_bytes(N, F, s=8, i=4):
-    """Algorithmic bytes of one launch of each solver kernel: every array
-    counted once per read and once per write, gathers as one N-stream.
-    The three momentum components share one matrix read."""
+    """Algorithmic bytes of one launch of each solver kernel as (shared,
+    per component): every array counted once per read and once per write,
+    gathers as one N-stream; the three momentum components share one matrix
+    read and D^-1.  k_bi_p and k_bi_x skip a converged component's rows, the
+    two SpMVs always carry all three."""
     spmv_sym = 3 * s * N + s * F + 2 * i * F       # x in, y out, diag + one coefficient per face, indices
     mat3 = s * N + 2 * s * F + 2 * i * F           # diag + both coefficients + indices, shared by 3 components
-    return {"cg_spmv": spmv_sym, "cg_update": 7 * s * N, "cg_p": 4 * s * N,
-            # r, p, v, invD in; p, z out
-            "bi_p": 16 * s * N,
-            # z in (gathered), v out, r0 in
-            "bi_spmv1": 9 * s * N + mat3,
-            # r, v, invD in (gathered); t out
-            "bi_spmv2": 10 * s * N + mat3,
-            # x, z, r, v, t, r0, invD in; x, r out
-            "bi_x": 25 * s * N,
-            "dic_apply": 3 * s * N + 2 * (s * F + 2 * i * F)}
+    return {"cg_spmv": (spmv_sym, 0), "cg_update": (7 * s * N, 0), "cg_p": (4 * s * N, 0),
+            # invD in; per component r, p, v in, p, z out
+            "bi_p": (s * N, 5 * s * N),
+            # matrix; per component z in (gathered), v out, r0 in
+            "bi_spmv1": (mat3, 3 * s * N),
+            # matrix, invD (gathered); per component r, v in (gathered), t out
+            "bi_spmv2": (mat3 + s * N, 3 * s * N),
+            # invD; per component x, z, r, v, t, r0 in, x, r out
+            "bi_x": (s * N, 8 * s * N),
+            "dic_apply": (3 * s * N + 2 * (s * F + 2 * i * F), 0)}
 
 
-def simple_step_bytes(N, F, Fb, n_orth, it_u, it_p, precond, s=8, i=4):
+SKIPS_DONE = ("bi_p", "bi_x")
+
+
+def simple_step_bytes(N, F, Fb, n_orth, it_p, precond, solver_bytes, s=8, i=4):
     """Algorithmic bytes of one SIMPLE outer iteration: the fixed face and
-    cell passes plus the inner solves, per component-iteration of BiCGStab
-    (2 SpMVs with their own matrix read + 20 vector streams) and per PCG
-    iteration (SpMV + 11 streams; DIC adds both triangular sweeps)."""
+    cell passes (gradients, correctors, assemblies, fluxes, updates) plus
+    `solver_bytes`, the solver kernels' own per-launch bytes times their
+    launches; with the AMG pressure (whose kernels are not event-timed) its
+    flexible-CG iterations are added at the model's per-iteration bytes."""
     Ft = F + Fb
     grad_plain = Ft * (2 * i + 4 * s) + 5 * s * N
     grad_corr = grad_plain + 2 * (Ft * (2 * i + 7 * s) + 8 * s * N)
@@ -104,20 +123,15 @@ def simple_step_bytes(N, F, Fb, n_orth, it_u, it_p, precond, s=8, i=4):
              + Ft * (2 * i + 9 * s) + 4 * s * N          # correctFluxes
              + 21 * s * N                                # cell updates
              + Ft * (i + s) + s * N)                     # divPhi
-    spmv_sym = 3 * s * N + s * F + 2 * i * F
-    spmv_asym1 = 3 * s * N + 2 * s * F + 2 * i * F
-    per_u = 2 * spmv_asym1 + 20 * s * N
-    per_p = spmv_sym + 11 * s * N
-    if precond == "DIC":
-        per_p += 2 * (s * F + 2 * i * F) + 3 * s * N
-    elif precond == "AMG":
+    extra = 0
+    if precond == "AMG":
         # flexible CG: FP64 SpMV + 9 vector streams, and the V-cycle: at the
         # finest level two FP32 SELL passes (value + column per entry, N + 2F
         # entries) and 12 four-byte vector streams; the coarser levels add
         # about 30% (their rows are 1/7 as many but longer)
         fine = 2 * (N + 2 * F) * 8 + 12 * 4 * N
-        per_p = spmv_sym + 9 * s * N + 1.3 * fine
-    return fixed + it_u * per_u + it_p * per_p
+        extra = it_p * (3 * s * N + s * F + 2 * i * F + 9 * s * N + 1.3 * fine)
+    return fixed + solver_bytes + extra
 
 
 def make_case(n, device, precond="Jacobi"):
@@ -255,9 +269,13 @@ def pinned_core():
         return None
 
 
-def run_reference_cpu(n, points, timeout=3600):
-    """One SIMPLE outer iteration of the reference's own build on this host,
-    pinned to one core."""
+def run_reference_cpu(n, points, timeout=3600, fields=False):
+    """One SIMPLE outer iteration from rest of the n^3 cavity by the
+    reference's own build (oracle/_ref/cf_ref_driver, its sources compiled
+    with g++ -O3) on this host, pinned to one core (the reference is serial).
+    The reference has no pressure reference cell, so it solves its singular
+    Neumann pressure system with its Jacobi-PCG.  Returns (seconds, kind,
+    what, (U, p, phi) or None)."""
     drv = os.path.join(ROOT, "oracle", "_ref", "cf_ref_driver")
     with tempfile.TemporaryDirectory() as td:
         cp = os.path.join(td, "case.dict")
@@ -271,7 +289,11 @@ def run_reference_cpu(n, points, timeout=3600):
             if r.returncode != 0:
                 raise RuntimeError(r.stderr)
             res = open(os.path.join(td, "result.txt")).read().split()
-            return float(res[4]), "reference", "oracle/_ref/cf_ref_driver (the reference's sources, g++ -O3)"
+            out = None
+            if fields:
+                out = (np.fromfile(os.path.join(td, "U.f64")).reshape(-1, 3), np.fromfile(os.path.join(td, "p.f64")),
+                       np.fromfile(os.path.join(td, "phi.f64")))
+            return float(res[4]), "reference", "oracle/_ref/cf_ref_driver (the reference's sources, g++ -O3)", out
         # the C restatement of the same algorithm, when the reference was not built
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import _oracle as O
@@ -281,8 +303,8 @@ def run_reference_cpu(n, points, timeout=3600):
                       p_type=["zeroGradient"] * 6, p_value=[0] * 6, nu=NU, max_iterations=1, linear_tol=1e-8,
                       non_orth=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02)
         t0 = time.perf_counter()
-        case.run()
-        return time.perf_counter() - t0, "port", "oracle/cfo.c (C restatement)"
+        U, p, phi, _ = case.run()
+        return time.perf_counter() - t0, "port", "oracle/cfo.c (C restatement)", ((U, p, phi) if fields else None)
 
 
 def cpu_info():
@@ -301,29 +323,21 @@ def cpu_info():
 
 
 def main_reference(args, world, rank, dist):
-    """The reference's CPU SIMPLE on the same workload: one outer iteration of
-    the 128^3 case from rest per step, single thread (the reference is serial)."""
+    """The reference arm: the reference's CPU SIMPLE on the workload's mesh
+    (built here in numpy, without the product library) -- one outer
+    iteration from rest, single thread (the reference is serial)."""
     if rank != 0:
         return
     n = args.cells
-    import chuanflow_b200 as cf
-    mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (n, n, n), {s: (nm, "wall") for s, nm in zip(SIDES, NAMES)})
-    mesh.jitter_interior(JITTER, SEED)
-    pts = mesh.addressing()["points"]
-    del mesh
     steps = 1
-    secs, kind, what = run_reference_cpu(n, pts)
+    secs, kind, what, _ = run_reference_cpu(n, cavity_points(n))
     v = n ** 3 * steps / secs
     out = {"metric": METRIC, "impl": "reference", "value": v, "unit": "cell-iter/s", "n_gpus": args.gpus,
            "steps": steps, "warmup": 0, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           # the same config object as the B200 line; the reference's own solver choice is in the sample
-           "config": dict(workload_config(n, args.p_precond), parallelism="reference CPU, one core"),
+           "config": workload_config(n, args.p_precond),
            "cpu_baseline": {"value": v, "unit": "cell-iter/s", "cores": 1, "kind": kind,
-                            "sample": f"one SIMPLE outer iteration of the {n}^3 case from rest (a step of the "
-                                      f"timed loop); the reference has no pressure reference cell, so its "
-                                      f"pressure solve runs the unpinned system with its only PCG, Jacobi (it has "
-                                      f"no DIC); {what}; {cpu_info()}"},
+                            "sample": f"one SIMPLE outer iteration of the {n}^3 case from rest; {what}; {cpu_info()}"},
            "e2e": {"value": v, "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -611,7 +625,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--cells", type=int, default=CELLS)
-    ap.add_argument("--cpu-sample-cells", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--p-precond", default="AMG", choices=["Jacobi", "DIC", "AMG"])
     ap.add_argument("--no-variant", action="store_true",
@@ -653,7 +666,49 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
+    rc = main_simple(args, world, rank, local, dist)
+    if dist is not None:
+        dist.destroy_process_group()
+    sys.exit(rc)
 
+
+class Steps:
+    """K outer iterations with their device time, launches, inner counts and
+    the divergence test of simpleSolver.cpp:360-364 (non-finite continuity,
+    pressure step or fields), which SimpleResult.diverged carries."""
+
+    def __init__(self):
+        self.ms, self.launches, self.u, self.p, self.diverged, self.cont = 0.0, 0, 0, 0, 0, []
+
+    def run(self, case, ctl, k):
+        for _ in range(k):
+            r = case.solve(ctl)
+            ms, nl = case.last_timing()
+            self.ms += ms[7]
+            self.launches += nl
+            self.u += r.u_inner_iterations
+            self.p += r.p_inner_iterations
+            self.diverged += int(r.diverged or not np.isfinite(r.final_continuity_error))
+            self.cont.append(r.final_continuity_error)
+        return self
+
+
+def rel_l2(a, b):
+    d = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / d) if d > 0 else float(np.linalg.norm(a - b))
+
+
+def field_errors(U, p, phi, U0, p0, phi0, mean_free=False):
+    """Relative L2 errors per field (p mean-removed when no cell pins it)."""
+    if mean_free:
+        p, p0 = p - p.mean(), p0 - p0.mean()
+    return {"U": rel_l2(U, U0), "p": rel_l2(p, p0), "phi": rel_l2(phi, phi0)}
+
+
+def main_simple(args, world, rank, local, dist):
+    """The headline: K SIMPLE outer iterations of the 128^3 cavity on
+    device-resident fields after W warm-up iterations.  Every leg counts
+    its diverged iterations; a run with any is reported and exits 1."""
     n = args.cells
     mesh, case, ctl = make_case(n, local, args.p_precond)
     ncell = mesh.n_cells
@@ -672,29 +727,22 @@ def main():
         print(json.dumps({"profile": workload_config(n, args.p_precond)["workload"], "steps": args.steps,
                           "warm": args.profile_warm, "u_inner": r.u_inner_iterations,
                           "p_inner": r.p_inner_iterations}))
-        return
-    for _ in range(max(3, args.warmup)):
-        case.solve(ctl)
-    # the state every leg starts from: the timed, end-to-end and kernel-timing
-    # legs all run the same K outer iterations from it
+        return 0
+    W = max(3, args.warmup)
+    warm = Steps().run(case, ctl, W)
+    # the state every leg starts from: the timed, end-to-end, kernel-timing
+    # and comparison legs all run the same K outer iterations from it
     U0, p0, phi0 = case.download()
+
     # ---- timed region: K outer iterations on device-resident fields ----
     barrier(dist)
-    dev_ms = 0.0
-    launches = 0
-    u_inner = p_inner = 0
     with Clocks(local) as clk:
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            r = case.solve(ctl)
-            ms, nl = case.last_timing()
-            dev_ms += ms[7]
-            launches += nl
-            u_inner += r.u_inner_iterations
-            p_inner += r.p_inner_iterations
+        timed = Steps().run(case, ctl, args.steps)
         wall = time.perf_counter() - t0
     barrier(dist)
-    t_max = allreduce_max(dist, dev_ms / 1e3)
+    U1, p1, phi1 = case.download()
+    t_max = allreduce_max(dist, timed.ms / 1e3)
     value = world * ncell * args.steps / t_max
 
     # ---- end to end through the public API with host buffers: the same K
@@ -707,22 +755,25 @@ def main():
         pin = np.ascontiguousarray
     U, p, phi = pin(U0), pin(p0), pin(phi0)
     h2d = (U.nbytes + p.nbytes + phi.nbytes)
-    e2e_steps = args.steps
+    e2e_div = 0
     barrier(dist)
     t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         case.upload(U, p, phi)
-        case.solve(ctl)
+        r = case.solve(ctl)
         case.download(U, p, phi)
+        e2e_div += int(r.diverged)
     e2e_wall = allreduce_max(dist, time.perf_counter() - t0)
-    e2e = world * ncell * e2e_steps / e2e_wall
+    e2e = world * ncell * args.steps / e2e_wall
+    e2e_same = bool(np.array_equal(U, U1) and np.array_equal(p, p1) and np.array_equal(phi, phi1))
 
     # ---- per-kernel event timing (outside the timed region: the events
     # keep the solver chunks out of CUDA graphs) over the first iteration ----
     case.upload(U0, p0, phi0)
     case.kernel_timing(True)
-    case.solve(ctl)
+    ktimed = Steps().run(case, ctl, 1)
     kstats = case.kernel_stats()
+    kcomp = case.kernel_components()
     case.kernel_timing(False)
 
     # ---- rooflines: every solver kernel, the dominant one, and the whole step ----
@@ -735,11 +786,21 @@ def main():
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     alg = kernel_bytes(ncell, mesh.n_internal_faces)
     kernels = {}
+    solver_bytes = 0.0
     for k, (cnt, tot) in kstats.items():
         if cnt:
             us = tot / cnt * 1e3
-            kernels[k] = {"launches": cnt, "total_ms": tot, "avg_us": us, "alg_bytes": alg[k],
-                          "achieved_gbs": alg[k] / (us * 1e-6) / 1e9}
+            shared, per = alg[k]
+            comps = kcomp[k] / cnt if k in SKIPS_DONE else (3 if k.startswith("bi_") else 0)
+            b = shared + per * comps
+            kernels[k] = {"launches": cnt, "total_ms": tot, "avg_us": us, "alg_bytes": b,
+                          "components_per_launch": comps if k.startswith("bi_") else None,
+                          "achieved_gbs": b / (us * 1e-6) / 1e9}
+            # scaled from the kernel-timing iteration to the timed region's
+            # mean inner counts
+            scale = ((timed.u / args.steps) / max(1, ktimed.u) if k.startswith("bi_")
+                     else (timed.p / args.steps) / max(1, ktimed.p))
+            solver_bytes += cnt * b * scale
     top = max(kernels, key=lambda k: kernels[k]["total_ms"])
     kt = kernels[top]
     # DRAM bytes per launch from one ncu capture of this workload (128^3,
@@ -751,33 +812,34 @@ def main():
             "avg_launch_us": kt["avg_us"], "timing": "CUDA events around each launch over one outer iteration "
                                                      "from the timed region's start state",
             "kernels": kernels}
-    step_bytes = simple_step_bytes(ncell, mesh.n_internal_faces, mesh.n_boundary_faces, 1, u_inner / args.steps,
-                                   p_inner / args.steps, args.p_precond)
+    step_bytes = simple_step_bytes(ncell, mesh.n_internal_faces, mesh.n_boundary_faces, 1, timed.p / args.steps,
+                                   args.p_precond, solver_bytes)
     step_s = t_max / args.steps
     simple_roof = {"bytes_per_step": step_bytes, "achieved_gbs": step_bytes / step_s / 1e9,
                    "frac": step_bytes / step_s / 1e9 / peak, "peak": peak,
-                   "model": "per-kernel algorithmic bytes summed over the outer iteration with the measured inner "
-                            "iteration counts (BiCGStab 352 B/cell per component-iteration, PCG 160, DIC-PCG 280, "
-                            "AMG flexible CG about 350 B/cell per iteration at hex face counts) / device time per step; "
-                            "the per-component BiCGStab figure counts the matrix and 20 vector streams for each "
-                            "component, while the fused kernels read the shared matrix once for all three and form "
-                            "s^ on chip, so this whole-step figure can exceed 1; the fused kernels' own algorithmic "
-                            "bytes and rates are in roofline.kernels"}
+                   "model": "this build's per-kernel algorithmic bytes (roofline.kernels) per solver iteration times "
+                            "the timed region's inner iteration counts, plus the fixed face and cell passes of an "
+                            "outer iteration, over the device time per step"}
 
     out = {"metric": METRIC, "value": value, "unit": "cell-iter/s", "n_gpus": world, "steps": args.steps,
-           "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
+           "warmup": W, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": dict(workload_config(n, args.p_precond), parallelism=f"replicas x{world}"),
+           "config": workload_config(n, args.p_precond),
            "e2e": {"value": e2e, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
-                   "steps": e2e_steps},
-           "gpu_launches": launches, "roofline": roof, "simple_roofline": simple_roof, "clocks": clk.summary(),
-           "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": u_inner / args.steps,
-                                         "pressure_pcg": p_inner / args.steps},
+                   "steps": args.steps, "same_fields_as_timed": e2e_same},
+           "gpu_launches": timed.launches, "roofline": roof, "simple_roofline": simple_roof, "clocks": clk.summary(),
+           "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": timed.u / args.steps,
+                                         "pressure": timed.p / args.steps},
+           "continuity": {"first": timed.cont[0], "last": timed.cont[-1], "max": max(timed.cont)},
+           "diverged_steps": {"warmup": warm.diverged, "timed": timed.diverged, "e2e": e2e_div},
            "wall_s_timed": wall}
-    # the same K outer iterations from the same start state with the other
-    # FP64-tolerance pressure solver (FP64 multicolour DIC-PCG, or the AMG
-    # flexible CG when DIC is the headline), after one untimed iteration that
-    # sets it up
+    diverged = warm.diverged + timed.diverged + e2e_div
+
+    # ---- the same K outer iterations from the same start state with the
+    # other FP64-tolerance pressure solver, after one untimed iteration that
+    # sets it up; with FP64 DIC-PCG (FP64 throughout) as the other solver,
+    # its fields are the FP64 solve the headline's fields are measured
+    # against ----
     if not args.no_variant:
         other = "DIC" if args.p_precond == "AMG" else "AMG"
         c2 = dataclasses.replace(ctl, p_preconditioner=other)
@@ -785,34 +847,51 @@ def main():
         case.solve(c2)
         case.upload(U0, p0, phi0)
         barrier(dist)
-        v_ms, v_u, v_p = 0.0, 0, 0
-        for _ in range(args.steps):
-            r = case.solve(c2)
-            v_ms += case.last_timing()[0][7]
-            v_u += r.u_inner_iterations
-            v_p += r.p_inner_iterations
+        var = Steps().run(case, c2, args.steps)
         barrier(dist)
-        v_t = allreduce_max(dist, v_ms / 1e3)
+        U2, p2, phi2 = case.download()
+        v_t = allreduce_max(dist, var.ms / 1e3)
         out["variant"] = {"pressure": workload_config(n, other)["workload"].split("pressure ")[1],
                           "value": world * ncell * args.steps / v_t, "ms_per_step": v_t * 1e3 / args.steps,
-                          "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": v_u / args.steps,
-                                                        "pressure": v_p / args.steps},
+                          "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": var.u / args.steps,
+                                                        "pressure": var.p / args.steps},
+                          "continuity": {"first": var.cont[0], "last": var.cont[-1]},
+                          "diverged_steps": var.diverged,
                           "note": "same start state and steps as the headline, timed the same way"}
+        diverged += var.diverged
+        fp64 = (U2, p2, phi2) if other == "DIC" else (U1, p1, phi1)
+        test = (U1, p1, phi1) if other == "DIC" else (U2, p2, phi2)
+        out["field_error"] = dict(field_errors(*test, *fp64),
+                                  against="FP64 DIC-PCG pressure (FP64 throughout), the same K iterations from the same "
+                                          "start state; relative L2")
+
+    # ---- the reference's own work on the GPU: its first outer iteration
+    # from rest exactly as it runs it (no pressure reference cell, Jacobi-
+    # PCG), timed and compared with the reference's CPU run of that
+    # iteration (the cpu_baseline leg) ----
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        m2 = args.cpu_sample_cells
-        import chuanflow_b200 as cf
-        sm = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (m2, m2, m2), {s_: (nm, "wall") for s_, nm in zip(SIDES, NAMES)})
-        sm.jitter_interior(JITTER, SEED)
-        secs, kind, what = run_reference_cpu(m2, sm.addressing()["points"])
-        out["cpu_baseline"] = {"value": m2 ** 3 / secs, "unit": "cell-iter/s", "cores": 1, "kind": kind,
-                               "sample": f"one SIMPLE outer iteration of the same case family on a {m2}^3 mesh "
-                                         f"({secs:.1f} s; the full {n}^3 iteration takes minutes on one core); "
-                                         f"unpinned pressure (the reference has no reference cell); {what}; "
-                                         f"{cpu_info()}"}
+        case.upload(np.zeros((ncell, 3)), np.zeros(ncell), np.zeros(mesh.n_faces))
+        case.init_flux()
+        rc = dataclasses.replace(ctl, p_preconditioner="Jacobi", p_ref_cell=-1)
+        same = Steps().run(case, rc, 1)
+        Ug, pg, phig = case.download()
+        secs, kind, what, ref_fields = run_reference_cpu(n, mesh.addressing()["points"], fields=True)
+        out["cpu_baseline"] = {"value": ncell / secs, "unit": "cell-iter/s", "cores": 1, "kind": kind,
+                               "sample": f"one SIMPLE outer iteration of the same {n}^3 mesh and settings from rest "
+                                         f"({secs:.1f} s), as the reference runs it: no pressure reference cell, "
+                                         f"Jacobi-PCG; {what}; {cpu_info()}"}
+        out["reference_step_same_work"] = {
+            "what": "the reference's first outer iteration from rest (no reference cell, Jacobi-PCG), on this GPU "
+                    "and by the reference on one core",
+            "gpu_ms": same.ms, "cpu_ms": secs * 1e3, "speedup": secs * 1e3 / same.ms,
+            "inner_iterations_gpu": {"momentum": same.u, "pressure": same.p},
+            "field_error_vs_reference": (field_errors(Ug, pg, phig, *ref_fields, mean_free=True)
+                                         if ref_fields else None),
+            "diverged": same.diverged}
     if rank == 0:
+        out["valid"] = diverged == 0
         print(json.dumps(out), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    return 1 if diverged else 0
 
 
 if __name__ == "__main__":

@@ -358,6 +358,9 @@ class SolverReport:
 CELL_ORDER = {None: -1, "identity": 0, "colour": 1, "rcm": 2, "rcm-colour": 3}
 
 
+KERNEL_SLOTS = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_spmv2", "bi_x", "dic_apply")
+
+
 class SimpleCase:
     """U, p, phi and their boundary conditions on one device."""
 
@@ -441,8 +444,14 @@ class SimpleCase:
     def kernel_stats(self):
         out = np.zeros(16)
         _check(lib().cfg_kernel_stats(self._h, _dp(out)))
-        names = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_spmv2", "bi_x", "dic_apply")
-        return {n: (int(out[2 * i]), float(out[2 * i + 1])) for i, n in enumerate(names)}
+        return {n: (int(out[2 * i]), float(out[2 * i + 1])) for i, n in enumerate(KERNEL_SLOTS)}
+
+    def kernel_components(self):
+        """Per solver kernel, its timed launches weighted by the vector
+        components each still iterated on."""
+        out = np.zeros(8)
+        _check(lib().cfg_kernel_components(self._h, _dp(out)))
+        return {n: float(out[i]) for i, n in enumerate(KERNEL_SLOTS)}
 
     # ---- the pressure-Poisson system on its own ----
     def poisson_setup(self, ref_cell=-1):
@@ -774,7 +783,7 @@ SimpleCase.detail_loss = _detail_loss
 class Batch:
     """Detail-block cases evaluated together, one stream each."""
 
-    CANDIDATES = [(1, 0), (8, 1), (16, 1), (16, -1), (32, -1), (64, -1)]
+    CANDIDATES = [(1, 0), (8, 1), (16, 1), (16, -1), (32, -1), (64, -1), (0, 1), (0, 2), (0, -1)]
 
     def __init__(self, cases):
         self.cases = list(cases)

@@ -432,6 +432,14 @@ int cfg_kernel_stats(const cfg_ctx* ctx, double out[16])
     });
 }
 
+int cfg_kernel_components(const cfg_ctx* ctx, double out[8])
+{
+    return guard([&] {
+        need(ctx && out, "cfg_kernel_components: null argument");
+        for (int k = 0; k < cfg::Ctx::KS_COUNT; ++k) out[k] = ctx->c->kcomp[k];
+    });
+}
+
 int cfg_sparse_solve(const cfg_ctx* ctx, int32_t device, int64_t n, const int64_t* rs, const int64_t* cols,
                      const double* vals, const double* b, double* x, double tol, int32_t maxIter, int32_t method,
                      cfg_solver_report* rep)
@@ -856,7 +864,7 @@ void cfg_batch_destroy(cfg_batch* batch) { delete batch; }
 int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t rowBlocks)
 {
     return guard([&] {
-        need(batch && workers > 0 && rowBlocks >= -1, "cfg_batch_set_schedule: bad argument");
+        need(batch && workers >= 0 && rowBlocks >= -1, "cfg_batch_set_schedule: bad argument");
         batch->workers = workers;
         batch->rowBlocks = rowBlocks;
     });
@@ -892,20 +900,41 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
 {
     return guard([&] {
         need(batch && q && controls && workers && rowBlocks, "cfg_batch_autotune: null argument");
-        static const int cand[][2] = {{1, 0}, {8, 1}, {16, 1}, {16, -1}, {32, -1}, {64, -1}};
+        // {host workers, solver blocks per SM}; 0 workers: the pass as one
+        // captured graph (Jacobi / DIC pressure, one outer iteration)
+        static const int cand[][2] = {{1, 0}, {8, 1}, {16, 1}, {16, -1}, {32, -1}, {64, -1},
+                                      {0, 1}, {0, 2}, {0, -1}};
+        constexpr int nCand = sizeof(cand) / sizeof(cand[0]);
+        bool graphable = true;
+        for (size_t i = 0; i < batch->blocks.size(); ++i)
+            graphable = graphable && controls[i].max_iterations == 1 && controls[i].p_precond != CFG_PRECOND_AMG &&
+                        controls[i].p_precond != CFG_PRECOND_MPNN &&
+                        batch->blocks[i]->turbulenceModelName() != "gammaTransition";
         std::vector<cfg_detail_measure> m(batch->blocks.size());
         double best = 0;
         int bi = 0;
         // every candidate runs the same pass from the same saved fields; the
         // chosen one then runs it for real
         for (cfg::Ctx* c : batch->blocks) c->saveState();
-        for (int k = 0; k < 6; ++k)
+        for (int k = 0; k < nCand; ++k)
         {
+            if (cand[k][0] == 0 && !graphable)
+            {
+                if (times) times[k] = -1.0;
+                continue;
+            }
             for (cfg::Ctx* c : batch->blocks) c->restoreState();
             batch->workers = cand[k][0];
             batch->rowBlocks = cand[k][1];
             double ms = 0;
             cfg::batchPass(*batch, q, controls, m.data(), &ms);
+            if (cand[k][0] == 0)
+            {
+                // the first graph pass of a schedule includes its capture:
+                // time a replay of the same pass
+                for (cfg::Ctx* c : batch->blocks) c->restoreState();
+                cfg::batchPass(*batch, q, controls, m.data(), &ms);
+            }
             if (times) times[k] = ms;
             if (k == 0 || ms < best)
             {

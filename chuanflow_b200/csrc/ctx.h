@@ -60,6 +60,20 @@ public:
     void download(double* U, double* p, double* phi);
     void initFlux(const double* u0);
     void iterate(const cfg_simple_controls& ctl, cfg_simple_result& res);
+    /// The pieces of iterate: host set-up, one outer iteration enqueued
+    /// (capturable with device loops on), and the host's reading of its
+    /// scalars (1: stop).
+    void prepareIterate(const cfg_simple_controls& ctl);
+    void enqueueOuter(const cfg_simple_controls& ctl, int64_t& uInner, int64_t& pInner);
+    int finishOuter(const cfg_simple_controls& ctl, int iter, double& contLag1, double& contLag2,
+                    cfg_simple_result& res);
+    /// Device-side solver loops (conditional while-nodes) instead of host
+    /// polling, for enqueueOuter under stream capture.
+    void setDeviceLoops(bool on) { devLoop_ = on; }
+    cudaStream_t stream() const { return stream_; }
+    /// the inner iteration counts a device-loop iteration left in the
+    /// scalars: momentum, pressure, RANS model
+    void deviceInner(int64_t& u, int64_t& p, int64_t& t) const;
     /// one transient PISO step (pisoSolver.cpp)
     void pisoStep(const cfg_piso_controls& ctl, cfg_piso_result& res);
 
@@ -67,6 +81,11 @@ public:
     /// patches, cross-sections and the inlet profile, then lossAt(q).
     void detailSetup(const std::string& shape, double rho);
     void detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out);
+    /// lossAt in pieces, for a pass captured as one graph: host set-up for
+    /// rate q, the measure enqueued, the drop from the measured sums
+    void detailPrepare(double q, const cfg_simple_controls& ctl);
+    void detailEnqueueMeasure();
+    void detailFinish(double q, const cfg_simple_result& res, double deviceMs, cfg_detail_measure& out);
     void detailTurbulence(const std::string& model, double intensity, double lengthScale, double relaxation,
                           double nu);
     /// Solver grid of at most k blocks per SM (0: the context's own).
@@ -133,6 +152,10 @@ public:
         KS_COUNT
     };
     double kstat[KS_COUNT][2] = {};
+    /// per slot, the launches weighted by the components still iterating
+    /// (the fused BiCGStab kernels skip converged components; 1 per launch
+    /// for the single-vector kernels)
+    double kcomp[KS_COUNT] = {};
 
     const Mesh& mesh() const { return mesh_; }
 
@@ -156,6 +179,15 @@ private:
     int linUpwindGrad(const BcTab& ub, int gradScheme);
     template <class F>
     void launchChunk(const std::string& key, int n, F&& body);
+    /// While stream_ is being captured: a while-node whose body is what
+    /// `body` enqueues, repeated until the solver state is done (at most
+    /// maxBodies times).
+    template <class F>
+    void captureWhile(int maxBodies, F&& body);
+    bool devLoop_ = false;
+    double* tally_ = nullptr;  // {iterations, unconverged} of device-loop solves
+    cudaStream_t bodyStream_ = nullptr;
+    int* loopCount_ = nullptr;
     void dicSetup(const double* vals, const double* diag);
     void dicApply(const double* r, double* z);
     void runDICCG(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
@@ -306,7 +338,7 @@ private:
     static constexpr int kEvPerIter = 6;  // events per solver iteration of a chunk (kernels + 1)
     std::vector<cudaEvent_t> kev_;
     void tmark(int k, int j);
-    void harvest(int ran, const int* slots, int nSlots);
+    void harvest(int ran, const int* slots, int nSlots, int active = 1);
 };
 
 }  // namespace cfg
@@ -340,11 +372,21 @@ struct cfg_ctx
     std::unique_ptr<cfg::Ctx> c;
 };
 
+namespace cfg
+{
+struct BatchGraph;
+struct BatchGraphDeleter
+{
+    void operator()(BatchGraph* g) const;
+};
+}  // namespace cfg
+
 struct cfg_batch
 {
     std::vector<cfg::Ctx*> blocks;
-    int workers = 1;
+    int workers = 1;    // 0: the whole pass as one captured CUDA graph
     int rowBlocks = 0;  // 0: each block's own solver grid
+    std::unique_ptr<cfg::BatchGraph, cfg::BatchGraphDeleter> graph;
 };
 
 namespace cfg

@@ -272,14 +272,17 @@ void Ctx::detailSetup(const std::string& shape, double rho)
     detail_.reset(d.release());
 }
 
-void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out)
+/// lossAt's host side before the solve (coupledNetwork.cpp:1080-1113): the
+/// block's boundary conditions for rate q (applyBoundary, :878-926), the
+/// boundary flux, the RANS model on the first call, and the outer
+/// iteration's host set-up.
+void Ctx::detailPrepare(double q, const cfg_simple_controls& ctl)
 {
     if (!detail_) fail(CFG_EINVAL, "cfg_detail_loss: call cfg_detail_setup first");
     if (!(q > 0)) fail(CFG_EINVAL, "detailBlock: asked for the drop of a detailed region at a non-positive rate");
     CFG_CUDA(cudaSetDevice(device_));
     DetailState& d = *detail_;
     const Mesh& M = mesh_;
-    // applyBoundary (coupledNetwork.cpp:878-926)
     double inletU[3] = {0, 0, 0};
     inletU[d.axis] = d.flowSign * q / d.inletArea;
     const double zero[3] = {0, 0, 0};
@@ -319,9 +322,15 @@ void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measur
     initFlux(nullptr);  // phi.correctBoundaryFlux(U)
     if (!turb_ && d.turbModel != "laminar")
         turbulenceSetup(d.turbModel, d.turbIntensity, d.turbLength, d.turbRelax, d.turbNu);
-    cfg_simple_result res{};
-    iterate(ctl, res);
-    // measure (coupledNetwork.cpp:1154-1195)
+    prepareIterate(ctl);
+}
+
+/// The volume-weighted section pressures and the patch fluxes of measure
+/// (coupledNetwork.cpp:1154-1195), and their copy to the host, enqueued.
+void Ctx::detailEnqueueMeasure()
+{
+    DetailState& d = *detail_;
+    const Mesh& M = mesh_;
     const auto& pin = M.patches[static_cast<size_t>(d.inlet)];
     const auto& pout = M.patches[static_cast<size_t>(d.outlet)];
     k_detail_measure<<<4, TPB, 0, stream_>>>(d.dFirst, static_cast<int>(d.first.size()), d.dLast,
@@ -330,11 +339,17 @@ void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measur
                                              static_cast<int>(pout.size), dm_.V, p_, phi_, d.dOut);
     launchCheck("detail_measure");
     CFG_CUDA(cudaMemcpyAsync(d.hOut, d.dOut, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-    CFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+/// The drop from the measured sums and lossAt's own checks of it
+/// (coupledNetwork.cpp:1146-1151), once the device work is done.
+void Ctx::detailFinish(double q, const cfg_simple_result& res, double deviceMs, cfg_detail_measure& out)
+{
+    DetailState& d = *detail_;
     const double* h = d.hOut;
     const double p0 = h[1] > 0 ? h[0] / h[1] : 0.0, p1 = h[3] > 0 ? h[2] / h[3] : 0.0;
     out = cfg_detail_measure{};
-    out.cells = M.nCells;
+    out.cells = mesh_.nCells;
     out.sweeps = res.iterations;
     out.converged = res.converged;
     out.diverged = res.diverged;
@@ -344,12 +359,21 @@ void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measur
     out.flux_out = h[5];
     out.inlet_area = d.inletArea;
     out.plug_speed = q / d.inletArea;
-    out.device_ms = lastMs[7];
+    out.device_ms = deviceMs;
     out.u_inner_iterations = res.u_inner_iterations;
     out.p_inner_iterations = res.p_inner_iterations;
-    // lossAt's own checks of the measured drop (coupledNetwork.cpp:1146-1151)
     if (!std::isfinite(out.dp_pa)) out.status = CFG_ENUMERIC;
     else if (out.dp_pa <= 0) out.status = CFG_ENUMERIC;
+}
+
+void Ctx::detailLoss(double q, const cfg_simple_controls& ctl, cfg_detail_measure& out)
+{
+    detailPrepare(q, ctl);
+    cfg_simple_result res{};
+    iterate(ctl, res);
+    detailEnqueueMeasure();
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    detailFinish(q, res, lastMs[7], out);
 }
 
 void Ctx::detailTurbulence(const std::string& model, double intensity, double lengthScale, double relaxation,
@@ -441,12 +465,181 @@ void DetailDeleter::operator()(DetailState* d) const
     delete d;
 }
 
-/// One coupling pass: every block's lossAt at its own rate.  Blocks are
-/// taken largest first by `workers` host threads, each block on its own
-/// context stream, so up to `workers` blocks run on the GPU at once.
+/// The captured graph of a whole coupling pass (batch schedule with
+/// workers == 0): every block's outer iteration and measure as parallel
+/// branches, its solver loops as device-side while-nodes.
+struct BatchGraph
+{
+    std::string key;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t exec = nullptr;
+    ~BatchGraph()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (cudaEvent_t e : join) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (origin) cudaStreamDestroy(origin);
+    }
+};
+
+void BatchGraphDeleter::operator()(BatchGraph* g) const { delete g; }
+
+namespace
+{
+
+/// Runs fn(i) for i in [0, n) on up to `threads` host threads; the error
+/// of the lowest failing block is raised after all have run.
+template <class F>
+void forBlocks(int n, int threads, F&& fn)
+{
+    std::atomic<int> next{0};
+    std::vector<std::string> errs(static_cast<size_t>(n));
+    std::vector<int> codes(static_cast<size_t>(n), CFG_OK);
+    auto work = [&]() {
+        for (int i; (i = next.fetch_add(1)) < n;)
+        {
+            try
+            {
+                fn(i);
+            }
+            catch (const Error& e)
+            {
+                errs[static_cast<size_t>(i)] = e.what();
+                codes[static_cast<size_t>(i)] = e.code;
+            }
+            catch (const std::exception& e)
+            {
+                errs[static_cast<size_t>(i)] = e.what();
+                codes[static_cast<size_t>(i)] = CFG_EINVAL;
+            }
+        }
+    };
+    const int w = std::max(1, std::min(threads, n));
+    if (w == 1) work();
+    else
+    {
+        std::vector<std::thread> th;
+        for (int t = 0; t < w; ++t) th.emplace_back(work);
+        for (auto& t : th) t.join();
+    }
+    for (int i = 0; i < n; ++i)
+        if (codes[static_cast<size_t>(i)] != CFG_OK)
+            fail(codes[static_cast<size_t>(i)], "block " + std::to_string(i) + ": " + errs[static_cast<size_t>(i)]);
+}
+
+/// One coupling pass as a single CUDA-graph launch.  The host sets every
+/// block's boundary values for its rate (on host threads), launches the
+/// pass graph -- captured on the first pass of a schedule and set of
+/// controls, replayed after -- and reads each block's scalars and sums.
+void batchPassGraph(cfg_batch& b, const double* q, const cfg_simple_controls* ctl, cfg_detail_measure* out,
+                    double* wallMs)
+{
+    const int n = static_cast<int>(b.blocks.size());
+    for (cfg::Ctx* c : b.blocks)
+        c->setRowBlocks(b.rowBlocks >= 0 ? b.rowBlocks
+                                         : static_cast<int>(std::min<int64_t>(4, std::max<int64_t>(
+                                                                                  1, c->mesh().nCells / 32768))));
+    const auto t0 = std::chrono::steady_clock::now();
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    forBlocks(n, static_cast<int>(std::min(hw, 16u)),
+              [&](int i) { b.blocks[static_cast<size_t>(i)]->detailPrepare(q[i], ctl[i]); });
+    std::string key = std::to_string(b.rowBlocks);
+    for (int i = 0; i < n; ++i) key.append(reinterpret_cast<const char*>(&ctl[i]), sizeof(cfg_simple_controls));
+    if (!b.graph || b.graph->key != key)
+    {
+        b.graph.reset(new BatchGraph());
+        BatchGraph& g = *b.graph;
+        g.key = key;
+        CFG_CUDA(cudaStreamCreateWithFlags(&g.origin, cudaStreamNonBlocking));
+        CFG_CUDA(cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming));
+        g.join.resize(static_cast<size_t>(n));
+        for (auto& e : g.join) CFG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        // every block's own set-up work is finished before its branch is
+        // captured after it
+        for (cfg::Ctx* c : b.blocks) CFG_CUDA(cudaStreamSynchronize(c->stream()));
+        CFG_CUDA(cudaStreamBeginCapture(g.origin, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t graph = nullptr;
+        try
+        {
+            CFG_CUDA(cudaEventRecord(g.fork, g.origin));
+            for (int i = 0; i < n; ++i)
+            {
+                cfg::Ctx& c = *b.blocks[static_cast<size_t>(i)];
+                CFG_CUDA(cudaStreamWaitEvent(c.stream(), g.fork, 0));
+                c.setDeviceLoops(true);
+                int64_t u = 0, p = 0;
+                try
+                {
+                    c.enqueueOuter(ctl[i], u, p);
+                    c.detailEnqueueMeasure();
+                }
+                catch (...)
+                {
+                    c.setDeviceLoops(false);
+                    throw;
+                }
+                c.setDeviceLoops(false);
+                CFG_CUDA(cudaEventRecord(g.join[static_cast<size_t>(i)], c.stream()));
+                CFG_CUDA(cudaStreamWaitEvent(g.origin, g.join[static_cast<size_t>(i)], 0));
+            }
+        }
+        catch (...)
+        {
+            cudaStreamEndCapture(g.origin, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            b.graph.reset();
+            throw;
+        }
+        CFG_CUDA(cudaStreamEndCapture(g.origin, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess)
+        {
+            b.graph.reset();
+            fail(CFG_ECUDA, std::string("batch pass graph: cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        }
+    }
+    BatchGraph& g = *b.graph;
+    for (cfg::Ctx* c : b.blocks) CFG_CUDA(cudaStreamSynchronize(c->stream()));
+    CFG_CUDA(cudaGraphLaunch(g.exec, g.origin));
+    CFG_CUDA(cudaStreamSynchronize(g.origin));
+    const auto t1 = std::chrono::steady_clock::now();
+    const double ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (wallMs) *wallMs = ms;
+    for (int i = 0; i < n; ++i)
+    {
+        cfg::Ctx& c = *b.blocks[static_cast<size_t>(i)];
+        cfg_simple_result res{};
+        double lag1 = INFINITY, lag2 = INFINITY;
+        c.finishOuter(ctl[i], 1, lag1, lag2, res);
+        int64_t t = 0;
+        c.deviceInner(res.u_inner_iterations, res.p_inner_iterations, t);
+        c.detailFinish(q[i], res, ms, out[i]);
+    }
+}
+
+}  // namespace
+
+/// One coupling pass: every block's lossAt at its own rate.  With workers
+/// == 0 the pass is one CUDA-graph launch (batchPassGraph); otherwise
+/// blocks are taken largest first by `workers` host threads, each block on
+/// its own context stream, so up to `workers` blocks run on the GPU at once.
 void batchPass(cfg_batch& b, const double* q, const cfg_simple_controls* ctl, cfg_detail_measure* out,
                double* wallMs)
 {
+    if (b.workers == 0)
+    {
+        for (int i = 0; i < static_cast<int>(b.blocks.size()); ++i)
+            if (ctl[i].max_iterations != 1 || ctl[i].p_precond == CFG_PRECOND_AMG ||
+                ctl[i].p_precond == CFG_PRECOND_MPNN ||
+                b.blocks[static_cast<size_t>(i)]->turbulenceModelName() == "gammaTransition")
+                fail(CFG_EINVAL, "batch: the single-graph pass runs one outer iteration per block with Jacobi or DIC "
+                                 "pressure and no gammaTransition model");
+        batchPassGraph(b, q, ctl, out, wallMs);
+        return;
+    }
     const int n = static_cast<int>(b.blocks.size());
     std::vector<int> order(static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) order[i] = i;

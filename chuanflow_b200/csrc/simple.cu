@@ -29,6 +29,12 @@ enum Slot
     S_NONFINITE,
     S_NET,          // adjustPhi sums
     S_FREE,
+    S_UINNER,       // device-side loops: momentum inner iterations, unconverged solves
+    S_UUNCONV,
+    S_TINNER,       // device-side loops: RANS model inner iterations, unconverged solves
+    S_TUNCONV,
+    S_PINNER,       // device-side loops: pressure inner iterations, unconverged solves
+    S_PUNCONV,
     S_COUNT
 };
 
@@ -611,6 +617,7 @@ Ctx::~Ctx()
     for (int i = 0; i < 16; ++i) cudaEventDestroy(tm_.ev[i]);
     for (auto& e : kev_) cudaEventDestroy(e);
     for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
+    if (bodyStream_) cudaStreamDestroy(bodyStream_);
     if (ownStream_) cudaStreamDestroy(stream_);
 }
 
@@ -974,6 +981,8 @@ void Ctx::buildDevice()
     partials_ = alloc<double>(static_cast<size_t>(16) * std::max(std::max(std::max(G_, GF_), GS_), dicPartials_));
     st_ = alloc<SolveState>(1);
     scal_ = alloc<double>(S_COUNT);
+    loopCount_ = alloc<int>(1);
+    CFG_CUDA(cudaStreamCreateWithFlags(&bodyStream_, cudaStreamNonBlocking));
     CFG_CUDA(cudaMallocHost(&stHost_, sizeof(SolveState)));
     CFG_CUDA(cudaMallocHost(&scalHost_, sizeof(double) * S_COUNT));
     CFG_CUDA(cudaStreamSynchronize(stream_));
@@ -1319,6 +1328,53 @@ void Ctx::launchChunk(const std::string& key, int n, F&& body)
     CFG_CUDA(cudaGraphLaunch(it->second, stream_));
 }
 
+/// Appends to the graph being captured on stream_ a conditional while-node
+/// whose body holds what body() enqueues followed by k_loop_cond on the
+/// solver state st_: the device re-runs the body until the solve is done.
+/// The body is captured on bodyStream_ into the node's own graph.
+template <class F>
+void Ctx::captureWhile(int maxBodies, F&& body)
+{
+    CFG_CUDA(cudaMemsetAsync(loopCount_, 0, sizeof(int), stream_));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nDeps = 0;
+    CFG_CUDA(cudaStreamGetCaptureInfo(stream_, &cs, nullptr, &g, &deps, &nDeps));
+    if (cs != cudaStreamCaptureStatusActive) fail(CFG_EINVAL, "device loops need a stream under capture");
+    cudaGraphConditionalHandle h;
+    CFG_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CFG_CUDA(cudaGraphAddNode(&node, g, deps, nDeps, &np));
+    CFG_CUDA(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t bodyGraph = np.conditional.phGraph_out[0];
+    CFG_CUDA(cudaStreamBeginCaptureToGraph(bodyStream_, bodyGraph, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+    const cudaStream_t outer = stream_;
+    stream_ = bodyStream_;
+    try
+    {
+        body();
+        k_loop_cond<<<1, 32, 0, stream_>>>(h, st_, loopCount_, maxBodies);
+        launchCheck("loop_cond");
+    }
+    catch (...)
+    {
+        stream_ = outer;
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(bodyStream_, &junk);
+        throw;
+    }
+    stream_ = outer;
+    cudaGraph_t captured = nullptr;
+    CFG_CUDA(cudaStreamEndCapture(bodyStream_, &captured));
+}
+
 namespace
 {
 std::string ptrKey(const char* kind, std::initializer_list<const void*> ps, int extra = 0)
@@ -1345,6 +1401,28 @@ void Ctx::runCG(const double* vals, const double* diag, const double* b, double*
     init.nComp = 1;
     init.normType = normType;
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    if (devLoop_)
+    {
+        k_state_reset<<<1, 32, 0, stream_>>>(st_, tol, maxIter, 1, normType);
+        dispatchW(maxW_, [&](auto Wc) {
+            constexpr int W = decltype(Wc)::value;
+            k_cg_init<W><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
+            constexpr int CH = 8;
+            captureWhile((maxIter + CH - 1) / CH + 1, [&] {
+                for (int k = 0; k < CH; ++k)
+                {
+                    k_cg_spmv<W><<<GS_, TPB, 0, stream_>>>(A, vals, cp_, cAp_, partials_, st_);
+                    k_cg_update<double><<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cp_, cAp_, x, cr_, partials_, st_);
+                    k_cg_p<double><<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, cr_, cp_, st_);
+                }
+                launchCheck("cg_iter", 0);
+            });
+        });
+        if (tally_) k_state_tally<<<1, 32, 0, stream_>>>(st_, 1, tally_);
+        launchCheck("cg_tally");
+        *rep = cfg_solver_report{};
+        return;
+    }
     dispatchW(maxW_, [&](auto Wc) {
         constexpr int W = decltype(Wc)::value;
         k_cg_init<W><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cp_, partials_, st_);
@@ -1395,14 +1473,42 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     init.tol = tol;
     init.maxIter = maxIter;
     init.nComp = nComp;
-    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     const int n = dm_.nC;
+    if (devLoop_)
+    {
+        k_state_reset<<<1, 32, 0, stream_>>>(st_, tol, maxIter, nComp, 0);
+        auto dloop = [&](auto Wc, auto NCc) {
+            constexpr int W = decltype(Wc)::value;
+            constexpr int NC = decltype(NCc)::value;
+            k_bi_init<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, diag, bInvD_, b, x, br_, br0_, bp_, bv_, partials_, st_);
+            constexpr int CH = 4;
+            captureWhile((maxIter + CH - 1) / CH + 1, [&] {
+                for (int k = 0; k < CH; ++k)
+                {
+                    k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, bInvD_, br_, bp_, bv_, bz_, st_);
+                    k_bi_spmv1<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
+                    k_bi_spmv2<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, bInvD_, br_, bv_, bt_, partials_, st_);
+                    k_bi_x<NC><<<GS_, TPB, 0, stream_>>>(n, bInvD_, x, bz_, bv_, bt_, br_, br0_, partials_, st_);
+                }
+                launchCheck("bicg_iter", 0);
+            });
+        };
+        dispatchW(maxW_, [&](auto Wc) {
+            if (nComp == 3) dloop(Wc, std::integral_constant<int, 3>{});
+            else dloop(Wc, std::integral_constant<int, 1>{});
+        });
+        if (tally_) k_state_tally<<<1, 32, 0, stream_>>>(st_, nComp, tally_);
+        launchCheck("bicg_tally");
+        for (int q = 0; q < nComp; ++q) reps[q] = cfg_solver_report{};
+        return;
+    }
+    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     auto loop = [&](auto Wc, auto NCc) {
         constexpr int W = decltype(Wc)::value;
         constexpr int NC = decltype(NCc)::value;
         k_bi_init<W, NC><<<GS_, TPB, 0, stream_>>>(A, vals, diag, bInvD_, b, x, br_, br0_, bp_, bv_, partials_, st_);
         launchCheck("bicg_init");
-        int itBefore = 0, lastChunk = 0;
+        int itBefore = 0, lastChunk = 0, activeBefore = NC;
         auto itMax = [&] {
             int m = 0;
             for (int q = 0; q < NC; ++q) m = std::max(m, stHost_->it[q]);
@@ -1415,11 +1521,15 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
             if (lastChunk > 0)
             {
                 static const int slots[4] = {KS_BI_P, KS_BI_SPMV1, KS_BI_SPMV2, KS_BI_X};
-                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 4);
+                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 4, activeBefore);
             }
             itBefore = itMax();
+            activeBefore = 0;
+            for (int q = 0; q < NC; ++q) activeBefore += stHost_->done[q] ? 0 : 1;
             if (stHost_->allDone || launched >= maxIter) break;
-            const int m = std::min(chunk, maxIter - launched);
+            // timed launches go one iteration at a time, so each is charged
+            // with the components that were still iterating
+            const int m = ktime_ ? 1 : std::min(chunk, maxIter - launched);
             launchChunk(ptrKey("bicg", {vals, diag, x.c[0], x.c[1], x.c[2]}, W * 8 + NC), m, [&](int k) {
                 tmark(k, 0);
                 k_bi_p<NC><<<GS_, TPB, 0, stream_>>>(n, bInvD_, br_, bp_, bv_, bz_, st_);
@@ -1511,6 +1621,31 @@ void Ctx::dicCGT(const DDicT<T>& D, const T* vals, const T* diag, const T* b, T*
     init.maxIter = maxIter;
     init.nComp = 1;
     init.normType = normType;
+    if (devLoop_)
+    {
+        k_state_reset<<<1, 32, 0, stream_>>>(st_, tol, maxIter, 1, normType);
+        dispatchW(maxW_, [&](auto Wc) {
+            constexpr int W = decltype(Wc)::value;
+            k_cg_init<W, T><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, r, p, partials_, st_);
+            dicApplyT<T>(D, r, z);
+            k_cg_pz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, z, p, st_);
+            constexpr int CH = 8;
+            captureWhile((maxIter + CH - 1) / CH + 1, [&] {
+                for (int k = 0; k < CH; ++k)
+                {
+                    k_cg_spmv<W, T><<<GS_, TPB, 0, stream_>>>(A, vals, p, Ap, partials_, st_);
+                    k_cg_update_nz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, p, Ap, x, r, partials_, st_);
+                    dicApplyT<T>(D, r, z);
+                    k_cg_pz<T><<<GS_, TPB, 0, stream_>>>(dm_.nC, z, p, st_);
+                }
+                launchCheck("dic_cg_iter", 0);
+            });
+        });
+        if (tally_) k_state_tally<<<1, 32, 0, stream_>>>(st_, 1, tally_);
+        launchCheck("dic_cg_tally");
+        *rep = cfg_solver_report{};
+        return;
+    }
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     dispatchW(maxW_, [&](auto Wc) {
         constexpr int W = decltype(Wc)::value;
@@ -1607,6 +1742,7 @@ void Ctx::setKernelTiming(bool on)
     }
     ktime_ = on;
     for (auto& r : kstat) r[0] = r[1] = 0.0;
+    for (auto& c : kcomp) c = 0.0;
 }
 
 /// Event j of iteration k of the chunk being enqueued (kernel timing on).
@@ -1616,8 +1752,9 @@ void Ctx::tmark(int k, int j)
 }
 
 /// Adds the first `ran` iterations of the last timed chunk to kstat: the
-/// interval between events j and j+1 of an iteration is kernel slots[j].
-void Ctx::harvest(int ran, const int* slots, int nSlots)
+/// interval between events j and j+1 of an iteration is kernel slots[j];
+/// `active` components were iterating in each.
+void Ctx::harvest(int ran, const int* slots, int nSlots, int active)
 {
     if (!ktime_) return;
     for (int k = 0; k < ran; ++k)
@@ -1627,6 +1764,7 @@ void Ctx::harvest(int ran, const int* slots, int nSlots)
             CFG_CUDA(cudaEventElapsedTime(&ms, kev_[kEvPerIter * k + j], kev_[kEvPerIter * k + j + 1]));
             kstat[slots[j]][0] += 1;
             kstat[slots[j]][1] += ms;
+            kcomp[slots[j]] += active;
         }
 }
 
@@ -1907,14 +2045,26 @@ void Ctx::initFlux(const double* u0)
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
+/// The host side of an outer iteration's set-up: the boundary tables, the
+/// momentum boundary checks and the laminar face viscosity.
+void Ctx::prepareIterate(const cfg_simple_controls& ctl)
 {
     CFG_CUDA(cudaSetDevice(device_));
     refreshBc();
     checkMomentumBcs();
     if (!turb_) setNu(ctl.nu);  // with a RANS model the model's nu + nut is the diffusivity
-    std::memset(&res, 0, sizeof res);
-    lastTurbInner = 0;
+    if (ctl.p_ref_cell >= dm_.nC) fail(CFG_EINVAL, "p_ref_cell beyond the last cell");
+}
+
+/// Enqueues one SIMPLE outer iteration (simpleSolver.cpp:52-357) on stream_,
+/// ending with the copy of its scalars to scalHost_.  With devLoop_ the
+/// linear solvers iterate in device-side loops and nothing here waits for
+/// the device, so the whole iteration can be captured into a CUDA graph; the
+/// inner iteration counts then arrive in the S_*INNER slots.  Otherwise the
+/// solvers poll their state from the host and add their counts to `uInner`
+/// and `pInner`.
+void Ctx::enqueueOuter(const cfg_simple_controls& ctl, int64_t& uInner, int64_t& pInner)
+{
     const int nC = dm_.nC;
     const int gs = schemes_.grad;
     const double alpha = schemes_.div == CFG_DIV_BLEND ? schemes_.blend_coeff : (schemes_.div == CFG_DIV_LINEAR ? 1.0 : 0.0);
@@ -1922,93 +2072,119 @@ void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
     const BcTab hb{{hc_[0], hc_[1], hc_[2]}, {hk_[0], hk_[1], hk_[2]}};
     const BcTab pb{{pc_, pc_, pc_}, {pk_, pk_, pk_}};
     const bool doAdjust = needReference_ && nFreeUFaces_ > 0;
-    if (ctl.p_ref_cell >= nC) fail(CFG_EINVAL, "p_ref_cell beyond the last cell");
     const int refCell = deviceCell(ctl.p_ref_cell);
+    CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
+    tally_ = scal_ + S_TINNER;
+    if (turb_) turbCorrect(lastTurbInner);  // simpleSolver.cpp:52
+    tally_ = scal_ + S_UINNER;
+    // ---- momentum ----
+    {
+        const double* xs[1] = {p_};
+        V3P g[1] = {gPn_};
+        gradCells(xs, 1, pb, gs, true, g);
+    }
+    MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
+               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, 0.0, CV3P{}};
+    ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
+    k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
+    launchCheck("assemble_U");
+    solveMomentum(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, uInner);
+    k_hfree<<<G_, TPB, 0, stream_>>>(dm_, uDiag_, cv(U_), cv(ux_), ctl.relax_u, Hf_, rAUr_);
+    launchCheck("hfree");
+    // ---- predictor flux ----
+    k_flux<<<GF_, TPB, 0, stream_>>>(dm_, cv(Hf_), hb, nullptr, phi_);
+    launchCheck("flux");
+    if (doAdjust)
+    {
+        k_adjust_sums<<<1, 32, 0, stream_>>>(phi_, dpStart_, dpSize_, dpFree_, static_cast<int>(mesh_.patches.size()),
+                                             scal_);
+        launchCheck("adjust_sums");
+        k_adjust_scale<<<GF_, TPB, 0, stream_>>>(dm_.nB, dm_.nI, dFreeFace_, phi_, scal_);
+        launchCheck("adjust_scale");
+    }
+    // ---- pressure ----
+    k_face_interp<<<GF_, TPB, 0, stream_>>>(dm_, rAUr_, rAUf_);
+    launchCheck("face_interp");
+    k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, phi_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_, refCell,
+                                          ctl.p_ref_value);
+    launchCheck("assemble_p");
+    tally_ = scal_ + S_PINNER;
+    solvePressure(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, ctl.p_precond, pInner);
+    tally_ = nullptr;
+    {
+        const double* xs[1] = {px_};
+        V3P g[1] = {gPF_};
+        gradCells(xs, 1, pb, gs, true, g);
+    }
+    k_correct_flux<<<GF_, TPB, 0, stream_>>>(dm_, px_, cv(gPF_), rAUf_, pc_, pk_, schemes_.laplacian_corrected, phi_);
+    launchCheck("correct_flux");
+    k_pstep<<<G_, TPB, 0, stream_>>>(nC, px_, p_, scal_);
+    launchCheck("pstep");
+    k_update<<<G_, TPB, 0, stream_>>>(nC, px_, p_, U_, cv(Hf_), cv(gPF_), cv(gPn_), rAUr_, ctl.relax_p,
+                                      ctl.p_relax_start, scal_);
+    launchCheck("update");
+    k_continuity<<<G_, TPB, 0, stream_>>>(dm_, phi_, scal_, S_CONT_AFTER);
+    launchCheck("continuity");
+    CFG_CUDA(cudaMemcpyAsync(scalHost_, scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+}
+
+/// The host's reading of an outer iteration's scalars (simpleSolver.cpp:
+/// 334-390): the result fields, and 1 when the loop stops (diverged or
+/// converged).
+int Ctx::finishOuter(const cfg_simple_controls& ctl, int iter, double& contLag1, double& contLag2,
+                     cfg_simple_result& res)
+{
+    const double* S = scalHost_;
+    const double contErr = S[S_CONT], errAfter = S[S_CONT_AFTER], pDeltaMax = S[S_PDELTA];
+    const double uRes = S[S_DUMAX] / std::max(S[S_UMAX], 1e-300);
+    if (ctl.verbose)
+        std::printf("[chflow] SIMPLE iter %d: continuity %g (corrected %g, dp %g, dU %g)\n", iter, contErr, errAfter,
+                    pDeltaMax, uRes);
+    res.iterations = iter;
+    res.final_continuity_error = contErr;
+    res.final_momentum_residual = uRes;
+    res.last_dp = pDeltaMax;
+    res.last_continuity_corrected = errAfter;
+    if (!std::isfinite(contErr) || !std::isfinite(pDeltaMax) || S[S_NONFINITE] > 0)
+    {
+        res.diverged = 1;
+        if (ctl.verbose) std::printf("[chflow] error: SIMPLE: diverged at iteration %d\n", iter);
+        return 1;
+    }
+    const bool settled = contErr <= contLag2 * 1.01 + 1e-12;
+    const bool momentumSettled = !(ctl.momentum_tol > 0) || uRes <= ctl.momentum_tol;
+    if (momentumSettled &&
+        (contErr < ctl.continuity_tol || (iter >= 5 && ctl.pcorr_tol > 0 && pDeltaMax < ctl.pcorr_tol && settled)))
+    {
+        res.converged = 1;
+        return 1;
+    }
+    contLag2 = contLag1;
+    contLag1 = contErr;
+    return 0;
+}
+
+void Ctx::deviceInner(int64_t& u, int64_t& p, int64_t& t) const
+{
+    u = static_cast<int64_t>(scalHost_[S_UINNER]);
+    p = static_cast<int64_t>(scalHost_[S_PINNER]);
+    t = static_cast<int64_t>(scalHost_[S_TINNER]);
+}
+
+void Ctx::iterate(const cfg_simple_controls& ctl, cfg_simple_result& res)
+{
+    prepareIterate(ctl);
+    std::memset(&res, 0, sizeof res);
+    lastTurbInner = 0;
     double contLag1 = INFINITY, contLag2 = INFINITY;
     launches_ = 0;
     for (int k = 0; k < 8; ++k) lastMs[k] = 0.0;
     CFG_CUDA(cudaEventRecord(tm_.ev[0], stream_));
     for (int iter = 1; iter <= ctl.max_iterations; ++iter)
     {
-        if (turb_) turbCorrect(lastTurbInner);  // simpleSolver.cpp:52
-        CFG_CUDA(cudaMemsetAsync(scal_, 0, S_COUNT * sizeof(double), stream_));
-        // ---- momentum ----
-        {
-            const double* xs[1] = {p_};
-            V3P g[1] = {gPn_};
-            gradCells(xs, 1, pb, gs, true, g);
-        }
-        MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
-                   linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, 0.0, CV3P{}};
-        ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
-        k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
-        launchCheck("assemble_U");
-        solveMomentum(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, res.u_inner_iterations);
-        k_hfree<<<G_, TPB, 0, stream_>>>(dm_, uDiag_, cv(U_), cv(ux_), ctl.relax_u, Hf_, rAUr_);
-        launchCheck("hfree");
-        // ---- predictor flux ----
-        k_flux<<<GF_, TPB, 0, stream_>>>(dm_, cv(Hf_), hb, nullptr, phi_);
-        launchCheck("flux");
-        if (doAdjust)
-        {
-            k_adjust_sums<<<1, 32, 0, stream_>>>(phi_, dpStart_, dpSize_, dpFree_,
-                                                 static_cast<int>(mesh_.patches.size()), scal_);
-            launchCheck("adjust_sums");
-            k_adjust_scale<<<GF_, TPB, 0, stream_>>>(dm_.nB, dm_.nI, dFreeFace_, phi_, scal_);
-            launchCheck("adjust_scale");
-        }
-        // ---- pressure ----
-        k_face_interp<<<GF_, TPB, 0, stream_>>>(dm_, rAUr_, rAUf_);
-        launchCheck("face_interp");
-        k_assemble_p<<<G_, TPB, 0, stream_>>>(dm_, phi_, rAUf_, pc_, pk_, pVal_d_, pDiag_, pBase_, scal_, refCell,
-                                              ctl.p_ref_value);
-        launchCheck("assemble_p");
-        solvePressure(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, ctl.p_precond,
-                      res.p_inner_iterations);
-        {
-            const double* xs[1] = {px_};
-            V3P g[1] = {gPF_};
-            gradCells(xs, 1, pb, gs, true, g);
-        }
-        k_correct_flux<<<GF_, TPB, 0, stream_>>>(dm_, px_, cv(gPF_), rAUf_, pc_, pk_, schemes_.laplacian_corrected,
-                                                 phi_);
-        launchCheck("correct_flux");
-        k_pstep<<<G_, TPB, 0, stream_>>>(nC, px_, p_, scal_);
-        launchCheck("pstep");
-        k_update<<<G_, TPB, 0, stream_>>>(nC, px_, p_, U_, cv(Hf_), cv(gPF_), cv(gPn_), rAUr_, ctl.relax_p,
-                                          ctl.p_relax_start, scal_);
-        launchCheck("update");
-        k_continuity<<<G_, TPB, 0, stream_>>>(dm_, phi_, scal_, S_CONT_AFTER);
-        launchCheck("continuity");
-        CFG_CUDA(cudaMemcpyAsync(scalHost_, scal_, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        enqueueOuter(ctl, res.u_inner_iterations, res.p_inner_iterations);
         CFG_CUDA(cudaStreamSynchronize(stream_));
-        const double* S = scalHost_;
-        const double contErr = S[S_CONT], errAfter = S[S_CONT_AFTER], pDeltaMax = S[S_PDELTA];
-        const double uRes = S[S_DUMAX] / std::max(S[S_UMAX], 1e-300);
-        if (ctl.verbose)
-            std::printf("[chflow] SIMPLE iter %d: continuity %g (corrected %g, dp %g, dU %g)\n", iter, contErr, errAfter,
-                        pDeltaMax, uRes);
-        res.iterations = iter;
-        res.final_continuity_error = contErr;
-        res.final_momentum_residual = uRes;
-        res.last_dp = pDeltaMax;
-        res.last_continuity_corrected = errAfter;
-        if (!std::isfinite(contErr) || !std::isfinite(pDeltaMax) || S[S_NONFINITE] > 0)
-        {
-            res.diverged = 1;
-            if (ctl.verbose) std::printf("[chflow] error: SIMPLE: diverged at iteration %d\n", iter);
-            break;
-        }
-        const bool settled = contErr <= contLag2 * 1.01 + 1e-12;
-        const bool momentumSettled = !(ctl.momentum_tol > 0) || uRes <= ctl.momentum_tol;
-        if (momentumSettled && (contErr < ctl.continuity_tol ||
-                                (iter >= 5 && ctl.pcorr_tol > 0 && pDeltaMax < ctl.pcorr_tol && settled)))
-        {
-            res.converged = 1;
-            break;
-        }
-        contLag2 = contLag1;
-        contLag1 = contErr;
+        if (finishOuter(ctl, iter, contLag1, contLag2, res)) break;
     }
     CFG_CUDA(cudaEventRecord(tm_.ev[1], stream_));
     CFG_CUDA(cudaEventSynchronize(tm_.ev[1]));

@@ -15,6 +15,48 @@ __device__ __forceinline__ double inv_diag_cg(double d) { return (fabs(d) > 1e-3
 __device__ __forceinline__ float inv_diag_cg(float d) { return (fabs(static_cast<double>(d)) > 1e-300) ? 1.0f / d : 1.0f; }
 __device__ __forceinline__ double inv_diag_bicg(double d) { return (d > 1e-300) ? 1.0 / d : 1.0; }
 
+// ------------------------- device-side solver loops -----------------------
+// Inside a captured CUDA graph a solver loop cannot poll its state from the
+// host: the iterations run as the body of a conditional while-node, and the
+// body's last kernel decides whether it runs again.
+
+/// The solver state cleared and its limits set, by a kernel (a captured
+/// graph cannot copy them from a host struct).
+static __global__ void k_state_reset(SolveState* st, double tol, int maxIter, int nComp, int normType)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    unsigned char* b = reinterpret_cast<unsigned char*>(st);
+    for (size_t i = 0; i < sizeof(SolveState); ++i) b[i] = 0;
+    st->tol = tol;
+    st->maxIter = maxIter;
+    st->nComp = nComp;
+    st->normType = normType;
+}
+
+/// The while-condition of a device-side solver loop: run the body again
+/// while the solve is not done, for at most maxBodies bodies (each body
+/// advances at least one iteration until the state's own maxIter test marks
+/// the solve done, so the bound is only a backstop).
+static __global__ void k_loop_cond(cudaGraphConditionalHandle h, const SolveState* st, int* count, int maxBodies)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int c = *count + 1;
+    *count = c;
+    cudaGraphSetConditional(h, (!st->allDone && c < maxBodies) ? 1u : 0u);
+}
+
+/// A finished solve's iteration counts added to acc (component sum), and
+/// its non-convergence counted in acc[1].
+static __global__ void k_state_tally(const SolveState* st, int nComp, double* acc)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int q = 0; q < nComp; ++q)
+    {
+        acc[0] += st->it[q];
+        acc[1] += st->conv[q] ? 0.0 : 1.0;
+    }
+}
+
 /// the residual norm of the stopping test from |r|inf and sum r^2
 __device__ __forceinline__ double resid_norm(const SolveState* st, double inf, double sumsq)
 {

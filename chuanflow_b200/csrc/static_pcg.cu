@@ -42,7 +42,8 @@ std::mutex g_setupMutex;
 unsigned char* g_scratchAddr[kMaxDevices] = {};
 
 /// The device address of g_pcgScratch on `device` (current), looked up on
-/// the first call for that device and cached.
+/// the first call for that device and kept for the life of the process (a
+/// cudaDeviceReset of the device would leave it stale; the header says so).
 unsigned char* scratchOn(int device)
 {
     std::lock_guard<std::mutex> lock(g_setupMutex);

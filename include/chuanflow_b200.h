@@ -303,6 +303,11 @@ int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
  * t = As^, x/r update); the whole DIC application z = M^-1 r. */
 int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable);
 int cfg_kernel_stats(const cfg_ctx* ctx, double out[16]);
+/* The same slots' launches weighted by the vector components each launch
+ * still iterated on (the fused three-component BiCGStab kernels skip a
+ * converged component's rows; 1 per launch elsewhere), for per-launch byte
+ * counts (no reference counterpart). */
+int cfg_kernel_components(const cfg_ctx* ctx, double out[8]);
 
 /* ---- the linear-solver call surface ------------------------------------ */
 
@@ -396,10 +401,14 @@ int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t 
  * this call allocates nothing: its work vectors live in one static device
  * array of the library, sized for at most 262,144 rows (about 8.5 MB, held
  * on every GPU that loads the library until the process exits); larger n is
- * rejected with CFG_EINVAL.  The first call on each device looks that
- * array's address up, so make it before any stream capture.  Calls share the
- * array and keep no state between them, but two calls whose work overlaps on
- * the GPU (different streams or host threads at once) race on it. */
+ * rejected with CFG_EINVAL.  The call synchronises its stream once per chunk
+ * of iterations to test convergence, so it cannot be captured into a CUDA
+ * graph.  The first call on each device looks that array's address up and
+ * keeps it for the life of the process: after a cudaDeviceReset on that
+ * device the kept address is stale, so do not call it again after a reset.
+ * Calls share the array and keep no state between them, but two calls whose
+ * work overlaps on the GPU (different streams or host threads at once) race
+ * on it. */
 int cfg_pcg_solve_static(int32_t device, int64_t n, const int32_t* row_start_dev, const int32_t* cols_dev,
                          const double* vals_dev, const double* b_dev, double* x_dev, double tol, int32_t max_iter,
                          void* stream, cfg_solver_report* report);
@@ -554,7 +563,13 @@ void cfg_batch_destroy(cfg_batch* batch);
 /* The schedule: `workers` blocks in flight at once (1 = one after another),
  * each block's solver kernels on a grid of at most `row_blocks_per_sm`
  * blocks per SM (0 = the context's own grid; -1 = by block size, one per
- * 32k cells between 1 and 4). */
+ * 32k cells between 1 and 4).  workers = 0 runs each pass as ONE CUDA-graph
+ * launch: every block's outer iteration and measure are parallel branches
+ * of a graph captured on the first pass (per schedule and controls), their
+ * linear solvers iterate in device-side conditional while-nodes, and the
+ * host only writes the blocks' boundary values before the launch and reads
+ * their sums after it; it needs one outer iteration per pass, Jacobi or DIC
+ * pressure and no gammaTransition model. */
 int cfg_batch_set_schedule(cfg_batch* batch, int32_t workers, int32_t row_blocks_per_sm);
 /* One coupling pass: lossAt(q[i]) of every block i with controls[i]; wall_ms
  * (may be NULL) is the pass's host wall time.  A block whose drop lossAt
@@ -568,9 +583,10 @@ int cfg_batch_restore(cfg_batch* batch);
 /* Chooses the schedule by measurement: every candidate runs the same pass
  * from the blocks' current fields (saved and restored around each), the
  * fastest is kept and then runs that pass for real; the chosen schedule and
- * each candidate's wall time are returned (times: 6 doubles, may be NULL).
- * Candidates (workers, row blocks per SM): (1,0), (8,1), (16,1), (16,-1),
- * (32,-1), (64,-1). */
+ * each candidate's wall time are returned (times: 9 doubles, may be NULL;
+ * -1 for a candidate the controls exclude).  Candidates (workers, row blocks
+ * per SM): (1,0), (8,1), (16,1), (16,-1), (32,-1), (64,-1), and the
+ * single-graph pass (0,1), (0,2), (0,-1), timed on a replay. */
 int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
                        int32_t* row_blocks_per_sm, double* times);
 

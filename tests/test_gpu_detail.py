@@ -3,6 +3,8 @@ batched evaluation.  The oracle side restates the block's set-up (inlet
 profile, cross-sections), boundary conditions and measurement in numpy
 around the oracle's SIMPLE; the device block must match it within the FP64
 bar, and a batch must reproduce its blocks evaluated alone."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -194,3 +196,49 @@ def test_rans_blocks_batch_and_restore():
     for x, y, a, bb in zip(r1, r2, t1, t2):
         assert x["dp_pa"] == y["dp_pa"] and np.isfinite(x["dp_pa"])
         assert np.array_equal(a, bb)
+
+
+@pytest.mark.parametrize("pressure", ["DIC", "Jacobi"])
+def test_graph_pass_matches_blocks_alone(pressure):
+    """The whole coupling pass as one CUDA-graph launch (schedule workers 0:
+    every block's outer iteration a branch of the graph, its solver loops
+    device-side while-nodes) gives, pass after pass, the bits of the same
+    blocks evaluated one after another with the same solver grid -- drops,
+    fluxes, inner iteration counts and fields -- for laminar and k-epsilon
+    blocks alike."""
+    import chuanflow_b200 as cf
+    from chuanflow_b200 import meshgen
+    spec = meshgen.detail_block_set(6, seed=5, cells_min=500, cells_max=8000)
+
+    def build():
+        cases = []
+        for k, s in enumerate(spec):
+            c = cf.SimpleCase(meshgen.channel_block(s["cells"], s["aspect"]))
+            c.detail_setup(s["shape"])
+            if k % 2:
+                c.detail_turbulence("kEpsilon", nu=s["speed"] * 0.1 / 2e4)
+            cases.append(c)
+        return cases
+
+    ctls = [cf.SimpleControls(max_iterations=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02, non_orth_correctors=1,
+                              linear_tol=1e-8, nu=(1e-4 if k % 2 == 0 else s["speed"] * 0.1 / 2e4),
+                              p_preconditioner=pressure) for k, s in enumerate(spec)]
+    q = [s["speed"] * 0.01 for s in spec]
+    a_cases, b_cases = build(), build()
+    a, b = cf.Batch(a_cases), cf.Batch(b_cases)
+    a.set_schedule(1, 1)
+    b.set_schedule(0, 1)
+    for _ in range(3):
+        ra, _ = a.loss(q, ctls)
+        rb, _ = b.loss(q, ctls)
+        for x, y in zip(ra, rb):
+            assert x["dp_pa"] == y["dp_pa"] and x["flux_out"] == y["flux_out"] and x["flux_in"] == y["flux_in"]
+            assert x["u_inner_iterations"] == y["u_inner_iterations"]
+            assert x["p_inner_iterations"] == y["p_inner_iterations"]
+            assert x["sweeps"] == y["sweeps"] == 1 and x["status"] == y["status"]
+    for ca, cb in zip(a_cases, b_cases):
+        for u, v in zip(ca.download(), cb.download()):
+            assert np.array_equal(u, v)
+    # the controls the single-graph pass cannot take are refused
+    with pytest.raises(cf.CfgError, match="single-graph"):
+        b.loss(q, [dataclasses.replace(c, max_iterations=2) for c in ctls])

@@ -10,7 +10,9 @@ keeps its own work vectors in a static device array of the library.
 The test calls it through the C ABI, twice in a row on different systems,
 and checks each answer against the existing cfg_sparse_solve (which copies
 host arrays to memory it allocates) to 1e-10 relative L2, with the same
-iteration count.  Its device buffers are allocated here, by the test; the
+iteration count; the second system is the reference's own CG fixture
+(solve_cg.npz, from src/common/src/Matrix.cpp:153-222 run on the host), whose
+stored solution the answer must also match.  Its device buffers are allocated here, by the test; the
 entry point itself allocates nothing.  This file is collected last so a run
 that stops at its first failure has already run every other test.
 """
@@ -87,6 +89,13 @@ def test_static_pcg_matches_sparse_solve_twice(golden):
         assert rep.converged and r_ref.converged
         assert abs(rep.iterations - r_ref.iterations) <= 1
         assert rel(x, x_ref) < REL_TOL, rel(x, x_ref)
+    # the reference's own solve of its fixture, from its right-hand side and
+    # initial guess
+    rs, cols, vals, n = small
+    x, rep = solve_static(rs, cols, vals, g["b"], g["x0"], float(g["tol"]), int(g["max_iter"]))
+    assert rep.converged == bool(g["converged"])
+    assert abs(rep.iterations - int(g["iterations"])) <= 1
+    assert rel(x, g["x"]) < 1e-9, rel(x, g["x"])
 
 
 def test_static_pcg_rejects_oversized_systems():
