@@ -1,27 +1,29 @@
 #!/usr/bin/env python
-"""SIMPLE cell-iterations/s on the 2M-cell jittered lid-driven cavity.
+"""SIMPLE cell-iterations/s on a 2M-cell jittered channel.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 A step is one SIMPLE outer iteration (momentum predictor with its non-
 orthogonal passes, predictor flux, pressure equation with its passes, flux
-correction, relaxed updates) over the whole 128^3 mesh, on fields that stay
+correction, relaxed updates) over the whole mesh, on fields that stay
 resident in HBM between steps.  N > 1 runs independent replicas, one per GPU
 (one case per GPU: the SIMPLE loop is not split across GPUs), launched
 by torchrun; value is the whole job's cells*iterations / max-over-ranks time.
 
-The workload: 128^3 = 2,097,152 hex cells in the unit box, interior mesh
-points jittered by a seeded uniform +-10% of the cell size, lid (ymax)
-U = (1 0 0), other walls no-slip, nu = 1/400 (Re 400), schemes upwind /
-corrected / corrected, 1 non-orthogonal corrector, relaxU 0.7, relaxP 0.3,
-pRelaxStart 0.02, momentum by the reference's Jacobi-BiCGStab, pressure to
-1e-8 (infinity norm relative to the right-hand side, the reference's test)
-with at most 2000 iterations by FP64 flexible CG preconditioned with an FP32
-aggregation-AMG V-cycle (--p-precond; the line's `variant` runs the same
-steps with FP64 multicolour DIC-PCG), and a pressure reference cell (cell 0)
--- without it the reference's singular Neumann pressure system, made
-inconsistent by its own boundary non-orthogonal correction, drives p to
-~1e12 in the first iteration.
+The workload: the 16,000-cell verification channel's family (2.0 x 0.1 x
+0.1 m, inlet 0.1 m/s, fixed-p outlet, no-slip walls, nu 1e-4) at 512 x 64 x
+64 = 2,097,152 hex cells -- the cell count of the 128^3 cavity -- with the
+cavity's mesh treatment (interior points jittered by a seeded uniform +-10%
+of the cell size, so every face is non-orthogonal), schemes upwind /
+corrected / corrected, 1 non-orthogonal corrector, and the reference's own
+channel relaxation (relaxU 0.9, relaxP 0.03, pRelaxStart 0.02).  Momentum by
+the reference's Jacobi-BiCGStab; pressure to 1e-8 (infinity norm relative to
+the right-hand side, the reference's test) with at most 2000 iterations by
+FP64 flexible CG preconditioned with an FP32 aggregation-AMG V-cycle
+(--p-precond; the line's `variant` runs the same steps with FP64 multicolour
+DIC-PCG).  The lid-driven cavity of the same cell count is not the
+headline: the reference's SIMPLE diverges on it, on the GPU and in the C
+restatement alike, under every relaxation tried.
 
 Every leg counts the outer iterations that diverged (simpleSolver.cpp:360-364:
 non-finite continuity, pressure step or fields); the JSON line carries them
@@ -44,24 +46,36 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-CELLS = 128
+CELLS = 64                      # the channel's cells across; 8x along: 512 x 64 x 64 = 2,097,152
+LENGTH = (2.0, 0.1, 0.1)
+U_IN, NU = 0.1, 1e-4            # Re 100 on the channel height
 JITTER, SEED = 0.1, 7
-NU = 1.0 / 400.0
-NAMES = ["left", "right", "bottom", "lid", "front", "back"]
 SIDES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
+CH_NAMES = ["inlet", "outlet", "bottom", "top", "front", "back"]
+CH_TYPES = ["inlet", "outlet", "wall", "wall", "wall", "wall"]
+RELAX = {"relax_u": 0.9, "relax_p": 0.03, "p_relax_start": 0.02}
 METRIC = "SIMPLE cell-iter/s at 2M cells; time to 1e-8 p-residual, learned vs plain PCG"
-REFERENCE_ARM = ("the reference's CPU SIMPLE (its own sources) on the same mesh and settings, one outer iteration "
-                 "from rest as a bounded sample (a whole 128^3 iteration takes minutes on one core); the reference "
-                 "has no pressure reference cell and no DIC or AMG, so it solves its singular Neumann pressure "
-                 "system with Jacobi-PCG to the same 1e-8 / 2000-iteration limits; one core, pinned")
+REFERENCE_ARM = ("the reference's CPU SIMPLE (its own sources, its Jacobi-PCG pressure and Jacobi-BiCGStab "
+                 "momentum) on the same mesh, boundary conditions and settings, one outer iteration from rest as "
+                 "a bounded sample (a whole 2M-cell iteration takes minutes on one core); one core, pinned")
+# the lid-driven cavity the tests still run (the reference's SIMPLE diverges on it at these sizes)
+CAV_NAMES = ["left", "right", "bottom", "lid", "front", "back"]
+CAV_NU = 1.0 / 400.0
+
+
+def dims(n):
+    return (8 * n, n, n)
 
 
 def workload_config(n, precond="DIC"):
     solve = ("FP64 flexible CG with an FP32 aggregation-AMG V-cycle" if precond == "AMG" else f"{precond}-PCG")
-    return {"workload": f"lid-driven cavity {n}^3 hex ({n ** 3} cells), interior points jittered +-10% "
-                        f"(seed {SEED}), Re 400, upwind/corrected/corrected, nonOrth 1, relaxU 0.7 relaxP 0.3 "
-                        f"pRelaxStart 0.02, pressure {solve} tol 1e-8 (|r|inf/|b|inf) maxIter 2000, pRefCell 0",
-            "cells": n ** 3, "step": "one SIMPLE outer iteration",
+    nx, ny, nz = dims(n)
+    return {"workload": f"3D channel {LENGTH[0]} x {LENGTH[1]} x {LENGTH[2]} m, {nx} x {ny} x {nz} hex "
+                        f"({nx * ny * nz} cells), interior points jittered +-10% (seed {SEED}), inlet {U_IN} m/s, "
+                        f"fixed-p outlet, no-slip walls, nu {NU} (Re 100), upwind/corrected/corrected, nonOrth 1, "
+                        f"relaxU 0.9 relaxP 0.03 pRelaxStart 0.02 (the reference's channel settings), momentum "
+                        f"Jacobi-BiCGStab, pressure {solve}, tol 1e-8 (|r|inf/|b|inf), maxIter 2000",
+            "cells": nx * ny * nz, "step": "one SIMPLE outer iteration",
             "l2": "inputs larger than L2 (about 1.3 GB of fields, matrices and mesh resident in HBM)",
             "precision": ("FP64, the pressure preconditioner FP32" if precond == "AMG" else "FP64 throughout"),
             "parallelism": "one case per GPU (replicas); the reference arm on one host core",
@@ -80,7 +94,7 @@ KERNEL_NAMES = {
 }
 
 
-MEASURED_TRAFFIC = {"bi_spmv2": 334e6}
+MEASURED_TRAFFIC = {}
 
 
 def kernel_bytes(N, F, s=8, i=4):
@@ -135,16 +149,37 @@ def simple_step_bytes(N, F, Fb, n_orth, it_p, precond, solver_bytes, s=8, i=4):
 
 
 def make_case(n, device, precond="Jacobi"):
+    """The headline channel on `device`, at rest with its boundary flux."""
     import chuanflow_b200 as cf
-    mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (n, n, n), {s: (nm, "wall") for s, nm in zip(SIDES, NAMES)})
+    mesh = cf.PolyMesh.block((0, 0, 0), LENGTH, dims(n), {s: (nm, t) for s, nm, t in zip(SIDES, CH_NAMES, CH_TYPES)})
     mesh.jitter_interior(JITTER, SEED)
     case = cf.SimpleCase(mesh, device)
-    for nm in NAMES:
+    case.set_patch_bc("U", "inlet", "fixedValue", (U_IN, 0, 0))
+    case.set_patch_bc("p", "inlet", "zeroGradient", 0.0)
+    case.set_patch_bc("U", "outlet", "zeroGradient", (0, 0, 0))
+    case.set_patch_bc("p", "outlet", "fixedValue", 0.0)
+    for nm in CH_NAMES[2:]:
+        case.set_patch_bc("U", nm, "fixedValue", (0, 0, 0))
+        case.set_patch_bc("p", nm, "zeroGradient", 0.0)
+    case.init_flux()
+    ctl = cf.SimpleControls(max_iterations=1, non_orth_correctors=1, linear_tol=1e-8, linear_max_iter=2000, nu=NU,
+                            p_preconditioner=precond, **RELAX)
+    return mesh, case, ctl
+
+
+def make_cavity_case(n, device, precond="Jacobi"):
+    """The jittered n^3 lid-driven cavity (Re 400, relaxation 0.7 / 0.3 /
+    pRelaxStart 0.02, pressure reference cell 0)."""
+    import chuanflow_b200 as cf
+    mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (n, n, n), {s: (nm, "wall") for s, nm in zip(SIDES, CAV_NAMES)})
+    mesh.jitter_interior(JITTER, SEED)
+    case = cf.SimpleCase(mesh, device)
+    for nm in CAV_NAMES:
         case.set_patch_bc("U", nm, "fixedValue", (1.0, 0, 0) if nm == "lid" else (0, 0, 0))
         case.set_patch_bc("p", nm, "zeroGradient", 0.0)
     case.init_flux()
     ctl = cf.SimpleControls(max_iterations=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02, non_orth_correctors=1,
-                            linear_tol=1e-8, linear_max_iter=2000, nu=NU, p_ref_cell=0, p_ref_value=0.0,
+                            linear_tol=1e-8, linear_max_iter=2000, nu=CAV_NU, p_ref_cell=0, p_ref_value=0.0,
                             p_preconditioner=precond)
     return mesh, case, ctl
 
@@ -157,36 +192,48 @@ def _splitmix64(x):
     return z ^ (z >> np.uint64(31))
 
 
-def cavity_points(n, fraction=JITTER, seed=SEED):
-    """The points of the jittered n^3 unit-box cavity, computed in numpy
-    with the same IEEE operations as BlockMesh::create's coordAt
-    (blockMesh.cpp:52-57) and cfg_mesh_jitter_interior (every interior point
-    moves by (2u - 1) fraction h per axis, u = splitmix64(seed *
-    0x100000001B3 ^ (3 point + axis)) >> 11 over 2^53), so the reference arm
-    needs no product library to build the same mesh."""
-    c = 0.0 + (1.0 - 0.0) * np.arange(n + 1, dtype=np.float64) / float(n)
-    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+def block_points(cells, length, fraction=JITTER, seed=SEED):
+    """The points of a jittered block mesh from the origin to `length`,
+    computed in numpy with the same IEEE operations as BlockMesh::create's
+    coordAt (blockMesh.cpp:52-57) and cfg_mesh_jitter_interior (every
+    interior point moves by (2u - 1) fraction h per axis, u =
+    splitmix64(seed * 0x100000001B3 ^ (3 point + axis)) >> 11 over 2^53), so
+    the reference arm needs no product library to build the same mesh."""
+    nx, ny, nz = cells
+    cx, cy, cz = (0.0 + (length[a] - 0.0) * np.arange(cells[a] + 1, dtype=np.float64) / float(cells[a])
+                  for a in range(3))
+    z, y, x = np.meshgrid(cz, cy, cx, indexing="ij")
     pts = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
-    inner = np.arange(1, n)
-    k, j, i = np.meshgrid(inner, inner, inner, indexing="ij")
-    pid = (i + (n + 1) * (j + (n + 1) * k)).ravel().astype(np.uint64)
+    k, j, i = np.meshgrid(np.arange(1, nz), np.arange(1, ny), np.arange(1, nx), indexing="ij")
+    pid = (i + (nx + 1) * (j + (ny + 1) * k)).ravel().astype(np.uint64)
     s0 = np.uint64((seed * 0x100000001B3) & ((1 << 64) - 1))
-    h = (1.0 - 0.0) / float(n)
     with np.errstate(over="ignore"):
         for a in range(3):
+            h = (length[a] - 0.0) / float(cells[a])
             r = _splitmix64(s0 ^ (pid * np.uint64(3) + np.uint64(a)))
             u = (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
             pts[pid.astype(np.int64), a] += (u * 2.0 - 1.0) * fraction * h
     return pts
 
 
+def cavity_points(n, fraction=JITTER, seed=SEED):
+    return block_points((n, n, n), (1.0, 1.0, 1.0), fraction, seed)
+
+
 def case_dict(n):
-    sides = "\n".join(f"    {s} {{ name {nm}; type wall; }}" for s, nm in zip(SIDES, NAMES))
-    pats = "\n".join(f"    {nm} {{ U ({'1' if nm == 'lid' else '0'} 0 0); }}" for nm in NAMES)
-    return (f"block\n{{\n    min (0 0 0);\n    max (1 1 1);\n    cells ({n} {n} {n});\n{sides}\n}}\n"
-            f"nu {NU!r};\npatches\n{{\n{pats}\n}}\n"
+    """The headline channel as a reference case dictionary (simpleFoamApp's
+    keys); its points come separately (the jitter)."""
+    nx, ny, nz = dims(n)
+    sides = "\n".join(f"    {s} {{ name {nm}; type {t}; }}" for s, nm, t in zip(SIDES, CH_NAMES, CH_TYPES))
+    return (f"block\n{{\n    min (0 0 0);\n    max ({LENGTH[0]!r} {LENGTH[1]!r} {LENGTH[2]!r});\n"
+            f"    cells ({nx} {ny} {nz});\n{sides}\n}}\n"
+            f"nu {NU!r};\npatches\n{{\n"
+            f"    inlet  {{ U ({U_IN!r} 0 0); UType fixedValue; pType zeroGradient; }}\n"
+            f"    outlet {{ UType zeroGradient; p 0; pType fixedValue; }}\n"
+            + "".join(f"    {nm} {{ U (0 0 0); }}\n" for nm in CH_NAMES[2:]) +
+            "}\n"
             "schemes { ddt steady; div upwind; laplacian corrected; grad corrected; }\n"
-            "simple { maxIterations 1; relaxU 0.7; relaxP 0.3; pRelaxStart 0.02; nonOrthCorrectors 1; "
+            "simple { maxIterations 1; relaxU 0.9; relaxP 0.03; pRelaxStart 0.02; nonOrthCorrectors 1; "
             "linearTol 1e-08; linearMaxIter 2000; }\n")
 
 
@@ -270,12 +317,11 @@ def pinned_core():
 
 
 def run_reference_cpu(n, points, timeout=3600, fields=False):
-    """One SIMPLE outer iteration from rest of the n^3 cavity by the
+    """One SIMPLE outer iteration from rest of the headline channel by the
     reference's own build (oracle/_ref/cf_ref_driver, its sources compiled
-    with g++ -O3) on this host, pinned to one core (the reference is serial).
-    The reference has no pressure reference cell, so it solves its singular
-    Neumann pressure system with its Jacobi-PCG.  Returns (seconds, kind,
-    what, (U, p, phi) or None)."""
+    with g++ -O3) on this host, pinned to one core (the reference is serial),
+    with its Jacobi-PCG pressure.  Returns (seconds, kind, what, (U, p, phi)
+    or None)."""
     drv = os.path.join(ROOT, "oracle", "_ref", "cf_ref_driver")
     with tempfile.TemporaryDirectory() as td:
         cp = os.path.join(td, "case.dict")
@@ -297,11 +343,11 @@ def run_reference_cpu(n, points, timeout=3600, fields=False):
         # the C restatement of the same algorithm, when the reference was not built
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import _oracle as O
-        m = O.block_mesh((0, 0, 0), (1, 1, 1), (n, n, n), NAMES, ["wall"] * 6).with_points(points)
-        case = O.Case(m, u_type=["fixedValue"] * 6,
-                      u_value=[(1.0, 0, 0) if nm == "lid" else (0, 0, 0) for nm in m.patch_names],
-                      p_type=["zeroGradient"] * 6, p_value=[0] * 6, nu=NU, max_iterations=1, linear_tol=1e-8,
-                      non_orth=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02)
+        m = O.block_mesh((0, 0, 0), LENGTH, dims(n), CH_NAMES, CH_TYPES).with_points(points)
+        case = O.Case(m, u_type=["fixedValue", "zeroGradient"] + ["fixedValue"] * 4,
+                      u_value=[(U_IN, 0, 0)] + [(0, 0, 0)] * 5, p_type=["zeroGradient", "fixedValue"] +
+                      ["zeroGradient"] * 4, p_value=[0] * 6, nu=NU, max_iterations=1, linear_tol=1e-8,
+                      non_orth=1, **RELAX)
         t0 = time.perf_counter()
         U, p, phi, _ = case.run()
         return time.perf_counter() - t0, "port", "oracle/cfo.c (C restatement)", ((U, p, phi) if fields else None)
@@ -330,14 +376,15 @@ def main_reference(args, world, rank, dist):
         return
     n = args.cells
     steps = 1
-    secs, kind, what, _ = run_reference_cpu(n, cavity_points(n))
-    v = n ** 3 * steps / secs
+    secs, kind, what, _ = run_reference_cpu(n, block_points(dims(n), LENGTH))
+    v = float(np.prod(dims(n))) * steps / secs
     out = {"metric": METRIC, "impl": "reference", "value": v, "unit": "cell-iter/s", "n_gpus": args.gpus,
            "steps": steps, "warmup": 0, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": workload_config(n, args.p_precond),
            "cpu_baseline": {"value": v, "unit": "cell-iter/s", "cores": 1, "kind": kind,
-                            "sample": f"one SIMPLE outer iteration of the {n}^3 case from rest; {what}; {cpu_info()}"},
+                            "sample": f"one SIMPLE outer iteration of the headline channel from rest; {what}; "
+                                      f"{cpu_info()}"},
            "e2e": {"value": v, "unit": "cell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -635,7 +682,7 @@ def main():
     ap.add_argument("--profile-warm", type=int, default=0,
                     help="with --profile: outer iterations run before the profiler range opens")
     ap.add_argument("--workload", default="simple", choices=["simple", "poisson", "blocks", "transient"],
-                    help="simple: the 2M-cell SIMPLE cavity (the headline); poisson: the ~4M-tet "
+                    help="simple: the 2M-cell SIMPLE channel (the headline); poisson: the ~4M-tet "
                          "pressure-Poisson solve, FP64 DIC-PCG vs FP32-in-FP64 refinement; blocks: 64 detail "
                          "blocks of a coupled network, one coupling pass per step, batched vs one after another")
     ap.add_argument("--blocks", type=int, default=64, help="blocks: number of detail blocks")
@@ -706,7 +753,7 @@ def field_errors(U, p, phi, U0, p0, phi0, mean_free=False):
 
 
 def main_simple(args, world, rank, local, dist):
-    """The headline: K SIMPLE outer iterations of the 128^3 cavity on
+    """The headline: K SIMPLE outer iterations of the 2M-cell channel on
     device-resident fields after W warm-up iterations.  Every leg counts
     its diverged iterations; a run with any is reported and exits 1."""
     n = args.cells
@@ -803,9 +850,9 @@ def main_simple(args, world, rank, local, dist):
             solver_bytes += cnt * b * scale
     top = max(kernels, key=lambda k: kernels[k]["total_ms"])
     kt = kernels[top]
-    # DRAM bytes per launch from one ncu capture of this workload (128^3,
-    # the section capture of the four BiCGStab kernels); null for a kernel without one
-    traffic = MEASURED_TRAFFIC.get(top) if n == 128 else None
+    # DRAM bytes per launch of the top kernel from one ncu capture of this
+    # workload (profiles/), null for a kernel without one
+    traffic = MEASURED_TRAFFIC.get(top) if n == CELLS else None
     roof = {"kernel": KERNEL_NAMES[top], "bound": "hbm", "achieved": kt["achieved_gbs"], "peak": peak,
             "unit": "GB/s", "frac": kt["achieved_gbs"] / peak, "peak_source": peak_src, "traffic": traffic,
             "algorithmic_bytes_per_launch": kt["alg_bytes"], "launches_timed": kt["launches"],
@@ -872,21 +919,20 @@ def main_simple(args, world, rank, local, dist):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         case.upload(np.zeros((ncell, 3)), np.zeros(ncell), np.zeros(mesh.n_faces))
         case.init_flux()
-        rc = dataclasses.replace(ctl, p_preconditioner="Jacobi", p_ref_cell=-1)
+        rc = dataclasses.replace(ctl, p_preconditioner="Jacobi")
         same = Steps().run(case, rc, 1)
         Ug, pg, phig = case.download()
         secs, kind, what, ref_fields = run_reference_cpu(n, mesh.addressing()["points"], fields=True)
         out["cpu_baseline"] = {"value": ncell / secs, "unit": "cell-iter/s", "cores": 1, "kind": kind,
-                               "sample": f"one SIMPLE outer iteration of the same {n}^3 mesh and settings from rest "
-                                         f"({secs:.1f} s), as the reference runs it: no pressure reference cell, "
-                                         f"Jacobi-PCG; {what}; {cpu_info()}"}
+                               "sample": f"one SIMPLE outer iteration of the same mesh and settings from rest "
+                                         f"({secs:.1f} s), with the reference's Jacobi-PCG pressure; {what}; "
+                                         f"{cpu_info()}"}
         out["reference_step_same_work"] = {
-            "what": "the reference's first outer iteration from rest (no reference cell, Jacobi-PCG), on this GPU "
+            "what": "the reference's first outer iteration from rest with its own Jacobi-PCG pressure, on this GPU "
                     "and by the reference on one core",
             "gpu_ms": same.ms, "cpu_ms": secs * 1e3, "speedup": secs * 1e3 / same.ms,
             "inner_iterations_gpu": {"momentum": same.u, "pressure": same.p},
-            "field_error_vs_reference": (field_errors(Ug, pg, phig, *ref_fields, mean_free=True)
-                                         if ref_fields else None),
+            "field_error_vs_reference": (field_errors(Ug, pg, phig, *ref_fields) if ref_fields else None),
             "diverged": same.diverged}
     if rank == 0:
         out["valid"] = diverged == 0

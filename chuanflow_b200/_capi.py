@@ -14,7 +14,7 @@ BC = {"fixedValue": 0, "zeroGradient": 1, "fixedGradient": 2, "symmetry": 3, "ou
       "empty": 6}
 GRAD = {"linear": 0, "corrected": 1, "leastSquares": 2}
 DIV = {"upwind": 0, "linear": 1, "blend": 2, "linearUpwind": 3}
-PRECOND = {"Jacobi": 0, "DIC": 1, "MPNN": 2, "AMG": 3}
+PRECOND = {"Jacobi": 0, "DIC": 1, "MPNN": 2, "AMG": 3, "IR32": 4, "AMG_MPNN": 5}
 
 _f64p = C.POINTER(C.c_double)
 _i64p = C.POINTER(C.c_int64)
@@ -666,6 +666,31 @@ def _mpnn_loss_grad(self, r):
     return loss.value, g
 
 
+def _mpnn_loss_grad_pair(self, r, t):
+    """One (residual, converged correction) pair's energy-norm loss and
+    its gradient."""
+    n = C.c_int64()
+    _check(lib().cfg_mpnn_params(self._h, C.byref(n)))
+    g = np.zeros(n.value, np.float32)
+    loss = C.c_double()
+    _check(lib().cfg_mpnn_loss_grad_pair(self._h, _dp(_f64(r)), _dp(_f64(t)), C.byref(loss),
+                                         g.ctypes.data_as(C.POINTER(C.c_float))))
+    return loss.value, g
+
+
+def _mpnn_train_pairs(self, samples, targets, epochs=1, lr=1e-3):
+    """Adam over (residual, converged correction) pairs (rows); returns the
+    per-epoch mean losses."""
+    s = np.ascontiguousarray(samples, np.float64)
+    t = np.ascontiguousarray(targets, np.float64)
+    if s.shape != t.shape:
+        raise ValueError("mpnn_train_pairs: samples and targets differ in shape")
+    losses = np.zeros(epochs)
+    _check(lib().cfg_mpnn_train_pairs(self._h, _dp(s), _dp(t), C.c_int32(s.shape[0]), C.c_int32(epochs),
+                                      C.c_float(lr), _dp(losses)))
+    return losses
+
+
 def _mpnn_apply(self, r):
     z = np.zeros(self.mesh.n_cells)
     _check(lib().cfg_mpnn_apply(self._h, _dp(_f64(r)), _dp(z)))
@@ -772,6 +797,8 @@ SimpleCase.mpnn_weights = _mpnn_weights
 SimpleCase.mpnn_loss_grad = _mpnn_loss_grad
 SimpleCase.mpnn_apply = _mpnn_apply
 SimpleCase.mpnn_train = _mpnn_train
+SimpleCase.mpnn_loss_grad_pair = _mpnn_loss_grad_pair
+SimpleCase.mpnn_train_pairs = _mpnn_train_pairs
 SimpleCase.poisson_residual = _poisson_residual
 SimpleCase.detail_turbulence = _detail_turbulence
 SimpleCase.turbulence_setup = _turbulence_setup

@@ -727,7 +727,10 @@ CaseSpec parseCase(const char* path)
     {
         const cfg::Dict& g = d.dict("gpu");
         const std::string pp = g.wordOr("pPreconditioner", "Jacobi");
-        c.p_precond = pp == "DIC" ? CFG_PRECOND_DIC : (pp == "AMG" ? CFG_PRECOND_AMG : CFG_PRECOND_JACOBI);
+        c.p_precond = pp == "DIC"    ? CFG_PRECOND_DIC
+                      : pp == "AMG"  ? CFG_PRECOND_AMG
+                      : pp == "IR32" ? CFG_PRECOND_IR32
+                                     : CFG_PRECOND_JACOBI;
         c.p_ref_cell = static_cast<int64_t>(g.numberOr("pRefCell", -1));
         c.p_ref_value = g.numberOr("pRefValue", 0.0);
         c.verbose = static_cast<int32_t>(g.numberOr("verbose", 1));
@@ -908,7 +911,8 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
         bool graphable = true;
         for (size_t i = 0; i < batch->blocks.size(); ++i)
             graphable = graphable && controls[i].max_iterations == 1 && controls[i].p_precond != CFG_PRECOND_AMG &&
-                        controls[i].p_precond != CFG_PRECOND_MPNN &&
+                        controls[i].p_precond != CFG_PRECOND_MPNN && controls[i].p_precond != CFG_PRECOND_IR32 &&
+                        controls[i].p_precond != CFG_PRECOND_AMG_MPNN &&
                         batch->blocks[i]->turbulenceModelName() != "gammaTransition";
         std::vector<cfg_detail_measure> m(batch->blocks.size());
         double best = 0;
@@ -1026,6 +1030,23 @@ int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t nSamples, int32_
     return guard([&] {
         need(ctx && samples, "cfg_mpnn_train: null argument");
         ctx->c->mpnnTrainHost(samples, nSamples, epochs, lr, losses);
+    });
+}
+
+int cfg_mpnn_train_pairs(cfg_ctx* ctx, const double* samples, const double* targets, int32_t nSamples,
+                         int32_t epochs, float lr, double* losses)
+{
+    return guard([&] {
+        need(ctx && samples && targets, "cfg_mpnn_train_pairs: null argument");
+        ctx->c->mpnnTrainHost(samples, nSamples, epochs, lr, losses, targets);
+    });
+}
+
+int cfg_mpnn_loss_grad_pair(cfg_ctx* ctx, const double* r, const double* t, double* loss, float* grad)
+{
+    return guard([&] {
+        need(ctx && r && t && loss, "cfg_mpnn_loss_grad_pair: null argument");
+        *loss = ctx->c->mpnnLossGradHost(r, grad, t);
     });
 }
 

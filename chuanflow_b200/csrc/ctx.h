@@ -106,9 +106,10 @@ public:
     void mpnnCreate(int layers, uint64_t seed);
     void mpnnWeights(float* get, const float* set, int64_t n);
     int mpnnParams() const;
-    double mpnnLossGradHost(const double* r, float* grad);
+    double mpnnLossGradHost(const double* r, float* grad, const double* t = nullptr);
     void mpnnApplyHost(const double* r, double* z);
-    void mpnnTrainHost(const double* samples, int nSamples, int epochs, float lr, double* losses);
+    void mpnnTrainHost(const double* samples, int nSamples, int epochs, float lr, double* losses,
+                       const double* targets = nullptr);
     /// residuals the pressure solves start from, kept as training samples
     void mpnnCollect(int mode, int maxSamples);
     int mpnnCollected() const { return static_cast<int>(collected_.size()); }
@@ -240,17 +241,23 @@ private:
     void amgInfo(double* out);
     bool amgFresh_ = false;  // the hierarchy's values match the Poisson system
     void mpnnApply(const double* vals, const double* diag, const double* r, double* z);
-    double mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z);
+    double mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z,
+                        const double* t = nullptr);
+    void mpnnGuess(const double* vals, const double* diag, const double* b, double* x);
+    double* trainBuf_ = nullptr;
+    size_t trainCap_ = 0;
     void mpnnAdam(float lr);
     void mpnnMatrix(const double** vals, const double** diag) const;
-    void mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses);
+    void mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses,
+                   const double* targets = nullptr);
     void mpnnFcg(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
                  int window, int64_t* out, int normType, int pc = 0);
     double fcgNorm(const double* v, int normType);
     void mpnnResidualHost(const double* vals, const double* b, const double* x, double* rHost);
     bool collectOn_ = false;
     int collectMax_ = 0;
-    std::vector<std::vector<double>> collected_;
+    std::vector<std::vector<double>> collected_;   // residual each collected solve started from
+    std::vector<std::vector<double>> collectedT_;  // the correction it converged to
     void fcgSpmv(const double* vals, const double* x, double* y);
     void fcgDots(int np, const double* const* a, const double* const* b, double* out);
     const double** fcgPtrs_ = nullptr;
@@ -319,6 +326,10 @@ private:
     DDicT<float> dic32_{};
     double *pb64_ = nullptr, *px64_ = nullptr;
     bool poissonReady_ = false;
+    bool mixedReady_ = false;
+    void ensureMixed();
+    void runIR32(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                 double innerTol, cfg_solver_report* rep);
     // multicolour DIC
     DDic dic_{};
     std::vector<DicPhase> dicPhase_;

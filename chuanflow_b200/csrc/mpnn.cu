@@ -15,9 +15,14 @@
 // |A M(r) - r|^2 / |r|^2 over residual samples with Adam; the gradient is
 // with respect to the BF16 weights, applied to the FP32 master.
 //
-// Device layout: one warp per cell, lane k owning hidden unit k, so the
-// hidden vector of a neighbour is one coalesced 128-byte load and the 32x32
-// transforms run as shuffles against weights staged in shared memory.
+// Device layout: hidden states are FP32 rows of 32 (one 128-byte line per
+// cell).  A layer's warp takes 16 cells at a time: lane k gathers channel k
+// of each cell's state and message (one coalesced line per neighbour), the
+// 16 x 64 block [h | m] is rounded to BF16 in shared memory, and the 32 x 64
+// contraction with [A | B] runs on the tensor cores (mma.sync m16n8k16,
+// BF16 operands, FP32 accumulation).  The backward kernels use the same
+// BF16-rounded operands for the weight gradients and pass gradients through
+// the rounding unchanged.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -96,39 +101,105 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_enc(int n, const double* _
     }
 }
 
-/// one residual message-passing layer
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16(x)); }
+
+__device__ __forceinline__ uint32_t ld_pair(const __nv_bfloat16* p)
+{
+    return *reinterpret_cast<const uint32_t*>(p);
+}
+
+/// D (16x8, FP32) += A (16x16, BF16, row) * B (16x8, BF16, col)
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                               uint32_t b0, uint32_t b1)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+constexpr int XP = 2 * H + 8;  // padded BF16 row of [h | m] and of the weights (144 bytes)
+
+/// one residual message-passing layer: hout = hin + relu(A h + B m + b) for
+/// 16 cells per warp step, the contraction on the tensor cores
 __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const double* __restrict__ val,
                                                             const double* __restrict__ diag,
                                                             const __nv_bfloat16* __restrict__ wl,
                                                             const float* __restrict__ hin, float* __restrict__ hout,
                                                             unsigned* __restrict__ mask)
 {
-    __shared__ float sA[H * WP], sB[H * WP], sb[H];
+    // sW[o][k]: output unit o, input k (k < 32: A, k >= 32: B)
+    __shared__ __align__(16) __nv_bfloat16 sW[H][XP];
+    __shared__ float sb[H];
+    __shared__ __align__(16) __nv_bfloat16 sX[kWarps][16][XP];
+    __shared__ float sU[kWarps][16][H + 1];
     for (int t = threadIdx.x; t < H * H; t += blockDim.x)
     {
-        const int k = t / H, q = t % H;
-        sA[k * WP + q] = __bfloat162float(wl[t]);
-        sB[k * WP + q] = __bfloat162float(wl[H * H + t]);
+        const int o = t / H, k = t % H;
+        sW[o][k] = wl[t];
+        sW[o][H + k] = wl[H * H + t];
     }
     for (int t = threadIdx.x; t < H; t += blockDim.x) sb[t] = __bfloat162float(wl[2 * H * H + t]);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int warp = blockIdx.x * kWarps + (threadIdx.x >> 5), nw = gridDim.x * kWarps;
-    for (int i = warp; i < A.n; i += nw)
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int groups = (A.n + 15) / 16;
+    for (int g = blockIdx.x * kWarps + w; g < groups; g += gridDim.x * kWarps)
     {
-        const float h = hin[static_cast<size_t>(i) * H + lane];
-        const float m = message(A, val, diag, hin, i, lane);
-        float u = sb[lane];
+        const int c0 = g * 16;
+        float hr[16];
 #pragma unroll
-        for (int q = 0; q < H; ++q)
+        for (int t = 0; t < 16; ++t)
         {
-            const float hq = __shfl_sync(0xffffffffu, h, q);
-            const float mq = __shfl_sync(0xffffffffu, m, q);
-            u += sA[lane * WP + q] * hq + sB[lane * WP + q] * mq;
+            const int i = c0 + t;
+            float h = 0.f, m = 0.f;
+            if (i < A.n)
+            {
+                h = hin[static_cast<size_t>(i) * H + lane];
+                m = message(A, val, diag, hin, i, lane);
+            }
+            hr[t] = h;
+            sX[w][t][lane] = __float2bfloat16(h);
+            sX[w][t][H + lane] = __float2bfloat16(m);
         }
-        hout[static_cast<size_t>(i) * H + lane] = h + (u > 0.f ? u : 0.f);
-        const unsigned bits = __ballot_sync(0xffffffffu, u > 0.f);
-        if (lane == 0) mask[i] = bits;
+        __syncwarp();
+        float d[4][4] = {};
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks)
+        {
+            const int k0 = ks * 16 + tig * 2;
+            const uint32_t a0 = ld_pair(&sX[w][gid][k0]), a1 = ld_pair(&sX[w][gid + 8][k0]);
+            const uint32_t a2 = ld_pair(&sX[w][gid][k0 + 8]), a3 = ld_pair(&sX[w][gid + 8][k0 + 8]);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt)
+            {
+                const int o = nt * 8 + gid;
+                mma_bf16_16816(d[nt], a0, a1, a2, a3, ld_pair(&sW[o][k0]), ld_pair(&sW[o][k0 + 8]));
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int row = gid + (j >> 1) * 8, col = nt * 8 + tig * 2 + (j & 1);
+                sU[w][row][col] = d[nt][j] + sb[col];
+            }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+        {
+            const int i = c0 + t;
+            const float u = sU[w][t][lane];
+            const unsigned bits = __ballot_sync(0xffffffffu, u > 0.f);
+            if (i < A.n)
+            {
+                hout[static_cast<size_t>(i) * H + lane] = hr[t] + (u > 0.f ? u : 0.f);
+                if (lane == 0) mask[i] = bits;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -186,11 +257,13 @@ __global__ void __launch_bounds__(TPB) k_mpnn_resid(DMat A, const double* __rest
     if (threadIdx.x == 0) atomicAdd(acc, sm[0]);
 }
 
-/// the output gradient dL/dh_i = s g_i wout with g = 2 A res / |r|^2, and the
-/// wout gradient sum_i s g_i h_i
+/// the output gradient dL/dh_i = s g_i wout with g = 2 A res / rr (rr: |r|^2
+/// for the residual loss, t.At for the energy-norm loss), and the wout
+/// gradient sum_i s g_i h_i
 template <int W>
 __global__ void __launch_bounds__(kWarps * 32) k_mpnn_out_bwd(DMat A, const double* __restrict__ val,
                                                               const double* __restrict__ res, const double* s,
+                                                              const double* rrp,
                                                               const __nv_bfloat16* __restrict__ wout,
                                                               const float* __restrict__ h, float* __restrict__ dh,
                                                               float* __restrict__ gwout)
@@ -200,7 +273,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_out_bwd(DMat A, const doub
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const float w = __bfloat162float(wout[lane]);
-    const double sc = s[0], rr = s[2];
+    const double sc = s[0], rr = *rrp;
     const int warp = blockIdx.x * kWarps + (threadIdx.x >> 5), nw = gridDim.x * kWarps;
     float acc = 0.f;
     const double* xs[1] = {res};
@@ -254,8 +327,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer_bwd(DMat A, const do
     for (int i = warp; i < A.n; i += nw)
     {
         const size_t o = static_cast<size_t>(i) * H + lane;
-        const float h = hin[o];
-        const float m = message(A, val, diag, hin, i, lane);
+        // the operands the forward multiplied: h and m rounded to BF16
+        const float h = bf16r(hin[o]);
+        const float m = bf16r(message(A, val, diag, hin, i, lane));
         const float d = (mask[i] >> lane) & 1u ? dh[o] : 0.f;
         rb += d;
         float at = 0.f, bt = 0.f;
@@ -441,6 +515,7 @@ struct MpnnState
     float *h = nullptr, *dh0 = nullptr, *dh1 = nullptr, *v = nullptr;  // h: (L+1) n H
     unsigned* mask = nullptr;                                         // (L+1) n
     double *s = nullptr, *res = nullptr, *acc = nullptr;
+    double *ae = nullptr, *at = nullptr;  // A e and A t of the energy-norm loss
     int step = 0;
 };
 
@@ -481,6 +556,8 @@ void Ctx::mpnnCreate(int layers, uint64_t seed)
     m->mask = alloc<unsigned>(static_cast<size_t>(layers + 1) * m->n);
     m->s = alloc<double>(4);
     m->res = alloc<double>(m->n);
+    m->ae = alloc<double>(m->n);
+    m->at = alloc<double>(m->n);
     m->acc = alloc<double>(1);
     launchCheck("mpnn_init");
     mpnn_.reset(m.release());
@@ -521,8 +598,11 @@ void Ctx::mpnnApply(const double* vals, const double* diag, const double* r, dou
     launchCheck("mpnn_apply", 3 + m.L);
 }
 
-/// loss |A M(r) - r|^2 / |r|^2 and its gradient (into m.g) for one sample
-double Ctx::mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z)
+/// One sample's loss and its gradient (into m.g).  Without a target t: the
+/// residual loss |A M(r) - r|^2 / |r|^2.  With t, the converged correction
+/// for the residual r (A t = r): the energy-norm loss e.Ae / t.At with
+/// e = M(r) - t -- the error CG itself minimises.
+double Ctx::mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z, const double* t)
 {
     MpnnState& m = *mpnn_;
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
@@ -532,24 +612,41 @@ double Ctx::mpnnLossGrad(const double* vals, const double* diag, const double* r
     mpnnApply(vals, diag, r, z);
     CFG_CUDA(cudaMemsetAsync(m.acc, 0, sizeof(double), stream_));
     CFG_CUDA(cudaMemsetAsync(m.g, 0, m.P * sizeof(float), stream_));
+    const double* rrp = m.s + 2;
+    double eAe = 0, tAt = 0;
+    if (t)
+    {
+        // e = z - t, Ae, At, e.Ae and t.At (on the device for the gradient)
+        k_fcg_p<<<GS_, TPB, 0, stream_>>>(n, z, 0.0, m.res);
+        k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, -1.0, t, m.res);
+        fcgSpmv(vals, m.res, m.ae);
+        fcgSpmv(vals, t, m.at);
+        const double* a[2] = {m.res, t};
+        const double* b[2] = {m.ae, m.at};
+        double d[3];
+        fcgDots(2, a, b, d);
+        eAe = d[0];
+        tAt = d[1];
+        rrp = fcgOut_ + 1;
+    }
     {
         const int W = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
         if (W == 7)
         {
-            k_mpnn_resid<7><<<GS_, TPB, 0, stream_>>>(A, vals, z, r, m.res, m.acc);
-            k_mpnn_out_bwd<7><<<blocks, kWarps * 32, 0, stream_>>>(A, vals, m.res, m.s, m.wb + offLayer(m.L),
+            if (!t) k_mpnn_resid<7><<<GS_, TPB, 0, stream_>>>(A, vals, z, r, m.res, m.acc);
+            k_mpnn_out_bwd<7><<<blocks, kWarps * 32, 0, stream_>>>(A, vals, m.res, m.s, rrp, m.wb + offLayer(m.L),
                                                                    m.h + m.L * nH, m.dh0, m.g + offLayer(m.L));
         }
         else if (W == 16)
         {
-            k_mpnn_resid<16><<<GS_, TPB, 0, stream_>>>(A, vals, z, r, m.res, m.acc);
-            k_mpnn_out_bwd<16><<<blocks, kWarps * 32, 0, stream_>>>(A, vals, m.res, m.s, m.wb + offLayer(m.L),
+            if (!t) k_mpnn_resid<16><<<GS_, TPB, 0, stream_>>>(A, vals, z, r, m.res, m.acc);
+            k_mpnn_out_bwd<16><<<blocks, kWarps * 32, 0, stream_>>>(A, vals, m.res, m.s, rrp, m.wb + offLayer(m.L),
                                                                     m.h + m.L * nH, m.dh0, m.g + offLayer(m.L));
         }
         else
         {
-            k_mpnn_resid<0><<<GS_, TPB, 0, stream_>>>(A, vals, z, r, m.res, m.acc);
-            k_mpnn_out_bwd<0><<<blocks, kWarps * 32, 0, stream_>>>(A, vals, m.res, m.s, m.wb + offLayer(m.L),
+            if (!t) k_mpnn_resid<0><<<GS_, TPB, 0, stream_>>>(A, vals, z, r, m.res, m.acc);
+            k_mpnn_out_bwd<0><<<blocks, kWarps * 32, 0, stream_>>>(A, vals, m.res, m.s, rrp, m.wb + offLayer(m.L),
                                                                    m.h + m.L * nH, m.dh0, m.g + offLayer(m.L));
         }
     }
@@ -565,6 +662,7 @@ double Ctx::mpnnLossGrad(const double* vals, const double* diag, const double* r
     }
     k_mpnn_enc_bwd<<<blocks, kWarps * 32, 0, stream_>>>(n, r, m.s + 1, m.mask, dh, m.g);
     launchCheck("mpnn_backward", 3 + 2 * m.L);
+    if (t) return tAt > 0 ? eAe / tAt : 0.0;
     double h[3];
     CFG_CUDA(cudaMemcpyAsync(h, m.acc, sizeof(double), cudaMemcpyDeviceToHost, stream_));
     CFG_CUDA(cudaMemcpyAsync(h + 1, m.s + 2, sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -590,14 +688,20 @@ void Ctx::mpnnMatrix(const double** vals, const double** diag) const
     *diag = pDiag_;
 }
 
-double Ctx::mpnnLossGradHost(const double* r, float* grad)
+double Ctx::mpnnLossGradHost(const double* r, float* grad, const double* t)
 {
     if (!mpnn_) fail(CFG_EINVAL, "mpnn: call cfg_mpnn_create first");
     CFG_CUDA(cudaSetDevice(device_));
     const double *vals, *diag;
     mpnnMatrix(&vals, &diag);
     toDevCells(cr_, r, 1, 0);
-    const double loss = mpnnLossGrad(vals, diag, cr_, cz_);
+    double* td = nullptr;
+    if (t)
+    {
+        td = bt_.c[2];  // free outside the momentum solve
+        toDevCells(td, t, 1, 0);
+    }
+    const double loss = mpnnLossGrad(vals, diag, cr_, cz_, td);
     if (grad)
     {
         CFG_CUDA(cudaMemcpyAsync(grad, mpnn_->g, mpnn_->P * sizeof(float), cudaMemcpyDeviceToHost, stream_));
@@ -618,8 +722,10 @@ void Ctx::mpnnApplyHost(const double* r, double* z)
 }
 
 /// Adam over `nSamples` residual samples (device, nSamples x nC, device
-/// numbering) for `epochs` passes; losses[e] = the epoch's mean loss
-void Ctx::mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses)
+/// numbering), with their converged corrections when `targets` is given,
+/// for `epochs` passes; losses[e] = the epoch's mean loss
+void Ctx::mpnnTrain(const double* samples, int nSamples, int epochs, float lr, double* losses,
+                    const double* targets)
 {
     if (!mpnn_) fail(CFG_EINVAL, "mpnn: call cfg_mpnn_create first");
     const double *vals, *diag;
@@ -630,7 +736,7 @@ void Ctx::mpnnTrain(const double* samples, int nSamples, int epochs, float lr, d
         double sum = 0;
         for (int k = 0; k < nSamples; ++k)
         {
-            sum += mpnnLossGrad(vals, diag, samples + k * n, cz_);
+            sum += mpnnLossGrad(vals, diag, samples + k * n, cz_, targets ? targets + k * n : nullptr);
             mpnnAdam(lr);
         }
         if (losses) losses[e] = sum / std::max(1, nSamples);
@@ -638,31 +744,68 @@ void Ctx::mpnnTrain(const double* samples, int nSamples, int epochs, float lr, d
     CFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Ctx::mpnnTrainHost(const double* samples, int nSamples, int epochs, float lr, double* losses)
+void Ctx::mpnnTrainHost(const double* samples, int nSamples, int epochs, float lr, double* losses,
+                        const double* targets)
 {
     if (!mpnn_) fail(CFG_EINVAL, "mpnn: call cfg_mpnn_create first");
     if (nSamples <= 0 || epochs <= 0) fail(CFG_EINVAL, "mpnn: no samples or epochs");
     CFG_CUDA(cudaSetDevice(device_));
     const size_t n = static_cast<size_t>(dm_.nC);
-    double* d = alloc<double>(n * nSamples);  // released with the context
+    // the training set on the device, kept across calls when it fits
+    const size_t need = n * nSamples * (targets ? 2 : 1);
+    if (need > trainCap_)
+    {
+        trainBuf_ = alloc<double>(need);  // released with the context
+        trainCap_ = need;
+    }
+    double* d = trainBuf_;
     for (int k = 0; k < nSamples; ++k) toDevCells(d + k * n, samples + k * n, 1, 0);
-    mpnnTrain(d, nSamples, epochs, lr, losses);
+    double* t = nullptr;
+    if (targets)
+    {
+        t = d + n * nSamples;
+        for (int k = 0; k < nSamples; ++k) toDevCells(t + k * n, targets + k * n, 1, 0);
+    }
+    mpnnTrain(d, nSamples, epochs, lr, losses, t);
 }
 
 void Ctx::mpnnCollect(int mode, int maxSamples)
 {
-    if (mode == 2) collected_.clear();
+    if (mode == 2)
+    {
+        collected_.clear();
+        collectedT_.clear();
+    }
     collectOn_ = mode != 0;
     collectMax_ = std::max(0, maxSamples);
 }
 
+/// Training on the collected pairs: the residual each pressure solve started
+/// from and the correction the plain solver converged to from there.
 void Ctx::mpnnTrainCollected(int epochs, float lr, double* losses)
 {
     if (collected_.empty()) fail(CFG_EINVAL, "mpnn: no collected samples");
     const size_t n = static_cast<size_t>(dm_.nC);
-    std::vector<double> all(collected_.size() * n);
-    for (size_t k = 0; k < collected_.size(); ++k) std::copy(collected_[k].begin(), collected_[k].end(), all.begin() + k * n);
-    mpnnTrainHost(all.data(), static_cast<int>(collected_.size()), epochs, lr, losses);
+    const size_t k = collected_.size();
+    std::vector<double> all(k * n), tgt(k * n);
+    for (size_t j = 0; j < k; ++j)
+    {
+        std::copy(collected_[j].begin(), collected_[j].end(), all.begin() + j * n);
+        std::copy(collectedT_[j].begin(), collectedT_[j].end(), tgt.begin() + j * n);
+    }
+    mpnnTrainHost(all.data(), static_cast<int>(k), epochs, lr, losses, tgt.data());
+}
+
+/// The network's initial guess: x += M(b - A x).
+void Ctx::mpnnGuess(const double* vals, const double* diag, const double* b, double* x)
+{
+    const int n = dm_.nC;
+    fcgSpmv(vals, x, cAp_);
+    CFG_CUDA(cudaMemcpyAsync(cr_, b, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, -1.0, cAp_, cr_);
+    mpnnApply(vals, diag, cr_, cz_);
+    k_fcg_axpy<<<GS_, TPB, 0, stream_>>>(n, 1.0, cz_, x);
+    launchCheck("mpnn_guess", 2);
 }
 
 void Ctx::poissonResidual(const double* b, const double* x, double* r)

@@ -1841,13 +1841,23 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
         {
             CFG_CUDA(cudaMemcpyAsync(pRhs_, pBase_, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
         }
-        if (collectOn_ && pass == 0 && static_cast<int>(collected_.size()) < collectMax_)
+        // a training pair of the learned preconditioner: the residual this
+        // solve starts from, and (below) the correction it converges to
+        const bool collect = collectOn_ && pass == 0 && static_cast<int>(collected_.size()) < collectMax_;
+        std::vector<double> x0;
+        if (collect)
         {
-            // a training sample of the learned preconditioner: the residual
-            // this solve starts from
             std::vector<double> r(static_cast<size_t>(n));
             mpnnResidualHost(pVal_d_, pRhs_, px_, r.data());
             collected_.push_back(std::move(r));
+            x0.resize(static_cast<size_t>(n));
+            fromDevCells(x0.data(), px_, 1, 0);
+        }
+        if (pass == 0 && (precond == CFG_PRECOND_MPNN || precond == CFG_PRECOND_AMG_MPNN))
+        {
+            // the network's initial guess from the residual of the given one
+            if (!mpnn_) fail(CFG_ESETUP, "pressure: the learned preconditioner needs cfg_mpnn_create");
+            mpnnGuess(pVal_d_, pDiag_, pRhs_, px_);
         }
         cfg_solver_report rep;
         if (precond == CFG_PRECOND_DIC) runDICCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
@@ -1859,7 +1869,7 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
             rep.iterations = static_cast<int32_t>(o[0] + o[1]);
             lastFallbackIters += o[1];
         }
-        else if (precond == CFG_PRECOND_AMG)
+        else if (precond == CFG_PRECOND_AMG || precond == CFG_PRECOND_AMG_MPNN)
         {
             // the FP32 AMG hierarchy follows this outer iteration's matrix
             if (pass == 0)
@@ -1873,8 +1883,31 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
             }
             amgFcg(pVal_d_, pRhs_, px_, tol, maxIter, 0, &rep);
         }
+        else if (precond == CFG_PRECOND_IR32)
+        {
+            if (devLoop_) fail(CFG_EINVAL, "pressure: the mixed-precision refinement is host driven");
+            if (pass == 0)
+            {
+                // the FP32 copy of this outer iteration's matrix and its FP32 DIC factor
+                ensureMixed();
+                const int nE = nSlicesEntries_;
+                k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, pVal_d_, pVal32_);
+                k_to_float<<<G_, TPB, 0, stream_>>>(n, pDiag_, pDiag32_);
+                launchCheck("ir32_float", 2);
+                dicSetupT<float>(dic32_, pVal_d_, pDiag32_);
+                amgFresh_ = false;  // pVal32_ now holds this matrix
+            }
+            runIR32(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, 1e-4, &rep);
+        }
         else runCG(pVal_d_, pDiag_, pRhs_, px_, tol, maxIter, &rep);
         inner += rep.iterations;
+        if (collect)
+        {
+            std::vector<double> x1(static_cast<size_t>(n));
+            fromDevCells(x1.data(), px_, 1, 0);
+            for (size_t i = 0; i < x1.size(); ++i) x1[i] -= x0[i];
+            collectedT_.push_back(std::move(x1));
+        }
     }
 }
 
@@ -2444,37 +2477,96 @@ void Ctx::gradient(const double* data, const double* bvals, int scheme, int volQ
     for (int q = 0; q < 3; ++q) fromDevCells(out, gPF_.c[q], 3, q);
 }
 
+/// The FP32 copies of the pressure system and the vectors of its FP32
+/// solves (mixed-precision refinement), allocated on first use.
+void Ctx::ensureMixed()
+{
+    if (mixedReady_) return;
+    const int nC = dm_.nC;
+    if (!pVal32_) pVal32_ = alloc<float>(static_cast<size_t>(nSlicesEntries_));
+    pDiag32_ = alloc<float>(nC);
+    r32_ = alloc<float>(nC);
+    p32_ = alloc<float>(nC);
+    Ap32_ = alloc<float>(nC);
+    z32_ = alloc<float>(nC);
+    e32_ = alloc<float>(nC);
+    b32_ = alloc<float>(nC);
+    dic32_.nColours = dic_.nColours;
+    dic32_.rows = dic_.rows;
+    dic32_.lStart = dic_.lStart;
+    dic32_.lCol = dic_.lCol;
+    dic32_.lSrc = dic_.lSrc;
+    dic32_.uStart = dic_.uStart;
+    dic32_.uCol = dic_.uCol;
+    dic32_.uSrc = dic_.uSrc;
+    dic32_.lVal = alloc<float>(nLo_);
+    dic32_.uVal = alloc<float>(nUp_);
+    dic32_.rD = alloc<float>(nC);
+    dic32_.rDinv = alloc<float>(nC);
+    mixedReady_ = true;
+}
+
+/// FP32 DIC-PCG corrections inside FP64 iterative refinement, on the
+/// pressure system whose FP32 copy and FP32 DIC factor are current: each
+/// refinement step computes r = b - A x and the reference's test |r|inf /
+/// |b|inf < tol in FP64 (Matrix.cpp:166-180), solves A32 e = r32 in FP32 to
+/// innerTol (2-norm relative), and adds e to x in FP64.  rep counts the
+/// inner iterations (at most maxIter over all steps).
+void Ctx::runIR32(const double* vals, const double* diag, const double* b, double* x, double tol, int maxIter,
+                  double innerTol, cfg_solver_report* rep)
+{
+    const int nC = dm_.nC;
+    const DMat A{nC, dm_.mStart, dm_.mCol};
+    int64_t inner = 0;
+    int outer = 0;
+    double init = -1.0, fin = 0.0;
+    bool conv = false;
+    for (;;)
+    {
+        SolveState s0{};
+        s0.tol = tol;
+        s0.maxIter = 0;
+        s0.normType = 0;
+        CFG_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+        dispatchW(maxW_, [&](auto Wc) {
+            constexpr int W = decltype(Wc)::value;
+            k_cg_init<W, double><<<GS_, TPB, 0, stream_>>>(A, vals, diag, b, x, cr_, cz_, partials_, st_);
+        });
+        launchCheck("ir_residual");
+        CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+        fin = stHost_->init[0];
+        if (init < 0) init = fin;
+        conv = stHost_->conv[0] != 0;
+        if (conv || std::isnan(fin) || inner >= maxIter || outer >= 64) break;
+        k_to_float<<<G_, TPB, 0, stream_>>>(nC, cr_, b32_);
+        CFG_CUDA(cudaMemsetAsync(e32_, 0, nC * sizeof(float), stream_));
+        cfg_solver_report r2{};
+        dicCGT<float>(dic32_, pVal32_, pDiag32_, b32_, e32_, r32_, p32_, Ap32_, z32_, innerTol,
+                      static_cast<int>(std::min<int64_t>(2000, maxIter - inner)), 1, &r2);
+        k_add_f32<<<G_, TPB, 0, stream_>>>(nC, e32_, x);
+        launchCheck("ir_update");
+        inner += r2.iterations;
+        ++outer;
+        if (r2.iterations == 0) break;  // no progress in FP32
+    }
+    rep->iterations = static_cast<int32_t>(inner);
+    rep->converged = conv;
+    rep->initial_residual = init;
+    rep->final_residual = fin;
+}
+
 void Ctx::poissonSetup(int64_t refCell)
 {
     CFG_CUDA(cudaSetDevice(device_));
     refreshBc();
     const int nC = dm_.nC, nF = dm_.nF;
     if (refCell >= nC) fail(CFG_EINVAL, "cfg_poisson_setup: reference cell beyond the last cell");
+    ensureMixed();
     if (!poissonReady_)
     {
-        const size_t nE = static_cast<size_t>(nSlicesEntries_);
-        pVal32_ = alloc<float>(nE);
-        pDiag32_ = alloc<float>(nC);
-        r32_ = alloc<float>(nC);
-        p32_ = alloc<float>(nC);
-        Ap32_ = alloc<float>(nC);
-        z32_ = alloc<float>(nC);
-        e32_ = alloc<float>(nC);
-        b32_ = alloc<float>(nC);
         pb64_ = alloc<double>(nC);
         px64_ = alloc<double>(nC);
-        dic32_.nColours = dic_.nColours;
-        dic32_.rows = dic_.rows;
-        dic32_.lStart = dic_.lStart;
-        dic32_.lCol = dic_.lCol;
-        dic32_.lSrc = dic_.lSrc;
-        dic32_.uStart = dic_.uStart;
-        dic32_.uCol = dic_.uCol;
-        dic32_.uSrc = dic_.uSrc;
-        dic32_.lVal = alloc<float>(nLo_);
-        dic32_.uVal = alloc<float>(nUp_);
-        dic32_.rD = alloc<float>(nC);
-        dic32_.rDinv = alloc<float>(nC);
         poissonReady_ = true;
     }
     // unit face coefficient, no flux: laplacianFace(1) and the p conditions

@@ -60,12 +60,28 @@ enum cfg_div_scheme { CFG_DIV_UPWIND = 0, CFG_DIV_LINEAR = 1, CFG_DIV_BLEND = 2,
 enum cfg_lin_method { CFG_SOLVE_CG = 0, CFG_SOLVE_BICGSTAB = 1 };
 /* pressure preconditioner: the reference's Jacobi PCG, or this library's
  * multicolour DIC (no reference counterpart) */
-enum cfg_precond { CFG_PRECOND_JACOBI = 0, CFG_PRECOND_DIC = 1, CFG_PRECOND_MPNN = 2, CFG_PRECOND_AMG = 3 };
+enum cfg_precond
+{
+    CFG_PRECOND_JACOBI = 0,
+    CFG_PRECOND_DIC = 1,
+    CFG_PRECOND_MPNN = 2,
+    CFG_PRECOND_AMG = 3,
+    CFG_PRECOND_IR32 = 4,
+    CFG_PRECOND_AMG_MPNN = 5
+};
 /* CFG_PRECOND_MPNN: flexible CG with the learned preconditioner (cfg_mpnn_*),
  * the reference's infinity-norm test, FP64 DIC-PCG when it stalls.
  * CFG_PRECOND_AMG: FP64 flexible CG, device-resident, preconditioned by an
  * FP32 aggregation-AMG V-cycle rebuilt from each outer iteration's matrix
- * (hierarchy structure once per context), the reference's infinity-norm test */
+ * (hierarchy structure once per context), the reference's infinity-norm test.
+ * CFG_PRECOND_IR32: mixed precision -- the matrix rounded to FP32 each outer
+ * iteration, FP32 multicolour DIC-PCG corrections (to 1e-4 relative) inside
+ * an FP64 iterative refinement whose residual b - A x and infinity-norm test
+ * (Matrix.cpp:166-180) are FP64; the inner iterations are what is counted.
+ * CFG_PRECOND_MPNN and CFG_PRECOND_AMG_MPNN start each pressure solve from
+ * the network's initial guess x0 + M(b - A x0), then iterate with flexible
+ * CG preconditioned by the network (MPNN) or by the FP32 AMG V-cycle
+ * (AMG_MPNN). */
 
 /* Schemes (src/3d/include/cf/fvm/FvMatrix.h:30-38) */
 typedef struct cfg_schemes
@@ -501,6 +517,15 @@ int cfg_mpnn_apply(cfg_ctx* ctx, const double* r, double* z);
 /* Adam (lr) over n_samples residual samples (n_samples x nCells, original
  * order), `epochs` passes; losses[epoch] = mean loss (may be NULL). */
 int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t n_samples, int32_t epochs, float lr, double* losses);
+/* The same on (residual, converged correction) pairs: r_k the residual a
+ * pressure solve starts from, t_k the correction the plain solver converged
+ * to from there (A t_k = r_k); the loss is the energy-norm error
+ * e.Ae / t.At with e = M(r) - t, the error CG minimises.  targets has the
+ * layout of samples.  cfg_mpnn_loss_grad_pair gives one pair's loss and
+ * gradient. */
+int cfg_mpnn_train_pairs(cfg_ctx* ctx, const double* samples, const double* targets, int32_t n_samples,
+                         int32_t epochs, float lr, double* losses);
+int cfg_mpnn_loss_grad_pair(cfg_ctx* ctx, const double* r, const double* t, double* loss, float* grad);
 /* Keep (on = 1) up to max_samples of the residuals the SIMPLE / PISO
  * pressure solves start from (b - A x0 of their first pass, original
  * order) as training samples; on = 2 first drops those kept; on = 0 stops.

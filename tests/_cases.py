@@ -143,6 +143,60 @@ def channel_case(nx, ny, nz, jitter=0.1, seed=5, nu=1e-3, iters=4, linear_tol=1e
                   linear_tol=linear_tol, non_orth=non_orth, relax_u=0.9, relax_p=0.03, p_relax_start=0.02)
 
 
+def poiseuille_dict(nx=100, ny=20, length=4.0, height=0.2, depth=0.1, u_mean=0.1, nu=0.01, iters=300):
+    """The reference's verification channel (tests/cases/poiseuilleChannel,
+    checked by tests/check_poiseuille.py): a planar nx x ny x 1 channel,
+    uniform inlet, fixed-p outlet, no-slip top and bottom, symmetry front and
+    back, run to the outer stop of its simple{} settings."""
+    return f"""block
+{{
+    min (0 0 0);
+    max ({length!r} {height!r} {depth!r});
+    cells ({nx} {ny} 1);
+    xmin {{ name inlet; type inlet; }}
+    xmax {{ name outlet; type outlet; }}
+    ymin {{ name bottom; type wall; }}
+    ymax {{ name top; type wall; }}
+    zmin {{ name front; type symmetry; }}
+    zmax {{ name back; type symmetry; }}
+}}
+nu {nu!r};
+patches
+{{
+    inlet  {{ U ({u_mean!r} 0 0); UType fixedValue; pType zeroGradient; }}
+    outlet {{ UType zeroGradient; p 0; pType fixedValue; }}
+    bottom {{ U (0 0 0); UType fixedValue; pType zeroGradient; }}
+    top    {{ U (0 0 0); UType fixedValue; pType zeroGradient; }}
+}}
+schemes {{ ddt steady; div upwind; laplacian corrected; grad corrected; }}
+simple
+{{
+    maxIterations {iters};
+    continuityTol 1e-6;
+    pcorrTol 1e-4;
+    momentumTol 1e-4;
+    relaxU 0.9;
+    relaxP 0.03;
+    pRelaxStart 0.02;
+}}
+"""
+
+
+def poiseuille_bands(C, U, height=0.2, u_mean=0.1, x_dev=3.0, x_col=3.5, dx=0.04):
+    """check_poiseuille.py's verdict on the developed region (cell centres
+    past x_dev): max |v|, the largest deviation from the parabola
+    1.5 u_mean (1 - ((y - h/2) / (h/2))^2), the centreline speed, and the
+    flux of the one cell column at x_col against u_mean h."""
+    dev = C[:, 0] > x_dev
+    y = C[dev, 1]
+    exact = 1.5 * u_mean * (1.0 - ((y - height / 2) / (height / 2)) ** 2)
+    col = np.abs(C[:, 0] - x_col) < 0.125 * dx
+    ny = int(col.sum())
+    flux = float((U[col, 0] * (height / ny)).sum())
+    return {"v_max": float(np.abs(U[dev, 1]).max()), "profile_err": float(np.abs(U[dev, 0] - exact).max()),
+            "centreline": float(U[dev, 0].max()), "flux_err": abs(flux / (u_mean * height) - 1.0), "column": ny}
+
+
 def channel_dict(nx, ny, nz, nu=1e-3, iters=4, linear_tol=1e-10, non_orth=2, L=(1.0, 0.2, 0.2)):
     sides = "\n".join(f"    {s} {{ name {n}; type {t}; }}" for s, n, t in zip(SIDES, CHANNEL_NAMES, CHANNEL_TYPES))
     return f"""block

@@ -19,8 +19,10 @@ Fixtures (small .npz files):
   eqns_cavity.npz          the assembly probes of one outer iteration (eqns mode)
   solve_cg.npz, solve_bicgstab.npz   one CSR solve each
   piso_channel.npz         16x6x6 jittered channel: 4 transient PISO steps (dt 0.05, 2 correctors)
-  simple_channel40.npz     the 16,000-cell channel: 20 reference iterations, and 20 with linear-upwind,
-                           Gauss linear and DIC-PCG by the C restatement (checksums, samples)
+  simple_channel40.npz     the 16,000-cell channel: all 300 reference iterations, and 20 with
+                           linear-upwind, Gauss linear and DIC-PCG by the C restatement (checksums, samples)
+  poiseuille.npz           the reference's verification channel (100x20x1, K.poiseuille_dict) run by the
+                           reference to its own outer stop: iterations and the whole U, p, phi
   simple_cavity128.npz     the 2M-cell bench cavity (pinned, so by the C restatement): checksums and
                            4096 seeded cell/face samples after one outer iteration
   vtk_cavity.npz           the reference's VtkWriter output (ASCII .vtu) of a jittered 3x3x2 cavity
@@ -36,8 +38,9 @@ Fixtures (small .npz files):
   piso_rans_keps.npz, piso_rans_sst.npz   the same channel stepped by the reference's PISO
                            (4 steps, dt 0.05) with k-epsilon and with k-omega SST
 
-`python tests/golden/make_golden.py coupled` (or `rans`) rebuilds only the coupled (or the
-three extra RANS) fixtures.
+`python tests/golden/make_golden.py coupled` (or `rans`, `channel40`, `poiseuille`) rebuilds
+only the coupled (or the three extra RANS, the 16,000-cell channel, the verification channel)
+fixtures.
 """
 import os
 import subprocess
@@ -216,18 +219,19 @@ def cavity128_npz(name, n=128, iters=1, linear_tol=1e-11):
     print("wrote", name, r.iterations, r.uItersTotal, r.pItersTotal)
 
 
-def channel40_npz(name, iters=20):
+def channel40_npz(name, iters=300, lu_iters=20):
     """The 40x20x20 channel (2 x 0.1 x 0.1 m, inlet 0.1 m/s, nu 1e-4, the
     reference's stable relaxation 0.9 / 0.03 / pRelaxStart 0.02, nonOrth 2):
-    the reference's own run, checksums and seeded samples; and the same case
-    with linear-upwind convection, Gauss linear gradients and DIC-PCG by the
-    C restatement (no reference counterpart)."""
+    the reference's own run of all 300 outer iterations, checksums and seeded
+    samples; and lu_iters iterations of the same case with linear-upwind
+    convection, Gauss linear gradients and DIC-PCG by the C restatement (no
+    reference counterpart)."""
     text = K.channel_dict(40, 20, 20, nu=1e-4, iters=iters, L=(2.0, 0.1, 0.1))
     m = K._block((0, 0, 0), (2.0, 0.1, 0.1), (40, 20, 20), K.CHANNEL_NAMES, K.CHANNEL_TYPES, 0.0, 0)
     rng = np.random.default_rng(40)
     cells = np.sort(rng.choice(m.nC, 2048, replace=False))
     faces = np.sort(rng.choice(m.nF, 2048, replace=False))
-    out = {"cells": cells, "faces": faces, "iters": iters}
+    out = {"cells": cells, "faces": faces, "iters": iters, "lu_iters": lu_iters}
     with tempfile.TemporaryDirectory() as td:
         cp = os.path.join(td, "case.dict")
         open(cp, "w").write(text)
@@ -240,7 +244,7 @@ def channel40_npz(name, iters=20):
                ref_U_cells=U[cells], ref_p_cells=p[cells], ref_phi_faces=phi[faces])
     c = O.Case(m, u_type=["fixedValue", "zeroGradient"] + ["fixedValue"] * 4,
                u_value=[(0.1, 0, 0)] + [(0, 0, 0)] * 5, p_type=["zeroGradient", "fixedValue"] + ["zeroGradient"] * 4,
-               p_value=[0] * 6, nu=1e-4, max_iterations=iters, linear_tol=1e-8, non_orth=2, relax_u=0.7,
+               p_value=[0] * 6, nu=1e-4, max_iterations=lu_iters, linear_tol=1e-8, non_orth=2, relax_u=0.7,
                relax_p=0.3, p_relax_start=0.02, div="linearUpwind", grad="linear")
     c.p_precond = 1
     U, p, phi, r = c.run()
@@ -248,6 +252,23 @@ def channel40_npz(name, iters=20):
                lu_p_sum=p.sum(), lu_U_cells=U[cells], lu_p_cells=p[cells], lu_phi_faces=phi[faces])
     np.savez_compressed(os.path.join(HERE, name), **out)
     print("wrote", name, res[:2], r.iterations)
+
+
+def poiseuille_npz(name):
+    """The reference's verification channel (K.poiseuille_dict) run by the
+    reference to its own outer stop: iterations, convergence and the whole
+    U, p, phi."""
+    with tempfile.TemporaryDirectory() as td:
+        cp = os.path.join(td, "case.dict")
+        open(cp, "w").write(K.poiseuille_dict())
+        O.ref_run(["simple", cp, td])
+        res = open(os.path.join(td, "result.txt")).read().split()
+        U = O.read(os.path.join(td, "U.f64"), shape=(-1, 3))
+        p = O.read(os.path.join(td, "p.f64"))
+        phi = O.read(os.path.join(td, "phi.f64"))
+    np.savez_compressed(os.path.join(HERE, name), iterations=int(res[0]), continuity=float(res[1]),
+                        momentum=float(res[2]), converged=int(res[3]), U=U, p=p, phi=phi)
+    print("wrote", name, res[:4])
 
 
 def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
@@ -309,6 +330,12 @@ def main():
     if sys.argv[1:] == ["rans"]:
         rans_fixtures()
         return
+    if sys.argv[1:] == ["channel40"]:
+        channel40_npz("simple_channel40.npz")
+        return
+    if sys.argv[1:] == ["poiseuille"]:
+        poiseuille_npz("poiseuille.npz")
+        return
     mesh_npz("mesh_block_2x2x2.npz", "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\n")
     mesh_npz("mesh_tets22.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeTets_22.msh"; }}\n', grad_fields=True)
     mesh_npz("mesh_hex41.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeHex_41.msh"; }}\n', grad_fields=True)
@@ -333,6 +360,7 @@ def main():
                                     f'outlet {{ type outlet; }} }} }}\n')
 
     channel40_npz("simple_channel40.npz")
+    poiseuille_npz("poiseuille.npz")
     cavity128_npz("simple_cavity128.npz")
 
     vc = K.cavity_case(3, 3, 2)

@@ -191,7 +191,7 @@ def test_full_size_cavity_matches_oracle_checksums(golden):
     continuity, field checksums and 4096 seeded cell and face samples."""
     import bench
     g = golden("simple_cavity128.npz")
-    mesh, case, ctl = bench.make_case(int(g["n"]), 0, "Jacobi")
+    mesh, case, ctl = bench.make_cavity_case(int(g["n"]), 0, "Jacobi")
     assert np.array_equal(mesh.addressing()["points"].sum(0), g["points_sum"])
     ctl.max_iterations = int(g["iters"])
     ctl.linear_tol = float(g["linear_tol"])
@@ -230,8 +230,9 @@ def channel40_product(schemes=None):
 
 
 def test_config1_channel_matches_reference(golden):
-    """The 16,000-cell channel (40x20x20, 2 x 0.1 x 0.1 m, Re 100) for 20
-    iterations at the reference's stable relaxation, against its own run."""
+    """The 16,000-cell channel (40x20x20, 2 x 0.1 x 0.1 m, Re 100) for all
+    300 outer iterations of the workload at the reference's stable
+    relaxation, against its own run of them."""
     import chuanflow_b200 as cf
     g = golden("simple_channel40.npz")
     mesh, case = channel40_product()
@@ -253,10 +254,79 @@ def test_config1_linear_upwind_dic_matches_oracle(golden):
     import chuanflow_b200 as cf
     g = golden("simple_channel40.npz")
     mesh, case = channel40_product(cf.Schemes(div="linearUpwind", grad="linear"))
-    ctl = cf.SimpleControls(max_iterations=int(g["iters"]), relax_u=0.7, relax_p=0.3, p_relax_start=0.02,
+    ctl = cf.SimpleControls(max_iterations=int(g["lu_iters"]), relax_u=0.7, relax_p=0.3, p_relax_start=0.02,
                             non_orth_correctors=2, linear_tol=1e-8, nu=1e-4, p_preconditioner="DIC")
     r = case.solve(ctl)
     U, p, phi = case.download()
     assert r.iterations == int(g["lu_iterations"])
     assert rel(U[g["cells"]], g["lu_U_cells"]) < REL_TOL and rel(p[g["cells"]], g["lu_p_cells"]) < REL_TOL
     assert rel(phi[g["faces"]], g["lu_phi_faces"]) < REL_TOL
+
+
+def test_poiseuille_verification_case_converges_like_the_reference(golden, tmp_path):
+    """The reference's own converged-state check (tests/check_poiseuille.py
+    on tests/cases/poiseuilleChannel): its case file run end to end through
+    cfg_run_case_file to the outer stop of its simple{} block stops at the
+    reference's iteration, with U, p and phi within the FP64 bar of the
+    reference's run, and passes the check's bands -- |v| < 5e-3 downstream,
+    the parabola within 0.012, the centreline within 8% and the column flux
+    within 2%."""
+    import chuanflow_b200 as cf
+    g = golden("poiseuille.npz")
+    path = tmp_path / "case.dict"
+    path.write_text(K.poiseuille_dict())
+    res, counts, (U, p, phi) = cf.run_case_file(path, fields=True)
+    assert res.converged and not res.diverged
+    assert res.iterations == int(g["iterations"])
+    assert rel(U, g["U"]) < REL_TOL and rel(p, g["p"]) < REL_TOL and rel(phi, g["phi"]) < REL_TOL
+    mesh = cf.PolyMesh.block((0, 0, 0), (4.0, 0.2, 0.1), (100, 20, 1))
+    b = K.poiseuille_bands(mesh.geometry()["C"], U)
+    assert b["column"] == 20
+    assert b["v_max"] < 5e-3 and b["profile_err"] < 0.012
+    assert abs(b["centreline"] / 0.15 - 1.0) < 0.08 and b["flux_err"] < 0.02
+
+
+def test_headline_amg_pressure_fields_match_fp64_oracle():
+    """The headline's configuration (bench.make_case: the jittered channel,
+    the reference's channel relaxation, nonOrth 1, tolerance 1e-8) at 64 x 8
+    x 8 cells, with the FP32-AMG flexible-CG pressure solve, over 12 outer
+    iterations from rest, against the C restatement's FP64 DIC-PCG run of the
+    same iterations: every field within the FP64 bar (relative L2) and no
+    iteration diverged."""
+    import bench
+    n, iters = 8, 12
+    m = K._block((0, 0, 0), bench.LENGTH, bench.dims(n), K.CHANNEL_NAMES, K.CHANNEL_TYPES, bench.JITTER, bench.SEED)
+    oc = O.Case(m, u_type=["fixedValue", "zeroGradient"] + ["fixedValue"] * 4,
+                u_value=[(bench.U_IN, 0, 0)] + [(0, 0, 0)] * 5, p_type=["zeroGradient", "fixedValue"] +
+                ["zeroGradient"] * 4, p_value=[0] * 6, nu=bench.NU, max_iterations=iters, linear_tol=1e-8,
+                non_orth=1, **bench.RELAX)
+    oc.p_precond = 1
+    U0, p0, phi0, r0 = oc.run()
+    mesh, case, ctl = bench.make_case(n, 0, "AMG")
+    assert np.array_equal(mesh.addressing()["points"], m.points)
+    for k in range(iters):
+        r = case.solve(ctl)
+        assert not r.diverged, k
+    U, p, phi = case.download()
+    errs = {"U": rel(U, U0), "p": rel(p, p0), "phi": rel(phi, phi0)}
+    assert all(v < REL_TOL for v in errs.values()), errs
+
+
+def test_simple_cavity_mixed_precision_pressure_matches_fp64_oracle():
+    """SIMPLE with the mixed-precision pressure solve (the matrix rounded to
+    FP32, FP32 DIC-PCG corrections inside FP64 iterative refinement whose
+    residual and infinity-norm test are FP64) against the oracle's FP64
+    DIC run of the same outer iterations.  The refinement stops on the same
+    FP64 test, so every field stays within the FP64 bar; stated per field:
+    U, p and phi each within 1e-6 relative L2."""
+    oc = K.cavity_case(12, 11, 10, jitter=0.1, iters=6, linear_tol=1e-10, nu=0.0025)
+    oc.p_ref_cell = 0
+    oc.p_precond = 1
+    U0, p0, phi0, r0 = oc.run()
+    mesh, case = K.cavity_product(12, 11, 10, jitter=0.1)
+    res = case.solve(K.controls_from(oc, p_preconditioner="IR32"))
+    U, p, phi = case.download()
+    assert res.iterations == r0.iterations and not res.diverged
+    assert rel(U, U0) < 1e-6, rel(U, U0)
+    assert rel(p, p0) < 1e-6, rel(p, p0)
+    assert rel(phi, phi0) < 1e-6, rel(phi, phi0)

@@ -357,3 +357,16 @@ def test_gmsh_reader_outcomes_match_reference(tmp_path, case):
     for k in ("face_offsets", "face_verts", "owner", "points"):
         assert np.array_equal(a[k], r[k]), k
     assert [(n, t, s, z) for n, t, s, z in m.patches] == [(p[0], p[1], int(p[2]), int(p[3])) for p in r["patches"]]
+
+
+def test_poiseuille_fixture_passes_the_reference_check(golden):
+    """The reference's run of its verification channel (poiseuille.npz)
+    passes tests/check_poiseuille.py's bands as restated in
+    _cases.poiseuille_bands, so the GPU test's bands check the same thing."""
+    g = golden("poiseuille.npz")
+    assert int(g["converged"]) == 1
+    m = O.block_mesh((0, 0, 0), (4.0, 0.2, 0.1), (100, 20, 1))
+    b = K.poiseuille_bands(m.C, g["U"])
+    assert b["column"] == 20
+    assert b["v_max"] < 5e-3 and b["profile_err"] < 0.012
+    assert abs(b["centreline"] / 0.15 - 1.0) < 0.08 and b["flux_err"] < 0.02
