@@ -390,14 +390,15 @@ def main_reference(args, world, rank, dist):
 
 
 def main_transient(args, world, rank, local, dist):
-    """The learned preconditioner in a transient run: a 2D-extruded channel
-    (nx x nx/4 x 4 hex cells) with a square obstacle of a quarter of the
-    height, Re 200 on the obstacle, implicit-Euler PISO at CFL 0.5.  The
-    first 75% of the steps run with DIC-PCG pressure and keep (a spread of)
-    the residuals their pressure solves start from; the network trains on
-    them; the last 25% then run twice from the same fields -- DIC-PCG, and
-    flexible CG with the network (warm-started from the previous pressure,
-    DIC fallback) -- to the same 1e-8 test."""
+    """The learned part in a transient run: a 2D-extruded channel (nx x
+    nx/4 x 4 hex cells) with a square obstacle of a quarter of the height,
+    Re 200 on the obstacle, implicit-Euler PISO at CFL 0.5.  The first 75%
+    of the steps run with DIC-PCG pressure and keep (residual each pressure
+    solve starts from, correction it converges to) pairs; the network trains
+    on them in the energy norm; the last 25% then run four times from the
+    same fields -- DIC-PCG, the FP32-AMG flexible CG, the network's initial
+    guess followed by the AMG flexible CG, and the network's guess followed
+    by flexible CG with the network -- to the same 1e-8 test."""
     import chuanflow_b200 as cf
     from chuanflow_b200 import meshgen
     nx = args.transient_nx
@@ -427,13 +428,13 @@ def main_transient(args, world, rank, local, dist):
                           p_preconditioner="DIC")
     steps = args.transient_steps
     n_train = (3 * steps) // 4
-    every = max(1, n_train // 32)
+    every = max(1, n_train // args.train_pairs)
     case.mpnn_create(4, seed=3)
     t0 = time.perf_counter()
     for s in range(n_train):
-        case.mpnn_collect(2 if s == 0 else (1 if s % every == 0 else 0), 64)
+        case.mpnn_collect(2 if s == 0 else (1 if s % every == 0 else 0), args.train_pairs)
         case.piso_step(ctl)
-    case.mpnn_collect(0, 64)
+    n_pairs = case.mpnn_collect(0, args.train_pairs)
     sim_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     losses = case.mpnn_train_collected(args.train_epochs, 2e-3)
@@ -441,37 +442,62 @@ def main_transient(args, world, rank, local, dist):
     batch = cf.Batch([case])
     batch.save()
     legs = {}
-    for name, pre in (("dic64", "DIC"), ("amg32", "AMG"), ("learned_fcg", "MPNN")):
+    for name, pre in (("dic64", "DIC"), ("amg32", "AMG"), ("learned_guess_amg32", "AMG_MPNN"),
+                      ("learned_guess_fcg", "MPNN")):
         batch.restore()
         c2 = dataclasses.replace(ctl, p_preconditioner=pre)
-        ms, pit, fin = [], 0, None
+        ms, pit, fin, div = [], 0, None, 0
         for s in range(n_train, steps):
             r = case.piso_step(c2)
             ms.append(r["device_ms"])
             pit += r["p_inner_iterations"]
+            div += int(r.get("diverged", 0))
             fin = r
         U, p, phi = case.download()
         legs[name] = {"ms_per_step": statistics.mean(ms), "pressure_iterations_per_step": pit / max(1, len(ms)),
-                      "continuity_last": fin["continuity_error"], "U": U}
-    dU = float(np.linalg.norm(legs["learned_fcg"]["U"] - legs["dic64"]["U"]) / np.linalg.norm(legs["dic64"]["U"]))
-    dUa = float(np.linalg.norm(legs["amg32"]["U"] - legs["dic64"]["U"]) / np.linalg.norm(legs["dic64"]["U"]))
+                      "continuity_last": fin["continuity_error"], "diverged_steps": div, "U": U}
+    for k in legs:
+        if k != "dic64":
+            legs[k]["rel_L2_U_vs_dic64"] = float(np.linalg.norm(legs[k]["U"] - legs["dic64"]["U"]) /
+                                                 np.linalg.norm(legs["dic64"]["U"]))
     for v in legs.values():
         v.pop("U")
+    # the network's own cost on this mesh: one application, and one
+    # message-passing layer against its algorithmic bytes (state in, the
+    # neighbours' states as one stream, state out, mask; the matrix row; the
+    # diagonal)
+    app_ms, layer_ms = case.mpnn_time(20)
+    entries = mesh.n_cells + 2 * mesh.n_internal_faces
+    layer_bytes = mesh.n_cells * (3 * 128 + 4 + 8) + 12 * entries
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
     if rank == 0:
-        out = {"metric": "transient obstacle channel: device ms per PISO step, learned FCG vs DIC-PCG pressure",
-               "value": legs["learned_fcg"]["ms_per_step"], "unit": "ms", "n_gpus": world,
+        base = legs["amg32"]["ms_per_step"]
+        out = {"metric": "transient obstacle channel: device ms per PISO step, learned initial guess + FP32-AMG "
+                         "flexible CG vs the FP32-AMG flexible CG alone",
+               "value": legs["learned_guess_amg32"]["ms_per_step"], "unit": "ms", "n_gpus": world,
                "steps": steps - n_train, "warmup": n_train, "higher_is_better": False, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64 (network: bf16 weights, f32 activations)", "data": "synthetic",
+               "vs_baseline": None, "dtype": "f64 (network: bf16 weights and tensor-core operands, f32 accumulation)",
+               "data": "synthetic",
                "config": {"workload": f"2D-extruded channel {nx}x{ny}x4 hex with a square obstacle (blockage 0.25), "
                                       f"{ncell} cells, Re 200 on the obstacle, implicit Euler PISO (2 correctors) "
                                       f"at CFL 0.5 (dt {dt:g}), {steps} steps: the first {n_train} with DIC-PCG "
-                                      f"generate the training residuals, the rest are timed twice from the same "
+                                      f"generate the training pairs, the rest are timed four times from the same "
                                       f"fields", "cells": ncell},
-               "legs": legs, "rel_L2_U_learned_vs_dic": dU, "rel_L2_U_amg32_vs_dic": dUa,
-               "simulation_s_training_steps": sim_s,
-               "train_s": train_s, "train_loss_first": float(losses[0]), "train_loss_last": float(losses[-1]),
-               "speedup_learned_vs_dic": legs["dic64"]["ms_per_step"] / legs["learned_fcg"]["ms_per_step"],
-               "speedup_amg32_vs_dic": legs["dic64"]["ms_per_step"] / legs["amg32"]["ms_per_step"]}
+               "legs": legs, "simulation_s_training_steps": sim_s, "train_s": train_s,
+               "train_pairs": n_pairs,
+               "train_loss_first": float(losses[0]), "train_loss_last": float(losses[-1]),
+               "network": {"ms_per_application": app_ms, "layer_ms": layer_ms, "layer_alg_bytes": layer_bytes,
+                           "layer_achieved_gbs": layer_bytes / (layer_ms * 1e-3) / 1e9,
+                           "layer_frac_of_hbm_peak": layer_bytes / (layer_ms * 1e-3) / 1e9 / peak, "peak": peak},
+               "speedup_learned_guess_amg_vs_amg": base / legs["learned_guess_amg32"]["ms_per_step"],
+               "speedup_amg32_vs_dic": legs["dic64"]["ms_per_step"] / base,
+               "speedup_learned_guess_fcg_vs_dic": legs["dic64"]["ms_per_step"] /
+                                                   legs["learned_guess_fcg"]["ms_per_step"]}
         print(json.dumps(out), flush=True)
 
 
@@ -691,6 +717,7 @@ def main():
     ap.add_argument("--tet-n", type=int, default=84, help="poisson: lattice intervals per axis (6 n^3 tets)")
     ap.add_argument("--no-learned", action="store_true", help="poisson: skip the learned preconditioner")
     ap.add_argument("--train-epochs", type=int, default=30, help="poisson: training epochs of the network")
+    ap.add_argument("--train-pairs", type=int, default=64, help="transient: training pairs kept from the first 75%%")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup()
     if args.workload == "transient":

@@ -39,7 +39,7 @@ class _Controls(C.Structure):
                 ("non_orth_correctors", C.c_int32), ("relax_u", C.c_double), ("relax_p", C.c_double),
                 ("p_relax_start", C.c_double), ("body_force", C.c_double * 3), ("nu", C.c_double),
                 ("p_precond", C.c_int32), ("verbose", C.c_int32), ("p_ref_cell", C.c_int64),
-                ("p_ref_value", C.c_double)]
+                ("p_ref_value", C.c_double), ("dt", C.c_double), ("u_time_old", C.c_int32)]
 
 
 class _Result(C.Structure):
@@ -311,6 +311,8 @@ class SimpleControls:
     verbose: bool = False
     p_ref_cell: int = -1
     p_ref_value: float = 0.0
+    dt: float = 0.0          # SimpleControls::dt (pseudo-) time step; 0: steady
+    u_time_old: int = 0      # 1: the velocity at the start of the call is the old level
 
     def _c(self):
         c = _Controls()
@@ -331,6 +333,8 @@ class SimpleControls:
         c.verbose = int(self.verbose)
         c.p_ref_cell = self.p_ref_cell
         c.p_ref_value = self.p_ref_value
+        c.dt = self.dt
+        c.u_time_old = int(self.u_time_old)
         return c
 
 
@@ -691,6 +695,14 @@ def _mpnn_train_pairs(self, samples, targets, epochs=1, lr=1e-3):
     return losses
 
 
+def _mpnn_time(self, reps):
+    """(ms per application, ms per message-passing layer launch), CUDA
+    events, on the current pressure matrix."""
+    out = np.zeros(2)
+    _check(lib().cfg_mpnn_time(self._h, C.c_int32(reps), _dp(out)))
+    return float(out[0]), float(out[1])
+
+
 def _mpnn_apply(self, r):
     z = np.zeros(self.mesh.n_cells)
     _check(lib().cfg_mpnn_apply(self._h, _dp(_f64(r)), _dp(z)))
@@ -777,8 +789,9 @@ SimpleCase.write_vtu = _write_vtu
 SimpleCase.write_hdf5 = _write_hdf5
 SimpleCase.piso_step = _piso_step
 def _mpnn_collect(self, on=1, max_samples=64):
-    """Keep (1) / stop keeping (0) / drop and keep (2) the residuals later
-    pressure solves start from; returns the count kept."""
+    """Keep (1) / stop keeping (0) / drop and keep (2) training pairs of
+    later pressure solves (the residual each starts from and the correction
+    it converges to); returns the count kept."""
     n = C.c_int32()
     _check(lib().cfg_mpnn_collect(self._h, C.c_int32(int(on)), C.c_int32(max_samples), C.byref(n)))
     return n.value
@@ -799,6 +812,7 @@ SimpleCase.mpnn_apply = _mpnn_apply
 SimpleCase.mpnn_train = _mpnn_train
 SimpleCase.mpnn_loss_grad_pair = _mpnn_loss_grad_pair
 SimpleCase.mpnn_train_pairs = _mpnn_train_pairs
+SimpleCase.mpnn_time = lambda self, reps=20: _mpnn_time(self, reps)
 SimpleCase.poisson_residual = _poisson_residual
 SimpleCase.detail_turbulence = _detail_turbulence
 SimpleCase.turbulence_setup = _turbulence_setup

@@ -69,6 +69,8 @@ inline cfg_simple_controls toControls(const SimpleControls& ctl, scalar nu)
     cc.verbose = 0;
     cc.p_ref_cell = -1;
     cc.p_ref_value = 0.0;
+    cc.dt = ctl.dt;
+    cc.u_time_old = ctl.uTimeOld ? 2 : 0;
     return cc;
 }
 

@@ -137,6 +137,22 @@ SimpleResult SimpleSession::solve(volVectorField& U, volScalarField& p, surfaceS
     check(cfg_fields_upload(c_, u.data(), p.internalField().data(), phi.values().data()), "cfg_fields_upload");
 
     cfg_simple_controls cc = detail::toControls(ctl, nu);
+    if (ctl.uTimeOld)
+    {
+        // the caller's velocity at the previous time level
+        std::vector<double> uo(3 * static_cast<std::size_t>(nC));
+        for (label c = 0; c < nC && static_cast<std::size_t>(c) < ctl.uTimeOld->size(); ++c)
+        {
+            const Vector& v = (*ctl.uTimeOld)[static_cast<std::size_t>(c)];
+            uo[3 * c] = v.x;
+            uo[3 * c + 1] = v.y;
+            uo[3 * c + 2] = v.z;
+        }
+        if (ctl.uTimeOld->size() != static_cast<std::size_t>(nC))
+            throw Error("SIMPLE: the old velocity carries " + std::to_string(ctl.uTimeOld->size()) +
+                        " cells for a mesh of " + std::to_string(nC));
+        check(cfg_fields_upload_old(c_, uo.data()), "cfg_fields_upload_old");
+    }
     cc.p_precond = opt_.dicPressure ? CFG_PRECOND_DIC : CFG_PRECOND_JACOBI;
     cc.verbose = opt_.verbose ? 1 : 0;
     cc.p_ref_cell = opt_.pRefCell;

@@ -378,6 +378,14 @@ int cfg_fields_upload(cfg_ctx* ctx, const double* U, const double* p, const doub
     });
 }
 
+int cfg_fields_upload_old(cfg_ctx* ctx, const double* U_old)
+{
+    return guard([&] {
+        need(ctx && U_old, "cfg_fields_upload_old: null argument");
+        ctx->c->uploadOld(U_old);
+    });
+}
+
 int cfg_fields_download(cfg_ctx* ctx, double* U, double* p, double* phi)
 {
     return guard([&] {
@@ -1030,6 +1038,14 @@ int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t nSamples, int32_
     return guard([&] {
         need(ctx && samples, "cfg_mpnn_train: null argument");
         ctx->c->mpnnTrainHost(samples, nSamples, epochs, lr, losses);
+    });
+}
+
+int cfg_mpnn_time(cfg_ctx* ctx, int32_t reps, double out[2])
+{
+    return guard([&] {
+        need(ctx && out && reps > 0, "cfg_mpnn_time: bad argument");
+        ctx->c->mpnnTime(reps, out);
     });
 }
 

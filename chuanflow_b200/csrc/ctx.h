@@ -57,6 +57,8 @@ public:
     void setSchemes(const cfg_schemes& s) { schemes_ = s; }
 
     void upload(const double* U, const double* p, const double* phi);
+    /// SimpleControls::uTimeOld (cfg_fields_upload_old)
+    void uploadOld(const double* U);
     void download(double* U, double* p, double* phi);
     void initFlux(const double* u0);
     void iterate(const cfg_simple_controls& ctl, cfg_simple_result& res);
@@ -244,6 +246,14 @@ private:
     double mpnnLossGrad(const double* vals, const double* diag, const double* r, double* z,
                         const double* t = nullptr);
     void mpnnGuess(const double* vals, const double* diag, const double* b, double* x);
+    bool mpnnTimeLayers_ = false;
+    double mpnnLayerMs_ = 0;
+    int64_t mpnnLayerLaunches_ = 0;
+
+public:
+    void mpnnTime(int reps, double* out);
+
+private:
     double* trainBuf_ = nullptr;
     size_t trainCap_ = 0;
     void mpnnAdam(float lr);
@@ -273,6 +283,7 @@ private:
     double turbCDES_ = 0.61, turbReOnset_ = 0.0, turbOnsetWidth_ = -1.0, turbGammaRate_ = 4.0;
     double* saved_ = nullptr;
     V3P uOld_{};
+    bool oldUploaded_ = false;
     double* savedT_ = nullptr;
     bool savedTurb_ = false;
     void turbCopy(double* buf, bool save);

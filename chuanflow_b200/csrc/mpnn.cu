@@ -222,18 +222,25 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_out(int n, const double* _
     }
 }
 
-/// s = sqrt(sum r^2 / n) (one block) and 1/s
-__global__ void k_mpnn_scale(int n, const double* __restrict__ r, double* s)
+/// s = sqrt(sum r^2 / n), 1/s and sum r^2: block partials, then the block
+/// that finishes last sums them in a fixed order
+__global__ void __launch_bounds__(TPB) k_mpnn_scale(int n, const double* __restrict__ r, double* partials,
+                                                    unsigned* ticket, double* s)
 {
     double v[1] = {0.0};
-    for (int i = threadIdx.x; i < n; i += TPB) v[0] += r[i] * r[i];
+    FOR_ROWS(i, n) v[0] += r[i] * r[i];
     block_sum<1>(v);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+    if (!last_block(ticket)) return;
+    double f[1];
+    final_sum<1>(partials, gridDim.x, f);
     if (threadIdx.x == 0)
     {
-        const double rms = sqrt(v[0] / n);
+        *ticket = 0;
+        const double rms = sqrt(f[0] / n);
         s[0] = rms;
         s[1] = rms > 0 ? 1.0 / rms : 0.0;
-        s[2] = v[0];
+        s[2] = f[0];
     }
 }
 
@@ -516,6 +523,7 @@ struct MpnnState
     unsigned* mask = nullptr;                                         // (L+1) n
     double *s = nullptr, *res = nullptr, *acc = nullptr;
     double *ae = nullptr, *at = nullptr;  // A e and A t of the energy-norm loss
+    unsigned* ticket = nullptr;
     int step = 0;
 };
 
@@ -556,6 +564,7 @@ void Ctx::mpnnCreate(int layers, uint64_t seed)
     m->mask = alloc<unsigned>(static_cast<size_t>(layers + 1) * m->n);
     m->s = alloc<double>(4);
     m->res = alloc<double>(m->n);
+    m->ticket = alloc<unsigned>(1);
     m->ae = alloc<double>(m->n);
     m->at = alloc<double>(m->n);
     m->acc = alloc<double>(1);
@@ -589,11 +598,23 @@ void Ctx::mpnnApply(const double* vals, const double* diag, const double* r, dou
     const int n = dm_.nC;
     const size_t nH = static_cast<size_t>(n) * H;
     const int blocks = std::max(1, std::min((n + kWarps - 1) / kWarps, sms_ * 16));
-    k_mpnn_scale<<<1, TPB, 0, stream_>>>(n, r, m.s);
+    k_mpnn_scale<<<GS_, TPB, 0, stream_>>>(n, r, partials_, m.ticket, m.s);
     k_mpnn_enc<<<blocks, kWarps * 32, 0, stream_>>>(n, r, m.s + 1, m.wb, m.h, m.mask);
     for (int l = 0; l < m.L; ++l)
+    {
+        if (mpnnTimeLayers_) CFG_CUDA(cudaEventRecord(tm_.ev[4 + 2 * (l % 4)], stream_));
         k_mpnn_layer<<<blocks, kWarps * 32, 0, stream_>>>(A, vals, diag, m.wb + offLayer(l), m.h + l * nH,
                                                           m.h + (l + 1) * nH, m.mask + static_cast<size_t>(l + 1) * n);
+        if (mpnnTimeLayers_)
+        {
+            CFG_CUDA(cudaEventRecord(tm_.ev[5 + 2 * (l % 4)], stream_));
+            CFG_CUDA(cudaEventSynchronize(tm_.ev[5 + 2 * (l % 4)]));
+            float ms = 0;
+            CFG_CUDA(cudaEventElapsedTime(&ms, tm_.ev[4 + 2 * (l % 4)], tm_.ev[5 + 2 * (l % 4)]));
+            mpnnLayerMs_ += ms;
+            ++mpnnLayerLaunches_;
+        }
+    }
     k_mpnn_out<<<blocks, kWarps * 32, 0, stream_>>>(n, r, diag, m.s, m.wb + offLayer(m.L), m.h + m.L * nH, z);
     launchCheck("mpnn_apply", 3 + m.L);
 }
@@ -708,6 +729,31 @@ double Ctx::mpnnLossGradHost(const double* r, float* grad, const double* t)
         CFG_CUDA(cudaStreamSynchronize(stream_));
     }
     return loss;
+}
+
+/// Event-timed applications of the network on the current pressure matrix
+/// (input: the residual buffer's contents): out = {ms per application, ms
+/// per message-passing layer launch}.
+void Ctx::mpnnTime(int reps, double* out)
+{
+    if (!mpnn_) fail(CFG_EINVAL, "mpnn: call cfg_mpnn_create first");
+    CFG_CUDA(cudaSetDevice(device_));
+    const double *vals, *diag;
+    mpnnMatrix(&vals, &diag);
+    mpnnApply(vals, diag, cr_, cz_);  // warm
+    CFG_CUDA(cudaEventRecord(tm_.ev[2], stream_));
+    for (int k = 0; k < reps; ++k) mpnnApply(vals, diag, cr_, cz_);
+    CFG_CUDA(cudaEventRecord(tm_.ev[3], stream_));
+    CFG_CUDA(cudaEventSynchronize(tm_.ev[3]));
+    float ms = 0;
+    CFG_CUDA(cudaEventElapsedTime(&ms, tm_.ev[2], tm_.ev[3]));
+    out[0] = ms / std::max(1, reps);
+    mpnnTimeLayers_ = true;
+    mpnnLayerMs_ = 0;
+    mpnnLayerLaunches_ = 0;
+    for (int k = 0; k < reps; ++k) mpnnApply(vals, diag, cr_, cz_);
+    mpnnTimeLayers_ = false;
+    out[1] = mpnnLayerMs_ / std::max<int64_t>(1, mpnnLayerLaunches_);
 }
 
 void Ctx::mpnnApplyHost(const double* r, double* z)

@@ -2087,6 +2087,32 @@ void Ctx::prepareIterate(const cfg_simple_controls& ctl)
     checkMomentumBcs();
     if (!turb_) setNu(ctl.nu);  // with a RANS model the model's nu + nut is the diffusivity
     if (ctl.p_ref_cell >= dm_.nC) fail(CFG_EINVAL, "p_ref_cell beyond the last cell");
+    // the time term (simpleSolver.cpp:75-97): dt and the old velocity together
+    if (ctl.dt > 0 || ctl.u_time_old != 0)
+    {
+        if (!(ctl.dt > 0)) fail(CFG_EINVAL, "SIMPLE: an old velocity was supplied with no time step");
+        if (ctl.u_time_old != 1 && ctl.u_time_old != 2)
+            fail(CFG_EINVAL, "SIMPLE: a time step was supplied with no velocity at the previous time level");
+        if (ctl.u_time_old == 2 && !oldUploaded_)
+            fail(CFG_EINVAL, "SIMPLE: u_time_old 2 needs cfg_fields_upload_old first");
+        if (!uOld_.c[0])
+            for (int q = 0; q < 3; ++q) uOld_.c[q] = alloc<double>(dm_.nC);
+        if (ctl.u_time_old == 1)
+            for (int q = 0; q < 3; ++q)
+                CFG_CUDA(cudaMemcpyAsync(uOld_.c[q], U_.c[q], dm_.nC * sizeof(double), cudaMemcpyDeviceToDevice,
+                                         stream_));
+    }
+}
+
+void Ctx::uploadOld(const double* U)
+{
+    CFG_CUDA(cudaSetDevice(device_));
+    if (!uOld_.c[0])
+        for (int q = 0; q < 3; ++q) uOld_.c[q] = alloc<double>(dm_.nC);
+    double* const dev[3] = {uOld_.c[0], uOld_.c[1], uOld_.c[2]};
+    cellsToDev(dev, 3, U);
+    CFG_CUDA(cudaStreamSynchronize(stream_));
+    oldUploaded_ = true;
 }
 
 /// Enqueues one SIMPLE outer iteration (simpleSolver.cpp:52-357) on stream_,
@@ -2116,8 +2142,10 @@ void Ctx::enqueueOuter(const cfg_simple_controls& ctl, int64_t& uInner, int64_t&
         V3P g[1] = {gPn_};
         gradCells(xs, 1, pb, gs, true, g);
     }
+    const bool timeTerm = ctl.dt > 0;
     MomArgs ma{phi_, gU_, ub, alpha, {ctl.body_force[0], ctl.body_force[1], ctl.body_force[2]}, cv(gPn_),
-               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, 0.0, CV3P{}};
+               linUpwindGrad(ub, gs), {}, mVal_, uDiag_, uBase_, timeTerm ? ctl.dt : 0.0,
+               timeTerm ? cv(uOld_) : CV3P{}};
     ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
     k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
     launchCheck("assemble_U");

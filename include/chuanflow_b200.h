@@ -117,6 +117,14 @@ typedef struct cfg_simple_controls
      * gains diag * p_ref_value and its diagonal doubles. */
     int64_t p_ref_cell;
     double p_ref_value;
+    /* SimpleControls::dt / uTimeOld (SimpleSolver.h:44-63, simpleSolver.cpp:
+     * 75-97): dt > 0 puts fvm::ddt(U, Uold, dt) (Euler) into every sweep's
+     * momentum equation, so the loop's fixed point is one implicit-Euler step
+     * and rAU is bounded by dt.  u_time_old: 0 none, 1 the velocity at the
+     * start of this call, 2 the field last given to cfg_fields_upload_old.
+     * The reference refuses either without the other; so does this. */
+    double dt;
+    int32_t u_time_old;
 } cfg_simple_controls;
 
 /* SimpleResult (SimpleSolver.h:66-72) plus inner-solver statistics */
@@ -255,6 +263,9 @@ int cfg_set_schemes(cfg_ctx* ctx, const cfg_schemes* schemes);
  * original cell and face order; NULL skips a field. */
 int cfg_fields_upload(cfg_ctx* ctx, const double* U, const double* p, const double* phi);
 int cfg_fields_download(cfg_ctx* ctx, double* U, double* p, double* phi);
+/* The velocity at the previous time level for cfg_simple_controls.u_time_old
+ * = 2 (nCells x 3, original order): SimpleControls::uTimeOld. */
+int cfg_fields_upload_old(cfg_ctx* ctx, const double* U_old);
 
 /* The initial flux of src/3d/apps/simpleFoamApp.cpp:94-95 and
  * src/3d/apps/caseInit.h:18-31: boundary phi from U's conditions
@@ -526,10 +537,16 @@ int cfg_mpnn_train(cfg_ctx* ctx, const double* samples, int32_t n_samples, int32
 int cfg_mpnn_train_pairs(cfg_ctx* ctx, const double* samples, const double* targets, int32_t n_samples,
                          int32_t epochs, float lr, double* losses);
 int cfg_mpnn_loss_grad_pair(cfg_ctx* ctx, const double* r, const double* t, double* loss, float* grad);
-/* Keep (on = 1) up to max_samples of the residuals the SIMPLE / PISO
- * pressure solves start from (b - A x0 of their first pass, original
- * order) as training samples; on = 2 first drops those kept; on = 0 stops.
- * cfg_mpnn_train_collected trains on them; n returns how many are kept. */
+/* reps event-timed applications of the network on the context's current
+ * pressure matrix: out[0] ms per application, out[1] ms per message-passing
+ * layer launch (no reference counterpart). */
+int cfg_mpnn_time(cfg_ctx* ctx, int32_t reps, double out[2]);
+/* Keep (on = 1) up to max_samples training pairs of the SIMPLE / PISO
+ * pressure solves: the residual each starts from (b - A x0 of its first
+ * pass, original order) and the correction that pass converges to (x - x0);
+ * on = 2 first drops those kept; on = 0 stops.  cfg_mpnn_train_collected
+ * trains on the pairs in the energy norm (cfg_mpnn_train_pairs); n returns
+ * how many are kept. */
 int cfg_mpnn_collect(cfg_ctx* ctx, int32_t on, int32_t max_samples, int32_t* n);
 int cfg_mpnn_train_collected(cfg_ctx* ctx, int32_t epochs, float lr, double* losses);
 /* r = b - A x on the cfg_poisson_setup system (training samples from the

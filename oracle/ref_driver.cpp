@@ -376,9 +376,35 @@ int modeSimple(int argc, char** argv)
     if (argc > 5) loadState(argv[5], U, p, phi);
     const Schemes schemes = loadSchemes(caseDict);
     const SimpleControls ctl = readControls(caseDict);
+    // simple { dt ...; }: pseudo-time stepping through SimpleControls::dt and
+    // uTimeOld -- each of the maxIterations outer iterations is its own call
+    // with one sweep, the velocity at the call's start as the old level
+    const double pseudoDt = caseDict.getDict("simple").getScalarOr("dt", 0.0);
 
     const auto t0 = std::chrono::steady_clock::now();
-    const SimpleResult res = SIMPLE_SOLVE(mesh, U, p, phi, nu, schemes, ctl);
+    SimpleResult res;
+    if (pseudoDt > 0)
+    {
+        Schemes eul = schemes;
+        eul.ddt = "Euler";
+        SimpleControls one = ctl;
+        one.maxIterations = 1;
+        one.dt = pseudoDt;
+        int done = 0;
+        for (int k = 0; k < ctl.maxIterations; ++k)
+        {
+            const Field<Vector> uOld = U.internalField();
+            one.uTimeOld = &uOld;
+            res = SIMPLE_SOLVE(mesh, U, p, phi, nu, eul, one);
+            ++done;
+            if (!std::isfinite(res.finalContinuityError)) break;
+        }
+        res.iterations = done;
+    }
+    else
+    {
+        res = SIMPLE_SOLVE(mesh, U, p, phi, nu, schemes, ctl);
+    }
     const auto t1 = std::chrono::steady_clock::now();
     const double secs = std::chrono::duration<double>(t1 - t0).count();
 

@@ -21,6 +21,8 @@ Fixtures (small .npz files):
   piso_channel.npz         16x6x6 jittered channel: 4 transient PISO steps (dt 0.05, 2 correctors)
   simple_channel40.npz     the 16,000-cell channel: all 300 reference iterations, and 20 with
                            linear-upwind, Gauss linear and DIC-PCG by the C restatement (checksums, samples)
+  simple_channel_dt.npz    the 10x6x5 channel by the reference's SIMPLE with its time term (dt 0.05,
+                           uTimeOld the velocity each call starts from): six one-sweep calls
   poiseuille.npz           the reference's verification channel (100x20x1, K.poiseuille_dict) run by the
                            reference to its own outer stop: iterations and the whole U, p, phi
   simple_cavity128.npz     the 2M-cell bench cavity (pinned, so by the C restatement): checksums and
@@ -271,6 +273,16 @@ def poiseuille_npz(name):
     print("wrote", name, res[:4])
 
 
+def pseudo_npz():
+    """The reference's SIMPLE with its time term (SimpleControls::dt and
+    uTimeOld, simpleSolver.cpp:75-97) on the 10x6x5 jittered channel: six
+    calls of one sweep each, every call's old velocity the one it starts
+    from (the driver's simple { dt } mode)."""
+    ch = K.channel_case(10, 6, 5)
+    text = K.channel_dict(10, 6, 5, iters=6).replace("maxIterations 6;", "maxIterations 6;\n    dt 0.05;")
+    simple_npz("simple_channel_dt.npz", ch, text, ch.mesh.points)
+
+
 def solve_npz(name, method, rs, cols, vals, b, x0, tol, max_iter):
     n = rs.size - 1
     rows = np.repeat(np.arange(n), np.diff(rs))
@@ -336,6 +348,9 @@ def main():
     if sys.argv[1:] == ["poiseuille"]:
         poiseuille_npz("poiseuille.npz")
         return
+    if sys.argv[1:] == ["pseudo"]:
+        pseudo_npz()
+        return
     mesh_npz("mesh_block_2x2x2.npz", "block { min (0 0 0); max (1 1 1); cells (2 2 2); }\n")
     mesh_npz("mesh_tets22.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeTets_22.msh"; }}\n', grad_fields=True)
     mesh_npz("mesh_hex41.npz", f'mesh {{ format gmsh; file "{REF_MESHES}/cubeHex_41.msh"; }}\n', grad_fields=True)
@@ -372,6 +387,7 @@ def main():
     simple_npz("simple_cavity.npz", cav, K.cavity_dict(6, 5, 4, iters=3), cav.mesh.points)
     ch = K.channel_case(10, 6, 5)
     simple_npz("simple_channel.npz", ch, K.channel_dict(10, 6, 5, iters=4), ch.mesh.points)
+    pseudo_npz()
 
     pc = K.channel_case(16, 6, 6)
     piso_npz("piso_channel.npz", K.piso_channel_dict(), pc.mesh.points)

@@ -79,6 +79,30 @@ def test_simple_channel_matches_reference(golden):
     assert abs(res.final_continuity_error - float(g["continuity"])) <= 1e-6 * abs(float(g["continuity"]))
 
 
+def test_simple_channel_time_term_matches_reference(golden):
+    """SIMPLE with the reference's time term (SimpleControls::dt and
+    uTimeOld, simpleSolver.cpp:75-97): six one-sweep calls with dt 0.05, each
+    taking the velocity it starts from as the old time level, against the
+    reference's own six calls; and the reference's refusals of a time step
+    without an old velocity and the reverse."""
+    import dataclasses
+    import chuanflow_b200 as cf
+    g = golden("simple_channel_dt.npz")
+    mesh, case = K.channel_product(10, 6, 5)
+    ctl = dataclasses.replace(K.controls_from(K.channel_case(10, 6, 5)), max_iterations=1, dt=0.05, u_time_old=1)
+    for _ in range(int(g["iterations"])):
+        res = case.solve(ctl)
+        assert not res.diverged
+    U, p, phi = case.download()
+    for a, b, name in ((U, g["U"], "U"), (p, g["p"], "p"), (phi, g["phi"], "phi")):
+        assert rel(a, b) < REL_TOL, (name, rel(a, b))
+    assert abs(res.final_continuity_error - float(g["continuity"])) <= 1e-6 * abs(float(g["continuity"]))
+    with pytest.raises(cf.CfgError, match="no velocity at the previous time level"):
+        case.solve(dataclasses.replace(ctl, u_time_old=0))
+    with pytest.raises(cf.CfgError, match="no time step"):
+        case.solve(dataclasses.replace(ctl, dt=0.0))
+
+
 @pytest.mark.parametrize("cells,jitter,pin,iters", [((8, 8, 8), 0.0, -1, 5), ((12, 12, 12), 0.1, 0, 8)])
 def test_simple_cavity_matches_oracle(cells, jitter, pin, iters):
     """The lid-driven cavity: orthogonal (the reference's own set-up) and
