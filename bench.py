@@ -532,15 +532,26 @@ def main_blocks(args, world, rank, local, dist):
     for _ in range(max(3, args.warmup)):
         batch.loss(qs, ctls)
     sched, cand = batch.autotune(qs, ctls)
+    # the single-graph pass, timed on its own whether or not the autotuner
+    # picked it (its first pass captures the graph)
+    graph_sched = (0, -1)
+    batch.save()
+    batch.set_schedule(*graph_sched)
+    batch.loss(qs, ctls)
+    batch.restore()
     barrier(dist)
-    # each step: the same pass from the same fields, batched and then one
-    # block after another, the batched result kept
-    batched, serial = [], []
+    # each step: the same pass from the same fields, one block after another,
+    # as one graph launch, and under the autotuned schedule, the last kept
+    batched, serial, graphed = [], [], []
     for _ in range(args.steps):
         batch.save()
         batch.set_schedule(1, 0)
         r2, ms = batch.loss(qs, ctls)
         serial.append(ms)
+        batch.restore()
+        batch.set_schedule(*graph_sched)
+        r3, ms = batch.loss(qs, ctls)
+        graphed.append(ms)
         batch.restore()
         batch.set_schedule(*sched)
         r, ms = batch.loss(qs, ctls)
@@ -548,6 +559,26 @@ def main_blocks(args, world, rank, local, dist):
     barrier(dist)
     t_b = allreduce_max(dist, statistics.median(batched))
     t_s = allreduce_max(dist, statistics.median(serial))
+    t_g = allreduce_max(dist, statistics.median(graphed))
+    # the pass's algorithmic bytes: per block its fixed face and cell passes,
+    # its momentum BiCGStab component-iterations (each the component's share
+    # of both matrix reads plus its vector streams) and its DIC-PCG
+    # iterations; the k-epsilon blocks' two scalar solves are not counted
+    byts = 0.0
+    for c, x in zip(cases, r):
+        N, F, Fb = c.mesh.n_cells, c.mesh.n_internal_faces, c.mesh.n_boundary_faces
+        kb = kernel_bytes(N, F)
+        per_u = (kb["bi_spmv1"][0] + kb["bi_spmv2"][0] + kb["bi_p"][0] + kb["bi_x"][0]) / 3 + \
+            kb["bi_p"][1] + kb["bi_spmv1"][1] + kb["bi_spmv2"][1] + kb["bi_x"][1]
+        per_p = kb["cg_spmv"][0] + kb["cg_update"][0] + kb["cg_p"][0] + kb["dic_apply"][0]
+        byts += simple_step_bytes(N, F, Fb, 1, 0, "DIC", x["u_inner_iterations"] * per_u +
+                                  x["p_inner_iterations"] * per_p)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
     if rank == 0:
         out = {"metric": "coupling pass time, 64 detail blocks x one SIMPLE outer iteration", "value": t_b,
                "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
@@ -559,6 +590,12 @@ def main_blocks(args, world, rank, local, dist):
                           "cells": cells, "schedule": {"workers": sched[0], "row_blocks_per_sm": sched[1]},
                           "autotune_ms": {f"{w}x{r}": v for (w, r), v in cand.items()}},
                "one_after_another_ms": t_s, "speedup_vs_one_after_another": t_s / t_b,
+               "single_graph_ms": t_g, "speedup_single_graph_vs_one_after_another": t_s / t_g,
+               "roofline": {"bound": "hbm", "achieved": byts / (t_b * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                            "frac": byts / (t_b * 1e-3) / 1e9 / peak, "traffic": None,
+                            "model": "sum over blocks of the outer iteration's fixed passes plus the measured inner "
+                                     "iterations at this build's per-kernel bytes (k-epsilon solves not counted), "
+                                     "over the pass's wall time"},
                "cell_iter_per_s": cells / (t_b * 1e-3),
                "inner_iterations_last_pass": {"u": sum(x["u_inner_iterations"] for x in r),
                                               "p": sum(x["p_inner_iterations"] for x in r)},
@@ -938,6 +975,29 @@ def main_simple(args, world, rank, local, dist):
         out["field_error"] = dict(field_errors(*test, *fp64),
                                   against="FP64 DIC-PCG pressure (FP64 throughout), the same K iterations from the same "
                                           "start state; relative L2")
+
+    # ---- mixed precision: the same K iterations with the pressure matrix
+    # rounded to FP32 and FP32 DIC-PCG corrections inside FP64 refinement
+    # (FP64 residual and infinity-norm test), against the FP64 DIC fields ----
+    if not args.no_variant:
+        c3 = dataclasses.replace(ctl, p_preconditioner="IR32")
+        case.upload(U0, p0, phi0)
+        case.solve(c3)
+        case.upload(U0, p0, phi0)
+        barrier(dist)
+        mix = Steps().run(case, c3, args.steps)
+        barrier(dist)
+        U3, p3, phi3 = case.download()
+        m_t = allreduce_max(dist, mix.ms / 1e3)
+        out["mixed_precision"] = {
+            "pressure": "matrix rounded to FP32, FP32 multicolour DIC-PCG corrections to 1e-4 inside FP64 iterative "
+                        "refinement, FP64 residual and |r|inf/|b|inf test at 1e-8",
+            "value": world * ncell * args.steps / m_t, "ms_per_step": m_t * 1e3 / args.steps,
+            "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": mix.u / args.steps,
+                                          "pressure_fp32": mix.p / args.steps},
+            "diverged_steps": mix.diverged,
+            "field_error_vs_fp64_dic": field_errors(U3, p3, phi3, *fp64)}
+        diverged += mix.diverged
 
     # ---- the reference's own work on the GPU: its first outer iteration
     # from rest exactly as it runs it (no pressure reference cell, Jacobi-

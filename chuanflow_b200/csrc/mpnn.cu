@@ -58,21 +58,35 @@ __device__ __forceinline__ Row sell_row(const DMat& A, int i)
     return Row{A.start[sl] + l, A.start[sl + 1]};
 }
 
+/// The message coefficients c_ij = -a_ij / a_ii of every off-diagonal SELL
+/// entry (row i), in FP32, once per matrix; 0 on the diagonal and the pads.
+__global__ void __launch_bounds__(TPB) k_mpnn_coef(DMat A, const double* __restrict__ val,
+                                                   const double* __restrict__ diag, float* __restrict__ coef)
+{
+    FOR_ROWS(i, A.n)
+    {
+        const int sl = i >> 5, l = i & 31;
+        const double aii = diag[i];
+        for (int e = A.start[sl] + l; e < A.start[sl + 1]; e += 32)
+        {
+            const int j = A.col[e];
+            coef[e] = (j < 0 || j == i) ? 0.f : static_cast<float>(-val[e] / aii);
+        }
+    }
+}
+
 /// m_k = sum_j c_ij x[j*H + k] over the off-diagonal entries of row i
-__device__ __forceinline__ float message(const DMat& A, const double* __restrict__ val,
-                                         const double* __restrict__ diag, const float* __restrict__ x, int i,
-                                         int lane)
+__device__ __forceinline__ float message(const DMat& A, const float* __restrict__ coef, const float* __restrict__ x,
+                                         int i, int lane)
 {
     const Row r = sell_row(A, i);
-    const double aii = diag[i];
     float m = 0.f;
     for (int e = r.e0; e < r.e1; e += 32)
     {
-        const int j = A.col[e];
+        const int j = __ldg(A.col + e);
         if (j < 0) break;
         if (j == i) continue;
-        const float c = static_cast<float>(-val[e] / aii);
-        m += c * x[static_cast<size_t>(j) * H + lane];
+        m += __ldg(coef + e) * x[static_cast<size_t>(j) * H + lane];
     }
     return m;
 }
@@ -123,8 +137,7 @@ constexpr int XP = 2 * H + 8;  // padded BF16 row of [h | m] and of the weights 
 
 /// one residual message-passing layer: hout = hin + relu(A h + B m + b) for
 /// 16 cells per warp step, the contraction on the tensor cores
-__global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const double* __restrict__ val,
-                                                            const double* __restrict__ diag,
+__global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const float* __restrict__ coef,
                                                             const __nv_bfloat16* __restrict__ wl,
                                                             const float* __restrict__ hin, float* __restrict__ hout,
                                                             unsigned* __restrict__ mask)
@@ -157,7 +170,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const double
             if (i < A.n)
             {
                 h = hin[static_cast<size_t>(i) * H + lane];
-                m = message(A, val, diag, hin, i, lane);
+                m = message(A, coef, hin, i, lane);
             }
             hr[t] = h;
             sX[w][t][lane] = __float2bfloat16(h);
@@ -306,8 +319,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_out_bwd(DMat A, const doub
 /// backward of one layer, part 1: delta = dh (.) relu'(u); weight gradients;
 /// dhin = dh + A^T delta (the residual path plus the self transform); v =
 /// B^T delta for the transposed message of part 2
-__global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer_bwd(DMat A, const double* __restrict__ val,
-                                                                const double* __restrict__ diag,
+__global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer_bwd(DMat A, const float* __restrict__ coef,
                                                                 const __nv_bfloat16* __restrict__ wl,
                                                                 const float* __restrict__ hin,
                                                                 const unsigned* __restrict__ mask,
@@ -336,7 +348,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer_bwd(DMat A, const do
         const size_t o = static_cast<size_t>(i) * H + lane;
         // the operands the forward multiplied: h and m rounded to BF16
         const float h = bf16r(hin[o]);
-        const float m = bf16r(message(A, val, diag, hin, i, lane));
+        const float m = bf16r(message(A, coef, hin, i, lane));
         const float d = (mask[i] >> lane) & 1u ? dh[o] : 0.f;
         rb += d;
         float at = 0.f, bt = 0.f;
@@ -524,6 +536,7 @@ struct MpnnState
     double *s = nullptr, *res = nullptr, *acc = nullptr;
     double *ae = nullptr, *at = nullptr;  // A e and A t of the energy-norm loss
     unsigned* ticket = nullptr;
+    float* coef = nullptr;  // message coefficients, one per SELL entry
     int step = 0;
 };
 
@@ -565,6 +578,7 @@ void Ctx::mpnnCreate(int layers, uint64_t seed)
     m->s = alloc<double>(4);
     m->res = alloc<double>(m->n);
     m->ticket = alloc<unsigned>(1);
+    m->coef = alloc<float>(static_cast<size_t>(nSlicesEntries_));
     m->ae = alloc<double>(m->n);
     m->at = alloc<double>(m->n);
     m->acc = alloc<double>(1);
@@ -598,12 +612,13 @@ void Ctx::mpnnApply(const double* vals, const double* diag, const double* r, dou
     const int n = dm_.nC;
     const size_t nH = static_cast<size_t>(n) * H;
     const int blocks = std::max(1, std::min((n + kWarps - 1) / kWarps, sms_ * 16));
+    k_mpnn_coef<<<GS_, TPB, 0, stream_>>>(A, vals, diag, m.coef);
     k_mpnn_scale<<<GS_, TPB, 0, stream_>>>(n, r, partials_, m.ticket, m.s);
     k_mpnn_enc<<<blocks, kWarps * 32, 0, stream_>>>(n, r, m.s + 1, m.wb, m.h, m.mask);
     for (int l = 0; l < m.L; ++l)
     {
         if (mpnnTimeLayers_) CFG_CUDA(cudaEventRecord(tm_.ev[4 + 2 * (l % 4)], stream_));
-        k_mpnn_layer<<<blocks, kWarps * 32, 0, stream_>>>(A, vals, diag, m.wb + offLayer(l), m.h + l * nH,
+        k_mpnn_layer<<<blocks, kWarps * 32, 0, stream_>>>(A, m.coef, m.wb + offLayer(l), m.h + l * nH,
                                                           m.h + (l + 1) * nH, m.mask + static_cast<size_t>(l + 1) * n);
         if (mpnnTimeLayers_)
         {
@@ -616,7 +631,7 @@ void Ctx::mpnnApply(const double* vals, const double* diag, const double* r, dou
         }
     }
     k_mpnn_out<<<blocks, kWarps * 32, 0, stream_>>>(n, r, diag, m.s, m.wb + offLayer(m.L), m.h + m.L * nH, z);
-    launchCheck("mpnn_apply", 3 + m.L);
+    launchCheck("mpnn_apply", 4 + m.L);
 }
 
 /// One sample's loss and its gradient (into m.g).  Without a target t: the
@@ -675,7 +690,7 @@ double Ctx::mpnnLossGrad(const double* vals, const double* diag, const double* r
     float* dn = m.dh1;
     for (int l = m.L - 1; l >= 0; --l)
     {
-        k_mpnn_layer_bwd<<<blocks, kWarps * 32, 0, stream_>>>(A, vals, diag, m.wb + offLayer(l), m.h + l * nH,
+        k_mpnn_layer_bwd<<<blocks, kWarps * 32, 0, stream_>>>(A, m.coef, m.wb + offLayer(l), m.h + l * nH,
                                                               m.mask + static_cast<size_t>(l + 1) * n, dh, dn, m.v,
                                                               m.g + offLayer(l));
         k_mpnn_msg_bwd<<<blocks, kWarps * 32, 0, stream_>>>(A, vals, diag, m.v, dn);
