@@ -16,14 +16,17 @@ The workload: the 16,000-cell verification channel's family (2.0 x 0.1 x
 cavity's mesh treatment (interior points jittered by a seeded uniform +-10%
 of the cell size, so every face is non-orthogonal), schemes upwind /
 corrected / corrected, 1 non-orthogonal corrector, and the reference's own
-channel relaxation (relaxU 0.9, relaxP 0.03, pRelaxStart 0.02).  Momentum by
+channel relaxation (relaxU 0.9, relaxP 0.03) with the startup floor of its
+adaptive pressure relaxation at pRelaxStart 0.002 (its 16,000-cell value,
+0.02, lets the 2M-cell SIMPLE diverge within five iterations).  Momentum by
 the reference's Jacobi-BiCGStab; pressure to 1e-8 (infinity norm relative to
 the right-hand side, the reference's test) with at most 2000 iterations by
 FP64 flexible CG preconditioned with an FP32 aggregation-AMG V-cycle
 (--p-precond; the line's `variant` runs the same steps with FP64 multicolour
-DIC-PCG).  The lid-driven cavity of the same cell count is not the
-headline: the reference's SIMPLE diverges on it, on the GPU and in the C
-restatement alike, under every relaxation tried.
+DIC-PCG).  `--workload cavity` times the lid-driven cavity of the same cell
+count (128^3, Re 400, relaxation 0.7 / 0.3 / pRelaxStart 5e-4, pressure
+reference cell 0), which the reference cannot run as such: it has no
+reference cell.
 
 Every leg counts the outer iterations that diverged (simpleSolver.cpp:360-364:
 non-finite continuity, pressure step or fields); the JSON line carries them
@@ -53,7 +56,10 @@ JITTER, SEED = 0.1, 7
 SIDES = ["xmin", "xmax", "ymin", "ymax", "zmin", "zmax"]
 CH_NAMES = ["inlet", "outlet", "bottom", "top", "front", "back"]
 CH_TYPES = ["inlet", "outlet", "wall", "wall", "wall", "wall"]
-RELAX = {"relax_u": 0.9, "relax_p": 0.03, "p_relax_start": 0.02}
+# the reference's channel relaxation; the startup floor of its adaptive
+# pressure relaxation lowered from its 16,000-cell value 0.02, with which its
+# SIMPLE diverges at 2M cells
+RELAX = {"relax_u": 0.9, "relax_p": 0.03, "p_relax_start": 0.002}
 METRIC = "SIMPLE cell-iter/s at 2M cells; time to 1e-8 p-residual, learned vs plain PCG"
 REFERENCE_ARM = ("the reference's CPU SIMPLE (its own sources, its Jacobi-PCG pressure and Jacobi-BiCGStab "
                  "momentum) on the same mesh, boundary conditions and settings, one outer iteration from rest as "
@@ -73,7 +79,7 @@ def workload_config(n, precond="DIC"):
     return {"workload": f"3D channel {LENGTH[0]} x {LENGTH[1]} x {LENGTH[2]} m, {nx} x {ny} x {nz} hex "
                         f"({nx * ny * nz} cells), interior points jittered +-10% (seed {SEED}), inlet {U_IN} m/s, "
                         f"fixed-p outlet, no-slip walls, nu {NU} (Re 100), upwind/corrected/corrected, nonOrth 1, "
-                        f"relaxU 0.9 relaxP 0.03 pRelaxStart 0.02 (the reference's channel settings), momentum "
+                        f"relaxU 0.9 relaxP 0.03 pRelaxStart 0.002, momentum "
                         f"Jacobi-BiCGStab, pressure {solve}, tol 1e-8 (|r|inf/|b|inf), maxIter 2000",
             "cells": nx * ny * nz, "step": "one SIMPLE outer iteration",
             "l2": "inputs larger than L2 (about 1.3 GB of fields, matrices and mesh resident in HBM)",
@@ -148,6 +154,18 @@ def simple_step_bytes(N, F, Fb, n_orth, it_p, precond, solver_bytes, s=8, i=4):
     return fixed + solver_bytes + extra
 
 
+def cavity_config(n, precond="DIC"):
+    solve = ("FP64 flexible CG with an FP32 aggregation-AMG V-cycle" if precond == "AMG" else f"{precond}-PCG")
+    return {"workload": f"lid-driven cavity {n}^3 hex ({n ** 3} cells), interior points jittered +-10% (seed {SEED}), "
+                        f"Re 400, upwind/corrected/corrected, nonOrth 1, relaxU 0.7 relaxP 0.3 pRelaxStart 5e-4, "
+                        f"pressure {solve} tol 1e-8 (|r|inf/|b|inf) maxIter 2000, pressure reference cell 0",
+            "cells": n ** 3, "step": "one SIMPLE outer iteration",
+            "l2": "inputs larger than L2 (about 1.3 GB of fields, matrices and mesh resident in HBM)",
+            "precision": ("FP64, the pressure preconditioner FP32" if precond == "AMG" else "FP64 throughout"),
+            "parallelism": "one case per GPU (replicas)",
+            "reference_arm": "none for this workload: the reference has no pressure reference cell"}
+
+
 def make_case(n, device, precond="Jacobi"):
     """The headline channel on `device`, at rest with its boundary flux."""
     import chuanflow_b200 as cf
@@ -167,9 +185,10 @@ def make_case(n, device, precond="Jacobi"):
     return mesh, case, ctl
 
 
-def make_cavity_case(n, device, precond="Jacobi"):
-    """The jittered n^3 lid-driven cavity (Re 400, relaxation 0.7 / 0.3 /
-    pRelaxStart 0.02, pressure reference cell 0)."""
+def make_cavity_case(n, device, precond="Jacobi", p_relax_start=0.02):
+    """The jittered n^3 lid-driven cavity (Re 400, relaxation 0.7 / 0.3,
+    pressure reference cell 0); pRelaxStart 0.02 by default (the golden
+    fixtures' value), 5e-4 for the 128^3 workload, where 0.02 diverges."""
     import chuanflow_b200 as cf
     mesh = cf.PolyMesh.block((0, 0, 0), (1, 1, 1), (n, n, n), {s: (nm, "wall") for s, nm in zip(SIDES, CAV_NAMES)})
     mesh.jitter_interior(JITTER, SEED)
@@ -178,9 +197,9 @@ def make_cavity_case(n, device, precond="Jacobi"):
         case.set_patch_bc("U", nm, "fixedValue", (1.0, 0, 0) if nm == "lid" else (0, 0, 0))
         case.set_patch_bc("p", nm, "zeroGradient", 0.0)
     case.init_flux()
-    ctl = cf.SimpleControls(max_iterations=1, relax_u=0.7, relax_p=0.3, p_relax_start=0.02, non_orth_correctors=1,
-                            linear_tol=1e-8, linear_max_iter=2000, nu=CAV_NU, p_ref_cell=0, p_ref_value=0.0,
-                            p_preconditioner=precond)
+    ctl = cf.SimpleControls(max_iterations=1, relax_u=0.7, relax_p=0.3, p_relax_start=p_relax_start,
+                            non_orth_correctors=1, linear_tol=1e-8, linear_max_iter=2000, nu=CAV_NU, p_ref_cell=0,
+                            p_ref_value=0.0, p_preconditioner=precond)
     return mesh, case, ctl
 
 
@@ -233,7 +252,7 @@ def case_dict(n):
             + "".join(f"    {nm} {{ U (0 0 0); }}\n" for nm in CH_NAMES[2:]) +
             "}\n"
             "schemes { ddt steady; div upwind; laplacian corrected; grad corrected; }\n"
-            "simple { maxIterations 1; relaxU 0.9; relaxP 0.03; pRelaxStart 0.02; nonOrthCorrectors 1; "
+            "simple { maxIterations 1; relaxU 0.9; relaxP 0.03; pRelaxStart 0.002; nonOrthCorrectors 1; "
             "linearTol 1e-08; linearMaxIter 2000; }\n")
 
 
@@ -744,7 +763,7 @@ def main():
                          "baselines: the command line the ncu captures run")
     ap.add_argument("--profile-warm", type=int, default=0,
                     help="with --profile: outer iterations run before the profiler range opens")
-    ap.add_argument("--workload", default="simple", choices=["simple", "poisson", "blocks", "transient"],
+    ap.add_argument("--workload", default="simple", choices=["simple", "cavity", "poisson", "blocks", "transient"],
                     help="simple: the 2M-cell SIMPLE channel (the headline); poisson: the ~4M-tet "
                          "pressure-Poisson solve, FP64 DIC-PCG vs FP32-in-FP64 refinement; blocks: 64 detail "
                          "blocks of a coupled network, one coupling pass per step, batched vs one after another")
@@ -769,6 +788,13 @@ def main():
         return
     if args.workload == "poisson":
         main_poisson(args, world, rank, local, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    if args.impl == "reference" and args.workload == "cavity":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no pressure reference cell, "
+                                                                  "which the cavity workload needs"}), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -820,8 +846,13 @@ def main_simple(args, world, rank, local, dist):
     """The headline: K SIMPLE outer iterations of the 2M-cell channel on
     device-resident fields after W warm-up iterations.  Every leg counts
     its diverged iterations; a run with any is reported and exits 1."""
-    n = args.cells
-    mesh, case, ctl = make_case(n, local, args.p_precond)
+    cavity = args.workload == "cavity"
+    n = args.cells if not cavity else 2 * args.cells
+    if cavity:
+        mesh, case, ctl = make_cavity_case(n, local, args.p_precond, p_relax_start=5e-4)
+    else:
+        mesh, case, ctl = make_case(n, local, args.p_precond)
+    config = cavity_config(n, args.p_precond) if cavity else workload_config(n, args.p_precond)
     ncell = mesh.n_cells
     if args.profile:
         import torch
@@ -835,7 +866,7 @@ def main_simple(args, world, rank, local, dist):
             r = case.solve(ctl)
         torch.cuda.synchronize(local)
         torch.cuda.profiler.stop()
-        print(json.dumps({"profile": workload_config(n, args.p_precond)["workload"], "steps": args.steps,
+        print(json.dumps({"profile": config["workload"], "steps": args.steps,
                           "warm": args.profile_warm, "u_inner": r.u_inner_iterations,
                           "p_inner": r.p_inner_iterations}))
         return 0
@@ -935,7 +966,7 @@ def main_simple(args, world, rank, local, dist):
     out = {"metric": METRIC, "value": value, "unit": "cell-iter/s", "n_gpus": world, "steps": args.steps,
            "warmup": W, "ms_per_step": t_max * 1e3 / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": workload_config(n, args.p_precond),
+           "config": config,
            "e2e": {"value": e2e, "unit": "cell-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
                    "steps": args.steps, "same_fields_as_timed": e2e_same},
            "gpu_launches": timed.launches, "roofline": roof, "simple_roofline": simple_roof, "clocks": clk.summary(),
@@ -962,7 +993,8 @@ def main_simple(args, world, rank, local, dist):
         barrier(dist)
         U2, p2, phi2 = case.download()
         v_t = allreduce_max(dist, var.ms / 1e3)
-        out["variant"] = {"pressure": workload_config(n, other)["workload"].split("pressure ")[1],
+        out["variant"] = {"pressure": other + (" (FP64 flexible CG, FP32 AMG V-cycle)" if other == "AMG" else
+                                               " (FP64 multicolour DIC-PCG)"),
                           "value": world * ncell * args.steps / v_t, "ms_per_step": v_t * 1e3 / args.steps,
                           "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": var.u / args.steps,
                                                         "pressure": var.p / args.steps},
@@ -1003,7 +1035,7 @@ def main_simple(args, world, rank, local, dist):
     # from rest exactly as it runs it (no pressure reference cell, Jacobi-
     # PCG), timed and compared with the reference's CPU run of that
     # iteration (the cpu_baseline leg) ----
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not cavity:
         case.upload(np.zeros((ncell, 3)), np.zeros(ncell), np.zeros(mesh.n_faces))
         case.init_flux()
         rc = dataclasses.replace(ctl, p_preconditioner="Jacobi")
