@@ -88,8 +88,11 @@ SimpleResult SimpleSession::solve(volVectorField& U, volScalarField& p, surfaceS
 {
     if (&U.mesh() != &mesh_ || &p.mesh() != &mesh_ || &phi.mesh() != &mesh_)
         throw Error("chuanflow_b200: fields belong to another mesh than the session's");
-    if (ctl.cellForce || ctl.dt != 0 || ctl.uTimeOld)
-        throw Error("chuanflow_b200: cell forces and time steps are not on the GPU SIMPLE path");
+    if (ctl.cellForce) throw Error("chuanflow_b200: cell forces are not on the GPU SIMPLE path");
+    // the time term's own checks (simpleSolver.cpp:75-97)
+    if ((ctl.dt > 0 || ctl.uTimeOld) && schemes.ddt != "Euler")
+        throw Error("SIMPLE: the momentum equation is asked to step in time while schemes ddt is '" + schemes.ddt +
+                    "', not 'Euler'");
 
     // boundary conditions, patch by patch, then the per-face velocity values
     // (Fields.h:42, :90, :97): every face of a fixed-value U patch is sent
