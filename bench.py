@@ -29,8 +29,9 @@ reference cell 0), which the reference cannot run as such: it has no
 reference cell.
 
 Every leg counts the outer iterations that diverged (simpleSolver.cpp:360-364:
-non-finite continuity, pressure step or fields); the JSON line carries them
-and the run exits 1 when any did.
+non-finite continuity, pressure step or fields; and, before a blow-up
+overflows, a continuity error 100x the first warm-up step's); the JSON line
+carries them and the run exits 1 when any did.
 """
 import argparse
 import dataclasses
@@ -809,10 +810,19 @@ def main():
     sys.exit(rc)
 
 
+# a step whose continuity error is this many times the first warm-up
+# step's also counts as diverged: a blow-up stays finite (1e17, 1e30) for
+# several iterations before it overflows into the reference's test
+GROWTH = 100.0
+
+
 class Steps:
     """K outer iterations with their device time, launches, inner counts and
     the divergence test of simpleSolver.cpp:360-364 (non-finite continuity,
-    pressure step or fields), which SimpleResult.diverged carries."""
+    pressure step or fields), which SimpleResult.diverged carries, plus a
+    growth test against `ref`, the first warm-up step's continuity error."""
+
+    ref = None
 
     def __init__(self):
         self.ms, self.launches, self.u, self.p, self.diverged, self.cont = 0.0, 0, 0, 0, 0, []
@@ -825,9 +835,16 @@ class Steps:
             self.launches += nl
             self.u += r.u_inner_iterations
             self.p += r.p_inner_iterations
-            self.diverged += int(r.diverged or not np.isfinite(r.final_continuity_error))
-            self.cont.append(r.final_continuity_error)
+            c = r.final_continuity_error
+            if Steps.ref is None and np.isfinite(c):
+                Steps.ref = c
+            self.diverged += int(r.diverged or not np.isfinite(c) or grown(c))
+            self.cont.append(c)
         return self
+
+
+def grown(c):
+    return Steps.ref is not None and c > GROWTH * max(Steps.ref, 1e-300)
 
 
 def rel_l2(a, b):
@@ -904,7 +921,7 @@ def main_simple(args, world, rank, local, dist):
         case.upload(U, p, phi)
         r = case.solve(ctl)
         case.download(U, p, phi)
-        e2e_div += int(r.diverged)
+        e2e_div += int(r.diverged or not np.isfinite(r.final_continuity_error) or grown(r.final_continuity_error))
     e2e_wall = allreduce_max(dist, time.perf_counter() - t0)
     e2e = world * ncell * args.steps / e2e_wall
     e2e_same = bool(np.array_equal(U, U1) and np.array_equal(p, p1) and np.array_equal(phi, phi1))

@@ -526,6 +526,16 @@ __global__ void __launch_bounds__(TPB) k_explicit_op(DMat A, const double* __res
     }
 }
 
+/// Keeps the stream busy for about `us` microseconds (a fixed number of
+/// sleeps; it waits on nothing).
+__global__ void k_hold(int us)
+{
+    for (int i = 0; i < us; ++i) __nanosleep(1000);
+}
+/// the hold before an event-timed chunk: longer than the host takes to
+/// enqueue one timed iteration (four kernels and five events)
+constexpr int kHoldUs = 200;
+
 __global__ void __launch_bounds__(TPB) k_fill(int n, double v, double* a)
 {
     ROW_LOOP(i, n) a[i] = v;
@@ -1306,6 +1316,11 @@ void Ctx::launchChunk(const std::string& key, int n, F&& body)
     const int64_t counted = launches_;
     if (!useGraphs_ || ktime_)
     {
+        // a timed chunk starts behind a short sleep, so that its events and
+        // kernels are all queued before the GPU reaches the first event: on
+        // an idle stream an event's timestamp would also hold the time the
+        // host took to submit the kernel after it
+        if (ktime_) k_hold<<<1, 32, 0, stream_>>>(kHoldUs);
         for (int i = 0; i < n; ++i) body(i);
         launches_ = counted;
         return;
