@@ -98,10 +98,20 @@ KERNEL_NAMES = {
     "bi_spmv2": "k_bi_spmv2 (momentum BiCGStab, 3 components: t = A s^, s^ formed per column, + t.t, t.s)",
     "bi_x": "k_bi_x (momentum BiCGStab, 3 components: x += alpha z + omega s^, r update + |r| + r0.r)",
     "dic_apply": "k_dic_fwd/k_dic_bwd (multicolour DIC z = M^-1 r, all colour phases)",
+    "bia_p": "k_bia_p (AMG momentum BiCGStab, 3 components: p update)",
+    "bia_vcycle_z": "amgCycle3 z = M p (FP32 V-cycle of the momentum matrix, 3 components, all levels)",
+    "bia_spmv1": "k_bi_spmv1 (AMG momentum BiCGStab, 3 components: v = A z + r0.v)",
+    "bia_s": "k_bia_s (AMG momentum BiCGStab, 3 components: s = r - alpha v)",
+    "bia_vcycle_s": "amgCycle3 s^ = M s (FP32 V-cycle of the momentum matrix, 3 components, all levels)",
+    "bia_spmv2": "k_bia_spmv2 (AMG momentum BiCGStab, 3 components: t = A s^ + t.t, t.s)",
+    "bia_x": "k_bia_x (AMG momentum BiCGStab, 3 components: x += alpha z + omega s^, r update + |r| + r0.r)",
 }
 
 
-MEASURED_TRAFFIC = {}
+# DRAM bytes (read + write) per launch from one full-set ncu capture of
+# k_bi_spmv2 on the 2M-cell channel (launches 21-22 of its third outer
+# iteration: 334.2 and 333.3 MB)
+MEASURED_TRAFFIC = {"bi_spmv2": 334.2e6}
 
 
 def kernel_bytes(N, F, s=8, i=4):
@@ -112,6 +122,14 @@ def kernel_bytes(N, F, s=8, i=4):
     two SpMVs always carry all three."""
     spmv_sym = 3 * s * N + s * F + 2 * i * F       # x in, y out, diag + one coefficient per face, indices
     mat3 = s * N + 2 * s * F + 2 * i * F           # diag + both coefficients + indices, shared by 3 components
+    # the three-component V-cycle at its finest level: two FP32 SELL passes
+    # (value and column per entry, N + 2F entries), D^-1 twice, the
+    # aggregate map and member list; per component the FP64 input read by
+    # both passes, the FP32 sweep and residual written, the residual read by
+    # the restriction, the sweep read again and the FP64 output written; the
+    # coarser levels add about 30% (as for the pressure V-cycle)
+    f4 = 4
+    vcycle3 = (1.3 * (2 * (N + 2 * F) * 2 * f4 + 4 * f4 * N), 1.3 * (2 * s * N + 4 * f4 * N + s * N))
     return {"cg_spmv": (spmv_sym, 0), "cg_update": (7 * s * N, 0), "cg_p": (4 * s * N, 0),
             # invD in; per component r, p, v in, p, z out
             "bi_p": (s * N, 5 * s * N),
@@ -121,10 +139,21 @@ def kernel_bytes(N, F, s=8, i=4):
             "bi_spmv2": (mat3 + s * N, 3 * s * N),
             # invD; per component x, z, r, v, t, r0 in, x, r out
             "bi_x": (s * N, 8 * s * N),
-            "dic_apply": (3 * s * N + 2 * (s * F + 2 * i * F), 0)}
+            "dic_apply": (3 * s * N + 2 * (s * F + 2 * i * F), 0),
+            # the AMG-preconditioned momentum BiCGStab: per component r, p, v
+            # in, p out
+            "bia_p": (0, 4 * s * N),
+            "bia_vcycle_z": vcycle3, "bia_vcycle_s": vcycle3,
+            "bia_spmv1": (mat3, 3 * s * N),
+            # per component r, v in, s out
+            "bia_s": (0, 3 * s * N),
+            # matrix; per component s^ in (gathered), s in, t out
+            "bia_spmv2": (mat3, 3 * s * N),
+            # per component x, z, s, s^, t, r0 in, x, r out
+            "bia_x": (0, 8 * s * N)}
 
 
-SKIPS_DONE = ("bi_p", "bi_x")
+SKIPS_DONE = ("bi_p", "bi_x", "bia_p", "bia_vcycle_z", "bia_s", "bia_vcycle_s", "bia_x")
 
 
 def simple_step_bytes(N, F, Fb, n_orth, it_p, precond, solver_bytes, s=8, i=4):
@@ -757,6 +786,9 @@ def main():
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--p-precond", default="AMG", choices=["Jacobi", "DIC", "AMG"])
+    ap.add_argument("--u-precond", default="Jacobi", choices=["Jacobi", "AMG"],
+                    help="simple: the momentum BiCGStab's preconditioner (Jacobi: the reference's; AMG: the FP32 "
+                         "V-cycle of the momentum matrix)")
     ap.add_argument("--no-variant", action="store_true",
                     help="simple: skip the second pressure solver's timing from the same start state")
     ap.add_argument("--profile", action="store_true",
@@ -869,6 +901,7 @@ def main_simple(args, world, rank, local, dist):
         mesh, case, ctl = make_cavity_case(n, local, args.p_precond, p_relax_start=5e-4)
     else:
         mesh, case, ctl = make_case(n, local, args.p_precond)
+    ctl = dataclasses.replace(ctl, u_preconditioner=args.u_precond)
     config = cavity_config(n, args.p_precond) if cavity else workload_config(n, args.p_precond)
     ncell = mesh.n_cells
     if args.profile:
@@ -950,14 +983,14 @@ def main_simple(args, world, rank, local, dist):
         if cnt:
             us = tot / cnt * 1e3
             shared, per = alg[k]
-            comps = kcomp[k] / cnt if k in SKIPS_DONE else (3 if k.startswith("bi_") else 0)
+            comps = kcomp[k] / cnt if k in SKIPS_DONE else (3 if k.startswith("bi") else 0)
             b = shared + per * comps
             kernels[k] = {"launches": cnt, "total_ms": tot, "avg_us": us, "alg_bytes": b,
-                          "components_per_launch": comps if k.startswith("bi_") else None,
+                          "components_per_launch": comps if k.startswith("bi") else None,
                           "achieved_gbs": b / (us * 1e-6) / 1e9}
             # scaled from the kernel-timing iteration to the timed region's
             # mean inner counts
-            scale = ((timed.u / args.steps) / max(1, ktimed.u) if k.startswith("bi_")
+            scale = ((timed.u / args.steps) / max(1, ktimed.u) if k.startswith("bi")
                      else (timed.p / args.steps) / max(1, ktimed.p))
             solver_bytes += cnt * b * scale
     top = max(kernels, key=lambda k: kernels[k]["total_ms"])
@@ -1024,6 +1057,32 @@ def main_simple(args, world, rank, local, dist):
         out["field_error"] = dict(field_errors(*test, *fp64),
                                   against="FP64 DIC-PCG pressure (FP64 throughout), the same K iterations from the same "
                                           "start state; relative L2")
+
+    # ---- the other momentum preconditioner: the same K iterations from the
+    # same start state with the reference's Jacobi-BiCGStab momentum solve
+    # or the AMG-preconditioned one, against the FP64 DIC fields ----
+    if not args.no_variant:
+        other_u = "AMG" if args.u_precond == "Jacobi" else "Jacobi"
+        c4 = dataclasses.replace(ctl, u_preconditioner=other_u)
+        case.upload(U0, p0, phi0)
+        case.solve(c4)
+        case.upload(U0, p0, phi0)
+        barrier(dist)
+        mom = Steps().run(case, c4, args.steps)
+        barrier(dist)
+        U4, p4, phi4 = case.download()
+        u_t = allreduce_max(dist, mom.ms / 1e3)
+        out["momentum_" + other_u.lower()] = {
+            "momentum": ("BiCGStab with the FP32 AMG V-cycle of the momentum matrix as right preconditioner (one "
+                         "V-cycle for the three components), FP64 vectors and |r|inf/|b|inf test at 1e-8"
+                         if other_u == "AMG" else "the reference's Jacobi-BiCGStab"),
+            "value": world * ncell * args.steps / u_t, "ms_per_step": u_t * 1e3 / args.steps,
+            "inner_iterations_per_step": {"momentum_bicgstab_sum_over_components": mom.u / args.steps,
+                                          "pressure": mom.p / args.steps},
+            "continuity": {"first": mom.cont[0], "last": mom.cont[-1]},
+            "diverged_steps": mom.diverged,
+            "field_error_vs_fp64_dic": field_errors(U4, p4, phi4, *fp64)}
+        diverged += mom.diverged
 
     # ---- mixed precision: the same K iterations with the pressure matrix
     # rounded to FP32 and FP32 DIC-PCG corrections inside FP64 refinement

@@ -39,7 +39,8 @@ class _Controls(C.Structure):
                 ("non_orth_correctors", C.c_int32), ("relax_u", C.c_double), ("relax_p", C.c_double),
                 ("p_relax_start", C.c_double), ("body_force", C.c_double * 3), ("nu", C.c_double),
                 ("p_precond", C.c_int32), ("verbose", C.c_int32), ("p_ref_cell", C.c_int64),
-                ("p_ref_value", C.c_double), ("dt", C.c_double), ("u_time_old", C.c_int32)]
+                ("p_ref_value", C.c_double), ("dt", C.c_double), ("u_time_old", C.c_int32),
+                ("u_precond", C.c_int32)]
 
 
 class _Result(C.Structure):
@@ -313,6 +314,7 @@ class SimpleControls:
     p_ref_value: float = 0.0
     dt: float = 0.0          # SimpleControls::dt (pseudo-) time step; 0: steady
     u_time_old: int = 0      # 1: the velocity at the start of the call is the old level
+    u_preconditioner: str = "Jacobi"  # the momentum BiCGStab's: "Jacobi" (the reference's) or "AMG"
 
     def _c(self):
         c = _Controls()
@@ -335,6 +337,7 @@ class SimpleControls:
         c.p_ref_value = self.p_ref_value
         c.dt = self.dt
         c.u_time_old = int(self.u_time_old)
+        c.u_precond = U_PRECOND[self.u_preconditioner]
         return c
 
 
@@ -362,7 +365,9 @@ class SolverReport:
 CELL_ORDER = {None: -1, "identity": 0, "colour": 1, "rcm": 2, "rcm-colour": 3}
 
 
-KERNEL_SLOTS = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_spmv2", "bi_x", "dic_apply")
+U_PRECOND = {"Jacobi": 0, "AMG": 3}
+KERNEL_SLOTS = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_spmv2", "bi_x", "dic_apply",
+                "bia_p", "bia_vcycle_z", "bia_spmv1", "bia_s", "bia_vcycle_s", "bia_spmv2", "bia_x")
 
 
 class SimpleCase:
@@ -446,15 +451,15 @@ class SimpleCase:
         _check(lib().cfg_kernel_timing(self._h, C.c_int32(int(enable))))
 
     def kernel_stats(self):
-        out = np.zeros(16)
-        _check(lib().cfg_kernel_stats(self._h, _dp(out)))
+        out = np.zeros(2 * len(KERNEL_SLOTS))
+        _check(lib().cfg_kernel_stats(self._h, _dp(out), C.c_int32(len(KERNEL_SLOTS))))
         return {n: (int(out[2 * i]), float(out[2 * i + 1])) for i, n in enumerate(KERNEL_SLOTS)}
 
     def kernel_components(self):
         """Per solver kernel, its timed launches weighted by the vector
         components each still iterated on."""
-        out = np.zeros(8)
-        _check(lib().cfg_kernel_components(self._h, _dp(out)))
+        out = np.zeros(len(KERNEL_SLOTS))
+        _check(lib().cfg_kernel_components(self._h, _dp(out), C.c_int32(len(KERNEL_SLOTS))))
         return {n: float(out[i]) for i, n in enumerate(KERNEL_SLOTS)}
 
     # ---- the pressure-Poisson system on its own ----
@@ -488,6 +493,15 @@ class SimpleCase:
         z = np.zeros(self.mesh.n_cells)
         _check(lib().cfg_poisson_amg_apply(self._h, _dp(_f64(r)), _dp(z)))
         return z
+
+    def poisson_amg_apply3(self, r3, z3=None, done=(0, 0, 0)):
+        """The three-component V-cycle on r3 (3 x n); component q is left as
+        z3[q] (zeros by default) when done[q]."""
+        n = self.mesh.n_cells
+        z = np.zeros(3 * n) if z3 is None else np.array(z3, np.float64, copy=True).reshape(-1)
+        d = (C.c_int32 * 3)(*[int(v) for v in done])
+        _check(lib().cfg_poisson_amg_apply3(self._h, _dp(_f64(np.asarray(r3).reshape(-1))), _dp(z), d))
+        return z.reshape(3, n)
 
     # ---- diagnostics ----
     def probe_equations(self, controls: SimpleControls, xprobe):

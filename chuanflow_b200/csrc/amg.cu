@@ -48,6 +48,9 @@ struct AmgLevel
     int nnzNext = 0;
     // work vectors: rhs, first sweep, residual, output
     float *b = nullptr, *x = nullptr, *r = nullptr, *xo = nullptr;
+    // the same for the three-component V-cycle (component q at q * n),
+    // allocated on its first use
+    float *b3 = nullptr, *x3 = nullptr, *r3 = nullptr, *xo3 = nullptr;
 };
 
 /// Device scalars of the device-resident flexible CG (amgFcg)
@@ -293,6 +296,262 @@ __global__ void __launch_bounds__(TPB) k_amg_dinv(int n, const int* __restrict__
 __global__ void __launch_bounds__(TPB) k_amg_dinv0(int n, const double* __restrict__ diag, float* __restrict__ dinv)
 {
     FOR_ROWS(i, n) dinv[i] = diag[i] != 0.0 ? static_cast<float>(1.0 / diag[i]) : 1.0f;
+}
+
+// ---- the V-cycle on three right-hand sides at once (the momentum
+// components share their matrix): the same arithmetic per component as the
+// single V-cycle above, with the matrix read once for the three.  Level
+// vectors hold component q at offset q * n.  `done` (the BiCGStab's
+// per-component flags) skips a converged component's work; its outputs are
+// left as they were.
+
+/// one SELL row of the finest operator against three vectors
+template <int W, class F>
+__device__ __forceinline__ void sell_row3(const DMat& A, const float* __restrict__ val, int c, float (&s)[3], F f)
+{
+    const int sl = c >> 5, lane = c & 31;
+    const int e0 = __ldg(A.start + sl) + lane, e1 = __ldg(A.start + sl + 1);
+    s[0] = s[1] = s[2] = 0.0f;
+    if constexpr (W > 0)
+    {
+        constexpr int CH = W > 8 ? 8 : W;
+#pragma unroll
+        for (int k0 = 0; k0 < W; k0 += CH)
+        {
+            int col[CH];
+            float v[CH];
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+            {
+                const int e = e0 + 32 * (k0 + k);
+                col[k] = (k0 + k < W && e < e1) ? __ldg(A.col + e) : -1;
+                v[k] = (k0 + k < W && e < e1) ? __ldg(val + e) : 0.0f;
+            }
+            float g[CH][3];
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+            {
+                if (col[k] >= 0) f(col[k], g[k]);
+                else g[k][0] = g[k][1] = g[k][2] = 0.0f;
+            }
+#pragma unroll
+            for (int k = 0; k < CH; ++k)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) s[q] += v[k] * g[k][q];
+        }
+    }
+    else
+    {
+        for (int e = e0; e < e1; e += 32)
+        {
+            const int col = __ldg(A.col + e);
+            if (col < 0) break;
+            float g[3];
+            f(col, g);
+            const float v = __ldg(val + e);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) s[q] += v * g[q];
+        }
+    }
+}
+
+/// a coarse CSR row against three vectors, summed by a group of G lanes
+template <int G, class F>
+__device__ __forceinline__ void group_row3(const int* __restrict__ rs, const int* __restrict__ cols,
+                                           const float* __restrict__ val, int i, int l, float (&s)[3], F f)
+{
+    s[0] = s[1] = s[2] = 0.0f;
+    if (i >= 0)
+        for (int e = __ldg(rs + i) + l; e < __ldg(rs + i + 1); e += G)
+        {
+            float g[3];
+            f(__ldg(cols + e), g);
+            const float v = __ldg(val + e);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) s[q] += v * g[q];
+        }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+}
+
+struct Active3
+{
+    bool a[3];
+    __device__ bool none() const { return !(a[0] || a[1] || a[2]); }
+};
+__device__ __forceinline__ Active3 active3(const int* done)
+{
+    return Active3{{done[0] == 0, done[1] == 0, done[2] == 0}};
+}
+
+/// finest level, first sweep and residual for three FP64 right-hand sides
+template <int W>
+__global__ void __launch_bounds__(TPB) k_amgv_pre0(const int* __restrict__ done, DMat A, const float* __restrict__ val,
+                                                   const float* __restrict__ dinv, CV3P b, float* __restrict__ x,
+                                                   float* __restrict__ r)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    const int n = A.n;
+    FOR_ROWS(c, n)
+    {
+        float s[3];
+        sell_row3<W>(A, val, c, s, [&](int j, float (&g)[3]) {
+            const float wd = kOmega * __ldg(dinv + j);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? wd * static_cast<float>(__ldg(b.c[q] + j)) : 0.0f;
+        });
+        const float dc = dinv[c];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (act.a[q])
+            {
+                const float bc = static_cast<float>(b.c[q][c]);
+                x[q * n + c] = kOmega * dc * bc;
+                r[q * n + c] = bc - s[q];
+            }
+    }
+}
+
+/// coarse level, the same on CSR
+__global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, int n, const int* __restrict__ rs,
+                                                  const int* __restrict__ cols, const float* __restrict__ val,
+                                                  const float* __restrict__ dinv, const float* __restrict__ b,
+                                                  float* __restrict__ x, float* __restrict__ r)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    const int l = threadIdx.x % kGroup;
+    const int stride = gridDim.x * (TPB / kGroup);
+    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
+    {
+        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        float s[3];
+        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) {
+            const float wd = kOmega * __ldg(dinv + j);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? wd * __ldg(b + q * n + j) : 0.0f;
+        });
+        if (i >= 0 && l == 0)
+        {
+            const float di = dinv[i];
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (act.a[q])
+                {
+                    const float bi = b[q * n + i];
+                    x[q * n + i] = kOmega * di * bi;
+                    r[q * n + i] = bi - s[q];
+                }
+        }
+    }
+}
+
+/// the residuals summed over each aggregate
+__global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ done, int n, int nc,
+                                                       const int* __restrict__ ms, const int* __restrict__ mem,
+                                                       const float* __restrict__ r, float* __restrict__ bc)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    FOR_ROWS(I, nc)
+    {
+        float s[3] = {0.0f, 0.0f, 0.0f};
+        for (int k = ms[I]; k < ms[I + 1]; ++k)
+        {
+            const int i = mem[k];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) s[q] += r[q * n + i];
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (act.a[q]) bc[q * nc + I] = s[q];
+    }
+}
+
+/// the coarsest solve for each component (block q: component q)
+__global__ void __launch_bounds__(kDenseMax) k_amgv_dense(const int* __restrict__ done, int n,
+                                                          const float* __restrict__ m, const float* __restrict__ b,
+                                                          float* __restrict__ x)
+{
+    const int q = blockIdx.x;
+    if (done[q]) return;
+    const int i = threadIdx.x;
+    if (i >= n) return;
+    float s = 0.0f;
+    for (int j = 0; j < n; ++j) s += m[i * n + j] * b[q * n + j];
+    x[q * n + i] = s;
+}
+
+/// coarse level: xo = x + s P xc + w D^-1 (b - A (x + s P xc))
+__global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done, int n, int nNext,
+                                                   const int* __restrict__ rs, const int* __restrict__ cols,
+                                                   const float* __restrict__ val, const float* __restrict__ dinv,
+                                                   const float* __restrict__ b, const float* __restrict__ x,
+                                                   const float* __restrict__ xc, const int* __restrict__ agg,
+                                                   float* __restrict__ xo)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    const int l = threadIdx.x % kGroup;
+    const int stride = gridDim.x * (TPB / kGroup);
+    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
+    {
+        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        float s[3];
+        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) {
+            const int aj = __ldg(agg + j);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                g[q] = act.a[q] ? __ldg(x + q * n + j) + kScale * __ldg(xc + q * nNext + aj) : 0.0f;
+        });
+        if (i >= 0 && l == 0)
+        {
+            const int ai = agg[i];
+            const float di = dinv[i];
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (act.a[q])
+                    xo[q * n + i] = x[q * n + i] + kScale * xc[q * nNext + ai] + kOmega * di * (b[q * n + i] - s[q]);
+        }
+    }
+}
+
+/// finest level: z = y + w D^-1 (b - A y), y = x + s P xc, into FP64
+template <int W>
+__global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done, DMat A, int nNext,
+                                                    const float* __restrict__ val, const float* __restrict__ dinv,
+                                                    CV3P b, const float* __restrict__ x, const float* __restrict__ xc,
+                                                    const int* __restrict__ agg, V3P z)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    const int n = A.n;
+    FOR_ROWS(c, n)
+    {
+        float s[3];
+        sell_row3<W>(A, val, c, s, [&](int j, float (&g)[3]) {
+            const int aj = __ldg(agg + j);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                g[q] = act.a[q] ? __ldg(x + q * n + j) + kScale * __ldg(xc + q * nNext + aj) : 0.0f;
+        });
+        const int ac = agg[c];
+        const float dc = dinv[c];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (act.a[q])
+            {
+                const float y = x[q * n + c] + kScale * xc[q * nNext + ac];
+                z.c[q][c] = static_cast<double>(y + kOmega * dc * (static_cast<float>(b.c[q][c]) - s[q]));
+            }
+    }
 }
 
 /// a host CSR pattern whose entries remember where their values live
@@ -589,6 +848,73 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
     }
     launchCheck("amg_vcycle", 3 * (L - 1) + 1);
 }
+
+/// z_q = V-cycle(b_q) for the three components whose done flag is clear
+/// (the BiCGStab's flags; a converged component keeps its old z_q)
+void Ctx::amgCycle3(CV3P b, V3P z, const int* done)
+{
+    AmgState& a = *amg_;
+    if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
+    if (!a.lv[0].x3) fail(CFG_EINVAL, "amg: the three-component vectors are not allocated (amgVectors3)");
+    const int L = static_cast<int>(a.lv.size());
+    const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
+    auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
+    auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
+    const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
+    for (int l = 0; l + 1 < L; ++l)
+    {
+        AmgLevel& V = a.lv[l];
+        AmgLevel& N = a.lv[l + 1];
+        if (l == 0)
+        {
+            if (Wsel == 7) k_amgv_pre0<7><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
+            else if (Wsel == 16) k_amgv_pre0<16><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
+            else k_amgv_pre0<0><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
+        }
+        else
+            k_amgv_pre<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.x3, V.r3);
+        k_amgv_restrict<<<grid(N.n), TPB, 0, stream_>>>(done, V.n, N.n, V.ms, V.mem, V.r3, N.b3);
+    }
+    k_amgv_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
+    for (int l = L - 2; l >= 0; --l)
+    {
+        AmgLevel& V = a.lv[l];
+        const AmgLevel& N = a.lv[l + 1];
+        const float* xc = (l + 1 == L - 1) ? N.x3 : N.xo3;
+        if (l == 0)
+        {
+            if (Wsel == 7)
+                k_amgv_post0<7><<<GS_, TPB, 0, stream_>>>(done, A, N.n, amgVals32_, V.dinv, b, V.x3, xc, V.agg, z);
+            else if (Wsel == 16)
+                k_amgv_post0<16><<<GS_, TPB, 0, stream_>>>(done, A, N.n, amgVals32_, V.dinv, b, V.x3, xc, V.agg, z);
+            else
+                k_amgv_post0<0><<<GS_, TPB, 0, stream_>>>(done, A, N.n, amgVals32_, V.dinv, b, V.x3, xc, V.agg, z);
+        }
+        else
+            k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.x3, xc,
+                                                          V.agg, V.xo3);
+    }
+    launchCheck("amg_vcycle3", 3 * (L - 1) + 1);
+}
+
+/// The level vectors of the three-component V-cycle, allocated once (before
+/// any stream capture that launches amgCycle3).
+void Ctx::amgVectors3()
+{
+    if (!amg_) amgSetup();
+    for (auto& V : amg_->lv)
+        if (!V.x3)
+        {
+            const size_t m = 3 * static_cast<size_t>(V.n);
+            V.b3 = alloc<float>(m);
+            V.x3 = alloc<float>(m);
+            V.r3 = alloc<float>(m);
+            V.xo3 = alloc<float>(m);
+        }
+}
+
+/// The number of kernels one amgCycle3 launches.
+int Ctx::amgCycleKernels() const { return amg_ ? 3 * (static_cast<int>(amg_->lv.size()) - 1) + 1 : 0; }
 
 namespace
 {

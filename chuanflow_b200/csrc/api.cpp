@@ -428,11 +428,14 @@ int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable)
     });
 }
 
-int cfg_kernel_stats(const cfg_ctx* ctx, double out[16])
+static_assert(cfg::Ctx::KS_COUNT == CFG_KERNEL_SLOTS, "the header's slot count");
+
+int cfg_kernel_stats(const cfg_ctx* ctx, double* out, int32_t slots)
 {
     return guard([&] {
         need(ctx && out, "cfg_kernel_stats: null argument");
-        for (int k = 0; k < cfg::Ctx::KS_COUNT; ++k)
+        need(slots >= 0, "cfg_kernel_stats: negative slot count");
+        for (int k = 0; k < cfg::Ctx::KS_COUNT && k < slots; ++k)
         {
             out[2 * k] = ctx->c->kstat[k][0];
             out[2 * k + 1] = ctx->c->kstat[k][1];
@@ -440,11 +443,12 @@ int cfg_kernel_stats(const cfg_ctx* ctx, double out[16])
     });
 }
 
-int cfg_kernel_components(const cfg_ctx* ctx, double out[8])
+int cfg_kernel_components(const cfg_ctx* ctx, double* out, int32_t slots)
 {
     return guard([&] {
         need(ctx && out, "cfg_kernel_components: null argument");
-        for (int k = 0; k < cfg::Ctx::KS_COUNT; ++k) out[k] = ctx->c->kcomp[k];
+        need(slots >= 0, "cfg_kernel_components: negative slot count");
+        for (int k = 0; k < cfg::Ctx::KS_COUNT && k < slots; ++k) out[k] = ctx->c->kcomp[k];
     });
 }
 
@@ -515,6 +519,14 @@ int cfg_poisson_amg_apply(cfg_ctx* ctx, const double* r, double* z)
     return guard([&] {
         need(ctx && r && z, "cfg_poisson_amg_apply: null argument");
         ctx->c->poissonAmgApply(r, z);
+    });
+}
+
+int cfg_poisson_amg_apply3(cfg_ctx* ctx, const double* r, double* z, const int32_t done[3])
+{
+    return guard([&] {
+        need(ctx && r && z && done, "cfg_poisson_amg_apply3: null argument");
+        ctx->c->poissonAmgApply3(r, z, done);
     });
 }
 
@@ -739,6 +751,10 @@ CaseSpec parseCase(const char* path)
                       : pp == "AMG"  ? CFG_PRECOND_AMG
                       : pp == "IR32" ? CFG_PRECOND_IR32
                                      : CFG_PRECOND_JACOBI;
+        const std::string up = g.wordOr("uPreconditioner", "Jacobi");
+        if (up != "Jacobi" && up != "AMG")
+            cfg::fail(CFG_ESETUP, "gpu: unknown uPreconditioner '" + up + "' (Jacobi | AMG)");
+        c.u_precond = up == "AMG" ? CFG_PRECOND_AMG : CFG_PRECOND_JACOBI;
         c.p_ref_cell = static_cast<int64_t>(g.numberOr("pRefCell", -1));
         c.p_ref_value = g.numberOr("pRefValue", 0.0);
         c.verbose = static_cast<int32_t>(g.numberOr("verbose", 1));
@@ -775,7 +791,7 @@ int cfg_case_inspect(const char* path, char* out, size_t size)
             c.pcorr_tol, c.momentum_tol, c.linear_tol, c.linear_max_iter, c.non_orth_correctors, c.relax_u, c.relax_p,
             c.p_relax_start);
         add("force %.17g %.17g %.17g\nnu %.17g\n", c.body_force[0], c.body_force[1], c.body_force[2], c.nu);
-        add("gpu %d %lld %.17g\n", c.p_precond, static_cast<long long>(c.p_ref_cell), c.p_ref_value);
+        add("gpu %d %lld %.17g %d\n", c.p_precond, static_cast<long long>(c.p_ref_cell), c.p_ref_value, c.u_precond);
         if (cs.hasU0) add("initialU %.17g %.17g %.17g\n", cs.u0[0], cs.u0[1], cs.u0[2]);
         add("turbulence %s %.17g %.17g %.17g %.17g %.17g %.17g %.17g\n", cs.turbModel.c_str(), cs.turbIntensity,
             cs.turbLength, cs.turbRelax, cs.cDES, cs.reOnset, cs.onsetWidth, cs.gammaRate);
@@ -919,6 +935,7 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
         bool graphable = true;
         for (size_t i = 0; i < batch->blocks.size(); ++i)
             graphable = graphable && controls[i].max_iterations == 1 && controls[i].p_precond != CFG_PRECOND_AMG &&
+                        controls[i].u_precond == CFG_PRECOND_JACOBI &&
                         controls[i].p_precond != CFG_PRECOND_MPNN && controls[i].p_precond != CFG_PRECOND_IR32 &&
                         controls[i].p_precond != CFG_PRECOND_AMG_MPNN &&
                         batch->blocks[i]->turbulenceModelName() != "gammaTransition";

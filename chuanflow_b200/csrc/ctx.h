@@ -152,6 +152,14 @@ public:
         KS_BI_SPMV2,
         KS_BI_X,
         KS_DIC_APPLY,
+        // the momentum BiCGStab with the AMG V-cycle (u_precond AMG)
+        KS_BIA_P,
+        KS_BIA_VC_Z,
+        KS_BIA_SPMV1,
+        KS_BIA_S,
+        KS_BIA_VC_S,
+        KS_BIA_SPMV2,
+        KS_BIA_X,
         KS_COUNT
     };
     double kstat[KS_COUNT][2] = {};
@@ -178,6 +186,13 @@ private:
                cfg_solver_report* rep, int normType = 0);
     void runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nComp, double tol, int maxIter,
                   cfg_solver_report* reps);
+    void runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, double tol, int maxIter,
+                    cfg_solver_report* reps);
+    /// the momentum preconditioner of the outer iteration being enqueued
+    /// (cfg_simple_controls.u_precond) and the FP32 copy of the momentum
+    /// values the V-cycle's finest level reads
+    int uPrecond_ = CFG_PRECOND_JACOBI;
+    float* uVal32_ = nullptr;
     void launchCheck(const char* what, int kernels = 1);
     int linUpwindGrad(const BcTab& ub, int gradScheme);
     template <class F>
@@ -213,6 +228,7 @@ public:
     /// the AMG hierarchy for the Poisson system's current values
     void poissonAmg(double* out);
     void poissonAmgApply(const double* r, double* z);
+    void poissonAmgApply3(const double* r, double* z, const int32_t done[3]);
 
 private:
     void setNu(double nu);
@@ -238,6 +254,9 @@ private:
     void amgValues(const double* vals, const double* diag, const float* vals32);
     void amgApply(const double* r, double* z);
     void amgCycle(const double* r, double* z, const double* q, FcgState* st);
+    void amgCycle3(CV3P b, V3P z, const int* done);
+    void amgVectors3();
+    int amgCycleKernels() const;
     void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,
                 cfg_solver_report* rep);
     void amgInfo(double* out);
@@ -357,7 +376,7 @@ private:
     bool ktime_ = false;
     bool useGraphs_ = true;
     std::map<std::string, cudaGraphExec_t> graphs_;
-    static constexpr int kEvPerIter = 6;  // events per solver iteration of a chunk (kernels + 1)
+    static constexpr int kEvPerIter = 8;  // events per solver iteration of a chunk (kernels + 1)
     std::vector<cudaEvent_t> kev_;
     void tmark(int k, int j);
     void harvest(int ran, const int* slots, int nSlots, int active = 1);

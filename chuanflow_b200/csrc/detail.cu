@@ -634,10 +634,10 @@ void batchPass(cfg_batch& b, const double* q, const cfg_simple_controls* ctl, cf
         for (int i = 0; i < static_cast<int>(b.blocks.size()); ++i)
             if (ctl[i].max_iterations != 1 || ctl[i].p_precond == CFG_PRECOND_AMG ||
                 ctl[i].p_precond == CFG_PRECOND_MPNN || ctl[i].p_precond == CFG_PRECOND_IR32 ||
-                ctl[i].p_precond == CFG_PRECOND_AMG_MPNN ||
+                ctl[i].p_precond == CFG_PRECOND_AMG_MPNN || ctl[i].u_precond != CFG_PRECOND_JACOBI ||
                 b.blocks[static_cast<size_t>(i)]->turbulenceModelName() == "gammaTransition")
                 fail(CFG_EINVAL, "batch: the single-graph pass runs one outer iteration per block with Jacobi or DIC "
-                                 "pressure and no gammaTransition model");
+                                 "pressure, Jacobi momentum and no gammaTransition model");
         batchPassGraph(b, q, ctl, out, wallMs);
         return;
     }

@@ -1576,6 +1576,84 @@ void Ctx::runBiCG3(const double* vals, const double* diag, V3P b, V3P x, int nCo
     }
 }
 
+/// The momentum BiCGStab of runBiCG3 with the FP32 AMG V-cycle of the
+/// momentum matrix as right preconditioner (z = M p, s^ = M s in place of
+/// the reference's D^-1 scaling, Matrix.cpp:262-300); the three components
+/// iterate in lockstep, each with its own scalars and stopping test, and a
+/// V-cycle serves all components still iterating.  The hierarchy's values
+/// must be this matrix's (amgValues).  Host-polled chunks of iterations,
+/// each chunk a CUDA graph after its first launch.
+void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, double tol, int maxIter,
+                     cfg_solver_report* reps)
+{
+    const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
+    SolveState init{};
+    init.tol = tol;
+    init.maxIter = maxIter;
+    init.nComp = 3;
+    const int n = dm_.nC;
+    const int* done = reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done));
+    const int vk = amgCycleKernels();
+    CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    auto loop = [&](auto Wc) {
+        constexpr int W = decltype(Wc)::value;
+        k_bi_init<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, diag, bInvD_, b, x, br_, br0_, bp_, bv_, partials_, st_);
+        launchCheck("bicga_init");
+        int itBefore = 0, lastChunk = 0, activeBefore = 3;
+        auto itMax = [&] {
+            int m = 0;
+            for (int q = 0; q < 3; ++q) m = std::max(m, stHost_->it[q]);
+            return m;
+        };
+        for (int launched = 0, chunk = 2;;)
+        {
+            CFG_CUDA(cudaMemcpyAsync(stHost_, st_, sizeof(SolveState), cudaMemcpyDeviceToHost, stream_));
+            CFG_CUDA(cudaStreamSynchronize(stream_));
+            if (lastChunk > 0)
+            {
+                static const int slots[7] = {KS_BIA_P, KS_BIA_VC_Z, KS_BIA_SPMV1, KS_BIA_S,
+                                             KS_BIA_VC_S, KS_BIA_SPMV2, KS_BIA_X};
+                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 7, activeBefore);
+            }
+            itBefore = itMax();
+            activeBefore = 0;
+            for (int q = 0; q < 3; ++q) activeBefore += stHost_->done[q] ? 0 : 1;
+            if (stHost_->allDone || launched >= maxIter) break;
+            const int m = ktime_ ? 1 : std::min(chunk, maxIter - launched);
+            launchChunk(ptrKey("bicga", {vals, diag, x.c[0], x.c[1], x.c[2]}, W), m, [&](int k) {
+                tmark(k, 0);
+                k_bia_p<3><<<GS_, TPB, 0, stream_>>>(n, br_, bp_, bv_, st_);
+                tmark(k, 1);
+                amgCycle3(cv(bp_), bz_, done);
+                tmark(k, 2);
+                k_bi_spmv1<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
+                tmark(k, 3);
+                k_bia_s<3><<<GS_, TPB, 0, stream_>>>(n, br_, bv_, bs_, st_);
+                tmark(k, 4);
+                amgCycle3(cv(bs_), bsh_, done);
+                tmark(k, 5);
+                k_bia_spmv2<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bs_, bt_, partials_, st_);
+                tmark(k, 6);
+                k_bia_x<3><<<GS_, TPB, 0, stream_>>>(n, x, bz_, bs_, bsh_, bt_, br_, br0_, partials_, st_);
+                tmark(k, 7);
+                launchCheck("bicga_iter", 0);
+            });
+            launches_ += static_cast<int64_t>(m) * (5 + 2 * vk);
+            launched += m;
+            lastChunk = m;
+            chunk = std::min(chunk * 2, 16);
+        }
+    };
+    dispatchW(maxW_, [&](auto Wc) { loop(Wc); });
+    for (int q = 0; q < 3; ++q)
+    {
+        reps[q].iterations = stHost_->it[q];
+        reps[q].converged = stHost_->conv[q];
+        reps[q].initial_residual = stHost_->init[q];
+        reps[q].final_residual = stHost_->fin[q];
+    }
+}
+
 /// Blocks for a grid-stride row loop over `rows` rows.
 int Ctx::rowGrid(int rows) const
 {
@@ -1743,7 +1821,23 @@ void Ctx::solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, in
                 CFG_CUDA(cudaMemcpyAsync(uRhs_.c[q], uBase_.c[q], n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
         }
         cfg_solver_report reps[3];
-        runBiCG3(mVal_, uDiag_, uRhs_, ux_, 3, tol, maxIter, reps);
+        if (uPrecond_ == CFG_PRECOND_AMG)
+        {
+            if (pass == 0)
+            {
+                // the FP32 AMG hierarchy follows this outer iteration's
+                // momentum matrix (the pressure solve refreshes its own)
+                const int nE = nSlicesEntries_;
+                if (!uVal32_) uVal32_ = alloc<float>(static_cast<size_t>(nE));
+                k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, mVal_, uVal32_);
+                launchCheck("amg_u_float");
+                amgValues(mVal_, uDiag_, uVal32_);
+                amgVectors3();
+                amgFresh_ = false;
+            }
+            runBiCGAmg(mVal_, uDiag_, uRhs_, ux_, tol, maxIter, reps);
+        }
+        else runBiCG3(mVal_, uDiag_, uRhs_, ux_, 3, tol, maxIter, reps);
         for (int q = 0; q < 3; ++q) inner += reps[q].iterations;
     }
 }
@@ -2102,6 +2196,10 @@ void Ctx::prepareIterate(const cfg_simple_controls& ctl)
     checkMomentumBcs();
     if (!turb_) setNu(ctl.nu);  // with a RANS model the model's nu + nut is the diffusivity
     if (ctl.p_ref_cell >= dm_.nC) fail(CFG_EINVAL, "p_ref_cell beyond the last cell");
+    if (ctl.u_precond != CFG_PRECOND_JACOBI && ctl.u_precond != CFG_PRECOND_AMG)
+        fail(CFG_EINVAL, "SIMPLE: u_precond must be CFG_PRECOND_JACOBI or CFG_PRECOND_AMG");
+    if (ctl.u_precond == CFG_PRECOND_AMG && devLoop_)
+        fail(CFG_EINVAL, "SIMPLE: the AMG momentum preconditioner is host driven (no device-side loops)");
     // the time term (simpleSolver.cpp:75-97): dt and the old velocity together
     if (ctl.dt > 0 || ctl.u_time_old != 0)
     {
@@ -2164,7 +2262,9 @@ void Ctx::enqueueOuter(const cfg_simple_controls& ctl, int64_t& uInner, int64_t&
     ma.gUc = CGrad3{{cv(gA_), cv(gB_), cv(Hf_)}};
     k_assemble_U<<<G_, TPB, 0, stream_>>>(dm_, ma);
     launchCheck("assemble_U");
+    uPrecond_ = ctl.u_precond;
     solveMomentum(ctl.non_orth_correctors, gs, ctl.linear_tol, ctl.linear_max_iter, uInner);
+    uPrecond_ = CFG_PRECOND_JACOBI;
     k_hfree<<<G_, TPB, 0, stream_>>>(dm_, uDiag_, cv(U_), cv(ux_), ctl.relax_u, Hf_, rAUr_);
     launchCheck("hfree");
     // ---- predictor flux ----
@@ -2648,6 +2748,25 @@ void Ctx::poissonAmgApply(const double* r, double* z)
     toDevCells(cr_, r, 1, 0);
     amgApply(cr_, cz_);
     fromDevCells(z, cz_, 1, 0);
+}
+
+void Ctx::poissonAmgApply3(const double* r, double* z, const int32_t done[3])
+{
+    if (!amgFresh_)
+    {
+        double info[11];
+        poissonAmg(info);
+    }
+    // the three vectors in the momentum solver's p and z buffers, the done
+    // flags in the solver state (as the momentum BiCGStab hands them over)
+    for (int q = 0; q < 3; ++q) toDevCells(bp_.c[q], r + static_cast<size_t>(q) * dm_.nC, 1, 0);
+    amgVectors3();
+    SolveState s0{};
+    for (int q = 0; q < 3; ++q) s0.done[q] = done[q];
+    CFG_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
+    for (int q = 0; q < 3; ++q) toDevCells(bz_.c[q], z + static_cast<size_t>(q) * dm_.nC, 1, 0);
+    amgCycle3(cv(bp_), bz_, reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done)));
+    for (int q = 0; q < 3; ++q) fromDevCells(z + static_cast<size_t>(q) * dm_.nC, bz_.c[q], 1, 0);
 }
 
 void Ctx::poissonSolve(const double* b, double* x, int method, double tol, int maxIter, int innerMax, double innerTol,

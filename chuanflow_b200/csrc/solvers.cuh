@@ -440,6 +440,48 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv1(DMat A, cons
     }
 }
 
+/// The end of the second BiCGStab product: block sums of t.t (sm[q]) and
+/// t.s (sm[NC + q]) into partials; the last block sets omega, or takes the
+/// tDenom breakdown exit (Matrix.cpp:291-300).
+template <int NC>
+__device__ __forceinline__ void omega_epilogue(double (&sm)[2 * NC], double* partials, SolveState* st)
+{
+    block_sum<2 * NC>(sm);
+    const int G = gridDim.x;
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = sm[q];
+    if (!last_block(&st->ticket[0])) return;
+    double fs[2 * NC];
+    final_sum<2 * NC>(partials, G, fs);
+    if (threadIdx.x == 0)
+    {
+        st->ticket[0] = 0;
+        int all = 1;
+        for (int q = 0; q < NC; ++q)
+        {
+            if (!st->done[q])
+            {
+                const double tDenom = fs[q];
+                if (tDenom < 1e-300)
+                {
+                    // r = s and the iteration counts; k_bi_x applies this
+                    // iteration's x += alpha z and reports |s|inf
+                    st->special[q] = 1;
+                    st->it[q] = st->it[q] + 1;
+                    st->done[q] = 1;
+                }
+                else
+                {
+                    st->omega[q] = fs[NC + q] / tDenom;
+                }
+            }
+            all &= st->done[q];
+        }
+        st->allDone = all;
+    }
+}
+
 /// t = A sh with sh = (r - alpha v) D^-1 formed per column as the row is
 /// read; t.t and t.s; omega, or the tDenom breakdown exit (Matrix.cpp:
 /// 277-300).  s and sh are never stored: every reader forms them from r, v
@@ -477,38 +519,69 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv2(DMat A, cons
             sm[NC + q] += y[q] * si;
         }
     }
-    block_sum<2 * NC>(sm);
+    omega_epilogue<NC>(sm, partials, st);
+}
+
+/// The end of the BiCGStab update: block reductions of |r|inf (mx[q]), the
+/// NaN flags (mx[NC + q]) and r0.r (sm[q]); the last block applies the
+/// stopping test (Matrix.cpp:301-315), or finishes a component that broke
+/// down in the second product with |s|inf as its final residual.
+template <int NC>
+__device__ __forceinline__ void update_epilogue(double (&mx)[2 * NC], double (&sm)[NC], double* partials,
+                                                SolveState* st)
+{
+    block_max<2 * NC>(mx);
+    __syncthreads();
+    block_sum<NC>(sm);
     const int G = gridDim.x;
     if (threadIdx.x == 0)
+    {
 #pragma unroll
-        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = sm[q];
+        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = mx[q];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) partials[(2 * NC + q) * G + blockIdx.x] = sm[q];
+    }
     if (!last_block(&st->ticket[0])) return;
-    double fs[2 * NC];
-    final_sum<2 * NC>(partials, G, fs);
+    double fm[2 * NC], fs[NC];
+    final_max<2 * NC>(partials, G, fm);
+    __syncthreads();
+    final_sum<NC>(partials + 2 * NC * G, G, fs);
     if (threadIdx.x == 0)
     {
         st->ticket[0] = 0;
         int all = 1;
         for (int q = 0; q < NC; ++q)
         {
-            if (!st->done[q])
+            if (st->special[q])
             {
-                const double tDenom = fs[q];
-                if (tDenom < 1e-300)
+                st->fin[q] = fm[NC + q] > 0 ? NAN : fm[q];
+                st->conv[q] = st->fin[q] / st->bnorm[q] < st->tol;
+            }
+            else if (!st->done[q])
+            {
+                const int it = st->it[q] + 1;
+                st->it[q] = it;
+                const double fin = fm[NC + q] > 0 ? NAN : fm[q];
+                st->fin[q] = fin;
+                if (fin / st->bnorm[q] < st->tol)
                 {
-                    // r = s and the iteration counts; k_bi_x applies this
-                    // iteration's x += alpha z and reports |s|inf
-                    st->special[q] = 1;
-                    st->it[q] = st->it[q] + 1;
+                    st->conv[q] = 1;
+                    st->done[q] = 1;
+                }
+                else if (isnan(fin))
+                {
+                    st->it[q] = st->maxIter;
                     st->done[q] = 1;
                 }
                 else
                 {
-                    st->omega[q] = fs[NC + q] / tDenom;
+                    st->rz[q] = fs[q];
+                    if (it >= st->maxIter || fabs(fs[q]) < 1e-300) st->done[q] = 1;
                 }
             }
             all &= st->done[q];
         }
+        for (int q = 0; q < 3; ++q) st->special[q] = 0;
         st->allDone = all;
     }
 }
@@ -564,60 +637,151 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, const dou
             sm[q] += r0v * ri;
         }
     }
-    block_max<2 * NC>(mx);
-    __syncthreads();
-    block_sum<NC>(sm);
-    const int G = gridDim.x;
-    if (threadIdx.x == 0)
+    update_epilogue<NC>(mx, sm, partials, st);
+}
+
+
+// ------------- BiCGStab with the AMG V-cycle as right preconditioner --------
+// The reference's iteration (Matrix.cpp:262-315) with M = the V-cycle in
+// place of D^-1: z = M p and sh = M s are applied between these kernels by
+// amgCycle3, so p and s are stored here for it to read.
+
+/// p = r + beta (p - omega v)  (Matrix.cpp:262-270)
+template <int NC>
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_p(int n, V3P r, V3P p, V3P v, const SolveState* st)
+{
+    if (st->allDone) return;
+    double beta[NC], om[NC];
+    int dn[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
     {
-#pragma unroll
-        for (int q = 0; q < 2 * NC; ++q) partials[q * G + blockIdx.x] = mx[q];
-#pragma unroll
-        for (int q = 0; q < NC; ++q) partials[(2 * NC + q) * G + blockIdx.x] = sm[q];
+        dn[q] = st->done[q];
+        beta[q] = (st->rz[q] / st->rho[q]) * (st->alpha[q] / st->omega[q]);
+        om[q] = st->omega[q];
     }
-    if (!last_block(&st->ticket[0])) return;
-    double fm[2 * NC], fs[NC];
-    final_max<2 * NC>(partials, G, fm);
-    __syncthreads();
-    final_sum<NC>(partials + 2 * NC * G, G, fs);
-    if (threadIdx.x == 0)
+    FOR_ROWS(c, n)
     {
-        st->ticket[0] = 0;
-        int all = 1;
+        double rv[NC], pv[NC], vv[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q])
+            {
+                rv[q] = r.c[q][c];
+                pv[q] = p.c[q][c];
+                vv[q] = v.c[q][c];
+            }
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q]) p.c[q][c] = rv[q] + beta[q] * (pv[q] - om[q] * vv[q]);
+    }
+}
+
+/// s = r - alpha v  (Matrix.cpp:277)
+template <int NC>
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_s(int n, V3P r, V3P v, V3P s, const SolveState* st)
+{
+    if (st->allDone) return;
+    double al[NC];
+    int dn[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+    {
+        dn[q] = st->done[q];
+        al[q] = st->alpha[q];
+    }
+    FOR_ROWS(c, n)
+    {
+        double rv[NC], vv[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q])
+            {
+                rv[q] = r.c[q][c];
+                vv[q] = v.c[q][c];
+            }
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+            if (!dn[q]) s.c[q][c] = rv[q] - al[q] * vv[q];
+    }
+}
+
+/// t = A sh; t.t and t.s; omega or the breakdown exit (Matrix.cpp:278-300)
+template <int W, int NC>
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_spmv2(DMat A, const double* __restrict__ val, V3P sh,
+                                                                     V3P s, V3P t, double* partials, SolveState* st)
+{
+    if (st->allDone) return;
+    double sm[2 * NC];
+#pragma unroll
+    for (int q = 0; q < 2 * NC; ++q) sm[q] = 0.0;
+    const double* xs[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) xs[q] = sh.c[q];
+    FOR_ROWS(c, A.n)
+    {
+        double y[NC];
+        spmv_row<W, NC>(A, val, c, xs, y);
+#pragma unroll
         for (int q = 0; q < NC; ++q)
         {
-            if (st->special[q])
-            {
-                st->fin[q] = fm[NC + q] > 0 ? NAN : fm[q];
-                st->conv[q] = st->fin[q] / st->bnorm[q] < st->tol;
-            }
-            else if (!st->done[q])
-            {
-                const int it = st->it[q] + 1;
-                st->it[q] = it;
-                const double fin = fm[NC + q] > 0 ? NAN : fm[q];
-                st->fin[q] = fin;
-                if (fin / st->bnorm[q] < st->tol)
-                {
-                    st->conv[q] = 1;
-                    st->done[q] = 1;
-                }
-                else if (isnan(fin))
-                {
-                    st->it[q] = st->maxIter;
-                    st->done[q] = 1;
-                }
-                else
-                {
-                    st->rz[q] = fs[q];
-                    if (it >= st->maxIter || fabs(fs[q]) < 1e-300) st->done[q] = 1;
-                }
-            }
-            all &= st->done[q];
+            const double si = s.c[q][c];
+            t.c[q][c] = y[q];
+            sm[q] += y[q] * y[q];
+            sm[NC + q] += y[q] * si;
         }
-        for (int q = 0; q < 3; ++q) st->special[q] = 0;
-        st->allDone = all;
     }
+    omega_epilogue<NC>(sm, partials, st);
+}
+
+/// x = (x + alpha z) + omega sh; r = s - omega t; |r|inf test; next r0.r
+/// (Matrix.cpp:280-282, 301-315, 263-264); a component that broke down in
+/// k_bia_spmv2 takes x + alpha z and |s|inf as its final residual
+template <int NC>
+__global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_x(int n, V3P x, V3P z, V3P s, V3P sh, V3P t, V3P r,
+                                                                 V3P r0, double* partials, SolveState* st)
+{
+    if (st->allDone && !(st->special[0] | st->special[1] | st->special[2])) return;
+    double om[NC], al[NC];
+    int dn[NC], sp[NC];
+    double mx[2 * NC], sm[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+    {
+        dn[q] = st->done[q];
+        sp[q] = st->special[q];
+        om[q] = st->omega[q];
+        al[q] = st->alpha[q];
+        mx[q] = mx[NC + q] = 0.0;
+        sm[q] = 0.0;
+    }
+    FOR_ROWS(c, n)
+    {
+#pragma unroll
+        for (int q = 0; q < NC; ++q)
+        {
+            if (dn[q])
+            {
+                if (sp[q])
+                {
+                    x.c[q][c] = x.c[q][c] + al[q] * z.c[q][c];
+                    const double si = s.c[q][c];
+                    if (isnan(si)) mx[NC + q] = 1.0;
+                    mx[q] = smax(mx[q], fabs(si));
+                }
+                continue;
+            }
+            const double xv = x.c[q][c], zv = z.c[q][c], si = s.c[q][c];
+            const double hv = sh.c[q][c], tv = t.c[q][c], r0v = r0.c[q][c];
+            x.c[q][c] = (xv + al[q] * zv) + om[q] * hv;
+            const double ri = si - om[q] * tv;
+            r.c[q][c] = ri;
+            if (isnan(ri)) mx[NC + q] = 1.0;
+            mx[q] = smax(mx[q], fabs(ri));
+            sm[q] += r0v * ri;
+        }
+    }
+    update_epilogue<NC>(mx, sm, partials, st);
 }
 
 }  // namespace cfg

@@ -125,6 +125,13 @@ typedef struct cfg_simple_controls
      * The reference refuses either without the other; so does this. */
     double dt;
     int32_t u_time_old;
+    /* gpu{} uPreconditioner: the momentum BiCGStab's right preconditioner.
+     * CFG_PRECOND_JACOBI (0, the reference's: z = p D^-1, Matrix.cpp:262-
+     * 300) or CFG_PRECOND_AMG (3): the FP32 aggregation-AMG V-cycle of the
+     * momentum matrix, one V-cycle for the three components at once, inside
+     * the same FP64 BiCGStab and the same |r|inf / |b|inf test.  Other
+     * values are refused. */
+    int32_t u_precond;
 } cfg_simple_controls;
 
 /* SimpleResult (SimpleSolver.h:66-72) plus inner-solver statistics */
@@ -324,17 +331,21 @@ int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
 /* Opt-in CUDA-event timing of every linear-solver kernel launch on the
  * context's stream (no reference counterpart); while it is on, solver
  * iterations are launched one by one rather than as CUDA graphs.  Enabling
- * clears the counts; cfg_kernel_stats gives {launches, total ms} for, in
- * order: the PCG SpMV + p.Ap, the x/r update + norms + r.z, the
- * search-direction update; the four BiCGStab kernels (p/z update, v = Az,
- * t = As^, x/r update); the whole DIC application z = M^-1 r. */
+ * clears the counts; cfg_kernel_stats gives {launches, total ms} for the
+ * first `slots` (at most CFG_KERNEL_SLOTS) of, in order: the PCG SpMV +
+ * p.Ap, the x/r update + norms + r.z, the search-direction update; the four
+ * BiCGStab kernels (p/z update, v = Az, t = As^, x/r update); the whole DIC
+ * application z = M^-1 r; the AMG-preconditioned momentum BiCGStab's p
+ * update, V-cycle z = M p, v = Az, s = r - alpha v, V-cycle s^ = M s,
+ * t = As^ and x/r update.  out holds 2 * slots doubles. */
+#define CFG_KERNEL_SLOTS 15
 int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable);
-int cfg_kernel_stats(const cfg_ctx* ctx, double out[16]);
+int cfg_kernel_stats(const cfg_ctx* ctx, double* out, int32_t slots);
 /* The same slots' launches weighted by the vector components each launch
  * still iterated on (the fused three-component BiCGStab kernels skip a
  * converged component's rows; 1 per launch elsewhere), for per-launch byte
- * counts (no reference counterpart). */
-int cfg_kernel_components(const cfg_ctx* ctx, double out[8]);
+ * counts (no reference counterpart); out holds `slots` doubles. */
+int cfg_kernel_components(const cfg_ctx* ctx, double* out, int32_t slots);
 
 /* ---- the linear-solver call surface ------------------------------------ */
 
@@ -394,6 +405,11 @@ int cfg_poisson_amg_setup(cfg_ctx* ctx, double out[11]);
 /* One V-cycle of that hierarchy, z = V(r) (host vectors, original order):
  * the preconditioner as CFG_POISSON_FCG_AMG applies it, for tests. */
 int cfg_poisson_amg_apply(cfg_ctx* ctx, const double* r, double* z);
+/* The three-component V-cycle the AMG momentum BiCGStab applies, on the
+ * same hierarchy: r and z hold three vectors one after another (3 n
+ * values); component q is skipped, its z left as given, when done[q] != 0.
+ * Each applied component equals cfg_poisson_amg_apply of it, for tests. */
+int cfg_poisson_amg_apply3(cfg_ctx* ctx, const double* r, double* z, const int32_t done[3]);
 
 /* ---- diagnostics used by the parity tests (no reference counterpart) ----- */
 

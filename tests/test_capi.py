@@ -93,7 +93,7 @@ def test_case_file_keys_follow_the_reference(tmp_path):
     assert (mi, ctol, pcorr, mtol, ltol, lmax, northo) == (300, 1e-6, 1e-4, 1e-4, 1e-8, 2000, 2)
     assert (ru, rp, rps) == (0.9, 0.03, 0.02)
     assert s["force"] == [1.0, 0.0, 0.0] and s["nu"] == [0.01]
-    assert s["gpu"] == [0.0, -1.0, 0.0]
+    assert s["gpu"] == [0.0, -1.0, 0.0, 0.0]
     assert s["initialU"] == [0.1, 0.0, 0.0]
 
 
@@ -102,10 +102,14 @@ def test_case_file_defaults_and_gpu_block(tmp_path):
     s = cf.inspect_case_file(write(tmp_path, text))
     assert s["simple"] == [200.0, 1e-6, 0.0, 0.0, 1e-7, 2000.0, 2.0, 0.7, 0.3, 0.0]
     assert s["schemes"] == [0.0, 1.0, 1.0, 0.9]
-    assert s["gpu"] == [0.0, 3.0, 1.5]
+    assert s["gpu"] == [0.0, 3.0, 1.5, 0.0]
     for word, code in (("DIC", 1.0), ("AMG", 3.0)):
         s = cf.inspect_case_file(write(tmp_path, text.replace("gpu {", f"gpu {{ pPreconditioner {word};")))
-        assert s["gpu"] == [code, 3.0, 1.5]
+        assert s["gpu"] == [code, 3.0, 1.5, 0.0]
+    s = cf.inspect_case_file(write(tmp_path, text.replace("gpu {", "gpu { uPreconditioner AMG;")))
+    assert s["gpu"] == [0.0, 3.0, 1.5, 3.0]
+    with pytest.raises(cf.CfgError, match="unknown uPreconditioner 'DIC'"):
+        cf.inspect_case_file(write(tmp_path, text.replace("gpu {", "gpu { uPreconditioner DIC;")))
 
 
 @pytest.mark.parametrize("text,msg", [

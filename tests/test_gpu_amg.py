@@ -67,3 +67,20 @@ def test_fcg_amg_reaches_oracle_solution(method):
         _, jac = case.poisson_solve(b, "jacobi64", tol=1e-10)
         assert rep["inner_iterations"] * 4 < jac["inner_iterations"], (rep["inner_iterations"],
                                                                        jac["inner_iterations"])
+
+
+def test_three_vector_vcycle_equals_single_vcycles():
+    """The V-cycle the AMG momentum BiCGStab applies (three right-hand sides
+    over one matrix read) gives each component the single V-cycle's result
+    bit for bit, and leaves a component flagged done untouched."""
+    mesh, case, A, _ = _system()
+    case.poisson_amg_setup()
+    rng = np.random.default_rng(7)
+    r3 = rng.standard_normal((3, mesh.n_cells))
+    z3 = case.poisson_amg_apply3(r3)
+    for q in range(3):
+        assert np.array_equal(z3[q], case.poisson_amg_apply(r3[q])), q
+    keep = rng.standard_normal((3, mesh.n_cells))
+    z3b = case.poisson_amg_apply3(r3, keep, done=(0, 1, 0))
+    assert np.array_equal(z3b[1], keep[1])
+    assert np.array_equal(z3b[0], z3[0]) and np.array_equal(z3b[2], z3[2])
