@@ -144,6 +144,21 @@ __device__ __forceinline__ float group_row(const int* __restrict__ rs, const int
 }
 constexpr int kGroup = 8;
 
+/// the sum of an aggregate's members, by a group of G lanes: lane l of the
+/// group takes members l, l + G, ...; every lane of the group holds the
+/// sum after the shuffle tree
+template <int G>
+__device__ __forceinline__ float group_members(const int* __restrict__ ms, const int* __restrict__ mem,
+                                               const float* __restrict__ r, int I, int l)
+{
+    float s = 0.0f;
+    if (I >= 0)
+        for (int k = __ldg(ms + I) + l; k < __ldg(ms + I + 1); k += G) s += __ldg(r + __ldg(mem + k));
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
 /// finest level, first sweep and residual: x = w D^-1 b, r = b - A x
 template <int W>
 __global__ void __launch_bounds__(TPB) k_amg_pre0(const int* __restrict__ stop, DMat A, const float* __restrict__ val,
@@ -162,16 +177,14 @@ __global__ void __launch_bounds__(TPB) k_amg_pre0(const int* __restrict__ stop, 
 }
 
 /// coarse level, the same on CSR
-__global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, int n, const int* __restrict__ rs,
-                                                 const int* __restrict__ cols, const float* __restrict__ val,
-                                                 const float* __restrict__ dinv, const float* __restrict__ b,
-                                                 float* __restrict__ x, float* __restrict__ r)
+__device__ __forceinline__ void amg_pre_rows(int n, const int* __restrict__ rs, const int* __restrict__ cols,
+                                             const float* __restrict__ val, const float* __restrict__ dinv,
+                                             const float* __restrict__ b, float* __restrict__ x,
+                                             float* __restrict__ r, int first, int stride)
 {
-    if (stop && *stop) return;
     const int l = threadIdx.x % kGroup;
-    const int stride = gridDim.x * (TPB / kGroup);
     // whole warps iterate together (the shuffle needs every lane)
-    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
+    for (int i0 = first;; i0 += stride)
     {
         const int base = i0 - (threadIdx.x % 32) / kGroup;  // the warp's first row this round
         if (base >= n) break;
@@ -186,28 +199,58 @@ __global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, i
     }
 }
 
-/// the residual summed over each aggregate: the next level's right-hand side
+__global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, int n, const int* __restrict__ rs,
+                                                 const int* __restrict__ cols, const float* __restrict__ val,
+                                                 const float* __restrict__ dinv, const float* __restrict__ b,
+                                                 float* __restrict__ x, float* __restrict__ r)
+{
+    if (stop && *stop) return;
+    amg_pre_rows(n, rs, cols, val, dinv, b, x, r, blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup,
+                 gridDim.x * (TPB / kGroup));
+}
+
+/// the residual summed over each aggregate (a group of lanes per aggregate):
+/// the next level's right-hand side
+__device__ __forceinline__ void amg_restrict_rows(int nc, const int* __restrict__ ms, const int* __restrict__ mem,
+                                                  const float* __restrict__ r, float* __restrict__ bc, int first,
+                                                  int stride)
+{
+    const int l = threadIdx.x % kGroup;
+    for (int I0 = first;; I0 += stride)
+    {
+        const int base = I0 - (threadIdx.x % 32) / kGroup;
+        if (base >= nc) break;
+        const int I = I0 < nc ? I0 : -1;
+        const float s = group_members<kGroup>(ms, mem, r, I, l);
+        if (I >= 0 && l == 0) bc[I] = s;
+    }
+}
+
 __global__ void __launch_bounds__(TPB) k_amg_restrict(const int* __restrict__ stop, int nc, const int* __restrict__ ms,
                                                       const int* __restrict__ mem, const float* __restrict__ r,
                                                       float* __restrict__ bc)
 {
     if (stop && *stop) return;
-    FOR_ROWS(I, nc)
-    {
-        float s = 0.0f;
-        for (int k = ms[I]; k < ms[I + 1]; ++k) s += r[mem[k]];
-        bc[I] = s;
-    }
+    amg_restrict_rows(nc, ms, mem, r, bc, blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup,
+                      gridDim.x * (TPB / kGroup));
 }
 
-/// finest level: y = x + s P xc, then z = y + w D^-1 (b - A y), in FP64
-/// out; inside the device FCG (st given) also z.q and, in the block that
-/// finishes last, beta = -z.q / p.q
+/// the coarse correction brought to this level: y = x + s P xc
+__global__ void __launch_bounds__(TPB) k_amg_prolong(const int* __restrict__ stop, int n, const float* __restrict__ x,
+                                                     const float* __restrict__ xc, const int* __restrict__ agg,
+                                                     float* __restrict__ y)
+{
+    if (stop && *stop) return;
+    FOR_ROWS(i, n) y[i] = x[i] + kScale * xc[agg[i]];
+}
+
+/// finest level: z = y + w D^-1 (b - A y), in FP64 out; inside the device
+/// FCG (st given) also z.q and, in the block that finishes last,
+/// beta = -z.q / p.q
 template <int W>
 __global__ void __launch_bounds__(TPB) k_amg_post0(const int* __restrict__ stop, DMat A, const float* __restrict__ val,
                                                    const float* __restrict__ dinv, const double* __restrict__ b,
-                                                   const float* __restrict__ x, const float* __restrict__ xc,
-                                                   const int* __restrict__ agg, double* __restrict__ z,
+                                                   const float* __restrict__ y, double* __restrict__ z,
                                                    const double* __restrict__ q, double* partials, FcgState* st)
 {
     if (stop && *stop) return;
@@ -215,10 +258,8 @@ __global__ void __launch_bounds__(TPB) k_amg_post0(const int* __restrict__ stop,
     double zq[1] = {0.0};
     FOR_ROWS(c, A.n)
     {
-        const float y = x[c] + kScale * xc[agg[c]];
-        const float s =
-            sell_row<W>(A, val, c, [&](int j) { return __ldg(x + j) + kScale * __ldg(xc + __ldg(agg + j)); });
-        const double zc = static_cast<double>(y + kOmega * dinv[c] * (static_cast<float>(b[c]) - s));
+        const float s = sell_row<W>(A, val, c, [&](int j) { return __ldg(y + j); });
+        const double zc = static_cast<double>(y[c] + kOmega * dinv[c] * (static_cast<float>(b[c]) - s));
         z[c] = zc;
         if (dot) zq[0] += zc * q[c];
     }
@@ -235,38 +276,88 @@ __global__ void __launch_bounds__(TPB) k_amg_post0(const int* __restrict__ stop,
     }
 }
 
-/// coarse level, the same on CSR
-__global__ void __launch_bounds__(TPB) k_amg_post(const int* __restrict__ stop, int n, const int* __restrict__ rs,
-                                                  const int* __restrict__ cols, const float* __restrict__ val,
-                                                  const float* __restrict__ dinv, const float* __restrict__ b,
-                                                  const float* __restrict__ x, const float* __restrict__ xc,
-                                                  const int* __restrict__ agg, float* __restrict__ xo)
+/// coarse level, the same on CSR: xo = y + w D^-1 (b - A y)
+__device__ __forceinline__ void amg_post_rows(int n, const int* __restrict__ rs, const int* __restrict__ cols,
+                                              const float* __restrict__ val, const float* __restrict__ dinv,
+                                              const float* __restrict__ b, const float* __restrict__ y,
+                                              float* __restrict__ xo, int first, int stride)
 {
-    if (stop && *stop) return;
     const int l = threadIdx.x % kGroup;
-    const int stride = gridDim.x * (TPB / kGroup);
-    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup; ; i0 += stride)
+    for (int i0 = first;; i0 += stride)
     {
         const int base = i0 - (threadIdx.x % 32) / kGroup;
         if (base >= n) break;
         const int i = i0 < n ? i0 : -1;
-        const float s =
-            group_row<kGroup>(rs, cols, val, i, l, [&](int j) { return __ldg(x + j) + kScale * __ldg(xc + __ldg(agg + j)); });
-        if (i >= 0 && l == 0) xo[i] = x[i] + kScale * xc[agg[i]] + kOmega * dinv[i] * (b[i] - s);
+        const float s = group_row<kGroup>(rs, cols, val, i, l, [&](int j) { return __ldg(y + j); });
+        if (i >= 0 && l == 0) xo[i] = y[i] + kOmega * dinv[i] * (b[i] - s);
     }
 }
 
-/// the coarsest solve: x = M^-1 b with the dense inverse (one block)
-__global__ void __launch_bounds__(kDenseMax) k_amg_dense(const int* __restrict__ stop, int n,
+__global__ void __launch_bounds__(TPB) k_amg_post(const int* __restrict__ stop, int n, const int* __restrict__ rs,
+                                                  const int* __restrict__ cols, const float* __restrict__ val,
+                                                  const float* __restrict__ dinv, const float* __restrict__ b,
+                                                  const float* __restrict__ y, float* __restrict__ xo)
+{
+    if (stop && *stop) return;
+    amg_post_rows(n, rs, cols, val, dinv, b, y, xo, blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup,
+                  gridDim.x * (TPB / kGroup));
+}
+
+/// The last aggregation level (at most kTailMax rows) and the coarsest
+/// solve in one block per vector: pre-sweep and residual, restriction,
+/// the dense coarsest inverse, prolongation and post-sweep, separated by
+/// block barriers only (the same arithmetic and orders as the per-level
+/// kernels).  Block q works on vector q (offset q * n at every level) and
+/// does nothing when done[q] is set (done may be null).
+constexpr int kTailMax = 1024;
+constexpr int kTailThreads = 1024;
+
+struct TailLevel
+{
+    int n, nc;
+    const int *rs, *cols, *agg, *ms, *mem;
+    const float *val, *dinv, *dense;
+    float *b, *x, *r, *y, *xo;  // this level's vectors (n per vector)
+    float *bc, *xc;             // the coarsest level's (nc per vector)
+};
+
+__global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict__ done, TailLevel T)
+{
+    const int q = blockIdx.x;
+    if (done && done[q]) return;
+    const int n = T.n, nc = T.nc;
+    float *b = T.b + q * n, *x = T.x + q * n, *r = T.r + q * n, *y = T.y + q * n, *xo = T.xo + q * n;
+    float *bc = T.bc + q * nc, *xc = T.xc + q * nc;
+    const int first = threadIdx.x / kGroup, stride = kTailThreads / kGroup;
+    amg_pre_rows(n, T.rs, T.cols, T.val, T.dinv, b, x, r, first, stride);
+    __syncthreads();
+    amg_restrict_rows(nc, T.ms, T.mem, r, bc, first, stride);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nc; i += kTailThreads)
+    {
+        float s = 0.0f;
+        for (int j = 0; j < nc; ++j) s += T.dense[i * nc + j] * bc[j];
+        xc[i] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += kTailThreads) y[i] = x[i] + kScale * xc[T.agg[i]];
+    __syncthreads();
+    amg_post_rows(n, T.rs, T.cols, T.val, T.dinv, b, y, xo, first, stride);
+}
+
+/// the coarsest solve, x = M^-1 b with the dense inverse, when the finest
+/// level is the last aggregated one (block q: vector q at offset q * n)
+__global__ void __launch_bounds__(kDenseMax) k_amg_dense(const int* __restrict__ done, int n,
                                                          const float* __restrict__ m, const float* __restrict__ b,
                                                          float* __restrict__ x)
 {
-    if (stop && *stop) return;
+    const int q = blockIdx.x;
+    if (done && done[q]) return;
     const int i = threadIdx.x;
     if (i >= n) return;
     float s = 0.0f;
-    for (int j = 0; j < n; ++j) s += m[i * n + j] * b[j];
-    x[i] = s;
+    for (int j = 0; j < n; ++j) s += m[i * n + j] * b[q * n + j];
+    x[q * n + i] = s;
 }
 
 /// next-level entries as sums of this level's: FP64 sums of FP64 (finest,
@@ -451,49 +542,51 @@ __global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, 
     }
 }
 
-/// the residuals summed over each aggregate
+/// the residuals summed over each aggregate (a group of lanes per aggregate)
 __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ done, int n, int nc,
                                                        const int* __restrict__ ms, const int* __restrict__ mem,
                                                        const float* __restrict__ r, float* __restrict__ bc)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
-    FOR_ROWS(I, nc)
+    const int l = threadIdx.x % kGroup;
+    const int stride = gridDim.x * (TPB / kGroup);
+    for (int I0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; I0 += stride)
     {
-        float s[3] = {0.0f, 0.0f, 0.0f};
-        for (int k = ms[I]; k < ms[I + 1]; ++k)
-        {
-            const int i = mem[k];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) s[q] += r[q * n + i];
-        }
+        const int base = I0 - (threadIdx.x % 32) / kGroup;
+        if (base >= nc) break;
+        const int I = I0 < nc ? I0 : -1;
 #pragma unroll
         for (int q = 0; q < 3; ++q)
-            if (act.a[q]) bc[q * nc + I] = s[q];
+        {
+            if (!act.a[q]) continue;
+            const float s = group_members<kGroup>(ms, mem, r + q * n, I, l);
+            if (I >= 0 && l == 0) bc[q * nc + I] = s;
+        }
     }
 }
 
-/// the coarsest solve for each component (block q: component q)
-__global__ void __launch_bounds__(kDenseMax) k_amgv_dense(const int* __restrict__ done, int n,
-                                                          const float* __restrict__ m, const float* __restrict__ b,
-                                                          float* __restrict__ x)
+/// the coarse corrections brought to this level: y = x + s P xc
+__global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ done, int n, int nNext,
+                                                      const float* __restrict__ x, const float* __restrict__ xc,
+                                                      const int* __restrict__ agg, float* __restrict__ y)
 {
-    const int q = blockIdx.x;
-    if (done[q]) return;
-    const int i = threadIdx.x;
-    if (i >= n) return;
-    float s = 0.0f;
-    for (int j = 0; j < n; ++j) s += m[i * n + j] * b[q * n + j];
-    x[q * n + i] = s;
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    FOR_ROWS(i, n)
+    {
+        const int ai = agg[i];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (act.a[q]) y[q * n + i] = x[q * n + i] + kScale * xc[q * nNext + ai];
+    }
 }
 
-/// coarse level: xo = x + s P xc + w D^-1 (b - A (x + s P xc))
-__global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done, int n, int nNext,
-                                                   const int* __restrict__ rs, const int* __restrict__ cols,
-                                                   const float* __restrict__ val, const float* __restrict__ dinv,
-                                                   const float* __restrict__ b, const float* __restrict__ x,
-                                                   const float* __restrict__ xc, const int* __restrict__ agg,
-                                                   float* __restrict__ xo)
+/// coarse level: xo = y + w D^-1 (b - A y)
+__global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done, int n, const int* __restrict__ rs,
+                                                   const int* __restrict__ cols, const float* __restrict__ val,
+                                                   const float* __restrict__ dinv, const float* __restrict__ b,
+                                                   const float* __restrict__ y, float* __restrict__ xo)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
@@ -506,29 +599,24 @@ __global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done,
         const int i = i0 < n ? i0 : -1;
         float s[3];
         group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) {
-            const int aj = __ldg(agg + j);
 #pragma unroll
-            for (int q = 0; q < 3; ++q)
-                g[q] = act.a[q] ? __ldg(x + q * n + j) + kScale * __ldg(xc + q * nNext + aj) : 0.0f;
+            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? __ldg(y + q * n + j) : 0.0f;
         });
         if (i >= 0 && l == 0)
         {
-            const int ai = agg[i];
             const float di = dinv[i];
 #pragma unroll
             for (int q = 0; q < 3; ++q)
-                if (act.a[q])
-                    xo[q * n + i] = x[q * n + i] + kScale * xc[q * nNext + ai] + kOmega * di * (b[q * n + i] - s[q]);
+                if (act.a[q]) xo[q * n + i] = y[q * n + i] + kOmega * di * (b[q * n + i] - s[q]);
         }
     }
 }
 
-/// finest level: z = y + w D^-1 (b - A y), y = x + s P xc, into FP64
+/// finest level: z = y + w D^-1 (b - A y), into FP64
 template <int W>
-__global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done, DMat A, int nNext,
-                                                    const float* __restrict__ val, const float* __restrict__ dinv,
-                                                    CV3P b, const float* __restrict__ x, const float* __restrict__ xc,
-                                                    const int* __restrict__ agg, V3P z)
+__global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done, DMat A, const float* __restrict__ val,
+                                                    const float* __restrict__ dinv, CV3P b, const float* __restrict__ y,
+                                                    V3P z)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
@@ -537,20 +625,14 @@ __global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done
     {
         float s[3];
         sell_row3<W>(A, val, c, s, [&](int j, float (&g)[3]) {
-            const int aj = __ldg(agg + j);
 #pragma unroll
-            for (int q = 0; q < 3; ++q)
-                g[q] = act.a[q] ? __ldg(x + q * n + j) + kScale * __ldg(xc + q * nNext + aj) : 0.0f;
+            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? __ldg(y + q * n + j) : 0.0f;
         });
-        const int ac = agg[c];
         const float dc = dinv[c];
 #pragma unroll
         for (int q = 0; q < 3; ++q)
             if (act.a[q])
-            {
-                const float y = x[q * n + c] + kScale * xc[q * nNext + ac];
-                z.c[q][c] = static_cast<double>(y + kOmega * dc * (static_cast<float>(b.c[q][c]) - s[q]));
-            }
+                z.c[q][c] = static_cast<double>(y[q * n + c] + kOmega * dc * (static_cast<float>(b.c[q][c]) - s[q]));
     }
 }
 
@@ -801,19 +883,56 @@ void Ctx::amgApply(const double* r, double* z)
     amgCycle(r, z, nullptr, nullptr);
 }
 
+/// The level of the fused tail kernel (the last aggregated level, when it is
+/// not the finest and has at most kTailMax rows), or -1.
+static int tailLevel(const AmgState& a)
+{
+    const int L = static_cast<int>(a.lv.size());
+    return (L >= 3 && a.lv[L - 2].n <= kTailMax) ? L - 2 : -1;
+}
+
+/// The tail kernel's view of level T and the coarsest level: the single
+/// vectors (v3 false) or the three-vector ones.
+static TailLevel tailView(const AmgState& a, int T, bool v3)
+{
+    const AmgLevel& V = a.lv[static_cast<size_t>(T)];
+    const AmgLevel& C = a.lv[static_cast<size_t>(T) + 1];
+    TailLevel t{};
+    t.n = V.n;
+    t.nc = C.n;
+    t.rs = V.rs;
+    t.cols = V.cols;
+    t.agg = V.agg;
+    t.ms = V.ms;
+    t.mem = V.mem;
+    t.val = V.val;
+    t.dinv = V.dinv;
+    t.dense = a.dense;
+    t.b = v3 ? V.b3 : V.b;
+    t.x = v3 ? V.x3 : V.x;
+    t.r = v3 ? V.r3 : V.r;
+    t.y = t.r;  // the residual is restricted before the prolongation overwrites it
+    t.xo = v3 ? V.xo3 : V.xo;
+    t.bc = v3 ? C.b3 : C.b;
+    t.xc = v3 ? C.x3 : C.x;
+    return t;
+}
+
 void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
 {
     AmgState& a = *amg_;
     if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
     const int L = static_cast<int>(a.lv.size());
+    const int T = tailLevel(a);
+    const int last = T >= 0 ? T : L - 1;  // levels [0, last) run level by level
     const int* stop = st ? &st->done : nullptr;
     auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
-    // a group of kGroup lanes per coarse row
+    // a group of kGroup lanes per coarse row or aggregate
     auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
     const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
     // down
-    for (int l = 0; l + 1 < L; ++l)
+    for (int l = 0; l < last; ++l)
     {
         AmgLevel& V = a.lv[l];
         AmgLevel& N = a.lv[l + 1];
@@ -825,28 +944,30 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
         }
         else
             k_amg_pre<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
-        k_amg_restrict<<<grid(N.n), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
+        k_amg_restrict<<<ggrid(N.n), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
     }
-    k_amg_dense<<<1, kDenseMax, 0, stream_>>>(stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
+    if (T >= 0) k_amg_tail<<<1, kTailThreads, 0, stream_>>>(stop, tailView(a, T, false));
+    else k_amg_dense<<<1, kDenseMax, 0, stream_>>>(stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
     // up: each level corrects with the next level's output
-    for (int l = L - 2; l >= 0; --l)
+    for (int l = last - 1; l >= 0; --l)
     {
         AmgLevel& V = a.lv[l];
-        const float* xc = (l + 1 == L - 1) ? a.lv[l + 1].x : a.lv[l + 1].xo;
+        const AmgLevel& N = a.lv[l + 1];
+        const float* xc = (l + 1 == L - 1) ? N.x : N.xo;
+        k_amg_prolong<<<grid(V.n), TPB, 0, stream_>>>(stop, V.n, V.x, xc, V.agg, V.r);
         if (l == 0)
         {
             if (Wsel == 7)
-                k_amg_post0<7><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, xc, V.agg, z, q, partials_, st);
+                k_amg_post0<7><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
             else if (Wsel == 16)
-                k_amg_post0<16><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, xc, V.agg, z, q, partials_,
-                                                          st);
+                k_amg_post0<16><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
             else
-                k_amg_post0<0><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, xc, V.agg, z, q, partials_, st);
+                k_amg_post0<0><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
         }
         else
-            k_amg_post<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, xc, V.agg, V.xo);
+            k_amg_post<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.r, V.xo);
     }
-    launchCheck("amg_vcycle", 3 * (L - 1) + 1);
+    launchCheck("amg_vcycle", amgCycleKernels());
 }
 
 /// z_q = V-cycle(b_q) for the three components whose done flag is clear
@@ -857,11 +978,13 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done)
     if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
     if (!a.lv[0].x3) fail(CFG_EINVAL, "amg: the three-component vectors are not allocated (amgVectors3)");
     const int L = static_cast<int>(a.lv.size());
+    const int T = tailLevel(a);
+    const int last = T >= 0 ? T : L - 1;
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
     auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
     auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
     const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
-    for (int l = 0; l + 1 < L; ++l)
+    for (int l = 0; l < last; ++l)
     {
         AmgLevel& V = a.lv[l];
         AmgLevel& N = a.lv[l + 1];
@@ -873,28 +996,26 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done)
         }
         else
             k_amgv_pre<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.x3, V.r3);
-        k_amgv_restrict<<<grid(N.n), TPB, 0, stream_>>>(done, V.n, N.n, V.ms, V.mem, V.r3, N.b3);
+        k_amgv_restrict<<<ggrid(N.n), TPB, 0, stream_>>>(done, V.n, N.n, V.ms, V.mem, V.r3, N.b3);
     }
-    k_amgv_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
-    for (int l = L - 2; l >= 0; --l)
+    if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true));
+    else k_amg_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
+    for (int l = last - 1; l >= 0; --l)
     {
         AmgLevel& V = a.lv[l];
         const AmgLevel& N = a.lv[l + 1];
         const float* xc = (l + 1 == L - 1) ? N.x3 : N.xo3;
+        k_amgv_prolong<<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, V.x3, xc, V.agg, V.r3);
         if (l == 0)
         {
-            if (Wsel == 7)
-                k_amgv_post0<7><<<GS_, TPB, 0, stream_>>>(done, A, N.n, amgVals32_, V.dinv, b, V.x3, xc, V.agg, z);
-            else if (Wsel == 16)
-                k_amgv_post0<16><<<GS_, TPB, 0, stream_>>>(done, A, N.n, amgVals32_, V.dinv, b, V.x3, xc, V.agg, z);
-            else
-                k_amgv_post0<0><<<GS_, TPB, 0, stream_>>>(done, A, N.n, amgVals32_, V.dinv, b, V.x3, xc, V.agg, z);
+            if (Wsel == 7) k_amgv_post0<7><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
+            else if (Wsel == 16) k_amgv_post0<16><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
+            else k_amgv_post0<0><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
         }
         else
-            k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.x3, xc,
-                                                          V.agg, V.xo3);
+            k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.r3, V.xo3);
     }
-    launchCheck("amg_vcycle3", 3 * (L - 1) + 1);
+    launchCheck("amg_vcycle3", amgCycleKernels());
 }
 
 /// The level vectors of the three-component V-cycle, allocated once (before
@@ -914,7 +1035,13 @@ void Ctx::amgVectors3()
 }
 
 /// The number of kernels one amgCycle3 launches.
-int Ctx::amgCycleKernels() const { return amg_ ? 3 * (static_cast<int>(amg_->lv.size()) - 1) + 1 : 0; }
+int Ctx::amgCycleKernels() const
+{
+    if (!amg_) return 0;
+    const int T = tailLevel(*amg_);
+    const int last = T >= 0 ? T : static_cast<int>(amg_->lv.size()) - 1;
+    return 4 * last + 1;
+}
 
 namespace
 {
@@ -1141,7 +1268,7 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
         if (ge) CFG_CUDA(cudaGraphLaunch(ge, stream_));
         else
             for (int k = 0; k < m; ++k) iteration();
-        launches_ = counted + static_cast<int64_t>(m) * (3 + 3 * (static_cast<int>(a.lv.size()) - 1) + 1);
+        launches_ = counted + static_cast<int64_t>(m) * (3 + amgCycleKernels());
         launched += m;
         chunk = std::min(chunk * 2, 32);
     }
