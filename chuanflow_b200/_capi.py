@@ -367,7 +367,7 @@ CELL_ORDER = {None: -1, "identity": 0, "colour": 1, "rcm": 2, "rcm-colour": 3}
 
 U_PRECOND = {"Jacobi": 0, "AMG": 3}
 KERNEL_SLOTS = ("cg_spmv", "cg_update", "cg_p", "bi_p", "bi_spmv1", "bi_spmv2", "bi_x", "dic_apply",
-                "bia_p", "bia_vcycle_z", "bia_spmv1", "bia_s", "bia_vcycle_s", "bia_spmv2", "bia_x")
+                "bia_p", "amgv_pre0", "amgv_coarse", "amgv_post0", "bia_spmv1", "bia_s", "bia_spmv2", "bia_x")
 
 
 class SimpleCase:

@@ -556,12 +556,22 @@ __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ d
         const int base = I0 - (threadIdx.x % 32) / kGroup;
         if (base >= nc) break;
         const int I = I0 < nc ? I0 : -1;
+        // the members' indices once for the three vectors; per vector the
+        // lane-strided sums and shuffle tree of group_members
+        float s[3] = {0.0f, 0.0f, 0.0f};
+        if (I >= 0)
+            for (int k = __ldg(ms + I) + l; k < __ldg(ms + I + 1); k += kGroup)
+            {
+                const int m = __ldg(mem + k);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) s[q] += act.a[q] ? __ldg(r + q * n + m) : 0.0f;
+            }
 #pragma unroll
         for (int q = 0; q < 3; ++q)
         {
-            if (!act.a[q]) continue;
-            const float s = group_members<kGroup>(ms, mem, r + q * n, I, l);
-            if (I >= 0 && l == 0) bc[q * nc + I] = s;
+#pragma unroll
+            for (int o = kGroup / 2; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+            if (act.a[q] && I >= 0 && l == 0) bc[q * nc + I] = s[q];
         }
     }
 }
@@ -972,7 +982,7 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
 
 /// z_q = V-cycle(b_q) for the three components whose done flag is clear
 /// (the BiCGStab's flags; a converged component keeps its old z_q)
-void Ctx::amgCycle3(CV3P b, V3P z, const int* done)
+void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int)>& mark)
 {
     AmgState& a = *amg_;
     if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
@@ -993,6 +1003,7 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done)
             if (Wsel == 7) k_amgv_pre0<7><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
             else if (Wsel == 16) k_amgv_pre0<16><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
             else k_amgv_pre0<0><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
+            if (mark) mark(0);
         }
         else
             k_amgv_pre<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.x3, V.r3);
@@ -1008,6 +1019,7 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done)
         k_amgv_prolong<<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, V.x3, xc, V.agg, V.r3);
         if (l == 0)
         {
+            if (mark) mark(1);
             if (Wsel == 7) k_amgv_post0<7><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
             else if (Wsel == 16) k_amgv_post0<16><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
             else k_amgv_post0<0><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);

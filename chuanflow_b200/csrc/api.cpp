@@ -957,13 +957,11 @@ int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_contr
             batch->rowBlocks = cand[k][1];
             double ms = 0;
             cfg::batchPass(*batch, q, controls, m.data(), &ms);
-            if (cand[k][0] == 0)
-            {
-                // the first graph pass of a schedule includes its capture:
-                // time a replay of the same pass
-                for (cfg::Ctx* c : batch->blocks) c->restoreState();
-                cfg::batchPass(*batch, q, controls, m.data(), &ms);
-            }
+            // a schedule's first pass includes its first-time costs (graph
+            // captures of the chunks, or of the whole pass): time a second
+            // run of the same pass from the same fields
+            for (cfg::Ctx* c : batch->blocks) c->restoreState();
+            cfg::batchPass(*batch, q, controls, m.data(), &ms);
             if (times) times[k] = ms;
             if (k == 0 || ms < best)
             {

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <map>
 #include <string>
 #include <algorithm>
@@ -152,12 +153,16 @@ public:
         KS_BI_SPMV2,
         KS_BI_X,
         KS_DIC_APPLY,
-        // the momentum BiCGStab with the AMG V-cycle (u_precond AMG)
+        // the momentum BiCGStab with the AMG V-cycle (u_precond AMG); the
+        // two V-cycles of an iteration share the three V-cycle slots: the
+        // finest pre-sweep and residual, everything coarser (restriction
+        // to prolongation), the finest post-sweep
         KS_BIA_P,
-        KS_BIA_VC_Z,
+        KS_AMGV_PRE0,
+        KS_AMGV_COARSE,
+        KS_AMGV_POST0,
         KS_BIA_SPMV1,
         KS_BIA_S,
-        KS_BIA_VC_S,
         KS_BIA_SPMV2,
         KS_BIA_X,
         KS_COUNT
@@ -254,7 +259,9 @@ private:
     void amgValues(const double* vals, const double* diag, const float* vals32);
     void amgApply(const double* r, double* z);
     void amgCycle(const double* r, double* z, const double* q, FcgState* st);
-    void amgCycle3(CV3P b, V3P z, const int* done);
+    /// mark(0) after the finest pre-sweep, mark(1) before the finest
+    /// post-sweep (kernel timing), when given
+    void amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int)>& mark = {});
     void amgVectors3();
     int amgCycleKernels() const;
     void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,
@@ -376,7 +383,7 @@ private:
     bool ktime_ = false;
     bool useGraphs_ = true;
     std::map<std::string, cudaGraphExec_t> graphs_;
-    static constexpr int kEvPerIter = 8;  // events per solver iteration of a chunk (kernels + 1)
+    static constexpr int kEvPerIter = 12;  // events per solver iteration of a chunk (timed segments + 1)
     std::vector<cudaEvent_t> kev_;
     void tmark(int k, int j);
     void harvest(int ran, const int* slots, int nSlots, int active = 1);

@@ -1611,9 +1611,10 @@ void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, doubl
             CFG_CUDA(cudaStreamSynchronize(stream_));
             if (lastChunk > 0)
             {
-                static const int slots[7] = {KS_BIA_P, KS_BIA_VC_Z, KS_BIA_SPMV1, KS_BIA_S,
-                                             KS_BIA_VC_S, KS_BIA_SPMV2, KS_BIA_X};
-                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 7, activeBefore);
+                static const int slots[11] = {KS_BIA_P,     KS_AMGV_PRE0, KS_AMGV_COARSE, KS_AMGV_POST0,
+                                              KS_BIA_SPMV1, KS_BIA_S,     KS_AMGV_PRE0,   KS_AMGV_COARSE,
+                                              KS_AMGV_POST0, KS_BIA_SPMV2, KS_BIA_X};
+                harvest(std::min(lastChunk, std::max(0, itMax() - itBefore)), slots, 11, activeBefore);
             }
             itBefore = itMax();
             activeBefore = 0;
@@ -1621,21 +1622,23 @@ void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, doubl
             if (stHost_->allDone || launched >= maxIter) break;
             const int m = ktime_ ? 1 : std::min(chunk, maxIter - launched);
             launchChunk(ptrKey("bicga", {vals, diag, x.c[0], x.c[1], x.c[2]}, W), m, [&](int k) {
+                const std::function<void(int)> markZ = [&](int j) { tmark(k, 2 + j); };
+                const std::function<void(int)> markS = [&](int j) { tmark(k, 7 + j); };
                 tmark(k, 0);
                 k_bia_p<3><<<GS_, TPB, 0, stream_>>>(n, br_, bp_, bv_, st_);
                 tmark(k, 1);
-                amgCycle3(cv(bp_), bz_, done);
-                tmark(k, 2);
-                k_bi_spmv1<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
-                tmark(k, 3);
-                k_bia_s<3><<<GS_, TPB, 0, stream_>>>(n, br_, bv_, bs_, st_);
+                amgCycle3(cv(bp_), bz_, done, ktime_ ? markZ : std::function<void(int)>{});
                 tmark(k, 4);
-                amgCycle3(cv(bs_), bsh_, done);
+                k_bi_spmv1<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
                 tmark(k, 5);
-                k_bia_spmv2<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bs_, bt_, partials_, st_);
+                k_bia_s<3><<<GS_, TPB, 0, stream_>>>(n, br_, bv_, bs_, st_);
                 tmark(k, 6);
+                amgCycle3(cv(bs_), bsh_, done, ktime_ ? markS : std::function<void(int)>{});
+                tmark(k, 9);
+                k_bia_spmv2<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bs_, bt_, partials_, st_);
+                tmark(k, 10);
                 k_bia_x<3><<<GS_, TPB, 0, stream_>>>(n, x, bz_, bs_, bsh_, bt_, br_, br0_, partials_, st_);
-                tmark(k, 7);
+                tmark(k, 11);
                 launchCheck("bicga_iter", 0);
             });
             launches_ += static_cast<int64_t>(m) * (5 + 2 * vk);

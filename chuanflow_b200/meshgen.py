@@ -71,7 +71,7 @@ def detail_block_set(n=64, seed=2024, cells_min=2_000, cells_max=200_000):
     log-uniformly in [cells_min, cells_max], aspect ratios uniform in
     [5, 20], inlet profiles cycling flat / parabolic / power1over7, mean
     inlet speeds uniform in [0.05, 0.5] m/s; even-numbered blocks laminar
-    (nu 1e-4), odd-numbered ones marked for k-epsilon at Re_H ~ 2e4.
+    (nu 1e-4), odd-numbered ones marked for k-epsilon (their viscosity is the caller's).
     Seeded numpy draws.  Returns a list of dicts."""
     rng = np.random.default_rng(seed)
     out = []

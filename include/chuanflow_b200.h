@@ -336,9 +336,11 @@ int cfg_last_timing(const cfg_ctx* ctx, double kernel_ms[8], int64_t* launches);
  * p.Ap, the x/r update + norms + r.z, the search-direction update; the four
  * BiCGStab kernels (p/z update, v = Az, t = As^, x/r update); the whole DIC
  * application z = M^-1 r; the AMG-preconditioned momentum BiCGStab's p
- * update, V-cycle z = M p, v = Az, s = r - alpha v, V-cycle s^ = M s,
+ * update, then its two V-cycles' finest pre-sweep and residual, everything
+ * coarser (restriction to prolongation) and finest post-sweep (both
+ * V-cycles of an iteration in these three slots), v = Az, s = r - alpha v,
  * t = As^ and x/r update.  out holds 2 * slots doubles. */
-#define CFG_KERNEL_SLOTS 15
+#define CFG_KERNEL_SLOTS 16
 int cfg_kernel_timing(cfg_ctx* ctx, int32_t enable);
 int cfg_kernel_stats(const cfg_ctx* ctx, double* out, int32_t slots);
 /* The same slots' launches weighted by the vector components each launch
@@ -644,7 +646,8 @@ int cfg_batch_restore(cfg_batch* batch);
  * each candidate's wall time are returned (times: 9 doubles, may be NULL;
  * -1 for a candidate the controls exclude).  Candidates (workers, row blocks
  * per SM): (1,0), (8,1), (16,1), (16,-1), (32,-1), (64,-1), and the
- * single-graph pass (0,1), (0,2), (0,-1), timed on a replay. */
+ * single-graph pass (0,1), (0,2), (0,-1); each is timed on a second run of
+ * the pass (the first carries its graph captures). */
 int cfg_batch_autotune(cfg_batch* batch, const double* q, const cfg_simple_controls* controls, int32_t* workers,
                        int32_t* row_blocks_per_sm, double* times);
 
