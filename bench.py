@@ -351,7 +351,11 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """Replicas: one process per GPU from torchrun's RANK / LOCAL_RANK /
+    WORLD_SIZE, NCCL between them (gloo on a host without CUDA, which the
+    host-side tests use).  No data-path collective: only the barriers and
+    the max-over-ranks reduction of the timings."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -360,18 +364,29 @@ def dist_setup():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local, dist
 
 
 def allreduce_max(dist, v):
+    """The largest of the ranks' values (every rank gets it)."""
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(world, units_per_rank, seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units: all units over the slowest rank's time."""
+    return world * units_per_rank / seconds
 
 
 def barrier(dist):
@@ -978,7 +993,7 @@ def main_simple(args, world, rank, local, dist):
     barrier(dist)
     U1, p1, phi1 = case.download()
     t_max = allreduce_max(dist, timed.ms / 1e3)
-    value = world * ncell * args.steps / t_max
+    value = job_rate(world, ncell * args.steps, t_max)
 
     # ---- end to end through the public API with host buffers: the same K
     # iterations, each uploading its input from pinned host memory and
@@ -999,7 +1014,7 @@ def main_simple(args, world, rank, local, dist):
         case.download(U, p, phi)
         e2e_div += int(r.diverged or not np.isfinite(r.final_continuity_error) or grown(r.final_continuity_error))
     e2e_wall = allreduce_max(dist, time.perf_counter() - t0)
-    e2e = world * ncell * args.steps / e2e_wall
+    e2e = job_rate(world, ncell * args.steps, e2e_wall)
     e2e_same = bool(np.array_equal(U, U1) and np.array_equal(p, p1) and np.array_equal(phi, phi1))
 
     # ---- per-kernel event timing (outside the timed region: the events

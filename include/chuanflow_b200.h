@@ -446,11 +446,12 @@ int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t 
  * this call allocates nothing: its work vectors live in one static device
  * array of the library, sized for at most 262,144 rows (about 8.5 MB, held
  * on every GPU that loads the library until the process exits); larger n is
- * rejected with CFG_EINVAL.  The call synchronises its stream once per chunk
- * of iterations to test convergence, so it cannot be captured into a CUDA
- * graph.  The first call on each device looks that array's address up and
- * keeps it for the life of the process: after a cudaDeviceReset on that
- * device the kept address is stale, so do not call it again after a reset.
+ * rejected with CFG_EINVAL.  The call waits on its stream once per chunk of
+ * iterations to test convergence.  The first call on each device looks that
+ * array's address up (cudaGetSymbolAddress, with the device current) and
+ * keeps it for the life of the process, so make that first call before any
+ * stream capture begins; after a cudaDeviceReset on that device the kept
+ * address is stale, so do not call it again after a reset.
  * Calls share the array and keep no state between them, but two calls whose
  * work overlaps on the GPU (different streams or host threads at once) race
  * on it. */
