@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <mutex>
 #include <numeric>
 #include <utility>
 #include <vector>
@@ -89,6 +90,31 @@ namespace
 constexpr float kOmega = 0.8f;    // damped Jacobi
 constexpr float kScale = 2.0f;    // coarse-correction scaling
 constexpr int kDenseMax = 128;
+
+/// One full wave of a grid-stride row kernel of TPB threads: the SMs times
+/// the blocks of this kernel one SM holds at once (its registers decide),
+/// at most one block per TPB rows.  The finest-level V-cycle passes and the
+/// FCG's SpMV are bound by the latency of their gathers (each waits on the
+/// column loaded before it), so every warp slot an SM has is filled; the
+/// count is looked up once per kernel.
+int waveGrid(const void* kernel, int sms, int rows)
+{
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> perSM;
+    int per = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (const auto& k : perSM)
+            if (k.first == kernel) per = k.second;
+        if (per == 0)
+        {
+            CFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, TPB, 0));
+            per = std::max(1, per);
+            perSM.push_back({kernel, per});
+        }
+    }
+    return std::max(1, std::min((rows + TPB - 1) / TPB, sms * per));
+}
 
 /// one SELL row of the finest operator: sum over its entries of val * f(col).
 /// W bounds the row length at compile time: all columns and values of the
@@ -333,11 +359,18 @@ __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict
     __syncthreads();
     amg_restrict_rows(nc, T.ms, T.mem, r, bc, first, stride);
     __syncthreads();
-    for (int i = threadIdx.x; i < nc; i += kTailThreads)
+    // the coarsest solve xc = M bc: a warp per row, its lanes over the
+    // columns (coalesced reads of the inverse), then a shuffle tree
     {
-        float s = 0.0f;
-        for (int j = 0; j < nc; ++j) s += T.dense[i * nc + j] * bc[j];
-        xc[i] = s;
+        const int lane = threadIdx.x & 31;
+        for (int i = threadIdx.x >> 5; i < nc; i += kTailThreads / 32)
+        {
+            float s = 0.0f;
+            for (int j = lane; j < nc; j += 32) s += T.dense[i * nc + j] * bc[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) xc[i] = s;
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += kTailThreads) y[i] = x[i] + kScale * xc[T.agg[i]];
@@ -948,9 +981,9 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
         AmgLevel& N = a.lv[l + 1];
         if (l == 0)
         {
-            if (Wsel == 7) k_amg_pre0<7><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, V.r);
-            else if (Wsel == 16) k_amg_pre0<16><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, V.r);
-            else k_amg_pre0<0><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.x, V.r);
+            const auto pre0 = Wsel == 7 ? k_amg_pre0<7> : (Wsel == 16 ? k_amg_pre0<16> : k_amg_pre0<0>);
+            pre0<<<waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_>>>(
+                stop, A, amgVals32_, V.dinv, r, V.x, V.r);
         }
         else
             k_amg_pre<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
@@ -967,12 +1000,11 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
         k_amg_prolong<<<grid(V.n), TPB, 0, stream_>>>(stop, V.n, V.x, xc, V.agg, V.r);
         if (l == 0)
         {
-            if (Wsel == 7)
-                k_amg_post0<7><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
-            else if (Wsel == 16)
-                k_amg_post0<16><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
-            else
-                k_amg_post0<0><<<GS_, TPB, 0, stream_>>>(stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
+            // one block partial per block: the grid is at most G_ blocks,
+            // which partials_ holds
+            const auto post0 = Wsel == 7 ? k_amg_post0<7> : (Wsel == 16 ? k_amg_post0<16> : k_amg_post0<0>);
+            post0<<<waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_>>>(
+                stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
         }
         else
             k_amg_post<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.r, V.xo);
@@ -1000,9 +1032,9 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
         AmgLevel& N = a.lv[l + 1];
         if (l == 0)
         {
-            if (Wsel == 7) k_amgv_pre0<7><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
-            else if (Wsel == 16) k_amgv_pre0<16><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
-            else k_amgv_pre0<0><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
+            const auto pre0 = Wsel == 7 ? k_amgv_pre0<7> : (Wsel == 16 ? k_amgv_pre0<16> : k_amgv_pre0<0>);
+            pre0<<<waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_>>>(
+                done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
             if (mark) mark(0);
         }
         else
@@ -1020,9 +1052,9 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
         if (l == 0)
         {
             if (mark) mark(1);
-            if (Wsel == 7) k_amgv_post0<7><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
-            else if (Wsel == 16) k_amgv_post0<16><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
-            else k_amgv_post0<0><<<GS_, TPB, 0, stream_>>>(done, A, amgVals32_, V.dinv, b, V.r3, z);
+            const auto post0 = Wsel == 7 ? k_amgv_post0<7> : (Wsel == 16 ? k_amgv_post0<16> : k_amgv_post0<0>);
+            post0<<<waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_>>>(
+                done, A, amgVals32_, V.dinv, b, V.r3, z);
         }
         else
             k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.r3, V.xo3);
@@ -1245,10 +1277,10 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
     amgCycle(r, z, nullptr, a.st);
     k_fcgd_p<<<GS_, TPB, 0, stream_>>>(n, z, p, a.st, 1);
     launchCheck("fcgd_p0");
+    const auto spmv = Wsel == 7 ? k_fcgd_spmv<7> : (Wsel == 16 ? k_fcgd_spmv<16> : k_fcgd_spmv<0>);
+    const int spmvGrid = waveGrid(reinterpret_cast<const void*>(spmv), sms_, n);
     auto iteration = [&]() {
-        if (Wsel == 7) k_fcgd_spmv<7><<<GS_, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
-        else if (Wsel == 16) k_fcgd_spmv<16><<<GS_, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
-        else k_fcgd_spmv<0><<<GS_, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
+        spmv<<<spmvGrid, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
         k_fcgd_update<<<GS_, TPB, 0, stream_>>>(n, p, q, x, r, partials_, a.st);
         amgCycle(r, z, q, a.st);
         k_fcgd_p<<<GS_, TPB, 0, stream_>>>(n, z, p, a.st, 0);
