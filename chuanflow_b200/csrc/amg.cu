@@ -49,8 +49,8 @@ struct AmgLevel
     int nnzNext = 0;
     // work vectors: rhs, first sweep, residual, output
     float *b = nullptr, *x = nullptr, *r = nullptr, *xo = nullptr;
-    // the same for the three-component V-cycle (component q at q * n),
-    // allocated on its first use
+    // the same for the three-component V-cycle (a float4 per row above the
+    // last level, component q at q * n on it), allocated on its first use
     float *b3 = nullptr, *x3 = nullptr, *r3 = nullptr, *xo3 = nullptr;
 };
 
@@ -424,10 +424,10 @@ __global__ void __launch_bounds__(TPB) k_amg_dinv0(int n, const double* __restri
 
 // ---- the V-cycle on three right-hand sides at once (the momentum
 // components share their matrix): the same arithmetic per component as the
-// single V-cycle above, with the matrix read once for the three.  Level
-// vectors hold component q at offset q * n.  `done` (the BiCGStab's
-// per-component flags) skips a converged component's work; its outputs are
-// left as they were.
+// single V-cycle above, with the matrix read once for the three.  `done`
+// (the BiCGStab's per-component flags) zeroes a converged component's input
+// lanes and leaves its output z_q as it was; the V-cycle returns at once
+// when all three are done.
 
 /// one SELL row of the finest operator against three vectors
 template <int W, class F>
@@ -510,11 +510,28 @@ __device__ __forceinline__ Active3 active3(const int* done)
     return Active3{{done[0] == 0, done[1] == 0, done[2] == 0}};
 }
 
-/// finest level, first sweep and residual for three FP64 right-hand sides
+// Level vectors of the three-component V-cycle, above the last level, hold
+// one float4 per row: the three components in x, y, z (w is zero).  A row
+// gathered by a neighbour's sweep or by its aggregate's restriction is one
+// 16-byte load, not three scattered ones.  The last level (the fused tail or
+// the dense coarsest solve) keeps component q at offset q * n, as the single
+// V-cycle's kernels there expect.  A converged component's lanes carry zeros
+// (its input lanes are read as zero), so every lane is computed and stored.
+
+__device__ __forceinline__ float4 pack3(const float (&v)[3]) { return make_float4(v[0], v[1], v[2], 0.0f); }
+__device__ __forceinline__ void unpack3(float4 p, float (&v)[3])
+{
+    v[0] = p.x;
+    v[1] = p.y;
+    v[2] = p.z;
+}
+
+/// finest level, first sweep and residual for three FP64 right-hand sides:
+/// x = w D^-1 b and r = b - A x
 template <int W>
-__global__ void __launch_bounds__(TPB) k_amgv_pre0(const int* __restrict__ done, DMat A, const float* __restrict__ val,
-                                                   const float* __restrict__ dinv, CV3P b, float* __restrict__ x,
-                                                   float* __restrict__ r)
+__global__ void __launch_bounds__(TPB, (W > 0 && W <= 8) ? 6 : 1) k_amgv_pre0(const int* __restrict__ done, DMat A, const float* __restrict__ val,
+                                                   const float* __restrict__ dinv, CV3P b, float4* __restrict__ x,
+                                                   float4* __restrict__ r)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
@@ -528,57 +545,29 @@ __global__ void __launch_bounds__(TPB) k_amgv_pre0(const int* __restrict__ done,
             for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? wd * static_cast<float>(__ldg(b.c[q] + j)) : 0.0f;
         });
         const float dc = dinv[c];
+        float xv[3], rv[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q)
-            if (act.a[q])
-            {
-                const float bc = static_cast<float>(b.c[q][c]);
-                x[q * n + c] = kOmega * dc * bc;
-                r[q * n + c] = bc - s[q];
-            }
-    }
-}
-
-/// coarse level, the same on CSR
-__global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, int n, const int* __restrict__ rs,
-                                                  const int* __restrict__ cols, const float* __restrict__ val,
-                                                  const float* __restrict__ dinv, const float* __restrict__ b,
-                                                  float* __restrict__ x, float* __restrict__ r)
-{
-    const Active3 act = active3(done);
-    if (act.none()) return;
-    const int l = threadIdx.x % kGroup;
-    const int stride = gridDim.x * (TPB / kGroup);
-    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
-    {
-        const int base = i0 - (threadIdx.x % 32) / kGroup;
-        if (base >= n) break;
-        const int i = i0 < n ? i0 : -1;
-        float s[3];
-        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) {
-            const float wd = kOmega * __ldg(dinv + j);
-#pragma unroll
-            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? wd * __ldg(b + q * n + j) : 0.0f;
-        });
-        if (i >= 0 && l == 0)
         {
-            const float di = dinv[i];
-#pragma unroll
-            for (int q = 0; q < 3; ++q)
-                if (act.a[q])
-                {
-                    const float bi = b[q * n + i];
-                    x[q * n + i] = kOmega * di * bi;
-                    r[q * n + i] = bi - s[q];
-                }
+            const float bc = act.a[q] ? static_cast<float>(b.c[q][c]) : 0.0f;
+            xv[q] = kOmega * dc * bc;
+            rv[q] = bc - s[q];
         }
+        x[c] = pack3(xv);
+        r[c] = pack3(rv);
     }
 }
 
-/// the residuals summed over each aggregate (a group of lanes per aggregate)
-__global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ done, int n, int nc,
-                                                       const int* __restrict__ ms, const int* __restrict__ mem,
-                                                       const float* __restrict__ r, float* __restrict__ bc)
+/// the residuals summed over each aggregate (a group of lanes per aggregate,
+/// lane l taking members l, l + G, ..., then the shuffle tree): the next
+/// level's right-hand side.  Into a level above the last one it also stores
+/// that level's first sweep w D^-1 b, which the level's residual pass
+/// gathers; into the last level it writes component q at offset q * nc.
+template <bool kLast>
+__global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ done, int nc, const int* __restrict__ ms,
+                                                       const int* __restrict__ mem, const float4* __restrict__ r,
+                                                       const float* __restrict__ dinvc, float4* __restrict__ bc,
+                                                       float4* __restrict__ xc, float* __restrict__ bcLast)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
@@ -589,47 +578,44 @@ __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ d
         const int base = I0 - (threadIdx.x % 32) / kGroup;
         if (base >= nc) break;
         const int I = I0 < nc ? I0 : -1;
-        // the members' indices once for the three vectors; per vector the
-        // lane-strided sums and shuffle tree of group_members
         float s[3] = {0.0f, 0.0f, 0.0f};
         if (I >= 0)
             for (int k = __ldg(ms + I) + l; k < __ldg(ms + I + 1); k += kGroup)
             {
-                const int m = __ldg(mem + k);
+                float v[3];
+                unpack3(__ldg(r + __ldg(mem + k)), v);
 #pragma unroll
-                for (int q = 0; q < 3; ++q) s[q] += act.a[q] ? __ldg(r + q * n + m) : 0.0f;
+                for (int q = 0; q < 3; ++q) s[q] += v[q];
             }
 #pragma unroll
         for (int q = 0; q < 3; ++q)
-        {
 #pragma unroll
             for (int o = kGroup / 2; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
-            if (act.a[q] && I >= 0 && l == 0) bc[q * nc + I] = s[q];
+        if (I < 0 || l != 0) continue;
+        if constexpr (kLast)
+        {
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (act.a[q]) bcLast[q * nc + I] = s[q];
+        }
+        else
+        {
+            const float wd = kOmega * dinvc[I];
+            float xv[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) xv[q] = wd * s[q];
+            bc[I] = pack3(s);
+            xc[I] = pack3(xv);
         }
     }
 }
 
-/// the coarse corrections brought to this level: y = x + s P xc
-__global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ done, int n, int nNext,
-                                                      const float* __restrict__ x, const float* __restrict__ xc,
-                                                      const int* __restrict__ agg, float* __restrict__ y)
-{
-    const Active3 act = active3(done);
-    if (act.none()) return;
-    FOR_ROWS(i, n)
-    {
-        const int ai = agg[i];
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-            if (act.a[q]) y[q * n + i] = x[q * n + i] + kScale * xc[q * nNext + ai];
-    }
-}
-
-/// coarse level: xo = y + w D^-1 (b - A y)
-__global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done, int n, const int* __restrict__ rs,
-                                                   const int* __restrict__ cols, const float* __restrict__ val,
-                                                   const float* __restrict__ dinv, const float* __restrict__ b,
-                                                   const float* __restrict__ y, float* __restrict__ xo)
+/// coarse level, the residual of the first sweep: r = b - A x, with x the
+/// sweep the restriction into this level stored
+__global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, int n, const int* __restrict__ rs,
+                                                  const int* __restrict__ cols, const float* __restrict__ val,
+                                                  const float4* __restrict__ x, const float4* __restrict__ b,
+                                                  float4* __restrict__ r)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
@@ -641,24 +627,80 @@ __global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done,
         if (base >= n) break;
         const int i = i0 < n ? i0 : -1;
         float s[3];
-        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) {
-#pragma unroll
-            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? __ldg(y + q * n + j) : 0.0f;
-        });
+        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) { unpack3(__ldg(x + j), g); });
         if (i >= 0 && l == 0)
         {
-            const float di = dinv[i];
+            float bi[3], rv[3];
+            unpack3(b[i], bi);
 #pragma unroll
-            for (int q = 0; q < 3; ++q)
-                if (act.a[q]) xo[q * n + i] = y[q * n + i] + kOmega * di * (b[q * n + i] - s[q]);
+            for (int q = 0; q < 3; ++q) rv[q] = bi[q] - s[q];
+            r[i] = pack3(rv);
         }
     }
 }
 
-/// finest level: z = y + w D^-1 (b - A y), into FP64
+/// the coarse corrections brought to this level: y = x + s P xc, with xc
+/// one float4 per row, or component q at offset q * nNext from the last level
+template <bool kFromLast>
+__global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ done, int n, int nNext,
+                                                      const float4* __restrict__ x, const float4* __restrict__ xc,
+                                                      const float* __restrict__ xcLast, const int* __restrict__ agg,
+                                                      float4* __restrict__ y)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    FOR_ROWS(i, n)
+    {
+        const int ai = agg[i];
+        float xv[3], cv[3], yv[3];
+        unpack3(x[i], xv);
+        if constexpr (kFromLast)
+        {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) cv[q] = act.a[q] ? xcLast[q * nNext + ai] : 0.0f;
+        }
+        else
+            unpack3(xc[ai], cv);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) yv[q] = xv[q] + kScale * cv[q];
+        y[i] = pack3(yv);
+    }
+}
+
+/// coarse level: xo = y + w D^-1 (b - A y)
+__global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done, int n, const int* __restrict__ rs,
+                                                   const int* __restrict__ cols, const float* __restrict__ val,
+                                                   const float* __restrict__ dinv, const float4* __restrict__ b,
+                                                   const float4* __restrict__ y, float4* __restrict__ xo)
+{
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    const int l = threadIdx.x % kGroup;
+    const int stride = gridDim.x * (TPB / kGroup);
+    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
+    {
+        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        float s[3];
+        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) { unpack3(__ldg(y + j), g); });
+        if (i >= 0 && l == 0)
+        {
+            const float di = dinv[i];
+            float bi[3], yi[3], xv[3];
+            unpack3(b[i], bi);
+            unpack3(y[i], yi);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) xv[q] = yi[q] + kOmega * di * (bi[q] - s[q]);
+            xo[i] = pack3(xv);
+        }
+    }
+}
+
+/// finest level: z = y + w D^-1 (b - A y), into FP64 (active components only)
 template <int W>
 __global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done, DMat A, const float* __restrict__ val,
-                                                    const float* __restrict__ dinv, CV3P b, const float* __restrict__ y,
+                                                    const float* __restrict__ dinv, CV3P b, const float4* __restrict__ y,
                                                     V3P z)
 {
     const Active3 act = active3(done);
@@ -667,15 +709,14 @@ __global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done
     FOR_ROWS(c, n)
     {
         float s[3];
-        sell_row3<W>(A, val, c, s, [&](int j, float (&g)[3]) {
-#pragma unroll
-            for (int q = 0; q < 3; ++q) g[q] = act.a[q] ? __ldg(y + q * n + j) : 0.0f;
-        });
+        sell_row3<W>(A, val, c, s, [&](int j, float (&g)[3]) { unpack3(__ldg(y + j), g); });
         const float dc = dinv[c];
+        float yc[3];
+        unpack3(y[c], yc);
 #pragma unroll
         for (int q = 0; q < 3; ++q)
             if (act.a[q])
-                z.c[q][c] = static_cast<double>(y[q * n + c] + kOmega * dc * (static_cast<float>(b.c[q][c]) - s[q]));
+                z.c[q][c] = static_cast<double>(yc[q] + kOmega * dc * (static_cast<float>(b.c[q][c]) - s[q]));
     }
 }
 
@@ -1026,6 +1067,9 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
     auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
     auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
     const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
+    // levels above `last` hold a float4 per row; `last` (the tail level or
+    // the dense coarsest) holds component q at q * n
+    auto f4 = [](float* p) { return reinterpret_cast<float4*>(p); };
     for (int l = 0; l < last; ++l)
     {
         AmgLevel& V = a.lv[l];
@@ -1034,12 +1078,17 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
         {
             const auto pre0 = Wsel == 7 ? k_amgv_pre0<7> : (Wsel == 16 ? k_amgv_pre0<16> : k_amgv_pre0<0>);
             pre0<<<waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_>>>(
-                done, A, amgVals32_, V.dinv, b, V.x3, V.r3);
+                done, A, amgVals32_, V.dinv, b, f4(V.x3), f4(V.r3));
             if (mark) mark(0);
         }
         else
-            k_amgv_pre<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.x3, V.r3);
-        k_amgv_restrict<<<ggrid(N.n), TPB, 0, stream_>>>(done, V.n, N.n, V.ms, V.mem, V.r3, N.b3);
+            k_amgv_pre<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, f4(V.x3), f4(V.b3), f4(V.r3));
+        if (l + 1 == last)
+            k_amgv_restrict<true><<<ggrid(N.n), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), nullptr, nullptr,
+                                                                   nullptr, N.b3);
+        else
+            k_amgv_restrict<false><<<ggrid(N.n), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), N.dinv, f4(N.b3),
+                                                                    f4(N.x3), nullptr);
     }
     if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true));
     else k_amg_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
@@ -1047,17 +1096,22 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
     {
         AmgLevel& V = a.lv[l];
         const AmgLevel& N = a.lv[l + 1];
-        const float* xc = (l + 1 == L - 1) ? N.x3 : N.xo3;
-        k_amgv_prolong<<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, V.x3, xc, V.agg, V.r3);
+        if (l + 1 == last)
+            k_amgv_prolong<true><<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, f4(V.x3), nullptr,
+                                                                 (l + 1 == L - 1) ? N.x3 : N.xo3, V.agg, f4(V.r3));
+        else
+            k_amgv_prolong<false><<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, f4(V.x3), f4(N.xo3), nullptr, V.agg,
+                                                                  f4(V.r3));
         if (l == 0)
         {
             if (mark) mark(1);
             const auto post0 = Wsel == 7 ? k_amgv_post0<7> : (Wsel == 16 ? k_amgv_post0<16> : k_amgv_post0<0>);
             post0<<<waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_>>>(
-                done, A, amgVals32_, V.dinv, b, V.r3, z);
+                done, A, amgVals32_, V.dinv, b, f4(V.r3), z);
         }
         else
-            k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, V.b3, V.r3, V.xo3);
+            k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, f4(V.b3), f4(V.r3),
+                                                         f4(V.xo3));
     }
     launchCheck("amg_vcycle3", amgCycleKernels());
 }
@@ -1070,7 +1124,7 @@ void Ctx::amgVectors3()
     for (auto& V : amg_->lv)
         if (!V.x3)
         {
-            const size_t m = 3 * static_cast<size_t>(V.n);
+            const size_t m = 4 * static_cast<size_t>(V.n);  // a float4 per row, or three rows of n
             V.b3 = alloc<float>(m);
             V.x3 = alloc<float>(m);
             V.r3 = alloc<float>(m);
