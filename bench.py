@@ -142,11 +142,13 @@ def kernel_bytes(N, F, s=8, i=4):
     # and column per entry, N + 2F entries) and D^-1 each; per component the
     # pre-sweep reads the FP64 input (gathered) and writes the FP32 sweep and
     # residual, the post-sweep reads the FP64 input and the prolongated FP32
-    # correction (gathered) and writes the FP64 output.  Everything between
-    # (restriction of the residual with the member list, the coarse levels,
-    # the prolongation: the sweep, the aggregate map and the coarse output
-    # read, the correction written) is counted at its finest-level streams
-    # plus about 30% for the coarser levels.
+    # correction (gathered) and writes the FP64 output.  The level vectors
+    # hold a float4 per row; only the three components' 12 bytes are
+    # counted, not the fourth word.  Everything between (restriction of the
+    # residual with the member list, the coarse levels, the prolongation:
+    # the sweep, the aggregate map and the coarse output read, the
+    # correction written) is counted at its finest-level streams plus about
+    # 30% for the coarser levels.
     f4 = 4
     sell32 = (N + 2 * F) * 2 * f4 + f4 * N
     coarse3 = (1.3 * 3 * f4 * N, 1.3 * 3 * f4 * N)

@@ -80,6 +80,10 @@ struct AmgState
     std::vector<int> hrs, hcols;  // coarsest CSR on the host
     bool valuesReady = false;
     double setupMs = 0, valuesMs = 0;
+    // the tail level in shared memory: the dynamic size (0: it does not
+    // fit, k_amg_tail runs from global memory) and the level's entries
+    size_t tailSmem = 0;
+    int tailNnz = 0;
 };
 
 void AmgDeleter::operator()(AmgState* a) const { delete a; }
@@ -168,7 +172,7 @@ __device__ __forceinline__ float group_row(const int* __restrict__ rs, const int
     for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;
 }
-constexpr int kGroup = 8;
+constexpr int kGroup = 4;
 
 /// the sum of an aggregate's members, by a group of G lanes: lane l of the
 /// group takes members l, l + G, ...; every lane of the group holds the
@@ -376,6 +380,127 @@ __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict
     for (int i = threadIdx.x; i < n; i += kTailThreads) y[i] = x[i] + kScale * xc[T.agg[i]];
     __syncthreads();
     amg_post_rows(n, T.rs, T.cols, T.val, T.dinv, b, y, xo, first, stride);
+}
+
+/// Shared-memory layout of k_amg_tail_smem (4-byte words): the level's CSR
+/// (rs n + 1, cols nnz, val nnz), dinv n, agg n, the aggregates' member
+/// lists (ms nc + 1, mem n), the dense inverse nc * nc, and the vectors b,
+/// x, r (then y) n each, bc and xc nc each.
+__host__ __device__ constexpr size_t tailSmemWords(int n, int nnz, int nc)
+{
+    return static_cast<size_t>(n + 1) + 2 * static_cast<size_t>(nnz) + 2 * static_cast<size_t>(n) +
+           static_cast<size_t>(nc + 1) + static_cast<size_t>(n) + static_cast<size_t>(nc) * nc + 3 * static_cast<size_t>(n) +
+           2 * static_cast<size_t>(nc);
+}
+
+/// k_amg_tail with the level held in shared memory: one coalesced load of
+/// the level's matrix, aggregates, dense inverse and right-hand side, then
+/// every phase (pre-sweep and residual, restriction, dense solve,
+/// prolongation, post-sweep) reads shared memory only, with the same lane
+/// groups, orders and arithmetic as k_amg_tail.  Block q works on vector q;
+/// only the output xo goes back to global memory.
+__global__ void __launch_bounds__(kTailThreads) k_amg_tail_smem(const int* __restrict__ done, TailLevel T, int nnz)
+{
+    const int q = blockIdx.x;
+    if (done && done[q]) return;
+    extern __shared__ __align__(16) int tsm[];
+    const int n = T.n, nc = T.nc, t = threadIdx.x;
+    int* rs = tsm;
+    int* cols = rs + (n + 1);
+    float* val = reinterpret_cast<float*>(cols + nnz);
+    float* dinv = val + nnz;
+    int* agg = reinterpret_cast<int*>(dinv + n);
+    int* ms = agg + n;
+    int* mem = ms + (nc + 1);
+    float* dense = reinterpret_cast<float*>(mem + n);
+    float* b = dense + static_cast<size_t>(nc) * nc;
+    float* x = b + n;
+    float* r = x + n;
+    float* bc = r + n;
+    float* xc = bc + nc;
+    for (int i = t; i <= n; i += kTailThreads) rs[i] = T.rs[i];
+    for (int e = t; e < nnz; e += kTailThreads)
+    {
+        cols[e] = T.cols[e];
+        val[e] = T.val[e];
+    }
+    for (int i = t; i < n; i += kTailThreads)
+    {
+        dinv[i] = T.dinv[i];
+        agg[i] = T.agg[i];
+        mem[i] = T.mem[i];
+        b[i] = T.b[static_cast<size_t>(q) * n + i];
+    }
+    for (int i = t; i <= nc; i += kTailThreads) ms[i] = T.ms[i];
+    for (int i = t; i < nc * nc; i += kTailThreads) dense[i] = T.dense[i];
+    __syncthreads();
+    const int l = t % kGroup, first = t / kGroup, stride = kTailThreads / kGroup;
+    // pre-sweep and residual: x = w D^-1 b, r = b - A x
+    for (int i0 = first;; i0 += stride)
+    {
+        const int base = i0 - (t % 32) / kGroup;
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        float s = 0.0f;
+        if (i >= 0)
+            for (int e = rs[i] + l; e < rs[i + 1]; e += kGroup)
+            {
+                const int j = cols[e];
+                s += val[e] * (kOmega * dinv[j] * b[j]);
+            }
+#pragma unroll
+        for (int o = kGroup / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (i >= 0 && l == 0)
+        {
+            x[i] = kOmega * dinv[i] * b[i];
+            r[i] = b[i] - s;
+        }
+    }
+    __syncthreads();
+    // restriction
+    for (int I0 = first;; I0 += stride)
+    {
+        const int base = I0 - (t % 32) / kGroup;
+        if (base >= nc) break;
+        const int I = I0 < nc ? I0 : -1;
+        float s = 0.0f;
+        if (I >= 0)
+            for (int k = ms[I] + l; k < ms[I + 1]; k += kGroup) s += r[mem[k]];
+#pragma unroll
+        for (int o = kGroup / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (I >= 0 && l == 0) bc[I] = s;
+    }
+    __syncthreads();
+    // the coarsest solve xc = M bc, a warp per row
+    {
+        const int lane = t & 31;
+        for (int i = t >> 5; i < nc; i += kTailThreads / 32)
+        {
+            float s = 0.0f;
+            for (int j = lane; j < nc; j += 32) s += dense[i * nc + j] * bc[j];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) xc[i] = s;
+        }
+    }
+    __syncthreads();
+    // prolongation into r (the residual is no longer needed)
+    for (int i = t; i < n; i += kTailThreads) r[i] = x[i] + kScale * xc[agg[i]];
+    __syncthreads();
+    // post-sweep: xo = y + w D^-1 (b - A y)
+    float* xo = T.xo + static_cast<size_t>(q) * n;
+    for (int i0 = first;; i0 += stride)
+    {
+        const int base = i0 - (t % 32) / kGroup;
+        if (base >= n) break;
+        const int i = i0 < n ? i0 : -1;
+        float s = 0.0f;
+        if (i >= 0)
+            for (int e = rs[i] + l; e < rs[i + 1]; e += kGroup) s += val[e] * r[cols[e]];
+#pragma unroll
+        for (int o = kGroup / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (i >= 0 && l == 0) xo[i] = r[i] + kOmega * dinv[i] * (b[i] - s);
+    }
 }
 
 /// the coarsest solve, x = M^-1 b with the dense inverse, when the finest
@@ -757,6 +882,8 @@ int aggregate(const Pattern& A, std::vector<int>& agg)
 
 }  // namespace
 
+static int tailLevel(const AmgState& a);
+
 /// The hierarchy's structure from the device pressure pattern.
 void Ctx::amgSetup()
 {
@@ -871,6 +998,22 @@ void Ctx::amgSetup()
         AmgLevel& L = a->lv.back();
         L.val = alloc<float>(std::max<size_t>(P.cols.size(), 1));
         a->dense = alloc<float>(static_cast<size_t>(P.n) * P.n);
+    }
+    // the tail level's shared-memory copy, when it and the dense inverse fit
+    // in one block's opt-in shared memory (set before any stream capture)
+    if (const int T = tailLevel(*a); T >= 0)
+    {
+        const int nnz = a->lv[static_cast<size_t>(T) - 1].nnzNext;
+        const size_t bytes = 4 * tailSmemWords(a->lv[T].n, nnz, a->lv[static_cast<size_t>(T) + 1].n);
+        int optin = 0;
+        CFG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+        if (bytes <= static_cast<size_t>(optin))
+        {
+            CFG_CUDA(cudaFuncSetAttribute(k_amg_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(bytes)));
+            a->tailSmem = bytes;
+            a->tailNnz = nnz;
+        }
     }
     CFG_CUDA(cudaStreamSynchronize(stream_));
     a->setupMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1030,7 +1173,9 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
             k_amg_pre<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
         k_amg_restrict<<<ggrid(N.n), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
     }
-    if (T >= 0) k_amg_tail<<<1, kTailThreads, 0, stream_>>>(stop, tailView(a, T, false));
+    if (T >= 0 && a.tailSmem)
+        k_amg_tail_smem<<<1, kTailThreads, a.tailSmem, stream_>>>(stop, tailView(a, T, false), a.tailNnz);
+    else if (T >= 0) k_amg_tail<<<1, kTailThreads, 0, stream_>>>(stop, tailView(a, T, false));
     else k_amg_dense<<<1, kDenseMax, 0, stream_>>>(stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
     // up: each level corrects with the next level's output
     for (int l = last - 1; l >= 0; --l)
@@ -1090,7 +1235,9 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
             k_amgv_restrict<false><<<ggrid(N.n), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), N.dinv, f4(N.b3),
                                                                     f4(N.x3), nullptr);
     }
-    if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true));
+    if (T >= 0 && a.tailSmem)
+        k_amg_tail_smem<<<3, kTailThreads, a.tailSmem, stream_>>>(done, tailView(a, T, true), a.tailNnz);
+    else if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true));
     else k_amg_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
     for (int l = last - 1; l >= 0; --l)
     {

@@ -134,9 +134,15 @@ __device__ __forceinline__ void mma_bf16_16816(float (&d)[4], uint32_t a0, uint3
 }
 
 constexpr int XP = 2 * H + 8;  // padded BF16 row of [h | m] and of the weights (144 bytes)
+constexpr int kSlots = 8;      // entry slots a SELL slice may have for the staged message path
 
 /// one residual message-passing layer: hout = hin + relu(A h + B m + b) for
-/// 16 cells per warp step, the contraction on the tensor cores
+/// 16 cells per warp step, the contraction on the tensor cores.  The 16
+/// cells of a step are consecutive rows of one SELL slice: their entries
+/// (column, coefficient) are loaded two slots per warp-wide load into shared
+/// memory first, so the neighbour-state gathers of all 16 cells are
+/// independent of each other and issue back to back (lane k gathers
+/// channel k of each neighbour: one 128-byte line per neighbour).
 __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const float* __restrict__ coef,
                                                             const __nv_bfloat16* __restrict__ wl,
                                                             const float* __restrict__ hin, float* __restrict__ hout,
@@ -147,6 +153,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const float*
     __shared__ float sb[H];
     __shared__ __align__(16) __nv_bfloat16 sX[kWarps][16][XP];
     __shared__ float sU[kWarps][16][H + 1];
+    // the step's row entries: slot k of cell t at [k][t] (column; -1 for a
+    // pad, the diagonal or a cell past the end), coefficient beside it
+    __shared__ int2 sE[kWarps][kSlots][16];
     for (int t = threadIdx.x; t < H * H; t += blockDim.x)
     {
         const int o = t / H, k = t % H;
@@ -161,20 +170,60 @@ __global__ void __launch_bounds__(kWarps * 32) k_mpnn_layer(DMat A, const float*
     for (int g = blockIdx.x * kWarps + w; g < groups; g += gridDim.x * kWarps)
     {
         const int c0 = g * 16;
+        const int s0 = __ldg(A.start + (c0 >> 5)), nSlots = (__ldg(A.start + (c0 >> 5) + 1) - s0) >> 5;
         float hr[16];
-#pragma unroll
-        for (int t = 0; t < 16; ++t)
+        if (nSlots <= kSlots)
         {
-            const int i = c0 + t;
-            float h = 0.f, m = 0.f;
-            if (i < A.n)
+            const int t = lane & 15, i = c0 + t;
+            for (int k = lane >> 4; k < nSlots; k += 2)
             {
-                h = hin[static_cast<size_t>(i) * H + lane];
-                m = message(A, coef, hin, i, lane);
+                const int e = s0 + (c0 & 31) + t + 32 * k;
+                int j = __ldg(A.col + e);
+                if (i >= A.n || j == i) j = -1;
+                sE[w][k][t] = make_int2(j, __float_as_int(__ldg(coef + e)));
             }
-            hr[t] = h;
-            sX[w][t][lane] = __float2bfloat16(h);
-            sX[w][t][H + lane] = __float2bfloat16(m);
+            __syncwarp();
+            float m[16];
+#pragma unroll
+            for (int t2 = 0; t2 < 16; ++t2)
+            {
+                hr[t2] = c0 + t2 < A.n ? hin[static_cast<size_t>(c0 + t2) * H + lane] : 0.f;
+                m[t2] = 0.f;
+            }
+            // slot by slot, the same order as message(): the gathers of the
+            // 16 cells in one slot are independent
+            for (int k = 0; k < nSlots; ++k)
+            {
+#pragma unroll
+                for (int t2 = 0; t2 < 16; ++t2)
+                {
+                    const int2 p = sE[w][k][t2];
+                    if (p.x >= 0) m[t2] += __int_as_float(p.y) * hin[static_cast<size_t>(p.x) * H + lane];
+                }
+            }
+#pragma unroll
+            for (int t2 = 0; t2 < 16; ++t2)
+            {
+                sX[w][t2][lane] = __float2bfloat16(hr[t2]);
+                sX[w][t2][H + lane] = __float2bfloat16(m[t2]);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int t = 0; t < 16; ++t)
+            {
+                const int i = c0 + t;
+                float h = 0.f, m = 0.f;
+                if (i < A.n)
+                {
+                    h = hin[static_cast<size_t>(i) * H + lane];
+                    m = message(A, coef, hin, i, lane);
+                }
+                hr[t] = h;
+                sX[w][t][lane] = __float2bfloat16(h);
+                sX[w][t][H + lane] = __float2bfloat16(m);
+            }
         }
         __syncwarp();
         float d[4][4] = {};
