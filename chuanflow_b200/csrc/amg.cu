@@ -25,6 +25,7 @@
 #include <cmath>
 #include <mutex>
 #include <numeric>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -47,6 +48,9 @@ struct AmgLevel
     int *ms = nullptr, *mem = nullptr;
     int *gs = nullptr, *gl = nullptr;
     int nnzNext = 0;
+    // lanes per row of this level's passes (levels >= 1) and per aggregate
+    // of its restriction into the next level
+    int gRow = 4, gAgg = 4;
     // work vectors: rhs, first sweep, residual, output
     float *b = nullptr, *x = nullptr, *r = nullptr, *xo = nullptr;
     // the same for the three-component V-cycle (a float4 per row above the
@@ -118,6 +122,19 @@ int waveGrid(const void* kernel, int sms, int rows)
         }
     }
     return std::max(1, std::min((rows + TPB - 1) / TPB, sms * per));
+}
+
+/// f(std::integral_constant<int, G>{}) for the lane group g (4, 8, 16 or 32)
+template <class F>
+void withGroup(int g, F&& f)
+{
+    switch (g)
+    {
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 16: f(std::integral_constant<int, 16>{}); break;
+        case 32: f(std::integral_constant<int, 32>{}); break;
+        default: f(std::integral_constant<int, 4>{}); break;
+    }
 }
 
 /// one SELL row of the finest operator: sum over its entries of val * f(col).
@@ -206,20 +223,21 @@ __global__ void __launch_bounds__(TPB) k_amg_pre0(const int* __restrict__ stop, 
     }
 }
 
-/// coarse level, the same on CSR
+/// coarse level, the same on CSR, a group of G lanes per row
+template <int G>
 __device__ __forceinline__ void amg_pre_rows(int n, const int* __restrict__ rs, const int* __restrict__ cols,
                                              const float* __restrict__ val, const float* __restrict__ dinv,
                                              const float* __restrict__ b, float* __restrict__ x,
                                              float* __restrict__ r, int first, int stride)
 {
-    const int l = threadIdx.x % kGroup;
+    const int l = threadIdx.x % G;
     // whole warps iterate together (the shuffle needs every lane)
     for (int i0 = first;; i0 += stride)
     {
-        const int base = i0 - (threadIdx.x % 32) / kGroup;  // the warp's first row this round
+        const int base = i0 - (threadIdx.x % 32) / G;  // the warp's first row this round
         if (base >= n) break;
         const int i = i0 < n ? i0 : -1;
-        const float s = group_row<kGroup>(rs, cols, val, i, l, [&](int j) { return kOmega * __ldg(dinv + j) * __ldg(b + j); });
+        const float s = group_row<G>(rs, cols, val, i, l, [&](int j) { return kOmega * __ldg(dinv + j) * __ldg(b + j); });
         if (i >= 0 && l == 0)
         {
             const float bi = b[i];
@@ -229,40 +247,41 @@ __device__ __forceinline__ void amg_pre_rows(int n, const int* __restrict__ rs, 
     }
 }
 
+template <int G>
 __global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, int n, const int* __restrict__ rs,
                                                  const int* __restrict__ cols, const float* __restrict__ val,
                                                  const float* __restrict__ dinv, const float* __restrict__ b,
                                                  float* __restrict__ x, float* __restrict__ r)
 {
     if (stop && *stop) return;
-    amg_pre_rows(n, rs, cols, val, dinv, b, x, r, blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup,
-                 gridDim.x * (TPB / kGroup));
+    amg_pre_rows<G>(n, rs, cols, val, dinv, b, x, r, blockIdx.x * (TPB / G) + threadIdx.x / G, gridDim.x * (TPB / G));
 }
 
-/// the residual summed over each aggregate (a group of lanes per aggregate):
-/// the next level's right-hand side
+/// the residual summed over each aggregate (a group of G lanes per
+/// aggregate): the next level's right-hand side
+template <int G>
 __device__ __forceinline__ void amg_restrict_rows(int nc, const int* __restrict__ ms, const int* __restrict__ mem,
                                                   const float* __restrict__ r, float* __restrict__ bc, int first,
                                                   int stride)
 {
-    const int l = threadIdx.x % kGroup;
+    const int l = threadIdx.x % G;
     for (int I0 = first;; I0 += stride)
     {
-        const int base = I0 - (threadIdx.x % 32) / kGroup;
+        const int base = I0 - (threadIdx.x % 32) / G;
         if (base >= nc) break;
         const int I = I0 < nc ? I0 : -1;
-        const float s = group_members<kGroup>(ms, mem, r, I, l);
+        const float s = group_members<G>(ms, mem, r, I, l);
         if (I >= 0 && l == 0) bc[I] = s;
     }
 }
 
+template <int G>
 __global__ void __launch_bounds__(TPB) k_amg_restrict(const int* __restrict__ stop, int nc, const int* __restrict__ ms,
                                                       const int* __restrict__ mem, const float* __restrict__ r,
                                                       float* __restrict__ bc)
 {
     if (stop && *stop) return;
-    amg_restrict_rows(nc, ms, mem, r, bc, blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup,
-                      gridDim.x * (TPB / kGroup));
+    amg_restrict_rows<G>(nc, ms, mem, r, bc, blockIdx.x * (TPB / G) + threadIdx.x / G, gridDim.x * (TPB / G));
 }
 
 /// the coarse correction brought to this level: y = x + s P xc
@@ -306,31 +325,33 @@ __global__ void __launch_bounds__(TPB) k_amg_post0(const int* __restrict__ stop,
     }
 }
 
-/// coarse level, the same on CSR: xo = y + w D^-1 (b - A y)
+/// coarse level, the same on CSR: xo = y + w D^-1 (b - A y), a group of G
+/// lanes per row
+template <int G>
 __device__ __forceinline__ void amg_post_rows(int n, const int* __restrict__ rs, const int* __restrict__ cols,
                                               const float* __restrict__ val, const float* __restrict__ dinv,
                                               const float* __restrict__ b, const float* __restrict__ y,
                                               float* __restrict__ xo, int first, int stride)
 {
-    const int l = threadIdx.x % kGroup;
+    const int l = threadIdx.x % G;
     for (int i0 = first;; i0 += stride)
     {
-        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        const int base = i0 - (threadIdx.x % 32) / G;
         if (base >= n) break;
         const int i = i0 < n ? i0 : -1;
-        const float s = group_row<kGroup>(rs, cols, val, i, l, [&](int j) { return __ldg(y + j); });
+        const float s = group_row<G>(rs, cols, val, i, l, [&](int j) { return __ldg(y + j); });
         if (i >= 0 && l == 0) xo[i] = y[i] + kOmega * dinv[i] * (b[i] - s);
     }
 }
 
+template <int G>
 __global__ void __launch_bounds__(TPB) k_amg_post(const int* __restrict__ stop, int n, const int* __restrict__ rs,
                                                   const int* __restrict__ cols, const float* __restrict__ val,
                                                   const float* __restrict__ dinv, const float* __restrict__ b,
                                                   const float* __restrict__ y, float* __restrict__ xo)
 {
     if (stop && *stop) return;
-    amg_post_rows(n, rs, cols, val, dinv, b, y, xo, blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup,
-                  gridDim.x * (TPB / kGroup));
+    amg_post_rows<G>(n, rs, cols, val, dinv, b, y, xo, blockIdx.x * (TPB / G) + threadIdx.x / G, gridDim.x * (TPB / G));
 }
 
 /// The last aggregation level (at most kTailMax rows) and the coarsest
@@ -359,9 +380,9 @@ __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict
     float *b = T.b + q * n, *x = T.x + q * n, *r = T.r + q * n, *y = T.y + q * n, *xo = T.xo + q * n;
     float *bc = T.bc + q * nc, *xc = T.xc + q * nc;
     const int first = threadIdx.x / kGroup, stride = kTailThreads / kGroup;
-    amg_pre_rows(n, T.rs, T.cols, T.val, T.dinv, b, x, r, first, stride);
+    amg_pre_rows<kGroup>(n, T.rs, T.cols, T.val, T.dinv, b, x, r, first, stride);
     __syncthreads();
-    amg_restrict_rows(nc, T.ms, T.mem, r, bc, first, stride);
+    amg_restrict_rows<kGroup>(nc, T.ms, T.mem, r, bc, first, stride);
     __syncthreads();
     // the coarsest solve xc = M bc: a warp per row, its lanes over the
     // columns (coalesced reads of the inverse), then a shuffle tree
@@ -379,7 +400,7 @@ __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += kTailThreads) y[i] = x[i] + kScale * xc[T.agg[i]];
     __syncthreads();
-    amg_post_rows(n, T.rs, T.cols, T.val, T.dinv, b, y, xo, first, stride);
+    amg_post_rows<kGroup>(n, T.rs, T.cols, T.val, T.dinv, b, y, xo, first, stride);
 }
 
 /// Shared-memory layout of k_amg_tail_smem (4-byte words): the level's CSR
@@ -688,7 +709,7 @@ __global__ void __launch_bounds__(TPB, (W > 0 && W <= 8) ? 6 : 1) k_amgv_pre0(co
 /// level's right-hand side.  Into a level above the last one it also stores
 /// that level's first sweep w D^-1 b, which the level's residual pass
 /// gathers; into the last level it writes component q at offset q * nc.
-template <bool kLast>
+template <bool kLast, int G>
 __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ done, int nc, const int* __restrict__ ms,
                                                        const int* __restrict__ mem, const float4* __restrict__ r,
                                                        const float* __restrict__ dinvc, float4* __restrict__ bc,
@@ -696,16 +717,16 @@ __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ d
 {
     const Active3 act = active3(done);
     if (act.none()) return;
-    const int l = threadIdx.x % kGroup;
-    const int stride = gridDim.x * (TPB / kGroup);
-    for (int I0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; I0 += stride)
+    const int l = threadIdx.x % G;
+    const int stride = gridDim.x * (TPB / G);
+    for (int I0 = blockIdx.x * (TPB / G) + threadIdx.x / G;; I0 += stride)
     {
-        const int base = I0 - (threadIdx.x % 32) / kGroup;
+        const int base = I0 - (threadIdx.x % 32) / G;
         if (base >= nc) break;
         const int I = I0 < nc ? I0 : -1;
         float s[3] = {0.0f, 0.0f, 0.0f};
         if (I >= 0)
-            for (int k = __ldg(ms + I) + l; k < __ldg(ms + I + 1); k += kGroup)
+            for (int k = __ldg(ms + I) + l; k < __ldg(ms + I + 1); k += G)
             {
                 float v[3];
                 unpack3(__ldg(r + __ldg(mem + k)), v);
@@ -715,7 +736,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ d
 #pragma unroll
         for (int q = 0; q < 3; ++q)
 #pragma unroll
-            for (int o = kGroup / 2; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
+            for (int o = G / 2; o > 0; o >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], o);
         if (I < 0 || l != 0) continue;
         if constexpr (kLast)
         {
@@ -737,6 +758,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ d
 
 /// coarse level, the residual of the first sweep: r = b - A x, with x the
 /// sweep the restriction into this level stored
+template <int G>
 __global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, int n, const int* __restrict__ rs,
                                                   const int* __restrict__ cols, const float* __restrict__ val,
                                                   const float4* __restrict__ x, const float4* __restrict__ b,
@@ -744,15 +766,15 @@ __global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, 
 {
     const Active3 act = active3(done);
     if (act.none()) return;
-    const int l = threadIdx.x % kGroup;
-    const int stride = gridDim.x * (TPB / kGroup);
-    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
+    const int l = threadIdx.x % G;
+    const int stride = gridDim.x * (TPB / G);
+    for (int i0 = blockIdx.x * (TPB / G) + threadIdx.x / G;; i0 += stride)
     {
-        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        const int base = i0 - (threadIdx.x % 32) / G;
         if (base >= n) break;
         const int i = i0 < n ? i0 : -1;
         float s[3];
-        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) { unpack3(__ldg(x + j), g); });
+        group_row3<G>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) { unpack3(__ldg(x + j), g); });
         if (i >= 0 && l == 0)
         {
             float bi[3], rv[3];
@@ -793,6 +815,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ do
 }
 
 /// coarse level: xo = y + w D^-1 (b - A y)
+template <int G>
 __global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done, int n, const int* __restrict__ rs,
                                                    const int* __restrict__ cols, const float* __restrict__ val,
                                                    const float* __restrict__ dinv, const float4* __restrict__ b,
@@ -800,15 +823,15 @@ __global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done,
 {
     const Active3 act = active3(done);
     if (act.none()) return;
-    const int l = threadIdx.x % kGroup;
-    const int stride = gridDim.x * (TPB / kGroup);
-    for (int i0 = blockIdx.x * (TPB / kGroup) + threadIdx.x / kGroup;; i0 += stride)
+    const int l = threadIdx.x % G;
+    const int stride = gridDim.x * (TPB / G);
+    for (int i0 = blockIdx.x * (TPB / G) + threadIdx.x / G;; i0 += stride)
     {
-        const int base = i0 - (threadIdx.x % 32) / kGroup;
+        const int base = i0 - (threadIdx.x % 32) / G;
         if (base >= n) break;
         const int i = i0 < n ? i0 : -1;
         float s[3];
-        group_row3<kGroup>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) { unpack3(__ldg(y + j), g); });
+        group_row3<G>(rs, cols, val, i, l, s, [&](int j, float (&g)[3]) { unpack3(__ldg(y + j), g); });
         if (i >= 0 && l == 0)
         {
             const float di = dinv[i];
@@ -999,6 +1022,25 @@ void Ctx::amgSetup()
         L.val = alloc<float>(std::max<size_t>(P.cols.size(), 1));
         a->dense = alloc<float>(static_cast<size_t>(P.n) * P.n);
     }
+    // lane groups: about two entries (or aggregate members) per lane, at
+    // least four lanes, and fewer while the level's rows times the group
+    // would need more than one wave of resident threads
+    {
+        const double resident = static_cast<double>(sms_) * 2048;
+        auto pick = [&](double avg, int count) {
+            int g = 4;
+            while (g < 32 && g < avg / 2.0) g *= 2;
+            while (g > 4 && static_cast<double>(count) * g > resident) g /= 2;
+            return g;
+        };
+        for (size_t l = 0; l + 1 < a->lv.size(); ++l)
+        {
+            AmgLevel& V = a->lv[l];
+            const AmgLevel& N = a->lv[l + 1];
+            V.gAgg = pick(static_cast<double>(V.n) / N.n, N.n);
+            if (l >= 1) V.gRow = pick(static_cast<double>(a->lv[l - 1].nnzNext) / V.n, V.n);
+        }
+    }
     // the tail level's shared-memory copy, when it and the dense inverse fit
     // in one block's opt-in shared memory (set before any stream capture)
     if (const int T = tailLevel(*a); T >= 0)
@@ -1155,8 +1197,8 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
     const int last = T >= 0 ? T : L - 1;  // levels [0, last) run level by level
     const int* stop = st ? &st->done : nullptr;
     auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
-    // a group of kGroup lanes per coarse row or aggregate
-    auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
+    // a group of G lanes per coarse row or aggregate
+    auto ggrid = [&](int n, int G) { return std::max(1, std::min((n + TPB / G - 1) / (TPB / G), sms_ * 8)); };
     const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
     // down
     for (int l = 0; l < last; ++l)
@@ -1170,8 +1212,14 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
                 stop, A, amgVals32_, V.dinv, r, V.x, V.r);
         }
         else
-            k_amg_pre<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
-        k_amg_restrict<<<ggrid(N.n), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
+            withGroup(V.gRow, [&](auto Gc) {
+                constexpr int G = decltype(Gc)::value;
+                k_amg_pre<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
+            });
+        withGroup(V.gAgg, [&](auto Gc) {
+            constexpr int G = decltype(Gc)::value;
+            k_amg_restrict<G><<<ggrid(N.n, G), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
+        });
     }
     if (T >= 0 && a.tailSmem)
         k_amg_tail_smem<<<1, kTailThreads, a.tailSmem, stream_>>>(stop, tailView(a, T, false), a.tailNnz);
@@ -1193,7 +1241,10 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
                 stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
         }
         else
-            k_amg_post<<<ggrid(V.n), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.r, V.xo);
+            withGroup(V.gRow, [&](auto Gc) {
+                constexpr int G = decltype(Gc)::value;
+                k_amg_post<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.r, V.xo);
+            });
     }
     launchCheck("amg_vcycle", amgCycleKernels());
 }
@@ -1210,7 +1261,7 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
     const int last = T >= 0 ? T : L - 1;
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
     auto grid = [&](int n) { return std::max(1, std::min((n + TPB - 1) / TPB, sms_ * 8)); };
-    auto ggrid = [&](int n) { return std::max(1, std::min((n + TPB / kGroup - 1) / (TPB / kGroup), sms_ * 8)); };
+    auto ggrid = [&](int n, int G) { return std::max(1, std::min((n + TPB / G - 1) / (TPB / G), sms_ * 8)); };
     const int Wsel = maxW_ <= 7 ? 7 : (maxW_ <= 16 ? 16 : 0);
     // levels above `last` hold a float4 per row; `last` (the tail level or
     // the dense coarsest) holds component q at q * n
@@ -1227,13 +1278,20 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
             if (mark) mark(0);
         }
         else
-            k_amgv_pre<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, f4(V.x3), f4(V.b3), f4(V.r3));
-        if (l + 1 == last)
-            k_amgv_restrict<true><<<ggrid(N.n), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), nullptr, nullptr,
-                                                                   nullptr, N.b3);
-        else
-            k_amgv_restrict<false><<<ggrid(N.n), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), N.dinv, f4(N.b3),
-                                                                    f4(N.x3), nullptr);
+            withGroup(V.gRow, [&](auto Gc) {
+                constexpr int G = decltype(Gc)::value;
+                k_amgv_pre<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, f4(V.x3), f4(V.b3),
+                                                                  f4(V.r3));
+            });
+        withGroup(V.gAgg, [&](auto Gc) {
+            constexpr int G = decltype(Gc)::value;
+            if (l + 1 == last)
+                k_amgv_restrict<true, G><<<ggrid(N.n, G), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), nullptr,
+                                                                             nullptr, nullptr, N.b3);
+            else
+                k_amgv_restrict<false, G><<<ggrid(N.n, G), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), N.dinv,
+                                                                              f4(N.b3), f4(N.x3), nullptr);
+        });
     }
     if (T >= 0 && a.tailSmem)
         k_amg_tail_smem<<<3, kTailThreads, a.tailSmem, stream_>>>(done, tailView(a, T, true), a.tailNnz);
@@ -1257,8 +1315,11 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
                 done, A, amgVals32_, V.dinv, b, f4(V.r3), z);
         }
         else
-            k_amgv_post<<<ggrid(V.n), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, f4(V.b3), f4(V.r3),
-                                                         f4(V.xo3));
+            withGroup(V.gRow, [&](auto Gc) {
+                constexpr int G = decltype(Gc)::value;
+                k_amgv_post<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, f4(V.b3),
+                                                                   f4(V.r3), f4(V.xo3));
+            });
     }
     launchCheck("amg_vcycle3", amgCycleKernels());
 }
