@@ -96,7 +96,7 @@ namespace
 {
 
 constexpr float kOmega = 0.8f;    // damped Jacobi
-constexpr float kScale = 2.0f;    // coarse-correction scaling
+constexpr float kScale = kAmgScalePressure;  // coarse-correction scaling of the single V-cycle
 constexpr int kDenseMax = 128;
 
 /// One full wave of a grid-stride row kernel of TPB threads: the SMs times
@@ -370,6 +370,7 @@ struct TailLevel
     const float *val, *dinv, *dense;
     float *b, *x, *r, *y, *xo;  // this level's vectors (n per vector)
     float *bc, *xc;             // the coarsest level's (nc per vector)
+    float scale;                // coarse-correction scaling
 };
 
 __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict__ done, TailLevel T)
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += kTailThreads) y[i] = x[i] + kScale * xc[T.agg[i]];
+    for (int i = threadIdx.x; i < n; i += kTailThreads) y[i] = x[i] + T.scale * xc[T.agg[i]];
     __syncthreads();
     amg_post_rows<kGroup>(n, T.rs, T.cols, T.val, T.dinv, b, y, xo, first, stride);
 }
@@ -506,7 +507,7 @@ __global__ void __launch_bounds__(kTailThreads) k_amg_tail_smem(const int* __res
     }
     __syncthreads();
     // prolongation into r (the residual is no longer needed)
-    for (int i = t; i < n; i += kTailThreads) r[i] = x[i] + kScale * xc[agg[i]];
+    for (int i = t; i < n; i += kTailThreads) r[i] = x[i] + T.scale * xc[agg[i]];
     __syncthreads();
     // post-sweep: xo = y + w D^-1 (b - A y)
     float* xo = T.xo + static_cast<size_t>(q) * n;
@@ -792,7 +793,7 @@ template <bool kFromLast>
 __global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ done, int n, int nNext,
                                                       const float4* __restrict__ x, const float4* __restrict__ xc,
                                                       const float* __restrict__ xcLast, const int* __restrict__ agg,
-                                                      float4* __restrict__ y)
+                                                      float4* __restrict__ y, float scale)
 {
     const Active3 act = active3(done);
     if (act.none()) return;
@@ -809,7 +810,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ do
         else
             unpack3(xc[ai], cv);
 #pragma unroll
-        for (int q = 0; q < 3; ++q) yv[q] = xv[q] + kScale * cv[q];
+        for (int q = 0; q < 3; ++q) yv[q] = xv[q] + scale * cv[q];
         y[i] = pack3(yv);
     }
 }
@@ -1162,7 +1163,7 @@ static int tailLevel(const AmgState& a)
 
 /// The tail kernel's view of level T and the coarsest level: the single
 /// vectors (v3 false) or the three-vector ones.
-static TailLevel tailView(const AmgState& a, int T, bool v3)
+static TailLevel tailView(const AmgState& a, int T, bool v3, float scale)
 {
     const AmgLevel& V = a.lv[static_cast<size_t>(T)];
     const AmgLevel& C = a.lv[static_cast<size_t>(T) + 1];
@@ -1184,6 +1185,7 @@ static TailLevel tailView(const AmgState& a, int T, bool v3)
     t.xo = v3 ? V.xo3 : V.xo;
     t.bc = v3 ? C.b3 : C.b;
     t.xc = v3 ? C.x3 : C.x;
+    t.scale = scale;
     return t;
 }
 
@@ -1222,8 +1224,8 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
         });
     }
     if (T >= 0 && a.tailSmem)
-        k_amg_tail_smem<<<1, kTailThreads, a.tailSmem, stream_>>>(stop, tailView(a, T, false), a.tailNnz);
-    else if (T >= 0) k_amg_tail<<<1, kTailThreads, 0, stream_>>>(stop, tailView(a, T, false));
+        k_amg_tail_smem<<<1, kTailThreads, a.tailSmem, stream_>>>(stop, tailView(a, T, false, kScale), a.tailNnz);
+    else if (T >= 0) k_amg_tail<<<1, kTailThreads, 0, stream_>>>(stop, tailView(a, T, false, kScale));
     else k_amg_dense<<<1, kDenseMax, 0, stream_>>>(stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
     // up: each level corrects with the next level's output
     for (int l = last - 1; l >= 0; --l)
@@ -1251,7 +1253,7 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
 
 /// z_q = V-cycle(b_q) for the three components whose done flag is clear
 /// (the BiCGStab's flags; a converged component keeps its old z_q)
-void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int)>& mark)
+void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::function<void(int)>& mark)
 {
     AmgState& a = *amg_;
     if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
@@ -1294,8 +1296,8 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
         });
     }
     if (T >= 0 && a.tailSmem)
-        k_amg_tail_smem<<<3, kTailThreads, a.tailSmem, stream_>>>(done, tailView(a, T, true), a.tailNnz);
-    else if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true));
+        k_amg_tail_smem<<<3, kTailThreads, a.tailSmem, stream_>>>(done, tailView(a, T, true, scale), a.tailNnz);
+    else if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true, scale));
     else k_amg_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
     for (int l = last - 1; l >= 0; --l)
     {
@@ -1303,10 +1305,11 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int
         const AmgLevel& N = a.lv[l + 1];
         if (l + 1 == last)
             k_amgv_prolong<true><<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, f4(V.x3), nullptr,
-                                                                 (l + 1 == L - 1) ? N.x3 : N.xo3, V.agg, f4(V.r3));
+                                                                 (l + 1 == L - 1) ? N.x3 : N.xo3, V.agg, f4(V.r3),
+                                                                 scale);
         else
             k_amgv_prolong<false><<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, f4(V.x3), f4(N.xo3), nullptr, V.agg,
-                                                                  f4(V.r3));
+                                                                  f4(V.r3), scale);
         if (l == 0)
         {
             if (mark) mark(1);

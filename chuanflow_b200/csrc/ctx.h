@@ -261,7 +261,7 @@ private:
     void amgCycle(const double* r, double* z, const double* q, FcgState* st);
     /// mark(0) after the finest pre-sweep, mark(1) before the finest
     /// post-sweep (kernel timing), when given
-    void amgCycle3(CV3P b, V3P z, const int* done, const std::function<void(int)>& mark = {});
+    void amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::function<void(int)>& mark = {});
     void amgVectors3();
     int amgCycleKernels() const;
     void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,

@@ -1627,13 +1627,13 @@ void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, doubl
                 tmark(k, 0);
                 k_bia_p<3><<<GS_, TPB, 0, stream_>>>(n, br_, bp_, bv_, st_);
                 tmark(k, 1);
-                amgCycle3(cv(bp_), bz_, done, ktime_ ? markZ : std::function<void(int)>{});
+                amgCycle3(cv(bp_), bz_, done, kAmgScaleMomentum, ktime_ ? markZ : std::function<void(int)>{});
                 tmark(k, 4);
                 k_bi_spmv1<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
                 tmark(k, 5);
                 k_bia_s<3><<<GS_, TPB, 0, stream_>>>(n, br_, bv_, bs_, st_);
                 tmark(k, 6);
-                amgCycle3(cv(bs_), bsh_, done, ktime_ ? markS : std::function<void(int)>{});
+                amgCycle3(cv(bs_), bsh_, done, kAmgScaleMomentum, ktime_ ? markS : std::function<void(int)>{});
                 tmark(k, 9);
                 k_bia_spmv2<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bs_, bt_, partials_, st_);
                 tmark(k, 10);
@@ -2768,7 +2768,10 @@ void Ctx::poissonAmgApply3(const double* r, double* z, const int32_t done[3])
     for (int q = 0; q < 3; ++q) s0.done[q] = done[q];
     CFG_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     for (int q = 0; q < 3; ++q) toDevCells(bz_.c[q], z + static_cast<size_t>(q) * dm_.nC, 1, 0);
-    amgCycle3(cv(bp_), bz_, reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done)));
+    // the pressure V-cycle's coarse-correction scale, so that each component
+    // equals the single V-cycle's result
+    amgCycle3(cv(bp_), bz_, reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done)),
+              kAmgScalePressure);
     for (int q = 0; q < 3; ++q) fromDevCells(z + static_cast<size_t>(q) * dm_.nC, bz_.c[q], 1, 0);
 }
 
