@@ -212,6 +212,7 @@ __global__ void __launch_bounds__(TPB) k_amg_pre0(const int* __restrict__ stop, 
                                                   const float* __restrict__ dinv, const double* __restrict__ b,
                                                   float* __restrict__ x, float* __restrict__ r)
 {
+    pdl_entry();
     if (stop && *stop) return;
     FOR_ROWS(c, A.n)
     {
@@ -253,6 +254,7 @@ __global__ void __launch_bounds__(TPB) k_amg_pre(const int* __restrict__ stop, i
                                                  const float* __restrict__ dinv, const float* __restrict__ b,
                                                  float* __restrict__ x, float* __restrict__ r)
 {
+    pdl_entry();
     if (stop && *stop) return;
     amg_pre_rows<G>(n, rs, cols, val, dinv, b, x, r, blockIdx.x * (TPB / G) + threadIdx.x / G, gridDim.x * (TPB / G));
 }
@@ -280,6 +282,7 @@ __global__ void __launch_bounds__(TPB) k_amg_restrict(const int* __restrict__ st
                                                       const int* __restrict__ mem, const float* __restrict__ r,
                                                       float* __restrict__ bc)
 {
+    pdl_entry();
     if (stop && *stop) return;
     amg_restrict_rows<G>(nc, ms, mem, r, bc, blockIdx.x * (TPB / G) + threadIdx.x / G, gridDim.x * (TPB / G));
 }
@@ -289,6 +292,7 @@ __global__ void __launch_bounds__(TPB) k_amg_prolong(const int* __restrict__ sto
                                                      const float* __restrict__ xc, const int* __restrict__ agg,
                                                      float* __restrict__ y)
 {
+    pdl_entry();
     if (stop && *stop) return;
     FOR_ROWS(i, n) y[i] = x[i] + kScale * xc[agg[i]];
 }
@@ -302,6 +306,7 @@ __global__ void __launch_bounds__(TPB) k_amg_post0(const int* __restrict__ stop,
                                                    const float* __restrict__ y, double* __restrict__ z,
                                                    const double* __restrict__ q, double* partials, FcgState* st)
 {
+    pdl_entry();
     if (stop && *stop) return;
     const bool dot = q != nullptr;  // inside the FCG iteration
     double zq[1] = {0.0};
@@ -350,6 +355,7 @@ __global__ void __launch_bounds__(TPB) k_amg_post(const int* __restrict__ stop, 
                                                   const float* __restrict__ dinv, const float* __restrict__ b,
                                                   const float* __restrict__ y, float* __restrict__ xo)
 {
+    pdl_entry();
     if (stop && *stop) return;
     amg_post_rows<G>(n, rs, cols, val, dinv, b, y, xo, blockIdx.x * (TPB / G) + threadIdx.x / G, gridDim.x * (TPB / G));
 }
@@ -375,6 +381,7 @@ struct TailLevel
 
 __global__ void __launch_bounds__(kTailThreads) k_amg_tail(const int* __restrict__ done, TailLevel T)
 {
+    pdl_entry();
     const int q = blockIdx.x;
     if (done && done[q]) return;
     const int n = T.n, nc = T.nc;
@@ -423,6 +430,7 @@ __host__ __device__ constexpr size_t tailSmemWords(int n, int nnz, int nc)
 /// only the output xo goes back to global memory.
 __global__ void __launch_bounds__(kTailThreads) k_amg_tail_smem(const int* __restrict__ done, TailLevel T, int nnz)
 {
+    pdl_entry();
     const int q = blockIdx.x;
     if (done && done[q]) return;
     extern __shared__ __align__(16) int tsm[];
@@ -531,6 +539,7 @@ __global__ void __launch_bounds__(kDenseMax) k_amg_dense(const int* __restrict__
                                                          const float* __restrict__ m, const float* __restrict__ b,
                                                          float* __restrict__ x)
 {
+    pdl_entry();
     const int q = blockIdx.x;
     if (done && done[q]) return;
     const int i = threadIdx.x;
@@ -680,6 +689,7 @@ __global__ void __launch_bounds__(TPB, (W > 0 && W <= 8) ? 6 : 1) k_amgv_pre0(co
                                                    const float* __restrict__ dinv, CV3P b, float4* __restrict__ x,
                                                    float4* __restrict__ r)
 {
+    pdl_entry();
     const Active3 act = active3(done);
     if (act.none()) return;
     const int n = A.n;
@@ -716,6 +726,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_restrict(const int* __restrict__ d
                                                        const float* __restrict__ dinvc, float4* __restrict__ bc,
                                                        float4* __restrict__ xc, float* __restrict__ bcLast)
 {
+    pdl_entry();
     const Active3 act = active3(done);
     if (act.none()) return;
     const int l = threadIdx.x % G;
@@ -765,6 +776,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_pre(const int* __restrict__ done, 
                                                   const float4* __restrict__ x, const float4* __restrict__ b,
                                                   float4* __restrict__ r)
 {
+    pdl_entry();
     const Active3 act = active3(done);
     if (act.none()) return;
     const int l = threadIdx.x % G;
@@ -795,6 +807,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_prolong(const int* __restrict__ do
                                                       const float* __restrict__ xcLast, const int* __restrict__ agg,
                                                       float4* __restrict__ y, float scale)
 {
+    pdl_entry();
     const Active3 act = active3(done);
     if (act.none()) return;
     FOR_ROWS(i, n)
@@ -822,6 +835,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_post(const int* __restrict__ done,
                                                    const float* __restrict__ dinv, const float4* __restrict__ b,
                                                    const float4* __restrict__ y, float4* __restrict__ xo)
 {
+    pdl_entry();
     const Active3 act = active3(done);
     if (act.none()) return;
     const int l = threadIdx.x % G;
@@ -852,6 +866,7 @@ __global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done
                                                     const float* __restrict__ dinv, CV3P b, const float4* __restrict__ y,
                                                     V3P z)
 {
+    pdl_entry();
     const Active3 act = active3(done);
     if (act.none()) return;
     const int n = A.n;
@@ -1210,42 +1225,42 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
         if (l == 0)
         {
             const auto pre0 = Wsel == 7 ? k_amg_pre0<7> : (Wsel == 16 ? k_amg_pre0<16> : k_amg_pre0<0>);
-            pre0<<<waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_>>>(
+            launchK(pdl_, pre0, waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_,
                 stop, A, amgVals32_, V.dinv, r, V.x, V.r);
         }
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
-                k_amg_pre<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
+                launchK(pdl_, k_amg_pre<G>, ggrid(V.n, G), TPB, 0, stream_, stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.x, V.r);
             });
         withGroup(V.gAgg, [&](auto Gc) {
             constexpr int G = decltype(Gc)::value;
-            k_amg_restrict<G><<<ggrid(N.n, G), TPB, 0, stream_>>>(stop, N.n, V.ms, V.mem, V.r, N.b);
+            launchK(pdl_, k_amg_restrict<G>, ggrid(N.n, G), TPB, 0, stream_, stop, N.n, V.ms, V.mem, V.r, N.b);
         });
     }
     if (T >= 0 && a.tailSmem)
-        k_amg_tail_smem<<<1, kTailThreads, a.tailSmem, stream_>>>(stop, tailView(a, T, false, kScale), a.tailNnz);
-    else if (T >= 0) k_amg_tail<<<1, kTailThreads, 0, stream_>>>(stop, tailView(a, T, false, kScale));
-    else k_amg_dense<<<1, kDenseMax, 0, stream_>>>(stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
+        launchK(pdl_, k_amg_tail_smem, 1, kTailThreads, a.tailSmem, stream_, stop, tailView(a, T, false, kScale), a.tailNnz);
+    else if (T >= 0) launchK(pdl_, k_amg_tail, 1, kTailThreads, 0, stream_, stop, tailView(a, T, false, kScale));
+    else launchK(pdl_, k_amg_dense, 1, kDenseMax, 0, stream_, stop, a.nc, a.dense, a.lv[L - 1].b, a.lv[L - 1].x);
     // up: each level corrects with the next level's output
     for (int l = last - 1; l >= 0; --l)
     {
         AmgLevel& V = a.lv[l];
         const AmgLevel& N = a.lv[l + 1];
         const float* xc = (l + 1 == L - 1) ? N.x : N.xo;
-        k_amg_prolong<<<grid(V.n), TPB, 0, stream_>>>(stop, V.n, V.x, xc, V.agg, V.r);
+        launchK(pdl_, k_amg_prolong, grid(V.n), TPB, 0, stream_, stop, V.n, V.x, xc, V.agg, V.r);
         if (l == 0)
         {
             // one block partial per block: the grid is at most G_ blocks,
             // which partials_ holds
             const auto post0 = Wsel == 7 ? k_amg_post0<7> : (Wsel == 16 ? k_amg_post0<16> : k_amg_post0<0>);
-            post0<<<waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_>>>(
+            launchK(pdl_, post0, waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_,
                 stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
         }
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
-                k_amg_post<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.r, V.xo);
+                launchK(pdl_, k_amg_post<G>, ggrid(V.n, G), TPB, 0, stream_, stop, V.n, V.rs, V.cols, V.val, V.dinv, V.b, V.r, V.xo);
             });
     }
     launchCheck("amg_vcycle", amgCycleKernels());
@@ -1275,52 +1290,52 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::func
         if (l == 0)
         {
             const auto pre0 = Wsel == 7 ? k_amgv_pre0<7> : (Wsel == 16 ? k_amgv_pre0<16> : k_amgv_pre0<0>);
-            pre0<<<waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_>>>(
+            launchK(pdl_, pre0, waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_,
                 done, A, amgVals32_, V.dinv, b, f4(V.x3), f4(V.r3));
             if (mark) mark(0);
         }
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
-                k_amgv_pre<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, f4(V.x3), f4(V.b3),
+                launchK(pdl_, k_amgv_pre<G>, ggrid(V.n, G), TPB, 0, stream_, done, V.n, V.rs, V.cols, V.val, f4(V.x3), f4(V.b3),
                                                                   f4(V.r3));
             });
         withGroup(V.gAgg, [&](auto Gc) {
             constexpr int G = decltype(Gc)::value;
             if (l + 1 == last)
-                k_amgv_restrict<true, G><<<ggrid(N.n, G), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), nullptr,
+                launchK(pdl_, k_amgv_restrict<true, G>, ggrid(N.n, G), TPB, 0, stream_, done, N.n, V.ms, V.mem, f4(V.r3), nullptr,
                                                                              nullptr, nullptr, N.b3);
             else
-                k_amgv_restrict<false, G><<<ggrid(N.n, G), TPB, 0, stream_>>>(done, N.n, V.ms, V.mem, f4(V.r3), N.dinv,
+                launchK(pdl_, k_amgv_restrict<false, G>, ggrid(N.n, G), TPB, 0, stream_, done, N.n, V.ms, V.mem, f4(V.r3), N.dinv,
                                                                               f4(N.b3), f4(N.x3), nullptr);
         });
     }
     if (T >= 0 && a.tailSmem)
-        k_amg_tail_smem<<<3, kTailThreads, a.tailSmem, stream_>>>(done, tailView(a, T, true, scale), a.tailNnz);
-    else if (T >= 0) k_amg_tail<<<3, kTailThreads, 0, stream_>>>(done, tailView(a, T, true, scale));
-    else k_amg_dense<<<3, kDenseMax, 0, stream_>>>(done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
+        launchK(pdl_, k_amg_tail_smem, 3, kTailThreads, a.tailSmem, stream_, done, tailView(a, T, true, scale), a.tailNnz);
+    else if (T >= 0) launchK(pdl_, k_amg_tail, 3, kTailThreads, 0, stream_, done, tailView(a, T, true, scale));
+    else launchK(pdl_, k_amg_dense, 3, kDenseMax, 0, stream_, done, a.nc, a.dense, a.lv[L - 1].b3, a.lv[L - 1].x3);
     for (int l = last - 1; l >= 0; --l)
     {
         AmgLevel& V = a.lv[l];
         const AmgLevel& N = a.lv[l + 1];
         if (l + 1 == last)
-            k_amgv_prolong<true><<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, f4(V.x3), nullptr,
+            launchK(pdl_, k_amgv_prolong<true>, grid(V.n), TPB, 0, stream_, done, V.n, N.n, f4(V.x3), nullptr,
                                                                  (l + 1 == L - 1) ? N.x3 : N.xo3, V.agg, f4(V.r3),
                                                                  scale);
         else
-            k_amgv_prolong<false><<<grid(V.n), TPB, 0, stream_>>>(done, V.n, N.n, f4(V.x3), f4(N.xo3), nullptr, V.agg,
+            launchK(pdl_, k_amgv_prolong<false>, grid(V.n), TPB, 0, stream_, done, V.n, N.n, f4(V.x3), f4(N.xo3), nullptr, V.agg,
                                                                   f4(V.r3), scale);
         if (l == 0)
         {
             if (mark) mark(1);
             const auto post0 = Wsel == 7 ? k_amgv_post0<7> : (Wsel == 16 ? k_amgv_post0<16> : k_amgv_post0<0>);
-            post0<<<waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_>>>(
+            launchK(pdl_, post0, waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_,
                 done, A, amgVals32_, V.dinv, b, f4(V.r3), z);
         }
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
-                k_amgv_post<G><<<ggrid(V.n, G), TPB, 0, stream_>>>(done, V.n, V.rs, V.cols, V.val, V.dinv, f4(V.b3),
+                launchK(pdl_, k_amgv_post<G>, ggrid(V.n, G), TPB, 0, stream_, done, V.n, V.rs, V.cols, V.val, V.dinv, f4(V.b3),
                                                                    f4(V.r3), f4(V.xo3));
             });
     }
@@ -1420,6 +1435,7 @@ __global__ void __launch_bounds__(TPB) k_fcgd_spmv(DMat A, const double* __restr
                                                    const double* __restrict__ r, double* __restrict__ q,
                                                    double* partials, FcgState* st)
 {
+    pdl_entry();
     if (st->done) return;
     double s[2] = {0.0, 0.0};
     const double* xs[1] = {p};
@@ -1459,6 +1475,7 @@ __global__ void __launch_bounds__(TPB) k_fcgd_update(int n, const double* __rest
                                                      double* __restrict__ x, double* __restrict__ r, double* partials,
                                                      FcgState* st)
 {
+    pdl_entry();
     if (st->done) return;
     const bool inf = st->normType == 0;
     const double al = st->alpha;
@@ -1498,6 +1515,7 @@ __global__ void __launch_bounds__(TPB) k_fcgd_update(int n, const double* __rest
 __global__ void __launch_bounds__(TPB) k_fcgd_p(int n, const double* __restrict__ z, double* __restrict__ p,
                                                 const FcgState* st, int first)
 {
+    pdl_entry();
     if (st->done) return;
     const double be = first ? 0.0 : st->beta;
     FOR_ROWS(c, n) p[c] = first ? z[c] : z[c] + be * p[c];
@@ -1540,15 +1558,15 @@ void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int
     else spmvInit(std::integral_constant<int, 0>{});
     launchCheck("fcgd_init");
     amgCycle(r, z, nullptr, a.st);
-    k_fcgd_p<<<GS_, TPB, 0, stream_>>>(n, z, p, a.st, 1);
+    launchK(pdl_, k_fcgd_p, GS_, TPB, 0, stream_, n, z, p, a.st, 1);
     launchCheck("fcgd_p0");
     const auto spmv = Wsel == 7 ? k_fcgd_spmv<7> : (Wsel == 16 ? k_fcgd_spmv<16> : k_fcgd_spmv<0>);
     const int spmvGrid = waveGrid(reinterpret_cast<const void*>(spmv), sms_, n);
     auto iteration = [&]() {
-        spmv<<<spmvGrid, TPB, 0, stream_>>>(A, vals, p, r, q, partials_, a.st);
-        k_fcgd_update<<<GS_, TPB, 0, stream_>>>(n, p, q, x, r, partials_, a.st);
+        launchK(pdl_, spmv, spmvGrid, TPB, 0, stream_, A, vals, p, r, q, partials_, a.st);
+        launchK(pdl_, k_fcgd_update, GS_, TPB, 0, stream_, n, p, q, x, r, partials_, a.st);
         amgCycle(r, z, q, a.st);
-        k_fcgd_p<<<GS_, TPB, 0, stream_>>>(n, z, p, a.st, 0);
+        launchK(pdl_, k_fcgd_p, GS_, TPB, 0, stream_, n, z, p, a.st, 0);
         launchCheck("fcgd_iter", 3);
     };
     for (int launched = 0, chunk = 8;;)

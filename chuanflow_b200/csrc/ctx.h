@@ -382,6 +382,13 @@ private:
     int64_t launches_ = 0;
     bool ktime_ = false;
     bool useGraphs_ = true;
+    // CHUANFLOW_PDL=1: the host-driven solver loops (AMG V-cycles, the AMG
+    // flexible CG, the AMG-preconditioned BiCGStab) launch their kernels as
+    // programmatic dependents of the kernel before.  Off by default: on the
+    // 2M-cell channel it shortened the eagerly launched V-cycle's coarse part
+    // (108.6 -> 94.7 us) but lengthened the graph-replayed outer iteration
+    // (265.5 -> 269.9 ms), with the same results
+    bool pdl_ = false;
     std::map<std::string, cudaGraphExec_t> graphs_;
     static constexpr int kEvPerIter = 12;  // events per solver iteration of a chunk (timed segments + 1)
     std::vector<cudaEvent_t> kev_;

@@ -3,8 +3,43 @@
 
 #include "dev_types.h"
 
+#include <utility>
+
 namespace cfg
 {
+
+/// Entry of a kernel that may be launched as a programmatic dependent of
+/// the kernel before it in the stream (launchK with pdl): first let the
+/// kernel after this one launch, then wait until the kernel before this one
+/// has completed and its writes are visible.  Nothing of this kernel reads
+/// or writes global memory before the wait, so the order of memory effects
+/// is that of plain stream order; what overlaps is the launch and block
+/// scheduling of one kernel with the tail of the one before.  Both
+/// instructions are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_entry()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+/// Launches kernel k on stream s; with pdl, as a programmatic dependent of
+/// the kernel before it, which requires k to begin with pdl_entry().
+template <class... KArgs, class... Args>
+inline void launchK(bool pdl, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                    Args&&... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    CFG_CUDA(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+}
 
 __device__ __forceinline__ double warp_sum(double v)
 {

@@ -648,6 +648,7 @@ void Ctx::buildDevice()
     G_ = std::max(1, std::min((nC + TPB - 1) / TPB, sms * 8));
     sms_ = sms;
     if (const char* e = std::getenv("CHUANFLOW_ROW_BLOCKS_PER_SM")) rowBlocksPerSM_ = std::max(0, std::atoi(e));
+    if (const char* e = std::getenv("CHUANFLOW_PDL")) pdl_ = std::atoi(e) != 0;
     GS_ = rowGrid(nC);
     initRowBlocks_ = rowBlocksPerSM_;
     initGS_ = GS_;
@@ -1625,19 +1626,19 @@ void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, doubl
                 const std::function<void(int)> markZ = [&](int j) { tmark(k, 2 + j); };
                 const std::function<void(int)> markS = [&](int j) { tmark(k, 7 + j); };
                 tmark(k, 0);
-                k_bia_p<3><<<GS_, TPB, 0, stream_>>>(n, br_, bp_, bv_, st_);
+                launchK(pdl_, k_bia_p<3>, GS_, TPB, 0, stream_, n, br_, bp_, bv_, st_);
                 tmark(k, 1);
                 amgCycle3(cv(bp_), bz_, done, kAmgScaleMomentum, ktime_ ? markZ : std::function<void(int)>{});
                 tmark(k, 4);
-                k_bi_spmv1<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bz_, bv_, br0_, partials_, st_);
+                launchK(pdl_, k_bi_spmv1<W, 3>, GS_, TPB, 0, stream_, A, vals, bz_, bv_, br0_, partials_, st_);
                 tmark(k, 5);
-                k_bia_s<3><<<GS_, TPB, 0, stream_>>>(n, br_, bv_, bs_, st_);
+                launchK(pdl_, k_bia_s<3>, GS_, TPB, 0, stream_, n, br_, bv_, bs_, st_);
                 tmark(k, 6);
                 amgCycle3(cv(bs_), bsh_, done, kAmgScaleMomentum, ktime_ ? markS : std::function<void(int)>{});
                 tmark(k, 9);
-                k_bia_spmv2<W, 3><<<GS_, TPB, 0, stream_>>>(A, vals, bsh_, bs_, bt_, partials_, st_);
+                launchK(pdl_, k_bia_spmv2<W, 3>, GS_, TPB, 0, stream_, A, vals, bsh_, bs_, bt_, partials_, st_);
                 tmark(k, 10);
-                k_bia_x<3><<<GS_, TPB, 0, stream_>>>(n, x, bz_, bs_, bsh_, bt_, br_, br0_, partials_, st_);
+                launchK(pdl_, k_bia_x<3>, GS_, TPB, 0, stream_, n, x, bz_, bs_, bsh_, bt_, br_, br0_, partials_, st_);
                 tmark(k, 11);
                 launchCheck("bicga_iter", 0);
             });

@@ -392,6 +392,7 @@ template <int W, int NC>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_spmv1(DMat A, const double* __restrict__ val, V3P z, V3P v, V3P r0,
                                                   double* partials, SolveState* st)
 {
+    pdl_entry();
     if (st->allDone) return;
     double sm[NC];
 #pragma unroll
@@ -650,6 +651,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bi_x(int n, const dou
 template <int NC>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_p(int n, V3P r, V3P p, V3P v, const SolveState* st)
 {
+    pdl_entry();
     if (st->allDone) return;
     double beta[NC], om[NC];
     int dn[NC];
@@ -681,6 +683,7 @@ __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_p(int n, V3P r, V
 template <int NC>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_s(int n, V3P r, V3P v, V3P s, const SolveState* st)
 {
+    pdl_entry();
     if (st->allDone) return;
     double al[NC];
     int dn[NC];
@@ -711,6 +714,7 @@ template <int W, int NC>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_spmv2(DMat A, const double* __restrict__ val, V3P sh,
                                                                      V3P s, V3P t, double* partials, SolveState* st)
 {
+    pdl_entry();
     if (st->allDone) return;
     double sm[2 * NC];
 #pragma unroll
@@ -741,6 +745,7 @@ template <int NC>
 __global__ void __launch_bounds__(TPB, kSolverMinBlocks) k_bia_x(int n, V3P x, V3P z, V3P s, V3P sh, V3P t, V3P r,
                                                                  V3P r0, double* partials, SolveState* st)
 {
+    pdl_entry();
     if (st->allDone && !(st->special[0] | st->special[1] | st->special[2])) return;
     double om[NC], al[NC];
     int dn[NC], sp[NC];
