@@ -127,7 +127,11 @@ KERNEL_NAMES = {
 # DRAM bytes (read + write) per launch from one full-set ncu capture of
 # k_bi_spmv2 on the 2M-cell channel (launches 21-22 of its third outer
 # iteration: 334.2 and 333.3 MB)
-MEASURED_TRAFFIC = {"bi_spmv2": 334.2e6}
+# DRAM bytes (read + write) per launch from one ncu capture of this
+# workload (profiles/), with what that launch carried
+MEASURED_TRAFFIC = {"bi_spmv2": (334.2e6, "all three components; profiles/k_bi_spmv2_channel2M_full.md"),
+                    "amgv_pre0": (219.3e6, "a launch with two of three components iterating (algorithmic 192.7 MB); "
+                                           "profiles/k_amgv_pre0_channel2M_full.md")}
 
 
 def kernel_bytes(N, F, s=8, i=4):
@@ -1058,9 +1062,10 @@ def main_simple(args, world, rank, local, dist):
     kt = kernels[top]
     # DRAM bytes per launch of the top kernel from one ncu capture of this
     # workload (profiles/), null for a kernel without one
-    traffic = MEASURED_TRAFFIC.get(top) if n == CELLS else None
+    traffic, traffic_note = MEASURED_TRAFFIC.get(top, (None, None)) if n == CELLS else (None, None)
     roof = {"kernel": KERNEL_NAMES[top], "bound": "hbm", "achieved": kt["achieved_gbs"], "peak": peak,
             "unit": "GB/s", "frac": kt["achieved_gbs"] / peak, "peak_source": peak_src, "traffic": traffic,
+            "traffic_note": traffic_note,
             "algorithmic_bytes_per_launch": kt["alg_bytes"], "launches_timed": kt["launches"],
             "avg_launch_us": kt["avg_us"], "timing": "CUDA events around each launch over one outer iteration "
                                                      "from the timed region's start state",
