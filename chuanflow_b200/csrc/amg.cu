@@ -51,6 +51,11 @@ struct AmgLevel
     // lanes per row of this level's passes (levels >= 1) and per aggregate
     // of its restriction into the next level
     int gRow = 4, gAgg = 4;
+    // a large coarse level's operator also as SELL-32 (one thread per row):
+    // slice starts, columns (-1 on the pads) and values, and per CSR entry
+    // its SELL position; sstart null: the level's passes use lane groups
+    int *sstart = nullptr, *scol = nullptr, *sellPos = nullptr;
+    float* sval = nullptr;
     // work vectors: rhs, first sweep, residual, output
     float *b = nullptr, *x = nullptr, *r = nullptr, *xo = nullptr;
     // the same for the three-component V-cycle (a float4 per row above the
@@ -98,6 +103,9 @@ namespace
 constexpr float kOmega = 0.8f;    // damped Jacobi
 constexpr float kScale = kAmgScalePressure;  // coarse-correction scaling of the single V-cycle
 constexpr int kDenseMax = 128;
+// coarse levels of at least this many rows keep a SELL-32 copy of their
+// operator: one thread per row fills the GPU in one wave there
+constexpr int kSellMinRows = 32768;
 
 /// One full wave of a grid-stride row kernel of TPB threads: the SMs times
 /// the blocks of this kernel one SM holds at once (its registers decide),
@@ -884,6 +892,133 @@ __global__ void __launch_bounds__(TPB) k_amgv_post0(const int* __restrict__ done
     }
 }
 
+// ---- large coarse levels in SELL-32, one thread per row: the same
+// arithmetic as the lane-group passes, each row summed in its CSR column
+// order (the single and the three-vector V-cycle alike)
+
+/// a coarse level's CSR values into its SELL-32 copy (the pads stay 0)
+__global__ void __launch_bounds__(TPB) k_amg_to_sell(int nnz, const int* __restrict__ pos, const float* __restrict__ val,
+                                                     float* __restrict__ sval)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += gridDim.x * blockDim.x) sval[pos[e]] = val[e];
+}
+
+/// row i of a SELL-32 operator: sum over its entries, slot by slot, of
+/// val * f(col) for NV values per column; columns and values of eight slots
+/// are loaded before their gathers
+template <int NV, class F>
+__device__ __forceinline__ void sell32_row(const int* __restrict__ sstart, const int* __restrict__ scol,
+                                           const float* __restrict__ sval, int i, float (&s)[NV], F f)
+{
+    const int e0 = __ldg(sstart + (i >> 5)) + (i & 31), e1 = __ldg(sstart + (i >> 5) + 1);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) s[q] = 0.0f;
+    for (int eb = e0; eb < e1; eb += 32 * 8)
+    {
+        int col[8];
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            const int e = eb + 32 * k;
+            col[k] = e < e1 ? __ldg(scol + e) : -1;
+            v[k] = e < e1 ? __ldg(sval + e) : 0.0f;
+        }
+        float g[8][NV];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            if (col[k] >= 0) f(col[k], g[k]);
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < NV; ++q) g[k][q] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+            for (int q = 0; q < NV; ++q) s[q] += v[k] * g[k][q];
+    }
+}
+
+/// single vector: x = w D^-1 b, r = b - A x
+__global__ void __launch_bounds__(TPB) k_amg_pre_sell(const int* __restrict__ stop, int n, const int* __restrict__ sstart,
+                                                      const int* __restrict__ scol, const float* __restrict__ sval,
+                                                      const float* __restrict__ dinv, const float* __restrict__ b,
+                                                      float* __restrict__ x, float* __restrict__ r)
+{
+    pdl_entry();
+    if (stop && *stop) return;
+    FOR_ROWS(i, n)
+    {
+        float s[1];
+        sell32_row<1>(sstart, scol, sval, i, s,
+                      [&](int j, float (&g)[1]) { g[0] = kOmega * __ldg(dinv + j) * __ldg(b + j); });
+        const float bi = b[i];
+        x[i] = kOmega * dinv[i] * bi;
+        r[i] = bi - s[0];
+    }
+}
+
+/// single vector: xo = y + w D^-1 (b - A y)
+__global__ void __launch_bounds__(TPB) k_amg_post_sell(const int* __restrict__ stop, int n, const int* __restrict__ sstart,
+                                                       const int* __restrict__ scol, const float* __restrict__ sval,
+                                                       const float* __restrict__ dinv, const float* __restrict__ b,
+                                                       const float* __restrict__ y, float* __restrict__ xo)
+{
+    pdl_entry();
+    if (stop && *stop) return;
+    FOR_ROWS(i, n)
+    {
+        float s[1];
+        sell32_row<1>(sstart, scol, sval, i, s, [&](int j, float (&g)[1]) { g[0] = __ldg(y + j); });
+        xo[i] = y[i] + kOmega * dinv[i] * (b[i] - s[0]);
+    }
+}
+
+/// three vectors: r = b - A x, x the sweep the restriction stored
+__global__ void __launch_bounds__(TPB) k_amgv_pre_sell(const int* __restrict__ done, int n, const int* __restrict__ sstart,
+                                                       const int* __restrict__ scol, const float* __restrict__ sval,
+                                                       const float4* __restrict__ x, const float4* __restrict__ b,
+                                                       float4* __restrict__ r)
+{
+    pdl_entry();
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    FOR_ROWS(i, n)
+    {
+        float s[3], bi[3], rv[3];
+        sell32_row<3>(sstart, scol, sval, i, s, [&](int j, float (&g)[3]) { unpack3(__ldg(x + j), g); });
+        unpack3(b[i], bi);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) rv[q] = bi[q] - s[q];
+        r[i] = pack3(rv);
+    }
+}
+
+/// three vectors: xo = y + w D^-1 (b - A y)
+__global__ void __launch_bounds__(TPB) k_amgv_post_sell(const int* __restrict__ done, int n, const int* __restrict__ sstart,
+                                                        const int* __restrict__ scol, const float* __restrict__ sval,
+                                                        const float* __restrict__ dinv, const float4* __restrict__ b,
+                                                        const float4* __restrict__ y, float4* __restrict__ xo)
+{
+    pdl_entry();
+    const Active3 act = active3(done);
+    if (act.none()) return;
+    FOR_ROWS(i, n)
+    {
+        float s[3], bi[3], yi[3], xv[3];
+        sell32_row<3>(sstart, scol, sval, i, s, [&](int j, float (&g)[3]) { unpack3(__ldg(y + j), g); });
+        const float di = dinv[i];
+        unpack3(b[i], bi);
+        unpack3(y[i], yi);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) xv[q] = yi[q] + kOmega * di * (bi[q] - s[q]);
+        xo[i] = pack3(xv);
+    }
+}
+
 /// a host CSR pattern whose entries remember where their values live
 struct Pattern
 {
@@ -1023,6 +1158,32 @@ void Ctx::amgSetup()
             L.cols = upload(P.cols);
             L.dpos = upload(dpos);
             L.val = alloc<float>(P.cols.size());
+            if (P.n >= kSellMinRows)
+            {
+                // SELL-32: slice s holds rows 32s..32s+31, entry k of row r at
+                // start[s] + (r & 31) + 32 k, slices as wide as their longest row
+                const int nsl = (P.n + 31) / 32;
+                std::vector<int> sst(static_cast<size_t>(nsl) + 1, 0);
+                for (int sl = 0; sl < nsl; ++sl)
+                {
+                    int w = 0;
+                    for (int r = sl * 32; r < std::min(P.n, sl * 32 + 32); ++r) w = std::max(w, P.rs[r + 1] - P.rs[r]);
+                    sst[static_cast<size_t>(sl) + 1] = sst[static_cast<size_t>(sl)] + 32 * w;
+                }
+                std::vector<int> scol(static_cast<size_t>(sst[static_cast<size_t>(nsl)]), -1), pos(P.cols.size());
+                for (int r = 0; r < P.n; ++r)
+                    for (int e = P.rs[r]; e < P.rs[r + 1]; ++e)
+                    {
+                        const int p = sst[static_cast<size_t>(r >> 5)] + (r & 31) + 32 * (e - P.rs[r]);
+                        scol[static_cast<size_t>(p)] = P.cols[e];
+                        pos[static_cast<size_t>(e)] = p;
+                    }
+                L.sstart = upload(sst);
+                L.scol = upload(scol);
+                L.sellPos = upload(pos);
+                L.sval = alloc<float>(std::max<size_t>(scol.size(), 1));
+                CFG_CUDA(cudaMemsetAsync(L.sval, 0, std::max<size_t>(scol.size(), 1) * sizeof(float), stream_));
+            }
         }
         L.dinv = alloc<float>(P.n);
         L.b = alloc<float>(P.n);
@@ -1095,6 +1256,7 @@ void Ctx::amgValues(const double* vals, const double* diag, const float* vals32)
         const int g = std::max(1, std::min((L.nnzNext + TPB - 1) / TPB, sms_ * 8));
         k_amg_galerkin<<<g, TPB, 0, stream_>>>(L.nnzNext, L.gs, L.gl, l == 0 ? vals : nullptr, l == 0 ? nullptr : L.val,
                                                N.val);
+        if (N.sstart) k_amg_to_sell<<<g, TPB, 0, stream_>>>(L.nnzNext, N.sellPos, N.val, N.sval);
         if (l + 2 < a.lv.size())
             k_amg_dinv<<<std::max(1, std::min((N.n + TPB - 1) / TPB, sms_ * 8)), TPB, 0, stream_>>>(N.n, N.dpos, N.val,
                                                                                                 N.dinv);
@@ -1228,6 +1390,9 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
             launchK(pdl_, pre0, waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_,
                 stop, A, amgVals32_, V.dinv, r, V.x, V.r);
         }
+        else if (V.sstart)
+            launchK(pdl_, k_amg_pre_sell, waveGrid(reinterpret_cast<const void*>(k_amg_pre_sell), sms_, V.n), TPB, 0,
+                    stream_, stop, V.n, V.sstart, V.scol, V.sval, V.dinv, V.b, V.x, V.r);
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
@@ -1257,6 +1422,9 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
             launchK(pdl_, post0, waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_,
                 stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
         }
+        else if (V.sstart)
+            launchK(pdl_, k_amg_post_sell, waveGrid(reinterpret_cast<const void*>(k_amg_post_sell), sms_, V.n), TPB, 0,
+                    stream_, stop, V.n, V.sstart, V.scol, V.sval, V.dinv, V.b, V.r, V.xo);
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
@@ -1294,6 +1462,9 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::func
                 done, A, amgVals32_, V.dinv, b, f4(V.x3), f4(V.r3));
             if (mark) mark(0);
         }
+        else if (V.sstart)
+            launchK(pdl_, k_amgv_pre_sell, waveGrid(reinterpret_cast<const void*>(k_amgv_pre_sell), sms_, V.n), TPB, 0,
+                    stream_, done, V.n, V.sstart, V.scol, V.sval, f4(V.x3), f4(V.b3), f4(V.r3));
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
@@ -1332,6 +1503,9 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::func
             launchK(pdl_, post0, waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_,
                 done, A, amgVals32_, V.dinv, b, f4(V.r3), z);
         }
+        else if (V.sstart)
+            launchK(pdl_, k_amgv_post_sell, waveGrid(reinterpret_cast<const void*>(k_amgv_post_sell), sms_, V.n), TPB, 0,
+                    stream_, done, V.n, V.sstart, V.scol, V.sval, V.dinv, f4(V.b3), f4(V.r3), f4(V.xo3));
         else
             withGroup(V.gRow, [&](auto Gc) {
                 constexpr int G = decltype(Gc)::value;
