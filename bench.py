@@ -26,7 +26,10 @@ components by BiCGStab with the momentum matrix's V-cycle (--u-precond; the
 line's `momentum_jacobi` runs the same steps with the reference's Jacobi-
 BiCGStab), the pressure by flexible CG (--p-precond; `variant` runs the
 same steps with FP64 multicolour DIC-PCG, FP64 throughout, whose fields the
-headline's are measured against).  `--workload cavity` times the lid-driven cavity of the same cell
+headline's are measured against).  The pressure hierarchy aggregates by
+strength of connection (--amg-theta 0.25: couplings under a quarter of a
+row's largest are left out, which here are those along the channel); the
+momentum hierarchy aggregates plainly.  `--workload cavity` times the lid-driven cavity of the same cell
 count (128^3, Re 400, relaxation 0.7 / 0.3 / pRelaxStart 5e-4, pressure
 reference cell 0), which the reference cannot run as such: it has no
 reference cell.
@@ -71,6 +74,10 @@ RELAX = {"relax_u": 0.9, "relax_p": 0.03, "p_relax_start": 0.002}
 RE_KEPS = 2e4
 BLOCK_P_RELAX_START = 0.002
 BLOCK_START = 60
+# the pressure AMG hierarchy aggregates by strength of connection: across
+# the channel the cells are 2.5x thinner than along it, so the couplings
+# along it are 0.16x the others and fall under this threshold
+AMG_THETA = 0.25
 METRIC = "SIMPLE cell-iter/s at 2M cells; time to 1e-8 p-residual, learned vs plain PCG"
 REFERENCE_ARM = ("the reference's CPU SIMPLE (its own sources, its Jacobi-PCG pressure and Jacobi-BiCGStab "
                  "momentum) on the same mesh, boundary conditions and settings, one outer iteration from rest as "
@@ -84,8 +91,10 @@ def dims(n):
     return (8 * n, n, n)
 
 
-def workload_config(n, precond="DIC", u_precond="Jacobi"):
-    solve = ("FP64 flexible CG with an FP32 aggregation-AMG V-cycle" if precond == "AMG" else f"{precond}-PCG")
+def workload_config(n, precond="DIC", u_precond="Jacobi", amg_theta=0.0):
+    solve = (("FP64 flexible CG with an FP32 aggregation-AMG V-cycle" +
+              (f" (aggregates by strength of connection, theta {amg_theta})" if amg_theta else " (plain aggregation)"))
+             if precond == "AMG" else f"{precond}-PCG")
     usolve = ("FP64 BiCGStab with the FP32 aggregation-AMG V-cycle of the momentum matrix (3 components per V-cycle)"
               if u_precond == "AMG" else "Jacobi-BiCGStab (the reference's)")
     nx, ny, nz = dims(n)
@@ -225,12 +234,16 @@ def cavity_config(n, precond="DIC"):
             "reference_arm": "none for this workload: the reference has no pressure reference cell"}
 
 
-def make_case(n, device, precond="Jacobi"):
-    """The headline channel on `device`, at rest with its boundary flux."""
+def make_case(n, device, precond="Jacobi", amg_theta=0.0):
+    """The headline channel on `device`, at rest with its boundary flux;
+    amg_theta > 0 aggregates the pressure AMG hierarchy by strength of
+    connection at that threshold."""
     import chuanflow_b200 as cf
     mesh = cf.PolyMesh.block((0, 0, 0), LENGTH, dims(n), {s: (nm, t) for s, nm, t in zip(SIDES, CH_NAMES, CH_TYPES)})
     mesh.jitter_interior(JITTER, SEED)
     case = cf.SimpleCase(mesh, device)
+    if amg_theta:
+        case.amg_strength(amg_theta)
     case.set_patch_bc("U", "inlet", "fixedValue", (U_IN, 0, 0))
     case.set_patch_bc("p", "inlet", "zeroGradient", 0.0)
     case.set_patch_bc("U", "outlet", "zeroGradient", (0, 0, 0))
@@ -474,7 +487,7 @@ def main_reference(args, world, rank, dist):
     out = {"metric": METRIC, "impl": "reference", "value": v, "unit": "cell-iter/s", "n_gpus": args.gpus,
            "steps": steps, "warmup": 0, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": workload_config(n, args.p_precond, args.u_precond),
+           "config": workload_config(n, args.p_precond, args.u_precond, args.amg_theta),
            "cpu_baseline": {"value": v, "unit": "cell-iter/s", "cores": 1, "kind": kind,
                             "sample": f"one SIMPLE outer iteration of the headline channel from rest; {what}; "
                                       f"{cpu_info()}"},
@@ -853,6 +866,8 @@ def main():
     ap.add_argument("--u-precond", default="AMG", choices=["Jacobi", "AMG"],
                     help="simple: the momentum BiCGStab's preconditioner (Jacobi: the reference's; AMG: the FP32 "
                          "V-cycle of the momentum matrix)")
+    ap.add_argument("--amg-theta", type=float, default=AMG_THETA,
+                    help="strength threshold of the pressure AMG aggregation (0: plain aggregation)")
     ap.add_argument("--no-variant", action="store_true",
                     help="simple: skip the second pressure solver's timing from the same start state")
     ap.add_argument("--profile", action="store_true",
@@ -964,9 +979,10 @@ def main_simple(args, world, rank, local, dist):
     if cavity:
         mesh, case, ctl = make_cavity_case(n, local, args.p_precond, p_relax_start=5e-4)
     else:
-        mesh, case, ctl = make_case(n, local, args.p_precond)
+        mesh, case, ctl = make_case(n, local, args.p_precond, args.amg_theta)
     ctl = dataclasses.replace(ctl, u_preconditioner=args.u_precond)
-    config = cavity_config(n, args.p_precond) if cavity else workload_config(n, args.p_precond, args.u_precond)
+    config = (cavity_config(n, args.p_precond) if cavity else
+              workload_config(n, args.p_precond, args.u_precond, args.amg_theta))
     ncell = mesh.n_cells
     if args.profile:
         import torch

@@ -80,6 +80,7 @@ def lib():
         _lib.cfg_version.restype = C.c_char_p
         _lib.cfg_last_error.restype = C.c_size_t
         _lib.cfg_mesh_jitter_interior.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
+        _lib.cfg_amg_strength.argtypes = [C.c_void_p, C.c_double]
         _lib.cfg_mesh_destroy.argtypes = [C.c_void_p]
         _lib.cfg_ctx_destroy.argtypes = [C.c_void_p]
         _lib.cfg_set_patch_bc.argtypes = [C.c_void_p, C.c_char, C.c_int32, C.c_int32, _f64p]
@@ -487,6 +488,11 @@ class SimpleCase:
         nl = int(out[0])
         return {"levels": nl, "rows": [int(v) for v in out[1:1 + min(nl, 8)]], "structure_ms": float(out[9]),
                 "values_ms": float(out[10])}
+
+    def amg_strength(self, theta):
+        """Strength-of-connection threshold of the pressure AMG hierarchy's
+        aggregation (0: plain); set before the first AMG pressure solve."""
+        _check(lib().cfg_amg_strength(self._h, float(theta)))
 
     def poisson_amg_apply(self, r):
         """One V-cycle z = V(r) of that hierarchy (FP32 inside, FP64 in and out)."""

@@ -89,6 +89,8 @@ struct AmgState
     std::vector<int> hrs, hcols;  // coarsest CSR on the host
     bool valuesReady = false;
     double setupMs = 0, valuesMs = 0;
+    double theta = 0;                 // strength threshold of the aggregation (0: plain)
+    const float* vals32 = nullptr;    // the finest operator's FP32 SELL values
     // the tail level in shared memory: the dynamic size (0: it does not
     // fit, k_amg_tail runs from global memory) and the level's entries
     size_t tailSmem = 0;
@@ -1026,25 +1028,30 @@ struct Pattern
     std::vector<int> rs, cols, pos;
 };
 
-/// plain aggregation (the two phases of the file comment)
-int aggregate(const Pattern& A, std::vector<int>& agg)
+/// aggregation (the two phases of the file comment) over the entries that
+/// `link` marks (null: every entry, plain aggregation); a row's own diagonal
+/// entry always counts
+int aggregate(const Pattern& A, std::vector<int>& agg, const std::vector<char>* link = nullptr)
 {
+    auto on = [&](int e) { return !link || (*link)[static_cast<size_t>(e)]; };
     agg.assign(static_cast<size_t>(A.n), -1);
     int na = 0;
     for (int i = 0; i < A.n; ++i)
     {
         if (agg[i] >= 0) continue;
         bool free = true;
-        for (int e = A.rs[i]; e < A.rs[i + 1] && free; ++e) free = agg[A.cols[e]] < 0;
+        for (int e = A.rs[i]; e < A.rs[i + 1] && free; ++e)
+            if (on(e)) free = agg[A.cols[e]] < 0;
         if (!free) continue;
-        for (int e = A.rs[i]; e < A.rs[i + 1]; ++e) agg[A.cols[e]] = na;
+        for (int e = A.rs[i]; e < A.rs[i + 1]; ++e)
+            if (on(e)) agg[A.cols[e]] = na;
         agg[i] = na++;
     }
     for (int i = 0; i < A.n; ++i)
     {
         if (agg[i] >= 0) continue;
         for (int e = A.rs[i]; e < A.rs[i + 1]; ++e)
-            if (agg[A.cols[e]] >= 0 && A.cols[e] != i)
+            if (on(e) && agg[A.cols[e]] >= 0 && A.cols[e] != i)
             {
                 agg[i] = agg[A.cols[e]];
                 break;
@@ -1054,15 +1061,38 @@ int aggregate(const Pattern& A, std::vector<int>& agg)
     return na;
 }
 
+/// The strong entries of a level for strength-of-connection aggregation:
+/// entry (i, j), j != i, is strong when |a_ij| >= theta * max over k != i of
+/// |a_ik| (values indexed by the pattern's positions); diagonal entries are
+/// marked too.  Aggregating over strong entries only lines the aggregates
+/// up with the strongly coupled directions of an anisotropic operator
+/// (cells much thinner across the channel than along it), where plain
+/// aggregation mixes weak and strong couplings and the V-cycle loses its
+/// contraction.
+std::vector<char> strongEntries(const Pattern& A, const std::vector<double>& v, double theta)
+{
+    std::vector<char> link(A.cols.size(), 0);
+    for (int i = 0; i < A.n; ++i)
+    {
+        double mx = 0.0;
+        for (int e = A.rs[i]; e < A.rs[i + 1]; ++e)
+            if (A.cols[e] != i) mx = std::max(mx, std::abs(v[static_cast<size_t>(A.pos[e])]));
+        for (int e = A.rs[i]; e < A.rs[i + 1]; ++e)
+            link[static_cast<size_t>(e)] = A.cols[e] == i || std::abs(v[static_cast<size_t>(A.pos[e])]) >= theta * mx;
+    }
+    return link;
+}
+
 }  // namespace
 
 static int tailLevel(const AmgState& a);
 
 /// The hierarchy's structure from the device pressure pattern.
-void Ctx::amgSetup()
+void Ctx::amgSetup(AmgUse use, const double* vals, double theta)
 {
     const auto t0 = std::chrono::steady_clock::now();
     std::unique_ptr<AmgState> a(new AmgState());
+    a->theta = theta;
     const int n0 = dm_.nC;
     // the finest pattern from the SELL slices, entries in row order
     Pattern P;
@@ -1085,6 +1115,17 @@ void Ctx::amgSetup()
             P.rs[c + 1] = static_cast<int>(P.cols.size());
         }
     }
+    // strength of connection needs the operator's values on every level: the
+    // finest from the device (indexed by SELL position), the coarser ones as
+    // FP64 Galerkin sums on the host, in the order the device sums them
+    std::vector<double> v;
+    if (theta > 0)
+    {
+        if (!vals) fail(CFG_EINVAL, "amg: strength-of-connection aggregation needs the operator's values");
+        v.resize(static_cast<size_t>(nSlicesEntries_));
+        CFG_CUDA(cudaMemcpyAsync(v.data(), vals, v.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CFG_CUDA(cudaStreamSynchronize(stream_));
+    }
     while (true)
     {
         AmgLevel L;
@@ -1101,7 +1142,16 @@ void Ctx::amgSetup()
             break;
         }
         std::vector<int> agg;
-        const int na = aggregate(P, agg);
+        int na = -1;
+        if (theta > 0)
+        {
+            // a level that the strong entries coarsen by less than half is
+            // aggregated plainly instead
+            const std::vector<char> link = strongEntries(P, v, theta);
+            na = aggregate(P, agg, &link);
+            if (na > P.n / 2) na = -1;
+        }
+        if (na < 0) na = aggregate(P, agg);
         if (na > P.n * 9 / 10 || na > 0x3fffffff)
             fail(CFG_ESETUP, "amg: the aggregation stopped coarsening above " + std::to_string(kDenseMax) + " rows");
         // members of each aggregate, in row order
@@ -1142,6 +1192,17 @@ void Ctx::amgSetup()
         }
         C.pos.resize(C.cols.size());
         std::iota(C.pos.begin(), C.pos.end(), 0);
+        if (theta > 0)
+        {
+            std::vector<double> vc(C.cols.size());
+            for (size_t k = 0; k < vc.size(); ++k)
+            {
+                double t = 0.0;
+                for (int g = gs[k]; g < gs[k + 1]; ++g) t += v[static_cast<size_t>(gl[static_cast<size_t>(g)])];
+                vc[k] = t;
+            }
+            v.swap(vc);
+        }
         L.agg = upload(agg);
         L.ms = upload(ms);
         L.mem = upload(mem);
@@ -1228,26 +1289,39 @@ void Ctx::amgSetup()
         CFG_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
         if (bytes <= static_cast<size_t>(optin))
         {
-            CFG_CUDA(cudaFuncSetAttribute(k_amg_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(bytes)));
+            // the attribute belongs to the kernel on this device, which every
+            // hierarchy of every context shares: it only ever grows
+            static std::mutex mu;
+            static std::vector<std::pair<int, size_t>> granted;  // (device, bytes)
+            std::lock_guard<std::mutex> lock(mu);
+            auto it = std::find_if(granted.begin(), granted.end(),
+                                   [&](const std::pair<int, size_t>& g) { return g.first == device_; });
+            if (it == granted.end() || it->second < bytes)
+            {
+                CFG_CUDA(cudaFuncSetAttribute(k_amg_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(bytes)));
+                if (it == granted.end()) granted.push_back({device_, bytes});
+                else it->second = bytes;
+            }
             a->tailSmem = bytes;
             a->tailNnz = nnz;
         }
     }
     CFG_CUDA(cudaStreamSynchronize(stream_));
     a->setupMs = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    amg_.reset(a.release());
+    amgSlot(use).reset(a.release());
 }
 
 /// The hierarchy's values from the finest operator (FP64 SELL values and
 /// diagonal): Galerkin sums level by level, inverse diagonals, and the
 /// coarsest level's dense inverse (on the host).
-void Ctx::amgValues(const double* vals, const double* diag, const float* vals32)
+void Ctx::amgValues(AmgUse use, const double* vals, const double* diag, const float* vals32)
 {
-    if (!amg_) amgSetup();
-    AmgState& a = *amg_;
+    auto& slot = amgSlot(use);
+    if (!slot) amgSetup(use, vals, use == kAmgPressure ? amgTheta_ : 0.0);
+    AmgState& a = *slot;
     const auto t0 = std::chrono::steady_clock::now();
-    amgVals32_ = vals32;
+    a.vals32 = vals32;
     k_amg_dinv0<<<GS_, TPB, 0, stream_>>>(dm_.nC, diag, a.lv[0].dinv);
     for (size_t l = 0; l + 1 < a.lv.size(); ++l)
     {
@@ -1368,6 +1442,7 @@ static TailLevel tailView(const AmgState& a, int T, bool v3, float scale)
 
 void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
 {
+    if (!amg_) fail(CFG_EINVAL, "amg: the hierarchy is not set up (amgValues)");
     AmgState& a = *amg_;
     if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
     const DMat A{dm_.nC, dm_.mStart, dm_.mCol};
@@ -1388,7 +1463,7 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
         {
             const auto pre0 = Wsel == 7 ? k_amg_pre0<7> : (Wsel == 16 ? k_amg_pre0<16> : k_amg_pre0<0>);
             launchK(pdl_, pre0, waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_,
-                stop, A, amgVals32_, V.dinv, r, V.x, V.r);
+                stop, A, a.vals32, V.dinv, r, V.x, V.r);
         }
         else if (V.sstart)
             launchK(pdl_, k_amg_pre_sell, waveGrid(reinterpret_cast<const void*>(k_amg_pre_sell), sms_, V.n), TPB, 0,
@@ -1420,7 +1495,7 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
             // which partials_ holds
             const auto post0 = Wsel == 7 ? k_amg_post0<7> : (Wsel == 16 ? k_amg_post0<16> : k_amg_post0<0>);
             launchK(pdl_, post0, waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_,
-                stop, A, amgVals32_, V.dinv, r, V.r, z, q, partials_, st);
+                stop, A, a.vals32, V.dinv, r, V.r, z, q, partials_, st);
         }
         else if (V.sstart)
             launchK(pdl_, k_amg_post_sell, waveGrid(reinterpret_cast<const void*>(k_amg_post_sell), sms_, V.n), TPB, 0,
@@ -1436,9 +1511,10 @@ void Ctx::amgCycle(const double* r, double* z, const double* q, FcgState* st)
 
 /// z_q = V-cycle(b_q) for the three components whose done flag is clear
 /// (the BiCGStab's flags; a converged component keeps its old z_q)
-void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::function<void(int)>& mark)
+void Ctx::amgCycle3(AmgUse use, CV3P b, V3P z, const int* done, float scale, const std::function<void(int)>& mark)
 {
-    AmgState& a = *amg_;
+    if (!amgSlot(use)) fail(CFG_EINVAL, "amg: the hierarchy is not set up (amgValues)");
+    AmgState& a = *amgSlot(use);
     if (!a.valuesReady) fail(CFG_EINVAL, "amg: values not set up");
     if (!a.lv[0].x3) fail(CFG_EINVAL, "amg: the three-component vectors are not allocated (amgVectors3)");
     const int L = static_cast<int>(a.lv.size());
@@ -1459,7 +1535,7 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::func
         {
             const auto pre0 = Wsel == 7 ? k_amgv_pre0<7> : (Wsel == 16 ? k_amgv_pre0<16> : k_amgv_pre0<0>);
             launchK(pdl_, pre0, waveGrid(reinterpret_cast<const void*>(pre0), sms_, A.n), TPB, 0, stream_,
-                done, A, amgVals32_, V.dinv, b, f4(V.x3), f4(V.r3));
+                done, A, a.vals32, V.dinv, b, f4(V.x3), f4(V.r3));
             if (mark) mark(0);
         }
         else if (V.sstart)
@@ -1501,7 +1577,7 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::func
             if (mark) mark(1);
             const auto post0 = Wsel == 7 ? k_amgv_post0<7> : (Wsel == 16 ? k_amgv_post0<16> : k_amgv_post0<0>);
             launchK(pdl_, post0, waveGrid(reinterpret_cast<const void*>(post0), sms_, A.n), TPB, 0, stream_,
-                done, A, amgVals32_, V.dinv, b, f4(V.r3), z);
+                done, A, a.vals32, V.dinv, b, f4(V.r3), z);
         }
         else if (V.sstart)
             launchK(pdl_, k_amgv_post_sell, waveGrid(reinterpret_cast<const void*>(k_amgv_post_sell), sms_, V.n), TPB, 0,
@@ -1513,15 +1589,24 @@ void Ctx::amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::func
                                                                    f4(V.r3), f4(V.xo3));
             });
     }
-    launchCheck("amg_vcycle3", amgCycleKernels());
+    launchCheck("amg_vcycle3", amgCycleKernels(use));
+}
+
+void Ctx::setAmgStrength(double theta)
+{
+    if (!(theta >= 0.0 && theta <= 1.0)) fail(CFG_EINVAL, "amg strength: theta must lie in [0, 1]");
+    if (amg_ && amg_->theta != theta)
+        fail(CFG_EINVAL, "amg strength: the pressure hierarchy is built already (with theta " +
+                             std::to_string(amg_->theta) + "); set the strength before the first AMG pressure solve");
+    amgTheta_ = theta;
 }
 
 /// The level vectors of the three-component V-cycle, allocated once (before
 /// any stream capture that launches amgCycle3).
-void Ctx::amgVectors3()
+void Ctx::amgVectors3(AmgUse use)
 {
-    if (!amg_) amgSetup();
-    for (auto& V : amg_->lv)
+    if (!amgSlot(use)) fail(CFG_EINVAL, "amg: the hierarchy is not set up (amgValues)");
+    for (auto& V : amgSlot(use)->lv)
         if (!V.x3)
         {
             const size_t m = 4 * static_cast<size_t>(V.n);  // a float4 per row, or three rows of n
@@ -1533,11 +1618,12 @@ void Ctx::amgVectors3()
 }
 
 /// The number of kernels one amgCycle3 launches.
-int Ctx::amgCycleKernels() const
+int Ctx::amgCycleKernels(AmgUse use) const
 {
-    if (!amg_) return 0;
-    const int T = tailLevel(*amg_);
-    const int last = T >= 0 ? T : static_cast<int>(amg_->lv.size()) - 1;
+    const AmgState* a = use == kAmgMomentum ? amgU_.get() : amg_.get();
+    if (!a) return 0;
+    const int T = tailLevel(*a);
+    const int last = T >= 0 ? T : static_cast<int>(a->lv.size()) - 1;
     return 4 * last + 1;
 }
 
@@ -1705,6 +1791,7 @@ __global__ void __launch_bounds__(TPB) k_fcgd_p(int n, const double* __restrict_
 void Ctx::amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,
                  cfg_solver_report* rep)
 {
+    if (!amg_) fail(CFG_EINVAL, "amg: the hierarchy is not set up (amgValues)");
     AmgState& a = *amg_;
     const int n = dm_.nC;
     const DMat A{n, dm_.mStart, dm_.mCol};

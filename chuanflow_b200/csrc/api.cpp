@@ -530,6 +530,14 @@ int cfg_poisson_amg_apply3(cfg_ctx* ctx, const double* r, double* z, const int32
     });
 }
 
+int cfg_amg_strength(cfg_ctx* ctx, double theta)
+{
+    return guard([&] {
+        need(ctx, "cfg_amg_strength: null argument");
+        ctx->c->setAmgStrength(theta);
+    });
+}
+
 int cfg_gradient(cfg_ctx* ctx, const double* data, const double* bvals, int32_t scheme, int32_t volQuirk, double* out)
 {
     return guard([&] {

@@ -234,6 +234,10 @@ public:
     void poissonAmg(double* out);
     void poissonAmgApply(const double* r, double* z);
     void poissonAmgApply3(const double* r, double* z, const int32_t done[3]);
+    /// strength threshold of the pressure hierarchy's aggregation (0: plain);
+    /// fixed once that hierarchy is built
+    void setAmgStrength(double theta);
+    double amgStrength() const { return amgTheta_; }
 
 private:
     void setNu(double nu);
@@ -252,18 +256,24 @@ private:
     std::unique_ptr<DetailState, DetailDeleter> detail_;
     std::unique_ptr<TurbState, TurbDeleter> turb_;
     std::unique_ptr<MpnnState, MpnnDeleter> mpnn_;
-    // aggregation AMG in FP32 (amg.cu)
-    std::unique_ptr<AmgState, AmgDeleter> amg_;
-    const float* amgVals32_ = nullptr;
-    void amgSetup();
-    void amgValues(const double* vals, const double* diag, const float* vals32);
+    // aggregation AMG in FP32 (amg.cu): one hierarchy for the pressure (and
+    // the Poisson system), aggregated by strength of connection when
+    // amgTheta_ > 0, and one for the momentum matrix, aggregated plainly.
+    // Each is built from its operator's pattern (and, for strength, values)
+    // on its first amgValues.
+    enum AmgUse { kAmgPressure = 0, kAmgMomentum = 1 };
+    std::unique_ptr<AmgState, AmgDeleter> amg_, amgU_;
+    std::unique_ptr<AmgState, AmgDeleter>& amgSlot(AmgUse use) { return use == kAmgMomentum ? amgU_ : amg_; }
+    double amgTheta_ = 0.0;
+    void amgSetup(AmgUse use, const double* vals, double theta);
+    void amgValues(AmgUse use, const double* vals, const double* diag, const float* vals32);
     void amgApply(const double* r, double* z);
     void amgCycle(const double* r, double* z, const double* q, FcgState* st);
     /// mark(0) after the finest pre-sweep, mark(1) before the finest
     /// post-sweep (kernel timing), when given
-    void amgCycle3(CV3P b, V3P z, const int* done, float scale, const std::function<void(int)>& mark = {});
-    void amgVectors3();
-    int amgCycleKernels() const;
+    void amgCycle3(AmgUse use, CV3P b, V3P z, const int* done, float scale, const std::function<void(int)>& mark = {});
+    void amgVectors3(AmgUse use);
+    int amgCycleKernels(AmgUse use = kAmgPressure) const;
     void amgFcg(const double* vals, const double* b, double* x, double tol, int maxIter, int normType,
                 cfg_solver_report* rep);
     void amgInfo(double* out);

@@ -1594,7 +1594,7 @@ void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, doubl
     init.nComp = 3;
     const int n = dm_.nC;
     const int* done = reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done));
-    const int vk = amgCycleKernels();
+    const int vk = amgCycleKernels(kAmgMomentum);
     CFG_CUDA(cudaMemcpyAsync(st_, &init, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     auto loop = [&](auto Wc) {
         constexpr int W = decltype(Wc)::value;
@@ -1628,13 +1628,13 @@ void Ctx::runBiCGAmg(const double* vals, const double* diag, V3P b, V3P x, doubl
                 tmark(k, 0);
                 launchK(pdl_, k_bia_p<3>, GS_, TPB, 0, stream_, n, br_, bp_, bv_, st_);
                 tmark(k, 1);
-                amgCycle3(cv(bp_), bz_, done, kAmgScaleMomentum, ktime_ ? markZ : std::function<void(int)>{});
+                amgCycle3(kAmgMomentum, cv(bp_), bz_, done, kAmgScaleMomentum, ktime_ ? markZ : std::function<void(int)>{});
                 tmark(k, 4);
                 launchK(pdl_, k_bi_spmv1<W, 3>, GS_, TPB, 0, stream_, A, vals, bz_, bv_, br0_, partials_, st_);
                 tmark(k, 5);
                 launchK(pdl_, k_bia_s<3>, GS_, TPB, 0, stream_, n, br_, bv_, bs_, st_);
                 tmark(k, 6);
-                amgCycle3(cv(bs_), bsh_, done, kAmgScaleMomentum, ktime_ ? markS : std::function<void(int)>{});
+                amgCycle3(kAmgMomentum, cv(bs_), bsh_, done, kAmgScaleMomentum, ktime_ ? markS : std::function<void(int)>{});
                 tmark(k, 9);
                 launchK(pdl_, k_bia_spmv2<W, 3>, GS_, TPB, 0, stream_, A, vals, bsh_, bs_, bt_, partials_, st_);
                 tmark(k, 10);
@@ -1835,9 +1835,8 @@ void Ctx::solveMomentum(int nonOrth, int gradScheme, double tol, int maxIter, in
                 if (!uVal32_) uVal32_ = alloc<float>(static_cast<size_t>(nE));
                 k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, mVal_, uVal32_);
                 launchCheck("amg_u_float");
-                amgValues(mVal_, uDiag_, uVal32_);
-                amgVectors3();
-                amgFresh_ = false;
+                amgValues(kAmgMomentum, mVal_, uDiag_, uVal32_);
+                amgVectors3(kAmgMomentum);
             }
             runBiCGAmg(mVal_, uDiag_, uRhs_, ux_, tol, maxIter, reps);
         }
@@ -1991,7 +1990,7 @@ void Ctx::solvePressure(int nonOrth, int gradScheme, double tol, int maxIter, in
                 if (!pVal32_) pVal32_ = alloc<float>(static_cast<size_t>(nE));
                 k_to_float<<<std::max(1, std::min((nE + TPB - 1) / TPB, 8192)), TPB, 0, stream_>>>(nE, pVal_d_, pVal32_);
                 launchCheck("amg_float");
-                amgValues(pVal_d_, pDiag_, pVal32_);
+                amgValues(kAmgPressure, pVal_d_, pDiag_, pVal32_);
                 amgFresh_ = false;  // the Poisson system, if any, must refresh its own
             }
             amgFcg(pVal_d_, pRhs_, px_, tol, maxIter, 0, &rep);
@@ -2737,7 +2736,7 @@ void Ctx::poissonAmg(double* out)
 {
     if (!poissonReady_) fail(CFG_EINVAL, "cfg_poisson_amg_setup: call cfg_poisson_setup first");
     CFG_CUDA(cudaSetDevice(device_));
-    amgValues(pVal_d_, pDiag_, pVal32_);
+    amgValues(kAmgPressure, pVal_d_, pDiag_, pVal32_);
     amgFresh_ = true;
     amgInfo(out);
 }
@@ -2764,14 +2763,14 @@ void Ctx::poissonAmgApply3(const double* r, double* z, const int32_t done[3])
     // the three vectors in the momentum solver's p and z buffers, the done
     // flags in the solver state (as the momentum BiCGStab hands them over)
     for (int q = 0; q < 3; ++q) toDevCells(bp_.c[q], r + static_cast<size_t>(q) * dm_.nC, 1, 0);
-    amgVectors3();
+    amgVectors3(kAmgPressure);
     SolveState s0{};
     for (int q = 0; q < 3; ++q) s0.done[q] = done[q];
     CFG_CUDA(cudaMemcpyAsync(st_, &s0, sizeof(SolveState), cudaMemcpyHostToDevice, stream_));
     for (int q = 0; q < 3; ++q) toDevCells(bz_.c[q], z + static_cast<size_t>(q) * dm_.nC, 1, 0);
     // the pressure V-cycle's coarse-correction scale, so that each component
     // equals the single V-cycle's result
-    amgCycle3(cv(bp_), bz_, reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done)),
+    amgCycle3(kAmgPressure, cv(bp_), bz_, reinterpret_cast<const int*>(reinterpret_cast<const char*>(st_) + offsetof(SolveState, done)),
               kAmgScalePressure);
     for (int q = 0; q < 3; ++q) fromDevCells(z + static_cast<size_t>(q) * dm_.nC, bz_.c[q], 1, 0);
 }

@@ -412,6 +412,18 @@ int cfg_poisson_amg_apply(cfg_ctx* ctx, const double* r, double* z);
  * values); component q is skipped, its z left as given, when done[q] != 0.
  * Each applied component equals cfg_poisson_amg_apply of it, for tests. */
 int cfg_poisson_amg_apply3(cfg_ctx* ctx, const double* r, double* z, const int32_t done[3]);
+/* Strength-of-connection aggregation for the pressure AMG hierarchy (the one
+ * the SIMPLE and PISO pressure solves and the Poisson system use; no
+ * counterpart in the reference, whose pressure solve is Jacobi-PCG,
+ * src/common/src/Matrix.cpp:153-222).  With theta > 0 an entry (i, j) joins
+ * the aggregation only when |a_ij| >= theta * max over k != i of |a_ik|, on
+ * every level (coarse values: FP64 Galerkin sums of the operator the
+ * hierarchy is first built for); a level that this coarsens by less than
+ * half is aggregated plainly.  theta 0 (the default) is plain aggregation.
+ * Set it before the first AMG pressure or Poisson solve: once the hierarchy
+ * is built, a different theta is refused with CFG_EINVAL.  The momentum
+ * hierarchy always aggregates plainly. */
+int cfg_amg_strength(cfg_ctx* ctx, double theta);
 
 /* ---- diagnostics used by the parity tests (no reference counterpart) ----- */
 

@@ -57,3 +57,51 @@ def test_restated_amg_coarsens_and_preconditions():
     assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1e-10
     _, rep = O.solve("cg", rs, cols, vals, b, np.zeros(A.shape[0]), 1e-10, 20000)
     assert 4 * it < rep.iterations, (it, rep.iterations)
+
+
+def _channel_system(cells=(96, 12, 12), jitter=0.1):
+    """The pressure system of a jittered channel whose cells are 2.5x longer
+    than wide (the 2M-cell channel's aspect): couplings across the channel
+    6.25x those along it; fixed p at the outlet."""
+    import _cases as K
+    names = ["inlet", "outlet", "bottom", "top", "front", "back"]
+    mn, mx = (0.0, 0.0, 0.0), (2.0, 0.1, 0.1)
+    om = O.block_mesh(mn, mx, cells, names, ["wall"] * 6)
+    om = om.with_points(K.jitter_points(om.points, cells, mn, mx, jitter, 7))
+    np_ = len(names)
+    oc = O.Case(om, u_type=["fixedValue"] * np_, u_value=[(0, 0, 0)] * np_,
+                p_type=["fixedValue" if n == "outlet" else "zeroGradient" for n in names],
+                p_value=[0] * np_, nu=1e-4)
+    rs, cols, vals = oc.pressure_csr(np.ones(om.nF))
+    return sp.csr_matrix((vals, cols, rs), shape=(om.nC, om.nC))
+
+
+def test_strength_aggregation_follows_the_strong_couplings():
+    A = _channel_system()
+    plain, strong = R.Hierarchy(A), R.Hierarchy(A, 0.25)
+    # theta 0 is plain aggregation
+    assert R.Hierarchy(A, 0.0).rows == plain.rows
+    agg0, _ = R.aggregate(A.tocsr(), 0.25)
+    # every aggregate of the finest level lies within one cross-section
+    # (cells of one x-index), since couplings along x are weak
+    nx = 96
+    xi = np.arange(A.shape[0]) % nx
+    for a in np.unique(agg0)[:200]:
+        assert np.ptp(xi[agg0 == a]) == 0
+    rng = np.random.default_rng(4)
+    b = rng.standard_normal(A.shape[0])
+    _, it_plain = fcg(A, b, plain.apply, 1e-8)
+    _, it_strong = fcg(A, b, strong.apply, 1e-8)
+    assert 3 * it_strong < 2 * it_plain, (it_strong, it_plain)
+
+
+def test_strength_aggregation_at_least_halves_every_level():
+    # each row's largest coupling is always strong, so every first-phase
+    # aggregate holds its root and at least one neighbour: even theta 1
+    # (only the largest coupling kept) halves each level
+    A = _channel_system((24, 6, 6))
+    for theta in (0.25, 0.5, 1.0):
+        rows = R.Hierarchy(A, theta).rows
+        assert rows[-1] <= R.DENSE_MAX
+        for a, b in zip(rows, rows[1:]):
+            assert 2 * b <= a, (theta, rows)

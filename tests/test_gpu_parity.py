@@ -312,13 +312,15 @@ def test_poiseuille_verification_case_converges_like_the_reference(golden, tmp_p
     assert abs(b["centreline"] / 0.15 - 1.0) < 0.08 and b["flux_err"] < 0.02
 
 
-def test_headline_amg_pressure_fields_match_fp64_oracle():
+@pytest.mark.parametrize("theta", [0.0, 0.25])
+def test_headline_amg_pressure_fields_match_fp64_oracle(theta):
     """The headline's configuration (bench.make_case: the jittered channel,
     the reference's channel relaxation, nonOrth 1, tolerance 1e-8) at 64 x 8
-    x 8 cells, with the FP32-AMG flexible-CG pressure solve, over 12 outer
-    iterations from rest, against the C restatement's FP64 DIC-PCG run of the
-    same iterations: every field within the FP64 bar (relative L2) and no
-    iteration diverged."""
+    x 8 cells, with the FP32-AMG flexible-CG pressure solve (its hierarchy
+    aggregated plainly, theta 0, or by strength of connection, theta 0.25),
+    over 12 outer iterations from rest, against the C restatement's FP64
+    DIC-PCG run of the same iterations: every field within the FP64 bar
+    (relative L2) and no iteration diverged."""
     import bench
     n, iters = 8, 12
     m = K._block((0, 0, 0), bench.LENGTH, bench.dims(n), K.CHANNEL_NAMES, K.CHANNEL_TYPES, bench.JITTER, bench.SEED)
@@ -328,7 +330,7 @@ def test_headline_amg_pressure_fields_match_fp64_oracle():
                 non_orth=1, **bench.RELAX)
     oc.p_precond = 1
     U0, p0, phi0, r0 = oc.run()
-    mesh, case, ctl = bench.make_case(n, 0, "AMG")
+    mesh, case, ctl = bench.make_case(n, 0, "AMG", theta)
     assert np.array_equal(mesh.addressing()["points"], m.points)
     for k in range(iters):
         r = case.solve(ctl)
