@@ -2,11 +2,14 @@
 // the FP64 flexible CG (no reference counterpart: the reference solves its
 // pressure with Jacobi-PCG, Matrix.cpp:153-222).
 //
-// Structure (host, once per mesh): plain aggregation of the matrix graph in
+// Structure (host, once per mesh): aggregation of the matrix graph in
 // device numbering.  Phase 1 visits rows in order and makes a row whose
 // neighbours are all free the root of an aggregate of itself and those
 // neighbours; phase 2 puts every row left over into the aggregate of its
-// first aggregated neighbour.  The coarse operator is the Galerkin product
+// first aggregated neighbour.  Plain aggregation counts every entry as a
+// neighbour; with strength of connection (the pressure hierarchy when its
+// threshold is set) only the strong entries count.  The momentum matrix
+// has a hierarchy of its own, aggregated plainly.  The coarse operator is the Galerkin product
 // P^T A P with the piecewise-constant P, so every coarse entry is a plain
 // sum of fine entries: the host lists, per coarse entry, the fine entries it
 // sums (in a fixed order), and the device forms the values with one gather
