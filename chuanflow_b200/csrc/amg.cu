@@ -9,11 +9,11 @@
 // first aggregated neighbour.  Plain aggregation counts every entry as a
 // neighbour; with strength of connection (the pressure hierarchy when its
 // threshold is set) only the strong entries count.  The momentum matrix
-// has a hierarchy of its own, aggregated plainly.  The coarse operator is the Galerkin product
-// P^T A P with the piecewise-constant P, so every coarse entry is a plain
-// sum of fine entries: the host lists, per coarse entry, the fine entries it
-// sums (in a fixed order), and the device forms the values with one gather
-// kernel per level.  Levels stop at <= 128 rows, whose operator is inverted
+// has a hierarchy of its own, aggregated plainly.  The coarse operator is
+// the Galerkin product P^T A P with the piecewise-constant P, so every
+// coarse entry is a plain sum of fine entries: the host lists, per coarse
+// entry, the fine entries it sums (in a fixed order), and the device forms
+// the values with one gather kernel per level.  Levels stop at <= 128 rows, whose operator is inverted
 // densely on the host (diagonally regularised when singular, as a pure
 // Neumann system is).
 //
@@ -1090,7 +1090,8 @@ std::vector<char> strongEntries(const Pattern& A, const std::vector<double>& v, 
 
 static int tailLevel(const AmgState& a);
 
-/// The hierarchy's structure from the device pressure pattern.
+/// A hierarchy's structure from the device matrix pattern (and, for
+/// strength of connection, the operator's values).
 void Ctx::amgSetup(AmgUse use, const double* vals, double theta)
 {
     const auto t0 = std::chrono::steady_clock::now();
