@@ -159,3 +159,14 @@ def test_case_file_turbulence_block(tmp_path):
                       ("turbulence { model kEpsilon; intensity -1; }", "intensity must be non-negative")):
         with pytest.raises(cf.CfgError, match=re.escape(msg)):
             cf.inspect_case_file(write(tmp_path, base + text + "\n"))
+
+
+def test_amg_strength_refuses_a_null_context():
+    """cfg_amg_strength reports a null context as CFG_EINVAL with its name
+    on the error channel (no device is touched)."""
+    import ctypes as C
+    lib = cf.lib()
+    assert lib.cfg_amg_strength(None, C.c_double(0.25)) == 1
+    buf = C.create_string_buffer(256)
+    lib.cfg_last_error(buf, 256)
+    assert b"cfg_amg_strength" in buf.value
